@@ -1,0 +1,354 @@
+#!/usr/bin/env python3
+"""Closest-hit cast benchmark: Mrays/s on a 1,048,576-triangle displaced sphere.
+
+Workload (one "step"): 16,777,216 rays, origins uniform in [-2, 2]^3, directions uniform on
+the sphere, min_t 0, max_t Ray_max_t, cast closest-hit against the SAH BVH of a tetra-sphere
+(n = 512) displaced by fBm of amplitude 0.1 (6 octaves, seed 1).  Rays (512 MiB) exceed
+the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sprout|reference]
+
+Multi-GPU (torchrun, one process per GPU): every rank casts its own 16,777,216 rays (ray
+indices rank*R .. rank*R+R-1) against its own copy of the tree; no collective touches the
+data path (weak scaling).  NCCL carries only the barrier and the max-over-ranks time.
+
+Prints one JSON line (rank 0).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+MESH_N = 512
+RAYS = 1 << 24
+SEED = 1
+ALGO_BYTES_PER_RAY = 40  # 32 B ray in + 4 B id + 4 B t out
+METRIC = "Mrays/s closest-hit"
+WORKLOAD = "cast: 1,048,576-tri fBm-displaced tetra-sphere (n=512, amp 0.1, seed 1), 16,777,216 rays o~U[-2,2]^3 d~S^2 (seed 1)"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["sprout", "reference"], default="sprout")
+    p.add_argument("--rays", type=int, default=RAYS)
+    p.add_argument("--mesh-n", type=int, default=MESH_N)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per ray of the closest-hit kernel, from the committed ncu summary."""
+    f = ROOT / "profiles" / "cast_closest_hit_ncu.txt"
+    if not f.exists():
+        return None
+    m = re.search(r"dram_bytes_per_ray:\s*([0-9.eE+-]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reference_run(mesh_path, rays_path, steps, warmup):
+    import oracle
+
+    with tempfile.TemporaryDirectory() as tmp:
+        out = os.path.join(tmp, "out.bin")
+        res = subprocess.run([str(oracle.REF_CAST), mesh_path, rays_path, out, "0", "hit", str(steps + warmup)],
+                             capture_output=True, text=True, check=True)
+    return json.loads(res.stdout.strip().splitlines()[-1])
+
+
+def write_inputs(tmp, pos, idx, rays):
+    import oracle
+
+    mesh_path = os.path.join(tmp, "mesh.bin")
+    rays_path = os.path.join(tmp, "rays.bin")
+    oracle.write_mesh(mesh_path, pos, idx)
+    oracle.write_rays(rays_path, rays)
+    return mesh_path, rays_path
+
+
+def cpu_lscpu():
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True).stdout
+        m = re.search(r"Model name:\s*(.+)", out)
+        return m.group(1).strip() if m else "unknown"
+    except OSError:
+        return "unknown"
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    import oracle
+    import sprout_b200 as sb
+
+    if not oracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_cast not built"}))
+        return
+    pos, idx = sb.sphere_mesh(args.mesh_n, 0.1, SEED)
+    rays = sb.random_rays(args.rays, seed=SEED)
+    with tempfile.TemporaryDirectory() as tmp:
+        mesh_path, rays_path = write_inputs(tmp, pos, idx, rays)
+        timing = reference_run(mesh_path, rays_path, args.steps, args.warmup)
+    times = timing["hit_s_list"][args.warmup:]
+    total = sum(times)
+    value = args.rays * len(times) / total / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s",
+        "n_gpus": world, "steps": len(times), "warmup": args.warmup,
+        "ms_per_step": round(1e3 * total / len(times), 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rays_per_step": args.rays, "triangles": int(idx.shape[0]),
+                   "l2": "inputs (rays, 512 MiB) larger than L2"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": timing["threads"],
+                         "kind": "reference", "cpu": cpu_lscpu(),
+                         "sample": f"full workload ({args.rays} rays) per step, reference Builder_SAH(16,64,4) "
+                                   f"tree (build {timing['build_s']:.3f} s, untimed) + Tree::intersect"},
+        "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        return
+
+    import torch
+
+    import sprout_b200 as sb
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    pos, idx = sb.sphere_mesh(args.mesh_n, 0.1, SEED)
+    rays_host = sb.random_rays(args.rays, seed=SEED, first=rank * args.rays)
+
+    tree = sb.Tree()
+    tree.build(pos, idx)
+    info = tree.info()
+
+    stream = torch.cuda.current_stream()
+    d_rays = torch.from_numpy(rays_host).cuda()
+    d_ids = torch.empty(args.rays, dtype=torch.int32, device="cuda")
+    d_t = torch.empty(args.rays, dtype=torch.float32, device="cuda")
+
+    for _ in range(args.warmup):
+        tree.intersect(d_rays, out=(d_ids, d_t, None))
+    barrier()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        barrier()
+        t_begin = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_begin.record(stream)
+        for k in range(args.steps):
+            starts[k].record(stream)
+            tree.intersect(d_rays, out=(d_ids, d_t, None))
+            ends[k].record(stream)
+        t_end.record(stream)
+        barrier()
+    elapsed = t_begin.elapsed_time(t_end) / 1e3
+    kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    if dist is not None:
+        tt = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed = float(tt.item())
+    assert tree.status() == 0
+
+    hit_fraction = float((d_ids != -1).float().mean().item())
+
+    # any-hit throughput (reported beside the headline)
+    d_occ = torch.empty(args.rays, dtype=torch.uint8, device="cuda")
+    for _ in range(2):
+        tree.intersect_p(d_rays, out=d_occ)
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(args.steps):
+        tree.intersect_p(d_rays, out=d_occ)
+    a1.record(stream)
+    torch.cuda.synchronize()
+    any_hit_mrays = args.rays * args.steps / (a0.elapsed_time(a1) / 1e3) / 1e6
+
+    # end to end through the host-pointer entry point: pinned rays in, ids + t out
+    e2e = None
+    if not args.no_e2e:
+        h_rays = torch.from_numpy(rays_host).pin_memory()
+        h_ids = torch.empty(args.rays, dtype=torch.int32).pin_memory()
+        h_t = torch.empty(args.rays, dtype=torch.float32).pin_memory()
+        out = (h_ids.numpy().view(np.uint32), h_t.numpy(), None)
+        rays_np = h_rays.numpy()
+        for _ in range(2):
+            tree.intersect(rays_np, out=out)
+        barrier()
+        e_steps = max(3, args.steps // 2)
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            tree.intersect(rays_np, out=out)
+        e_el = time.perf_counter() - t0
+        if dist is not None:
+            tt = torch.tensor([e_el], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e_el = float(tt.item())
+        e2e = {"value": round(world * args.rays * e_steps / e_el / 1e6, 3), "unit": "Mrays/s",
+               "h2d_bytes_per_step": 32 * args.rays, "d2h_bytes_per_step": 8 * args.rays,
+               "steps": e_steps, "path": "spb_intersect_host (pinned host buffers, 2-stream chunked copies)"}
+
+    value = world * args.rays * args.steps / elapsed / 1e6
+    mean_kernel_s = statistics.mean(kernel_ms) / 1e3
+    peak, peak_kind = measured_peaks()
+    achieved = ALGO_BYTES_PER_RAY * args.rays / mean_kernel_s / 1e9
+    traffic_per_ray = profiled_traffic()
+
+    cpu_baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+
+        if oracle.reference_available():
+            with tempfile.TemporaryDirectory() as tmp:
+                mesh_path, rays_path = write_inputs(tmp, pos, idx, rays_host)
+                timing = reference_run(mesh_path, rays_path, 2, 1)
+            t_cpu = statistics.mean(timing["hit_s_list"][1:])
+            cpu_baseline = {"value": round(args.rays / t_cpu / 1e6, 3), "unit": "Mrays/s",
+                            "cores": timing["threads"], "kind": "reference", "cpu": cpu_lscpu(),
+                            "sample": f"full workload ({args.rays} rays), reference Builder_SAH(16,64,4) + "
+                                      f"Tree::intersect on all host threads, mean of 2 passes"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * elapsed / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "rays_per_step_per_gpu": args.rays,
+                       "triangles": info["num_triangles"], "bvh_nodes": info["num_nodes"],
+                       "bvh_depth": info["max_depth"], "build_s": round(info["build_seconds"], 3),
+                       "parallelism": f"replicas x{world} (independent ray ranges)",
+                       "l2": "inputs (rays, 512 MiB) larger than L2; no flush",
+                       "hit_fraction": round(hit_fraction, 5)},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 5), "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_ray": ALGO_BYTES_PER_RAY,
+                         "kernel_ms_mean": round(1e3 * mean_kernel_s, 4),
+                         "traffic": (round(traffic_per_ray * args.rays) if traffic_per_ray else None),
+                         "note": "traversal is L1/L2-latency bound; HBM carries only rays and results"},
+            "any_hit_mrays_s": round(world * any_hit_mrays, 3),
+            "e2e": e2e,
+            "cpu_baseline": cpu_baseline,
+            "gpu_launches": args.steps,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line))
+
+    tree.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

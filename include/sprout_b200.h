@@ -1,0 +1,149 @@
+/*
+ * sprout_b200 — C ABI of the B200 ray-cast path (closest hit / any hit over an SAH BVH).
+ *
+ * This library replaces the reference's per-ray triangle-mesh traversal with a batched
+ * GPU cast.  Each entry point names the reference interface it stands in for
+ * (paths are relative to the reference project, Opioid/sprout).
+ *
+ * Conventions
+ *   - Every function returns int32_t: 0 on success, SPB_ERROR_ARGUMENT (-1) for a bad
+ *     argument (null pointer, size out of range), SPB_ERROR_STATE (-2) for a call that is
+ *     not valid in the object's current state (e.g. casting before a build), and
+ *     SPB_ERROR_CUDA (-3) when a CUDA call fails.  These mirror the reference capi's codes
+ *     (source/capi/capi.cpp:112-131: -1 no engine / bad argument, -2 invalid state).
+ *     spb_last_error() returns a readable message for the last failure on this thread.
+ *   - A ray is 8 floats, exactly the reference's math::ray storage order
+ *     (source/base/math/ray.hpp:8-28, ray.inl:11-16): origin.xyz, min_t, direction.xyz,
+ *     max_t.  Rays are read-only.
+ *   - Results are per ray: the caller's triangle index of the closest hit
+ *     (SPB_MISS = 0xFFFFFFFF for no hit), the hit distance t (the ray's max_t after the
+ *     call: the hit t, or the unchanged max_t on a miss, as the reference leaves
+ *     ray.max_t()), and optionally the barycentrics u, v of the hit.
+ *   - "_device" entry points take device pointers and a cudaStream_t (passed as void*,
+ *     NULL = the legacy default stream) and are asynchronous with respect to the host.
+ *     "_host" entry points take host pointers (pinned or pageable), copy the rays to the
+ *     GPU in chunks, cast, copy the results back and return when they are in host memory.
+ *   - Calls on one tree must not overlap on the GPU (they share the tree's work counter):
+ *     issue them on one stream, or synchronize between streams.  Different trees are
+ *     independent.  Like the reference engine, a tree object is not re-entrant from
+ *     several host threads.
+ */
+#ifndef SPROUT_B200_H
+#define SPROUT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define SPB_API __declspec(dllexport)
+#else
+#define SPB_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPB_OK 0
+#define SPB_ERROR_ARGUMENT -1
+#define SPB_ERROR_STATE -2
+#define SPB_ERROR_CUDA -3
+
+#define SPB_MISS 0xFFFFFFFFu
+
+/* Largest batch one call accepts (ray indices are 32-bit on the device). */
+#define SPB_MAX_RAYS_PER_CALL 0x7FFFFFFFull
+
+typedef struct spb_tree spb_tree;
+
+typedef struct spb_tree_info {
+    uint32_t num_triangles;   /* triangles given to spb_tree_build */
+    uint32_t num_nodes;       /* 8-wide nodes (80 bytes each) */
+    uint32_t num_leaves;      /* leaf slots (1-3 triangles each) */
+    uint32_t max_depth;       /* deepest node, root = 1 */
+    uint64_t device_bytes;    /* nodes + triangles resident on the device */
+    double   build_seconds;   /* host build + upload time of the last build */
+    double   sah_cost;        /* SAH cost of the 8-wide tree (traversal 1, triangle 1) */
+} spb_tree_info;
+
+/* Readable message for the last error on the calling thread ("" if none). */
+SPB_API char const* spb_last_error(void);
+
+/* Library version string. */
+SPB_API char const* spb_version(void);
+
+/*
+ * Create / release a tree bound to the current CUDA device.
+ * Replaces constructing scene::shape::triangle::bvh::Tree
+ * (source/core/scene/shape/triangle/bvh/triangle_bvh_tree.cpp:15-20).
+ */
+SPB_API int32_t spb_tree_create(spb_tree** tree);
+SPB_API int32_t spb_tree_release(spb_tree* tree);
+
+/*
+ * Build the BVH over an indexed triangle mesh and upload it.
+ * positions: num_vertices * 3 floats (host); indices: num_triangles * 3 uint32 (host).
+ * Replaces bvh::Builder_SAH(16, 64, 4).build(tree, ...)
+ * (source/core/scene/shape/triangle/triangle_mesh_provider.cpp:375-378,
+ *  source/core/scene/shape/triangle/bvh/triangle_bvh_builder_sah.cpp:21-67).
+ * num_threads: host build threads (0 = all hardware threads).
+ */
+SPB_API int32_t spb_tree_build(spb_tree* tree, uint32_t num_vertices, uint32_t num_triangles,
+                               float const* positions, uint32_t const* indices,
+                               uint32_t num_threads);
+
+SPB_API int32_t spb_tree_info_get(spb_tree const* tree, spb_tree_info* info);
+
+/*
+ * Closest hit for a batch of rays (device pointers).
+ * Replaces Tree::intersect (source/core/scene/shape/triangle/bvh/triangle_bvh_tree.cpp:41-90)
+ * called once per ray.  ids and ts are required; uvs (2 floats per ray) may be NULL.
+ */
+SPB_API int32_t spb_intersect_device(spb_tree* tree, float const* rays, uint64_t num_rays,
+                                     uint32_t* ids, float* ts, float* uvs, void* stream);
+
+/*
+ * Any hit (occlusion) for a batch of rays (device pointers): occluded[i] = 1 if some
+ * triangle is hit with min_t <= t <= max_t, else 0.
+ * Replaces Tree::intersect_p (source/core/scene/shape/triangle/bvh/triangle_bvh_tree.cpp:145-185).
+ */
+SPB_API int32_t spb_intersect_p_device(spb_tree* tree, float const* rays, uint64_t num_rays,
+                                       uint8_t* occluded, void* stream);
+
+/* Host-memory forms of the two calls above (copies and cast pipelined over streams). */
+SPB_API int32_t spb_intersect_host(spb_tree* tree, float const* rays, uint64_t num_rays,
+                                   uint32_t* ids, float* ts, float* uvs);
+SPB_API int32_t spb_intersect_p_host(spb_tree* tree, float const* rays, uint64_t num_rays,
+                                     uint8_t* occluded);
+
+/*
+ * Device-side status of the last cast on this tree: number of rays whose traversal
+ * stack would have overflowed (always 0 for trees this library builds; the kernel checks
+ * and drops such rays instead of writing out of bounds).  Synchronizes the tree's stream.
+ */
+SPB_API int32_t spb_tree_status(spb_tree* tree, uint32_t* overflowed_rays);
+
+/*
+ * Synthetic inputs of the cast benchmark (deterministic, host memory).
+ *
+ * spb_synth_sphere_mesh: a tetrahedron whose faces are subdivided n x n, projected to the
+ * unit sphere and displaced radially by amplitude * fBm (6 octaves, lacunarity 2, gain 0.5,
+ * gradient noise seeded by seed).  4 n^2 triangles, 2 n^2 + 2 vertices; every vertex has
+ * valence <= 6.  Pass NULL buffers to query the sizes only.
+ *
+ * spb_synth_rays: ray i (i = first .. first + count - 1) draws from a PCG32 stream
+ * (sequence i, state seed): origin uniform in [-extent, extent]^3, direction uniform on the
+ * unit sphere, min_t = 0, max_t = 3.4027715e38 (the reference's scene::Ray_max_t,
+ * source/core/scene/scene_constants.hpp:10).
+ */
+SPB_API int32_t spb_synth_sphere_mesh(uint32_t n, float amplitude, uint32_t seed,
+                                      uint32_t* num_vertices, uint32_t* num_triangles,
+                                      float* positions, uint32_t* indices);
+SPB_API int32_t spb_synth_rays(uint64_t first, uint64_t count, uint32_t seed, float extent,
+                               float* rays, uint32_t num_threads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

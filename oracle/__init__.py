@@ -1,0 +1,123 @@
+"""Checkers for the sprout_b200 ray cast.  TEST INFRASTRUCTURE ONLY.
+
+* :func:`restated_cast` -- the C restatement in ``cast_oracle.c`` (libcast_oracle.so).
+* :func:`reference_cast` -- the reference's own Builder_SAH + Tree::intersect/intersect_p,
+  compiled from the reference sources into ``_ref/ref_cast`` by ``Makefile``.
+
+Only tests, the smoke check and the bench's CPU-baseline leg use this package.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import pathlib
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "libcast_oracle.so"
+REF_CAST = HERE / "_ref" / "ref_cast"
+
+MODE_CLOSEST = 1
+MODE_ANY = 2
+MODE_BRUTE = 4
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not ORACLE_LIB.exists():
+            raise ImportError(f"{ORACLE_LIB} missing: run sprout_b200.build.build_oracle()")
+        lib = ctypes.CDLL(str(ORACLE_LIB))
+        lib.oracle_cast.restype = ctypes.c_int32
+        lib.oracle_cast.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int32]
+        lib.oracle_triangle_test.restype = ctypes.c_int32
+        lib.oracle_triangle_test.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_float, ctypes.c_void_p]
+        _lib = lib
+    return _lib
+
+
+def triangle_test(ray, a, b, c, tmax=None):
+    """One restated Möller-Trumbore test: (passes, t, u, v)."""
+    lib = _load()
+    r = np.ascontiguousarray(ray, np.float32).reshape(8)
+    pa, pb, pc = (np.ascontiguousarray(x, np.float32).reshape(3) for x in (a, b, c))
+    out = np.zeros(3, np.float32)
+    tm = float(r[7]) if tmax is None else float(tmax)
+    ok = lib.oracle_triangle_test(r.ctypes.data, pa.ctypes.data, pb.ctypes.data, pc.ctypes.data, tm,
+                                  out.ctypes.data)
+    return bool(ok), float(out[0]), float(out[1]), float(out[2])
+
+
+def restated_cast(positions, indices, rays, closest=True, any_hit=True, brute=False, threads=0):
+    """Returns dict with ids, t, uv (closest) and occluded (any hit)."""
+    lib = _load()
+    pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+    idx = np.ascontiguousarray(indices, np.uint32).reshape(-1, 3)
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    n = r.shape[0]
+    ids = np.empty(n, np.uint32)
+    ts = np.empty(n, np.float32)
+    uv = np.empty((n, 2), np.float32)
+    occ = np.empty(n, np.uint8)
+    mode = (MODE_CLOSEST if closest else 0) | (MODE_ANY if any_hit else 0) | (MODE_BRUTE if brute else 0)
+    threads = threads or os.cpu_count() or 1
+    st = lib.oracle_cast(pos.shape[0], idx.shape[0], pos.ctypes.data, idx.ctypes.data, n, r.ctypes.data,
+                         ids.ctypes.data, ts.ctypes.data, uv.ctypes.data, occ.ctypes.data, threads, mode)
+    if st != 0:
+        raise ValueError("oracle_cast rejected its arguments")
+    out = {}
+    if closest:
+        out.update(ids=ids, t=ts, uv=uv)
+    if any_hit:
+        out["occluded"] = occ
+    return out
+
+
+def reference_available() -> bool:
+    return REF_CAST.exists()
+
+
+def write_mesh(path, positions, indices):
+    pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+    idx = np.ascontiguousarray(indices, np.uint32).reshape(-1, 3)
+    with open(path, "wb") as f:
+        f.write(np.array([pos.shape[0], idx.shape[0]], np.uint32).tobytes())
+        f.write(pos.tobytes())
+        f.write(idx.tobytes())
+
+
+def write_rays(path, rays):
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    with open(path, "wb") as f:
+        f.write(np.array([r.shape[0]], np.uint64).tobytes())
+        f.write(r.tobytes())
+
+
+def reference_cast(positions, indices, rays, threads=0, mode="both", workdir=None):
+    """Runs the compiled reference; returns dict(ids, t, occluded, timing)."""
+    if not REF_CAST.exists():
+        raise FileNotFoundError(f"{REF_CAST} missing: build it with `make -C oracle`")
+    n = int(np.asarray(rays).reshape(-1, 8).shape[0])
+    with tempfile.TemporaryDirectory(dir=workdir) as tmp:
+        mesh_p = os.path.join(tmp, "mesh.bin")
+        rays_p = os.path.join(tmp, "rays.bin")
+        out_p = os.path.join(tmp, "out.bin")
+        write_mesh(mesh_p, positions, indices)
+        write_rays(rays_p, rays)
+        res = subprocess.run([str(REF_CAST), mesh_p, rays_p, out_p, str(threads), mode],
+                             capture_output=True, text=True, check=True)
+        timing = json.loads(res.stdout.strip().splitlines()[-1])
+        raw = np.fromfile(out_p, np.uint8)
+    ids = raw[: 4 * n].view(np.uint32)
+    ts = raw[4 * n: 8 * n].view(np.float32)
+    occ = raw[8 * n: 9 * n]
+    return {"ids": ids.copy(), "t": ts.copy(), "occluded": occ.copy(), "timing": timing}

@@ -1,0 +1,63 @@
+// Host-side BVH construction for the GPU cast: binned-SAH binary tree, greedy collapse to an
+// 8-wide tree, and encoding into 80-byte nodes with 8-bit quantized child boxes.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace spb {
+
+// One 8-wide node, 80 bytes = 5 x 16-byte words (loaded with five 128-bit loads).
+//   w0: origin.xyz (float), exponents ex|ey|ez (biased by 127, one byte each) | imask << 24
+//   w1: child_base, tri_base, meta[0..3], meta[4..7]
+//   w2: qlo_x[0..7], qlo_y[0..7]
+//   w3: qlo_z[0..7], qhi_x[0..7]
+//   w4: qhi_y[0..7], qhi_z[0..7]
+// Child slot i has the box origin + [qlo, qhi] * 2^(e - 127) per axis.  imask bit i marks an
+// internal child.  meta[i]: 0 = empty slot; internal child = 0b001 << 5 | (24 + i);
+// leaf = unary(triangle count) << 5 | offset, the leaf's triangles being
+// tri_base + offset .. tri_base + offset + count - 1 (count 1..3, offset 0..23).
+// Internal children are stored contiguously from child_base in slot order.
+struct alignas(16) Wide_node {
+    float    origin[3];
+    uint8_t  exponent[3];
+    uint8_t  imask;
+    uint32_t child_base;
+    uint32_t tri_base;
+    uint8_t  meta[8];
+    uint8_t  qlo[3][8];
+    uint8_t  qhi[3][8];
+};
+static_assert(sizeof(Wide_node) == 80, "Wide_node must be 80 bytes");
+
+// One triangle, 48 bytes: vertex a, edges b - a and c - a (exactly the values the
+// Möller-Trumbore test computes first), and the caller's triangle index.
+struct alignas(16) Wide_triangle {
+    float    a[3];
+    uint32_t id;
+    float    e1[3];
+    uint32_t pad0;
+    float    e2[3];
+    uint32_t pad1;
+};
+static_assert(sizeof(Wide_triangle) == 48, "Wide_triangle must be 48 bytes");
+
+struct Wide_bvh {
+    std::vector<Wide_node>     nodes;
+    std::vector<Wide_triangle> triangles;
+    uint32_t                   num_leaves = 0;
+    uint32_t                   max_depth  = 0;
+    double                     sah_cost   = 0.;
+    float                      pad        = 0.f;  // spatial padding applied to every child box
+};
+
+// Deepest tree the traversal kernels accept (their stack holds one entry per level).
+constexpr uint32_t Max_wide_depth = 48;
+
+// Builds the 8-wide tree.  Returns false (with a message) if the input is unusable.
+bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* positions,
+                    uint32_t const* indices, uint32_t num_threads, Wide_bvh& out,
+                    std::string& error);
+
+}  // namespace spb

@@ -1,0 +1,97 @@
+"""The C ABI: every symbol declared in include/*.h is exported, and argument errors are
+reported with the documented codes without touching a GPU."""
+
+import ctypes
+import pathlib
+import re
+import subprocess
+
+import numpy as np
+
+import sprout_b200 as sb
+from sprout_b200 import _lib
+
+INCLUDE = pathlib.Path(__file__).resolve().parent.parent / "include"
+
+
+def declared_symbols():
+    names = set()
+    for header in INCLUDE.glob("*.h"):
+        text = header.read_text()
+        names |= set(re.findall(r"SPB_API\s+[\w\s\*]+?\b(spb_\w+)\s*\(", text))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    assert {"spb_tree_create", "spb_tree_build", "spb_intersect_device", "spb_intersect_p_device",
+            "spb_intersect_host", "spb_intersect_p_host"} <= names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.LIBRARY_PATH)], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    missing = declared_symbols() - exported
+    assert not missing, f"declared but not exported: {sorted(missing)}"
+    for name in declared_symbols():
+        assert hasattr(lib, name)
+    # the ctypes prototypes cover the whole header
+    assert declared_symbols() <= set(_lib.PROTOTYPES)
+
+
+def test_argument_errors_use_documented_codes():
+    lib = _lib.load()
+    assert lib.spb_tree_create(None) == _lib.SPB_ERROR_ARGUMENT
+    assert b"null" in lib.spb_last_error()
+    assert lib.spb_tree_build(None, 3, 1, None, None, 0) == _lib.SPB_ERROR_ARGUMENT
+    assert lib.spb_intersect_device(None, None, 0, None, None, None, None) == _lib.SPB_ERROR_ARGUMENT
+    assert lib.spb_intersect_p_host(None, None, 0, None) == _lib.SPB_ERROR_ARGUMENT
+    assert lib.spb_tree_release(None) == _lib.SPB_ERROR_ARGUMENT
+    nv, nt = ctypes.c_uint32(), ctypes.c_uint32()
+    assert lib.spb_synth_sphere_mesh(0, 0.1, 1, ctypes.byref(nv), ctypes.byref(nt), None, None) == \
+        _lib.SPB_ERROR_ARGUMENT
+
+
+def test_no_silent_cpu_fallback_without_gpu():
+    """Creating a tree needs CUDA; without a usable GPU the call fails loudly."""
+    import torch
+
+    if torch.cuda.is_available():
+        return
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    assert lib.spb_tree_create(ctypes.byref(h)) == _lib.SPB_ERROR_CUDA
+    try:
+        sb.Tree()
+    except sb.SproutError as e:
+        assert e.code == _lib.SPB_ERROR_CUDA
+    else:
+        raise AssertionError("Tree() must fail without a GPU")
+
+
+def test_synthetic_mesh_is_closed_and_deterministic():
+    pos, idx = sb.sphere_mesh(16, 0.1, 1)
+    assert idx.shape == (4 * 16 * 16, 3) and pos.shape == (2 * 16 * 16 + 2, 3)
+    pos2, idx2 = sb.sphere_mesh(16, 0.1, 1)
+    assert np.array_equal(pos, pos2) and np.array_equal(idx, idx2)
+    edges = np.sort(np.concatenate([idx[:, [0, 1]], idx[:, [1, 2]], idx[:, [2, 0]]]), axis=1)
+    _, counts = np.unique(edges, axis=0, return_counts=True)
+    assert (counts == 2).all()  # every edge shared by exactly two triangles
+    valence = np.bincount(idx.ravel(), minlength=len(pos))
+    assert valence.max() <= 6
+    r = np.linalg.norm(pos, axis=1)
+    assert 0.85 < r.min() and r.max() < 1.15
+
+
+def test_synthetic_rays():
+    rays = sb.random_rays(100000, seed=1)
+    assert np.all(np.abs(rays[:, :3]) <= 2.0)
+    assert np.allclose(np.linalg.norm(rays[:, 4:7], axis=1), 1.0, atol=1e-6)
+    assert np.all(rays[:, 3] == 0) and np.all(rays[:, 7] == np.float32(3.4027715434167032e38))
+    # the stream of ray i does not depend on the batch it is generated in
+    part = sb.random_rays(100, seed=1, first=500)
+    assert np.array_equal(part, rays[500:600])
+    # directions are isotropic: mean close to zero
+    assert np.abs(rays[:, 4:7].mean(axis=0)).max() < 0.01

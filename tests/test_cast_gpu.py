@@ -1,0 +1,188 @@
+"""GPU cast parity: the sm_100a kernels against the CPU restatement (bit-exact ids, t, u, v
+and occlusion) and against the reference's golden answers (edge/tie disagreements only),
+through the C ABI on both its host-pointer and device-pointer entry points."""
+
+import json
+import pathlib
+
+import numpy as np
+import pytest
+
+import oracle
+import sprout_b200 as sb
+from cases import MISS, classify_mismatches, edge_rays
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = pathlib.Path(__file__).resolve().parent / "golden" / "cast_reference.npz"
+CASES = {"sphere32": (32, 65536, 7, True), "sphere128": (128, 16384, 9, True),
+         "bench512": (512, 16384, 1, False)}
+
+
+def _inputs(name):
+    n, count, seed, with_edges = CASES[name]
+    pos, idx = sb.sphere_mesh(n, 0.1, 1)
+    rays = sb.random_rays(count, seed=seed)
+    if with_edges:
+        rays = np.concatenate([rays, edge_rays(pos, idx)])
+    return pos, idx, rays
+
+
+def _bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+def assert_exact(got_ids, got_t, want):
+    bad = np.nonzero(got_ids != want["ids"])[0]
+    assert bad.size == 0, f"{bad.size} id mismatches, first rays {bad[:8]}"
+    assert np.array_equal(_bits(got_t), _bits(want["t"]))
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+
+    assert torch.cuda.is_available(), "GPU tests need CUDA"
+    return torch
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_host_path_bit_exact_vs_restatement(name):
+    pos, idx, rays = _inputs(name)
+    want = oracle.restated_cast(pos, idx, rays)
+    with sb.Tree() as tree:
+        tree.build(pos, idx)
+        ids, t, uv = tree.intersect(rays, want_uv=True)
+        occ = tree.intersect_p(rays)
+        assert tree.status() == 0
+    assert_exact(ids, t, want)
+    hit = ids != MISS
+    assert np.array_equal(_bits(uv[hit]), _bits(want["uv"][hit]))
+    assert np.array_equal(occ, want["occluded"])
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_against_reference_golden(name):
+    data = np.load(GOLDEN)
+    pos, idx, rays = _inputs(name)
+    with sb.Tree() as tree:
+        tree.build(pos, idx)
+        ids, t = tree.intersect(rays)
+        occ = tree.intersect_p(rays)
+    ref_ids, ref_t, ref_occ = data[f"{name}_ids"], data[f"{name}_t"], data[f"{name}_occ"]
+    explained, unexplained = classify_mismatches(pos, idx, rays, ref_ids, ref_t, ids, t, oracle.triangle_test)
+    assert unexplained == []
+    count = CASES[name][1]
+    assert sum(1 for i in explained if i < count) <= max(2, 1e-4 * count)
+    same = ref_ids == ids
+    ulps = np.abs(ref_t[same].view(np.int32).astype(np.int64) - t[same].view(np.int32))
+    assert ulps.max() <= 2
+    occ_diff = np.nonzero(ref_occ != occ)[0]
+    assert set(occ_diff.tolist()) <= set(explained)
+
+
+def test_device_path_matches_host_path(torch_cuda):
+    torch = torch_cuda
+    pos, idx, rays = _inputs("sphere128")
+    with sb.Tree() as tree:
+        tree.build(pos, idx)
+        h_ids, h_t, h_uv = tree.intersect(rays, want_uv=True)
+        h_occ = tree.intersect_p(rays)
+        d_rays = torch.from_numpy(rays).cuda()
+        side = torch.cuda.Stream()
+        with torch.cuda.stream(side):
+            d_ids, d_t, d_uv = tree.intersect(d_rays, want_uv=True)
+            d_occ = tree.intersect_p(d_rays)
+        side.synchronize()
+    assert np.array_equal(d_ids.cpu().numpy().view(np.uint32), h_ids)
+    assert np.array_equal(_bits(d_t.cpu().numpy()), _bits(h_t))
+    assert np.array_equal(_bits(d_uv.cpu().numpy()), _bits(h_uv))
+    assert np.array_equal(d_occ.cpu().numpy(), h_occ)
+
+
+def test_benchmark_size_properties(torch_cuda):
+    """Full benchmark size (1,048,576 triangles, 16,777,216 rays): size-independent checks
+    over every ray plus bit-exact agreement with the restatement on a 131,072-ray sample."""
+    torch = torch_cuda
+    pos, idx = sb.sphere_mesh(512, 0.1, 1)
+    n = 1 << 24
+    rays = sb.random_rays(n, seed=1)
+    with sb.Tree() as tree:
+        tree.build(pos, idx)
+        info = tree.info()
+        assert info["num_triangles"] == 1 << 20 and info["max_depth"] <= 48
+        d_rays = torch.from_numpy(rays).cuda()
+        ids, t = tree.intersect(d_rays)
+        occ = tree.intersect_p(d_rays)
+        torch.cuda.synchronize()
+        assert tree.status() == 0
+    ids = ids.cpu().numpy().view(np.uint32)
+    t = t.cpu().numpy()
+    occ = occ.cpu().numpy()
+    hit = ids != MISS
+    # any hit over [min_t, max_t] exists exactly when a closest hit exists
+    assert np.array_equal(occ == 1, hit)
+    assert 0.13 < hit.mean() < 0.18
+    assert np.all(ids[hit] < (1 << 20))
+    assert np.all(t[hit] >= 0) and np.all(t[hit] < 8.0)
+    assert np.all(t[~hit] == rays[~hit, 7])
+    # hit points lie on the displaced sphere (radius within [0.9, 1.1] up to rounding)
+    p = rays[hit, :3] + t[hit, None] * rays[hit, 4:7]
+    r = np.linalg.norm(p, axis=1)
+    assert r.min() > 0.89 and r.max() < 1.11
+    sample = np.random.default_rng(0).choice(n, 131072, replace=False)
+    want = oracle.restated_cast(pos, idx, rays[sample])
+    assert np.array_equal(ids[sample], want["ids"])
+    assert np.array_equal(_bits(t[sample]), _bits(want["t"]))
+    assert np.array_equal(occ[sample], want["occluded"])
+
+
+def test_empty_batch_and_state_errors():
+    pos, idx = sb.sphere_mesh(4, 0.1, 1)
+    with sb.Tree() as tree:
+        with pytest.raises(sb.SproutError) as e:
+            tree.intersect(np.zeros((1, 8), np.float32))
+        assert e.value.code == -2  # not built yet
+        with pytest.raises(sb.SproutError) as e:
+            tree.build(pos, np.array([[0, 1, 10**6]], np.uint32))
+        assert e.value.code == -1
+        tree.build(pos, idx)
+        ids, t = tree.intersect(np.zeros((0, 8), np.float32))
+        assert ids.size == 0 and t.size == 0
+        assert tree.intersect_p(np.zeros((0, 8), np.float32)).size == 0
+
+
+def test_single_and_duplicate_triangles():
+    pos = np.array([[-1, -1, 0], [1, -1, 0], [0, 1, 0]], np.float32)
+    rays = np.array([[0, 0, -1, 0, 0, 0, 1, 10],      # hits at t = 1
+                     [0, 0, -1, 0, 0, 0, 1, 0.5],     # max_t too short
+                     [0, 0, -1, 1.5, 0, 0, 1, 10],    # min_t past the hit
+                     [5, 5, -1, 0, 0, 0, 1, 10],      # misses
+                     [0, 0, 0, 0, 1, 0, 0, 10]], np.float32)  # in the plane: det = 0
+    for tris in ([[0, 1, 2]], [[0, 1, 2], [0, 1, 2], [0, 1, 2]]):
+        idx = np.array(tris, np.uint32)
+        want = oracle.restated_cast(pos, idx, rays, brute=True)
+        with sb.Tree() as tree:
+            tree.build(pos, idx)
+            ids, t = tree.intersect(rays)
+            occ = tree.intersect_p(rays)
+        assert_exact(ids, t, want)
+        assert np.array_equal(occ, want["occluded"])
+        assert ids[0] == 0 and t[0] == 1.0
+
+
+def test_degenerate_and_clustered_triangles():
+    rng = np.random.default_rng(4)
+    pos = rng.normal(size=(3000, 3)).astype(np.float32)
+    pos[:500] = pos[0]                      # 500 coincident vertices
+    pos[500:1000, 2] = 0.25                 # a flat sheet
+    idx = rng.integers(0, 3000, size=(5000, 3)).astype(np.uint32)
+    idx[:200] = [0, 1, 2]                   # zero-area triangles (all three vertices equal)
+    rays = np.concatenate([sb.random_rays(40000, seed=2, extent=3.0), edge_rays(pos, idx[200:])])
+    want = oracle.restated_cast(pos, idx, rays, brute=True)
+    with sb.Tree() as tree:
+        tree.build(pos, idx)
+        ids, t = tree.intersect(rays)
+        occ = tree.intersect_p(rays)
+    assert_exact(ids, t, want)
+    assert np.array_equal(occ, want["occluded"])
