@@ -15,6 +15,12 @@
  *     the current hit when its t is <= the current max_t, and max_t shrinks to that t;
  *   - the any-hit loop of Tree::intersect_p (triangle_bvh_tree.cpp:145-185).
  *
+ * A triangle counts as hit only when, in addition, the hit point o + t * d (fmaf per axis)
+ * lies within the triangle's bounds (a, a + (b - a), a + (c - a)) widened by the hit margin
+ * 2^-17 * max(scene extent, largest |coordinate|).  This never rejects a genuine hit; it
+ * removes the rounding noise the test returns for zero-area triangles, whose "hits" can lie
+ * anywhere along the ray (the reference's answer for those depends on its tree).
+ *
  * Two deliberate, documented differences from the compiled reference:
  *   1. 1/det is the IEEE quotient 1.0f/det.  The reference uses rcpss plus one Newton step
  *      (source/base/math/scalar.inl:67-71), whose result depends on the CPU vendor's rcp
@@ -28,6 +34,7 @@
  *
  * Build: gcc -O2 -ffp-contract=off -fPIC -shared -pthread cast_oracle.c -o libcast_oracle.so -lm
  */
+#include <float.h>
 #include <math.h>
 #include <pthread.h>
 #include <stdint.h>
@@ -55,6 +62,7 @@ typedef struct {
     double* bhi;
     uint32_t num_nodes;
     double pad;
+    float margin;
 } Tree;
 
 typedef struct {
@@ -102,6 +110,46 @@ static int mt_test(float const* ray, float const* a, float const* b, float const
 
     return (*u >= 0.f) & (*u <= 1.f) & (*v >= 0.f) & (uv <= 1.f) & (*t >= ray[3]) &
            (*t <= tmax);
+}
+
+static int within_bounds(float const* ray, float const* a, float const* b, float const* c,
+                         float t, float margin) {
+    int inside = 1;
+    for (int k = 0; k < 3; ++k) {
+        float const e1 = b[k] - a[k];
+        float const e2 = c[k] - a[k];
+        float const vb = a[k] + e1;
+        float const vc = a[k] + e2;
+        float const p = fmaf(t, ray[4 + k], ray[k]);
+        float lo = a[k] < vb ? a[k] : vb;
+        float hi = a[k] > vb ? a[k] : vb;
+        lo = vc < lo ? vc : lo;
+        hi = vc > hi ? vc : hi;
+        inside &= (p >= lo - margin) & (p <= hi + margin);
+    }
+    return inside;
+}
+
+/* The mesh's hit margin: 2^-17 * max(extent, magnitude) of the float vertex bounds. */
+static float hit_margin_of(uint32_t num_triangles, float const* pos, uint32_t const* idx) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY};
+    float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (uint64_t i = 0; i < 3 * (uint64_t)num_triangles; ++i) {
+        float const* p = pos + 3 * (size_t)idx[i];
+        for (int k = 0; k < 3; ++k) {
+            if (p[k] < lo[k]) lo[k] = p[k];
+            if (p[k] > hi[k]) hi[k] = p[k];
+        }
+    }
+    double extent = 0.0, magnitude = 0.0;
+    for (int k = 0; k < 3; ++k) {
+        double const e = (double)hi[k] - (double)lo[k];
+        if (e > extent) extent = e;
+        if (fabs((double)lo[k]) > magnitude) magnitude = fabs((double)lo[k]);
+        if (fabs((double)hi[k]) > magnitude) magnitude = fabs((double)hi[k]);
+    }
+    float const m = (float)ldexp(extent > magnitude ? extent : magnitude, -17);
+    return m > FLT_MIN ? m : FLT_MIN;
 }
 
 static void tri_verts(Tree const* tr, uint32_t i, float const** a, float const** b,
@@ -216,7 +264,8 @@ static void cast_one(Tree const* tr, float const* ray, int any, int brute, uint3
             float const *a, *b, *c;
             float t, u, v;
             tri_verts(tr, i, &a, &b, &c);
-            if (mt_test(ray, a, b, c, tbest, &t, &u, &v)) {
+            if (mt_test(ray, a, b, c, tbest, &t, &u, &v) &&
+                within_bounds(ray, a, b, c, t, tr->margin)) {
                 if (any) {
                     best = i;
                     break;
@@ -251,7 +300,8 @@ static void cast_one(Tree const* tr, float const* ray, int any, int brute, uint3
                     float const *a, *b, *c;
                     float t, u, v;
                     tri_verts(tr, i, &a, &b, &c);
-                    if (mt_test(ray, a, b, c, tbest, &t, &u, &v)) {
+                    if (mt_test(ray, a, b, c, tbest, &t, &u, &v) &&
+                within_bounds(ray, a, b, c, t, tr->margin)) {
                         if (any) {
                             best = i;
                             sp = 0;
@@ -324,6 +374,7 @@ int32_t oracle_cast(uint32_t num_vertices, uint32_t num_triangles, float const* 
     tr.num_tris = num_triangles;
     tr.pos = positions;
     tr.idx = indices;
+    tr.margin = hit_margin_of(num_triangles, positions, indices);
 
     if (!(mode & 4)) {
         tr.nodes = (Node*)malloc(sizeof(Node) * 2 * (size_t)num_triangles);

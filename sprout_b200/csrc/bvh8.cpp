@@ -11,8 +11,8 @@
 //    the order o, o^1, o^2, ... (Ylitie, Karras and Laine, "Efficient Incoherent Ray Traversal
 //    on GPUs Through Compressed Wide BVHs", HPG 2017, whose node encoding this follows).
 // 4. Child boxes are padded by a small absolute margin and quantized outward to 8 bits, so
-//    every stored box contains the exact triangle bounds with room for the rounding of the
-//    traversal's slab arithmetic.
+//    every stored box contains the triangle bounds widened by the hit margin (see cast.cu),
+//    with room for the rounding of the traversal's slab arithmetic.
 #include "bvh8.hpp"
 
 #include <algorithm>
@@ -295,6 +295,11 @@ float round_down(double x) {
 
 }  // namespace
 
+float hit_margin_for(double extent, double magnitude) {
+    float const m = float(std::ldexp(std::max(extent, magnitude), -17));
+    return m > std::numeric_limits<float>::min() ? m : std::numeric_limits<float>::min();
+}
+
 bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* positions,
                     uint32_t const* indices, uint32_t num_threads, Wide_bvh& out,
                     std::string& error) {
@@ -348,9 +353,11 @@ bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* 
         magnitude = std::max({magnitude, std::fabs(double(root_box.lo[a])),
                               std::fabs(double(root_box.hi[a]))});
     }
-    // Margin for the traversal's slab rounding: 2^-16 of the scene size.
-    double const pad = std::ldexp(std::max(extent, magnitude), -16) + 1e-30;
-    out.pad          = float(pad);
+    // A hit counts only if its point lies within the triangle's bounds widened by
+    // hit_margin (2^-17 of the scene size); child boxes are widened by twice that, which
+    // leaves hit_margin of room for the rounding of the traversal's slab arithmetic.
+    out.hit_margin   = hit_margin_for(extent, magnitude);
+    double const pad = 2.0 * double(out.hit_margin);
 
     double const root_area = std::max(double(root_box.area()), 1e-30);
 

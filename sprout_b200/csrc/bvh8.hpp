@@ -49,8 +49,13 @@ struct Wide_bvh {
     uint32_t                   num_leaves = 0;
     uint32_t                   max_depth  = 0;
     double                     sah_cost   = 0.;
-    float                      pad        = 0.f;  // spatial padding applied to every child box
+    float                      hit_margin = 0.f;  // see hit_margin_for
 };
+
+// Margin around a triangle's bounds within which a hit point must lie:
+// 2^-17 * max(scene extent, largest coordinate magnitude), at least FLT_MIN.  extent and
+// magnitude come from the float bounds of all triangle vertices, converted to double.
+float hit_margin_for(double extent, double magnitude);
 
 // Deepest tree the traversal kernels accept (their stack holds one entry per level).
 constexpr uint32_t Max_wide_depth = 48;

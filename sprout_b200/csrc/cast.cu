@@ -17,10 +17,13 @@
 //    reciprocal of the determinant in place of the reference's rcpss + Newton step
 //    (scalar.inl:67-71).  Every operation is an explicit _rn intrinsic so that nvcc does not
 //    contract them; results are bit-identical to the CPU restatement in oracle/.
-//  * Closest hit returns, among all triangles that pass the test with min_t <= t <= max_t,
-//    the one with the smallest t, ties going to the smaller triangle index.  That choice is
-//    independent of tree shape and traversal order, so any correct traversal returns the
-//    same triangle.
+//  * A triangle is hit when the test passes with min_t <= t <= max_t and the hit point
+//    o + t * d (one FMA per axis) lies within the triangle's bounds widened by the tree's hit
+//    margin (2^-17 of the scene size).  The second condition never rejects a genuine hit; it
+//    rejects the rounding noise the test returns for zero-area triangles, whose "hits" can lie
+//    anywhere along the ray.  Closest hit returns, among all hit triangles, the one with the
+//    smallest t, ties going to the smaller triangle index.  That choice is independent of
+//    tree shape and traversal order, so any correct traversal returns the same triangle.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -105,6 +108,24 @@ __device__ __forceinline__ bool triangle_test(Ray_state const& r, float4 a, floa
     return (u >= 0.f) & (u <= 1.f) & (v >= 0.f) & (uv <= 1.f) & (t >= r.tmin) & (t <= tmax);
 }
 
+// The hit point o + t * d lies within the triangle's bounds widened by margin.
+__device__ __forceinline__ bool within_bounds(Ray_state const& r, float4 a, float4 e1, float4 e2,
+                                              float t, float margin) {
+    float const p[3]  = {__fmaf_rn(t, r.dx, r.ox), __fmaf_rn(t, r.dy, r.oy),
+                         __fmaf_rn(t, r.dz, r.oz)};
+    float const va[3] = {a.x, a.y, a.z};
+    float const vb[3] = {__fadd_rn(a.x, e1.x), __fadd_rn(a.y, e1.y), __fadd_rn(a.z, e1.z)};
+    float const vc[3] = {__fadd_rn(a.x, e2.x), __fadd_rn(a.y, e2.y), __fadd_rn(a.z, e2.z)};
+    bool inside = true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float const lo = __fsub_rn(fminf(va[k], fminf(vb[k], vc[k])), margin);
+        float const hi = __fadd_rn(fmaxf(va[k], fmaxf(vb[k], vc[k])), margin);
+        inside &= (p[k] >= lo) & (p[k] <= hi);
+    }
+    return inside;
+}
+
 // Intersects the ray with the 8 child boxes of a node; returns the hit bits (internal
 // children in bits 24..31 permuted by the ray octant, leaf triangles in bits 0..23).
 __device__ __forceinline__ uint32_t node_test(Ray_state const& r, uint4 const* __restrict__ node,
@@ -187,7 +208,7 @@ __global__ void __launch_bounds__(Block)
     cast_kernel(uint4 const* __restrict__ nodes, float4 const* __restrict__ triangles,
                 float4 const* __restrict__ rays, uint32_t num_rays, uint32_t* __restrict__ ids,
                 float* __restrict__ ts, float2* __restrict__ uvs, uint8_t* __restrict__ occluded,
-                uint32_t* __restrict__ counters) {
+                uint32_t* __restrict__ counters, float hit_margin) {
     uint32_t const lane = threadIdx.x & 31u;
     uint32_t const lt   = (1u << lane) - 1u;
 
@@ -261,7 +282,8 @@ __global__ void __launch_bounds__(Block)
             float4 const  e1  = __ldg(tri + 1);
             float4 const  e2  = __ldg(tri + 2);
             float         t, u, v;
-            if (triangle_test(r, a, e1, e2, r.tbest, t, u, v)) {
+            if (triangle_test(r, a, e1, e2, r.tbest, t, u, v) &&
+                within_bounds(r, a, e1, e2, t, hit_margin)) {
                 uint32_t const id = __float_as_uint(a.w);
                 if (Any_hit) {
                     r.best_id = id;
@@ -339,6 +361,7 @@ struct spb_tree {
     float4*       d_tris     = nullptr;
     uint32_t*     d_counters = nullptr;
     bool          built      = false;
+    float         hit_margin = 0.f;
     spb_tree_info info{};
     Pipeline      pipe;
     cudaStream_t  last_stream = nullptr;
@@ -419,11 +442,11 @@ int32_t launch(spb_tree* tree, bool any_hit, uint32_t slot, float4 const* rays, 
     if (any_hit) {
         cast_kernel<true><<<grid, Block, 0, stream>>>(
             reinterpret_cast<uint4 const*>(tree->d_nodes), tree->d_tris, rays, n, nullptr,
-            nullptr, nullptr, occ, counters);
+            nullptr, nullptr, occ, counters, tree->hit_margin);
     } else {
         cast_kernel<false><<<grid, Block, 0, stream>>>(
             reinterpret_cast<uint4 const*>(tree->d_nodes), tree->d_tris, rays, n, ids, ts, uvs,
-            nullptr, counters);
+            nullptr, counters, tree->hit_margin);
     }
     SPB_CUDA(cudaGetLastError());
     return SPB_OK;
@@ -531,6 +554,7 @@ extern "C" SPB_API int32_t spb_tree_build(spb_tree* tree, uint32_t num_vertices,
     tree->info.device_bytes  = node_bytes + tri_bytes;
     tree->info.build_seconds = std::chrono::duration<double>(t1 - t0).count();
     tree->info.sah_cost      = bvh.sah_cost;
+    tree->hit_margin         = bvh.hit_margin;
     tree->built              = true;
     return SPB_OK;
 }

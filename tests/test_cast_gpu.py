@@ -178,7 +178,8 @@ def test_degenerate_and_clustered_triangles():
     pos[500:1000, 2] = 0.25                 # a flat sheet
     idx = rng.integers(0, 3000, size=(5000, 3)).astype(np.uint32)
     idx[:200] = [0, 1, 2]                   # zero-area triangles (all three vertices equal)
-    rays = np.concatenate([sb.random_rays(40000, seed=2, extent=3.0), edge_rays(pos, idx[200:])])
+    with np.errstate(invalid="ignore"):
+        rays = np.concatenate([sb.random_rays(40000, seed=2, extent=3.0), edge_rays(pos, idx[200:])])
     want = oracle.restated_cast(pos, idx, rays, brute=True)
     with sb.Tree() as tree:
         tree.build(pos, idx)

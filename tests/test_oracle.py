@@ -106,3 +106,22 @@ def test_duplicate_triangles_tie_to_smaller_index():
     rays = np.array([[0, 0, -1, 0, 0, 0, 1, 10]], np.float32)
     r = oracle.restated_cast(pos, idx, rays)
     assert r["ids"][0] == 0 and r["t"][0] == 1.0
+
+
+def test_tree_independence_on_degenerate_mesh():
+    """Zero-area and sliver triangles: the hit definition (test passes and the hit point lies
+    within the triangle's bounds widened by the hit margin) keeps brute force and any
+    conservative tree in agreement, bit for bit."""
+    rng = np.random.default_rng(4)
+    pos = rng.normal(size=(3000, 3)).astype(np.float32)
+    pos[:500] = pos[0]
+    pos[500:1000, 2] = 0.25
+    idx = rng.integers(0, 3000, size=(5000, 3)).astype(np.uint32)
+    idx[:200] = [0, 1, 2]
+    with np.errstate(invalid="ignore"):
+        rays = np.concatenate([sb.random_rays(20000, seed=2, extent=3.0), edge_rays(pos, idx[200:])])
+    a = oracle.restated_cast(pos, idx, rays, brute=True)
+    b = oracle.restated_cast(pos, idx, rays)
+    assert np.array_equal(a["ids"], b["ids"])
+    assert np.array_equal(a["t"].view(np.uint32), b["t"].view(np.uint32))
+    assert np.array_equal(a["occluded"], b["occluded"])
