@@ -23,7 +23,7 @@ ORACLE_LIB = ORACLE / "libcast_oracle.so"
 REFERENCE = pathlib.Path(os.environ.get("SPROUT_REFERENCE", "/root/reference"))
 
 SOURCES = ["common.cpp", "synth.cpp", "bvh8.cpp", "cast.cu"]
-HEADERS = ["common.hpp", "bvh8.hpp"]
+HEADERS = ["common.hpp", "bvh8.hpp", "traverse.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
