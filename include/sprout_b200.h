@@ -142,6 +142,15 @@ SPB_API int32_t spb_synth_sphere_mesh(uint32_t n, float amplitude, uint32_t seed
 SPB_API int32_t spb_synth_rays(uint64_t first, uint64_t count, uint32_t seed, float extent,
                                float* rays, uint32_t num_threads);
 
+/*
+ * The 32 x 32 GGX directional-albedo table the Substitute material's energy compensation
+ * reads (row = alpha index, column = cos(theta_o) index, both i / 31), as computed by this
+ * library.  Stands in for the reference's generated table E
+ * (source/core/scene/material/ggx/ggx_integral.inl, generator ggx_integrate.cpp:199-230).
+ * out: 1024 floats.
+ */
+SPB_API int32_t spb_ggx_albedo_table(float* out);
+
 #ifdef __cplusplus
 }
 #endif

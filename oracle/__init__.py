@@ -121,3 +121,90 @@ def reference_cast(positions, indices, rays, threads=0, mode="both", workdir=Non
     ts = raw[4 * n: 8 * n].view(np.float32)
     occ = raw[8 * n: 9 * n]
     return {"ids": ids.copy(), "t": ts.copy(), "occluded": occ.copy(), "timing": timing}
+
+
+# ---- renderer oracle: the reference's C API in its own process ----------------------------
+
+REF_RENDER = HERE / "_ref" / "ref_render"
+
+
+class ScriptRecorder:
+    """Records su_* calls (the subset the scene builders use) for _ref/ref_render to replay."""
+
+    def __init__(self):
+        self.lines = []
+        self.data = bytearray()
+        self.n = {"material": 0, "mesh": 0, "prop": 0}
+
+    def _blob(self, array):
+        while len(self.data) % 16:
+            self.data.append(0)
+        off = len(self.data)
+        self.data += np.ascontiguousarray(array).tobytes()
+        return off
+
+    def su_create_camera_perspective(self, w, h, fov):
+        self.lines.append(f"camera {w} {h} {float(fov):.9g}")
+        return 4000
+
+    def set_transformation(self, entity, matrix):
+        m = np.asarray(matrix, np.float32).reshape(16)
+        self.lines.append(f"trafo {entity} " + " ".join(f"{float(x):.9g}" for x in m))
+        return 0
+
+    def su_create_integrators(self, desc):
+        self.lines.append("integrators " + (desc.decode() if isinstance(desc, bytes) else desc))
+        return 0
+
+    def su_create_sampler(self, spp):
+        self.lines.append(f"sampler {int(spp)}")
+        return 0
+
+    def su_create_defaults(self):
+        self.lines.append("defaults")
+        return 0
+
+    def su_create_material(self, desc):
+        self.lines.append("material " + (desc.decode() if isinstance(desc, bytes) else desc))
+        self.n["material"] += 1
+        return 1000 + self.n["material"] - 1
+
+    def mesh(self, positions, normals, indices, parts=None):
+        assert parts is None
+        pos = np.asarray(positions, np.float32).reshape(-1, 3)
+        nrm = np.asarray(normals, np.float32).reshape(-1, 3)
+        idx = np.asarray(indices, np.uint32).reshape(-1, 3)
+        op, on, oi = self._blob(pos), self._blob(nrm), self._blob(idx)
+        self.lines.append(f"mesh {idx.shape[0]} {pos.shape[0]} {op} {on} {oi}")
+        self.n["mesh"] += 1
+        return 2000 + self.n["mesh"] - 1
+
+    def prop(self, shape, materials):
+        self.lines.append(f"prop {shape} {len(materials)} " + " ".join(str(int(m)) for m in materials))
+        self.n["prop"] += 1
+        return 3000 + self.n["prop"] - 1
+
+    def su_create_light(self, prop):
+        self.lines.append(f"light {prop}")
+        return 0
+
+
+def reference_render(build_scene, width, height, iterations, progressive=True, workdir=None):
+    """Renders with the compiled reference: build_scene(recorder) issues the scene's calls.
+    Returns (rgb image (H, W, 3) float32, timing dict)."""
+    if not REF_RENDER.exists():
+        raise FileNotFoundError(f"{REF_RENDER} missing: build it with `make -C oracle`")
+    rec = ScriptRecorder()
+    build_scene(rec)
+    head = [f"init {1 if progressive else 0}"]
+    tail = [f"progressive {iterations}"] if progressive else ["frame 0"]
+    with tempfile.TemporaryDirectory(dir=workdir) as tmp:
+        sp, dp, op = (os.path.join(tmp, n) for n in ("script.txt", "data.bin", "out.bin"))
+        with open(sp, "w") as f:
+            f.write("\n".join(head + rec.lines + tail) + "\n")
+        with open(dp, "wb") as f:
+            f.write(bytes(rec.data))
+        res = subprocess.run([str(REF_RENDER), sp, dp, op], capture_output=True, text=True, check=True)
+        timing = json.loads(res.stdout.strip().splitlines()[-1])
+        img = np.fromfile(op, np.float32).reshape(height, width, 4)
+    return img[:, :, :3].copy(), timing

@@ -53,6 +53,7 @@ PROTOTYPES = {
     "spb_synth_sphere_mesh": (c_i32, [c_u32, c_f32, c_u32, ctypes.POINTER(c_u32),
                                       ctypes.POINTER(c_u32), c_vp, c_vp]),
     "spb_synth_rays": (c_i32, [c_u64, c_u64, c_u32, c_f32, c_vp, c_u32]),
+    "spb_ggx_albedo_table": (c_i32, [c_vp]),
 }
 
 _lib = None

@@ -22,8 +22,8 @@ ORACLE = ROOT / "oracle"
 ORACLE_LIB = ORACLE / "libcast_oracle.so"
 REFERENCE = pathlib.Path(os.environ.get("SPROUT_REFERENCE", "/root/reference"))
 
-SOURCES = ["common.cpp", "synth.cpp", "bvh8.cpp", "cast.cu"]
-HEADERS = ["common.hpp", "bvh8.hpp", "traverse.cuh"]
+SOURCES = ["common.cpp", "synth.cpp", "bvh8.cpp", "ggx_table.cpp", "cast.cu", "render.cu", "capi.cpp"]
+HEADERS = ["common.hpp", "bvh8.hpp", "traverse.cuh", "material.cuh", "render.hpp", "json.hpp", "ggx_table.hpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -50,7 +50,7 @@ def _stale(target: pathlib.Path, inputs) -> bool:
 
 
 def build_library(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> pathlib.Path:
-    inputs = [CSRC / s for s in SOURCES] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "sprout_b200.h"]
+    inputs = [CSRC / s for s in SOURCES] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "sprout_b200.h", ROOT / "include" / "sprout.h"]
     if not force and not _stale(LIBRARY, inputs):
         return LIBRARY
     cmd = [_nvcc(), "-shared", "-o", str(LIBRARY)] + [str(CSRC / s) for s in SOURCES] + NVCC_FLAGS

@@ -1,0 +1,107 @@
+"""ctypes binding of the sprout C API (include/sprout.h), for any library that exports it.
+
+``SuLibrary(path)`` binds the su_* functions of a shared library: this package's
+libsprout_b200.so (the B200 path tracer) or, in tests, the reference's own libsprout.so --
+the same calls drive both, which is what makes one a drop-in for the other.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+import numpy as np
+
+from . import _lib
+
+u32, i32, f32, vp = ctypes.c_uint32, ctypes.c_int32, ctypes.c_float, ctypes.c_void_p
+SU_RESOURCE_NULL = 0xFFFFFFFF
+SU_UINT8 = 0
+SU_FLOAT32 = 2
+
+LOG_FUNC = ctypes.CFUNCTYPE(None, ctypes.c_uint32, ctypes.c_char_p)
+
+PROTOTYPES = {
+    "su_platform_revision": (ctypes.c_char_p, []),
+    "su_init": (i32, [ctypes.c_bool]),
+    "su_release": (i32, []),
+    "su_mount": (i32, [ctypes.c_char_p]),
+    "su_clear": (i32, []),
+    "su_load_take": (i32, [ctypes.c_char_p]),
+    "su_create_defaults": (i32, []),
+    "su_create_camera": (u32, [ctypes.c_char_p]),
+    "su_create_camera_perspective": (u32, [u32, u32, f32]),
+    "su_camera_set_resolution": (i32, [u32, u32]),
+    "su_create_sampler": (i32, [u32]),
+    "su_create_integrators": (i32, [ctypes.c_char_p]),
+    "su_create_image": (u32, [u32, u32, u32, u32, u32, u32, u32, vp]),
+    "su_create_material": (u32, [ctypes.c_char_p]),
+    "su_create_material_from_file": (u32, [ctypes.c_char_p]),
+    "su_create_triangle_mesh_async": (u32, [u32, u32, u32, vp, u32, vp, u32, vp, u32, vp, vp, u32, vp]),
+    "su_create_triangle_mesh_from_file": (u32, [ctypes.c_char_p]),
+    "su_create_prop": (u32, [u32, u32, vp]),
+    "su_create_light": (i32, [u32]),
+    "su_camera_entity": (u32, []),
+    "su_camera_sensor_dimensions": (i32, [vp]),
+    "su_entity_allocate_frames": (i32, [u32]),
+    "su_entity_transformation": (i32, [u32, vp]),
+    "su_entity_set_transformation": (i32, [u32, vp]),
+    "su_entity_set_transformation_frame": (i32, [u32, u32, vp]),
+    "su_render": (i32, []),
+    "su_render_frame": (i32, [u32]),
+    "su_export_frame": (i32, [u32]),
+    "su_start_render_frame": (i32, [u32]),
+    "su_set_expected_iterations": (i32, [u32]),
+    "su_render_iteration": (i32, []),
+    "su_postprocess": (i32, []),
+    "su_copy_framebuffer": (i32, [u32, u32, u32, u32, vp]),
+    "su_register_log": (i32, [LOG_FUNC]),
+    "su_register_progress": (i32, [vp, vp]),
+}
+
+
+class SuLibrary:
+    """The su_* entry points of one shared library."""
+
+    def __init__(self, path=None, log=True):
+        path = pathlib.Path(path) if path else _lib.LIBRARY_PATH
+        if path == _lib.LIBRARY_PATH:
+            self.lib = _lib.load()
+        else:
+            self.lib = ctypes.CDLL(str(path))
+        for name, (res, args) in PROTOTYPES.items():
+            fn = getattr(self.lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        self.messages = []
+        self._log = LOG_FUNC(lambda t, m: self.messages.append((int(t), m.decode(errors="replace"))))
+        if log:
+            self.lib.su_register_log(self._log)
+        self._keep = []  # buffers handed to the library stay alive as long as it might read them
+
+    def __getattr__(self, name):
+        return getattr(self.lib, name)
+
+    def mesh(self, positions, normals, indices, parts=None):
+        pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        nrm = np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+        idx = np.ascontiguousarray(indices, np.uint32).reshape(-1, 3)
+        prt = None if parts is None else np.ascontiguousarray(parts, np.uint32).reshape(-1, 3)
+        self._keep += [pos, nrm, idx, prt]
+        return self.lib.su_create_triangle_mesh_async(
+            idx.shape[0], pos.shape[0], 3, pos.ctypes.data, 3, nrm.ctypes.data, 0, None, 0, None,
+            idx.ctypes.data, 0 if prt is None else prt.shape[0], None if prt is None else prt.ctypes.data)
+
+    def prop(self, shape, materials):
+        mats = np.ascontiguousarray(materials, np.uint32)
+        self._keep.append(mats)
+        return self.lib.su_create_prop(shape, len(mats), mats.ctypes.data)
+
+    def set_transformation(self, entity, matrix):
+        m = np.ascontiguousarray(matrix, np.float32).reshape(16)
+        return self.lib.su_entity_set_transformation(entity, m.ctypes.data)
+
+    def framebuffer(self, width, height):
+        out = np.zeros((height, width, 4), np.float32)
+        status = self.lib.su_copy_framebuffer(SU_FLOAT32, width, height, 4, out.ctypes.data)
+        return out, status

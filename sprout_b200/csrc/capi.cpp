@@ -1,0 +1,754 @@
+// The reference's C API (source/capi/capi.cpp) on top of the B200 path tracer.
+//
+// A single global engine, as in the reference (capi.cpp:64-110): meshes, materials and props
+// are collected on the host; su_start_render_frame / su_render_frame flatten every prop into
+// one world-space triangle set (the props' transformations applied to their meshes), build the
+// 8-wide BVH and upload the scene; iterations then run entirely on the GPU (render.cu).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/sprout.h"
+#include "common.hpp"
+#include "json.hpp"
+#include "render.hpp"
+
+namespace {
+
+using spb::shading::Material;
+using spb::shading::V3;
+
+constexpr uint32_t Null          = 0xFFFFFFFFu;
+constexpr uint32_t First_mesh_id = 8;  // ids 0..7 are the built-in shapes (sprout.h:22-29)
+
+struct Mesh {
+    std::vector<float>    positions;  // 3 per vertex
+    std::vector<float>    normals;    // 3 per vertex
+    std::vector<uint32_t> indices;    // 3 per triangle
+    std::vector<uint32_t> part_of;    // part per triangle
+    std::vector<uint32_t> part_slot;  // material slot per part
+};
+
+struct Entity {
+    bool                  camera = false;
+    uint32_t              shape  = Null;
+    std::vector<uint32_t> materials;
+    float                 trafo[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+    bool                  light = false;
+};
+
+struct Engine {
+    explicit Engine(bool p) : progressive(p) {}
+
+    bool                  progressive;
+    std::vector<Mesh>     meshes;
+    std::vector<Material> materials;
+    std::vector<Entity>   entities;
+    uint32_t              camera_entity = Null;
+    uint32_t              width         = 0;
+    uint32_t              height        = 0;
+    float                 fov           = 0.f;
+    uint32_t              spp           = 1;
+    bool                  have_integrator = false;
+    spb::render::Settings settings;
+    spb::render::Renderer renderer;
+    bool                  frame_started = false;
+    bool                  tonemap_linear = false;  // su_create_defaults: Linear tonemapper
+    uint32_t              iteration     = 0;
+    std::vector<float>    target;  // resolved rgba
+};
+
+Engine* engine = nullptr;
+Post    log_post = nullptr;
+Progress_start progress_start = nullptr;
+Progress_tick  progress_tick  = nullptr;
+
+void log(uint32_t type, std::string const& text) {
+    if (log_post) {
+        log_post(type, text.c_str());
+    }
+}
+
+// sRGB -> ACEScg (AP1) primaries, applied to every colour the material descriptions carry,
+// as the reference does with SU_ACESCG (material_provider.cpp:1022-1028, spectrum/aces.hpp).
+V3 srgb_to_ap1(V3 c) {
+    return V3{0.61309732f * c.x + 0.33952285f * c.y + 0.04737928f * c.z,
+              0.07019422f * c.x + 0.91635557f * c.y + 0.01345259f * c.z,
+              0.02061560f * c.x + 0.10956983f * c.y + 0.86981512f * c.z};
+}
+
+bool read_color(spb::json::Value const* v, V3& out) {
+    if (!v) {
+        return false;
+    }
+    if (v->is_number()) {
+        // a single number is a grey level; the reference keeps the mapped green channel
+        float const g = srgb_to_ap1(V3{float(v->number), float(v->number), float(v->number)}).y;
+        out           = V3{g, g, g};
+        return true;
+    }
+    if (v->is_array() && v->array.size() >= 3) {
+        out = srgb_to_ap1(V3{float(v->array[0].number), float(v->array[1].number),
+                             float(v->array[2].number)});
+        return true;
+    }
+    if (v->is_object()) {
+        return read_color(v->find("value"), out);
+    }
+    return false;
+}
+
+bool ready() {
+    return engine && engine->camera_entity != Null && engine->width > 0 && engine->fov > 0.f &&
+           engine->have_integrator;
+}
+
+// Rotation rows (normalised) and translation of a row-major object-to-world matrix.
+void decompose(float const* m, float rot[9], float pos[3]) {
+    for (int r = 0; r < 3; ++r) {
+        float const len = std::sqrt(m[4 * r] * m[4 * r] + m[4 * r + 1] * m[4 * r + 1] +
+                                    m[4 * r + 2] * m[4 * r + 2]);
+        float const inv = len > 0.f ? 1.f / len : 0.f;
+        for (int c = 0; c < 3; ++c) {
+            rot[3 * r + c] = m[4 * r + c] * inv;
+        }
+    }
+    pos[0] = m[12];
+    pos[1] = m[13];
+    pos[2] = m[14];
+}
+
+int32_t compile_scene() {
+    spb::render::Scene_desc scene;
+    scene.materials = engine->materials;
+    // fallback material for unassigned slots: grey Substitute
+    Material fallback{};
+    fallback.type     = spb::shading::Type_substitute;
+    fallback.metallic = 0.f;
+    fallback.alpha    = 1.f;
+    fallback.albedo   = srgb_to_ap1(V3{0.5f, 0.5f, 0.5f});
+    fallback.f0       = V3{0.03497f, 0.03497f, 0.03497f};
+    uint32_t const fallback_id = uint32_t(scene.materials.size());
+    scene.materials.push_back(fallback);
+
+    for (Entity const& e : engine->entities) {
+        if (e.camera || e.shape == Null) {
+            continue;
+        }
+        Mesh const&    mesh = engine->meshes[e.shape - First_mesh_id];
+        uint32_t const base = uint32_t(scene.positions.size() / 3);
+        float const*   m    = e.trafo;
+        float          rot[9];
+        float          pos[3];
+        decompose(m, rot, pos);
+        for (size_t v = 0; v < mesh.positions.size() / 3; ++v) {
+            float const x = mesh.positions[3 * v];
+            float const y = mesh.positions[3 * v + 1];
+            float const z = mesh.positions[3 * v + 2];
+            // row vector times matrix: p' = x * row0 + y * row1 + z * row2 + row3
+            scene.positions.push_back(x * m[0] + y * m[4] + z * m[8] + m[12]);
+            scene.positions.push_back(x * m[1] + y * m[5] + z * m[9] + m[13]);
+            scene.positions.push_back(x * m[2] + y * m[6] + z * m[10] + m[14]);
+            float const nx = mesh.normals[3 * v];
+            float const ny = mesh.normals[3 * v + 1];
+            float const nz = mesh.normals[3 * v + 2];
+            scene.normals.push_back(nx * rot[0] + ny * rot[3] + nz * rot[6]);
+            scene.normals.push_back(nx * rot[1] + ny * rot[4] + nz * rot[7]);
+            scene.normals.push_back(nx * rot[2] + ny * rot[5] + nz * rot[8]);
+        }
+        for (size_t t = 0; t < mesh.indices.size() / 3; ++t) {
+            for (int k = 0; k < 3; ++k) {
+                scene.indices.push_back(base + mesh.indices[3 * t + k]);
+            }
+            uint32_t const slot = mesh.part_slot[mesh.part_of[t]];
+            uint32_t const mat  = slot < e.materials.size() ? e.materials[slot] : Null;
+            scene.tri_material.push_back(mat < engine->materials.size() ? mat : fallback_id);
+            scene.tri_light.push_back(e.light ? 1 : 0);
+        }
+    }
+    if (scene.indices.empty()) {
+        log(SU_LOG_ERROR, "scene has no triangles");
+        return -2;
+    }
+    if (int32_t const s = engine->renderer.set_scene(scene, 0)) {
+        log(SU_LOG_ERROR, engine->renderer.error());
+        return s == SPB_ERROR_CUDA ? -2 : -1;
+    }
+    spb::render::Camera_desc cam;
+    cam.width  = engine->width;
+    cam.height = engine->height;
+    cam.fov    = engine->fov;
+    decompose(engine->entities[engine->camera_entity].trafo, cam.rotation, cam.position);
+    if (engine->renderer.set_camera(cam)) {
+        log(SU_LOG_ERROR, engine->renderer.error());
+        return -2;
+    }
+    engine->renderer.set_settings(engine->settings);
+    return 0;
+}
+
+int32_t render_samples(uint32_t first, uint32_t count) {
+    if (progress_start) {
+        progress_start(count);
+    }
+    if (engine->renderer.render(first, count)) {
+        log(SU_LOG_ERROR, engine->renderer.error());
+        return -2;
+    }
+    if (progress_tick) {
+        for (uint32_t i = 0; i < count; ++i) {
+            progress_tick();
+        }
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+SU_LIBRARY_API char const* su_platform_revision(void) {
+    return "sprout_b200 (sm_100a wavefront path tracer)";
+}
+
+SU_LIBRARY_API int32_t su_init(bool progressive) {
+    if (engine) {
+        return -1;
+    }
+    engine = new Engine(progressive);
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_release(void) {
+    delete engine;
+    engine = nullptr;
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_mount(char const* folder) {
+    if (!engine) {
+        return -1;
+    }
+    (void)folder;
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_clear(void) {
+    if (!engine) {
+        return -1;
+    }
+    engine->entities.clear();
+    engine->meshes.clear();
+    engine->materials.clear();
+    engine->camera_entity = Null;
+    engine->frame_started = false;
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_load_take(char const* string) {
+    if (!engine) {
+        return -1;
+    }
+    (void)string;
+    log(SU_LOG_ERROR, "su_load_take: take files are not supported by this renderer");
+    return -2;
+}
+
+SU_LIBRARY_API int32_t su_create_defaults(void) {
+    if (!engine) {
+        return -1;
+    }
+    // take_loader.cpp:965-978: with ACEScg the default pipeline is the Linear tonemapper
+    // (exposure 0), which maps the AP1 film to linear sRGB (tonemapping/linear.cpp:10-27).
+    engine->tonemap_linear = true;
+    if (!engine->have_integrator) {
+        engine->settings        = spb::render::Settings();
+        engine->have_integrator = true;
+    }
+    return 0;
+}
+
+SU_LIBRARY_API uint32_t su_create_camera_perspective(uint32_t width, uint32_t height, float fov) {
+    if (!engine) {
+        return Null;
+    }
+    if (width == 0 || height == 0 || !(fov > 0.f)) {
+        log(SU_LOG_ERROR, "su_create_camera_perspective: invalid resolution or fov");
+        return Null;
+    }
+    Entity e;
+    e.camera = true;
+    engine->entities.push_back(e);
+    engine->camera_entity = uint32_t(engine->entities.size() - 1);
+    engine->width         = width;
+    engine->height        = height;
+    engine->fov           = fov;
+    return engine->camera_entity;
+}
+
+SU_LIBRARY_API uint32_t su_create_camera(char const* string) {
+    if (!engine) {
+        return Null;
+    }
+    spb::json::Value root;
+    if (!spb::json::parse(string, root)) {
+        log(SU_LOG_ERROR, "su_create_camera: JSON parse error");
+        return Null;
+    }
+    spb::json::Value const* persp = root.find("Perspective");
+    if (!persp) {
+        log(SU_LOG_ERROR, "su_create_camera: only Perspective cameras are supported");
+        return Null;
+    }
+    double fov_deg = 60.0;
+    if (auto const* params = persp->find("parameters")) {
+        fov_deg = spb::json::number_or(params->find("fov"), fov_deg);
+    }
+    uint32_t w = 0;
+    uint32_t h = 0;
+    if (auto const* sensor = persp->find("sensor")) {
+        if (auto const* res = sensor->find("resolution"); res && res->is_array() && res->array.size() == 2) {
+            w = uint32_t(res->array[0].number);
+            h = uint32_t(res->array[1].number);
+        }
+    }
+    if (w == 0 || h == 0) {
+        log(SU_LOG_ERROR, "su_create_camera: missing sensor resolution");
+        return Null;
+    }
+    return su_create_camera_perspective(w, h, float(fov_deg * 3.14159265358979323846 / 180.0));
+}
+
+SU_LIBRARY_API int32_t su_camera_set_resolution(uint32_t width, uint32_t height) {
+    if (!engine) {
+        return -1;
+    }
+    if (engine->camera_entity == Null) {
+        return -2;
+    }
+    engine->width         = width;
+    engine->height        = height;
+    engine->frame_started = false;
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_create_sampler(uint32_t num_samples) {
+    if (!engine) {
+        return -1;
+    }
+    engine->spp = std::max(1u, num_samples);
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
+    if (!engine) {
+        return -1;
+    }
+    spb::json::Value root;
+    if (!spb::json::parse(string, root)) {
+        log(SU_LOG_ERROR, "su_create_integrators: JSON parse error");
+        return 0;
+    }
+    // take_loader.cpp:617-738 defaults: min_bounces 4, max_bounces 8
+    spb::render::Settings s;
+    if (auto const* surface = root.find("surface")) {
+        spb::json::Value const* pt = surface->find("PTMIS");
+        if (!pt) {
+            log(SU_LOG_WARNING, "su_create_integrators: only PTMIS is implemented; using PTMIS");
+            pt = surface->object.empty() ? nullptr : &surface->object.front().second;
+        }
+        if (pt) {
+            s.min_bounces = uint32_t(spb::json::number_or(pt->find("min_bounces"), s.min_bounces));
+            s.max_bounces = uint32_t(spb::json::number_or(pt->find("max_bounces"), s.max_bounces));
+        }
+    }
+    if (s.max_bounces > 60) {
+        log(SU_LOG_WARNING, "su_create_integrators: max_bounces clamped to 60");
+        s.max_bounces = 60;
+    }
+    engine->settings        = s;
+    engine->have_integrator = true;
+    return 0;
+}
+
+SU_LIBRARY_API uint32_t su_create_image(uint32_t, uint32_t, uint32_t, uint32_t, uint32_t, uint32_t,
+                                        uint32_t, char const*) {
+    if (!engine) {
+        return Null;
+    }
+    log(SU_LOG_ERROR, "su_create_image: textures are not supported by this renderer");
+    return Null;
+}
+
+SU_LIBRARY_API uint32_t su_create_material(char const* string) {
+    if (!engine) {
+        return Null;
+    }
+    spb::json::Value root;
+    if (!spb::json::parse(string, root)) {
+        log(SU_LOG_ERROR, "su_create_material: JSON parse error");
+        return Null;
+    }
+    spb::json::Value const* rendering = root.find("rendering");
+    if (!rendering || !rendering->is_object() || rendering->object.empty()) {
+        log(SU_LOG_ERROR, "su_create_material: missing \"rendering\"");
+        return Null;
+    }
+    std::string const&      type = rendering->object.front().first;
+    spb::json::Value const& desc = rendering->object.front().second;
+
+    Material m{};
+    m.two_sided = spb::json::bool_or(desc.find("two_sided"), false) ? 1u : 0u;
+    if (type == "Light") {
+        // material_provider.cpp:298-364: "emission" is a radiance, default 10
+        V3 emission{10.f, 10.f, 10.f};
+        emission   = srgb_to_ap1(emission);
+        read_color(desc.find("emission"), emission);
+        m.type     = spb::shading::Type_light;
+        m.emission = emission;
+    } else if (type == "Substitute") {
+        // material_provider.cpp:483-760 defaults: color 0.5, roughness 0.8, metallic 0, ior 1.46
+        V3 color = srgb_to_ap1(V3{0.5f, 0.5f, 0.5f});
+        read_color(desc.find("color"), color);
+        float const roughness = float(spb::json::number_or(desc.find("roughness"), 0.8));
+        float const metallic  = float(spb::json::number_or(desc.find("metallic"), 0.0));
+        float const ior       = float(spb::json::number_or(desc.find("ior"), 1.46));
+        float const r         = std::max(roughness, spb::shading::Min_roughness);
+        float const f0d       = ((1.f - ior) / (1.f + ior)) * ((1.f - ior) / (1.f + ior));
+        m.type     = spb::shading::Type_substitute;
+        m.metallic = metallic;
+        m.alpha    = r * r;
+        m.albedo   = V3{(1.f - metallic) * color.x, (1.f - metallic) * color.y,
+                      (1.f - metallic) * color.z};
+        m.f0       = V3{f0d + metallic * (color.x - f0d), f0d + metallic * (color.y - f0d),
+                  f0d + metallic * (color.z - f0d)};
+        V3 emission{0.f, 0.f, 0.f};
+        if (read_color(desc.find("emission"), emission) &&
+            (emission.x > 0.f || emission.y > 0.f || emission.z > 0.f)) {
+            log(SU_LOG_WARNING, "su_create_material: Substitute emission is ignored by this renderer");
+        }
+    } else {
+        log(SU_LOG_ERROR, "su_create_material: unsupported material type " + type);
+        return Null;
+    }
+    engine->materials.push_back(m);
+    return uint32_t(engine->materials.size() - 1);
+}
+
+SU_LIBRARY_API uint32_t su_create_material_from_file(char const* filename) {
+    if (!engine) {
+        return Null;
+    }
+    (void)filename;
+    log(SU_LOG_ERROR, "su_create_material_from_file: files are not supported by this renderer");
+    return Null;
+}
+
+SU_LIBRARY_API uint32_t su_create_triangle_mesh_async(
+    uint32_t num_triangles, uint32_t num_vertices, uint32_t positions_stride,
+    float const* positions, uint32_t normals_stride, float const* normals, uint32_t /*tangents_stride*/,
+    float const* /*tangents*/, uint32_t /*uvs_stride*/, float const* /*uvs*/, uint32_t const* indices,
+    uint32_t num_parts, uint32_t const* parts) {
+    if (!engine) {
+        return Null;
+    }
+    // triangle_mesh_provider.cpp:176-247: positions and normals are required
+    if (!positions || !normals || num_triangles == 0 || num_vertices == 0 ||
+        positions_stride < 3 || normals_stride < 3) {
+        log(SU_LOG_ERROR, "Mesh does not contain vertex positions or normals.");
+        return Null;
+    }
+    Mesh mesh;
+    mesh.positions.resize(3 * size_t(num_vertices));
+    mesh.normals.resize(3 * size_t(num_vertices));
+    for (uint32_t v = 0; v < num_vertices; ++v) {
+        for (int k = 0; k < 3; ++k) {
+            mesh.positions[3 * v + k] = positions[size_t(v) * positions_stride + k];
+            mesh.normals[3 * v + k]   = normals[size_t(v) * normals_stride + k];
+        }
+    }
+    mesh.indices.resize(3 * size_t(num_triangles));
+    for (uint32_t t = 0; t < num_triangles; ++t) {
+        for (int k = 0; k < 3; ++k) {
+            uint32_t const i = indices ? indices[3 * size_t(t) + k] : 3 * t + uint32_t(k);
+            if (i >= num_vertices) {
+                log(SU_LOG_ERROR, "su_create_triangle_mesh_async: index out of range");
+                return Null;
+            }
+            mesh.indices[3 * size_t(t) + k] = i;
+        }
+    }
+    mesh.part_of.assign(num_triangles, 0);
+    if (parts && num_parts > 0) {
+        mesh.part_slot.resize(num_parts);
+        for (uint32_t p = 0; p < num_parts; ++p) {
+            uint32_t const start = parts[3 * p] / 3;
+            uint32_t const end   = std::min(num_triangles, (parts[3 * p] + parts[3 * p + 1]) / 3);
+            for (uint32_t t = start; t < end; ++t) {
+                mesh.part_of[t] = p;
+            }
+            mesh.part_slot[p] = parts[3 * p + 2];
+        }
+    } else {
+        mesh.part_slot.assign(1, 0);
+    }
+    engine->meshes.push_back(std::move(mesh));
+    engine->frame_started = false;
+    return First_mesh_id + uint32_t(engine->meshes.size() - 1);
+}
+
+SU_LIBRARY_API uint32_t su_create_triangle_mesh_from_file(char const* filename) {
+    if (!engine) {
+        return Null;
+    }
+    (void)filename;
+    log(SU_LOG_ERROR, "su_create_triangle_mesh_from_file: files are not supported by this renderer");
+    return Null;
+}
+
+SU_LIBRARY_API uint32_t su_create_prop(uint32_t shape, uint32_t num_materials,
+                                       uint32_t const* materials) {
+    if (!engine) {
+        return Null;
+    }
+    if (shape < First_mesh_id || shape - First_mesh_id >= engine->meshes.size()) {
+        log(SU_LOG_ERROR, "su_create_prop: only triangle meshes are supported by this renderer");
+        return Null;
+    }
+    Entity e;
+    e.shape = shape;
+    for (uint32_t i = 0; i < num_materials; ++i) {
+        e.materials.push_back(materials ? materials[i] : Null);
+    }
+    engine->entities.push_back(e);
+    engine->frame_started = false;
+    return uint32_t(engine->entities.size() - 1);
+}
+
+SU_LIBRARY_API int32_t su_create_light(uint32_t entity) {
+    if (!engine) {
+        return -1;
+    }
+    if (entity >= engine->entities.size() || engine->entities[entity].camera) {
+        return -2;
+    }
+    engine->entities[entity].light = true;
+    engine->frame_started          = false;
+    return 0;
+}
+
+SU_LIBRARY_API uint32_t su_camera_entity(void) {
+    if (!engine) {
+        return Null;
+    }
+    return engine->camera_entity;
+}
+
+SU_LIBRARY_API int32_t su_camera_sensor_dimensions(int32_t* dimensions) {
+    if (!engine) {
+        return -1;
+    }
+    if (engine->camera_entity == Null || !dimensions) {
+        return -2;
+    }
+    dimensions[0] = int32_t(engine->width);
+    dimensions[1] = int32_t(engine->height);
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_entity_allocate_frames(uint32_t entity) {
+    if (!engine) {
+        return -1;
+    }
+    (void)entity;
+    log(SU_LOG_ERROR, "su_entity_allocate_frames: animation is not supported by this renderer");
+    return -2;
+}
+
+SU_LIBRARY_API int32_t su_entity_transformation(uint32_t entity, float* trafo) {
+    if (!engine) {
+        return -1;
+    }
+    if (entity >= engine->entities.size() || !trafo) {
+        return -2;
+    }
+    std::memcpy(trafo, engine->entities[entity].trafo, sizeof(float) * 16);
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_entity_set_transformation(uint32_t entity, float const* trafo) {
+    if (!engine) {
+        return -1;
+    }
+    if (entity >= engine->entities.size() || !trafo) {
+        return -2;
+    }
+    std::memcpy(engine->entities[entity].trafo, trafo, sizeof(float) * 16);
+    engine->frame_started = false;
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_entity_set_transformation_frame(uint32_t entity, uint32_t frame,
+                                                          float const* trafo) {
+    if (!engine) {
+        return -1;
+    }
+    (void)entity;
+    (void)frame;
+    (void)trafo;
+    log(SU_LOG_ERROR, "su_entity_set_transformation_frame: animation is not supported");
+    return -2;
+}
+
+SU_LIBRARY_API int32_t su_start_render_frame(uint32_t frame) {
+    if (!engine) {
+        return -1;
+    }
+    (void)frame;
+    if (!ready()) {
+        return -2;
+    }
+    if (int32_t const s = compile_scene()) {
+        return s;
+    }
+    if (engine->renderer.start_frame()) {
+        log(SU_LOG_ERROR, engine->renderer.error());
+        return -2;
+    }
+    engine->frame_started = true;
+    engine->iteration     = 0;
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_set_expected_iterations(uint32_t iterations) {
+    if (!engine) {
+        return -1;
+    }
+    if (!ready()) {
+        return -2;
+    }
+    (void)iterations;  // only steers ray differentials in the reference; no effect here
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_render_iteration(void) {
+    if (!engine) {
+        return -1;
+    }
+    if (!ready() || !engine->frame_started) {
+        return -2;
+    }
+    if (int32_t const s = render_samples(engine->iteration, 1)) {
+        return s;
+    }
+    ++engine->iteration;
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_render_frame(uint32_t frame) {
+    if (!engine) {
+        return -1;
+    }
+    if (int32_t const s = su_start_render_frame(frame)) {
+        return s;
+    }
+    if (int32_t const s = render_samples(0, engine->spp)) {
+        return s;
+    }
+    engine->iteration = engine->spp;
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_render(void) {
+    return su_render_frame(0);
+}
+
+SU_LIBRARY_API int32_t su_export_frame(uint32_t frame) {
+    if (!engine) {
+        return -1;
+    }
+    (void)frame;
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_postprocess(void) {
+    if (!engine) {
+        return -1;
+    }
+    if (!ready() || !engine->frame_started) {
+        return -2;
+    }
+    engine->target.resize(4 * size_t(engine->width) * engine->height);
+    if (engine->renderer.resolve(engine->target.data())) {
+        log(SU_LOG_ERROR, engine->renderer.error());
+        return -2;
+    }
+    if (engine->tonemap_linear) {
+        for (size_t i = 0; i < engine->target.size(); i += 4) {
+            float* c        = &engine->target[i];
+            float const r   = c[0];
+            float const g   = c[1];
+            float const b   = c[2];
+            c[0]            = 1.70505155f * r - 0.62179068f * g - 0.08325840f * b;
+            c[1]            = -0.13025714f * r + 1.14080289f * g - 0.01054853f * b;
+            c[2]            = -0.02400328f * r - 0.12896877f * g + 1.15297171f * b;
+        }
+    }
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_copy_framebuffer(uint32_t type, uint32_t width, uint32_t height,
+                                           uint32_t num_channels, uint8_t* destination) {
+    if (!engine) {
+        return -1;
+    }
+    if (!destination || engine->target.empty()) {
+        return -2;
+    }
+    uint32_t const w = std::min(width, engine->width);
+    uint32_t const h = std::min(height, engine->height);
+    if (SU_UINT8 == type && 3 == num_channels) {
+        // linear -> gamma sRGB, rounded to bytes (capi.cpp:667-700)
+        for (uint32_t y = 0; y < h; ++y) {
+            for (uint32_t x = 0; x < w; ++x) {
+                size_t const i = size_t(y) * engine->width + x;
+                for (int c = 0; c < 3; ++c) {
+                    float       v = std::max(engine->target[4 * i + c], 0.f);
+                    v             = v <= 0.0031308f ? 12.92f * v
+                                                    : 1.055f * std::pow(v, 1.f / 2.4f) - 0.055f;
+                    float const b = std::min(std::max(v, 0.f), 1.f) * 255.f + 0.5f;
+                    destination[3 * i + c] = uint8_t(b);
+                }
+            }
+        }
+        return 0;
+    }
+    if (SU_FLOAT32 == type && 4 == num_channels) {
+        size_t const len = std::min(size_t(width) * height, size_t(engine->width) * engine->height);
+        std::memcpy(destination, engine->target.data(), len * 4 * sizeof(float));
+        return 0;
+    }
+    return -2;
+}
+
+SU_LIBRARY_API int32_t su_register_log(Post post) {
+    if (!post) {
+        return -1;
+    }
+    log_post = post;
+    return 0;
+}
+
+SU_LIBRARY_API int32_t su_register_progress(Progress_start start, Progress_tick tick) {
+    if (!engine) {
+        return -1;
+    }
+    progress_start = start;
+    progress_tick  = tick;
+    return 0;
+}
+
+}  // extern "C"

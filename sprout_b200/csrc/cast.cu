@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(Block)
 
     gpu::Ray_state r;
     gpu::Traversal tv;
+    uint2          stack[gpu::Stack_size];
     uint32_t       ray       = 0;
     bool           active    = false;
     bool           exhausted = false;
@@ -75,7 +76,7 @@ __global__ void __launch_bounds__(Block)
             continue;
         }
 
-        if (gpu::traversal_step<Any_hit>(r, tv, nodes, triangles, hit_margin, counters + 1)) {
+        if (gpu::traversal_step<Any_hit>(r, tv, stack, nodes, triangles, hit_margin, counters + 1)) {
             if (Any_hit) {
                 occluded[ray] = r.best_id != gpu::Miss ? 1 : 0;
             } else {

@@ -1,0 +1,83 @@
+// Wavefront MIS path tracer on the GPU: the device side of the su_* render entry points.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "material.cuh"
+
+namespace spb::render {
+
+// World-space scene as the host engine flattens it (one BVH over all props' triangles).
+struct Scene_desc {
+    std::vector<float>              positions;     // 3 per vertex, world space
+    std::vector<float>              normals;       // 3 per vertex, world space (shading)
+    std::vector<uint32_t>           indices;       // 3 per triangle
+    std::vector<uint32_t>           tri_material;  // per triangle, index into materials
+    std::vector<uint8_t>            tri_light;     // per triangle: 1 if it belongs to a light prop
+    std::vector<shading::Material>  materials;
+};
+
+struct Camera_desc {
+    uint32_t width  = 0;
+    uint32_t height = 0;
+    float    fov    = 0.f;              // horizontal, radians
+    float    rotation[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};  // rows: camera x, y, z axes in world
+    float    position[3] = {0, 0, 0};
+};
+
+struct Settings {
+    uint32_t min_bounces = 4;   // Russian roulette starts here
+    uint32_t max_bounces = 8;
+    uint32_t seed        = 0;
+};
+
+struct Stats {
+    uint64_t paths          = 0;  // camera samples traced
+    uint64_t extension_rays = 0;  // closest-hit rays (camera + continuation)
+    uint64_t shadow_rays    = 0;  // any-hit rays
+    double   seconds        = 0.0;  // device time of the last render call
+    uint32_t overflow       = 0;  // rays dropped by the traversal stack guard (0 expected)
+};
+
+class Renderer {
+  public:
+    Renderer();
+    ~Renderer();
+
+    int32_t set_scene(Scene_desc const& scene, uint32_t num_threads);
+    int32_t set_camera(Camera_desc const& camera);
+    void    set_settings(Settings const& s) { settings_ = s; }
+
+    // Clears the film (start of a frame).
+    int32_t start_frame();
+
+    // Traces num_samples samples per pixel, samples first .. first + num_samples - 1 of the
+    // frame; sample i of a pixel always uses the same random stream.
+    int32_t render(uint32_t first_sample, uint32_t num_samples);
+
+    // Film resolve: rgb / weight per pixel (ACEScg linear), alpha 1, into host rgba floats.
+    int32_t resolve(float* rgba);
+
+    Stats const& stats() const { return stats_; }
+
+    bool ready() const { return scene_ready_ && camera_ready_; }
+
+    std::string const& error() const { return error_; }
+
+  private:
+    struct Device;
+    Device*     d_ = nullptr;
+    Settings    settings_;
+    Camera_desc camera_;
+    Stats       stats_;
+    bool        scene_ready_  = false;
+    bool        camera_ready_ = false;
+    std::string error_;
+
+    int32_t ensure_buffers(uint32_t paths);
+    int32_t fail_cuda(char const* what, int code);
+};
+
+}  // namespace spb::render

@@ -190,11 +190,13 @@ __device__ __forceinline__ uint32_t node_test(Ray_state const& r, uint4 const* _
 }
 
 
+// Per-lane traversal state kept in registers; the node-group stack itself is a separate
+// array (local memory), so that dynamic indexing into it does not pull these scalars out of
+// registers.
 struct Traversal {
     uint2    group;      // node group: child base, internal-child hit bits << 24 | imask
     uint2    tri_group;  // triangle group: triangle base, triangle hit bits
     uint32_t sp;
-    uint2    stack[Stack_size];
 };
 
 // Loads one ray (math::ray order: origin, min_t / direction, max_t) and resets the state.
@@ -226,7 +228,7 @@ __device__ __forceinline__ void start_ray(Ray_state& r, Traversal& tv, float4 ro
 // overflow receives a count if the stack guard ever trips (it cannot for trees of depth
 // <= Max_wide_depth); the ray then ends as a miss instead of writing out of bounds.
 template <bool Any_hit>
-__device__ __forceinline__ bool traversal_step(Ray_state& r, Traversal& tv,
+__device__ __forceinline__ bool traversal_step(Ray_state& r, Traversal& tv, uint2* stack,
                                                uint4 const* __restrict__ nodes,
                                                float4 const* __restrict__ triangles,
                                                float hit_margin, uint32_t* overflow) {
@@ -261,7 +263,7 @@ __device__ __forceinline__ bool traversal_step(Ray_state& r, Traversal& tv,
         if (tv.sp == 0) {
             return true;
         }
-        tv.group = tv.stack[--tv.sp];
+        tv.group = stack[--tv.sp];
     }
 
     uint32_t const b = 31u - __clz(tv.group.y & 0xFF000000u);
@@ -275,7 +277,7 @@ __device__ __forceinline__ bool traversal_step(Ray_state& r, Traversal& tv,
             r.best_id = Miss;
             return true;
         }
-        tv.stack[tv.sp++] = tv.group;
+        stack[tv.sp++] = tv.group;
     }
     uint32_t child_base, tri_base, imask;
     uint32_t const hits = node_test(r, nodes + 5 * size_t(node), child_base, tri_base, imask);

@@ -1,0 +1,132 @@
+"""Synthetic scenes for the path tracer, built through the su_* C API.
+
+``cornell(su, ...)`` issues the same sequence of su_* calls against whichever library ``su``
+binds (this package's or the reference's), so both render the identical scene:
+
+* a Cornell box: floor, ceiling and back wall white (albedo 0.75), left wall red
+  (0.75, 0.05, 0.05), right wall green (0.05, 0.75, 0.05) -- Substitute, roughness 1,
+  metallic 0 (the reference has no pure Lambert material);
+* a 0.5 x 0.5 m ceiling quad light (0.25 m^2), radiance 17, one-sided, facing down;
+* an icosphere of radius 0.3 subdivided 6 times (81,920 triangles) with a GGX conductor,
+  alpha 0.3 (roughness sqrt(0.3)), F0 = (0.95, 0.64, 0.54);
+* a pinhole camera with a 40 degree horizontal field of view;
+* PTMIS, max_bounces 8 (min_bounces 4, the reference default).
+Colours are given in sRGB; both libraries map them to ACEScg.
+"""
+
+from __future__ import annotations
+
+import json
+import math
+
+import numpy as np
+
+
+def icosphere(subdivisions: int):
+    """Unit icosphere: 20 * 4^subdivisions triangles, vertex valence 5 or 6."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.array(v, np.float64) / np.linalg.norm(v) for v in verts]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+             (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdivisions):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    return np.array(verts, np.float32), np.array(faces, np.uint32)
+
+
+def _quad(p0, p1, p2, p3, normal):
+    """Two triangles p0 p1 p2, p0 p2 p3 wound so that cross(b - a, c - a) points along normal."""
+    pos = np.array([p0, p1, p2, p3], np.float32)
+    idx = np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
+    n = np.array(normal, np.float32)
+    g = np.cross(pos[1] - pos[0], pos[2] - pos[0])
+    if np.dot(g, n) < 0:
+        idx = idx[:, ::-1].copy()
+    return pos, np.tile(n, (4, 1)), idx
+
+
+def cornell_geometry(sphere_subdivisions: int = 6):
+    """name -> (positions, normals, indices) in world space (y up, box x, z in [-1, 1], y in [0, 2])."""
+    g = {}
+    g["floor"] = _quad((-1, 0, -1), (1, 0, -1), (1, 0, 1), (-1, 0, 1), (0, 1, 0))
+    g["ceiling"] = _quad((-1, 2, -1), (-1, 2, 1), (1, 2, 1), (1, 2, -1), (0, -1, 0))
+    g["back"] = _quad((-1, 0, 1), (1, 0, 1), (1, 2, 1), (-1, 2, 1), (0, 0, -1))
+    g["left"] = _quad((-1, 0, -1), (-1, 0, 1), (-1, 2, 1), (-1, 2, -1), (1, 0, 0))
+    g["right"] = _quad((1, 0, -1), (1, 2, -1), (1, 2, 1), (1, 0, 1), (-1, 0, 0))
+    g["light"] = _quad((-0.25, 1.98, -0.25), (0.25, 1.98, -0.25), (0.25, 1.98, 0.25), (-0.25, 1.98, 0.25),
+                       (0, -1, 0))
+    v, f = icosphere(sphere_subdivisions)
+    g["sphere"] = ((0.3 * v + np.array([0.0, 0.3, 0.0], np.float32)).astype(np.float32), v.copy(), f)
+    return g
+
+
+def _material(su, kind, **params):
+    return su.su_create_material(json.dumps({"rendering": {kind: params}}).encode())
+
+
+def translation(x, y, z):
+    m = np.eye(4, dtype=np.float32)
+    m[3, :3] = (x, y, z)
+    return m
+
+
+def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounces: int = 8,
+            min_bounces: int = 4, fov_degrees: float = 40.0, camera_position=(0.0, 1.0, -3.4),
+            spp: int = 64, tonemap: bool = False):
+    """Issues the scene's su_* calls on an initialised engine; returns the camera entity."""
+    cam = su.su_create_camera_perspective(width, height, math.radians(fov_degrees))
+    su.set_transformation(cam, translation(*camera_position))
+    su.su_create_integrators(json.dumps({"surface": {"PTMIS": {"min_bounces": min_bounces,
+                                                              "max_bounces": max_bounces}}}).encode())
+    su.su_create_sampler(spp)
+    if tonemap:
+        su.su_create_defaults()
+
+    white = _material(su, "Substitute", color=[0.75, 0.75, 0.75], roughness=1.0, metallic=0.0)
+    red = _material(su, "Substitute", color=[0.75, 0.05, 0.05], roughness=1.0, metallic=0.0)
+    green = _material(su, "Substitute", color=[0.05, 0.75, 0.05], roughness=1.0, metallic=0.0)
+    metal = _material(su, "Substitute", color=[0.95, 0.64, 0.54], roughness=math.sqrt(0.3), metallic=1.0)
+    light = _material(su, "Light", emission=[17.0, 17.0, 17.0])
+
+    geo = cornell_geometry(sphere_subdivisions)
+    assign = {"floor": white, "ceiling": white, "back": white, "left": red, "right": green,
+              "light": light, "sphere": metal}
+    for name, (pos, nrm, idx) in geo.items():
+        shape = su.mesh(pos, nrm, idx)
+        prop = su.prop(shape, [assign[name]])
+        # props carry no default world transformation in the reference: always set one
+        su.set_transformation(prop, np.eye(4, dtype=np.float32))
+        if name == "light":
+            su.su_create_light(prop)
+    return cam
+
+
+def render_progressive(su, width: int, height: int, iterations: int, **scene):
+    """Progressive rendering through the C API: returns the (H, W, 3) mean image."""
+    assert su.su_init(True) == 0
+    try:
+        cornell(su, width, height, **scene)
+        assert su.su_start_render_frame(0) == 0, su.messages
+        for _ in range(iterations):
+            assert su.su_render_iteration() == 0
+        assert su.su_postprocess() == 0
+        img, _status = su.framebuffer(width, height)
+        return img[:, :, :3].copy()
+    finally:
+        su.su_release()

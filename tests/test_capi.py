@@ -19,6 +19,7 @@ def declared_symbols():
     for header in INCLUDE.glob("*.h"):
         text = header.read_text()
         names |= set(re.findall(r"SPB_API\s+[\w\s\*]+?\b(spb_\w+)\s*\(", text))
+        names |= set(re.findall(r"SU_LIBRARY_API\s+[\w\s\*]+?\b(su_\w+)\s*\(", text))
     return names
 
 
@@ -37,8 +38,52 @@ def test_library_exports_every_declared_symbol():
     assert not missing, f"declared but not exported: {sorted(missing)}"
     for name in declared_symbols():
         assert hasattr(lib, name)
-    # the ctypes prototypes cover the whole header
-    assert declared_symbols() <= set(_lib.PROTOTYPES)
+    # the ctypes prototypes cover both headers
+    from sprout_b200 import capi
+
+    assert {n for n in declared_symbols() if n.startswith("spb_")} <= set(_lib.PROTOTYPES)
+    assert {n for n in declared_symbols() if n.startswith("su_")} == set(capi.PROTOTYPES)
+
+
+def test_c_api_has_the_reference_entry_points():
+    """include/sprout.h declares the reference's 35 su_* functions (source/capi/sprout.h:39-122)."""
+    names = {n for n in declared_symbols() if n.startswith("su_")}
+    assert len(names) == 35
+
+
+def test_c_api_without_gpu_state():
+    """Engine lifecycle calls that need no device work return the reference's codes."""
+    from sprout_b200 import capi
+
+    su = capi.SuLibrary()
+    assert su.su_render() == -1 and su.su_release() == 0
+    assert su.su_init(False) == 0
+    assert su.su_init(False) == -1
+    assert su.su_create_material(b'{"rendering": {"Substitute": {"color": [1, 0, 0]}}}') == 0
+    assert su.su_create_material(b'{"rendering": {"Glass": {}}}') == capi.SU_RESOURCE_NULL
+    assert su.su_render_iteration() == -2
+    assert su.su_create_light(5) == -2
+    assert su.su_release() == 0
+
+
+def test_ggx_albedo_table_matches_reference_table():
+    """The energy-compensation table computed by this project against the reference's
+    generated table (material/ggx/ggx_integral.inl), read from the reference sources when
+    they are on this machine."""
+    import pathlib
+
+    src = pathlib.Path("/root/reference/source/core/scene/material/ggx/ggx_integral.inl")
+    if not src.exists():
+        import pytest
+
+        pytest.skip("reference sources not present")
+    text = src.read_text()
+    body = text[text.index("E[32][32]"):]
+    body = body[: body.index("};")]
+    ref = np.array([float(x) for x in re.findall(r"([0-9.]+(?:e[-+]?[0-9]+)?)f", body)][:1024], np.float32)
+    mine = np.zeros(1024, np.float32)
+    assert _lib.load().spb_ggx_albedo_table(mine.ctypes.data) == 0
+    assert np.max(np.abs(mine - ref)) < 5e-5
 
 
 def test_argument_errors_use_documented_codes():
