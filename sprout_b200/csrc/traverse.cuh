@@ -232,6 +232,9 @@ __device__ __forceinline__ bool traversal_step(Ray_state& r, Traversal& tv, uint
                                                uint4 const* __restrict__ nodes,
                                                float4 const* __restrict__ triangles,
                                                float hit_margin, uint32_t* overflow) {
+    // Single exit (no early return): the place where the two branches rejoin decides where a
+    // diverged warp reconverges, and keeping it at the end measured fastest.
+    bool done = false;
     if (tv.tri_group.y != 0) {
         uint32_t const k = __ffs(tv.tri_group.y) - 1;
         tv.tri_group.y &= tv.tri_group.y - 1;
@@ -245,45 +248,47 @@ __device__ __forceinline__ bool traversal_step(Ray_state& r, Traversal& tv, uint
             uint32_t const id = __float_as_uint(a.w);
             if (Any_hit) {
                 r.best_id = id;
-                return true;
-            }
-            if (t < r.tbest || id < r.best_id) {
+                done      = true;
+            } else if (t < r.tbest || id < r.best_id) {
                 r.tbest   = t;
                 r.best_id = id;
                 r.u       = u;
                 r.v       = v;
             }
         }
-        return false;
-    }
-
-    // A spent node group is replaced by the next one from the stack in the same step, so no
-    // step is spent on the pop alone.
-    if (!(tv.group.y & 0xFF000000u)) {
-        if (tv.sp == 0) {
-            return true;
+    } else {
+        // A spent node group is replaced by the next one from the stack in the same step, so
+        // no step is spent on the pop alone.
+        if (!(tv.group.y & 0xFF000000u) && tv.sp > 0) {
+            tv.group = stack[--tv.sp];
         }
-        tv.group = stack[--tv.sp];
-    }
-
-    uint32_t const b = 31u - __clz(tv.group.y & 0xFF000000u);
-    tv.group.y &= ~(1u << b);
-    uint32_t const slot = (b - 24u) ^ r.oct_inv;
-    uint32_t const rel  = __popc(tv.group.y & 0xFFu & ((1u << slot) - 1u));
-    uint32_t const node = tv.group.x + rel;
-    if (tv.group.y & 0xFF000000u) {
-        if (tv.sp >= Stack_size) {
-            atomicAdd(overflow, 1u);
-            r.best_id = Miss;
-            return true;
+        if (tv.group.y & 0xFF000000u) {
+            uint32_t const b = 31u - __clz(tv.group.y & 0xFF000000u);
+            tv.group.y &= ~(1u << b);
+            uint32_t const slot = (b - 24u) ^ r.oct_inv;
+            uint32_t const rel  = __popc(tv.group.y & 0xFFu & ((1u << slot) - 1u));
+            uint32_t const node = tv.group.x + rel;
+            if (tv.group.y & 0xFF000000u) {
+                if (tv.sp < Stack_size) {
+                    stack[tv.sp++] = tv.group;
+                } else {
+                    atomicAdd(overflow, 1u);
+                    r.best_id = Miss;
+                    done      = true;
+                }
+            }
+            if (!done) {
+                uint32_t child_base, tri_base, imask;
+                uint32_t const hits =
+                    node_test(r, nodes + 5 * size_t(node), child_base, tri_base, imask);
+                tv.group     = make_uint2(child_base, (hits & 0xFF000000u) | imask);
+                tv.tri_group = make_uint2(tri_base, hits & 0x00FFFFFFu);
+            }
+        } else {
+            done = true;
         }
-        stack[tv.sp++] = tv.group;
     }
-    uint32_t child_base, tri_base, imask;
-    uint32_t const hits = node_test(r, nodes + 5 * size_t(node), child_base, tri_base, imask);
-    tv.group            = make_uint2(child_base, (hits & 0xFF000000u) | imask);
-    tv.tri_group        = make_uint2(tri_base, hits & 0x00FFFFFFu);
-    return false;
+    return done;
 }
 
 }  // namespace spb::gpu
