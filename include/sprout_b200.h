@@ -143,6 +143,28 @@ SPB_API int32_t spb_synth_rays(uint64_t first, uint64_t count, uint32_t seed, fl
                                float* rays, uint32_t num_threads);
 
 /*
+ * Closest hit without any device allocation: rays and results in host memory, staged through
+ * a fixed device array that the library reserves when it is loaded.  No counterpart in the
+ * reference (its CPU cast allocates nothing on a GPU).  It is for callers that cannot call
+ * cudaMalloc: a cudaMalloc may synchronize the device and may fail when device memory runs
+ * out, so a frame loop with a fixed time budget, or an application whose own allocator owns
+ * all device memory, must not allocate per call -- spb_intersect_host allocates staging
+ * buffers on its first call, this entry point never does.
+ *
+ * Limit: at most SPB_STATIC_MAX_RAYS rays per call (larger batches are rejected with
+ * SPB_ERROR_ARGUMENT); the fixed array (SPB_STATIC_MAX_RAYS * 40 bytes + 256 bytes, about
+ * 2.5 MiB) stays allocated on every GPU that loads the library until the process exits.
+ * The first call on a device looks up the array's device address (once per device).
+ * All calls share the one array, so calls that overlap on the GPU -- from several host
+ * threads, or on several trees at once -- race and must be serialized by the caller.
+ * Results are identical to spb_intersect_host.  Uses the legacy default stream and returns
+ * when the results are in host memory.
+ */
+#define SPB_STATIC_MAX_RAYS 65536ull
+SPB_API int32_t spb_intersect_host_static(spb_tree* tree, float const* rays, uint64_t num_rays,
+                                          uint32_t* ids, float* ts);
+
+/*
  * The 32 x 32 GGX directional-albedo table the Substitute material's energy compensation
  * reads (row = alpha index, column = cos(theta_o) index, both i / 31), as computed by this
  * library.  Stands in for the reference's generated table E

@@ -54,6 +54,7 @@ PROTOTYPES = {
                                       ctypes.POINTER(c_u32), c_vp, c_vp]),
     "spb_synth_rays": (c_i32, [c_u64, c_u64, c_u32, c_f32, c_vp, c_u32]),
     "spb_ggx_albedo_table": (c_i32, [c_vp]),
+    "spb_intersect_host_static": (c_i32, [c_vp, c_vp, c_u64, c_vp, c_vp]),
 }
 
 _lib = None

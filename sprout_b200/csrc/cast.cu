@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "bvh8.hpp"
@@ -453,5 +454,97 @@ extern "C" SPB_API int32_t spb_tree_status(spb_tree* tree, uint32_t* overflowed_
     uint32_t host[2 * Num_counter_slots];
     SPB_CUDA(cudaMemcpy(host, tree->d_counters, sizeof(host), cudaMemcpyDeviceToHost));
     *overflowed_rays = host[1] + host[3] + host[5];
+    return SPB_OK;
+}
+
+// ---- Closest hit without any device allocation ------------------------------------------
+//
+// Some callers cannot call cudaMalloc: a cudaMalloc may synchronize the whole device and may
+// fail once device memory is exhausted, so a frame loop with a fixed time budget, or a host
+// application whose own allocator owns all device memory, must not allocate on the way to a
+// cast.  spb_intersect_host allocates device staging buffers on its first call;
+// spb_intersect_host_static instead stages rays and results in the file-scope array below,
+// which every GPU that loads this library holds until the process exits.
+
+namespace {
+
+constexpr uint64_t Static_max_rays      = SPB_STATIC_MAX_RAYS;
+constexpr size_t   Static_counter_bytes = 256;  // work counter + overflow counter, padded
+constexpr size_t   Static_scratch_bytes = Static_counter_bytes + Static_max_rays * (32 + 4 + 4);
+constexpr int      Static_max_devices   = 64;
+
+__device__ __align__(256) unsigned char g_static_scratch[Static_scratch_bytes];
+
+std::mutex     g_static_mutex;
+unsigned char* g_static_address[Static_max_devices] = {};
+
+// Device address of g_static_scratch on the current device (set up once per device; the
+// host-side symbol g_static_scratch itself is not a device address).
+int32_t static_scratch(int device, unsigned char** out) {
+    if (device < 0 || device >= Static_max_devices) {
+        return spb::fail(SPB_ERROR_STATE, "spb_intersect_host_static: device %d not supported",
+                         device);
+    }
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_address[device]) {
+        void*             ptr = nullptr;
+        cudaError_t const e   = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (e != cudaSuccess) {
+            return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
+        }
+        g_static_address[device] = static_cast<unsigned char*>(ptr);
+    }
+    *out = g_static_address[device];
+    return SPB_OK;
+}
+
+}  // namespace
+
+extern "C" SPB_API int32_t spb_intersect_host_static(spb_tree* tree, float const* rays,
+                                                     uint64_t num_rays, uint32_t* ids,
+                                                     float* ts) {
+    spb::clear_error();
+    if (int32_t const s = check_cast(tree, rays, num_rays, ids && ts,
+                                     "spb_intersect_host_static")) {
+        return s;
+    }
+    if (num_rays > Static_max_rays) {
+        return spb::fail(SPB_ERROR_ARGUMENT,
+                         "spb_intersect_host_static: %llu rays exceed the static scratch limit "
+                         "of %llu rays per call",
+                         (unsigned long long)num_rays, (unsigned long long)Static_max_rays);
+    }
+    if (num_rays == 0) {
+        return SPB_OK;
+    }
+    Device_scope scope(tree->device);
+    unsigned char* base = nullptr;
+    if (int32_t const s = static_scratch(tree->device, &base)) {
+        return s;
+    }
+    auto* counters = reinterpret_cast<uint32_t*>(base);
+    auto* d_rays   = reinterpret_cast<float4*>(base + Static_counter_bytes);
+    auto* d_ids    = reinterpret_cast<uint32_t*>(base + Static_counter_bytes + Static_max_rays * 32);
+    auto* d_ts     = reinterpret_cast<float*>(base + Static_counter_bytes + Static_max_rays * 36);
+    uint32_t const n = uint32_t(num_rays);
+
+    // The array keeps the previous call's contents: both counters must start at zero.
+    SPB_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(uint32_t), nullptr));
+    SPB_CUDA(cudaMemcpyAsync(d_rays, rays, size_t(n) * 32, cudaMemcpyHostToDevice, nullptr));
+    int const grid = std::max(1, std::min(tree->grid_hit, int((n + Block - 1) / Block)));
+    cast_kernel<false><<<grid, Block, 0, nullptr>>>(reinterpret_cast<uint4 const*>(tree->d_nodes),
+                                                    tree->d_tris, d_rays, n, d_ids, d_ts, nullptr,
+                                                    nullptr, counters, tree->hit_margin);
+    SPB_CUDA(cudaGetLastError());
+    SPB_CUDA(cudaMemcpyAsync(ids, d_ids, size_t(n) * 4, cudaMemcpyDeviceToHost, nullptr));
+    SPB_CUDA(cudaMemcpyAsync(ts, d_ts, size_t(n) * 4, cudaMemcpyDeviceToHost, nullptr));
+    uint32_t overflow = 0;
+    SPB_CUDA(cudaMemcpyAsync(&overflow, counters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                             nullptr));
+    SPB_CUDA(cudaStreamSynchronize(nullptr));
+    if (overflow != 0) {
+        return spb::fail(SPB_ERROR_STATE, "spb_intersect_host_static: %u rays overflowed the stack",
+                         overflow);
+    }
     return SPB_OK;
 }
