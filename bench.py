@@ -18,6 +18,7 @@ Prints one JSON line (rank 0).
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import pathlib
@@ -52,6 +53,8 @@ def parse_args():
     p.add_argument("--mesh-n", type=int, default=MESH_N)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-render", action="store_true", help="skip the path-tracer measurement")
+    p.add_argument("--render-spp", type=int, default=64)
     return p.parse_args()
 
 
@@ -214,6 +217,80 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line))
 
 
+RENDER_SIZE = 512
+RENDER_CONFIG = ("Cornell box (5 walls, 0.25 m^2 light of radiance 17, 81,920-tri GGX conductor sphere "
+                 "alpha 0.3), 512x512, 64 spp, PTMIS max depth 8, seed 0")
+
+
+def rel_mse(x, r):
+    return float(np.mean((x - r) ** 2 / (r * r + 1e-2)))
+
+
+def measure_render(args, with_cpu):
+    """Plain MIS path tracing of the Cornell scene through the su_* C API (config 1)."""
+    from sprout_b200 import _lib, capi, scenes
+
+    lib = _lib.load()
+    stats = _lib.RenderStats()
+    su = capi.SuLibrary()
+    size, spp = RENDER_SIZE, args.render_spp
+    assert su.su_init(False) == 0
+    try:
+        scenes.cornell(su, size, size, sphere_subdivisions=6, tonemap=True, spp=spp)
+        assert su.su_render_frame(0) == 0, su.messages  # scene upload + BVH build + warm-up
+        times, wall = [], []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            assert su.su_render_frame(0) == 0
+            assert su.su_postprocess() == 0
+            img, _ = su.framebuffer(size, size)
+            wall.append(time.perf_counter() - t0)
+            lib.spb_render_last_stats(ctypes.byref(stats))
+            times.append(stats.device_seconds)
+        dev_s = statistics.median(times)
+        rays = stats.extension_rays + stats.shadow_rays
+        out = {"config": RENDER_CONFIG, "msamples_s": round(size * size * spp / dev_s / 1e6, 3),
+               "mrays_s": round(rays / dev_s / 1e6, 3), "ms_per_frame": round(1e3 * dev_s, 3),
+               "rays_per_sample": round(rays / (size * size * spp), 3),
+               "e2e_msamples_s": round(size * size * spp / statistics.median(wall) / 1e6, 3),
+               "e2e_note": "wall time of su_render_frame + su_postprocess + su_copy_framebuffer (host)"}
+
+        # time to relMSE 0.01 against a 4096-spp GPU image (plain MIS; guiding is not built)
+        scenes.cornell  # noqa: B018 (scene stays loaded; only the sample count changes)
+        assert su.su_create_sampler(4096) == 0
+        assert su.su_render_frame(0) == 0 and su.su_postprocess() == 0
+        ref, _ = su.framebuffer(size, size)
+        ref = ref[:, :, :3].copy()
+        k, reached = 1, None
+        while k <= 1024:
+            assert su.su_create_sampler(k) == 0
+            assert su.su_render_frame(0) == 0 and su.su_postprocess() == 0
+            lib.spb_render_last_stats(ctypes.byref(stats))
+            cur, _ = su.framebuffer(size, size)
+            e = rel_mse(cur[:, :, :3], ref)
+            if e <= 0.01:
+                reached = {"spp": k, "seconds": round(stats.device_seconds, 5), "rel_mse": round(e, 5)}
+                break
+            k *= 2
+        out["time_to_rel_mse_0.01"] = reached
+        out["rel_mse_reference"] = "4096-spp render of this renderer (FP32 Kahan film, FP64 resolve)"
+    finally:
+        su.su_release()
+
+    if with_cpu:
+        import oracle
+
+        if oracle.REF_RENDER.exists():
+            _, timing = oracle.reference_render(
+                lambda r: scenes.cornell(r, size, size, sphere_subdivisions=6, tonemap=True, spp=spp),
+                size, size, 0, progressive=False)
+            out["cpu_baseline"] = {"msamples_s": round(size * size * spp / timing["render_s"] / 1e6, 4),
+                                   "seconds": round(timing["render_s"], 3), "cores": os.cpu_count(),
+                                   "kind": "reference",
+                                   "sample": "full frame, reference su_render_frame (batch) on all host threads"}
+    return out
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_setup()
@@ -335,6 +412,10 @@ def main():
                             "sample": f"full workload ({args.rays} rays), reference Builder_SAH(16,64,4) + "
                                       f"Tree::intersect on all host threads, mean of 2 passes"}
 
+    render = None
+    if rank == 0 and not args.no_render:
+        render = measure_render(args, with_cpu=(world == 1 and not args.no_cpu_baseline))
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
@@ -354,6 +435,7 @@ def main():
                          "traffic": (round(traffic_per_ray * args.rays) if traffic_per_ray else None),
                          "note": "traversal is L1/L2-latency bound; HBM carries only rays and results"},
             "any_hit_mrays_s": round(world * any_hit_mrays, 3),
+            "render": render,
             "e2e": e2e,
             "cpu_baseline": cpu_baseline,
             "gpu_launches": args.steps,

@@ -165,6 +165,22 @@ SPB_API int32_t spb_intersect_host_static(spb_tree* tree, float const* rays, uin
                                           uint32_t* ids, float* ts);
 
 /*
+ * Counters of the path tracer's last su_render / su_render_frame / su_render_iteration call
+ * (the su_* engine of include/sprout.h): camera samples traced, closest-hit rays (camera and
+ * continuation), any-hit (shadow) rays, and the device time between the first and last
+ * kernel.  No counterpart in the reference (it logs wall-clock phases only,
+ * rendering_driver.cpp:99-136).  SPB_ERROR_ARGUMENT if there is no engine.
+ */
+typedef struct spb_render_stats {
+    uint64_t paths;
+    uint64_t extension_rays;
+    uint64_t shadow_rays;
+    double   device_seconds;
+    uint32_t overflow;
+} spb_render_stats;
+SPB_API int32_t spb_render_last_stats(spb_render_stats* out);
+
+/*
  * The 32 x 32 GGX directional-albedo table the Substitute material's energy compensation
  * reads (row = alpha index, column = cos(theta_o) index, both i / 31), as computed by this
  * library.  Stands in for the reference's generated table E

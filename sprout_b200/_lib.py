@@ -37,6 +37,16 @@ class TreeInfo(ctypes.Structure):
     ]
 
 
+class RenderStats(ctypes.Structure):
+    _fields_ = [
+        ("paths", c_u64),
+        ("extension_rays", c_u64),
+        ("shadow_rays", c_u64),
+        ("device_seconds", ctypes.c_double),
+        ("overflow", c_u32),
+    ]
+
+
 # name -> (restype, argtypes); mirrors include/sprout_b200.h one to one.
 PROTOTYPES = {
     "spb_last_error": (ctypes.c_char_p, []),
@@ -54,6 +64,7 @@ PROTOTYPES = {
                                       ctypes.POINTER(c_u32), c_vp, c_vp]),
     "spb_synth_rays": (c_i32, [c_u64, c_u64, c_u32, c_f32, c_vp, c_u32]),
     "spb_ggx_albedo_table": (c_i32, [c_vp]),
+    "spb_render_last_stats": (c_i32, [ctypes.POINTER(RenderStats)]),
     "spb_intersect_host_static": (c_i32, [c_vp, c_vp, c_u64, c_vp, c_vp]),
 }
 

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/sprout.h"
+#include "../../include/sprout_b200.h"
 #include "common.hpp"
 #include "json.hpp"
 #include "render.hpp"
@@ -56,6 +57,7 @@ struct Engine {
     spb::render::Settings settings;
     spb::render::Renderer renderer;
     bool                  frame_started = false;
+    bool                  scene_dirty    = true;   // host scene changed since the last upload
     bool                  tonemap_linear = false;  // su_create_defaults: Linear tonemapper
     uint32_t              iteration     = 0;
     std::vector<float>    target;  // resolved rgba
@@ -245,6 +247,7 @@ SU_LIBRARY_API int32_t su_clear(void) {
     engine->materials.clear();
     engine->camera_entity = Null;
     engine->frame_started = false;
+    engine->scene_dirty   = true;
     return 0;
 }
 
@@ -283,6 +286,7 @@ SU_LIBRARY_API uint32_t su_create_camera_perspective(uint32_t width, uint32_t he
     e.camera = true;
     engine->entities.push_back(e);
     engine->camera_entity = uint32_t(engine->entities.size() - 1);
+    engine->scene_dirty   = true;
     engine->width         = width;
     engine->height        = height;
     engine->fov           = fov;
@@ -332,6 +336,7 @@ SU_LIBRARY_API int32_t su_camera_set_resolution(uint32_t width, uint32_t height)
     engine->width         = width;
     engine->height        = height;
     engine->frame_started = false;
+    engine->scene_dirty   = true;
     return 0;
 }
 
@@ -371,6 +376,7 @@ SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
     }
     engine->settings        = s;
     engine->have_integrator = true;
+    engine->scene_dirty     = true;
     return 0;
 }
 
@@ -435,6 +441,7 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
         return Null;
     }
     engine->materials.push_back(m);
+    engine->scene_dirty = true;
     return uint32_t(engine->materials.size() - 1);
 }
 
@@ -497,6 +504,7 @@ SU_LIBRARY_API uint32_t su_create_triangle_mesh_async(
     }
     engine->meshes.push_back(std::move(mesh));
     engine->frame_started = false;
+    engine->scene_dirty   = true;
     return First_mesh_id + uint32_t(engine->meshes.size() - 1);
 }
 
@@ -525,6 +533,7 @@ SU_LIBRARY_API uint32_t su_create_prop(uint32_t shape, uint32_t num_materials,
     }
     engine->entities.push_back(e);
     engine->frame_started = false;
+    engine->scene_dirty   = true;
     return uint32_t(engine->entities.size() - 1);
 }
 
@@ -588,6 +597,7 @@ SU_LIBRARY_API int32_t su_entity_set_transformation(uint32_t entity, float const
     }
     std::memcpy(engine->entities[entity].trafo, trafo, sizeof(float) * 16);
     engine->frame_started = false;
+    engine->scene_dirty   = true;
     return 0;
 }
 
@@ -611,8 +621,12 @@ SU_LIBRARY_API int32_t su_start_render_frame(uint32_t frame) {
     if (!ready()) {
         return -2;
     }
-    if (int32_t const s = compile_scene()) {
-        return s;
+    // The scene is flattened, its BVH built and uploaded only when something changed.
+    if (engine->scene_dirty) {
+        if (int32_t const s = compile_scene()) {
+            return s;
+        }
+        engine->scene_dirty = false;
     }
     if (engine->renderer.start_frame()) {
         log(SU_LOG_ERROR, engine->renderer.error());
@@ -732,6 +746,19 @@ SU_LIBRARY_API int32_t su_copy_framebuffer(uint32_t type, uint32_t width, uint32
         return 0;
     }
     return -2;
+}
+
+SPB_API int32_t spb_render_last_stats(spb_render_stats* out) {
+    if (!engine || !out) {
+        return SPB_ERROR_ARGUMENT;
+    }
+    spb::render::Stats const& st = engine->renderer.stats();
+    out->paths          = st.paths;
+    out->extension_rays = st.extension_rays;
+    out->shadow_rays    = st.shadow_rays;
+    out->device_seconds = st.seconds;
+    out->overflow       = st.overflow;
+    return SPB_OK;
 }
 
 SU_LIBRARY_API int32_t su_register_log(Post post) {
