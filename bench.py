@@ -75,77 +75,89 @@ def profiled_traffic():
     return float(m.group(1)) if m else None
 
 
+CLOCK_SAMPLER = r"""
+import sys, time
+import pynvml
+pynvml.nvmlInit()
+entry = sys.argv[1]
+h = (pynvml.nvmlDeviceGetHandleByUUID(entry) if entry.startswith("GPU-")
+     else pynvml.nvmlDeviceGetHandleByIndex(int(entry)))
+print("max", pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM), flush=True)
+while True:
+    mhz = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+    bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+    print(f"{time.monotonic():.6f} {mhz} {bits}", flush=True)
+    time.sleep(0.002)
+"""
+
+
 class ClockSampler:
-    """SM clock and clock-event (throttle) reasons, read through NVML every 2 ms by a
-    background thread while the timed region runs (read-only queries; no setting changes)."""
+    """SM clock and clock-event (throttle) reasons read through NVML every 2 ms by a separate
+    process (read-only queries; no setting changes); mark() brackets the timed region and
+    summary() keeps the samples taken inside it."""
 
     REASONS = {
-        "hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
-        "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
-        "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
-        "sw_power_cap": "nvmlClocksEventReasonSwPowerCap",
-        "hw_power_brake": "nvmlClocksEventReasonHwPowerBrakeSlowdown",
+        "hw_slowdown": 0x8,
+        "sw_thermal_slowdown": 0x20,
+        "hw_thermal_slowdown": 0x40,
+        "hw_power_brake": 0x80,
+        "sw_power_cap": 0x4,
     }
 
-    def __init__(self, gpu_index: int, period_s: float = 0.002):
-        self.gpu = gpu_index
-        self.period = period_s
-        self.samples = []
+    def __init__(self, gpu_index: int):
+        visible = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
+        self.entry = visible[gpu_index] if gpu_index < len(visible) else str(gpu_index)
+        self.proc = None
+        self.lines = []
         self.max_mhz = None
-        self._stop = threading.Event()
-        self._nvml = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
-            import pynvml
-
-            pynvml.nvmlInit()
-            self._nvml = pynvml
-            visible = [v.strip() for v in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if v.strip()]
-            entry = visible[self.gpu] if self.gpu < len(visible) else None
-            if entry and entry.startswith("GPU-"):
-                self._handle = pynvml.nvmlDeviceGetHandleByUUID(entry)
-            else:
-                index = int(entry) if entry and entry.isdigit() else self.gpu
-                self._handle = pynvml.nvmlDeviceGetHandleByIndex(index)
-            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._handle, pynvml.NVML_CLOCK_SM)
-            self._masks = {k: getattr(pynvml, v) for k, v in self.REASONS.items() if hasattr(pynvml, v)}
-            self._thread = threading.Thread(target=self._run, daemon=True)
-            self._thread.start()
-        except Exception:  # NVML unavailable: the record says so
-            self._nvml = None
+            self.proc = subprocess.Popen([sys.executable, "-c", CLOCK_SAMPLER, self.entry],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+            deadline = time.monotonic() + 20.0
+            while len(self.lines) < 3 and time.monotonic() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
+        except OSError:
+            self.proc = None
         return self
 
-    def _run(self):
-        nv = self._nvml
-        while not self._stop.is_set():
-            try:
-                mhz = nv.nvmlDeviceGetClockInfo(self._handle, nv.NVML_CLOCK_SM)
-                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self._handle)
-                self.samples.append((mhz, reasons))
-            except Exception:
-                pass
-            time.sleep(self.period)
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.split())
+
+    def mark_start(self):
+        self.t0 = time.monotonic()
+
+    def mark_end(self):
+        self.t1 = time.monotonic()
+        time.sleep(0.01)
 
     def __exit__(self, *exc):
-        self._stop.set()
-        if self._nvml is not None:
-            self._thread.join(timeout=2)
+        if self.proc:
+            self.proc.terminate()
             try:
-                self._nvml.nvmlShutdown()
-            except Exception:
-                pass
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
 
     def summary(self):
-        if not self.samples:
+        samples = []
+        for parts in self.lines:
+            if parts and parts[0] == "max":
+                self.max_mhz = int(parts[1])
+            elif len(parts) == 3:
+                t, mhz, bits = float(parts[0]), int(parts[1]), int(parts[2])
+                if self.t0 is not None and self.t0 <= t <= (self.t1 or t):
+                    samples.append((mhz, bits))
+        if not samples:
             return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "samples": 0}
-        seen = set()
-        for _, bits in self.samples:
-            for name, mask in self._masks.items():
-                if bits & mask:
-                    seen.add(name)
-        return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
-                "reasons": sorted(seen), "samples": len(self.samples), "source": "NVML, 2 ms period"}
+        seen = sorted({name for _, bits in samples for name, mask in self.REASONS.items() if bits & mask})
+        return {"sm_mhz": statistics.median(m for m, _ in samples), "sm_max_mhz": self.max_mhz,
+                "reasons": seen, "samples": len(samples), "source": "NVML in a separate process, 2 ms period"}
 
 
 def dist_setup():
@@ -217,78 +229,12 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line))
 
 
-RENDER_SIZE = 512
-RENDER_CONFIG = ("Cornell box (5 walls, 0.25 m^2 light of radiance 17, 81,920-tri GGX conductor sphere "
-                 "alpha 0.3), 512x512, 64 spp, PTMIS max depth 8, seed 0")
-
-
-def rel_mse(x, r):
-    return float(np.mean((x - r) ** 2 / (r * r + 1e-2)))
-
-
 def measure_render(args, with_cpu):
     """Plain MIS path tracing of the Cornell scene through the su_* C API (config 1)."""
-    from sprout_b200 import _lib, capi, scenes
+    from sprout_b200 import render_bench
 
-    lib = _lib.load()
-    stats = _lib.RenderStats()
-    su = capi.SuLibrary()
-    size, spp = RENDER_SIZE, args.render_spp
-    assert su.su_init(False) == 0
-    try:
-        scenes.cornell(su, size, size, sphere_subdivisions=6, tonemap=True, spp=spp)
-        assert su.su_render_frame(0) == 0, su.messages  # scene upload + BVH build + warm-up
-        times, wall = [], []
-        for _ in range(3):
-            t0 = time.perf_counter()
-            assert su.su_render_frame(0) == 0
-            assert su.su_postprocess() == 0
-            img, _ = su.framebuffer(size, size)
-            wall.append(time.perf_counter() - t0)
-            lib.spb_render_last_stats(ctypes.byref(stats))
-            times.append(stats.device_seconds)
-        dev_s = statistics.median(times)
-        rays = stats.extension_rays + stats.shadow_rays
-        out = {"config": RENDER_CONFIG, "msamples_s": round(size * size * spp / dev_s / 1e6, 3),
-               "mrays_s": round(rays / dev_s / 1e6, 3), "ms_per_frame": round(1e3 * dev_s, 3),
-               "rays_per_sample": round(rays / (size * size * spp), 3),
-               "e2e_msamples_s": round(size * size * spp / statistics.median(wall) / 1e6, 3),
-               "e2e_note": "wall time of su_render_frame + su_postprocess + su_copy_framebuffer (host)"}
-
-        # time to relMSE 0.01 against a 4096-spp GPU image (plain MIS; guiding is not built)
-        scenes.cornell  # noqa: B018 (scene stays loaded; only the sample count changes)
-        assert su.su_create_sampler(4096) == 0
-        assert su.su_render_frame(0) == 0 and su.su_postprocess() == 0
-        ref, _ = su.framebuffer(size, size)
-        ref = ref[:, :, :3].copy()
-        k, reached = 1, None
-        while k <= 1024:
-            assert su.su_create_sampler(k) == 0
-            assert su.su_render_frame(0) == 0 and su.su_postprocess() == 0
-            lib.spb_render_last_stats(ctypes.byref(stats))
-            cur, _ = su.framebuffer(size, size)
-            e = rel_mse(cur[:, :, :3], ref)
-            if e <= 0.01:
-                reached = {"spp": k, "seconds": round(stats.device_seconds, 5), "rel_mse": round(e, 5)}
-                break
-            k *= 2
-        out["time_to_rel_mse_0.01"] = reached
-        out["rel_mse_reference"] = "4096-spp render of this renderer (FP32 Kahan film, FP64 resolve)"
-    finally:
-        su.su_release()
-
-    if with_cpu:
-        import oracle
-
-        if oracle.REF_RENDER.exists():
-            _, timing = oracle.reference_render(
-                lambda r: scenes.cornell(r, size, size, sphere_subdivisions=6, tonemap=True, spp=spp),
-                size, size, 0, progressive=False)
-            out["cpu_baseline"] = {"msamples_s": round(size * size * spp / timing["render_s"] / 1e6, 4),
-                                   "seconds": round(timing["render_s"], 3), "cores": os.cpu_count(),
-                                   "kind": "reference",
-                                   "sample": "full frame, reference su_render_frame (batch) on all host threads"}
-    return out
+    return render_bench.measure(size=512, spp=args.render_spp, frames=3, convergence=True,
+                                cpu_reference=with_cpu)
 
 
 def main():
@@ -336,6 +282,7 @@ def main():
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     with ClockSampler(local) as clocks:
         barrier()
+        clocks.mark_start()
         t_begin = torch.cuda.Event(enable_timing=True)
         t_end = torch.cuda.Event(enable_timing=True)
         t_begin.record(stream)
@@ -345,6 +292,7 @@ def main():
             ends[k].record(stream)
         t_end.record(stream)
         barrier()
+        clocks.mark_end()
     elapsed = t_begin.elapsed_time(t_end) / 1e3
     kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     if dist is not None:
