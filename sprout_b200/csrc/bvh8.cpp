@@ -302,7 +302,7 @@ float hit_margin_for(double extent, double magnitude) {
 
 bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* positions,
                     uint32_t const* indices, uint32_t num_threads, Wide_bvh& out,
-                    std::string& error) {
+                    std::string& error, uint32_t const* tri_class) {
     out = Wide_bvh();
 
     if (num_triangles == 0) {
@@ -537,7 +537,8 @@ bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* 
                         wt.e1[a] = pb[a] - pa[a];
                         wt.e2[a] = pc2[a] - pa[a];
                     }
-                    wt.id = t;
+                    wt.id        = t;
+                    wt.tri_class = tri_class ? tri_class[t] : 0u;
                     out.triangles.push_back(wt);
                 }
                 tri_offset += cnt;

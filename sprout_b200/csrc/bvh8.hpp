@@ -32,12 +32,13 @@ struct alignas(16) Wide_node {
 static_assert(sizeof(Wide_node) == 80, "Wide_node must be 80 bytes");
 
 // One triangle, 48 bytes: vertex a, edges b - a and c - a (exactly the values the
-// Möller-Trumbore test computes first), and the caller's triangle index.
+// Möller-Trumbore test computes first), the caller's triangle index and a class word the
+// traversal can filter on (the path tracer marks participating-medium boundaries).
 struct alignas(16) Wide_triangle {
     float    a[3];
     uint32_t id;
     float    e1[3];
-    uint32_t pad0;
+    uint32_t tri_class;
     float    e2[3];
     uint32_t pad1;
 };
@@ -61,8 +62,9 @@ float hit_margin_for(double extent, double magnitude);
 constexpr uint32_t Max_wide_depth = 48;
 
 // Builds the 8-wide tree.  Returns false (with a message) if the input is unusable.
+// tri_class (optional, one word per triangle) is stored with each triangle.
 bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* positions,
                     uint32_t const* indices, uint32_t num_threads, Wide_bvh& out,
-                    std::string& error);
+                    std::string& error, uint32_t const* tri_class = nullptr);
 
 }  // namespace spb

@@ -436,6 +436,42 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
             (emission.x > 0.f || emission.y > 0.f || emission.z > 0.f)) {
             log(SU_LOG_WARNING, "su_create_material: Substitute emission is ignored by this renderer");
         }
+    } else if (type == "Volumetric") {
+        // material_provider.cpp:767-849 (homogeneous case): colour 0.5 by default, attenuation
+        // and subsurface colours default to it, distance 1, anisotropy clamped to +-0.999;
+        // coefficients from attenuation() (collision_coefficients.inl:50-71).
+        if (desc.find("density") || desc.find("temperature")) {
+            log(SU_LOG_ERROR, "su_create_material: density/temperature grids are not supported");
+            return Null;
+        }
+        V3 color = srgb_to_ap1(V3{0.5f, 0.5f, 0.5f});
+        read_color(desc.find("color"), color);
+        V3 ac = color;
+        V3 ssc = color;
+        read_color(desc.find("attenuation_color"), ac);
+        read_color(desc.find("subsurface_color"), ssc);
+        float const distance = float(spb::json::number_or(desc.find("attenuation_distance"), 1.0));
+        float const g = std::clamp(float(spb::json::number_or(desc.find("anisotropy"), 0.0)), -0.999f,
+                                   0.999f);
+        float const acs[3]  = {ac.x, ac.y, ac.z};
+        float const sscs[3] = {ssc.x, ssc.y, ssc.z};
+        float       mu_a[3];
+        float       mu_s[3];
+        for (int k = 0; k < 3; ++k) {
+            float const ca     = std::clamp(acs[k], 0.01f, 0.991102f);
+            float const mu_t   = -std::log(ca) / distance;
+            float const x      = sscs[k];
+            float const root   = std::sqrt(9.59217f + 41.6808f * x + 17.7126f * x * x);
+            float const factor = std::clamp(4.097125f + 4.20863f * x - root, 0.f, 1.f);
+            float const fsq    = factor * factor;
+            float const pss    = (1.f - fsq) / (1.f - g * fsq);
+            mu_a[k]            = mu_t * (1.f - pss);
+            mu_s[k]            = mu_t - mu_a[k];
+        }
+        m.type = spb::shading::Type_volume;
+        m.g    = g;
+        m.mu_a = V3{mu_a[0], mu_a[1], mu_a[2]};
+        m.mu_s = V3{mu_s[0], mu_s[1], mu_s[2]};
     } else {
         log(SU_LOG_ERROR, "su_create_material: unsupported material type " + type);
         return Null;

@@ -119,20 +119,65 @@ SPB_HD V3 to_local(Frame const& f, V3 v) {
     return v3(dot(v, f.t), dot(v, f.b), dot(v, f.n));
 }
 
-// Material record shared by host and device (48 bytes).
+// Material record shared by host and device (80 bytes).
 struct Material {
-    uint32_t type;       // Type_substitute or Type_light
+    uint32_t type;       // Type_substitute, Type_light or Type_volume
     uint32_t two_sided;  // 1: back faces shade like front faces
     float    metallic;
     float    alpha;      // GGX alpha (roughness^2, roughness clamped below at 0.01314)
     V3       albedo;     // (1 - metallic) * color
     V3       f0;         // lerp(f0 of ior 1.46, color, metallic)
     V3       emission;   // radiance (Light) -- colours are ACEScg (AP1) linear
-    float    pad;
+    float    g;          // Henyey-Greenstein anisotropy (Volume), clamped to [-0.999, 0.999]
+    V3       mu_a;       // absorption coefficient per metre (Volume)
+    V3       mu_s;       // scattering coefficient per metre (Volume)
+    float    pad[2];
 };
 
 constexpr uint32_t Type_substitute = 0;
 constexpr uint32_t Type_light      = 1;
+constexpr uint32_t Type_volume     = 2;  // homogeneous medium inside a closed mesh
+
+// Henyey-Greenstein phase function of c = dot(wo, wi) (material.inl:15-19).
+SPB_HD float phase_hg(float c, float g) {
+    float const gg    = g * g;
+    float const denom = 1.f + gg + 2.f * g * c;
+    return (1.f / (4.f * Pi)) * (1.f - gg) / (denom * std::sqrt(denom));
+}
+
+// Samples the phase function around the forward direction -wo (material.inl:21-40); returns
+// wi and sets pdf (= the phase value).
+SPB_HD V3 sample_hg(V3 wo, float g, float xi0, float xi1, float& pdf) {
+    float cos_theta;
+    if (fabsf(g) < 0.001f) {
+        cos_theta = 1.f - 2.f * xi0;
+    } else {
+        float const gg  = g * g;
+        float const sqr = (1.f - gg) / (1.f - g + 2.f * g * xi0);
+        cos_theta       = (1.f + gg - sqr * sqr) / (2.f * g);
+    }
+    float const sin_theta = std::sqrt(fmaxf(0.f, 1.f - cos_theta * cos_theta));
+    float const phi       = xi1 * (2.f * Pi);
+    Frame const f         = make_frame(-wo);
+    V3 const    wi = (sin_theta * std::cos(phi)) * f.t + (sin_theta * std::sin(phi)) * f.b +
+                  cos_theta * f.n;
+    pdf = phase_hg(-cos_theta, g);
+    return wi;
+}
+
+// Phase anisotropy after depth bounces (Material::van_de_hulst_anisotropy,
+// material.cpp:128-140; similarity range 16..64 by default, take_loader.cpp:748-754).
+SPB_HD float van_de_hulst_anisotropy(float g, uint32_t depth) {
+    constexpr uint32_t low  = 16;
+    constexpr uint32_t high = 64;
+    if (depth < low) {
+        return g;
+    }
+    if (depth < high) {
+        return lerp(g, 0.f, float(depth - low) / float(high - low));
+    }
+    return 0.f;
+}
 
 // E table lookup: bilinear over x = cos(theta_o) (columns), y = alpha (rows), both in [0, 1]
 // (interpolated_function_2d.inl:109-130).

@@ -49,11 +49,15 @@ constexpr uint32_t Refill_threshold = 8;
 constexpr float    Ray_max_t        = 3.4027715434167032e+38f;
 constexpr int      Filter_samples   = 30;
 constexpr uint32_t Max_bounce_slots = 64;
+constexpr uint32_t Class_surface    = 1;  // Wide_triangle::tri_class of ordinary surfaces
+constexpr uint32_t Class_boundary   = 2;  // ... of participating-medium boundaries
 
-// Counter block (uint32): per bounce b, [4b] extension count, [4b+1] shadow count,
-// [4b+2] extend fetch, [4b+3] shadow fetch; then the overflow counter.
-constexpr uint32_t Counter_words = 4 * Max_bounce_slots + 4;
-constexpr uint32_t Overflow_slot = 4 * Max_bounce_slots;
+// Counter block (uint32): per bounce b, [8b] extension count, [8b+1] shadow count,
+// [8b+2] extend fetch, [8b+3] shadow fetch, [8b+4] transmittance count; then the overflow
+// counter.
+constexpr uint32_t Counter_stride = 8;
+constexpr uint32_t Counter_words  = Counter_stride * Max_bounce_slots + 4;
+constexpr uint32_t Overflow_slot  = Counter_stride * Max_bounce_slots;
 
 struct Scene_gpu {
     uint4 const*              nodes;
@@ -227,10 +231,14 @@ __global__ void k_generate(Cam cam, Wave wave, Paths p, uint32_t* queue, uint32_
 }
 
 // ---- extend / shadow: persistent traversal over a queue of path indices ----
-template <bool Any_hit>
+// Any_hit: shadow rays.  Media: the scene has participating media -- shadow rays ignore
+// medium boundaries and unoccluded ones go to the transmittance queue instead of adding
+// their contribution directly.
+template <bool Any_hit, bool Media = false>
 __global__ void __launch_bounds__(Trace_block)
     k_trace(Scene_gpu s, Paths p, uint32_t const* __restrict__ queue,
-            uint32_t const* __restrict__ count, uint32_t* fetch, uint32_t* overflow) {
+            uint32_t const* __restrict__ count, uint32_t* fetch, uint32_t* overflow,
+            uint32_t* transmit_queue = nullptr, uint32_t* transmit_count = nullptr) {
     uint32_t const num  = *count;
     uint32_t const lane = threadIdx.x & 31u;
     uint32_t const lt   = (1u << lane) - 1u;
@@ -274,15 +282,20 @@ __global__ void __launch_bounds__(Trace_block)
         if (!active) {
             continue;
         }
-        if (gpu::traversal_step<Any_hit>(r, tv, stack, s.nodes, s.tris, s.hit_margin, overflow)) {
+        if (gpu::traversal_step<Any_hit, Media>(r, tv, stack, s.nodes, s.tris, s.hit_margin,
+                                                 overflow, Class_boundary)) {
             if (Any_hit) {
                 if (r.best_id == gpu::Miss) {
-                    float4 const c = p.sh_L[path];
-                    float4       l = p.L[path];
-                    l.x += c.x;
-                    l.y += c.y;
-                    l.z += c.z;
-                    p.L[path] = l;
+                    if (Media) {
+                        transmit_queue[atomicAdd(transmit_count, 1u)] = path;
+                    } else {
+                        float4 const c = p.sh_L[path];
+                        float4       l = p.L[path];
+                        l.x += c.x;
+                        l.y += c.y;
+                        l.z += c.z;
+                        p.L[path] = l;
+                    }
                 }
             } else {
                 p.hit_id[path] = r.best_id;
@@ -292,6 +305,105 @@ __global__ void __launch_bounds__(Trace_block)
             active = false;
         }
     }
+}
+
+// Small step past a hit distance for a ray that continues through a null boundary
+// (scene::offset_f): 256 ulps, or 2^-16 near zero.
+__device__ __forceinline__ float offset_f(float t) {
+    return t < (1.f / 32.f) ? t + (1.f / 65536.f) : __int_as_float(__float_as_int(t) + 256);
+}
+
+constexpr float    Abort_epsilon  = 7.5e-4f;  // Tracking::Abort_epsilon, tracking.hpp:71
+
+__device__ __forceinline__ uint32_t pack_info(uint32_t vtx, uint32_t depth, bool singular,
+                                              uint32_t medium) {
+    return (vtx & 0xFFu) | ((depth & 0xFFu) << 8) | (singular ? (1u << 16) : 0u) | (medium << 17);
+}
+
+// Light sample for next-event estimation seen from ps: power-proportional triangle, uniform
+// point, solid-angle pdf (with the pick probability).  False if the sample is unusable
+// (grazing or behind a one-sided emitter, Mesh::sample in triangle_mesh.cpp:462-516).
+struct Light_sample {
+    V3    dir;
+    float dist;
+    float pdf;
+    V3    radiance;
+};
+
+__device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, float r, float r1, float r2,
+                                             Light_sample& ls) {
+    uint32_t lo = 0;
+    uint32_t hi = s.num_lights;
+    while (hi - lo > 1) {
+        uint32_t const mid = (lo + hi) >> 1;
+        if (s.light_cdf[mid] <= r) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    float4 const   la   = s.lights[3 * lo + 0];
+    float4 const   le1  = s.lights[3 * lo + 1];
+    float4 const   le2  = s.lights[3 * lo + 2];
+    uint32_t const ltri = __float_as_uint(le2.w);
+    float const    sq   = sqrtf(r1);
+    V3 const       q    = f3v(la) + (sq * (1.f - r2)) * f3v(le1) + (sq * r2) * f3v(le2);
+    V3             ln   = shading::normalize(shading::cross(f3v(le1), f3v(le2)));
+    shading::Material const lmat = s.materials[s.tri_info[ltri].w];
+    if (lmat.two_sided && shading::dot(ln, q - ps) > 0.f) {
+        ln = -ln;
+    }
+    V3 const    axis = offset_ray(q, ln) - ps;
+    float const d2   = shading::dot(axis, axis);
+    float const d    = sqrtf(d2);
+    V3 const    dir  = (1.f / d) * axis;
+    float const cl   = -shading::dot(ln, dir);
+    if (!(cl >= shading::Dot_min)) {
+        return false;
+    }
+    ls.dir      = dir;
+    ls.dist     = d;
+    ls.pdf      = le1.w * d2 / (cl * la.w);
+    ls.radiance = lmat.emission;
+    return true;
+}
+
+// Homogeneous-medium tracking over [t, d] with spectral MIS (Tracking::tracking for a
+// homogeneous medium, tracking.cpp:425-470): returns true on a scattering event at t_out;
+// lw receives the path weight either way.
+__device__ __forceinline__ bool track_homogeneous(shading::Material const& m, float t, float d,
+                                                  Rng& rng, float& t_out, V3& lw) {
+    V3 const    mu_t = m.mu_a + m.mu_s;
+    float const mt   = shading::max_component(mu_t);
+    lw               = v3(1.f, 1.f, 1.f);
+    if (!(mt > 1e-10f)) {
+        return false;
+    }
+    float const imt  = 1.f / mt;
+    V3 const    mu_n = v3(mt - mu_t.x, mt - mu_t.y, mt - mu_t.z);
+    for (int step = 0; step < 4096; ++step) {
+        float const r0 = rng.uniform();
+        t -= logf(1.f - r0) * imt;
+        if (t > d) {
+            return false;
+        }
+        float const ms = ((m.mu_s.x * lw.x) + (m.mu_s.y * lw.y) + (m.mu_s.z * lw.z)) * (1.f / 3.f);
+        float const mn = ((mu_n.x * lw.x) + (mu_n.y * lw.y) + (mu_n.z * lw.z)) * (1.f / 3.f);
+        float const mc = ms + mn;
+        if (mc < 1e-10f) {
+            return false;
+        }
+        float const ps = ms / mc;
+        float const pn = mn / mc;
+        float const r1 = rng.uniform();
+        if ((r1 <= 1.f - pn) & (ps > 0.f)) {
+            lw    = lw * ((1.f / (mt * ps)) * m.mu_s);
+            t_out = t;
+            return true;
+        }
+        lw = lw * ((1.f / (mt * pn)) * mu_n);
+    }
+    return false;
 }
 
 // ---- shade: one path vertex ----
@@ -307,25 +419,89 @@ __global__ void __launch_bounds__(Shade_block)
     uint32_t path   = 0;
 
     if (i < num) {
-        path             = q_in[i];
-        uint32_t info    = p.info[path];
-        uint32_t vtx     = info & 0xFFu;
-        uint32_t depth   = (info >> 8) & 0xFFu;
+        path              = q_in[i];
+        uint32_t info     = p.info[path];
+        uint32_t vtx      = info & 0xFFu;
+        uint32_t depth    = (info >> 8) & 0xFFu;
         bool     singular = (info >> 16) & 1u;
-        float4   T4      = p.T[path];
-        V3       T       = f3v(T4);
+        uint32_t medium   = info >> 17;  // material index + 1 of the medium the path is in
+        float4   T4       = p.T[path];
+        V3       T        = f3v(T4);
         float    bsdf_pdf = T4.w;
-        float4   L4      = p.L[path];
-        V3       L       = f3v(L4);
+        float4   L4       = p.L[path];
+        V3       L        = f3v(L4);
         uint32_t const id = p.hit_id[path];
-        bool     done    = id == gpu::Miss;
+        bool     done     = false;
+        float4 const ro   = p.ray_o[path];
+        float4 const rd   = p.ray_d[path];
+        V3 const     dir_in = v3(rd.x, rd.y, rd.z);
 
         Rng rng;
         rng.load(p.rng[path]);
 
-        if (!done) {
-            float4 const ro  = p.ray_o[path];
-            float4 const rd  = p.ray_d[path];
+        // Inside a medium: track to the next surface (Tracking_multi::integrate,
+        // tracking_multi.cpp:45-238); leaving to infinity ends the path.
+        bool  scatter = false;
+        float t_sc    = 0.f;
+        if (id == gpu::Miss) {
+            done = true;
+        } else if (medium != 0) {
+            shading::Material const m = s.materials[medium - 1];
+            V3 lw;
+            scatter = track_homogeneous(m, ro.w, p.hit_t[path], rng, t_sc, lw);
+            T       = T * lw;
+            if (!(lw.x >= Abort_epsilon || lw.y >= Abort_epsilon || lw.z >= Abort_epsilon)) {
+                done = true;
+            }
+        }
+
+        if (!done && scatter) {
+            // Scattering vertex inside the medium (volumetric::Sample, HG phase function).
+            if (depth >= wave.max_bounces) {
+                done = true;
+            } else if (depth >= wave.min_bounces) {
+                float const q = shading::max_component(T);
+                if (rng.uniform() > q) {
+                    done = true;
+                } else {
+                    T = (1.f / q) * T;
+                }
+            }
+            if (!done) {
+                shading::Material const m = s.materials[medium - 1];
+                float const g   = shading::van_de_hulst_anisotropy(m.g, depth);
+                V3 const    pos = v3(ro.x + t_sc * rd.x, ro.y + t_sc * rd.y, ro.z + t_sc * rd.z);
+                V3 const    wo  = -dir_in;
+                if (s.num_lights > 0) {
+                    float const  r  = rng.uniform();
+                    float const  r1 = rng.uniform();
+                    float const  r2 = rng.uniform();
+                    Light_sample ls;
+                    if (sample_light(s, pos, r, r1, r2, ls)) {
+                        float const f = shading::phase_hg(shading::dot(wo, ls.dir), g);
+                        float const w = ls.pdf / (ls.pdf * ls.pdf + f * f);
+                        V3 const contrib = (w * f) * (T * ls.radiance);
+                        if (shading::max_component(contrib) > 0.f) {
+                            p.sh_o[path] = make_float4(pos.x, pos.y, pos.z, 0.f);
+                            p.sh_d[path] = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
+                            p.sh_L[path] = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
+                            shadow       = true;
+                        }
+                    }
+                }
+                float const x0 = rng.uniform();
+                float const x1 = rng.uniform();
+                float       pdf;
+                V3 const    wi = shading::sample_hg(wo, g, x0, x1, pdf);
+                p.ray_o[path]  = make_float4(pos.x, pos.y, pos.z, 0.f);
+                p.ray_d[path]  = make_float4(wi.x, wi.y, wi.z, Ray_max_t);
+                bsdf_pdf       = pdf;  // reflection / pdf == 1
+                singular       = false;
+                ++depth;
+                ++vtx;
+                extend = true;
+            }
+        } else if (!done) {
             uint4 const  tri = s.tri_info[id];
             V3 const     a   = f3v(s.positions[tri.x]);
             V3 const     b   = f3v(s.positions[tri.y]);
@@ -338,7 +514,7 @@ __global__ void __launch_bounds__(Shade_block)
             V3 const     nb  = f3v(s.normals[tri.y]);
             V3 const     nc  = f3v(s.normals[tri.z]);
             V3           ns  = shading::normalize(bw * na + uv.x * nb + uv.y * nc);
-            V3 const     wo  = v3(-rd.x, -rd.y, -rd.z);
+            V3 const     wo  = -dir_in;
             shading::Material const mat = s.materials[tri.w];
             float const  cos_o = shading::dot(geo_n, wo);
             bool const   front = cos_o > 0.f;
@@ -375,11 +551,18 @@ __global__ void __launch_bounds__(Shade_block)
                 done = true;
             }
 
-            if (!done && !front && !mat.two_sided) {
+            if (!done && mat.type == shading::Type_volume) {
+                // Null boundary of a medium: the ray continues unchanged past the hit, the
+                // medium changes (interface_change), depth and MIS state are kept
+                // (pathtracer_mis.cpp:180-205, Straight_transmission).
+                medium        = front ? tri.w + 1 : 0;
+                p.ray_o[path] = make_float4(ro.x, ro.y, ro.z, offset_f(p.hit_t[path]));
+                p.ray_d[path] = make_float4(rd.x, rd.y, rd.z, Ray_max_t);
+                ++vtx;
+                extend = true;
+            } else if (!done && !front && !mat.two_sided) {
                 done = true;  // back face of a one-sided material: no evaluation, no sample
-            }
-
-            if (!done) {
+            } else if (!done) {
                 if (!front) {
                     geo_n = -geo_n;
                     ns    = -ns;
@@ -391,44 +574,19 @@ __global__ void __launch_bounds__(Shade_block)
 
                 // Next-event estimation (sample_lights / evaluate_light, pathtracer_mis.cpp:281-347).
                 if (s.num_lights > 0) {
-                    float const    r  = rng.uniform();
-                    float const    r1 = rng.uniform();
-                    float const    r2 = rng.uniform();
-                    uint32_t       lo = 0;
-                    uint32_t       hi = s.num_lights;
-                    while (hi - lo > 1) {
-                        uint32_t const mid = (lo + hi) >> 1;
-                        if (s.light_cdf[mid] <= r) {
-                            lo = mid;
-                        } else {
-                            hi = mid;
-                        }
-                    }
-                    float4 const la  = s.lights[3 * lo + 0];
-                    float4 const le1 = s.lights[3 * lo + 1];
-                    float4 const le2 = s.lights[3 * lo + 2];
-                    uint32_t const ltri = __float_as_uint(le2.w);
-                    float const sq  = sqrtf(r1);
-                    V3 const    q   = f3v(la) + (sq * (1.f - r2)) * f3v(le1) + (sq * r2) * f3v(le2);
-                    V3          ln  = shading::normalize(shading::cross(f3v(le1), f3v(le2)));
-                    shading::Material const lmat = s.materials[s.tri_info[ltri].w];
-                    V3 const    ps  = offset_ray(pos, geo_n);
-                    if (lmat.two_sided && shading::dot(ln, q - ps) > 0.f) {
-                        ln = -ln;
-                    }
-                    V3 const    axis = offset_ray(q, ln) - ps;
-                    float const d2   = shading::dot(axis, axis);
-                    float const d    = sqrtf(d2);
-                    V3 const    dir  = (1.f / d) * axis;
-                    float const cl   = -shading::dot(ln, dir);
-                    if (cl >= shading::Dot_min) {
-                        float const pdf_l = le1.w * d2 / (cl * la.w);
-                        shading::Bxdf const f = shading::substitute_evaluate(mat, s.e_table, ctx, dir);
-                        float const w = pdf_l / (pdf_l * pdf_l + f.pdf * f.pdf);
-                        V3 const contrib = w * (T * (lmat.emission * f.reflection));
+                    float const  r  = rng.uniform();
+                    float const  r1 = rng.uniform();
+                    float const  r2 = rng.uniform();
+                    V3 const     ps = offset_ray(pos, geo_n);
+                    Light_sample ls;
+                    if (sample_light(s, ps, r, r1, r2, ls)) {
+                        shading::Bxdf const f =
+                            shading::substitute_evaluate(mat, s.e_table, ctx, ls.dir);
+                        float const w = ls.pdf / (ls.pdf * ls.pdf + f.pdf * f.pdf);
+                        V3 const contrib = w * (T * (ls.radiance * f.reflection));
                         if (shading::max_component(contrib) > 0.f) {
                             p.sh_o[path] = make_float4(ps.x, ps.y, ps.z, 0.f);
-                            p.sh_d[path] = make_float4(dir.x, dir.y, dir.z, d);
+                            p.sh_d[path] = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
                             p.sh_L[path] = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
                             shadow       = true;
                         }
@@ -453,13 +611,12 @@ __global__ void __launch_bounds__(Shade_block)
                     extend = true;
                 }
             }
-            (void)ro;
         }
 
         p.T[path]    = make_float4(T.x, T.y, T.z, bsdf_pdf);
         p.L[path]    = make_float4(L.x, L.y, L.z, 0.f);
         p.rng[path]  = rng.save();
-        p.info[path] = (vtx & 0xFFu) | ((depth & 0xFFu) << 8) | (singular ? (1u << 16) : 0u);
+        p.info[path] = pack_info(vtx, depth, singular, medium);
     }
 
     uint32_t const slot = append(count_out, extend);
@@ -470,6 +627,58 @@ __global__ void __launch_bounds__(Shade_block)
     if (shadow) {
         sq[sslot] = path;
     }
+}
+
+// ---- shadow rays through media: Worker::transmittance (rendering_worker.cpp:209-267) ----
+// For each unoccluded shadow ray of a scene with media, walks the medium boundaries along the
+// ray (closest hits on boundary triangles only), accumulates the optical depth of each
+// homogeneous segment, and adds exp(-optical depth) times the light contribution.
+__global__ void __launch_bounds__(Trace_block)
+    k_transmit(Scene_gpu s, Paths p, uint32_t const* __restrict__ queue,
+               uint32_t const* __restrict__ count, uint32_t* overflow) {
+    uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *count) {
+        return;
+    }
+    uint32_t const path   = queue[i];
+    uint32_t       medium = p.info[path] >> 17;
+    float4 const   ro     = p.sh_o[path];
+    float4 const   rd     = p.sh_d[path];
+    float          t0     = ro.w;
+    V3             tau    = v3(0.f, 0.f, 0.f);
+    uint2          stack[gpu::Stack_size];
+    for (int crossing = 0; crossing < 64; ++crossing) {
+        gpu::Ray_state r;
+        gpu::Traversal tv;
+        gpu::start_ray(r, tv, make_float4(ro.x, ro.y, ro.z, t0), rd);
+        while (!gpu::traversal_step<false, true>(r, tv, stack, s.nodes, s.tris, s.hit_margin,
+                                                 overflow, Class_surface)) {
+        }
+        bool const  hit = r.best_id != gpu::Miss;
+        float const end = hit ? r.tbest : rd.w;
+        if (medium != 0) {
+            shading::Material const m = s.materials[medium - 1];
+            float const len = fmaxf(end - t0, 0.f);
+            tau = tau + len * (m.mu_a + m.mu_s);
+        }
+        if (!hit) {
+            break;
+        }
+        uint4 const tri = s.tri_info[r.best_id];
+        V3 const    a   = f3v(s.positions[tri.x]);
+        V3 const    geo = shading::cross(f3v(s.positions[tri.y]) - a, f3v(s.positions[tri.z]) - a);
+        medium          = shading::dot(geo, v3(rd.x, rd.y, rd.z)) < 0.f ? tri.w + 1 : 0;
+        t0              = offset_f(r.tbest);
+        if (t0 >= rd.w) {
+            break;
+        }
+    }
+    float4 const c = p.sh_L[path];
+    float4       l = p.L[path];
+    l.x += expf(-tau.x) * c.x;
+    l.y += expf(-tau.y) * c.y;
+    l.z += expf(-tau.z) * c.z;
+    p.L[path] = l;
 }
 
 // ---- film: Filtered_1p0::add_sample (sensor/filtered.inl:125-187) as a gather ----
@@ -559,8 +768,10 @@ struct Renderer::Device {
     uint32_t  capacity = 0;
     Paths     paths{};
     uint32_t* queue[2] = {nullptr, nullptr};
-    uint32_t* shadow_queue = nullptr;
-    uint32_t* counters     = nullptr;
+    uint32_t* shadow_queue   = nullptr;
+    uint32_t* transmit_queue = nullptr;
+    uint32_t* counters       = nullptr;
+    bool      has_media      = false;
     // film
     float4*   film = nullptr;
     float4*   comp = nullptr;
@@ -647,6 +858,7 @@ Renderer::~Renderer() {
     free_ptr(d_->queue[0]);
     free_ptr(d_->queue[1]);
     free_ptr(d_->shadow_queue);
+    free_ptr(d_->transmit_queue);
     free_ptr(d_->counters);
     free_ptr(d_->film);
     free_ptr(d_->comp);
@@ -679,10 +891,19 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
         error_ = "scene has no triangles";
         return SPB_ERROR_STATE;
     }
+    // Triangles of medium boundaries get their own class so shadow rays can pass them.
+    std::vector<uint32_t> tri_class(nt, Class_surface);
+    d_->has_media = false;
+    for (uint32_t t = 0; t < nt; ++t) {
+        if (scene.materials[scene.tri_material[t]].type == shading::Type_volume) {
+            tri_class[t]  = Class_boundary;
+            d_->has_media = true;
+        }
+    }
     Wide_bvh    bvh;
     std::string err;
     if (!build_wide_bvh(nv, nt, scene.positions.data(), scene.indices.data(), num_threads, bvh,
-                        err)) {
+                        err, tri_class.data())) {
         error_ = "BVH build: " + err;
         return SPB_ERROR_ARGUMENT;
     }
@@ -824,6 +1045,7 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     free_ptr(d_->queue[0]);
     free_ptr(d_->queue[1]);
     free_ptr(d_->shadow_queue);
+    free_ptr(d_->transmit_queue);
     size_t const n = paths;
     SPB_RCUDA(cudaMalloc(&p.ray_o, n * sizeof(float4)));
     SPB_RCUDA(cudaMalloc(&p.ray_d, n * sizeof(float4)));
@@ -841,6 +1063,7 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     SPB_RCUDA(cudaMalloc(&d_->queue[0], n * sizeof(uint32_t)));
     SPB_RCUDA(cudaMalloc(&d_->queue[1], n * sizeof(uint32_t)));
     SPB_RCUDA(cudaMalloc(&d_->shadow_queue, n * sizeof(uint32_t)));
+    SPB_RCUDA(cudaMalloc(&d_->transmit_queue, n * sizeof(uint32_t)));
     if (!d_->counters) {
         SPB_RCUDA(cudaMalloc(&d_->counters, Counter_words * sizeof(uint32_t)));
     }
@@ -909,14 +1132,21 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         for (uint32_t b = 0; b < bounces; ++b) {
             uint32_t* const q_in  = d_->queue[b & 1];
             uint32_t* const q_out = d_->queue[(b + 1) & 1];
-            k_trace<false><<<d_->trace_grid, Trace_block, 0, st>>>(
-                sg, d_->paths, q_in, ctr + 4 * b, ctr + 4 * b + 2, ctr + Overflow_slot);
+            uint32_t* const c = ctr + Counter_stride * b;
+            k_trace<false><<<d_->trace_grid, Trace_block, 0, st>>>(sg, d_->paths, q_in, c, c + 2,
+                                                                   ctr + Overflow_slot);
             k_shade<<<(paths + Shade_block - 1) / Shade_block, Shade_block, 0, st>>>(
-                sg, wave, d_->paths, q_in, ctr + 4 * b, q_out, ctr + 4 * (b + 1), d_->shadow_queue,
-                ctr + 4 * b + 1);
-            k_trace<true><<<d_->trace_grid, Trace_block, 0, st>>>(
-                sg, d_->paths, d_->shadow_queue, ctr + 4 * b + 1, ctr + 4 * b + 3,
-                ctr + Overflow_slot);
+                sg, wave, d_->paths, q_in, c, q_out, c + Counter_stride, d_->shadow_queue, c + 1);
+            if (d_->has_media) {
+                k_trace<true, true><<<d_->trace_grid, Trace_block, 0, st>>>(
+                    sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot,
+                    d_->transmit_queue, c + 4);
+                k_transmit<<<(paths + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
+                    sg, d_->paths, d_->transmit_queue, c + 4, ctr + Overflow_slot);
+            } else {
+                k_trace<true><<<d_->trace_grid, Trace_block, 0, st>>>(
+                    sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot);
+            }
         }
         k_gather<<<(pixels + 255) / 256, 256, 0, st>>>(d_->paths, camera_.width, camera_.height, k,
                                                       d_->film, d_->comp);
@@ -925,8 +1155,8 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
                                   cudaMemcpyDeviceToHost, st));
         SPB_RCUDA(cudaStreamSynchronize(st));
         for (uint32_t b = 0; b < bounces; ++b) {
-            stats_.extension_rays += host_ctr[4 * b];
-            stats_.shadow_rays += host_ctr[4 * b + 1];
+            stats_.extension_rays += host_ctr[Counter_stride * b];
+            stats_.shadow_rays += host_ctr[Counter_stride * b + 1];
         }
         stats_.overflow += host_ctr[Overflow_slot];
         stats_.paths += paths;

@@ -227,11 +227,15 @@ __device__ __forceinline__ void start_ray(Ray_state& r, Traversal& tv, float4 ro
 // Returns true when the ray is finished (any hit found, or nothing left to visit).
 // overflow receives a count if the stack guard ever trips (it cannot for trees of depth
 // <= Max_wide_depth); the ray then ends as a miss instead of writing out of bounds.
-template <bool Any_hit>
+// Filter: triangles whose class word (Wide_triangle::tri_class) shares a bit with skip_class
+// are ignored (the path tracer skips medium boundaries for shadow rays, and surfaces when it
+// walks the boundaries along a shadow ray).
+template <bool Any_hit, bool Filter = false>
 __device__ __forceinline__ bool traversal_step(Ray_state& r, Traversal& tv, uint2* stack,
                                                uint4 const* __restrict__ nodes,
                                                float4 const* __restrict__ triangles,
-                                               float hit_margin, uint32_t* overflow) {
+                                               float hit_margin, uint32_t* overflow,
+                                               uint32_t skip_class = 0) {
     // Single exit (no early return): the place where the two branches rejoin decides where a
     // diverged warp reconverges, and keeping it at the end measured fastest.
     bool done = false;
@@ -243,7 +247,8 @@ __device__ __forceinline__ bool traversal_step(Ray_state& r, Traversal& tv, uint
         float4 const  e1  = __ldg(tri + 1);
         float4 const  e2  = __ldg(tri + 2);
         float         t, u, v;
-        if (triangle_test(r, a, e1, e2, r.tbest, t, u, v) &&
+        bool const    candidate = !Filter || !(__float_as_uint(e1.w) & skip_class);
+        if (candidate && triangle_test(r, a, e1, e2, r.tbest, t, u, v) &&
             within_bounds(r, a, e1, e2, t, hit_margin)) {
             uint32_t const id = __float_as_uint(a.w);
             if (Any_hit) {

@@ -88,8 +88,12 @@ def translation(x, y, z):
 
 def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounces: int = 8,
             min_bounces: int = 4, fov_degrees: float = 40.0, camera_position=(0.0, 1.0, -3.4),
-            spp: int = 64, tonemap: bool = False):
-    """Issues the scene's su_* calls on an initialised engine; returns the camera entity."""
+            spp: int = 64, tonemap: bool = False, medium=None):
+    """Issues the scene's su_* calls on an initialised engine; returns the camera entity.
+
+    medium: optional dict of Volumetric material parameters (e.g. color, attenuation_distance,
+    anisotropy); the sphere then becomes a homogeneous participating medium instead of metal.
+    """
     cam = su.su_create_camera_perspective(width, height, math.radians(fov_degrees))
     su.set_transformation(cam, translation(*camera_position))
     su.su_create_integrators(json.dumps({"surface": {"PTMIS": {"min_bounces": min_bounces,
@@ -101,7 +105,10 @@ def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounc
     white = _material(su, "Substitute", color=[0.75, 0.75, 0.75], roughness=1.0, metallic=0.0)
     red = _material(su, "Substitute", color=[0.75, 0.05, 0.05], roughness=1.0, metallic=0.0)
     green = _material(su, "Substitute", color=[0.05, 0.75, 0.05], roughness=1.0, metallic=0.0)
-    metal = _material(su, "Substitute", color=[0.95, 0.64, 0.54], roughness=math.sqrt(0.3), metallic=1.0)
+    if medium is None:
+        metal = _material(su, "Substitute", color=[0.95, 0.64, 0.54], roughness=math.sqrt(0.3), metallic=1.0)
+    else:
+        metal = _material(su, "Volumetric", **medium)
     light = _material(su, "Light", emission=[17.0, 17.0, 17.0])
 
     geo = cornell_geometry(sphere_subdivisions)

@@ -22,22 +22,28 @@ sys.path.insert(0, str(ROOT))
 import oracle  # noqa: E402
 from sprout_b200 import scenes  # noqa: E402
 
-# name -> (width, height, spp, sphere subdivisions)
+# A homogeneous scattering sphere in place of the metal one (Volumetric material).
+MEDIUM = {"color": [0.8, 0.8, 0.8], "attenuation_distance": 0.05, "anisotropy": 0.5}
+
+# name -> (width, height, spp, sphere subdivisions, medium)
 CASES = {
-    "cornell64_sub3": (64, 64, 4096, 3),
-    "cornell128_sub6": (128, 128, 2048, 6),
+    "cornell64_sub3": (64, 64, 4096, 3, None),
+    "cornell128_sub6": (128, 128, 2048, 6, None),
+    "cornell64_medium": (64, 64, 4096, 4, MEDIUM),
 }
 
 
 def main():
     out = {}
     meta = {"generator": "oracle/_ref/ref_render (reference su_* C API, batch mode)", "cases": {}}
-    for name, (w, h, spp, sub) in CASES.items():
+    for name, (w, h, spp, sub, medium) in CASES.items():
         img, timing = oracle.reference_render(
-            lambda su: scenes.cornell(su, w, h, sphere_subdivisions=sub, tonemap=True, spp=spp),
+            lambda su: scenes.cornell(su, w, h, sphere_subdivisions=sub, tonemap=True, spp=spp,
+                                      medium=medium),
             w, h, 0, progressive=False)
         out[name] = img.astype(np.float32)
         meta["cases"][name] = {"width": w, "height": h, "spp": spp, "sphere_subdivisions": sub,
+                               "medium": medium,
                                "render_s": timing["render_s"], "mean": [float(x) for x in img.mean(axis=(0, 1))]}
         print(name, meta["cases"][name])
     out["meta"] = np.frombuffer(json.dumps(meta).encode(), np.uint8)

@@ -5,7 +5,9 @@ made by the reference's own C API).
 Monte Carlo images agree only in expectation, so the checks are statistical: the image means
 per channel within 1.5%, 8x8-pixel block means within 4% (plus a small absolute floor), and
 the relative MSE of the whole image (mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2))
-below a bound that the reference's own noise at its sample count dominates.
+below a bound that the reference's own noise at its sample count dominates.  One case replaces
+the metal sphere by a homogeneous scattering medium (Volumetric material: delta tracking,
+Henyey-Greenstein phase function, transmittance along shadow rays).
 """
 
 import json
@@ -30,11 +32,11 @@ def block_means(img, b):
     return img[: h - h % b, : w - w % b].reshape(h // b, b, w // b, b, c).mean(axis=(1, 3))
 
 
-def render(width, height, spp, sub, progressive=False, iterations=0):
+def render(width, height, spp, sub, progressive=False, iterations=0, medium=None):
     su = capi.SuLibrary()
     assert su.su_init(progressive) == 0
     try:
-        scenes.cornell(su, width, height, sphere_subdivisions=sub, tonemap=True, spp=spp)
+        scenes.cornell(su, width, height, sphere_subdivisions=sub, tonemap=True, spp=spp, medium=medium)
         if progressive:
             assert su.su_start_render_frame(0) == 0, su.messages
             for _ in range(iterations):
@@ -49,13 +51,13 @@ def render(width, height, spp, sub, progressive=False, iterations=0):
         su.su_release()
 
 
-@pytest.mark.parametrize("name", ["cornell64_sub3", "cornell128_sub6"])
+@pytest.mark.parametrize("name", ["cornell64_sub3", "cornell128_sub6", "cornell64_medium"])
 def test_converged_image_matches_reference(name):
     data = np.load(GOLDEN)
     meta = json.loads(bytes(data["meta"]).decode())["cases"][name]
     ref = data[name]
     w, h, sub = meta["width"], meta["height"], meta["sphere_subdivisions"]
-    img = render(w, h, 4 * meta["spp"], sub)
+    img = render(w, h, 4 * meta["spp"], sub, medium=meta.get("medium"))
     assert np.all(np.isfinite(img))
     m_ref = ref.mean(axis=(0, 1))
     m_img = img.mean(axis=(0, 1))
