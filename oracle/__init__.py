@@ -134,7 +134,7 @@ class ScriptRecorder:
     def __init__(self):
         self.lines = []
         self.data = bytearray()
-        self.n = {"material": 0, "mesh": 0, "prop": 0}
+        self.n = {"material": 0, "mesh": 0, "prop": 0, "image": 0}
 
     def _blob(self, array):
         while len(self.data) % 16:
@@ -168,6 +168,16 @@ class ScriptRecorder:
         self.lines.append("material " + (desc.decode() if isinstance(desc, bytes) else desc))
         self.n["material"] += 1
         return 1000 + self.n["material"] - 1
+
+    def image(self, pixels):
+        """su_create_image of a float32 array (depth, height, width) or (height, width): one
+        channel.  Returns the image id the reference assigns (images are numbered from 0)."""
+        a = np.ascontiguousarray(pixels, np.float32)
+        d, h, w = (a.shape if a.ndim == 3 else (1,) + a.shape)
+        off = self._blob(a)
+        self.lines.append(f"image 2 1 {w} {h} {d} {off}")
+        self.n["image"] += 1
+        return self.n["image"] - 1
 
     def mesh(self, positions, normals, indices, parts=None):
         assert parts is None

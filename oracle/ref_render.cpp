@@ -14,6 +14,9 @@
 //     sampler <spp>
 //     defaults
 //     material <json>
+//     image <pixel type> <channels> <width> <height> <depth> <byte offset of the pixels>
+//       (su_create_image, tightly packed; the created image id must equal the number of images
+//       created before it, which the recorded material JSON refers to)
 //     mesh <num_triangles> <num_vertices> <byte offset of positions> <of normals> <of indices>
 //     prop <mesh handle> <num materials> <material handles...>
 //     light <prop handle>
@@ -56,7 +59,7 @@ int main(int argc, char** argv) {
     }
 
     std::map<uint32_t, uint32_t> handles;
-    uint32_t n_mat = 0, n_mesh = 0, n_prop = 0;
+    uint32_t n_mat = 0, n_mesh = 0, n_prop = 0, n_image = 0;
     uint32_t width = 0, height = 0;
     double   render_s = 0.0;
     int32_t  status   = 0;
@@ -95,6 +98,16 @@ int main(int argc, char** argv) {
             status |= su_create_defaults();
         } else if (c == "material") {
             handles[1000 + n_mat++] = su_create_material(rest);
+        } else if (c == "image") {
+            uint32_t type = 0, channels = 0, w = 0, h = 0, d = 0;
+            size_t   off  = 0;
+            std::sscanf(rest, "%u %u %u %u %u %zu", &type, &channels, &w, &h, &d, &off);
+            uint32_t const bytes = type == 0 ? 1u : (type == 1 ? 2u : 4u);
+            uint32_t const id    = su_create_image(type, channels, w, h, d, 0, bytes * channels,
+                                                   data.data() + off);
+            if (id != n_image++) {
+                status |= 0x100;
+            }
         } else if (c == "mesh") {
             uint32_t nt = 0, nv = 0;
             size_t   op = 0, on = 0, oi = 0;

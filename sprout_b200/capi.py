@@ -92,6 +92,12 @@ class SuLibrary:
             idx.shape[0], pos.shape[0], 3, pos.ctypes.data, 3, nrm.ctypes.data, 0, None, 0, None,
             idx.ctypes.data, 0 if prt is None else prt.shape[0], None if prt is None else prt.ctypes.data)
 
+    def image(self, pixels):
+        """su_create_image of one float channel: pixels (depth, height, width) or (height, width)."""
+        a = np.ascontiguousarray(pixels, np.float32)
+        d, h, w = a.shape if a.ndim == 3 else (1,) + a.shape
+        return self.lib.su_create_image(2, 1, w, h, d, 0, 4, a.ctypes.data)
+
     def prop(self, shape, materials):
         mats = np.ascontiguousarray(materials, np.uint32)
         self._keep.append(mats)

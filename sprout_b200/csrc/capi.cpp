@@ -33,6 +33,20 @@ struct Mesh {
     std::vector<uint32_t> part_slot;  // material slot per part
 };
 
+// su_create_image: pixels converted to float (Byte: unorm / 255, image_provider.cpp:90-170).
+struct Image {
+    uint32_t           dims[3]  = {0, 0, 0};
+    uint32_t           channels = 0;
+    std::vector<float> pixels;  // channels per pixel, x fastest
+};
+
+// Host-side part of a Volumetric material with a density grid (Grid, volumetric_grid.cpp).
+struct Grid_ref {
+    uint32_t image   = Null;   // density image id, Null for homogeneous media
+    bool     nearest = false;  // "sampler": {"filter": "Nearest"}
+    bool     repeat  = false;  // "sampler": {"address": "Repeat"}
+};
+
 struct Entity {
     bool                  camera = false;
     uint32_t              shape  = Null;
@@ -47,6 +61,8 @@ struct Engine {
     bool                  progressive;
     std::vector<Mesh>     meshes;
     std::vector<Material> materials;
+    std::vector<Grid_ref> material_grids;  // parallel to materials
+    std::vector<Image>    images;
     std::vector<Entity>   entities;
     uint32_t              camera_entity = Null;
     uint32_t              width         = 0;
@@ -123,6 +139,52 @@ void decompose(float const* m, float rot[9], float pos[3]) {
     pos[2] = m[14];
 }
 
+// World -> texture-space map of a prop (texture_space_ray, tracking.inl:12-29): the inverse of
+// the row-major object-to-world matrix m, then (local - mesh min) / mesh extent.  Computed in
+// double; rows of a 3x4 affine map.
+void texture_space(float const* m, Mesh const& mesh, float out[12]) {
+    double lo[3] = {1e300, 1e300, 1e300};
+    double hi[3] = {-1e300, -1e300, -1e300};
+    for (size_t v = 0; v < mesh.positions.size() / 3; ++v) {
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], double(mesh.positions[3 * v + a]));
+            hi[a] = std::max(hi[a], double(mesh.positions[3 * v + a]));
+        }
+    }
+    // object-to-world: p_world[c] = sum_r p_obj[r] * m[4r + c] + m[12 + c]; A[c][r] = m[4r + c]
+    double A[3][3];
+    for (int c = 0; c < 3; ++c) {
+        for (int r = 0; r < 3; ++r) {
+            A[c][r] = m[4 * r + c];
+        }
+    }
+    double const det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                       A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                       A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+    double const id = det != 0.0 ? 1.0 / det : 0.0;
+    double       inv[3][3];
+    inv[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) * id;
+    inv[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) * id;
+    inv[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) * id;
+    inv[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) * id;
+    inv[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) * id;
+    inv[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) * id;
+    inv[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) * id;
+    inv[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) * id;
+    inv[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) * id;
+    double const t[3] = {m[12], m[13], m[14]};
+    for (int a = 0; a < 3; ++a) {
+        double const extent = hi[a] - lo[a];
+        double const s      = extent > 0.0 ? 1.0 / extent : 0.0;
+        double       off    = 0.0;
+        for (int c = 0; c < 3; ++c) {
+            out[4 * a + c] = float(inv[a][c] * s);
+            off -= inv[a][c] * t[c];
+        }
+        out[4 * a + 3] = float((off - lo[a]) * s);
+    }
+}
+
 int32_t compile_scene() {
     spb::render::Scene_desc scene;
     scene.materials = engine->materials;
@@ -135,6 +197,7 @@ int32_t compile_scene() {
     fallback.f0       = V3{0.03497f, 0.03497f, 0.03497f};
     uint32_t const fallback_id = uint32_t(scene.materials.size());
     scene.materials.push_back(fallback);
+    std::vector<uint32_t> grid_images;  // image id of each scene.grids entry
 
     for (Entity const& e : engine->entities) {
         if (e.camera || e.shape == Null) {
@@ -161,13 +224,46 @@ int32_t compile_scene() {
             scene.normals.push_back(nx * rot[1] + ny * rot[4] + nz * rot[7]);
             scene.normals.push_back(nx * rot[2] + ny * rot[5] + nz * rot[8]);
         }
+        // A density-grid medium samples its grid in the prop's texture space, so each prop gets
+        // its own copy of such a material (one per slot), pointing at its own medium record.
+        std::vector<uint32_t> slot_material(e.materials.size(), fallback_id);
+        for (size_t k = 0; k < e.materials.size(); ++k) {
+            uint32_t const mat = e.materials[k];
+            if (mat >= engine->materials.size()) {
+                continue;
+            }
+            slot_material[k] = mat;
+            Grid_ref const& gr = engine->material_grids[mat];
+            if (gr.image == Null) {
+                continue;
+            }
+            spb::render::Grid_medium gm;
+            auto const it = std::find(grid_images.begin(), grid_images.end(), gr.image);
+            gm.grid = uint32_t(it - grid_images.begin());
+            if (it == grid_images.end()) {
+                Image const&             img = engine->images[gr.image];
+                spb::render::Density_grid g;
+                std::copy(img.dims, img.dims + 3, g.dims);
+                g.density = img.pixels.data();
+                scene.grids.push_back(g);
+                grid_images.push_back(gr.image);
+            }
+            gm.nearest = gr.nearest;
+            gm.repeat  = gr.repeat;
+            texture_space(m, mesh, gm.world_to_uvw);
+            scene.media.push_back(gm);
+            Material copy = engine->materials[mat];
+            copy.medium   = uint32_t(scene.media.size());
+            slot_material[k] = uint32_t(scene.materials.size());
+            scene.materials.push_back(copy);
+        }
         for (size_t t = 0; t < mesh.indices.size() / 3; ++t) {
             for (int k = 0; k < 3; ++k) {
                 scene.indices.push_back(base + mesh.indices[3 * t + k]);
             }
             uint32_t const slot = mesh.part_slot[mesh.part_of[t]];
-            uint32_t const mat  = slot < e.materials.size() ? e.materials[slot] : Null;
-            scene.tri_material.push_back(mat < engine->materials.size() ? mat : fallback_id);
+            scene.tri_material.push_back(slot < slot_material.size() ? slot_material[slot]
+                                                                     : fallback_id);
             scene.tri_light.push_back(e.light ? 1 : 0);
         }
     }
@@ -245,6 +341,8 @@ SU_LIBRARY_API int32_t su_clear(void) {
     engine->entities.clear();
     engine->meshes.clear();
     engine->materials.clear();
+    engine->material_grids.clear();
+    engine->images.clear();
     engine->camera_entity = Null;
     engine->frame_started = false;
     engine->scene_dirty   = true;
@@ -380,13 +478,43 @@ SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
     return 0;
 }
 
-SU_LIBRARY_API uint32_t su_create_image(uint32_t, uint32_t, uint32_t, uint32_t, uint32_t, uint32_t,
-                                        uint32_t, char const*) {
+SU_LIBRARY_API uint32_t su_create_image(uint32_t pixel_type, uint32_t num_channels, uint32_t width,
+                                        uint32_t height, uint32_t depth, uint32_t num_elements,
+                                        uint32_t stride, char const* data) {
+    // capi.cpp:329-344 and image_provider.cpp:90-170: Byte (unorm) or Float pixels, 1 to 4
+    // channels, pixels stride bytes apart (0: packed); ids count from 0 in creation order.
     if (!engine) {
         return Null;
     }
-    log(SU_LOG_ERROR, "su_create_image: textures are not supported by this renderer");
-    return Null;
+    uint32_t const bytes = pixel_type == 0 ? 1u : (pixel_type == 2 ? 4u : 0u);
+    if (bytes == 0 || num_channels < 1 || num_channels > 4 || width == 0 || height == 0 || !data ||
+        num_elements > 1) {
+        log(SU_LOG_ERROR, "su_create_image: unsupported pixel type, channel count or size");
+        return Null;
+    }
+    Image img;
+    img.dims[0]  = width;
+    img.dims[1]  = height;
+    img.dims[2]  = std::max(depth, 1u);
+    img.channels = num_channels;
+    size_t const pixels = size_t(width) * height * img.dims[2];
+    size_t const step   = stride ? stride : size_t(bytes) * num_channels;
+    img.pixels.resize(pixels * num_channels);
+    for (size_t i = 0; i < pixels; ++i) {
+        char const* src = data + i * step;
+        for (uint32_t c = 0; c < num_channels; ++c) {
+            float v;
+            if (bytes == 1) {
+                v = float(uint8_t(src[c])) * (1.f / 255.f);
+            } else {
+                std::memcpy(&v, src + 4 * c, 4);
+            }
+            img.pixels[i * num_channels + c] = v;
+        }
+    }
+    engine->images.push_back(std::move(img));
+    engine->scene_dirty = true;
+    return uint32_t(engine->images.size() - 1);
 }
 
 SU_LIBRARY_API uint32_t su_create_material(char const* string) {
@@ -407,6 +535,7 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
     spb::json::Value const& desc = rendering->object.front().second;
 
     Material m{};
+    Grid_ref grid;
     m.two_sided = spb::json::bool_or(desc.find("two_sided"), false) ? 1u : 0u;
     if (type == "Light") {
         // material_provider.cpp:298-364: "emission" is a radiance, default 10
@@ -440,9 +569,39 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
         // material_provider.cpp:767-849 (homogeneous case): colour 0.5 by default, attenuation
         // and subsurface colours default to it, distance 1, anisotropy clamped to +-0.999;
         // coefficients from attenuation() (collision_coefficients.inl:50-71).
-        if (desc.find("density") || desc.find("temperature")) {
-            log(SU_LOG_ERROR, "su_create_material: density/temperature grids are not supported");
+        if (spb::json::Value const* density = desc.find("density")) {
+            // "density": {"id": image} or {"file": ...} (read_texture_description,
+            // material_provider.cpp:895-946); only in-memory images are supported here.
+            spb::json::Value const* id = density->is_object() ? density->find("id") : nullptr;
+            uint32_t const image = id && id->is_number() ? uint32_t(id->number) : Null;
+            if (image >= engine->images.size() || engine->images[image].channels != 1) {
+                log(SU_LOG_ERROR, "su_create_material: density must name a one-channel image id");
+                return Null;
+            }
+            grid.image = image;
+        }
+        if (desc.find("temperature")) {
+            log(SU_LOG_ERROR, "su_create_material: temperature grids are not supported");
             return Null;
+        }
+        V3 emission{0.f, 0.f, 0.f};
+        if (read_color(desc.find("emission"), emission) &&
+            (emission.x > 0.f || emission.y > 0.f || emission.z > 0.f)) {
+            log(SU_LOG_ERROR, "su_create_material: emissive media are not supported");
+            return Null;
+        }
+        if (spb::json::Value const* sampler = desc.find("sampler")) {
+            // read_sampler_settings, material_provider.cpp:866-892; 3-D lookups use address_u
+            if (spb::json::Value const* f = sampler->find("filter"); f && f->is_string()) {
+                grid.nearest = f->string == "Nearest";
+            }
+            spb::json::Value const* a = sampler->find("address");
+            if (a && a->is_array() && !a->array.empty()) {
+                a = &a->array[0];
+            }
+            if (a && a->is_string()) {
+                grid.repeat = a->string == "Repeat";
+            }
         }
         V3 color = srgb_to_ap1(V3{0.5f, 0.5f, 0.5f});
         read_color(desc.find("color"), color);
@@ -477,6 +636,7 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
         return Null;
     }
     engine->materials.push_back(m);
+    engine->material_grids.push_back(grid);
     engine->scene_dirty = true;
     return uint32_t(engine->materials.size() - 1);
 }

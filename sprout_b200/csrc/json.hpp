@@ -39,6 +39,9 @@ struct Value {
     bool is_array() const {
         return kind == Kind::Array;
     }
+    bool is_string() const {
+        return kind == Kind::String;
+    }
 };
 
 class Parser {

@@ -74,6 +74,9 @@ SPB_HD V3 normalize(V3 a) {
 SPB_HD float max_component(V3 a) {
     return fmaxf(a.x, fmaxf(a.y, a.z));
 }
+SPB_HD float min_component(V3 a) {
+    return fminf(a.x, fminf(a.y, a.z));
+}
 SPB_HD float clampf(float x, float lo, float hi) {
     return fminf(fmaxf(x, lo), hi);
 }
@@ -131,12 +134,13 @@ struct Material {
     float    g;          // Henyey-Greenstein anisotropy (Volume), clamped to [-0.999, 0.999]
     V3       mu_a;       // absorption coefficient per metre (Volume)
     V3       mu_s;       // scattering coefficient per metre (Volume)
-    float    pad[2];
+    uint32_t medium;     // Volume: 0 homogeneous, else 1 + index of the density-grid medium
+    uint32_t pad;
 };
 
 constexpr uint32_t Type_substitute = 0;
 constexpr uint32_t Type_light      = 1;
-constexpr uint32_t Type_volume     = 2;  // homogeneous medium inside a closed mesh
+constexpr uint32_t Type_volume     = 2;  // participating medium inside a closed mesh
 
 // Henyey-Greenstein phase function of c = dot(wo, wi) (material.inl:15-19).
 SPB_HD float phase_hg(float c, float g) {
@@ -177,6 +181,13 @@ SPB_HD float van_de_hulst_anisotropy(float g, uint32_t depth) {
         return lerp(g, 0.f, float(depth - low) / float(high - low));
     }
     return 0.f;
+}
+
+// Scale of the scattering coefficient that goes with the reduced anisotropy
+// (Material::similarity_relation_scale, material.cpp:108-112; van_de_hulst,
+// collision_coefficients.inl:9-11): (1 - g) / (1 - g').
+SPB_HD float similarity_relation_scale(float g, uint32_t depth) {
+    return (1.f - g) / (1.f - van_de_hulst_anisotropy(g, depth));
 }
 
 // E table lookup: bilinear over x = cos(theta_o) (columns), y = alpha (rows), both in [0, 1]

@@ -59,6 +59,18 @@ constexpr uint32_t Counter_stride = 8;
 constexpr uint32_t Counter_words  = Counter_stride * Max_bounce_slots + 4;
 constexpr uint32_t Overflow_slot  = Counter_stride * Max_bounce_slots;
 
+// A prop filled with a heterogeneous medium: world -> texture space map, its density grid and
+// the grid's majorant cells.
+struct Medium_gpu {
+    float4        m0, m1, m2;  // rows of the world -> texture-space affine map
+    float const*  density;     // nx * ny * nz, x fastest
+    float2 const* cells;       // per majorant cell: (min, max) density
+    int           nx, ny, nz;
+    int           cx, cy, cz;  // majorant cells per axis
+    uint32_t      flags;       // bit 0: Nearest filter; bit 1: Repeat address mode
+    uint32_t      pad;
+};
+
 struct Scene_gpu {
     uint4 const*              nodes;
     float4 const*             tris;
@@ -72,6 +84,7 @@ struct Scene_gpu {
     float const*              light_cdf;      // num_lights + 1 entries
     uint32_t                  num_lights;
     float const*              e_table;
+    Medium_gpu const*         media;  // Material::medium - 1 indexes this
 };
 
 struct Paths {
@@ -406,6 +419,274 @@ __device__ __forceinline__ bool track_homogeneous(shading::Material const& m, fl
     return false;
 }
 
+// ---- heterogeneous media: density grids (Grid material, volumetric_grid.cpp) ----
+// Majorants: the grid is cut into cells of Cell_dim^3 voxels; each cell stores the minimum and
+// maximum density over the voxels that trilinear filtering inside it can read (the cell plus
+// one voxel on every side), as the reference's Gridtree leaves do
+// (volumetric_octree_builder.cpp:105-207).  The reference refines 32^3 cells by an octree to
+// 8^3 leaves; here the cells are uniformly 8^3 and a 3-D DDA walks them.  Any majorant that
+// bounds the density gives the same expected result.
+constexpr int   Cell_log2 = 3;
+constexpr float Min_mt    = 1e-10f;  // Tracking::Min_mt, tracking.hpp:70
+
+__device__ __forceinline__ V3 to_texture(Medium_gpu const& g, V3 p) {
+    return v3(g.m0.x * p.x + g.m0.y * p.y + g.m0.z * p.z + g.m0.w,
+              g.m1.x * p.x + g.m1.y * p.y + g.m1.z * p.z + g.m1.w,
+              g.m2.x * p.x + g.m2.y * p.y + g.m2.z * p.z + g.m2.w);
+}
+
+__device__ __forceinline__ V3 to_texture_dir(Medium_gpu const& g, V3 d) {
+    return v3(g.m0.x * d.x + g.m0.y * d.y + g.m0.z * d.z, g.m1.x * d.x + g.m1.y * d.y + g.m1.z * d.z,
+              g.m2.x * d.x + g.m2.y * d.y + g.m2.z * d.z);
+}
+
+// Address modes (image/texture/address_mode.hpp): clamp saturates, repeat wraps.
+__device__ __forceinline__ float address(float x, bool repeat) {
+    return repeat ? x - floorf(x) : __saturatef(x);
+}
+
+__device__ __forceinline__ int lower_bound(int v, int max, bool repeat) {
+    return v < 0 ? (repeat ? max : 0) : v;
+}
+
+__device__ __forceinline__ int increment(int v, int max, bool repeat) {
+    return v >= max ? (repeat ? 0 : max) : v + 1;
+}
+
+// Density at texture-space point uvw: Linear_3D::sample_1 (texture_sampler.cpp:175-188,
+// map :256-283) or Nearest_3D (:124-172).
+__device__ float sample_density(Medium_gpu const& g, V3 uvw) {
+    bool const  repeat = g.flags & 2u;
+    float const u      = address(uvw.x, repeat);
+    float const v      = address(uvw.y, repeat);
+    float const w      = address(uvw.z, repeat);
+    if (g.flags & 1u) {
+        int const x = min(int(u * float(g.nx)), g.nx - 1);
+        int const y = min(int(v * float(g.ny)), g.ny - 1);
+        int const z = min(int(w * float(g.nz)), g.nz - 1);
+        return __ldg(g.density + (size_t(z) * g.ny + y) * g.nx + x);
+    }
+    float const fu = u * float(g.nx) - 0.5f;
+    float const fv = v * float(g.ny) - 0.5f;
+    float const fw = w * float(g.nz) - 0.5f;
+    float const lu = floorf(fu);
+    float const lv = floorf(fv);
+    float const lw = floorf(fw);
+    int const   x  = int(lu);
+    int const   y  = int(lv);
+    int const   z  = int(lw);
+    int const   x0 = lower_bound(x, g.nx - 1, repeat);
+    int const   y0 = lower_bound(y, g.ny - 1, repeat);
+    int const   z0 = lower_bound(z, g.nz - 1, repeat);
+    int const   x1 = increment(x, g.nx - 1, repeat);
+    int const   y1 = increment(y, g.ny - 1, repeat);
+    int const   z1 = increment(z, g.nz - 1, repeat);
+    float const s  = fu - lu;
+    float const t  = fv - lv;
+    float const r  = fw - lw;
+    size_t const p00 = (size_t(z0) * g.ny + y0) * g.nx;
+    size_t const p01 = (size_t(z0) * g.ny + y1) * g.nx;
+    size_t const p10 = (size_t(z1) * g.ny + y0) * g.nx;
+    size_t const p11 = (size_t(z1) * g.ny + y1) * g.nx;
+    float const c0 = __ldg(g.density + p00 + x0);
+    float const c1 = __ldg(g.density + p00 + x1);
+    float const c2 = __ldg(g.density + p01 + x0);
+    float const c3 = __ldg(g.density + p01 + x1);
+    float const c4 = __ldg(g.density + p10 + x0);
+    float const c5 = __ldg(g.density + p10 + x1);
+    float const c6 = __ldg(g.density + p11 + x0);
+    float const c7 = __ldg(g.density + p11 + x1);
+    float const b0 = (1.f - t) * ((1.f - s) * c0 + s * c1) + t * ((1.f - s) * c2 + s * c3);
+    float const b1 = (1.f - t) * ((1.f - s) * c4 + s * c5) + t * ((1.f - s) * c6 + s * c7);
+    return (1.f - r) * b0 + r * b1;
+}
+
+// Walks the majorant cells that the texture-space ray o + t d crosses for t in [t0, t1],
+// clipped to the grid's unit cube (outside it the medium is empty, as outside the reference's
+// Gridtree, volumetric_octree.cpp:64-75).  Calls visit(cell (min, max) density, ta, tb) for
+// each cell segment in order until visit returns true; returns whether it did.
+template <typename Visit>
+__device__ bool walk_cells(Medium_gpu const& g, V3 o, V3 d, float t0, float t1, Visit&& visit) {
+    float const tiny = 1e-30f;
+    V3 const    inv  = v3(1.f / (fabsf(d.x) < tiny ? copysignf(tiny, d.x) : d.x),
+                          1.f / (fabsf(d.y) < tiny ? copysignf(tiny, d.y) : d.y),
+                          1.f / (fabsf(d.z) < tiny ? copysignf(tiny, d.z) : d.z));
+    float lo = t0;
+    float hi = t1;
+    {
+        float const ax = -o.x * inv.x, bx = (1.f - o.x) * inv.x;
+        float const ay = -o.y * inv.y, by = (1.f - o.y) * inv.y;
+        float const az = -o.z * inv.z, bz = (1.f - o.z) * inv.z;
+        lo = fmaxf(lo, fmaxf(fminf(ax, bx), fmaxf(fminf(ay, by), fminf(az, bz))));
+        hi = fminf(hi, fminf(fmaxf(ax, bx), fminf(fmaxf(ay, by), fmaxf(az, bz))));
+    }
+    if (!(lo < hi)) {
+        return false;
+    }
+    // cells per texture-space unit along each axis
+    float const sx = float(g.nx) * (1.f / float(1 << Cell_log2));
+    float const sy = float(g.ny) * (1.f / float(1 << Cell_log2));
+    float const sz = float(g.nz) * (1.f / float(1 << Cell_log2));
+    // Starting cell from the entry point.  Should rounding put it in the neighbour behind a
+    // cell face, that cell's exit distance is <= lo: it is skipped (te > t fails) and the walk
+    // steps on.
+    int ix = min(max(int(floorf((o.x + lo * d.x) * sx)), 0), g.cx - 1);
+    int iy = min(max(int(floorf((o.y + lo * d.y) * sy)), 0), g.cy - 1);
+    int iz = min(max(int(floorf((o.z + lo * d.z) * sz)), 0), g.cz - 1);
+    int const   step_x = d.x > 0.f ? 1 : -1;
+    int const   step_y = d.y > 0.f ? 1 : -1;
+    int const   step_z = d.z > 0.f ? 1 : -1;
+    float       nx_t   = (float(ix + (step_x > 0)) / sx - o.x) * inv.x;
+    float       ny_t   = (float(iy + (step_y > 0)) / sy - o.y) * inv.y;
+    float       nz_t   = (float(iz + (step_z > 0)) / sz - o.z) * inv.z;
+    float const dx_t   = fabsf(inv.x) / sx;
+    float const dy_t   = fabsf(inv.y) / sy;
+    float const dz_t   = fabsf(inv.z) / sz;
+    float       t      = lo;
+    int const   max_steps = g.cx + g.cy + g.cz + 3;
+    for (int k = 0; k < max_steps; ++k) {
+        float const  te   = fminf(fminf(nx_t, ny_t), fminf(nz_t, hi));
+        float2 const cell = __ldg(g.cells + (size_t(iz) * g.cy + iy) * g.cx + ix);
+        if (te > t && visit(cell, t, te)) {
+            return true;
+        }
+        if (te >= hi) {
+            break;
+        }
+        t = fmaxf(t, te);
+        if (nx_t <= ny_t && nx_t <= nz_t) {
+            ix += step_x;
+            nx_t += dx_t;
+            if (ix < 0 || ix >= g.cx) {
+                break;
+            }
+        } else if (ny_t <= nz_t) {
+            iy += step_y;
+            ny_t += dy_t;
+            if (iy < 0 || iy >= g.cy) {
+                break;
+            }
+        } else {
+            iz += step_z;
+            nz_t += dz_t;
+            if (iz < 0 || iz >= g.cz) {
+                break;
+            }
+        }
+    }
+    return false;
+}
+
+constexpr int Max_tracking_steps = 1 << 16;
+
+// Delta tracking with spectral MIS through a density grid over the world ray (ro, rd) for t in
+// [t0, t1] (Tracking_multi::integrate heterogeneous branch, tracking_multi.cpp:98-164, with
+// Tracking::tracking over a majorant cell, tracking.cpp:286-349).  srs scales the scattering
+// coefficient (similarity relation).  Returns true on a scattering event at t_out; lw receives
+// the path weight either way.
+__device__ bool track_grid(Medium_gpu const& g, shading::Material const& m, float srs, V3 ro,
+                           V3 rd, float t0, float t1, Rng& rng, float& t_out, V3& lw) {
+    V3 const    o     = to_texture(g, ro);
+    V3 const    d     = to_texture_dir(g, rd);
+    V3 const    mu_s  = srs * m.mu_s;
+    float const maj_t = shading::max_component(m.mu_a) + shading::max_component(mu_s);
+    lw                = v3(1.f, 1.f, 1.f);
+    int  steps        = 0;
+    bool scattered    = false;
+    walk_cells(g, o, d, t0, t1, [&](float2 cell, float ta, float tb) {
+        float const mt = cell.y * maj_t;
+        if (mt < Min_mt) {
+            return false;
+        }
+        float const imt = 1.f / mt;
+        for (float t = ta; steps < Max_tracking_steps; ++steps) {
+            t -= logf(1.f - rng.uniform()) * imt;
+            if (t > tb) {
+                return false;
+            }
+            float const den  = sample_density(g, o + t * d);
+            V3 const    ma   = den * m.mu_a;
+            V3 const    ms3  = den * mu_s;
+            V3 const    mu_n = v3(mt - (ma.x + ms3.x), mt - (ma.y + ms3.y), mt - (ma.z + ms3.z));
+            float const ms   = ((ms3.x * lw.x) + (ms3.y * lw.y) + (ms3.z * lw.z)) * (1.f / 3.f);
+            float const mn   = ((mu_n.x * lw.x) + (mu_n.y * lw.y) + (mu_n.z * lw.z)) * (1.f / 3.f);
+            float const sum  = ms + mn;
+            if (!(sum > 0.f)) {
+                lw = v3(0.f, 0.f, 0.f);
+                return true;
+            }
+            float const ps = ms / sum;
+            float const pn = mn / sum;
+            if ((rng.uniform() <= 1.f - pn) & (ps > 0.f)) {
+                lw        = lw * ((1.f / (mt * ps)) * ms3);
+                t_out     = t;
+                scattered = true;
+                return true;
+            }
+            lw = lw * ((1.f / (mt * pn)) * mu_n);
+        }
+        return true;
+    });
+    return scattered;
+}
+
+__device__ __forceinline__ bool all_below_abort(V3 w) {
+    return w.x < Abort_epsilon && w.y < Abort_epsilon && w.z < Abort_epsilon;
+}
+
+// Transmittance of a density grid along the world ray for t in [t0, t1]: ratio tracking per
+// majorant cell, residual ratio tracking against the cell's minorant where it is positive
+// (tracking_transmitted / residual_ratio_tracking_transmitted, tracking.cpp:32-140).  w is
+// multiplied by the estimate; returns false when it falls below Abort_epsilon (the shadow
+// ray counts as blocked, Tracking::transmittance, tracking.cpp:143-180).
+__device__ bool transmit_grid(Medium_gpu const& g, shading::Material const& m, float srs, V3 ro,
+                              V3 rd, float t0, float t1, Rng& rng, V3& w) {
+    V3 const    o     = to_texture(g, ro);
+    V3 const    d     = to_texture_dir(g, rd);
+    V3 const    mu_s  = srs * m.mu_s;
+    float const maj_t = shading::max_component(m.mu_a) + shading::max_component(mu_s);
+    float const min_t = shading::min_component(m.mu_a) + shading::min_component(mu_s);
+    int  steps        = 0;
+    bool blocked      = false;
+    walk_cells(g, o, d, t0, t1, [&](float2 cell, float ta, float tb) {
+        float const mt = cell.y * maj_t;
+        if (mt < Min_mt) {
+            return false;
+        }
+        // Control medium: the cell's minorant mu_t, whose transmittance is analytic; ratio
+        // tracking then samples only the residual (plain ratio tracking when it is 0).
+        float const cm = fmaxf(cell.x * min_t, 0.f);
+        if (cm > 0.f) {
+            w = expf(-(tb - ta) * cm) * w;
+            if (all_below_abort(w)) {
+                blocked = true;
+                return true;
+            }
+        }
+        float const mr = mt - cm;
+        if (mr < Min_mt) {
+            return false;
+        }
+        float const imr = 1.f / mr;
+        for (float t = ta; steps < Max_tracking_steps; ++steps) {
+            t -= logf(1.f - rng.uniform()) * imr;
+            if (t > tb) {
+                return false;
+            }
+            float const den = sample_density(g, o + t * d);
+            V3 const    mt3 = den * (m.mu_a + mu_s);
+            w = v3(w.x * ((mr - (mt3.x - cm)) * imr), w.y * ((mr - (mt3.y - cm)) * imr),
+                   w.z * ((mr - (mt3.z - cm)) * imr));
+            if (all_below_abort(w)) {
+                blocked = true;
+                return true;
+            }
+        }
+        return false;
+    });
+    return !blocked;
+}
+
 // ---- shade: one path vertex ----
 __global__ void __launch_bounds__(Shade_block)
     k_shade(Scene_gpu s, Wave wave, Paths p, uint32_t const* __restrict__ q_in,
@@ -448,8 +729,14 @@ __global__ void __launch_bounds__(Shade_block)
         } else if (medium != 0) {
             shading::Material const m = s.materials[medium - 1];
             V3 lw;
-            scatter = track_homogeneous(m, ro.w, p.hit_t[path], rng, t_sc, lw);
-            T       = T * lw;
+            if (m.medium != 0) {
+                float const srs = shading::similarity_relation_scale(m.g, depth);
+                scatter = track_grid(s.media[m.medium - 1], m, srs, f3v(ro), dir_in, ro.w,
+                                     p.hit_t[path], rng, t_sc, lw);
+            } else {
+                scatter = track_homogeneous(m, ro.w, p.hit_t[path], rng, t_sc, lw);
+            }
+            T = T * lw;
             if (!(lw.x >= Abort_epsilon || lw.y >= Abort_epsilon || lw.z >= Abort_epsilon)) {
                 done = true;
             }
@@ -484,7 +771,7 @@ __global__ void __launch_bounds__(Shade_block)
                         if (shading::max_component(contrib) > 0.f) {
                             p.sh_o[path] = make_float4(pos.x, pos.y, pos.z, 0.f);
                             p.sh_d[path] = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
-                            p.sh_L[path] = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
+                            p.sh_L[path] = make_float4(contrib.x, contrib.y, contrib.z, float(depth));
                             shadow       = true;
                         }
                     }
@@ -587,7 +874,7 @@ __global__ void __launch_bounds__(Shade_block)
                         if (shading::max_component(contrib) > 0.f) {
                             p.sh_o[path] = make_float4(ps.x, ps.y, ps.z, 0.f);
                             p.sh_d[path] = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
-                            p.sh_L[path] = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
+                            p.sh_L[path] = make_float4(contrib.x, contrib.y, contrib.z, float(depth));
                             shadow       = true;
                         }
                     }
@@ -631,8 +918,9 @@ __global__ void __launch_bounds__(Shade_block)
 
 // ---- shadow rays through media: Worker::transmittance (rendering_worker.cpp:209-267) ----
 // For each unoccluded shadow ray of a scene with media, walks the medium boundaries along the
-// ray (closest hits on boundary triangles only), accumulates the optical depth of each
-// homogeneous segment, and adds exp(-optical depth) times the light contribution.
+// ray (closest hits on boundary triangles only).  Homogeneous segments add their optical depth;
+// density-grid segments multiply in a ratio-tracking estimate (which uses the path's random
+// stream).  The light contribution, times the transmittance, is added to the path's radiance.
 __global__ void __launch_bounds__(Trace_block)
     k_transmit(Scene_gpu s, Paths p, uint32_t const* __restrict__ queue,
                uint32_t const* __restrict__ count, uint32_t* overflow) {
@@ -644,8 +932,14 @@ __global__ void __launch_bounds__(Trace_block)
     uint32_t       medium = p.info[path] >> 17;
     float4 const   ro     = p.sh_o[path];
     float4 const   rd     = p.sh_d[path];
+    float4 const   c      = p.sh_L[path];
+    uint32_t const depth  = uint32_t(c.w);
     float          t0     = ro.w;
     V3             tau    = v3(0.f, 0.f, 0.f);
+    V3             w      = v3(1.f, 1.f, 1.f);
+    bool           random = false;  // the path's random stream was used
+    bool           blocked = false;
+    Rng            rng;
     uint2          stack[gpu::Stack_size];
     for (int crossing = 0; crossing < 64; ++crossing) {
         gpu::Ray_state r;
@@ -658,8 +952,21 @@ __global__ void __launch_bounds__(Trace_block)
         float const end = hit ? r.tbest : rd.w;
         if (medium != 0) {
             shading::Material const m = s.materials[medium - 1];
-            float const len = fmaxf(end - t0, 0.f);
-            tau = tau + len * (m.mu_a + m.mu_s);
+            if (m.medium != 0) {
+                if (!random) {
+                    rng.load(p.rng[path]);
+                    random = true;
+                }
+                float const srs = shading::similarity_relation_scale(m.g, depth);
+                if (!transmit_grid(s.media[m.medium - 1], m, srs, f3v(ro), f3v(rd), t0, end, rng,
+                                   w)) {
+                    blocked = true;
+                    break;
+                }
+            } else {
+                float const len = fmaxf(end - t0, 0.f);
+                tau = tau + len * (m.mu_a + m.mu_s);
+            }
         }
         if (!hit) {
             break;
@@ -673,11 +980,16 @@ __global__ void __launch_bounds__(Trace_block)
             break;
         }
     }
-    float4 const c = p.sh_L[path];
-    float4       l = p.L[path];
-    l.x += expf(-tau.x) * c.x;
-    l.y += expf(-tau.y) * c.y;
-    l.z += expf(-tau.z) * c.z;
+    if (random) {
+        p.rng[path] = rng.save();
+    }
+    if (blocked) {
+        return;
+    }
+    float4 l = p.L[path];
+    l.x += w.x * expf(-tau.x) * c.x;
+    l.y += w.y * expf(-tau.y) * c.y;
+    l.z += w.z * expf(-tau.z) * c.z;
     p.L[path] = l;
 }
 
@@ -762,6 +1074,9 @@ struct Renderer::Device {
     float4*            lights     = nullptr;
     float*             light_cdf  = nullptr;
     float*             e_table    = nullptr;
+    Medium_gpu*        media      = nullptr;
+    std::vector<float*>  grid_density;  // one per density grid
+    std::vector<float2*> grid_cells;
     uint32_t           num_lights = 0;
     float              hit_margin = 0.f;
     // paths
@@ -771,6 +1086,7 @@ struct Renderer::Device {
     uint32_t* shadow_queue   = nullptr;
     uint32_t* transmit_queue = nullptr;
     uint32_t* counters       = nullptr;
+    uint32_t* pinned_count   = nullptr;  // host-pinned word for the queue-length check
     bool      has_media      = false;
     // film
     float4*   film = nullptr;
@@ -803,7 +1119,63 @@ cudaError_t upload(T*& dst, void const* src, size_t bytes) {
     return bytes ? cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
 }
 
+// Majorant cells of a density grid: (min, max) density over each Cell_dim^3 block of voxels
+// plus one voxel on every side (wrapped for the repeat address mode, clipped otherwise), the
+// minimum starting at 1 as in Octree_builder::Splitter::split
+// (volumetric_octree_builder.cpp:170-186).
+std::vector<float2> majorant_cells(Density_grid const& g, bool repeat, int const cells[3]) {
+    int const           n[3] = {int(g.dims[0]), int(g.dims[1]), int(g.dims[2])};
+    int const           dim  = 1 << Cell_log2;
+    std::vector<float2> out(size_t(cells[0]) * cells[1] * cells[2]);
+    auto wrap = [&](int v, int axis) { return ((v % n[axis]) + n[axis]) % n[axis]; };
+    for (int cz = 0; cz < cells[2]; ++cz) {
+        for (int cy = 0; cy < cells[1]; ++cy) {
+            for (int cx = 0; cx < cells[0]; ++cx) {
+                int const c[3] = {cx, cy, cz};
+                int       lo[3];
+                int       hi[3];
+                for (int a = 0; a < 3; ++a) {
+                    lo[a] = c[a] * dim - 1;
+                    hi[a] = std::min((c[a] + 1) * dim + 1, n[a] + (repeat ? 1 : 0));
+                    if (!repeat) {
+                        lo[a] = std::max(lo[a], 0);
+                    }
+                }
+                float mn = 1.f;
+                float mx = 0.f;
+                for (int z = lo[2]; z < hi[2]; ++z) {
+                    for (int y = lo[1]; y < hi[1]; ++y) {
+                        size_t const row = (size_t(wrap(z, 2)) * n[1] + wrap(y, 1)) * n[0];
+                        for (int x = lo[0]; x < hi[0]; ++x) {
+                            float const v = g.density[row + wrap(x, 0)];
+                            mn            = std::min(mn, v);
+                            mx            = std::max(mx, v);
+                        }
+                    }
+                }
+                if (mn > mx) {
+                    mn = mx = 0.f;
+                }
+                out[(size_t(cz) * cells[1] + cy) * cells[0] + cx] = make_float2(mn, mx);
+            }
+        }
+    }
+    return out;
+}
+
 }  // namespace
+
+void Renderer::free_grids() {
+    for (float*& g : d_->grid_density) {
+        free_ptr(g);
+    }
+    for (float2*& c : d_->grid_cells) {
+        free_ptr(c);
+    }
+    d_->grid_density.clear();
+    d_->grid_cells.clear();
+    free_ptr(d_->media);
+}
 
 Renderer::Renderer() : d_(new Device) {
     float table[Filter_samples];
@@ -815,6 +1187,7 @@ Renderer::Renderer() : d_(new Device) {
     }
     cudaMemcpyToSymbol(c_filter, table, sizeof(table));
     cudaStreamCreateWithFlags(&d_->stream, cudaStreamNonBlocking);
+    cudaMallocHost(&d_->pinned_count, sizeof(uint32_t));
     cudaEventCreate(&d_->ev0);
     cudaEventCreate(&d_->ev1);
     int per_sm = 0;
@@ -841,6 +1214,7 @@ Renderer::~Renderer() {
     free_ptr(d_->lights);
     free_ptr(d_->light_cdf);
     free_ptr(d_->e_table);
+    free_grids();
     Paths& p = d_->paths;
     free_ptr(p.ray_o);
     free_ptr(p.ray_d);
@@ -860,6 +1234,9 @@ Renderer::~Renderer() {
     free_ptr(d_->shadow_queue);
     free_ptr(d_->transmit_queue);
     free_ptr(d_->counters);
+    if (d_->pinned_count) {
+        cudaFreeHost(d_->pinned_count);
+    }
     free_ptr(d_->film);
     free_ptr(d_->comp);
     free_ptr(d_->out);
@@ -990,6 +1367,45 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     SPB_RCUDA(upload(d_->light_cdf, cdf.data(), cdf.size() * sizeof(float)));
     SPB_RCUDA(upload(d_->e_table, ggx_albedo_table(),
                      Ggx_table_size * Ggx_table_size * sizeof(float)));
+
+    // Density grids and the media that sample them.
+    free_grids();
+    std::vector<Medium_gpu> media;
+    for (Density_grid const& g : scene.grids) {
+        size_t const n = size_t(g.dims[0]) * g.dims[1] * g.dims[2];
+        d_->grid_density.push_back(nullptr);
+        SPB_RCUDA(upload(d_->grid_density.back(), g.density, n * sizeof(float)));
+    }
+    d_->grid_cells.assign(scene.media.size(), nullptr);
+    for (size_t k = 0; k < scene.media.size(); ++k) {
+        Grid_medium const& gm = scene.media[k];
+        if (gm.grid >= scene.grids.size()) {
+            error_ = "medium refers to a missing density grid";
+            return SPB_ERROR_ARGUMENT;
+        }
+        Density_grid const& g = scene.grids[gm.grid];
+        Medium_gpu          mg{};
+        float const*        r = gm.world_to_uvw;
+        mg.m0      = make_float4(r[0], r[1], r[2], r[3]);
+        mg.m1      = make_float4(r[4], r[5], r[6], r[7]);
+        mg.m2      = make_float4(r[8], r[9], r[10], r[11]);
+        mg.density = d_->grid_density[gm.grid];
+        mg.nx      = int(g.dims[0]);
+        mg.ny      = int(g.dims[1]);
+        mg.nz      = int(g.dims[2]);
+        int const cells[3] = {(mg.nx + (1 << Cell_log2) - 1) >> Cell_log2,
+                              (mg.ny + (1 << Cell_log2) - 1) >> Cell_log2,
+                              (mg.nz + (1 << Cell_log2) - 1) >> Cell_log2};
+        mg.cx    = cells[0];
+        mg.cy    = cells[1];
+        mg.cz    = cells[2];
+        mg.flags = (gm.nearest ? 1u : 0u) | (gm.repeat ? 2u : 0u);
+        std::vector<float2> const cm = majorant_cells(g, gm.repeat, cells);
+        SPB_RCUDA(upload(d_->grid_cells[k], cm.data(), cm.size() * sizeof(float2)));
+        mg.cells = d_->grid_cells[k];
+        media.push_back(mg);
+    }
+    SPB_RCUDA(upload(d_->media, media.data(), media.size() * sizeof(Medium_gpu)));
     scene_ready_ = true;
     return SPB_OK;
 }
@@ -1076,6 +1492,10 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         error_ = "render needs a scene and a camera";
         return SPB_ERROR_STATE;
     }
+    if (!d_->pinned_count) {
+        error_ = "no pinned host memory (CUDA unavailable)";
+        return SPB_ERROR_CUDA;
+    }
     if (settings_.max_bounces + 2 > Max_bounce_slots) {
         error_ = "max_bounces too large";
         return SPB_ERROR_ARGUMENT;
@@ -1113,10 +1533,16 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     sg.light_cdf     = d_->light_cdf;
     sg.num_lights    = d_->num_lights;
     sg.e_table       = d_->e_table;
+    sg.media         = d_->media;
 
     cudaStream_t const st = d_->stream;
     uint32_t* const    ctr = d_->counters;
-    uint32_t const     bounces = settings_.max_bounces + 1;
+    // One iteration per path vertex.  Medium boundaries are null vertices: they take an
+    // iteration without counting as a bounce (Straight_transmission keeps ray.depth,
+    // pathtracer_mis.cpp:180-182), so with media the loop goes on while paths remain, up to the
+    // counter block's capacity (paths still alive after that many vertices are cut).
+    uint32_t const bounce_iterations = settings_.max_bounces + 1;
+    uint32_t const max_iterations = d_->has_media ? Max_bounce_slots - 1 : bounce_iterations;
 
     stats_ = Stats();
     std::vector<uint32_t> host_ctr(Counter_words);
@@ -1129,7 +1555,17 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         SPB_RCUDA(cudaMemsetAsync(ctr, 0, Counter_words * sizeof(uint32_t), st));
         k_generate<<<(paths + 255) / 256, 256, 0, st>>>(cam, wave, d_->paths, d_->queue[0], ctr,
                                                          paths);
-        for (uint32_t b = 0; b < bounces; ++b) {
+        uint32_t iterations = 0;
+        for (uint32_t b = 0; b < max_iterations; ++b) {
+            if (b >= bounce_iterations) {
+                SPB_RCUDA(cudaMemcpyAsync(d_->pinned_count, ctr + Counter_stride * b,
+                                          sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+                SPB_RCUDA(cudaStreamSynchronize(st));
+                if (*d_->pinned_count == 0) {
+                    break;
+                }
+            }
+            iterations = b + 1;
             uint32_t* const q_in  = d_->queue[b & 1];
             uint32_t* const q_out = d_->queue[(b + 1) & 1];
             uint32_t* const c = ctr + Counter_stride * b;
@@ -1154,7 +1590,7 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         SPB_RCUDA(cudaMemcpyAsync(host_ctr.data(), ctr, Counter_words * sizeof(uint32_t),
                                   cudaMemcpyDeviceToHost, st));
         SPB_RCUDA(cudaStreamSynchronize(st));
-        for (uint32_t b = 0; b < bounces; ++b) {
+        for (uint32_t b = 0; b < iterations; ++b) {
             stats_.extension_rays += host_ctr[Counter_stride * b];
             stats_.shadow_rays += host_ctr[Counter_stride * b + 1];
         }

@@ -9,6 +9,22 @@
 
 namespace spb::render {
 
+// A density grid (one-channel 3-D image, su_create_image), x fastest then y then z.
+struct Density_grid {
+    uint32_t     dims[3] = {0, 0, 0};
+    float const* density = nullptr;  // dims[0] * dims[1] * dims[2] values, read during set_scene
+};
+
+// One prop filled with a heterogeneous medium (Grid material, volumetric_grid.cpp): the grid it
+// samples and the map from world space to the grid's texture space [0, 1]^3 (the prop's
+// world-to-object transformation followed by its mesh bounds, tracking.inl:12-29).
+struct Grid_medium {
+    uint32_t grid           = 0;      // index into Scene_desc::grids
+    bool     nearest        = false;  // Nearest_3D filter instead of Linear_3D
+    bool     repeat         = false;  // Address_mode_repeat instead of clamp
+    float    world_to_uvw[12] = {};   // rows: uvw_k = dot(row_k.xyz, p) + row_k.w
+};
+
 // World-space scene as the host engine flattens it (one BVH over all props' triangles).
 struct Scene_desc {
     std::vector<float>              positions;     // 3 per vertex, world space
@@ -16,7 +32,9 @@ struct Scene_desc {
     std::vector<uint32_t>           indices;       // 3 per triangle
     std::vector<uint32_t>           tri_material;  // per triangle, index into materials
     std::vector<uint8_t>            tri_light;     // per triangle: 1 if it belongs to a light prop
-    std::vector<shading::Material>  materials;
+    std::vector<shading::Material>  materials;    // Volume materials: medium = 1 + grid medium
+    std::vector<Density_grid>       grids;
+    std::vector<Grid_medium>        media;
 };
 
 struct Camera_desc {
@@ -77,6 +95,7 @@ class Renderer {
     std::string error_;
 
     int32_t ensure_buffers(uint32_t paths);
+    void    free_grids();
     int32_t fail_cuda(char const* what, int code);
 };
 

@@ -12,6 +12,9 @@ binds (this package's or the reference's), so both render the identical scene:
 * a pinhole camera with a 40 degree horizontal field of view;
 * PTMIS, max_bounces 8 (min_bounces 4, the reference default).
 Colours are given in sRGB; both libraries map them to ACEScg.
+
+Variants replace the metal sphere by a participating medium: a homogeneous Volumetric sphere,
+or a rotated, scaled cube filled with a density grid (an in-memory 3-D image).
 """
 
 from __future__ import annotations
@@ -61,6 +64,52 @@ def _quad(p0, p1, p2, p3, normal):
     return pos, np.tile(n, (4, 1)), idx
 
 
+def box():
+    """Cube [-0.5, 0.5]^3 with outward faces: 12 triangles, 24 vertices (flat normals)."""
+    pos, nrm, idx = [], [], []
+    for axis in range(3):
+        for sign in (-1.0, 1.0):
+            n = np.zeros(3, np.float32)
+            n[axis] = sign
+            u, v = np.zeros(3, np.float32), np.zeros(3, np.float32)
+            u[(axis + 1) % 3], v[(axis + 2) % 3] = 0.5, 0.5
+            c = 0.5 * n
+            qp, qn, qi = _quad(c - u - v, c + u - v, c + u + v, c - u + v, n)
+            idx.append(qi + len(pos) * 4)
+            pos.append(qp)
+            nrm.append(qn)
+    return np.concatenate(pos), np.concatenate(nrm), np.concatenate(idx)
+
+
+def density_grid(nx: int = 24, ny: int = 20, nz: int = 28, seed: int = 4):
+    """Deterministic density image (nz, ny, nx) in [0, 1]: a smooth blob times seeded
+    low-frequency waves, exactly 0 near the corners (empty majorant cells)."""
+    rng = np.random.default_rng(seed)
+    z, y, x = np.meshgrid((np.arange(nz) + 0.5) / nz, (np.arange(ny) + 0.5) / ny,
+                          (np.arange(nx) + 0.5) / nx, indexing="ij")
+    d = np.zeros_like(x)
+    for _ in range(4):
+        f = rng.uniform(1.0, 4.0, 3)
+        ph = rng.uniform(0.0, 2.0 * np.pi, 3)
+        d += np.sin(2 * np.pi * f[0] * x + ph[0]) * np.sin(2 * np.pi * f[1] * y + ph[1]) * \
+            np.sin(2 * np.pi * f[2] * z + ph[2])
+    r = np.sqrt((x - 0.5) ** 2 + (y - 0.5) ** 2 + (z - 0.5) ** 2)
+    d = np.clip(0.55 + 0.35 * d, 0.0, 1.0) * np.clip(1.6 - 2.6 * r, 0.0, 1.0)
+    return d.astype(np.float32)
+
+
+def grid_box_transformation(angle_degrees: float = 30.0, scale: float = 0.7,
+                            position=(0.05, 0.45, 0.1)):
+    """Row-major object-to-world matrix of the medium cube: uniform scale, rotation about y,
+    translation."""
+    a = math.radians(angle_degrees)
+    c, s = math.cos(a), math.sin(a)
+    m = np.eye(4, dtype=np.float32)
+    m[:3, :3] = scale * np.array([[c, 0.0, -s], [0.0, 1.0, 0.0], [s, 0.0, c]], np.float32)
+    m[3, :3] = position
+    return m
+
+
 def cornell_geometry(sphere_subdivisions: int = 6):
     """name -> (positions, normals, indices) in world space (y up, box x, z in [-1, 1], y in [0, 2])."""
     g = {}
@@ -88,11 +137,13 @@ def translation(x, y, z):
 
 def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounces: int = 8,
             min_bounces: int = 4, fov_degrees: float = 40.0, camera_position=(0.0, 1.0, -3.4),
-            spp: int = 64, tonemap: bool = False, medium=None):
+            spp: int = 64, tonemap: bool = False, medium=None, density=None):
     """Issues the scene's su_* calls on an initialised engine; returns the camera entity.
 
     medium: optional dict of Volumetric material parameters (e.g. color, attenuation_distance,
     anisotropy); the sphere then becomes a homogeneous participating medium instead of metal.
+    density: optional (nz, ny, nx) float array; with medium, the sphere is replaced by the
+    cube of grid_box_transformation() filled with this density grid.
     """
     cam = su.su_create_camera_perspective(width, height, math.radians(fov_degrees))
     su.set_transformation(cam, translation(*camera_position))
@@ -107,18 +158,25 @@ def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounc
     green = _material(su, "Substitute", color=[0.05, 0.75, 0.05], roughness=1.0, metallic=0.0)
     if medium is None:
         metal = _material(su, "Substitute", color=[0.95, 0.64, 0.54], roughness=math.sqrt(0.3), metallic=1.0)
-    else:
+    elif density is None:
         metal = _material(su, "Volumetric", **medium)
+    else:
+        image = su.image(density)
+        metal = _material(su, "Volumetric", density={"id": int(image)}, **medium)
     light = _material(su, "Light", emission=[17.0, 17.0, 17.0])
 
     geo = cornell_geometry(sphere_subdivisions)
+    trafo = {}
+    if density is not None:
+        geo["sphere"] = box()
+        trafo["sphere"] = grid_box_transformation()
     assign = {"floor": white, "ceiling": white, "back": white, "left": red, "right": green,
               "light": light, "sphere": metal}
     for name, (pos, nrm, idx) in geo.items():
         shape = su.mesh(pos, nrm, idx)
         prop = su.prop(shape, [assign[name]])
         # props carry no default world transformation in the reference: always set one
-        su.set_transformation(prop, np.eye(4, dtype=np.float32))
+        su.set_transformation(prop, trafo.get(name, np.eye(4, dtype=np.float32)))
         if name == "light":
             su.su_create_light(prop)
     return cam

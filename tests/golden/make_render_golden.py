@@ -4,7 +4,8 @@ Renders the Cornell-box scene of sprout_b200.scenes.cornell through the referenc
 (oracle/_ref/ref_render replaying the su_* calls; batch mode, su_create_defaults, i.e. the
 Linear tonemapper to linear sRGB) at sizes the tests can compare against.
 
-    python tests/golden/make_render_golden.py
+    python tests/golden/make_render_golden.py [case ...]   (default: all cases; named cases
+                                                            are re-rendered into the existing file)
 """
 
 from __future__ import annotations
@@ -24,31 +25,50 @@ from sprout_b200 import scenes  # noqa: E402
 
 # A homogeneous scattering sphere in place of the metal one (Volumetric material).
 MEDIUM = {"color": [0.8, 0.8, 0.8], "attenuation_distance": 0.05, "anisotropy": 0.5}
+# An optically thin one, seen through: with max_bounces 1 the image is the direct light of the
+# surfaces behind it, reached through two null (boundary) vertices that must not count as
+# bounces.
+THIN_MEDIUM = {"color": [0.8, 0.8, 0.8], "attenuation_distance": 0.5, "anisotropy": 0.5}
+# A rotated, scaled cube filled with a density grid (Volumetric material with "density"),
+# colour-dependent attenuation so that spectral MIS matters.
+GRID_MEDIUM = {"color": [0.9, 0.6, 0.4], "attenuation_distance": 0.03, "anisotropy": 0.3}
 
-# name -> (width, height, spp, sphere subdivisions, medium)
+# name -> (width, height, spp, scenes.cornell keyword arguments, density grid or None)
 CASES = {
-    "cornell64_sub3": (64, 64, 4096, 3, None),
-    "cornell128_sub6": (128, 128, 2048, 6, None),
-    "cornell64_medium": (64, 64, 4096, 4, MEDIUM),
+    "cornell64_sub3": (64, 64, 4096, {"sphere_subdivisions": 3}, None),
+    "cornell128_sub6": (128, 128, 2048, {"sphere_subdivisions": 6}, None),
+    "cornell64_medium": (64, 64, 4096, {"sphere_subdivisions": 4, "medium": MEDIUM}, None),
+    "cornell64_thin_direct": (64, 64, 4096, {"sphere_subdivisions": 4, "medium": THIN_MEDIUM,
+                                             "max_bounces": 1, "min_bounces": 1}, None),
+    "cornell64_grid": (64, 64, 4096, {"sphere_subdivisions": 2, "medium": GRID_MEDIUM},
+                       scenes.density_grid()),
 }
+PATH = HERE / "cornell_reference.npz"
 
 
-def main():
-    out = {}
-    meta = {"generator": "oracle/_ref/ref_render (reference su_* C API, batch mode)", "cases": {}}
-    for name, (w, h, spp, sub, medium) in CASES.items():
+def main(names):
+    out, meta = {}, {"generator": "oracle/_ref/ref_render (reference su_* C API, batch mode)", "cases": {}}
+    if names and PATH.exists():
+        old = np.load(PATH)
+        out = {k: old[k] for k in old.files if k != "meta"}
+        meta = json.loads(bytes(old["meta"]).decode())
+    for name in names or CASES:
+        w, h, spp, kwargs, density = CASES[name]
         img, timing = oracle.reference_render(
-            lambda su: scenes.cornell(su, w, h, sphere_subdivisions=sub, tonemap=True, spp=spp,
-                                      medium=medium),
+            lambda su: scenes.cornell(su, w, h, tonemap=True, spp=spp, density=density, **kwargs),
             w, h, 0, progressive=False)
+        if timing["status"] != 0:
+            raise RuntimeError(f"{name}: reference status {timing['status']}")
         out[name] = img.astype(np.float32)
-        meta["cases"][name] = {"width": w, "height": h, "spp": spp, "sphere_subdivisions": sub,
-                               "medium": medium,
+        if density is not None:
+            out[name + "_density"] = density
+        meta["cases"][name] = {"width": w, "height": h, "spp": spp, "scene": kwargs,
+                               "density": None if density is None else name + "_density",
                                "render_s": timing["render_s"], "mean": [float(x) for x in img.mean(axis=(0, 1))]}
-        print(name, meta["cases"][name])
+        print(name, meta["cases"][name], flush=True)
     out["meta"] = np.frombuffer(json.dumps(meta).encode(), np.uint8)
-    np.savez_compressed(HERE / "cornell_reference.npz", **out)
+    np.savez_compressed(PATH, **out)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

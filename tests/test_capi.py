@@ -66,6 +66,36 @@ def test_c_api_without_gpu_state():
     assert su.su_release() == 0
 
 
+def test_density_images_and_grid_materials():
+    """su_create_image ids count from 0; a Volumetric "density" must name a one-channel image."""
+    import json
+
+    import numpy as np
+
+    from sprout_b200 import capi
+
+    su = capi.SuLibrary()
+    assert su.su_init(False) == 0
+    try:
+        grid = np.linspace(0, 1, 4 * 3 * 2, dtype=np.float32).reshape(2, 3, 4)
+        assert su.image(grid) == 0
+        rgb = np.zeros((2, 2, 3), np.uint8)
+        assert su.su_create_image(0, 3, 2, 2, 1, 0, 3, rgb.ctypes.data) == 1
+        assert su.su_create_image(1, 1, 2, 2, 1, 0, 2, rgb.ctypes.data) == capi.SU_RESOURCE_NULL
+
+        def volumetric(**p):
+            return su.su_create_material(json.dumps({"rendering": {"Volumetric": p}}).encode())
+
+        assert volumetric(density={"id": 0}, attenuation_distance=0.1) == 0
+        assert volumetric(density={"id": 0}, sampler={"filter": "Nearest", "address": "Repeat"}) == 1
+        assert volumetric(density={"id": 1}) == capi.SU_RESOURCE_NULL  # three channels
+        assert volumetric(density={"id": 7}) == capi.SU_RESOURCE_NULL  # no such image
+        assert volumetric(density={"file": "smoke.sub"}) == capi.SU_RESOURCE_NULL
+        assert volumetric(density={"id": 0}, emission=[1, 1, 1]) == capi.SU_RESOURCE_NULL
+    finally:
+        assert su.su_release() == 0
+
+
 def test_ggx_albedo_table_matches_reference_table():
     """The energy-compensation table computed by this project against the reference's
     generated table (material/ggx/ggx_integral.inl), read from the reference sources when
