@@ -180,12 +180,15 @@ class ScriptRecorder:
         return self.n["image"] - 1
 
     def mesh(self, positions, normals, indices, parts=None):
-        assert parts is None
         pos = np.asarray(positions, np.float32).reshape(-1, 3)
         nrm = np.asarray(normals, np.float32).reshape(-1, 3)
         idx = np.asarray(indices, np.uint32).reshape(-1, 3)
         op, on, oi = self._blob(pos), self._blob(nrm), self._blob(idx)
-        self.lines.append(f"mesh {idx.shape[0]} {pos.shape[0]} {op} {on} {oi}")
+        line = f"mesh {idx.shape[0]} {pos.shape[0]} {op} {on} {oi}"
+        if parts is not None:
+            prt = np.asarray(parts, np.uint32).reshape(-1, 3)
+            line += f" {prt.shape[0]} {self._blob(prt)}"
+        self.lines.append(line)
         self.n["mesh"] += 1
         return 2000 + self.n["mesh"] - 1
 

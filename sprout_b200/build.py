@@ -22,8 +22,9 @@ ORACLE = ROOT / "oracle"
 ORACLE_LIB = ORACLE / "libcast_oracle.so"
 REFERENCE = pathlib.Path(os.environ.get("SPROUT_REFERENCE", "/root/reference"))
 
-SOURCES = ["common.cpp", "synth.cpp", "bvh8.cpp", "ggx_table.cpp", "cast.cu", "render.cu", "capi.cpp"]
-HEADERS = ["common.hpp", "bvh8.hpp", "traverse.cuh", "material.cuh", "render.hpp", "json.hpp", "ggx_table.hpp"]
+SOURCES = ["common.cpp", "synth.cpp", "bvh8.cpp", "ggx_table.cpp", "light_tree.cpp", "cast.cu", "render.cu", "capi.cpp"]
+HEADERS = ["common.hpp", "bvh8.hpp", "traverse.cuh", "material.cuh", "render.hpp", "json.hpp", "ggx_table.hpp",
+           "light_tree.hpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

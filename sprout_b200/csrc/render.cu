@@ -32,6 +32,7 @@
 #include "bvh8.hpp"
 #include "common.hpp"
 #include "ggx_table.hpp"
+#include "light_tree.hpp"
 #include "render.hpp"
 #include "traverse.cuh"
 
@@ -79,9 +80,10 @@ struct Scene_gpu {
     float4 const*             positions;
     float4 const*             normals;
     shading::Material const*  materials;
-    float const*              tri_light_pdf;  // pick probability / area, 0 if not a sampled light
-    float4 const*             lights;         // 3 per light: (a, area), (e1, pick), (e2, tri id)
-    float const*              light_cdf;      // num_lights + 1 entries
+    float4 const*             light_nodes;  // light tree (light_tree.hpp): 3 per node
+    float4 const*             light_cones;  // 3 per light in tree order: bounds for importance
+    float4 const*             light_tris;   // 3 per light in tree order: (a, area), e1, (e2, tri)
+    uint32_t const*           light_order;  // per triangle: tree order, 0xFFFFFFFF if no light
     uint32_t                  num_lights;
     float const*              e_table;
     Medium_gpu const*         media;  // Material::medium - 1 indexes this
@@ -101,6 +103,7 @@ struct Paths {
     float4*   sh_o;
     float4*   sh_d;
     float4*   sh_L;
+    float4*   prev_n;  // geometric normal at the last scattering vertex; w 1: medium vertex
 };
 
 struct Cam {
@@ -333,9 +336,146 @@ __device__ __forceinline__ uint32_t pack_info(uint32_t vtx, uint32_t depth, bool
     return (vtx & 0xFFu) | ((depth & 0xFFu) << 8) | (singular ? (1u << 16) : 0u) | (medium << 17);
 }
 
-// Light sample for next-event estimation seen from ps: power-proportional triangle, uniform
-// point, solid-angle pdf (with the pick probability).  False if the sample is unusable
-// (grazing or behind a one-sided emitter, Mesh::sample in triangle_mesh.cpp:462-516).
+// ---- light tree (light_tree.hpp): importance, sampling and pdf ----
+// cos(max(a - b, 0)) and sin(max(a - b, 0)) from the cosines and sines of a and b.
+__device__ __forceinline__ float cos_sub_clamped(float ca, float cb, float sa, float sb) {
+    return ca > cb ? 1.f : ca * cb + sa * sb;
+}
+__device__ __forceinline__ float sin_sub_clamped(float ca, float cb, float sa, float sb) {
+    return ca > cb ? 0.f : sa * cb - ca * sb;
+}
+
+// Importance of a light cluster seen from p (normal n, or the whole sphere of directions for a
+// medium vertex): power / squared distance (not closer than half the bounding radius) times
+// the best cosines the bounding sphere and normal cone allow at the emitter and the receiver
+// (Estevez and Kulla 2018, eq. 3; the reference's importance(), light_tree.cpp:27-62).
+// Never 0, so that every light keeps a positive probability.
+__device__ float light_importance(float4 sphere, float4 cone, float power, V3 p, V3 n,
+                                  bool total_sphere) {
+    V3 const    v  = v3(sphere.x - p.x, sphere.y - p.y, sphere.z - p.z);
+    float const d2 = fmaxf(shading::dot(v, v), 1e-30f);
+    float const il = rsqrtf(d2);
+    V3 const    w  = il * v;  // towards the cluster
+    float const su = fminf(sphere.w * il, 1.f);
+    float const cu = sqrtf(fmaxf(1.f - su * su, 0.f));
+    // emitter side: angle between the cone axis and the direction from the cluster to p
+    float       ce = 1.f;
+    if (cone.w > -1.f) {
+        float const ca = -(cone.x * w.x + cone.y * w.y + cone.z * w.z);
+        float const sa = sqrtf(fmaxf(1.f - ca * ca, 0.f));
+        float const so = sqrtf(fmaxf(1.f - cone.w * cone.w, 0.f));
+        float const c1 = cos_sub_clamped(ca, cone.w, sa, so);
+        float const s1 = sin_sub_clamped(ca, cone.w, sa, so);
+        ce             = fmaxf(cos_sub_clamped(c1, cu, s1, su), 0.f);
+    }
+    // receiver side
+    float cr = 1.f;
+    if (!total_sphere) {
+        float const ci = shading::dot(n, w);
+        float const si = sqrtf(fmaxf(1.f - ci * ci, 0.f));
+        cr             = fmaxf(cos_sub_clamped(ci, cu, si, su), 0.f);
+    }
+    float const dist = fmaxf(d2, 0.25f * sphere.w * sphere.w);
+    return fmaxf(power * ce * cr / dist, 1e-30f);
+}
+
+// Picks a light (tree order) by walking the tree from the root with the random number r;
+// returns its index and sets pick to its probability.
+__device__ uint32_t pick_light(Scene_gpu const& s, V3 p, V3 n, bool total_sphere, float r,
+                               float& pick) {
+    float    pdf  = 1.f;
+    uint32_t node = 0;
+    for (int level = 0; level < 64; ++level) {
+        float4 const   meta  = s.light_nodes[3 * node + 2];
+        uint32_t const first = __float_as_uint(meta.y);
+        uint32_t const count = __float_as_uint(meta.z);
+        if (count != 0) {
+            float w[Light_leaf_size];
+            float sum = 0.f;
+            for (uint32_t k = 0; k < Light_leaf_size; ++k) {
+                w[k] = 0.f;
+                if (k < count) {
+                    uint32_t const l = first + k;
+                    w[k] = light_importance(s.light_cones[3 * l], s.light_cones[3 * l + 1],
+                                            s.light_cones[3 * l + 2].x, p, n, total_sphere);
+                    sum += w[k];
+                }
+            }
+            float    acc    = 0.f;
+            uint32_t chosen = count - 1;
+            for (uint32_t k = 0; k + 1 < count; ++k) {
+                acc += w[k];
+                if (r * sum < acc) {
+                    chosen = k;
+                    break;
+                }
+            }
+            pick = pdf * (w[chosen] / sum);
+            return first + chosen;
+        }
+        uint32_t const c0 = first;
+        float const    w0 = light_importance(s.light_nodes[3 * c0], s.light_nodes[3 * c0 + 1],
+                                             s.light_nodes[3 * c0 + 2].x, p, n, total_sphere);
+        float const    w1 = light_importance(s.light_nodes[3 * c0 + 3], s.light_nodes[3 * c0 + 4],
+                                             s.light_nodes[3 * c0 + 5].x, p, n, total_sphere);
+        float const    p0 = w0 / (w0 + w1);
+        if (r < p0) {
+            node = c0;
+            pdf *= p0;
+            r = fminf(r / p0, 0x1.fffffep-1f);
+        } else {
+            node = c0 + 1;
+            pdf *= 1.f - p0;
+            r = fminf((r - p0) / (1.f - p0), 0x1.fffffep-1f);
+        }
+    }
+    pick = 0.f;
+    return 0;
+}
+
+// Probability that pick_light from (p, n) returns the light at tree position order
+// (Tree::pdf, light_tree.cpp:564-640): the same importances along the path to its leaf.
+__device__ float light_pick_pdf(Scene_gpu const& s, V3 p, V3 n, bool total_sphere,
+                                uint32_t order) {
+    float    pdf  = 1.f;
+    uint32_t node = 0;
+    for (int level = 0; level < 64; ++level) {
+        float4 const   meta  = s.light_nodes[3 * node + 2];
+        uint32_t const first = __float_as_uint(meta.y);
+        uint32_t const count = __float_as_uint(meta.z);
+        if (count != 0) {
+            float sum = 0.f;
+            float mine = 0.f;
+            for (uint32_t k = 0; k < count && k < Light_leaf_size; ++k) {
+                uint32_t const l = first + k;
+                float const    w = light_importance(s.light_cones[3 * l], s.light_cones[3 * l + 1],
+                                                    s.light_cones[3 * l + 2].x, p, n, total_sphere);
+                sum += w;
+                mine = l == order ? w : mine;
+            }
+            return pdf * (mine / sum);
+        }
+        uint32_t const c0 = first;
+        float const    w0 = light_importance(s.light_nodes[3 * c0], s.light_nodes[3 * c0 + 1],
+                                             s.light_nodes[3 * c0 + 2].x, p, n, total_sphere);
+        float const    w1 = light_importance(s.light_nodes[3 * c0 + 3], s.light_nodes[3 * c0 + 4],
+                                             s.light_nodes[3 * c0 + 5].x, p, n, total_sphere);
+        float const    p0 = w0 / (w0 + w1);
+        if (order < __float_as_uint(meta.w)) {
+            node = c0;
+            pdf *= p0;
+        } else {
+            node = c0 + 1;
+            pdf *= 1.f - p0;
+        }
+    }
+    return 0.f;
+}
+
+// Light sample for next-event estimation seen from ps (normal n; total_sphere for medium
+// vertices): a light picked by the tree, a uniform point on it, the solid-angle pdf times the
+// pick probability.  False if the sample is unusable (grazing or behind a one-sided emitter,
+// Mesh::sample in triangle_mesh.cpp:462-516).
 struct Light_sample {
     V3    dir;
     float dist;
@@ -343,21 +483,16 @@ struct Light_sample {
     V3    radiance;
 };
 
-__device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, float r, float r1, float r2,
-                                             Light_sample& ls) {
-    uint32_t lo = 0;
-    uint32_t hi = s.num_lights;
-    while (hi - lo > 1) {
-        uint32_t const mid = (lo + hi) >> 1;
-        if (s.light_cdf[mid] <= r) {
-            lo = mid;
-        } else {
-            hi = mid;
-        }
+__device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, V3 n, bool total_sphere,
+                                             float r, float r1, float r2, Light_sample& ls) {
+    float          pick;
+    uint32_t const l = pick_light(s, ps, n, total_sphere, r, pick);
+    if (!(pick > 0.f)) {
+        return false;
     }
-    float4 const   la   = s.lights[3 * lo + 0];
-    float4 const   le1  = s.lights[3 * lo + 1];
-    float4 const   le2  = s.lights[3 * lo + 2];
+    float4 const   la   = s.light_tris[3 * l + 0];
+    float4 const   le1  = s.light_tris[3 * l + 1];
+    float4 const   le2  = s.light_tris[3 * l + 2];
     uint32_t const ltri = __float_as_uint(le2.w);
     float const    sq   = sqrtf(r1);
     V3 const       q    = f3v(la) + (sq * (1.f - r2)) * f3v(le1) + (sq * r2) * f3v(le2);
@@ -376,7 +511,7 @@ __device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, float r,
     }
     ls.dir      = dir;
     ls.dist     = d;
-    ls.pdf      = le1.w * d2 / (cl * la.w);
+    ls.pdf      = pick * d2 / (cl * la.w);
     ls.radiance = lmat.emission;
     return true;
 }
@@ -764,7 +899,7 @@ __global__ void __launch_bounds__(Shade_block)
                     float const  r1 = rng.uniform();
                     float const  r2 = rng.uniform();
                     Light_sample ls;
-                    if (sample_light(s, pos, r, r1, r2, ls)) {
+                    if (sample_light(s, pos, v3(0.f, 0.f, 1.f), true, r, r1, r2, ls)) {
                         float const f = shading::phase_hg(shading::dot(wo, ls.dir), g);
                         float const w = ls.pdf / (ls.pdf * ls.pdf + f * f);
                         V3 const contrib = (w * f) * (T * ls.radiance);
@@ -782,6 +917,7 @@ __global__ void __launch_bounds__(Shade_block)
                 V3 const    wi = shading::sample_hg(wo, g, x0, x1, pdf);
                 p.ray_o[path]  = make_float4(pos.x, pos.y, pos.z, 0.f);
                 p.ray_d[path]  = make_float4(wi.x, wi.y, wi.z, Ray_max_t);
+                p.prev_n[path] = make_float4(0.f, 0.f, 1.f, 1.f);
                 bsdf_pdf       = pdf;  // reflection / pdf == 1
                 singular       = false;
                 ++depth;
@@ -812,9 +948,16 @@ __global__ void __launch_bounds__(Shade_block)
                 if (emits) {
                     if (front || mat.two_sided) {
                         float w = 1.f;
-                        if (!singular) {
-                            float const t      = p.hit_t[path];
-                            float const pdf_l  = s.tri_light_pdf[id] * (t * t) / fabsf(cos_o);
+                        uint32_t const order = s.light_order[id];
+                        if (!singular && order != 0xFFFFFFFFu) {
+                            // the light-tree pick from the previous vertex (connect_light,
+                            // pathtracer_mis.cpp:349-380)
+                            float4 const pn    = p.prev_n[path];
+                            float const  pick  = light_pick_pdf(s, f3v(ro), f3v(pn), pn.w != 0.f,
+                                                                order);
+                            float const  t     = p.hit_t[path];
+                            float const  area  = s.light_tris[3 * order].w;
+                            float const  pdf_l = pick * (t * t) / (fabsf(cos_o) * area);
                             w                  = power_heuristic(bsdf_pdf, pdf_l);
                         }
                         L = L + w * (T * mat.emission);
@@ -866,7 +1009,7 @@ __global__ void __launch_bounds__(Shade_block)
                     float const  r2 = rng.uniform();
                     V3 const     ps = offset_ray(pos, geo_n);
                     Light_sample ls;
-                    if (sample_light(s, ps, r, r1, r2, ls)) {
+                    if (sample_light(s, ps, geo_n, false, r, r1, r2, ls)) {
                         shading::Bxdf const f =
                             shading::substitute_evaluate(mat, s.e_table, ctx, ls.dir);
                         float const w = ls.pdf / (ls.pdf * ls.pdf + f.pdf * f.pdf);
@@ -888,8 +1031,9 @@ __global__ void __launch_bounds__(Shade_block)
                     shading::substitute_sample(mat, s.e_table, ctx, xl, x0, x1);
                 if (smp.pdf > 0.f) {
                     V3 const o = offset_ray(pos, shading::dot(geo_n, smp.wi) > 0.f ? geo_n : -geo_n);
-                    p.ray_o[path] = make_float4(o.x, o.y, o.z, 0.f);
-                    p.ray_d[path] = make_float4(smp.wi.x, smp.wi.y, smp.wi.z, Ray_max_t);
+                    p.ray_o[path]  = make_float4(o.x, o.y, o.z, 0.f);
+                    p.ray_d[path]  = make_float4(smp.wi.x, smp.wi.y, smp.wi.z, Ray_max_t);
+                    p.prev_n[path] = make_float4(geo_n.x, geo_n.y, geo_n.z, 0.f);
                     T        = (1.f / smp.pdf) * (T * smp.reflection);
                     bsdf_pdf = smp.pdf;
                     singular = smp.specular;
@@ -1070,9 +1214,10 @@ struct Renderer::Device {
     float4*            positions  = nullptr;
     float4*            normals    = nullptr;
     shading::Material* materials  = nullptr;
-    float*             tri_light_pdf = nullptr;
-    float4*            lights     = nullptr;
-    float*             light_cdf  = nullptr;
+    float4*            light_nodes = nullptr;
+    float4*            light_cones = nullptr;
+    float4*            light_tris  = nullptr;
+    uint32_t*          light_order = nullptr;
     float*             e_table    = nullptr;
     Medium_gpu*        media      = nullptr;
     std::vector<float*>  grid_density;  // one per density grid
@@ -1210,9 +1355,10 @@ Renderer::~Renderer() {
     free_ptr(d_->positions);
     free_ptr(d_->normals);
     free_ptr(d_->materials);
-    free_ptr(d_->tri_light_pdf);
-    free_ptr(d_->lights);
-    free_ptr(d_->light_cdf);
+    free_ptr(d_->light_nodes);
+    free_ptr(d_->light_cones);
+    free_ptr(d_->light_tris);
+    free_ptr(d_->light_order);
     free_ptr(d_->e_table);
     free_grids();
     Paths& p = d_->paths;
@@ -1229,6 +1375,7 @@ Renderer::~Renderer() {
     free_ptr(p.sh_o);
     free_ptr(p.sh_d);
     free_ptr(p.sh_L);
+    free_ptr(p.prev_n);
     free_ptr(d_->queue[0]);
     free_ptr(d_->queue[1]);
     free_ptr(d_->shadow_queue);
@@ -1302,69 +1449,46 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
                              0.f);
     }
 
-    // Lights: every triangle of a light prop whose material emits, picked in proportion to
-    // its power (area * mean radiance).
-    std::vector<uint32_t> light_ids;
-    std::vector<double>   power;
-    std::vector<double>   area;
+    // Lights: every triangle of a light prop whose material emits, in a light tree.
+    std::vector<Light_input> emitters;
     for (uint32_t t = 0; t < nt; ++t) {
         shading::Material const& m = scene.materials[scene.tri_material[t]];
         if (!scene.tri_light[t] || m.type != shading::Type_light) {
             continue;
         }
-        float const* a = &scene.positions[3 * scene.indices[3 * t]];
-        float const* b = &scene.positions[3 * scene.indices[3 * t + 1]];
-        float const* c = &scene.positions[3 * scene.indices[3 * t + 2]];
-        double const e1[3] = {double(b[0]) - a[0], double(b[1]) - a[1], double(b[2]) - a[2]};
-        double const e2[3] = {double(c[0]) - a[0], double(c[1]) - a[1], double(c[2]) - a[2]};
-        double const cx = e1[1] * e2[2] - e1[2] * e2[1];
-        double const cy = e1[2] * e2[0] - e1[0] * e2[2];
-        double const cz = e1[0] * e2[1] - e1[1] * e2[0];
-        double const ar = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
-        double const pw = ar * (double(m.emission.x) + m.emission.y + m.emission.z) / 3.0;
-        if (ar > 0.0 && pw > 0.0) {
-            light_ids.push_back(t);
-            power.push_back(pw);
-            area.push_back(ar);
+        Light_input li;
+        for (int k = 0; k < 3; ++k) {
+            li.a[k] = scene.positions[3 * scene.indices[3 * t] + k];
+            li.b[k] = scene.positions[3 * scene.indices[3 * t + 1] + k];
+            li.c[k] = scene.positions[3 * scene.indices[3 * t + 2] + k];
+        }
+        double const e1[3] = {li.b[0] - li.a[0], li.b[1] - li.a[1], li.b[2] - li.a[2]};
+        double const e2[3] = {li.c[0] - li.a[0], li.c[1] - li.a[1], li.c[2] - li.a[2]};
+        double const cx    = e1[1] * e2[2] - e1[2] * e2[1];
+        double const cy    = e1[2] * e2[0] - e1[0] * e2[2];
+        double const cz    = e1[0] * e2[1] - e1[1] * e2[0];
+        double const area  = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+        li.two_sided       = m.two_sided != 0;
+        li.power = area * (double(m.emission.x) + m.emission.y + m.emission.z) / 3.0 *
+                   (li.two_sided ? 2.0 : 1.0);
+        li.tri = t;
+        if (area > 0.0 && li.power > 0.0) {
+            emitters.push_back(li);
         }
     }
-    double total = 0.0;
-    for (double pw : power) {
-        total += pw;
-    }
-    std::vector<float>  cdf(light_ids.size() + 1, 0.f);
-    std::vector<float4> lights(3 * light_ids.size());
-    std::vector<float>  tri_pdf(nt, 0.f);
-    double run = 0.0;
-    for (size_t l = 0; l < light_ids.size(); ++l) {
-        uint32_t const t    = light_ids[l];
-        double const   pick = power[l] / total;
-        float const*   a    = &scene.positions[3 * scene.indices[3 * t]];
-        float const*   b    = &scene.positions[3 * scene.indices[3 * t + 1]];
-        float const*   c    = &scene.positions[3 * scene.indices[3 * t + 2]];
-        lights[3 * l + 0]   = make_float4(a[0], a[1], a[2], float(area[l]));
-        lights[3 * l + 1]   = make_float4(b[0] - a[0], b[1] - a[1], b[2] - a[2], float(pick));
-        float4 e2           = make_float4(c[0] - a[0], c[1] - a[1], c[2] - a[2], 0.f);
-        uint32_t tid        = t;
-        std::memcpy(&e2.w, &tid, 4);
-        lights[3 * l + 2]   = e2;
-        run += pick;
-        cdf[l + 1] = float(run);
-        tri_pdf[t] = float(pick / area[l]);
-    }
-    if (!light_ids.empty()) {
-        cdf.back() = 1.f;
-    }
-    d_->num_lights = uint32_t(light_ids.size());
+    Light_tree tree;
+    build_light_tree(emitters, nt, tree);
+    d_->num_lights = tree.num_lights;
 
     SPB_RCUDA(upload(d_->tri_info, info.data(), info.size() * sizeof(uint4)));
     SPB_RCUDA(upload(d_->positions, pos.data(), pos.size() * sizeof(float4)));
     SPB_RCUDA(upload(d_->normals, nrm.data(), nrm.size() * sizeof(float4)));
     SPB_RCUDA(upload(d_->materials, scene.materials.data(),
                      scene.materials.size() * sizeof(shading::Material)));
-    SPB_RCUDA(upload(d_->tri_light_pdf, tri_pdf.data(), tri_pdf.size() * sizeof(float)));
-    SPB_RCUDA(upload(d_->lights, lights.data(), lights.size() * sizeof(float4)));
-    SPB_RCUDA(upload(d_->light_cdf, cdf.data(), cdf.size() * sizeof(float)));
+    SPB_RCUDA(upload(d_->light_nodes, tree.nodes.data(), tree.nodes.size() * sizeof(float)));
+    SPB_RCUDA(upload(d_->light_cones, tree.cones.data(), tree.cones.size() * sizeof(float)));
+    SPB_RCUDA(upload(d_->light_tris, tree.tris.data(), tree.tris.size() * sizeof(float)));
+    SPB_RCUDA(upload(d_->light_order, tree.order.data(), tree.order.size() * sizeof(uint32_t)));
     SPB_RCUDA(upload(d_->e_table, ggx_albedo_table(),
                      Ggx_table_size * Ggx_table_size * sizeof(float)));
 
@@ -1458,6 +1582,7 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     free_ptr(p.sh_o);
     free_ptr(p.sh_d);
     free_ptr(p.sh_L);
+    free_ptr(p.prev_n);
     free_ptr(d_->queue[0]);
     free_ptr(d_->queue[1]);
     free_ptr(d_->shadow_queue);
@@ -1476,6 +1601,7 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     SPB_RCUDA(cudaMalloc(&p.sh_o, n * sizeof(float4)));
     SPB_RCUDA(cudaMalloc(&p.sh_d, n * sizeof(float4)));
     SPB_RCUDA(cudaMalloc(&p.sh_L, n * sizeof(float4)));
+    SPB_RCUDA(cudaMalloc(&p.prev_n, n * sizeof(float4)));
     SPB_RCUDA(cudaMalloc(&d_->queue[0], n * sizeof(uint32_t)));
     SPB_RCUDA(cudaMalloc(&d_->queue[1], n * sizeof(uint32_t)));
     SPB_RCUDA(cudaMalloc(&d_->shadow_queue, n * sizeof(uint32_t)));
@@ -1528,9 +1654,10 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     sg.positions     = d_->positions;
     sg.normals       = d_->normals;
     sg.materials     = d_->materials;
-    sg.tri_light_pdf = d_->tri_light_pdf;
-    sg.lights        = d_->lights;
-    sg.light_cdf     = d_->light_cdf;
+    sg.light_nodes   = d_->light_nodes;
+    sg.light_cones   = d_->light_cones;
+    sg.light_tris    = d_->light_tris;
+    sg.light_order   = d_->light_order;
     sg.num_lights    = d_->num_lights;
     sg.e_table       = d_->e_table;
     sg.media         = d_->media;

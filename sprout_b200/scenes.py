@@ -110,6 +110,47 @@ def grid_box_transformation(angle_degrees: float = 30.0, scale: float = 0.7,
     return m
 
 
+def light_panel(n: int = 8, seed: int = 5, extent: float = 0.6, height: float = 1.98):
+    """An n x n grid of small one-sided emitting quads under the ceiling (one mesh, one part per
+    quad), plus two two-sided vertical quads near the side walls.  Returns (positions, normals,
+    indices, parts, emissions): parts are (first index, index count, material slot) triples and
+    emissions[k] the sRGB radiance of slot k -- log-uniform in [1, 40] times a random tint.
+    Quad sizes, offsets, heights and tilts are jittered.  (The reference's light-tree builder
+    recurses without end on many emitters with identical normals, so every quad is tilted.)"""
+    rng = np.random.default_rng(seed)
+    cell = 2.0 * extent / n
+    pos, nrm, idx, parts = [], [], [], []
+    for j in range(n):
+        for i in range(n):
+            cx = -extent + (i + 0.5 + rng.uniform(-0.15, 0.15)) * cell
+            cz = -extent + (j + 0.5 + rng.uniform(-0.15, 0.15)) * cell
+            hx, hz = rng.uniform(0.2, 0.33, 2) * cell
+            y = height - rng.uniform(0.0, 0.05)
+            sx, sz = rng.uniform(-0.3, 0.3, 2)  # slopes
+            corners = [(cx + u * hx, y + sx * u * hx + sz * v * hz, cz + v * hz)
+                       for u, v in ((-1, -1), (1, -1), (1, 1), (-1, 1))]
+            g = np.cross(np.subtract(corners[1], corners[0]), np.subtract(corners[2], corners[0]))
+            g = g / np.linalg.norm(g)
+            qp, qn, qi = _quad(*corners, g if g[1] < 0 else -g)
+            parts.append((3 * 2 * len(pos), 6, len(pos)))
+            idx.append(qi + 4 * len(pos))
+            pos.append(qp)
+            nrm.append(qn)
+    for x, z in ((-0.85, -0.07), (0.83, 0.11)):
+        qp, qn, qi = _quad((x, 0.6, z - 0.2), (x, 0.6, z + 0.2), (x, 1.03, z + 0.2), (x, 1.03, z - 0.2),
+                           (1, 0, 0))
+        parts.append((3 * 2 * len(pos), 6, len(pos)))
+        idx.append(qi + 4 * len(pos))
+        pos.append(qp)
+        nrm.append(qn)
+    k = len(pos)
+    radiance = np.exp(rng.uniform(np.log(1.0), np.log(40.0), k))
+    tint = rng.uniform(0.5, 1.0, (k, 3))
+    emissions = (radiance[:, None] * tint).astype(np.float32)
+    return (np.concatenate(pos), np.concatenate(nrm), np.concatenate(idx),
+            np.array(parts, np.uint32), emissions)
+
+
 def cornell_geometry(sphere_subdivisions: int = 6):
     """name -> (positions, normals, indices) in world space (y up, box x, z in [-1, 1], y in [0, 2])."""
     g = {}
@@ -137,13 +178,15 @@ def translation(x, y, z):
 
 def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounces: int = 8,
             min_bounces: int = 4, fov_degrees: float = 40.0, camera_position=(0.0, 1.0, -3.4),
-            spp: int = 64, tonemap: bool = False, medium=None, density=None):
+            spp: int = 64, tonemap: bool = False, medium=None, density=None, many_lights=False):
     """Issues the scene's su_* calls on an initialised engine; returns the camera entity.
 
     medium: optional dict of Volumetric material parameters (e.g. color, attenuation_distance,
     anisotropy); the sphere then becomes a homogeneous participating medium instead of metal.
     density: optional (nz, ny, nx) float array; with medium, the sphere is replaced by the
     cube of grid_box_transformation() filled with this density grid.
+    many_lights: the ceiling light is replaced by light_panel(): 66 emitters of different
+    radiance, two of them two-sided (a light-tree test).
     """
     cam = su.su_create_camera_perspective(width, height, math.radians(fov_degrees))
     su.set_transformation(cam, translation(*camera_position))
@@ -166,6 +209,8 @@ def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounc
     light = _material(su, "Light", emission=[17.0, 17.0, 17.0])
 
     geo = cornell_geometry(sphere_subdivisions)
+    if many_lights:
+        del geo["light"]
     trafo = {}
     if density is not None:
         geo["sphere"] = box()
@@ -179,6 +224,15 @@ def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounc
         su.set_transformation(prop, trafo.get(name, np.eye(4, dtype=np.float32)))
         if name == "light":
             su.su_create_light(prop)
+    if many_lights:
+        pos, nrm, idx, parts, emissions = light_panel()
+        slots = []
+        for k, e in enumerate(emissions):
+            two_sided = k >= len(emissions) - 2
+            slots.append(_material(su, "Light", emission=[float(x) for x in e], two_sided=two_sided))
+        prop = su.prop(su.mesh(pos, nrm, idx, parts=parts), slots)
+        su.set_transformation(prop, np.eye(4, dtype=np.float32))
+        su.su_create_light(prop)
     return cam
 
 

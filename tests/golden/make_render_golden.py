@@ -42,6 +42,8 @@ CASES = {
                                              "max_bounces": 1, "min_bounces": 1}, None),
     "cornell64_grid": (64, 64, 4096, {"sphere_subdivisions": 2, "medium": GRID_MEDIUM},
                        scenes.density_grid()),
+    # 66 emitters of different radiance and orientation, two of them two-sided (light tree)
+    "cornell64_lights": (64, 64, 4096, {"sphere_subdivisions": 3, "many_lights": True}, None),
 }
 PATH = HERE / "cornell_reference.npz"
 

@@ -51,7 +51,8 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
         su.su_release()
 
 
-CASES = ["cornell64_sub3", "cornell128_sub6", "cornell64_medium", "cornell64_thin_direct", "cornell64_grid"]
+CASES = ["cornell64_sub3", "cornell128_sub6", "cornell64_medium", "cornell64_thin_direct", "cornell64_grid",
+         "cornell64_lights"]
 
 
 @pytest.mark.parametrize("name", CASES)
