@@ -1,12 +1,18 @@
-"""Path-tracer measurement: the Cornell scene (sprout_b200.scenes.cornell) rendered through the
-su_* C API, timed on the device.
+"""Path-tracer measurement through the su_* C API, timed on the device.  Two workloads:
 
-    python -m sprout_b200.render_bench [--size 512] [--spp 64] [--frames 3] [--convergence]
+* cornell: the Cornell scene (sprout_b200.scenes.cornell), 512x512, 64 spp, max depth 8;
+* wavefront: 400 instances of a 5,000-triangle displaced sphere (2,000,000 triangles) lit by
+  4,096 emissive triangles through the light tree (sprout_b200.scenes.wavefront), 1920x1080,
+  256 spp, max depth 12.
+
+    python -m sprout_b200.render_bench [--scene cornell] [--width 512] [--height 512] [--spp 64]
+                                       [--frames 3] [--convergence] [--cpu-reference]
 
 Prints one JSON object: samples/s and rays/s (closest-hit + shadow) per frame, the end-to-end
 frame rate seen by the caller (render + postprocess + framebuffer copy to host), optionally
 the sample count and device time to reach relMSE 0.01 against a 4096-spp image of this
-renderer, and optionally the reference renderer's time for the same frame on the host cores.
+renderer, and optionally the reference renderer's rate on the host cores (the whole frame for
+cornell; a 480x270, 32-spp frame of the same scene for wavefront).
 """
 
 from __future__ import annotations
@@ -22,8 +28,17 @@ import numpy as np
 
 from . import _lib, capi, scenes
 
-CONFIG = ("Cornell box (5 walls, 0.25 m^2 light of radiance 17, 81,920-tri GGX conductor sphere alpha 0.3), "
-          "PTMIS max depth 8 (Russian roulette from depth 4)")
+SCENES = {
+    "cornell": ("Cornell box (5 walls, 0.25 m^2 light of radiance 17, 81,920-tri GGX conductor sphere alpha 0.3), "
+                "PTMIS max depth 8 (Russian roulette from depth 4)",
+                lambda su, w, h, spp: scenes.cornell(su, w, h, sphere_subdivisions=6, tonemap=True, spp=spp),
+                (512, 512, 64), None),
+    "wavefront": ("400 instances of a 5,000-tri displaced sphere (2,000,000 tris, Substitute roughness U[0.05,1], "
+                  "metallic Bernoulli(0.3)), 4,096 emissive tris of log-uniform radiance [0.1, 100] via the light "
+                  "tree, PTMIS max depth 12 (Russian roulette from depth 4)",
+                  lambda su, w, h, spp: scenes.wavefront(su, w, h, spp),
+                  (1920, 1080, 256), (480, 270, 32)),
+}
 
 
 def rel_mse(x, r):
@@ -31,27 +46,32 @@ def rel_mse(x, r):
     return float(np.mean((x - r) ** 2 / (r * r + 1e-2)))
 
 
-def measure(size=512, spp=64, frames=3, convergence=False, cpu_reference=False):
+def measure(scene="cornell", width=None, height=None, spp=None, frames=3, convergence=False,
+            cpu_reference=False):
+    config, build, (w0, h0, spp0), cpu_frame = SCENES[scene]
+    width, height, spp = width or w0, height or h0, spp or spp0
     lib = _lib.load()
     stats = _lib.RenderStats()
     su = capi.SuLibrary()
-    out = {"config": f"{CONFIG}, {size}x{size}, {spp} spp"}
+    out = {"workload": scene, "config": f"{config}, {width}x{height}, {spp} spp"}
     assert su.su_init(False) == 0
     try:
-        scenes.cornell(su, size, size, sphere_subdivisions=6, tonemap=True, spp=spp)
+        build(su, width, height, spp)
+        t0 = time.perf_counter()
         assert su.su_render_frame(0) == 0, su.messages  # scene upload + BVH build + warm-up
+        out["first_frame_s"] = round(time.perf_counter() - t0, 3)
         dev, wall = [], []
         for _ in range(frames):
             t0 = time.perf_counter()
             assert su.su_render_frame(0) == 0
             assert su.su_postprocess() == 0
-            su.framebuffer(size, size)
+            su.framebuffer(width, height)
             wall.append(time.perf_counter() - t0)
             assert lib.spb_render_last_stats(ctypes.byref(stats)) == 0
             dev.append(stats.device_seconds)
         dev_s = statistics.median(dev)
         rays = stats.extension_rays + stats.shadow_rays
-        samples = size * size * spp
+        samples = width * height * spp
         out.update({"msamples_s": round(samples / dev_s / 1e6, 3), "mrays_s": round(rays / dev_s / 1e6, 3),
                     "ms_per_frame": round(1e3 * dev_s, 3), "rays_per_sample": round(rays / samples, 3),
                     "e2e_msamples_s": round(samples / statistics.median(wall) / 1e6, 3),
@@ -59,13 +79,13 @@ def measure(size=512, spp=64, frames=3, convergence=False, cpu_reference=False):
         if convergence:
             assert su.su_create_sampler(4096) == 0
             assert su.su_render_frame(0) == 0 and su.su_postprocess() == 0
-            ref = su.framebuffer(size, size)[0][:, :, :3].copy()
+            ref = su.framebuffer(width, height)[0][:, :, :3].copy()
             k, reached = 1, None
             while k <= 1024:
                 assert su.su_create_sampler(k) == 0
                 assert su.su_render_frame(0) == 0 and su.su_postprocess() == 0
                 lib.spb_render_last_stats(ctypes.byref(stats))
-                e = rel_mse(su.framebuffer(size, size)[0][:, :, :3], ref)
+                e = rel_mse(su.framebuffer(width, height)[0][:, :, :3], ref)
                 if e <= 0.01:
                     reached = {"spp": k, "device_seconds": round(stats.device_seconds, 5), "rel_mse": round(e, 5)}
                     break
@@ -79,25 +99,28 @@ def measure(size=512, spp=64, frames=3, convergence=False, cpu_reference=False):
         import oracle  # test/baseline infrastructure: times the reference renderer
 
         if oracle.REF_RENDER.exists():
-            _, timing = oracle.reference_render(
-                lambda r: scenes.cornell(r, size, size, sphere_subdivisions=6, tonemap=True, spp=spp),
-                size, size, 0, progressive=False)
-            out["cpu_baseline"] = {"msamples_s": round(size * size * spp / timing["render_s"] / 1e6, 4),
+            cw, ch, cspp = cpu_frame or (width, height, spp)
+            _, timing = oracle.reference_render(lambda r: build(r, cw, ch, cspp), cw, ch, 0, progressive=False)
+            what = "full frame" if cpu_frame is None else f"{cw}x{ch}, {cspp} spp frame of the same scene"
+            out["cpu_baseline"] = {"msamples_s": round(cw * ch * cspp / timing["render_s"] / 1e6, 4),
                                    "seconds": round(timing["render_s"], 3), "cores": os.cpu_count(),
                                    "kind": "reference",
-                                   "sample": "full frame, the reference's su_render_frame (batch) on all host threads"}
+                                   "sample": f"{what}, the reference's su_render_frame (batch, scene build "
+                                             "included) on all host threads"}
     return out
 
 
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("--size", type=int, default=512)
-    p.add_argument("--spp", type=int, default=64)
+    p.add_argument("--scene", choices=sorted(SCENES), default="cornell")
+    p.add_argument("--width", type=int)
+    p.add_argument("--height", type=int)
+    p.add_argument("--spp", type=int)
     p.add_argument("--frames", type=int, default=3)
     p.add_argument("--convergence", action="store_true")
     p.add_argument("--cpu-reference", action="store_true")
     a = p.parse_args()
-    print(json.dumps(measure(a.size, a.spp, a.frames, a.convergence, a.cpu_reference)))
+    print(json.dumps(measure(a.scene, a.width, a.height, a.spp, a.frames, a.convergence, a.cpu_reference)))
 
 
 if __name__ == "__main__":

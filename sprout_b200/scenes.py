@@ -249,3 +249,145 @@ def render_progressive(su, width: int, height: int, iterations: int, **scene):
         return img[:, :, :3].copy()
     finally:
         su.su_release()
+
+
+# ---- many instances and many lights: the 1920x1080 wavefront workload ----
+
+def value_noise(p, seed: int):
+    """Smooth 3-D value noise in [-1, 1] at points p (n, 3): hashed lattice values, quintic
+    fade, trilinear blend."""
+    p = np.asarray(p, np.float64)
+    i = np.floor(p).astype(np.int64)
+    f = p - i
+    u = f * f * f * (f * (f * 6.0 - 15.0) + 10.0)
+
+    def lattice(ix, iy, iz):
+        h = (ix * 73856093) ^ (iy * 19349663) ^ (iz * 83492791) ^ (seed * 2654435761)
+        h = (h ^ (h >> 13)) * 1274126177
+        h = h ^ (h >> 16)
+        return (h & 0xFFFF).astype(np.float64) / 32767.5 - 1.0
+
+    out = 0.0
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                w = (np.where(dx, u[:, 0], 1 - u[:, 0]) * np.where(dy, u[:, 1], 1 - u[:, 1]) *
+                     np.where(dz, u[:, 2], 1 - u[:, 2]))
+                out = out + w * lattice(i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz)
+    return out
+
+
+def displaced_sphere(segments: int = 50, rings: int = 51, amplitude: float = 0.1, octaves: int = 6,
+                     seed: int = 2):
+    """Unit UV sphere of 2 * segments * (rings - 2) + 2 * segments triangles (5,000 with the
+    defaults), radius 1 + amplitude * fBm (lacunarity 2, gain 0.5); smooth vertex normals."""
+    theta = np.pi * np.arange(1, rings) / rings
+    phi = 2.0 * np.pi * np.arange(segments) / segments
+    st, ct = np.sin(theta), np.cos(theta)
+    ring = np.stack([np.outer(st, np.cos(phi)), np.repeat(ct[:, None], segments, 1),
+                     np.outer(st, np.sin(phi))], -1).reshape(-1, 3)
+    v = np.concatenate([[[0.0, 1.0, 0.0]], ring, [[0.0, -1.0, 0.0]]])
+    fbm, amp, freq = np.zeros(len(v)), 1.0, 2.0
+    for o in range(octaves):
+        fbm += amp * value_noise(v * freq, seed + o)
+        amp, freq = amp * 0.5, freq * 2.0
+    v = v * (1.0 + amplitude * fbm)[:, None]
+    faces = []
+    top, bottom = 0, len(v) - 1
+    for s in range(segments):
+        s1 = (s + 1) % segments
+        faces.append((top, 1 + s1, 1 + s))
+        for r in range(rings - 2):
+            a, b = 1 + r * segments + s, 1 + r * segments + s1
+            c, d = a + segments, b + segments
+            faces += [(a, b, d), (a, d, c)]
+        last = 1 + (rings - 2) * segments
+        faces.append((bottom, last + s, last + s1))
+    f = np.array(faces, np.uint32)
+    fn = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]])
+    if np.mean(np.einsum("ij,ij->i", fn, v[f[:, 0]])) < 0:  # wind outwards
+        f = f[:, ::-1].copy()
+        fn = -fn
+    n = np.zeros_like(v)
+    for k in range(3):
+        np.add.at(n, f[:, k], fn)
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    return v.astype(np.float32), n.astype(np.float32), f
+
+
+def _rotation(rng):
+    """Uniformly random rotation matrix (3x3, rows are the rotated axes)."""
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    w, x, y, z = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y + w * z), 2 * (x * z - w * y)],
+                     [2 * (x * y - w * z), 1 - 2 * (x * x + z * z), 2 * (y * z + w * x)],
+                     [2 * (x * z + w * y), 2 * (y * z - w * x), 1 - 2 * (x * x + y * y)]])
+
+
+def emitter_cloud(count: int = 4096, seed: int = 2, size: float = 0.25):
+    """count small emissive triangles above the instances, facing roughly down with random
+    tilt (one mesh, one part per triangle).  Returns (positions, normals, indices, parts,
+    radiance): the brightest channel log-uniform in [0.1, 100], the others a random tint of it."""
+    rng = np.random.default_rng(seed + 1000)
+    centre = np.stack([rng.uniform(-12, 12, count), rng.uniform(6.0, 9.0, count),
+                       rng.uniform(-12, 12, count)], 1)
+    pos = np.zeros((count, 3, 3))
+    for k in range(3):
+        a = 2.0 * np.pi * (k / 3.0) + rng.uniform(-0.3, 0.3, count)
+        pos[:, k] = centre + size * np.stack([np.cos(a), rng.uniform(-0.4, 0.4, count), np.sin(a)], 1)
+    g = np.cross(pos[:, 1] - pos[:, 0], pos[:, 2] - pos[:, 0])
+    flip = g[:, 1] > 0  # face down
+    pos[flip] = pos[flip][:, ::-1]
+    g[flip] = -g[flip]
+    g /= np.linalg.norm(g, axis=1, keepdims=True)
+    idx = np.arange(3 * count, dtype=np.uint32).reshape(count, 3)
+    parts = np.stack([3 * np.arange(count), np.full(count, 3), np.arange(count)], 1).astype(np.uint32)
+    radiance = np.exp(rng.uniform(np.log(0.1), np.log(100.0), count))
+    tint = rng.uniform(0.6, 1.0, (count, 3))
+    tint /= tint.max(axis=1, keepdims=True)
+    return (pos.reshape(-1, 3).astype(np.float32), np.repeat(g, 3, 0).astype(np.float32), idx, parts,
+            (radiance[:, None] * tint).astype(np.float32))
+
+
+def wavefront(su, width: int = 1920, height: int = 1080, spp: int = 256, max_bounces: int = 12,
+              min_bounces: int = 4, instances: int = 400, emitters: int = 4096, seed: int = 2,
+              tonemap: bool = True):
+    """The many-instances, many-lights scene: a ground plane; `instances` randomly placed,
+    scaled and rotated copies of one 5,000-triangle displaced sphere (props sharing a mesh, so
+    2,000,000 triangles for 400), each with a random Substitute material (roughness U[0.05, 1],
+    metallic Bernoulli(0.3), colour U[0, 1]^3); `emitters` emissive triangles with their own
+    Light materials; PTMIS, max depth 12; a pinhole camera with a 60 degree field of view."""
+    rng = np.random.default_rng(seed)
+    cam = su.su_create_camera_perspective(width, height, math.radians(60.0))
+    m = np.eye(4, dtype=np.float32)
+    # rows: camera x, y, z axes in world space; pitched down by 0.25 rad
+    m[1, 1], m[1, 2], m[2, 1], m[2, 2] = math.cos(0.25), math.sin(0.25), -math.sin(0.25), math.cos(0.25)
+    m[3, :3] = (0.0, 6.0, -17.0)
+    su.set_transformation(cam, m)
+    su.su_create_integrators(json.dumps({"surface": {"PTMIS": {"min_bounces": min_bounces,
+                                                              "max_bounces": max_bounces}}}).encode())
+    su.su_create_sampler(spp)
+    if tonemap:
+        su.su_create_defaults()
+    ground = _material(su, "Substitute", color=[0.6, 0.6, 0.6], roughness=0.9, metallic=0.0)
+    pos, nrm, idx = _quad((-30, 0, -30), (30, 0, -30), (30, 0, 30), (-30, 0, 30), (0, 1, 0))
+    prop = su.prop(su.mesh(pos, nrm, idx), [ground])
+    su.set_transformation(prop, np.eye(4, dtype=np.float32))
+    v, n, f = displaced_sphere(seed=seed)
+    sphere = su.mesh(v, n, f)
+    for _ in range(instances):
+        mat = _material(su, "Substitute", color=[float(c) for c in rng.uniform(0.0, 1.0, 3)],
+                        roughness=float(rng.uniform(0.05, 1.0)), metallic=float(rng.random() < 0.3))
+        t = np.eye(4, dtype=np.float32)
+        t[:3, :3] = float(rng.uniform(0.3, 1.0)) * _rotation(rng)
+        t[3, :3] = (rng.uniform(-11, 11), rng.uniform(1.0, 4.5), rng.uniform(-11, 11))
+        prop = su.prop(sphere, [mat])
+        su.set_transformation(prop, t)
+    if emitters:
+        pos, nrm, idx, parts, radiance = emitter_cloud(emitters, seed)
+        slots = [_material(su, "Light", emission=[float(x) for x in e]) for e in radiance]
+        prop = su.prop(su.mesh(pos, nrm, idx, parts=parts), slots)
+        su.set_transformation(prop, np.eye(4, dtype=np.float32))
+        su.su_create_light(prop)
+    return cam

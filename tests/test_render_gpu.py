@@ -3,7 +3,8 @@ the reference renderer's converged images of the same scene (tests/golden/cornel
 made by the reference's own C API).
 
 Monte Carlo images agree only in expectation, so the checks are statistical: the image means
-per channel within 0.5%, 8x8-pixel block means within 2% (plus a small absolute floor), and
+per channel within 0.5%, 8x8-pixel block means within 2% (16x16 for the many-emitter scene,
+whose reference image is noisier; plus a small absolute floor), and
 the relative MSE of the whole image (mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2))
 below a bound that the reference's own noise at its sample count dominates.  One case replaces
 the metal sphere by a homogeneous scattering medium (Volumetric material: delta tracking,
@@ -36,7 +37,10 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
     su = capi.SuLibrary()
     assert su.su_init(progressive) == 0
     try:
-        scenes.cornell(su, width, height, tonemap=True, spp=spp, **scene)
+        if scene.get("scene") == "wavefront":
+            scenes.wavefront(su, width, height, spp)
+        else:
+            scenes.cornell(su, width, height, tonemap=True, spp=spp, **scene)
         if progressive:
             assert su.su_start_render_frame(0) == 0, su.messages
             for _ in range(iterations):
@@ -52,7 +56,7 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
 
 
 CASES = ["cornell64_sub3", "cornell128_sub6", "cornell64_medium", "cornell64_thin_direct", "cornell64_grid",
-         "cornell64_lights"]
+         "cornell64_lights", "wavefront96"]
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -66,9 +70,10 @@ def test_converged_image_matches_reference(name):
     m_ref = ref.mean(axis=(0, 1))
     m_img = img.mean(axis=(0, 1))
     assert np.all(np.abs(m_img - m_ref) <= 0.005 * m_ref), (m_img, m_ref)
-    bi, br = block_means(img, 8), block_means(ref, 8)
+    b = meta.get("block", 8)  # larger where the reference image is noisier (see the generator)
+    bi, br = block_means(img, b), block_means(ref, b)
     worst = np.max(np.abs(bi - br) / (np.abs(br) + 0.01))
-    assert worst < 0.02, f"worst 8x8 block deviation {worst:.4f}"
+    assert worst < 0.02, f"worst {b}x{b} block deviation {worst:.4f}"
     assert rel_mse(img, ref) < 2e-3
 
 
