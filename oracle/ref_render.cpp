@@ -19,7 +19,7 @@
 //       created before it, which the recorded material JSON refers to)
 //     mesh <num_triangles> <num_vertices> <byte offset of positions> <of normals> <of indices>
 //          [<num parts> <byte offset of the parts: (first index, index count, material slot)>]
-//     prop <mesh handle> <num materials> <material handles...>
+//     prop <mesh handle or built-in shape id (< 8)> <num materials> <material handles...>
 //     light <prop handle>
 //     progressive <iterations>
 //     frame <frame>
@@ -132,7 +132,9 @@ int main(int argc, char** argv) {
                 p += k;
                 mats[i] = handles[h];
             }
-            handles[3000 + n_prop++] = su_create_prop(handles[mesh], nm, mats.data());
+            // ids below 8 are the built-in shapes (sprout.h:22-29), passed as they are
+            uint32_t const shape = mesh < 8 ? mesh : handles[mesh];
+            handles[3000 + n_prop++] = su_create_prop(shape, nm, mats.data());
         } else if (c == "light") {
             uint32_t h = 0;
             std::sscanf(rest, "%u", &h);

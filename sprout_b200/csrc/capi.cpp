@@ -5,10 +5,13 @@
 // one world-space triangle set (the props' transformations applied to their meshes), build the
 // 8-wide BVH and upload the scene; iterations then run entirely on the GPU (render.cu).
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/sprout.h"
@@ -24,6 +27,11 @@ using spb::shading::V3;
 
 constexpr uint32_t Null          = 0xFFFFFFFFu;
 constexpr uint32_t First_mesh_id = 8;  // ids 0..7 are the built-in shapes (sprout.h:22-29)
+constexpr uint32_t Shape_cube            = 1;
+constexpr uint32_t Shape_disk            = 2;
+constexpr uint32_t Shape_infinite_sphere = 4;
+constexpr uint32_t Shape_rectangle       = 6;
+constexpr uint32_t Shape_sphere          = 7;
 
 struct Mesh {
     std::vector<float>    positions;  // 3 per vertex
@@ -60,6 +68,7 @@ struct Engine {
 
     bool                  progressive;
     std::vector<Mesh>     meshes;
+    Mesh                  builtin[First_mesh_id];  // tessellated built-in shapes, made on first use
     std::vector<Material> materials;
     std::vector<Grid_ref> material_grids;  // parallel to materials
     std::vector<Image>    images;
@@ -117,6 +126,111 @@ bool read_color(spb::json::Value const* v, V3& out) {
         return read_color(v->find("value"), out);
     }
     return false;
+}
+
+// The reference's analytic unit shapes as triangle meshes, so that one traversal serves every
+// prop: Rectangle [-1, 1]^2 at z = 0 facing +z (rectangle.cpp:25-64), Disk of radius 1 facing
+// +z (disk.cpp), Cube [-1, 1]^3 (cube.cpp), Sphere of radius 1 (sphere.cpp).  The disk (256
+// segments) and the sphere (icosphere, 20,480 triangles, smooth normals) are scaled to the
+// exact areas, so emitters built from them carry the analytic shape's power.
+Mesh make_builtin(uint32_t shape) {
+    Mesh m;
+    auto vertex = [&m](double x, double y, double z, double nx, double ny, double nz) {
+        m.positions.insert(m.positions.end(), {float(x), float(y), float(z)});
+        m.normals.insert(m.normals.end(), {float(nx), float(ny), float(nz)});
+        return uint32_t(m.positions.size() / 3 - 1);
+    };
+    if (shape == Shape_rectangle) {
+        for (auto [x, y] : {std::pair{-1, -1}, {1, -1}, {1, 1}, {-1, 1}}) {
+            vertex(x, y, 0, 0, 0, 1);
+        }
+        m.indices = {0, 1, 2, 0, 2, 3};
+    } else if (shape == Shape_disk) {
+        int const    n = 256;
+        double const r = std::sqrt(3.14159265358979323846 /
+                                   (0.5 * n * std::sin(2.0 * 3.14159265358979323846 / n)));
+        vertex(0, 0, 0, 0, 0, 1);
+        for (int i = 0; i < n; ++i) {
+            double const a = 2.0 * 3.14159265358979323846 * i / n;
+            vertex(r * std::cos(a), r * std::sin(a), 0, 0, 0, 1);
+        }
+        for (uint32_t i = 0; i < uint32_t(n); ++i) {
+            m.indices.insert(m.indices.end(), {0u, 1 + i, 1 + (i + 1) % n});
+        }
+    } else if (shape == Shape_cube) {
+        for (int axis = 0; axis < 3; ++axis) {
+            for (int sign = -1; sign <= 1; sign += 2) {
+                int const u = (axis + 1) % 3, v = (axis + 2) % 3;
+                uint32_t  base = uint32_t(m.positions.size() / 3);
+                for (auto [a, b] : {std::pair{-1, -1}, {1, -1}, {1, 1}, {-1, 1}}) {
+                    double p[3], nn[3] = {0, 0, 0};
+                    p[axis]  = sign;
+                    p[u]     = a;
+                    p[v]     = b;
+                    nn[axis] = sign;
+                    vertex(p[0], p[1], p[2], nn[0], nn[1], nn[2]);
+                }
+                // (u, v, axis) is right-handed: counter-clockwise in (u, v) faces +axis
+                if (sign > 0) {
+                    m.indices.insert(m.indices.end(), {base, base + 1, base + 2, base, base + 2, base + 3});
+                } else {
+                    m.indices.insert(m.indices.end(), {base, base + 2, base + 1, base, base + 3, base + 2});
+                }
+            }
+        }
+    } else if (shape == Shape_sphere) {
+        double const t = (1.0 + std::sqrt(5.0)) / 2.0;
+        std::vector<std::array<double, 3>> v = {{-1, t, 0}, {1, t, 0}, {-1, -t, 0}, {1, -t, 0},
+                                                {0, -1, t}, {0, 1, t}, {0, -1, -t}, {0, 1, -t},
+                                                {t, 0, -1}, {t, 0, 1}, {-t, 0, -1}, {-t, 0, 1}};
+        std::vector<std::array<uint32_t, 3>> f = {
+            {0, 11, 5}, {0, 5, 1},  {0, 1, 7},   {0, 7, 10}, {0, 10, 11}, {1, 5, 9}, {5, 11, 4},
+            {11, 10, 2}, {10, 7, 6}, {7, 1, 8},  {3, 9, 4},  {3, 4, 2},   {3, 2, 6}, {3, 6, 8},
+            {3, 8, 9},  {4, 9, 5},  {2, 4, 11}, {6, 2, 10}, {8, 6, 7},   {9, 8, 1}};
+        auto unit = [](std::array<double, 3> a) {
+            double const l = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+            return std::array<double, 3>{a[0] / l, a[1] / l, a[2] / l};
+        };
+        for (auto& p : v) {
+            p = unit(p);
+        }
+        for (int level = 0; level < 5; ++level) {
+            std::map<std::pair<uint32_t, uint32_t>, uint32_t> mid;
+            auto middle = [&](uint32_t a, uint32_t b) {
+                auto const key = std::minmax(a, b);
+                auto const it  = mid.find(key);
+                if (it != mid.end()) {
+                    return it->second;
+                }
+                v.push_back(unit({v[a][0] + v[b][0], v[a][1] + v[b][1], v[a][2] + v[b][2]}));
+                return mid[key] = uint32_t(v.size() - 1);
+            };
+            std::vector<std::array<uint32_t, 3>> nf;
+            for (auto const& [a, b, c] : f) {
+                uint32_t const ab = middle(a, b), bc = middle(b, c), ca = middle(c, a);
+                nf.insert(nf.end(), {{a, ab, ca}, {b, bc, ab}, {c, ca, bc}, {ab, bc, ca}});
+            }
+            f.swap(nf);
+        }
+        double area = 0.0;
+        for (auto const& [a, b, c] : f) {
+            double const e1[3] = {v[b][0] - v[a][0], v[b][1] - v[a][1], v[b][2] - v[a][2]};
+            double const e2[3] = {v[c][0] - v[a][0], v[c][1] - v[a][1], v[c][2] - v[a][2]};
+            double const x = e1[1] * e2[2] - e1[2] * e2[1], y = e1[2] * e2[0] - e1[0] * e2[2],
+                         z = e1[0] * e2[1] - e1[1] * e2[0];
+            area += 0.5 * std::sqrt(x * x + y * y + z * z);
+        }
+        double const s = std::sqrt(4.0 * 3.14159265358979323846 / area);
+        for (auto const& p : v) {
+            vertex(s * p[0], s * p[1], s * p[2], p[0], p[1], p[2]);
+        }
+        for (auto const& [a, b, c] : f) {
+            m.indices.insert(m.indices.end(), {a, b, c});
+        }
+    }
+    m.part_of.assign(m.indices.size() / 3, 0);
+    m.part_slot = {0};
+    return m;
 }
 
 bool ready() {
@@ -203,7 +317,22 @@ int32_t compile_scene() {
         if (e.camera || e.shape == Null) {
             continue;
         }
-        Mesh const&    mesh = engine->meshes[e.shape - First_mesh_id];
+        if (e.shape == Shape_infinite_sphere) {
+            // Uniform environment (Infinite_sphere with a Light material, infinite_sphere.cpp):
+            // seen by rays that leave the scene; a light only after su_create_light.
+            uint32_t const mat = e.materials.empty() ? Null : e.materials[0];
+            if (mat < engine->materials.size() &&
+                engine->materials[mat].type == spb::shading::Type_light) {
+                V3 const em = engine->materials[mat].emission;
+                scene.environment[0] += em.x;
+                scene.environment[1] += em.y;
+                scene.environment[2] += em.z;
+                scene.environment_light |= e.light;
+            }
+            continue;
+        }
+        Mesh const& mesh =
+            e.shape < First_mesh_id ? engine->builtin[e.shape] : engine->meshes[e.shape - First_mesh_id];
         uint32_t const base = uint32_t(scene.positions.size() / 3);
         float const*   m    = e.trafo;
         float          rot[9];
@@ -718,8 +847,15 @@ SU_LIBRARY_API uint32_t su_create_prop(uint32_t shape, uint32_t num_materials,
     if (!engine) {
         return Null;
     }
-    if (shape < First_mesh_id || shape - First_mesh_id >= engine->meshes.size()) {
-        log(SU_LOG_ERROR, "su_create_prop: only triangle meshes are supported by this renderer");
+    bool const builtin = shape == Shape_cube || shape == Shape_disk || shape == Shape_rectangle ||
+                         shape == Shape_sphere;
+    if (builtin && engine->builtin[shape].indices.empty()) {
+        engine->builtin[shape] = make_builtin(shape);
+    }
+    if (!builtin && shape != Shape_infinite_sphere &&
+        (shape < First_mesh_id || shape - First_mesh_id >= engine->meshes.size())) {
+        log(SU_LOG_ERROR, "su_create_prop: shape not supported by this renderer (triangle meshes, "
+                          "Cube, Disk, Rectangle, Sphere and Infinite_sphere are)");
         return Null;
     }
     Entity e;

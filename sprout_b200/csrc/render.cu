@@ -85,6 +85,7 @@ struct Scene_gpu {
     float4 const*             light_tris;   // 3 per light in tree order: (a, area), e1, (e2, tri)
     uint32_t const*           light_order;  // per triangle: tree order, 0xFFFFFFFF if no light
     uint32_t                  num_lights;
+    float4                    env;  // uniform environment radiance; w: its pick probability in NEE
     float const*              e_table;
     Medium_gpu const*         media;  // Material::medium - 1 indexes this
 };
@@ -485,8 +486,27 @@ struct Light_sample {
 
 __device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, V3 n, bool total_sphere,
                                              float r, float r1, float r2, Light_sample& ls) {
+    if (r < s.env.w) {
+        // The environment: uniform directions over the hemisphere of n, or over the sphere at a
+        // medium vertex (Infinite_sphere::sample, infinite_sphere.cpp:68-101).
+        float const z   = total_sphere ? 1.f - 2.f * r1 : r1;
+        float const rad = sqrtf(fmaxf(0.f, 1.f - z * z));
+        float       sp, cp;
+        sincosf(2.f * shading::Pi * r2, &sp, &cp);
+        shading::Frame const f = shading::make_frame(n);
+        ls.dir      = (rad * cp) * f.t + (rad * sp) * f.b + z * f.n;
+        ls.dist     = Ray_max_t;
+        ls.pdf      = s.env.w * (total_sphere ? 1.f / (4.f * shading::Pi) : 1.f / (2.f * shading::Pi));
+        ls.radiance = v3(s.env.x, s.env.y, s.env.z);
+        return true;
+    }
+    if (s.num_lights == 0) {
+        return false;
+    }
+    r = fminf((r - s.env.w) / (1.f - s.env.w), 0x1.fffffep-1f);
     float          pick;
     uint32_t const l = pick_light(s, ps, n, total_sphere, r, pick);
+    pick *= 1.f - s.env.w;
     if (!(pick > 0.f)) {
         return false;
     }
@@ -860,6 +880,19 @@ __global__ void __launch_bounds__(Shade_block)
         bool  scatter = false;
         float t_sc    = 0.f;
         if (id == gpu::Miss) {
+            // Leaving the scene: the uniform environment (an Infinite_sphere prop).  The camera
+            // sees it; continuation rays only when it is a light, weighted against its NEE pdf
+            // from the previous vertex (connect_light, pathtracer_mis.cpp:349-380).
+            if (medium == 0 && (vtx == 0 || s.env.w > 0.f)) {
+                float w = 1.f;
+                if (vtx > 0 && !singular) {
+                    float4 const pn    = p.prev_n[path];
+                    float const  pdf_e = s.env.w * (pn.w != 0.f ? 1.f / (4.f * shading::Pi)
+                                                                : 1.f / (2.f * shading::Pi));
+                    w = power_heuristic(bsdf_pdf, pdf_e);
+                }
+                L = L + w * (T * v3(s.env.x, s.env.y, s.env.z));
+            }
             done = true;
         } else if (medium != 0) {
             shading::Material const m = s.materials[medium - 1];
@@ -894,7 +927,7 @@ __global__ void __launch_bounds__(Shade_block)
                 float const g   = shading::van_de_hulst_anisotropy(m.g, depth);
                 V3 const    pos = v3(ro.x + t_sc * rd.x, ro.y + t_sc * rd.y, ro.z + t_sc * rd.z);
                 V3 const    wo  = -dir_in;
-                if (s.num_lights > 0) {
+                if (s.num_lights > 0 || s.env.w > 0.f) {
                     float const  r  = rng.uniform();
                     float const  r1 = rng.uniform();
                     float const  r2 = rng.uniform();
@@ -947,14 +980,16 @@ __global__ void __launch_bounds__(Shade_block)
                 // Emission reached by the BSDF sample (connect_light, pathtracer_mis.cpp:349-380).
                 if (emits) {
                     if (front || mat.two_sided) {
-                        float w = 1.f;
+                        // only emitters registered as lights (su_create_light) are reached by
+                        // a continuation ray; others are seen from the camera only
                         uint32_t const order = s.light_order[id];
+                        float          w     = order != 0xFFFFFFFFu ? 1.f : 0.f;
                         if (!singular && order != 0xFFFFFFFFu) {
                             // the light-tree pick from the previous vertex (connect_light,
                             // pathtracer_mis.cpp:349-380)
                             float4 const pn    = p.prev_n[path];
-                            float const  pick  = light_pick_pdf(s, f3v(ro), f3v(pn), pn.w != 0.f,
-                                                                order);
+                            float const  pick  = (1.f - s.env.w) *
+                                                light_pick_pdf(s, f3v(ro), f3v(pn), pn.w != 0.f, order);
                             float const  t     = p.hit_t[path];
                             float const  area  = s.light_tris[3 * order].w;
                             float const  pdf_l = pick * (t * t) / (fabsf(cos_o) * area);
@@ -1003,7 +1038,7 @@ __global__ void __launch_bounds__(Shade_block)
                 ctx.wo    = wo;
 
                 // Next-event estimation (sample_lights / evaluate_light, pathtracer_mis.cpp:281-347).
-                if (s.num_lights > 0) {
+                if (s.num_lights > 0 || s.env.w > 0.f) {
                     float const  r  = rng.uniform();
                     float const  r1 = rng.uniform();
                     float const  r2 = rng.uniform();
@@ -1223,6 +1258,7 @@ struct Renderer::Device {
     std::vector<float*>  grid_density;  // one per density grid
     std::vector<float2*> grid_cells;
     uint32_t           num_lights = 0;
+    float4             env        = {0.f, 0.f, 0.f, 0.f};
     float              hit_margin = 0.f;
     // paths
     uint32_t  capacity = 0;
@@ -1480,6 +1516,32 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     build_light_tree(emitters, nt, tree);
     d_->num_lights = tree.num_lights;
 
+    // The environment's share of light picks: its power against the emitters', with the
+    // reference's power of an infinite light, squared scene extent x 4 pi x mean radiance
+    // (Light::power, light.cpp:38-48; Tree_builder, light_tree_builder.cpp:527-537).
+    float const* env = scene.environment;
+    d_->env          = make_float4(env[0], env[1], env[2], 0.f);
+    if (scene.environment_light && (env[0] > 0.f || env[1] > 0.f || env[2] > 0.f)) {
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (uint32_t v = 0; v < nv; ++v) {
+            for (int k = 0; k < 3; ++k) {
+                lo[k] = std::min(lo[k], double(scene.positions[3 * v + k]));
+                hi[k] = std::max(hi[k], double(scene.positions[3 * v + k]));
+            }
+        }
+        double ext2 = 0.0;
+        for (int k = 0; k < 3; ++k) {
+            ext2 += (hi[k] - lo[k]) * (hi[k] - lo[k]);
+        }
+        double const p_env = ext2 * 4.0 * 3.14159265358979323846 *
+                             (double(env[0]) + env[1] + env[2]) / 3.0;
+        double p_finite = 0.0;
+        for (Light_input const& li : emitters) {
+            p_finite += li.power;
+        }
+        d_->env.w = float(p_env / (p_env + p_finite));
+    }
+
     SPB_RCUDA(upload(d_->tri_info, info.data(), info.size() * sizeof(uint4)));
     SPB_RCUDA(upload(d_->positions, pos.data(), pos.size() * sizeof(float4)));
     SPB_RCUDA(upload(d_->normals, nrm.data(), nrm.size() * sizeof(float4)));
@@ -1659,6 +1721,7 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     sg.light_tris    = d_->light_tris;
     sg.light_order   = d_->light_order;
     sg.num_lights    = d_->num_lights;
+    sg.env           = d_->env;
     sg.e_table       = d_->e_table;
     sg.media         = d_->media;
 

@@ -35,6 +35,8 @@ struct Scene_desc {
     std::vector<shading::Material>  materials;    // Volume materials: medium = 1 + grid medium
     std::vector<Density_grid>       grids;
     std::vector<Grid_medium>        media;
+    float                           environment[3] = {0.f, 0.f, 0.f};  // uniform radiance at infinity
+    bool                            environment_light = false;  // also sampled by next-event estimation
 };
 
 struct Camera_desc {

@@ -46,6 +46,10 @@ CASES = {
     "cornell64_lights": (64, 64, 4096, {"sphere_subdivisions": 3, "many_lights": True}, None),
     # 400 instanced displaced spheres (rotated, scaled props sharing one mesh), 4,096 emitters
     "wavefront96": (96, 54, 2048, {"scene": "wavefront"}, None),
+    # Disk, Sphere, Cube and Rectangle built-in shapes under an Infinite_sphere light
+    "builtins96": (96, 72, 4096, {"scene": "builtins"}, None),
+    # the same with the environment seen by the camera only (not a light)
+    "builtins96_backdrop": (96, 72, 4096, {"scene": "builtins", "environment_light": False}, None),
 }
 PATH = HERE / "cornell_reference.npz"
 # Block size of the block-mean comparison where 8 is too small: many small, bright emitters
@@ -55,10 +59,15 @@ BLOCK = {"wavefront96": 16}
 
 
 def build(su, w, h, spp, kwargs, density=None):
-    """Issues a case's scene calls: scenes.wavefront for {"scene": "wavefront"}, else
+    """Issues a case's scene calls: {"scene": "wavefront"} -> scenes.wavefront,
+    {"scene": "builtins", ...} -> scenes.builtin_shapes with the other keys, else
     scenes.cornell with the keyword arguments."""
-    if kwargs.get("scene") == "wavefront":
-        return scenes.wavefront(su, w, h, spp)
+    kwargs = dict(kwargs)
+    name = kwargs.pop("scene", "cornell")
+    if name == "wavefront":
+        return scenes.wavefront(su, w, h, spp, **kwargs)
+    if name == "builtins":
+        return scenes.builtin_shapes(su, w, h, spp, **kwargs)
     return scenes.cornell(su, w, h, tonemap=True, spp=spp, density=density, **kwargs)
 
 

@@ -170,3 +170,23 @@ def test_synthetic_rays():
     assert np.array_equal(part, rays[500:600])
     # directions are isotropic: mean close to zero
     assert np.abs(rays[:, 4:7].mean(axis=0)).max() < 0.01
+
+
+def test_builtin_shapes_accepted():
+    """Cube, Disk, Infinite_sphere, Rectangle and Sphere props are created by shape id; Canopy,
+    Distant_sphere and Plane are not supported and return SU_RESOURCE_NULL."""
+    import numpy as np
+
+    from sprout_b200 import capi
+
+    su = capi.SuLibrary()
+    assert su.su_init(False) == 0
+    try:
+        mat = su.su_create_material(b'{"rendering": {"Light": {"emission": [1, 1, 1]}}}')
+        ids = np.array([mat], np.uint32)
+        for shape in (1, 2, 4, 6, 7):
+            assert su.su_create_prop(shape, 1, ids.ctypes.data) != capi.SU_RESOURCE_NULL, shape
+        for shape in (0, 3, 5):
+            assert su.su_create_prop(shape, 1, ids.ctypes.data) == capi.SU_RESOURCE_NULL, shape
+    finally:
+        assert su.su_release() == 0

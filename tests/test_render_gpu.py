@@ -37,8 +37,12 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
     su = capi.SuLibrary()
     assert su.su_init(progressive) == 0
     try:
-        if scene.get("scene") == "wavefront":
-            scenes.wavefront(su, width, height, spp)
+        scene = dict(scene)
+        name = scene.pop("scene", "cornell")
+        if name == "wavefront":
+            scenes.wavefront(su, width, height, spp, **scene)
+        elif name == "builtins":
+            scenes.builtin_shapes(su, width, height, spp, **scene)
         else:
             scenes.cornell(su, width, height, tonemap=True, spp=spp, **scene)
         if progressive:
@@ -56,7 +60,7 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
 
 
 CASES = ["cornell64_sub3", "cornell128_sub6", "cornell64_medium", "cornell64_thin_direct", "cornell64_grid",
-         "cornell64_lights", "wavefront96"]
+         "cornell64_lights", "wavefront96", "builtins96", "builtins96_backdrop"]
 
 
 @pytest.mark.parametrize("name", CASES)
