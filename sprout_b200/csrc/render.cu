@@ -105,7 +105,17 @@ struct Paths {
     float4*   sh_d;
     float4*   sh_L;
     float4*   prev_n;  // geometric normal at the last scattering vertex; w 1: medium vertex
+    // Second shadow ray of a vertex whose light selection is split (the environment and one
+    // emitter, see Split_bounces); its contributions accumulate in L2 (added to L by gather),
+    // so that no two kernel threads ever add to the same radiance.
+    float4*   sh2_o;
+    float4*   sh2_d;
+    float4*   sh2_L;
+    float4*   L2;
 };
+
+// Shadow-queue entries are path indices; this bit marks the vertex's second shadow ray.
+constexpr uint32_t Second_shadow = 0x80000000u;
 
 struct Cam {
     float3   left_top;
@@ -241,6 +251,7 @@ __global__ void k_generate(Cam cam, Wave wave, Paths p, uint32_t* queue, uint32_
     p.ray_d[i] = make_float4(w.x, w.y, w.z, Ray_max_t);
     p.T[i]     = make_float4(1.f, 1.f, 1.f, 0.f);
     p.L[i]     = make_float4(0.f, 0.f, 0.f, 0.f);
+    p.L2[i]    = make_float4(0.f, 0.f, 0.f, 0.f);
     p.puv[i]   = make_float2(u, v);
     p.rng[i]   = rng.save();
     p.info[i]  = 1u << 16;  // vertex 0, depth 0, treat as singular
@@ -288,7 +299,10 @@ __global__ void __launch_bounds__(Trace_block)
                 if (mine < num) {
                     path = queue[mine];
                     if (Any_hit) {
-                        gpu::start_ray(r, tv, p.sh_o[path], p.sh_d[path]);
+                        uint32_t const pi     = path & ~Second_shadow;
+                        bool const     second = path & Second_shadow;
+                        gpu::start_ray(r, tv, second ? p.sh2_o[pi] : p.sh_o[pi],
+                                       second ? p.sh2_d[pi] : p.sh_d[pi]);
                     } else {
                         gpu::start_ray(r, tv, p.ray_o[path], p.ray_d[path]);
                     }
@@ -306,12 +320,14 @@ __global__ void __launch_bounds__(Trace_block)
                     if (Media) {
                         transmit_queue[atomicAdd(transmit_count, 1u)] = path;
                     } else {
-                        float4 const c = p.sh_L[path];
-                        float4       l = p.L[path];
+                        uint32_t const pi = path & ~Second_shadow;
+                        float4* const  Lp = (path & Second_shadow) ? p.L2 : p.L;
+                        float4 const   c  = (path & Second_shadow) ? p.sh2_L[pi] : p.sh_L[pi];
+                        float4         l  = Lp[pi];
                         l.x += c.x;
                         l.y += c.y;
                         l.z += c.z;
-                        p.L[path] = l;
+                        Lp[pi] = l;
                     }
                 }
             } else {
@@ -484,9 +500,29 @@ struct Light_sample {
     V3    radiance;
 };
 
+// Light selection is split at the first Split_bounces vertices, as with the reference's
+// Adaptive light sampling (Pathtracer_MIS::splitting, pathtracer_mis.cpp:419-422;
+// Tree::random_light / pdf, light_tree.cpp:363-470, 564-640): there every infinite light is
+// sampled with probability 1 besides one emitter picked by the tree (so a vertex may send two
+// shadow rays).  The reference decides this from the depth at the vertex for next-event
+// estimation but from the depth after the bounce when it weighs the light hit (connect_light
+// runs after ++ray.depth), and this renderer does the same so that images agree.  The
+// reference's splitting of the emitter tree itself (several emitters per vertex) is not
+// mirrored: one emitter is picked.
+constexpr uint32_t Split_bounces = 3;  // Pathtracer_MIS::Num_dedicated_samplers
+
+// Which lights a sample may come from.
+enum Light_mode : int {
+    Any_light   = 0,  // the environment with probability env.w, else an emitter from the tree
+    Environment = 1,  // the environment, probability 1
+    Emitters    = 2,  // an emitter from the tree, probability 1 for the tree
+};
+
 __device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, V3 n, bool total_sphere,
-                                             float r, float r1, float r2, Light_sample& ls) {
-    if (r < s.env.w) {
+                                             float r, float r1, float r2, Light_sample& ls,
+                                             int mode = Any_light) {
+    float const env_p = mode == Any_light ? s.env.w : (mode == Environment ? 1.f : 0.f);
+    if (r < env_p) {
         // The environment: uniform directions over the hemisphere of n, or over the sphere at a
         // medium vertex (Infinite_sphere::sample, infinite_sphere.cpp:68-101).
         float const z   = total_sphere ? 1.f - 2.f * r1 : r1;
@@ -496,17 +532,17 @@ __device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, V3 n, bo
         shading::Frame const f = shading::make_frame(n);
         ls.dir      = (rad * cp) * f.t + (rad * sp) * f.b + z * f.n;
         ls.dist     = Ray_max_t;
-        ls.pdf      = s.env.w * (total_sphere ? 1.f / (4.f * shading::Pi) : 1.f / (2.f * shading::Pi));
+        ls.pdf      = env_p * (total_sphere ? 1.f / (4.f * shading::Pi) : 1.f / (2.f * shading::Pi));
         ls.radiance = v3(s.env.x, s.env.y, s.env.z);
         return true;
     }
     if (s.num_lights == 0) {
         return false;
     }
-    r = fminf((r - s.env.w) / (1.f - s.env.w), 0x1.fffffep-1f);
+    r = fminf((r - env_p) / (1.f - env_p), 0x1.fffffep-1f);
     float          pick;
     uint32_t const l = pick_light(s, ps, n, total_sphere, r, pick);
-    pick *= 1.f - s.env.w;
+    pick *= 1.f - env_p;
     if (!(pick > 0.f)) {
         return false;
     }
@@ -842,6 +878,44 @@ __device__ bool transmit_grid(Medium_gpu const& g, shading::Material const& m, f
     return !blocked;
 }
 
+// Light samples at a vertex of the given depth: two (the environment, and an emitter) where
+// the selection is split and both kinds of light exist, else one (0 without lights).
+__device__ __forceinline__ int num_light_samples(Scene_gpu const& s, uint32_t depth) {
+    if (s.num_lights == 0 && !(s.env.w > 0.f)) {
+        return 0;
+    }
+    return depth < Split_bounces && s.env.w > 0.f && s.num_lights > 0 ? 2 : 1;
+}
+
+__device__ __forceinline__ int light_mode(int samples, int k) {
+    return samples == 1 ? Any_light : (k == 0 ? Environment : Emitters);
+}
+
+// Probability factor of the environment (or, with emitter = true, of the emitter tree) in the
+// light selection of the vertex whose continuation ray arrives with depth `depth`.
+__device__ __forceinline__ float selection_share(Scene_gpu const& s, uint32_t depth, bool emitter) {
+    if (depth < Split_bounces) {
+        return 1.f;
+    }
+    return emitter ? 1.f - s.env.w : s.env.w;
+}
+
+__device__ __forceinline__ void store_shadow(Paths const& p, uint32_t path, bool second, V3 o,
+                                             Light_sample const& ls, V3 contrib, uint32_t depth) {
+    float4 const ro = make_float4(o.x, o.y, o.z, 0.f);
+    float4 const rd = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
+    float4 const c  = make_float4(contrib.x, contrib.y, contrib.z, float(depth));
+    if (second) {
+        p.sh2_o[path] = ro;
+        p.sh2_d[path] = rd;
+        p.sh2_L[path] = c;
+    } else {
+        p.sh_o[path] = ro;
+        p.sh_d[path] = rd;
+        p.sh_L[path] = c;
+    }
+}
+
 // ---- shade: one path vertex ----
 __global__ void __launch_bounds__(Shade_block)
     k_shade(Scene_gpu s, Wave wave, Paths p, uint32_t const* __restrict__ q_in,
@@ -850,9 +924,10 @@ __global__ void __launch_bounds__(Shade_block)
     uint32_t const i   = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t const num = *count_in;
 
-    bool     extend = false;
-    bool     shadow = false;
-    uint32_t path   = 0;
+    bool     extend  = false;
+    bool     shadow  = false;
+    bool     shadow2 = false;  // the vertex's second light sample (split selection)
+    uint32_t path    = 0;
 
     if (i < num) {
         path              = q_in[i];
@@ -887,8 +962,9 @@ __global__ void __launch_bounds__(Shade_block)
                 float w = 1.f;
                 if (vtx > 0 && !singular) {
                     float4 const pn    = p.prev_n[path];
-                    float const  pdf_e = s.env.w * (pn.w != 0.f ? 1.f / (4.f * shading::Pi)
-                                                                : 1.f / (2.f * shading::Pi));
+                    float const  pdf_e = selection_share(s, depth, false) *
+                                         (pn.w != 0.f ? 1.f / (4.f * shading::Pi)
+                                                      : 1.f / (2.f * shading::Pi));
                     w = power_heuristic(bsdf_pdf, pdf_e);
                 }
                 L = L + w * (T * v3(s.env.x, s.env.y, s.env.z));
@@ -927,20 +1003,20 @@ __global__ void __launch_bounds__(Shade_block)
                 float const g   = shading::van_de_hulst_anisotropy(m.g, depth);
                 V3 const    pos = v3(ro.x + t_sc * rd.x, ro.y + t_sc * rd.y, ro.z + t_sc * rd.z);
                 V3 const    wo  = -dir_in;
-                if (s.num_lights > 0 || s.env.w > 0.f) {
+                int const samples = num_light_samples(s, depth);
+                for (int k = 0; k < samples; ++k) {
                     float const  r  = rng.uniform();
                     float const  r1 = rng.uniform();
                     float const  r2 = rng.uniform();
                     Light_sample ls;
-                    if (sample_light(s, pos, v3(0.f, 0.f, 1.f), true, r, r1, r2, ls)) {
+                    if (sample_light(s, pos, v3(0.f, 0.f, 1.f), true, r, r1, r2, ls,
+                                     light_mode(samples, k))) {
                         float const f = shading::phase_hg(shading::dot(wo, ls.dir), g);
                         float const w = ls.pdf / (ls.pdf * ls.pdf + f * f);
                         V3 const contrib = (w * f) * (T * ls.radiance);
                         if (shading::max_component(contrib) > 0.f) {
-                            p.sh_o[path] = make_float4(pos.x, pos.y, pos.z, 0.f);
-                            p.sh_d[path] = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
-                            p.sh_L[path] = make_float4(contrib.x, contrib.y, contrib.z, float(depth));
-                            shadow       = true;
+                            store_shadow(p, path, k == 1, pos, ls, contrib, depth);
+                            (k == 1 ? shadow2 : shadow) = true;
                         }
                     }
                 }
@@ -988,7 +1064,7 @@ __global__ void __launch_bounds__(Shade_block)
                             // the light-tree pick from the previous vertex (connect_light,
                             // pathtracer_mis.cpp:349-380)
                             float4 const pn    = p.prev_n[path];
-                            float const  pick  = (1.f - s.env.w) *
+                            float const  pick  = selection_share(s, depth, true) *
                                                 light_pick_pdf(s, f3v(ro), f3v(pn), pn.w != 0.f, order);
                             float const  t     = p.hit_t[path];
                             float const  area  = s.light_tris[3 * order].w;
@@ -1038,22 +1114,21 @@ __global__ void __launch_bounds__(Shade_block)
                 ctx.wo    = wo;
 
                 // Next-event estimation (sample_lights / evaluate_light, pathtracer_mis.cpp:281-347).
-                if (s.num_lights > 0 || s.env.w > 0.f) {
+                int const samples = num_light_samples(s, depth);
+                V3 const  ps      = offset_ray(pos, geo_n);
+                for (int k = 0; k < samples; ++k) {
                     float const  r  = rng.uniform();
                     float const  r1 = rng.uniform();
                     float const  r2 = rng.uniform();
-                    V3 const     ps = offset_ray(pos, geo_n);
                     Light_sample ls;
-                    if (sample_light(s, ps, geo_n, false, r, r1, r2, ls)) {
+                    if (sample_light(s, ps, geo_n, false, r, r1, r2, ls, light_mode(samples, k))) {
                         shading::Bxdf const f =
                             shading::substitute_evaluate(mat, s.e_table, ctx, ls.dir);
                         float const w = ls.pdf / (ls.pdf * ls.pdf + f.pdf * f.pdf);
                         V3 const contrib = w * (T * (ls.radiance * f.reflection));
                         if (shading::max_component(contrib) > 0.f) {
-                            p.sh_o[path] = make_float4(ps.x, ps.y, ps.z, 0.f);
-                            p.sh_d[path] = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
-                            p.sh_L[path] = make_float4(contrib.x, contrib.y, contrib.z, float(depth));
-                            shadow       = true;
+                            store_shadow(p, path, k == 1, ps, ls, contrib, depth);
+                            (k == 1 ? shadow2 : shadow) = true;
                         }
                     }
                 }
@@ -1093,6 +1168,10 @@ __global__ void __launch_bounds__(Shade_block)
     if (shadow) {
         sq[sslot] = path;
     }
+    uint32_t const sslot2 = append(count_shadow, shadow2);
+    if (shadow2) {
+        sq[sslot2] = path | Second_shadow;
+    }
 }
 
 // ---- shadow rays through media: Worker::transmittance (rendering_worker.cpp:209-267) ----
@@ -1107,16 +1186,18 @@ __global__ void __launch_bounds__(Trace_block)
     if (i >= *count) {
         return;
     }
-    uint32_t const path   = queue[i];
+    uint32_t const entry  = queue[i];
+    uint32_t const path   = entry & ~Second_shadow;
+    bool const     second = entry & Second_shadow;
     uint32_t       medium = p.info[path] >> 17;
-    float4 const   ro     = p.sh_o[path];
-    float4 const   rd     = p.sh_d[path];
-    float4 const   c      = p.sh_L[path];
+    float4 const   ro     = second ? p.sh2_o[path] : p.sh_o[path];
+    float4 const   rd     = second ? p.sh2_d[path] : p.sh_d[path];
+    float4 const   c      = second ? p.sh2_L[path] : p.sh_L[path];
     uint32_t const depth  = uint32_t(c.w);
     float          t0     = ro.w;
     V3             tau    = v3(0.f, 0.f, 0.f);
     V3             w      = v3(1.f, 1.f, 1.f);
-    bool           random = false;  // the path's random stream was used
+    bool           random = false;  // this shadow ray's random stream was started
     bool           blocked = false;
     Rng            rng;
     uint2          stack[gpu::Stack_size];
@@ -1133,7 +1214,10 @@ __global__ void __launch_bounds__(Trace_block)
             shading::Material const m = s.materials[medium - 1];
             if (m.medium != 0) {
                 if (!random) {
-                    rng.load(p.rng[path]);
+                    // A stream of its own, seeded from the path's state (which this kernel
+                    // only reads: a vertex's two shadow rays may be in flight together).
+                    uint4 const st = p.rng[path];
+                    rng.start((uint64_t(st.y) << 32) | st.x, (uint64_t(path) << 1) | (second ? 1u : 0u));
                     random = true;
                 }
                 float const srs = shading::similarity_relation_scale(m.g, depth);
@@ -1159,17 +1243,15 @@ __global__ void __launch_bounds__(Trace_block)
             break;
         }
     }
-    if (random) {
-        p.rng[path] = rng.save();
-    }
     if (blocked) {
         return;
     }
-    float4 l = p.L[path];
+    float4* const Lp = second ? p.L2 : p.L;
+    float4        l  = Lp[path];
     l.x += w.x * expf(-tau.x) * c.x;
     l.y += w.y * expf(-tau.y) * c.y;
     l.z += w.z * expf(-tau.z) * c.z;
-    p.L[path] = l;
+    Lp[path] = l;
 }
 
 // ---- film: Filtered_1p0::add_sample (sensor/filtered.inl:125-187) as a gather ----
@@ -1208,10 +1290,11 @@ __global__ void k_gather(Paths p, uint32_t w, uint32_t h, uint32_t samples, floa
                 float2 const   uv   = p.puv[path];
                 float const    wt   = filter_weight(uv.x - 0.5f - float(dx)) *
                                  filter_weight(uv.y - 0.5f - float(dy));
-                float4 const L = p.L[path];
-                acc.x += wt * L.x;
-                acc.y += wt * L.y;
-                acc.z += wt * L.z;
+                float4 const L  = p.L[path];
+                float4 const L2 = p.L2[path];
+                acc.x += wt * (L.x + L2.x);
+                acc.y += wt * (L.y + L2.y);
+                acc.z += wt * (L.z + L2.z);
                 acc.w += wt;
             }
         }
@@ -1412,6 +1495,10 @@ Renderer::~Renderer() {
     free_ptr(p.sh_d);
     free_ptr(p.sh_L);
     free_ptr(p.prev_n);
+    free_ptr(p.sh2_o);
+    free_ptr(p.sh2_d);
+    free_ptr(p.sh2_L);
+    free_ptr(p.L2);
     free_ptr(d_->queue[0]);
     free_ptr(d_->queue[1]);
     free_ptr(d_->shadow_queue);
@@ -1645,6 +1732,10 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     free_ptr(p.sh_d);
     free_ptr(p.sh_L);
     free_ptr(p.prev_n);
+    free_ptr(p.sh2_o);
+    free_ptr(p.sh2_d);
+    free_ptr(p.sh2_L);
+    free_ptr(p.L2);
     free_ptr(d_->queue[0]);
     free_ptr(d_->queue[1]);
     free_ptr(d_->shadow_queue);
@@ -1664,10 +1755,15 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     SPB_RCUDA(cudaMalloc(&p.sh_d, n * sizeof(float4)));
     SPB_RCUDA(cudaMalloc(&p.sh_L, n * sizeof(float4)));
     SPB_RCUDA(cudaMalloc(&p.prev_n, n * sizeof(float4)));
+    SPB_RCUDA(cudaMalloc(&p.sh2_o, n * sizeof(float4)));
+    SPB_RCUDA(cudaMalloc(&p.sh2_d, n * sizeof(float4)));
+    SPB_RCUDA(cudaMalloc(&p.sh2_L, n * sizeof(float4)));
+    SPB_RCUDA(cudaMalloc(&p.L2, n * sizeof(float4)));
     SPB_RCUDA(cudaMalloc(&d_->queue[0], n * sizeof(uint32_t)));
     SPB_RCUDA(cudaMalloc(&d_->queue[1], n * sizeof(uint32_t)));
-    SPB_RCUDA(cudaMalloc(&d_->shadow_queue, n * sizeof(uint32_t)));
-    SPB_RCUDA(cudaMalloc(&d_->transmit_queue, n * sizeof(uint32_t)));
+    // up to two shadow rays per path vertex (split light selection)
+    SPB_RCUDA(cudaMalloc(&d_->shadow_queue, 2 * n * sizeof(uint32_t)));
+    SPB_RCUDA(cudaMalloc(&d_->transmit_queue, 2 * n * sizeof(uint32_t)));
     if (!d_->counters) {
         SPB_RCUDA(cudaMalloc(&d_->counters, Counter_words * sizeof(uint32_t)));
     }
@@ -1767,7 +1863,7 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
                 k_trace<true, true><<<d_->trace_grid, Trace_block, 0, st>>>(
                     sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot,
                     d_->transmit_queue, c + 4);
-                k_transmit<<<(paths + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
+                k_transmit<<<(2 * paths + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
                     sg, d_->paths, d_->transmit_queue, c + 4, ctr + Overflow_slot);
             } else {
                 k_trace<true><<<d_->trace_grid, Trace_block, 0, st>>>(

@@ -408,11 +408,13 @@ def _trafo(scale, rows, position):
 
 
 def builtin_shapes(su, width: int = 64, height: int = 48, spp: int = 64, environment=(0.4, 0.5, 0.7),
-                   environment_light: bool = True, max_bounces: int = 8, min_bounces: int = 4):
+                   environment_light: bool = True, max_bounces: int = 8, min_bounces: int = 4,
+                   lamp: bool = True):
     """Built-in analytic shapes created by id (su_create_prop with SU_SHAPE_*): a Disk of
     radius 3 as the ground, a metal Sphere, a rotated Cube, a Rectangle light of 0.6 x 0.6
     facing down (radiance 20), and an Infinite_sphere of uniform radiance `environment` (a
-    light unless environment_light is False, then only seen by the camera)."""
+    light unless environment_light is False, then only seen by the camera).  lamp=False leaves
+    the Rectangle light out."""
     cam = su.su_create_camera_perspective(width, height, math.radians(45.0))
     m = np.eye(4, dtype=np.float32)
     m[1, 1], m[1, 2], m[2, 1], m[2, 2] = math.cos(0.25), math.sin(0.25), -math.sin(0.25), math.cos(0.25)
@@ -425,7 +427,7 @@ def builtin_shapes(su, width: int = 64, height: int = 48, spp: int = 64, environ
     ground = _material(su, "Substitute", color=[0.7, 0.7, 0.7], roughness=0.8, metallic=0.0)
     metal = _material(su, "Substitute", color=[0.9, 0.8, 0.5], roughness=0.4, metallic=1.0)
     red = _material(su, "Substitute", color=[0.8, 0.1, 0.1], roughness=0.6, metallic=0.0)
-    lamp = _material(su, "Light", emission=[20.0, 20.0, 20.0])
+    lamp_mat = _material(su, "Light", emission=[20.0, 20.0, 20.0])
     sky = _material(su, "Light", emission=[float(x) for x in environment])
     a = math.radians(30.0)
     props = [
@@ -433,9 +435,11 @@ def builtin_shapes(su, width: int = 64, height: int = 48, spp: int = 64, environ
         (SHAPE_SPHERE, metal, _trafo(0.5, np.eye(3), (-0.7, 0.5, 0.3)), False),
         (SHAPE_CUBE, red, _trafo(0.4, [[math.cos(a), 0, -math.sin(a)], [0, 1, 0], [math.sin(a), 0, math.cos(a)]],
                                  (0.8, 0.4, -0.1)), False),
-        (SHAPE_RECTANGLE, lamp, _trafo(0.3, [[1, 0, 0], [0, 0, 1], [0, -1, 0]], (0.0, 2.5, 0.0)), True),
+        (SHAPE_RECTANGLE, lamp_mat, _trafo(0.3, [[1, 0, 0], [0, 0, 1], [0, -1, 0]], (0.0, 2.5, 0.0)), True),
         (SHAPE_INFINITE_SPHERE, sky, np.eye(4, dtype=np.float32), environment_light),
     ]
+    if not lamp:
+        del props[3]
     for shape, mat, trafo, light in props:
         prop = su.prop(shape, [mat])
         su.set_transformation(prop, trafo)

@@ -39,12 +39,13 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
     try:
         scene = dict(scene)
         name = scene.pop("scene", "cornell")
+        density = scene.pop("density", None)  # Cornell cases only
         if name == "wavefront":
             scenes.wavefront(su, width, height, spp, **scene)
         elif name == "builtins":
             scenes.builtin_shapes(su, width, height, spp, **scene)
         else:
-            scenes.cornell(su, width, height, tonemap=True, spp=spp, **scene)
+            scenes.cornell(su, width, height, tonemap=True, spp=spp, density=density, **scene)
         if progressive:
             assert su.su_start_render_frame(0) == 0, su.messages
             for _ in range(iterations):
