@@ -1,9 +1,12 @@
-"""Path-tracer measurement through the su_* C API, timed on the device.  Two workloads:
+"""Path-tracer measurement through the su_* C API, timed on the device.  Three workloads:
 
 * cornell: the Cornell scene (sprout_b200.scenes.cornell), 512x512, 64 spp, max depth 8;
 * wavefront: 400 instances of a 5,000-triangle displaced sphere (2,000,000 triangles) lit by
   4,096 emissive triangles through the light tree (sprout_b200.scenes.wavefront), 1920x1080,
-  256 spp, max depth 12.
+  256 spp, max depth 12;
+* volume: a 2 m cube of 256^3 fBm density lit by a sphere light and the environment
+  (sprout_b200.scenes.volume), a few of 64 seeded views of 256..1024 px, 128 spp, max depth
+  32.
 
     python -m sprout_b200.render_bench [--scene cornell] [--width 512] [--height 512] [--spp 64]
                                        [--frames 3] [--convergence] [--cpu-reference]
@@ -110,9 +113,63 @@ def measure(scene="cornell", width=None, height=None, spp=None, frames=3, conver
     return out
 
 
+VOLUME_CONFIG = ("2 m cube of 256^3 fBm density (5 octaves, seed 4), mu_t 20 per metre at density 1, albedo 0.9, "
+                 "HG g 0.6, lit by a sphere light of radius 0.25 and a uniform environment; PTMIS max depth 32; "
+                 "RGB delta/ratio tracking (the reference's transport; no hero wavelengths)")
+
+
+def measure_volume(views=4, spp=128, cpu_reference=False):
+    """The heterogeneous-volume workload: the first `views` of scenes.volume_views() (seeded
+    camera positions, image sides U[256, 1024]), one frame each; samples/s over the device
+    time of all views."""
+    lib = _lib.load()
+    stats = _lib.RenderStats()
+    density = scenes.fbm_density(256)
+    chosen = scenes.volume_views()[:views]
+    samples, seconds, rays, wall = 0, 0.0, 0, 0.0
+    for position, side in chosen:
+        su = capi.SuLibrary()
+        assert su.su_init(False) == 0
+        try:
+            scenes.volume(su, side, side, spp, density, position=position)
+            t0 = time.perf_counter()
+            assert su.su_render_frame(0) == 0, su.messages
+            assert su.su_postprocess() == 0
+            su.framebuffer(side, side)
+            wall += time.perf_counter() - t0
+            assert lib.spb_render_last_stats(ctypes.byref(stats)) == 0
+            seconds += stats.device_seconds
+            samples += side * side * spp
+            rays += stats.extension_rays + stats.shadow_rays
+        finally:
+            su.su_release()
+    out = {"workload": "volume", "config": f"{VOLUME_CONFIG}, {views} of 64 views (sides "
+                                           f"{[v[1] for v in chosen]}), {spp} spp",
+           "msamples_s": round(samples / seconds / 1e6, 3), "mrays_s": round(rays / seconds / 1e6, 3),
+           "device_seconds": round(seconds, 3),
+           "e2e_msamples_s": round(samples / wall / 1e6, 3),
+           "e2e_note": "per view: su_render_frame (scene upload and BVH build included) + su_postprocess + "
+                       "su_copy_framebuffer to host, wall clock"}
+    if cpu_reference:
+        import oracle  # test/baseline infrastructure: times the reference renderer
+
+        if oracle.REF_RENDER.exists():
+            position, _ = chosen[0]
+            cw, cspp = 128, 8
+            _, timing = oracle.reference_render(
+                lambda r: scenes.volume(r, cw, cw, cspp, density, position=position), cw, cw, 0, progressive=False)
+            out["cpu_baseline"] = {"msamples_s": round(cw * cw * cspp / timing["render_s"] / 1e6, 4),
+                                   "seconds": round(timing["render_s"], 3), "cores": os.cpu_count(),
+                                   "kind": "reference",
+                                   "sample": f"first view at {cw}x{cw}, {cspp} spp, the reference's su_render_frame "
+                                             "(batch, scene and majorant-tree build included) on all host threads"}
+    return out
+
+
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("--scene", choices=sorted(SCENES), default="cornell")
+    p.add_argument("--scene", choices=sorted(SCENES) + ["volume"], default="cornell")
+    p.add_argument("--views", type=int, default=4, help="volume workload: number of views")
     p.add_argument("--width", type=int)
     p.add_argument("--height", type=int)
     p.add_argument("--spp", type=int)
@@ -120,7 +177,10 @@ def main():
     p.add_argument("--convergence", action="store_true")
     p.add_argument("--cpu-reference", action="store_true")
     a = p.parse_args()
-    print(json.dumps(measure(a.scene, a.width, a.height, a.spp, a.frames, a.convergence, a.cpu_reference)))
+    if a.scene == "volume":
+        print(json.dumps(measure_volume(a.views, a.spp or 128, a.cpu_reference)))
+    else:
+        print(json.dumps(measure(a.scene, a.width, a.height, a.spp, a.frames, a.convergence, a.cpu_reference)))
 
 
 if __name__ == "__main__":

@@ -446,3 +446,85 @@ def builtin_shapes(su, width: int = 64, height: int = 48, spp: int = 64, environ
         if light:
             su.su_create_light(prop)
     return cam
+
+
+# ---- a heterogeneous medium lit by a sphere light and the environment ----
+
+# Volumetric colours for the medium: attenuation colour 0.5 over 0.034657 m gives
+# mu_t = -ln(0.5) / 0.034657 = 20 per metre at density 1; subsurface colour 0.32297 gives a
+# single-scattering albedo of 0.9 at anisotropy 0.6 through the reference's scattering()
+# mapping (collision_coefficients.inl:50-71).
+VOLUME_MEDIUM = {"attenuation_color": [0.5, 0.5, 0.5], "attenuation_distance": 0.0346574,
+                 "subsurface_color": [0.322972, 0.322972, 0.322972], "anisotropy": 0.6}
+
+
+def fbm_density(n: int = 256, octaves: int = 5, seed: int = 4):
+    """(n, n, n) float32 density in [0, 1] with maximum exactly 1: fBm of seeded value noise
+    (random lattices of 4 * 2^o cells per axis, trilinearly upsampled; gain 0.5), shifted and
+    clipped so that about a fifth of the cube is empty."""
+    from scipy import ndimage
+
+    rng = np.random.default_rng(seed)
+    f = np.zeros((n, n, n), np.float32)
+    amp = 1.0
+    for o in range(octaves):
+        cells = 4 << o
+        lattice = rng.uniform(-1.0, 1.0, (cells + 1,) * 3).astype(np.float32)
+        f += amp * ndimage.zoom(lattice, n / (cells + 1), order=1, mode="nearest", grid_mode=True)[:n, :n, :n]
+        amp *= 0.5
+    f = (f - f.mean()) / f.std()
+    d = np.clip(0.5 + 0.4 * f, 0.0, None)
+    return (d / d.max()).astype(np.float32)
+
+
+def volume_views(count: int = 64, seed: int = 4):
+    """Seeded camera views of the medium: (position on a sphere of radius 5 around the
+    cube's centre, image side U[256, 1024] px)."""
+    rng = np.random.default_rng(seed + 100)
+    out = []
+    for _ in range(count):
+        z = rng.uniform(-0.3, 0.8)
+        phi = rng.uniform(0.0, 2.0 * np.pi)
+        r = math.sqrt(1.0 - z * z)
+        out.append(((5.0 * r * math.cos(phi), 5.0 * z, 5.0 * r * math.sin(phi)), int(rng.integers(256, 1025))))
+    return out
+
+
+def _look_at(position, target=(0.0, 0.0, 0.0)):
+    """Camera-to-world matrix (rows: camera x, y, z axes, then the position): z towards the
+    target, x horizontal (world up cross z), y = z cross x."""
+    p = np.asarray(position, np.float64)
+    zc = np.asarray(target, np.float64) - p
+    zc /= np.linalg.norm(zc)
+    xc = np.cross([0.0, 1.0, 0.0], zc)
+    xc /= np.linalg.norm(xc)
+    yc = np.cross(zc, xc)
+    m = np.eye(4, dtype=np.float32)
+    m[0, :3], m[1, :3], m[2, :3], m[3, :3] = xc, yc, zc, p
+    return m
+
+
+def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -3.2),
+           max_bounces: int = 32, min_bounces: int = 4, environment=(0.3, 0.35, 0.4)):
+    """A 2 m Cube (built-in, [-1, 1]^3) filled with a density grid (VOLUME_MEDIUM), lit by a
+    Sphere light of radius 0.25 (radiance 60) and a uniform Infinite_sphere environment; a
+    pinhole camera at `position` looking at the centre with a 40 degree field of view; PTMIS
+    with max depth 32."""
+    cam = su.su_create_camera_perspective(width, height, math.radians(40.0))
+    su.set_transformation(cam, _look_at(position))
+    su.su_create_integrators(json.dumps({"surface": {"PTMIS": {"min_bounces": min_bounces,
+                                                              "max_bounces": max_bounces}}}).encode())
+    su.su_create_sampler(spp)
+    su.su_create_defaults()
+    image = su.image(density)
+    medium = _material(su, "Volumetric", density={"id": int(image)}, **VOLUME_MEDIUM)
+    lamp = _material(su, "Light", emission=[60.0, 60.0, 60.0])
+    sky = _material(su, "Light", emission=[float(x) for x in environment])
+    for shape, mat, trafo in ((SHAPE_CUBE, medium, np.eye(4, dtype=np.float32)),
+                              (SHAPE_SPHERE, lamp, _trafo(0.25, np.eye(3), (1.8, 2.2, -1.6))),
+                              (SHAPE_INFINITE_SPHERE, sky, np.eye(4, dtype=np.float32))):
+        prop = su.prop(shape, [mat])
+        su.set_transformation(prop, trafo)
+        if mat != medium:
+            su.su_create_light(prop)
+    return cam

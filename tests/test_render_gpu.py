@@ -44,6 +44,8 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
             scenes.wavefront(su, width, height, spp, **scene)
         elif name == "builtins":
             scenes.builtin_shapes(su, width, height, spp, **scene)
+        elif name == "volume":
+            scenes.volume(su, width, height, spp, density, **scene)
         else:
             scenes.cornell(su, width, height, tonemap=True, spp=spp, density=density, **scene)
         if progressive:
@@ -61,7 +63,7 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
 
 
 CASES = ["cornell64_sub3", "cornell128_sub6", "cornell64_medium", "cornell64_thin_direct", "cornell64_grid",
-         "cornell64_lights", "wavefront96", "builtins96", "builtins96_backdrop"]
+         "cornell64_lights", "wavefront96", "builtins96", "builtins96_backdrop", "volume64"]
 
 
 @pytest.mark.parametrize("name", CASES)
