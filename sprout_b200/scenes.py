@@ -528,3 +528,85 @@ def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -
         if mat != medium:
             su.su_create_light(prop)
     return cam
+
+
+# ---- an interior lit through a doorway: the path-guiding workload ----
+
+def _box_mesh(lo, hi):
+    """Axis-aligned box from corner lo to corner hi, outward faces (12 triangles)."""
+    p, n, f = box()
+    lo, hi = np.asarray(lo, np.float32), np.asarray(hi, np.float32)
+    return (p + 0.5) * (hi - lo) + lo, n, f
+
+
+def doorway(su, width: int = 1280, height: int = 720, spp: int = 64, seed: int = 3, spheres: int = 96,
+            boxes: int = 160, sphere_subdivisions: int = 4, max_bounces: int = 8, min_bounces: int = 4,
+            environment: float = 5.0):
+    """A 6 x 6 x 3 m room (x, z in [-3, 3], y in [0, 3]) whose only opening is a 1 x 2 m doorway
+    in the wall z = 3, outside a uniform environment of radiance `environment` (an
+    Infinite_sphere light).  Inside: `spheres` icospheres (20 * 4^subdivisions triangles each:
+    491,520 with the defaults) and `boxes` boxes at seeded random places; 70 % of the objects
+    Lambertian-like (Substitute, roughness 1, metallic 0), 30 % GGX conductors with alpha
+    U[0.1, 0.6].  Walls, floor and ceiling are grey Substitute (roughness 1).  A pinhole camera
+    in the room's far corner looks towards the doorway with a 60 degree field of view."""
+    rng = np.random.default_rng(seed)
+    eye = np.array([-2.4, 1.5, -2.7])
+    cam = su.su_create_camera_perspective(width, height, math.radians(60.0))
+    su.set_transformation(cam, _look_at(eye, (0.6, 0.9, 2.0)))
+
+    def clear(c, r):
+        """Keeps objects off the camera and out of the doorway."""
+        return (np.linalg.norm(np.asarray(c) - eye) > r + 1.0 and
+                not (abs(c[0]) < 0.5 + r + 0.3 and c[2] > 2.0 - r))
+    su.su_create_integrators(json.dumps({"surface": {"PTMIS": {"min_bounces": min_bounces,
+                                                              "max_bounces": max_bounces}}}).encode())
+    su.su_create_sampler(spp)
+    su.su_create_defaults()
+    wall = _material(su, "Substitute", color=[0.7, 0.7, 0.7], roughness=1.0, metallic=0.0)
+
+    def add(pos, nrm, idx, mat):
+        prop = su.prop(su.mesh(pos, nrm, idx), [mat])
+        su.set_transformation(prop, np.eye(4, dtype=np.float32))
+
+    # Room shell: quads facing inwards; the wall z = 3 is split around the doorway.
+    quads = [((-3, 0, -3), (3, 0, -3), (3, 0, 3), (-3, 0, 3), (0, 1, 0)),      # floor
+             ((-3, 3, -3), (-3, 3, 3), (3, 3, 3), (3, 3, -3), (0, -1, 0)),     # ceiling
+             ((-3, 0, -3), (-3, 3, -3), (3, 3, -3), (3, 0, -3), (0, 0, 1)),    # wall z = -3
+             ((-3, 0, -3), (-3, 0, 3), (-3, 3, 3), (-3, 3, -3), (1, 0, 0)),    # wall x = -3
+             ((3, 0, -3), (3, 3, -3), (3, 3, 3), (3, 0, 3), (-1, 0, 0)),       # wall x = 3
+             ((-3, 0, 3), (-0.5, 0, 3), (-0.5, 3, 3), (-3, 3, 3), (0, 0, -1)),  # z = 3, left of door
+             ((0.5, 0, 3), (3, 0, 3), (3, 3, 3), (0.5, 3, 3), (0, 0, -1)),     # z = 3, right of door
+             ((-0.5, 2, 3), (0.5, 2, 3), (0.5, 3, 3), (-0.5, 3, 3), (0, 0, -1))]  # above the door
+    for q in quads:
+        add(*_quad(*q), wall)
+
+    def material():
+        if rng.random() < 0.7:
+            return _material(su, "Substitute", color=[float(c) for c in rng.uniform(0.2, 0.9, 3)],
+                             roughness=1.0, metallic=0.0)
+        alpha = rng.uniform(0.1, 0.6)
+        return _material(su, "Substitute", color=[float(c) for c in rng.uniform(0.5, 1.0, 3)],
+                         roughness=float(math.sqrt(alpha)), metallic=1.0)
+
+    v, f = icosphere(sphere_subdivisions)
+    placed = 0
+    while placed < spheres:
+        r = rng.uniform(0.08, 0.3)
+        c = (rng.uniform(-2.7, 2.7), rng.uniform(r, 2.6), rng.uniform(-2.7, 2.7))
+        if clear(c, r):
+            add(r * v + np.array(c, np.float32), v, f, material())
+            placed += 1
+    placed = 0
+    while placed < boxes:
+        size = rng.uniform(0.1, 0.5, 3)
+        lo = np.array([rng.uniform(-2.9, 2.9 - size[0]),
+                       0.0 if rng.random() < 0.5 else rng.uniform(0.0, 2.9 - size[1]),
+                       rng.uniform(-2.9, 2.9 - size[2])])
+        if clear(lo + 0.5 * size, 0.5 * float(np.linalg.norm(size))):
+            add(*_box_mesh(lo, lo + size), material())
+            placed += 1
+    sky = _material(su, "Light", emission=[environment] * 3)
+    prop = su.prop(SHAPE_INFINITE_SPHERE, [sky])
+    su.set_transformation(prop, np.eye(4, dtype=np.float32))
+    su.su_create_light(prop)
+    return cam

@@ -53,13 +53,15 @@ CASES = {
     # a 2 m Cube of 32^3 fBm density (mu_t 20 per metre at density 1, albedo 0.9, g 0.6) lit
     # by a Sphere light and the environment, max depth 32
     "volume64": (64, 64, 2048, {"scene": "volume"}, scenes.fbm_density(32)),
+    # the guiding workload's room (plain MIS): lit only through a doorway by the environment
+    "doorway96": (96, 54, 8192, {"scene": "doorway"}, None),
 }
 PATH = HERE / "cornell_reference.npz"
 # Block size of the block-mean comparison where 8 is too small: many small, bright emitters
 # leave the 2048-spp reference image with 4 % noise in single 8x8 blocks (its 1024- and
 # 2048-spp images differ by that much), 1.6 % in 16x16 blocks; the dense medium 1.7 % and
 # 0.6 %.
-BLOCK = {"wavefront96": 16, "volume64": 16}
+BLOCK = {"wavefront96": 16, "volume64": 16, "doorway96": 16}
 
 
 def build(su, w, h, spp, kwargs, density=None):
@@ -74,6 +76,8 @@ def build(su, w, h, spp, kwargs, density=None):
         return scenes.builtin_shapes(su, w, h, spp, **kwargs)
     if name == "volume":
         return scenes.volume(su, w, h, spp, density, **kwargs)
+    if name == "doorway":
+        return scenes.doorway(su, w, h, spp, **kwargs)
     return scenes.cornell(su, w, h, tonemap=True, spp=spp, density=density, **kwargs)
 
 

@@ -46,6 +46,8 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
             scenes.builtin_shapes(su, width, height, spp, **scene)
         elif name == "volume":
             scenes.volume(su, width, height, spp, density, **scene)
+        elif name == "doorway":
+            scenes.doorway(su, width, height, spp, **scene)
         else:
             scenes.cornell(su, width, height, tonemap=True, spp=spp, density=density, **scene)
         if progressive:
@@ -63,7 +65,8 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
 
 
 CASES = ["cornell64_sub3", "cornell128_sub6", "cornell64_medium", "cornell64_thin_direct", "cornell64_grid",
-         "cornell64_lights", "wavefront96", "builtins96", "builtins96_backdrop", "volume64"]
+         "cornell64_lights", "wavefront96", "builtins96", "builtins96_backdrop", "volume64",
+         "doorway96"]
 
 
 @pytest.mark.parametrize("name", CASES)
