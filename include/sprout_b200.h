@@ -189,6 +189,26 @@ SPB_API int32_t spb_render_last_stats(spb_render_stats* out);
  */
 SPB_API int32_t spb_ggx_albedo_table(float* out);
 
+/*
+ * Path guiding (no counterpart in the reference, which has no path guiding).  The renderer's
+ * guiding network maps a 32-float encoding of a path vertex (position, normal, outgoing
+ * direction) through four hidden layers of 64 (ReLU) to 40 outputs: eight von Mises-Fisher
+ * lobes (unnormalised mean direction, log-concentration) and eight mixture logits.  Its
+ * parameters are packed per layer as W (outputs x inputs, row-major) then b; the products run
+ * with BF16 operands and FP32 accumulation.  These entry points expose the network's forward
+ * pass and its training gradient on host arrays, so that both can be checked against a CPU
+ * restatement.
+ *
+ * spb_guide_parameter_count: the packed parameter count (17,192).
+ * spb_guide_forward: outputs (n x 40) for inputs (n x 32).
+ * spb_guide_gradients: gradient (parameter count) of (1/n) sum_i weights[i] * (-log q_i),
+ *   q_i the mixture's density at directions[i] (n x 3, unit vectors) for inputs[i].
+ */
+SPB_API int32_t spb_guide_parameter_count(uint32_t* count);
+SPB_API int32_t spb_guide_forward(float const* params, float const* inputs, uint64_t n, float* outputs);
+SPB_API int32_t spb_guide_gradients(float const* params, float const* inputs, float const* directions,
+                                    float const* weights, uint64_t n, float* gradient);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,6 +65,9 @@ PROTOTYPES = {
     "spb_synth_rays": (c_i32, [c_u64, c_u64, c_u32, c_f32, c_vp, c_u32]),
     "spb_ggx_albedo_table": (c_i32, [c_vp]),
     "spb_render_last_stats": (c_i32, [ctypes.POINTER(RenderStats)]),
+    "spb_guide_parameter_count": (c_i32, [ctypes.POINTER(ctypes.c_uint32)]),
+    "spb_guide_forward": (c_i32, [c_vp, c_vp, ctypes.c_uint64, c_vp]),
+    "spb_guide_gradients": (c_i32, [c_vp, c_vp, c_vp, c_vp, ctypes.c_uint64, c_vp]),
     "spb_intersect_host_static": (c_i32, [c_vp, c_vp, c_u64, c_vp, c_vp]),
 }
 

@@ -1,0 +1,52 @@
+// Host side of the path-guiding network: its state on the device (FP32 master parameters,
+// Adam moments, BF16 weights) and the training step.  Kernels in guide.cu.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace spb::guide {
+
+// Shared memory of the forward / gradient tile kernels (176 KB).
+size_t tile_smem_bytes();
+
+class Network {
+  public:
+    Network() = default;
+    ~Network();
+    Network(Network const&)            = delete;
+    Network& operator=(Network const&) = delete;
+
+    // Allocates the state and initialises the parameters (He-uniform weights, zero biases,
+    // seeded); 0 or a cudaError_t.
+    int init(uint32_t seed);
+    // Replaces the parameters (host FP32, Parameters values); resets Adam.
+    int set_parameters(float const* host);
+    int get_parameters(float* host) const;
+
+    // Forward pass over n encoded inputs (device, n x 32 FP32) into n x 40 device outputs.
+    int forward(float const* inputs, uint64_t n, float* outputs, cudaStream_t stream);
+    // Gradient of (1/n) sum scale_i * (-log q(d_i | x_i)) into the device gradient buffer
+    // (`scale` already holds the 1/n).
+    int gradients(float const* inputs, float const* dirs, float const* scale, uint64_t n, cudaStream_t stream);
+    // One Adam step with the current gradient.
+    int adam(float lr, cudaStream_t stream);
+
+    float const*         gradient() const { return grads_; }
+    __nv_bfloat16 const* weights() const { return wbf_; }
+    float const*         parameters() const { return params_; }
+
+  private:
+    float*         params_  = nullptr;
+    float*         m_       = nullptr;
+    float*         v_       = nullptr;
+    float*         grads_   = nullptr;
+    __nv_bfloat16* wbf_     = nullptr;
+    float*         partial_ = nullptr;
+    uint64_t       partial_blocks_ = 0;
+    uint32_t       step_    = 0;
+};
+
+}  // namespace spb::guide
