@@ -595,6 +595,23 @@ SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
         if (pt) {
             s.min_bounces = uint32_t(spb::json::number_or(pt->find("min_bounces"), s.min_bounces));
             s.max_bounces = uint32_t(spb::json::number_or(pt->find("max_bounces"), s.max_bounces));
+            // "guiding": true, or an object of the Settings guide fields (this renderer's
+            // extension; the reference ignores the key)
+            if (spb::json::Value const* g = pt->find("guiding")) {
+                s.guiding = g->is_object() || spb::json::bool_or(g, false);
+                if (g->is_object()) {
+                    s.guide_fraction = float(spb::json::number_or(g->find("fraction"), s.guide_fraction));
+                    s.guide_batch    = uint32_t(spb::json::number_or(g->find("batch"), s.guide_batch));
+                    s.guide_steps    = uint32_t(spb::json::number_or(g->find("steps"), s.guide_steps));
+                    s.guide_lr       = float(spb::json::number_or(g->find("learning_rate"), s.guide_lr));
+                    s.record_depth   = uint32_t(spb::json::number_or(g->find("record_depth"), s.record_depth));
+                    s.guide_seed     = uint32_t(spb::json::number_or(g->find("seed"), s.guide_seed));
+                    s.guide_pass_spp = uint32_t(spb::json::number_or(g->find("pass_spp"), s.guide_pass_spp));
+                }
+                s.guide_fraction = std::clamp(s.guide_fraction, 0.f, 0.95f);
+                s.record_depth   = std::clamp(s.record_depth, 1u, 8u);
+                s.guide_batch    = std::clamp(s.guide_batch, 128u, 1u << 22);
+            }
         }
     }
     if (s.max_bounces > 60) {

@@ -27,6 +27,8 @@ struct Train_smem {
     __nv_bfloat16 a[4][Tile * Width];
     float         za[Tile * (Width + 1)];
     float         zb[Tile * (Width + 1)];
+    uint64_t      mbar;       // tensor-core completion barrier
+    uint32_t      tmem_slot;  // accumulator address written by tcgen05.alloc
 };
 
 // Loads rows [base, base + 128) of an n x 32 FP32 input matrix into the tiled BF16 a0 (rows
@@ -39,16 +41,19 @@ __device__ inline void load_inputs(__nv_bfloat16* a0, float const* __restrict__ 
     }
 }
 
+// Forward pass on the tensor cores (the renderer's inference path, guide_mlp.cuh).
 __global__ void __launch_bounds__(Block) k_forward(__nv_bfloat16 const* wbf, float const* params,
-                                                   float const* in, uint64_t n, float* out) {
+                                                   float const* in, uint64_t n, float* out, uint32_t* error) {
     extern __shared__ __align__(16) unsigned char raw[];
     Train_smem& s = *reinterpret_cast<Train_smem*>(raw);
     load_net(s.net, wbf, params);
     uint64_t const base = uint64_t(blockIdx.x) * Tile;
     load_inputs(s.a0, in, base, n);
-    __syncthreads();
+    fence_async_smem();
+    Tmem_tile tm = tc_setup(&s.tmem_slot, &s.mbar, error);
     __nv_bfloat16* const acts[Layers] = {s.a0, s.a[0], s.a[1], s.a[2], s.a[3]};
-    forward(s.net, acts, s.za);
+    forward_tc(s.net, acts, s.za, tm);
+    tc_teardown(tm);
     for (int i = threadIdx.x; i < Tile * Outputs; i += Block) {
         int const      r = i / Outputs, j = i % Outputs;
         uint64_t const g = base + r;
@@ -195,6 +200,7 @@ Network::~Network() {
     release(grads_);
     release(wbf_);
     release(partial_);
+    release(error_);
 }
 
 int Network::init(uint32_t seed) {
@@ -248,8 +254,24 @@ int Network::forward(float const* inputs, uint64_t n, float* outputs, cudaStream
         return 0;
     }
     uint64_t const blocks = (n + Tile - 1) / Tile;
-    k_forward<<<unsigned(blocks), Block, tile_smem_bytes(), stream>>>(wbf_, params_, inputs, n, outputs);
-    return cudaGetLastError();
+    if (!error_) {
+        if (cudaError_t const e = cudaMalloc(&error_, sizeof(uint32_t))) {
+            return e;
+        }
+    }
+    cudaError_t e = cudaMemsetAsync(error_, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) {
+        return e;
+    }
+    k_forward<<<unsigned(blocks), Block, tile_smem_bytes(), stream>>>(wbf_, params_, inputs, n, outputs, error_);
+    uint32_t flag = 0;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, error_, sizeof(flag), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e == cudaSuccess && flag) {
+        return int(cudaErrorLaunchTimeout);  // a tensor-core completion wait ran out
+    }
+    return e;
 }
 
 int Network::gradients(float const* inputs, float const* dirs, float const* scale, uint64_t n,

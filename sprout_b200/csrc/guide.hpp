@@ -26,7 +26,8 @@ class Network {
     int set_parameters(float const* host);
     int get_parameters(float* host) const;
 
-    // Forward pass over n encoded inputs (device, n x 32 FP32) into n x 40 device outputs.
+    // Forward pass over n encoded inputs (device, n x 32 FP32) into n x 40 device outputs, on
+    // the tensor cores; waits for completion.
     int forward(float const* inputs, uint64_t n, float* outputs, cudaStream_t stream);
     // Gradient of (1/n) sum scale_i * (-log q(d_i | x_i)) into the device gradient buffer
     // (`scale` already holds the 1/n).
@@ -47,6 +48,7 @@ class Network {
     float*         partial_ = nullptr;
     uint64_t       partial_blocks_ = 0;
     uint32_t       step_    = 0;
+    uint32_t*      error_   = nullptr;  // set by a tensor-core wait that ran out
 };
 
 }  // namespace spb::guide

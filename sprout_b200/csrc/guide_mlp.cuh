@@ -125,6 +125,203 @@ __device__ inline void forward(Net_smem const& s, __nv_bfloat16* const acts[Laye
     __syncthreads();
 }
 
+// ---- the same products on the tensor cores (tcgen05, sm_100a) ----
+// One M = 128 tile per layer: the layer's input tile (A, K-major) times its weights (B, K-major)
+// accumulated in FP32 in tensor memory (TMEM) by tcgen05.mma (kind::f16, BF16 operands), issued
+// by thread 0 in K steps of 16, completion signalled by tcgen05.commit on an mbarrier.  Each
+// warp then reads its 32-lane quarter of the accumulator (row = lane) with tcgen05.ld; bias,
+// ReLU and the BF16 store for the next layer follow as on the CUDA cores.  Operand descriptors:
+// the tiled layout above is the canonical K-major layout without swizzle, leading byte offset
+// 128 (the next 8 columns), stride byte offset K * 16 (the next 8 rows).
+struct Tmem_tile {
+    uint32_t  tmem;   // accumulator: lane 0 of its first column
+    uint32_t  mbar;   // shared-memory address of the completion mbarrier
+    uint32_t  phase;  // parity of the next completion
+    uint32_t* error;  // set to 1 when a completion wait runs out
+};
+
+__device__ __forceinline__ uint32_t smem_u32(void const* p) {
+    return uint32_t(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor, no swizzle, version 1 (sm_100); offsets in bytes.
+__device__ __forceinline__ uint64_t operand_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: BF16 A and B, FP32 accumulator, M x N, K- or MN-major.
+__host__ __device__ constexpr uint32_t instr_desc(int m, int n, bool a_mn = false, bool b_mn = false) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(a_mn) << 15) | (uint32_t(b_mn) << 16) |
+           (uint32_t(n >> 3) << 17) | (uint32_t(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+    uint32_t const mask = 0u;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+        :
+        : "r"(d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(mask));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Makes this thread's shared-memory stores visible to the tensor cores' operand reads.
+__device__ __forceinline__ void fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Waits (bounded) for the mbarrier to complete the given phase; false if it never did.
+__device__ inline bool mbar_wait(uint32_t mbar, uint32_t phase) {
+    for (uint32_t i = 0; i < (1u << 22); ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}"
+            : "=r"(done)
+            : "r"(mbar), "r"(phase)
+            : "memory");
+        if (done) {
+            return true;
+        }
+    }
+    return false;
+}
+
+// 32 / 8 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float v[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+        "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
+          "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+          "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        v[i] = __uint_as_float(r[i]);
+    }
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float v[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        v[i] = __uint_as_float(r[i]);
+    }
+}
+
+// One layer on the tensor cores.  Precondition: A and W are in shared memory, every writer
+// fenced its stores for the async proxy, and a block barrier (after tc_fence_before) followed.
+// Ends with the results stored and a barrier.
+template <int K, int N, bool Last>
+__device__ inline void layer_forward_tc(__nv_bfloat16 const* A, __nv_bfloat16 const* W, float const* b,
+                                        __nv_bfloat16* act, float* out, Tmem_tile& tm) {
+    constexpr int P = (N + 15) & ~15;
+    if (threadIdx.x == 0) {
+        tc_fence_after();
+        uint32_t const a0 = smem_u32(A);
+        uint32_t const b0 = smem_u32(W);
+#pragma unroll
+        for (int k = 0; k < K / 16; ++k) {
+            umma_bf16(tm.tmem, operand_desc(a0 + 256u * k, 128u, K * 16u), operand_desc(b0 + 256u * k, 128u, K * 16u),
+                      instr_desc(Tile, P), k > 0 ? 1u : 0u);
+        }
+        umma_commit(tm.mbar);
+    }
+    if (!mbar_wait(tm.mbar, tm.phase)) {
+        *tm.error = 1u;
+    }
+    tm.phase ^= 1u;
+    tc_fence_after();
+    int const      warp  = threadIdx.x >> 5;
+    int const      r     = threadIdx.x & (Tile - 1);
+    uint32_t const lanes = uint32_t(32 * (warp & 3)) << 16;
+    if (Last) {
+        if (threadIdx.x < Tile) {
+            float v[40];
+            tmem_ld32(tm.tmem + lanes, v);
+            tmem_ld8(tm.tmem + lanes + 32u, v + 32);
+#pragma unroll
+            for (int n = 0; n < N; ++n) {
+                out[r * Out_stride + n] = v[n] + b[n];
+            }
+        }
+    } else {
+        int const n0 = (threadIdx.x >> 7) * (N / 2);  // N = 64: 32 columns per thread
+        float     v[32];
+        tmem_ld32(tm.tmem + lanes + uint32_t(n0), v);
+#pragma unroll
+        for (int j = 0; j < 32; j += 8) {
+            __nv_bfloat162 h[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                h[q] = __floats2bfloat162_rn(fmaxf(v[j + 2 * q] + b[n0 + j + 2 * q], 0.f),
+                                             fmaxf(v[j + 2 * q + 1] + b[n0 + j + 2 * q + 1], 0.f));
+            }
+            *reinterpret_cast<uint4*>(act + tiled(r, n0 + j, N)) = *reinterpret_cast<uint4*>(h);
+        }
+        fence_async_smem();
+    }
+    tc_fence_before();
+    __syncthreads();
+}
+
+// Forward through all layers on the tensor cores (same contract as forward()).
+__device__ inline void forward_tc(Net_smem const& s, __nv_bfloat16* const acts[Layers], float* out, Tmem_tile& tm) {
+    layer_forward_tc<Inputs, Width, false>(acts[0], s.w + weight_tile_offset(0), s.b + bias_slot(0), acts[1], nullptr, tm);
+    layer_forward_tc<Width, Width, false>(acts[1], s.w + weight_tile_offset(1), s.b + bias_slot(1), acts[2], nullptr, tm);
+    layer_forward_tc<Width, Width, false>(acts[2], s.w + weight_tile_offset(2), s.b + bias_slot(2), acts[3], nullptr, tm);
+    layer_forward_tc<Width, Width, false>(acts[3], s.w + weight_tile_offset(3), s.b + bias_slot(3), acts[4], nullptr, tm);
+    layer_forward_tc<Width, Outputs, true>(acts[4], s.w + weight_tile_offset(4), s.b + bias_slot(4), nullptr, out, tm);
+}
+
+// TMEM columns for one accumulator tile (64 FP32 columns, a power of two >= 32).
+constexpr uint32_t Tmem_columns = 64;
+
+// Block set-up for tensor-core tiles: warp 0 allocates the accumulator, thread 0 initialises
+// the mbarrier; `slot` and `bar` live in shared memory.  Ends with a barrier.
+__device__ inline Tmem_tile tc_setup(uint32_t* slot, uint64_t* bar, uint32_t* error) {
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
+                     "r"(Tmem_columns));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    return Tmem_tile{*slot, smem_u32(bar), 0u, error};
+}
+
+// Releases the accumulator (warp 0; after the last tcgen05.ld of every warp and a barrier).
+__device__ inline void tc_teardown(Tmem_tile const& tm) {
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm.tmem), "r"(Tmem_columns));
+    }
+}
+
 // Gradient of scale * (-log q(d)) with respect to one sample's 40 outputs o (mixture from
 // guide.cuh; the log-concentration has zero gradient where it is clamped).
 __device__ inline void output_gradient(float const* o, shading::V3 d, float scale, float* g) {

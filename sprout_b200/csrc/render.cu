@@ -32,6 +32,8 @@
 #include "bvh8.hpp"
 #include "common.hpp"
 #include "ggx_table.hpp"
+#include "guide.hpp"
+#include "guide_mlp.cuh"
 #include "light_tree.hpp"
 #include "render.hpp"
 #include "traverse.cuh"
@@ -112,7 +114,17 @@ struct Paths {
     float4*   sh2_d;
     float4*   sh2_L;
     float4*   L2;
+    // Path guiding: the network's 40 outputs for the path's current vertex (guide_ok: valid),
+    // the training records of its first record_depth vertices (5 float4 each: position and
+    // normal x | normal yz, wo xy | wo z, wi | throughput | radiance mark, w = 1 once marked)
+    // and the record awaiting its radiance mark.
+    float*    guide_out;
+    uint8_t*  guide_ok;
+    float4*   rec;
+    uint32_t* open_record;
 };
+
+constexpr int Record_float4 = 5;
 
 // Shadow-queue entries are path indices; this bit marks the vertex's second shadow ray.
 constexpr uint32_t Second_shadow = 0x80000000u;
@@ -132,6 +144,11 @@ struct Wave {
     uint32_t seed;
     uint32_t min_bounces;
     uint32_t max_bounces;
+    uint32_t guiding;         // 1: sample the guide's mixture at surface vertices
+    float    guide_fraction;  // its share of continuation directions
+    uint32_t record_depth;    // vertices per path recorded for training (0: none)
+    float4   bounds_lo;       // scene box, for the guide's position encoding
+    float4   bounds_inv;      // 1 / its extent
 };
 
 // ---- PCG32 (O'Neill 2014), seeded as rnd::Generator::start (base/random/generator.inl) ----
@@ -256,6 +273,12 @@ __global__ void k_generate(Cam cam, Wave wave, Paths p, uint32_t* queue, uint32_
     p.rng[i]   = rng.save();
     p.info[i]  = 1u << 16;  // vertex 0, depth 0, treat as singular
     queue[i]   = i;
+    if (wave.record_depth) {
+        p.open_record[i] = 0xFFFFFFFFu;
+        for (uint32_t j = 0; j < wave.record_depth; ++j) {
+            p.rec[(size_t(i) * wave.record_depth + j) * Record_float4 + 4] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
 }
 
 // ---- extend / shadow: persistent traversal over a queue of path indices ----
@@ -916,6 +939,91 @@ __device__ __forceinline__ void store_shadow(Paths const& p, uint32_t path, bool
     }
 }
 
+// ---- guide: the network's mixture for every queued surface hit (before shading) ----
+// One tile of 128 queue entries per block: encodes the hit (position in the scene box,
+// geometric normal facing the ray's origin, outgoing direction), runs the network
+// (guide_mlp.cuh) and stores its 40 outputs for k_shade.  Hits on other than Substitute
+// surfaces are marked invalid.
+struct Infer_smem {
+    guide::Net_smem net;
+    __nv_bfloat16   a0[guide::Tile * guide::Inputs];
+    __nv_bfloat16   x[guide::Tile * guide::Width];
+    __nv_bfloat16   y[guide::Tile * guide::Width];
+    float           out[guide::Tile * guide::Out_stride];
+    uint32_t        path[guide::Tile];
+    uint64_t        mbar;       // tensor-core completion barrier
+    uint32_t        tmem_slot;  // accumulator address from tcgen05.alloc
+};
+
+// Position, geometric normal (facing -dir) and outgoing direction of a path's hit.
+__device__ __forceinline__ void hit_frame(Scene_gpu const& s, Paths const& p, uint32_t path, uint32_t id,
+                                          V3& pos, V3& geo_n, V3& wo) {
+    uint4 const  tri = s.tri_info[id];
+    V3 const     a   = f3v(s.positions[tri.x]);
+    V3 const     b   = f3v(s.positions[tri.y]);
+    V3 const     c   = f3v(s.positions[tri.z]);
+    float2 const uv  = p.hit_uv[path];
+    pos              = (1.f - uv.x - uv.y) * a + uv.x * b + uv.y * c;
+    geo_n            = shading::normalize(shading::cross(b - a, c - a));
+    wo               = -f3v(p.ray_d[path]);
+    if (shading::dot(geo_n, wo) < 0.f) {
+        geo_n = -geo_n;
+    }
+}
+
+__device__ __forceinline__ V3 box_coordinates(Wave const& wave, V3 pos) {
+    return v3((pos.x - wave.bounds_lo.x) * wave.bounds_inv.x, (pos.y - wave.bounds_lo.y) * wave.bounds_inv.y,
+              (pos.z - wave.bounds_lo.z) * wave.bounds_inv.z);
+}
+
+__global__ void __launch_bounds__(guide::Block)
+    k_guide(Scene_gpu s, Wave wave, Paths p, uint32_t const* __restrict__ queue,
+            uint32_t const* __restrict__ count, __nv_bfloat16 const* __restrict__ wbf,
+            float const* __restrict__ params, uint32_t* error) {
+    extern __shared__ __align__(16) unsigned char raw[];
+    Infer_smem&    m    = *reinterpret_cast<Infer_smem*>(raw);
+    uint32_t const num  = *count;
+    uint32_t const base = blockIdx.x * guide::Tile;
+    if (base >= num) {
+        return;  // the whole block: no barrier is skipped by only some threads
+    }
+    guide::load_net(m.net, wbf, params);
+    if (threadIdx.x < guide::Tile) {
+        uint32_t const q    = base + threadIdx.x;
+        uint32_t       path = 0xFFFFFFFFu;
+        float          in[guide::Inputs];
+        bool           ok = false;
+        if (q < num) {
+            path              = queue[q];
+            uint32_t const id = p.hit_id[path];
+            if (id != gpu::Miss && s.materials[s.tri_info[id].w].type == shading::Type_substitute) {
+                V3 pos, geo_n, wo;
+                hit_frame(s, p, path, id, pos, geo_n, wo);
+                guide::encode(box_coordinates(wave, pos), geo_n, wo, in);
+                ok = true;
+            }
+            p.guide_ok[path] = ok ? 1 : 0;
+        }
+        for (int k = 0; k < guide::Inputs; ++k) {
+            m.a0[guide::tiled(threadIdx.x, k, guide::Inputs)] = __float2bfloat16(ok ? in[k] : 0.f);
+        }
+        m.path[threadIdx.x] = ok ? path : 0xFFFFFFFFu;
+    }
+    guide::fence_async_smem();
+    guide::Tmem_tile tm = guide::tc_setup(&m.tmem_slot, &m.mbar, error);
+    __nv_bfloat16* const acts[guide::Layers] = {m.a0, m.x, m.y, m.x, m.y};
+    guide::forward_tc(m.net, acts, m.out, tm);
+    guide::tc_teardown(tm);
+    for (int i = threadIdx.x; i < guide::Tile * guide::Outputs; i += guide::Block) {
+        int const      r    = i / guide::Outputs;
+        int const      j    = i % guide::Outputs;
+        uint32_t const path = m.path[r];
+        if (path != 0xFFFFFFFFu) {
+            p.guide_out[size_t(path) * guide::Outputs + j] = m.out[r * guide::Out_stride + j];
+        }
+    }
+}
+
 // ---- shade: one path vertex ----
 __global__ void __launch_bounds__(Shade_block)
     k_shade(Scene_gpu s, Wave wave, Paths p, uint32_t const* __restrict__ q_in,
@@ -943,6 +1051,16 @@ __global__ void __launch_bounds__(Shade_block)
         V3       L        = f3v(L4);
         uint32_t const id = p.hit_id[path];
         bool     done     = false;
+        if (wave.record_depth) {
+            // The training record of the previous vertex learns what its continuation found:
+            // the radiance gathered so far (its own light samples included) marks the start.
+            uint32_t const open = p.open_record[path];
+            if (open != 0xFFFFFFFFu) {
+                float4 const l2 = p.L2[path];
+                p.rec[size_t(open) * Record_float4 + 4] = make_float4(L.x + l2.x, L.y + l2.y, L.z + l2.z, 1.f);
+                p.open_record[path] = 0xFFFFFFFFu;
+            }
+        }
         float4 const ro   = p.ray_o[path];
         float4 const rd   = p.ray_d[path];
         V3 const     dir_in = v3(rd.x, rd.y, rd.z);
@@ -1113,6 +1231,25 @@ __global__ void __launch_bounds__(Shade_block)
                 ctx.geo_n = geo_n;
                 ctx.wo    = wo;
 
+                // The guide's mixture for this vertex (k_guide); continuation directions come
+                // from it with probability gf, else from the BSDF, and every pdf the MIS
+                // weights use is the combination of both.
+                bool const  guided = wave.guiding && p.guide_ok[path];
+                float const gf     = guided ? wave.guide_fraction : 0.f;
+                guide::Lobe lobes[guide::Lobes];
+                if (guided) {
+                    float        o[guide::Outputs];
+                    float4 const* src = reinterpret_cast<float4 const*>(p.guide_out + size_t(path) * guide::Outputs);
+                    for (int k = 0; k < guide::Outputs / 4; ++k) {
+                        float4 const v = src[k];
+                        o[4 * k]       = v.x;
+                        o[4 * k + 1]   = v.y;
+                        o[4 * k + 2]   = v.z;
+                        o[4 * k + 3]   = v.w;
+                    }
+                    guide::mixture(o, lobes);
+                }
+
                 // Next-event estimation (sample_lights / evaluate_light, pathtracer_mis.cpp:281-347).
                 int const samples = num_light_samples(s, depth);
                 V3 const  ps      = offset_ray(pos, geo_n);
@@ -1124,7 +1261,9 @@ __global__ void __launch_bounds__(Shade_block)
                     if (sample_light(s, ps, geo_n, false, r, r1, r2, ls, light_mode(samples, k))) {
                         shading::Bxdf const f =
                             shading::substitute_evaluate(mat, s.e_table, ctx, ls.dir);
-                        float const w = ls.pdf / (ls.pdf * ls.pdf + f.pdf * f.pdf);
+                        float const pc = guided ? gf * guide::mixture_pdf(lobes, ls.dir) + (1.f - gf) * f.pdf
+                                                : f.pdf;
+                        float const w  = ls.pdf / (ls.pdf * ls.pdf + pc * pc);
                         V3 const contrib = w * (T * (ls.radiance * f.reflection));
                         if (shading::max_component(contrib) > 0.f) {
                             store_shadow(p, path, k == 1, ps, ls, contrib, depth);
@@ -1133,19 +1272,49 @@ __global__ void __launch_bounds__(Shade_block)
                     }
                 }
 
-                // BSDF sample (pathtracer_mis.cpp:153-201).
-                float const xl = rng.uniform();
-                float const x0 = rng.uniform();
-                float const x1 = rng.uniform();
-                shading::Sampled const smp =
-                    shading::substitute_sample(mat, s.e_table, ctx, xl, x0, x1);
+                // Continuation direction: the BSDF sample (pathtracer_mis.cpp:153-201), or with
+                // probability gf the guide's (no reflection below the surface).
+                shading::Sampled smp;
+                if (guided && rng.uniform() < gf) {
+                    float const g0 = rng.uniform();
+                    float const g1 = rng.uniform();
+                    float const g2 = rng.uniform();
+                    smp.wi       = guide::mixture_sample(lobes, g0, g1, g2);
+                    smp.specular = false;
+                    if (shading::dot(smp.wi, geo_n) > 0.f) {
+                        shading::Bxdf const f = shading::substitute_evaluate(mat, s.e_table, ctx, smp.wi);
+                        smp.reflection        = f.reflection;
+                        smp.pdf               = f.pdf;
+                    } else {
+                        smp.pdf = 0.f;
+                    }
+                } else {
+                    float const xl = rng.uniform();
+                    float const x0 = rng.uniform();
+                    float const x1 = rng.uniform();
+                    smp = shading::substitute_sample(mat, s.e_table, ctx, xl, x0, x1);
+                }
                 if (smp.pdf > 0.f) {
+                    float const pdf = guided && !smp.specular
+                                          ? gf * guide::mixture_pdf(lobes, smp.wi) + (1.f - gf) * smp.pdf
+                                          : smp.pdf;
+                    if (guided && depth < wave.record_depth) {
+                        // training record of this vertex (its radiance mark comes at the next)
+                        uint32_t const r = path * wave.record_depth + depth;
+                        float4* const  d = p.rec + size_t(r) * Record_float4;
+                        d[0] = make_float4(pos.x, pos.y, pos.z, geo_n.x);
+                        d[1] = make_float4(geo_n.y, geo_n.z, wo.x, wo.y);
+                        d[2] = make_float4(wo.z, smp.wi.x, smp.wi.y, smp.wi.z);
+                        d[3] = make_float4(T.x, T.y, T.z, 0.f);
+                        d[4] = make_float4(0.f, 0.f, 0.f, 0.f);
+                        p.open_record[path] = r;
+                    }
                     V3 const o = offset_ray(pos, shading::dot(geo_n, smp.wi) > 0.f ? geo_n : -geo_n);
                     p.ray_o[path]  = make_float4(o.x, o.y, o.z, 0.f);
                     p.ray_d[path]  = make_float4(smp.wi.x, smp.wi.y, smp.wi.z, Ray_max_t);
                     p.prev_n[path] = make_float4(geo_n.x, geo_n.y, geo_n.z, 0.f);
-                    T        = (1.f / smp.pdf) * (T * smp.reflection);
-                    bsdf_pdf = smp.pdf;
+                    T        = (1.f / pdf) * (T * smp.reflection);
+                    bsdf_pdf = pdf;
                     singular = smp.specular;
                     ++depth;
                     ++vtx;
@@ -1309,6 +1478,74 @@ __global__ void k_gather(Paths p, uint32_t w, uint32_t h, uint32_t samples, floa
     film[q]    = t;
 }
 
+// ---- guide training: samples from the wave's records ----
+// Batch entry i takes record hash(i, pass) of the wave; a finished record (radiance mark set)
+// gives the input encoding, the continuation direction and the weight
+// luminance((L_final - L_mark) / T): the continuation's radiance times f cos / pdf at the
+// vertex, the target of the product-guiding loss.  Other records give weight 0.
+__global__ void k_train_gather(Paths p, Wave wave, uint32_t records, uint32_t batch, uint32_t pass,
+                               float* in, float* dir, float* weight) {
+    uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= batch) {
+        return;
+    }
+    uint64_t const h = (uint64_t(i) * 0x9E3779B97F4A7C15ull) ^ (uint64_t(pass + 1) * 0xD1B54A32D192ED03ull);
+    uint32_t const r = uint32_t(((h ^ (h >> 29)) * 0xBF58476D1CE4E5B9ull >> 32) % records);
+    float4 const*  d = p.rec + size_t(r) * Record_float4;
+    float4 const   mark = d[4];
+    float          w    = 0.f;
+    float4 const   a = d[0], b = d[1], c = d[2], t = d[3];
+    if (mark.w == 1.f) {
+        uint32_t const path = r / wave.record_depth;
+        float4 const   l    = p.L[path];
+        float4 const   l2   = p.L2[path];
+        float const    cx   = t.x > 0.f ? (l.x + l2.x - mark.x) / t.x : 0.f;
+        float const    cy   = t.y > 0.f ? (l.y + l2.y - mark.y) / t.y : 0.f;
+        float const    cz   = t.z > 0.f ? (l.z + l2.z - mark.z) / t.z : 0.f;
+        // AP1 (ACEScg) luminance
+        float const lum = 0.2722287f * cx + 0.6740818f * cy + 0.0536895f * cz;
+        w               = (lum > 0.f && lum < 1e30f) ? lum : 0.f;
+    }
+    float enc[guide::Inputs];
+    guide::encode(box_coordinates(wave, v3(a.x, a.y, a.z)), v3(a.w, b.x, b.y), v3(b.z, b.w, c.x), enc);
+    for (int k = 0; k < guide::Inputs; ++k) {
+        in[size_t(i) * guide::Inputs + k] = w > 0.f ? enc[k] : 0.f;
+    }
+    dir[3 * size_t(i)]     = w > 0.f ? c.y : 0.f;
+    dir[3 * size_t(i) + 1] = w > 0.f ? c.z : 0.f;
+    dir[3 * size_t(i) + 2] = w > 0.f ? c.w : 1.f;
+    weight[i]              = w;
+}
+
+// sum = the weights' total, in a fixed order (one block of 1024 threads).
+__global__ void __launch_bounds__(1024) k_sum_weights(float const* weight, uint32_t n, float* sum) {
+    __shared__ float part[1024];
+    float            acc = 0.f;
+    for (uint32_t i = threadIdx.x; i < n; i += 1024) {
+        acc += weight[i];
+    }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 512; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            part[threadIdx.x] += part[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        *sum = part[0];
+    }
+}
+
+// scale_i = weight_i / sum: the batch loss becomes the weighted mean of -log q.
+__global__ void k_scale_weights(float const* weight, float const* sum, uint32_t n, float* scale) {
+    uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        float const s = *sum;
+        scale[i]      = s > 0.f ? weight[i] / s : 0.f;
+    }
+}
+
 __global__ void k_resolve(float4 const* film, float4 const* comp, uint32_t n, float4* out) {
     uint32_t const q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) {
@@ -1343,6 +1580,20 @@ struct Renderer::Device {
     uint32_t           num_lights = 0;
     float4             env        = {0.f, 0.f, 0.f, 0.f};
     float              hit_margin = 0.f;
+    float4             bounds_lo  = {0.f, 0.f, 0.f, 0.f};  // scene box (guide encoding)
+    float4             bounds_inv = {1.f, 1.f, 1.f, 0.f};
+    // path guiding
+    guide::Network     net;
+    bool               net_ready     = false;
+    uint32_t           guide_paths   = 0;  // paths the guide buffers hold
+    uint32_t           guide_records = 0;  // record depth they were sized for
+    uint32_t           train_capacity = 0;
+    float*             train_in    = nullptr;
+    float*             train_dir   = nullptr;
+    float*             train_w     = nullptr;
+    float*             train_scale = nullptr;
+    float*             train_sum   = nullptr;
+    uint32_t           pass        = 0;  // training passes since the scene was set
     // paths
     uint32_t  capacity = 0;
     Paths     paths{};
@@ -1468,6 +1719,11 @@ Renderer::~Renderer() {
         return;
     }
     cudaDeviceSynchronize();
+    free_ptr(d_->train_in);
+    free_ptr(d_->train_dir);
+    free_ptr(d_->train_w);
+    free_ptr(d_->train_scale);
+    free_ptr(d_->train_sum);
     free_ptr(d_->nodes);
     free_ptr(d_->tris);
     free_ptr(d_->tri_info);
@@ -1499,6 +1755,11 @@ Renderer::~Renderer() {
     free_ptr(p.sh2_d);
     free_ptr(p.sh2_L);
     free_ptr(p.L2);
+    free_ptr(p.guide_out);
+    free_ptr(p.guide_ok);
+    free_ptr(p.rec);
+    free_ptr(p.open_record);
+    d_->guide_paths = 0;
     free_ptr(d_->queue[0]);
     free_ptr(d_->queue[1]);
     free_ptr(d_->shadow_queue);
@@ -1602,6 +1863,21 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     Light_tree tree;
     build_light_tree(emitters, nt, tree);
     d_->num_lights = tree.num_lights;
+
+    // Scene box for the guide's position encoding; a new scene starts a new guide.
+    {
+        float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
+        for (uint32_t v = 0; v < nv; ++v) {
+            for (int k = 0; k < 3; ++k) {
+                lo[k] = std::min(lo[k], scene.positions[3 * v + k]);
+                hi[k] = std::max(hi[k], scene.positions[3 * v + k]);
+            }
+        }
+        d_->bounds_lo  = make_float4(lo[0], lo[1], lo[2], 0.f);
+        d_->bounds_inv = make_float4(1.f / std::max(hi[0] - lo[0], 1e-6f), 1.f / std::max(hi[1] - lo[1], 1e-6f),
+                                     1.f / std::max(hi[2] - lo[2], 1e-6f), 0.f);
+        d_->net_ready  = false;
+    }
 
     // The environment's share of light picks: its power against the emitters', with the
     // reference's power of an infinite light, squared scene extent x 4 pi x mean radiance
@@ -1736,6 +2012,11 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     free_ptr(p.sh2_d);
     free_ptr(p.sh2_L);
     free_ptr(p.L2);
+    free_ptr(p.guide_out);
+    free_ptr(p.guide_ok);
+    free_ptr(p.rec);
+    free_ptr(p.open_record);
+    d_->guide_paths = 0;
     free_ptr(d_->queue[0]);
     free_ptr(d_->queue[1]);
     free_ptr(d_->shadow_queue);
@@ -1771,6 +2052,66 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     return SPB_OK;
 }
 
+// Guide buffers for `paths` paths: network outputs, validity, training records; the training
+// batch arrays; the network itself (initialised once per scene).
+int32_t Renderer::ensure_guide(uint32_t paths) {
+    Paths&         p  = d_->paths;
+    uint32_t const rd = settings_.record_depth;
+    if (d_->guide_paths < paths || d_->guide_records != rd) {
+        free_ptr(p.guide_out);
+        free_ptr(p.guide_ok);
+        free_ptr(p.rec);
+        free_ptr(p.open_record);
+        size_t const n = d_->capacity;
+        SPB_RCUDA(cudaMalloc(&p.guide_out, n * guide::Outputs * sizeof(float)));
+        SPB_RCUDA(cudaMalloc(&p.guide_ok, n));
+        SPB_RCUDA(cudaMalloc(&p.rec, n * rd * Record_float4 * sizeof(float4)));
+        SPB_RCUDA(cudaMalloc(&p.open_record, n * sizeof(uint32_t)));
+        d_->guide_paths   = uint32_t(n);
+        d_->guide_records = rd;
+    }
+    uint32_t const batch = settings_.guide_batch;
+    if (d_->train_capacity < batch) {
+        free_ptr(d_->train_in);
+        free_ptr(d_->train_dir);
+        free_ptr(d_->train_w);
+        free_ptr(d_->train_scale);
+        free_ptr(d_->train_sum);
+        SPB_RCUDA(cudaMalloc(&d_->train_in, size_t(batch) * guide::Inputs * sizeof(float)));
+        SPB_RCUDA(cudaMalloc(&d_->train_dir, size_t(batch) * 3 * sizeof(float)));
+        SPB_RCUDA(cudaMalloc(&d_->train_w, size_t(batch) * sizeof(float)));
+        SPB_RCUDA(cudaMalloc(&d_->train_scale, size_t(batch) * sizeof(float)));
+        SPB_RCUDA(cudaMalloc(&d_->train_sum, sizeof(float)));
+        d_->train_capacity = batch;
+    }
+    if (!d_->net_ready) {
+        SPB_RCUDA(cudaError_t(d_->net.init(settings_.guide_seed)));
+        SPB_RCUDA(cudaFuncSetAttribute(k_guide, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(sizeof(Infer_smem))));
+        d_->net_ready = true;
+        d_->pass      = 0;
+    }
+    return SPB_OK;
+}
+
+// Training after a pass: guide_steps Adam steps, each on a fresh batch of the pass's records.
+int32_t Renderer::train_guide(uint32_t paths, void const* wave_ptr) {
+    Wave const&    wave    = *static_cast<Wave const*>(wave_ptr);
+    cudaStream_t   st      = d_->stream;
+    uint32_t const batch   = settings_.guide_batch;
+    uint32_t const records = paths * settings_.record_depth;
+    for (uint32_t step = 0; step < settings_.guide_steps; ++step) {
+        k_train_gather<<<(batch + 255) / 256, 256, 0, st>>>(d_->paths, wave, records, batch, d_->pass++,
+                                                            d_->train_in, d_->train_dir, d_->train_w);
+        k_sum_weights<<<1, 1024, 0, st>>>(d_->train_w, batch, d_->train_sum);
+        k_scale_weights<<<(batch + 255) / 256, 256, 0, st>>>(d_->train_w, d_->train_sum, batch,
+                                                             d_->train_scale);
+        SPB_RCUDA(cudaError_t(d_->net.gradients(d_->train_in, d_->train_dir, d_->train_scale, batch, st)));
+        SPB_RCUDA(cudaError_t(d_->net.adam(settings_.guide_lr, st)));
+    }
+    return SPB_OK;
+}
+
 int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     if (!ready()) {
         error_ = "render needs a scene and a camera";
@@ -1786,9 +2127,17 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     }
     uint32_t const pixels = camera_.width * camera_.height;
     // k samples per pixel per wave, up to about 4M paths per wave.
-    uint32_t const per_wave = std::max(1u, std::min(num_samples, (1u << 22) / std::max(1u, pixels)));
+    uint32_t per_wave = std::max(1u, std::min(num_samples, (1u << 22) / std::max(1u, pixels)));
+    if (settings_.guiding) {
+        per_wave = std::max(1u, std::min(per_wave, settings_.guide_pass_spp));  // train between passes
+    }
     if (int32_t const st = ensure_buffers(per_wave * pixels)) {
         return st;
+    }
+    if (settings_.guiding) {
+        if (int32_t const st = ensure_guide(per_wave * pixels)) {
+            return st;
+        }
     }
 
     float const ratio = float(camera_.height) / float(camera_.width);
@@ -1838,6 +2187,11 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         uint32_t const paths = k * pixels;
         Wave           wave{first_sample + done, k, settings_.seed, settings_.min_bounces,
                   settings_.max_bounces};
+        wave.guiding        = settings_.guiding ? 1u : 0u;
+        wave.guide_fraction = settings_.guide_fraction;
+        wave.record_depth   = settings_.guiding ? settings_.record_depth : 0u;
+        wave.bounds_lo      = d_->bounds_lo;
+        wave.bounds_inv     = d_->bounds_inv;
         SPB_RCUDA(cudaMemsetAsync(ctr, 0, Counter_words * sizeof(uint32_t), st));
         k_generate<<<(paths + 255) / 256, 256, 0, st>>>(cam, wave, d_->paths, d_->queue[0], ctr,
                                                          paths);
@@ -1857,6 +2211,11 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             uint32_t* const c = ctr + Counter_stride * b;
             k_trace<false><<<d_->trace_grid, Trace_block, 0, st>>>(sg, d_->paths, q_in, c, c + 2,
                                                                    ctr + Overflow_slot);
+            if (settings_.guiding) {
+                k_guide<<<(paths + guide::Tile - 1) / guide::Tile, guide::Block, sizeof(Infer_smem), st>>>(
+                    sg, wave, d_->paths, q_in, c, d_->net.weights(), d_->net.parameters(),
+                    ctr + Overflow_slot + 1);
+            }
             k_shade<<<(paths + Shade_block - 1) / Shade_block, Shade_block, 0, st>>>(
                 sg, wave, d_->paths, q_in, c, q_out, c + Counter_stride, d_->shadow_queue, c + 1);
             if (d_->has_media) {
@@ -1870,6 +2229,11 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
                     sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot);
             }
         }
+        if (settings_.guiding) {
+            if (int32_t const e = train_guide(paths, &wave)) {
+                return e;
+            }
+        }
         k_gather<<<(pixels + 255) / 256, 256, 0, st>>>(d_->paths, camera_.width, camera_.height, k,
                                                       d_->film, d_->comp);
         SPB_RCUDA(cudaGetLastError());
@@ -1881,6 +2245,10 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             stats_.shadow_rays += host_ctr[Counter_stride * b + 1];
         }
         stats_.overflow += host_ctr[Overflow_slot];
+        if (host_ctr[Overflow_slot + 1]) {
+            error_ = "path guiding: a tensor-core completion wait ran out";
+            return SPB_ERROR_CUDA;
+        }
         stats_.paths += paths;
         done += k;
     }

@@ -51,6 +51,19 @@ struct Settings {
     uint32_t min_bounces = 4;   // Russian roulette starts here
     uint32_t max_bounces = 8;
     uint32_t seed        = 0;
+    // Learned path guiding (no counterpart in the reference): at surface vertices the
+    // continuation direction comes from the network's vMF mixture with probability
+    // guide_fraction, else from the BSDF (one-sample MIS of the two).  The network is trained
+    // online, guide_steps Adam steps (learning rate guide_lr) on guide_batch samples after each
+    // pass of samples, from the first record_depth vertices of every path.
+    bool     guiding        = false;
+    float    guide_fraction = 0.5f;
+    uint32_t guide_batch    = 1u << 18;
+    uint32_t guide_steps    = 1;
+    float    guide_lr       = 1e-3f;
+    uint32_t record_depth   = 2;
+    uint32_t guide_seed     = 7;
+    uint32_t guide_pass_spp = 4;  // samples per pixel between training steps
 };
 
 struct Stats {
@@ -97,6 +110,8 @@ class Renderer {
     std::string error_;
 
     int32_t ensure_buffers(uint32_t paths);
+    int32_t ensure_guide(uint32_t paths);
+    int32_t train_guide(uint32_t paths, void const* wave);
     void    free_grids();
     int32_t fail_cuda(char const* what, int code);
 };

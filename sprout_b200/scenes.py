@@ -541,25 +541,29 @@ def _box_mesh(lo, hi):
 
 def doorway(su, width: int = 1280, height: int = 720, spp: int = 64, seed: int = 3, spheres: int = 96,
             boxes: int = 160, sphere_subdivisions: int = 4, max_bounces: int = 8, min_bounces: int = 4,
-            environment: float = 5.0):
+            environment: float = 5.0, guiding=None):
     """A 6 x 6 x 3 m room (x, z in [-3, 3], y in [0, 3]) whose only opening is a 1 x 2 m doorway
     in the wall z = 3, outside a uniform environment of radiance `environment` (an
     Infinite_sphere light).  Inside: `spheres` icospheres (20 * 4^subdivisions triangles each:
     491,520 with the defaults) and `boxes` boxes at seeded random places; 70 % of the objects
     Lambertian-like (Substitute, roughness 1, metallic 0), 30 % GGX conductors with alpha
     U[0.1, 0.6].  Walls, floor and ceiling are grey Substitute (roughness 1).  A pinhole camera
-    in the room's far corner looks towards the doorway with a 60 degree field of view."""
+    in the room's far corner looks towards the doorway with a 60 degree field of view.
+    guiding: None for plain MIS, else True or a dict of guide settings (this renderer's
+    "guiding" integrator key; the reference ignores it)."""
     rng = np.random.default_rng(seed)
     eye = np.array([-2.4, 1.5, -2.7])
     cam = su.su_create_camera_perspective(width, height, math.radians(60.0))
     su.set_transformation(cam, _look_at(eye, (0.6, 0.9, 2.0)))
+    ptmis = {"min_bounces": min_bounces, "max_bounces": max_bounces}
+    if guiding is not None:
+        ptmis["guiding"] = guiding
 
     def clear(c, r):
         """Keeps objects off the camera and out of the doorway."""
         return (np.linalg.norm(np.asarray(c) - eye) > r + 1.0 and
                 not (abs(c[0]) < 0.5 + r + 0.3 and c[2] > 2.0 - r))
-    su.su_create_integrators(json.dumps({"surface": {"PTMIS": {"min_bounces": min_bounces,
-                                                              "max_bounces": max_bounces}}}).encode())
+    su.su_create_integrators(json.dumps({"surface": {"PTMIS": ptmis}}).encode())
     su.su_create_sampler(spp)
     su.su_create_defaults()
     wall = _material(su, "Substitute", color=[0.7, 0.7, 0.7], roughness=1.0, metallic=0.0)
