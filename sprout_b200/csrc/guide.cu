@@ -63,49 +63,181 @@ __global__ void __launch_bounds__(Block) k_forward(__nv_bfloat16 const* wbf, flo
     }
 }
 
-// Gradient partials of one tile: loss sum_i scale_i * (-log q(d_i | x_i)) over the tile's
-// samples; writes Parameters floats per block to partial.
-__global__ void __launch_bounds__(Block) k_gradients(__nv_bfloat16 const* wbf, float const* params,
-                                                     float const* in, float const* dirs, float const* scale,
-                                                     uint64_t n, float* partial) {
+// ---- training tile on the tensor cores ----
+// Forward as in inference (keeping every layer's input), the loss gradient at the outputs, then
+// per layer l from the last: dW_l = dZ_l^T A_l (M = 128 over the neurons, padded with zero
+// rows; both operands MN-major) and dA_l = dZ_l W_l (M = 128 over the samples; dZ K-major, W
+// MN-major) into two TMEM accumulators, committed together; dZ_{l-1} = dA_l masked by ReLU.
+// dZ is held as BF16 in a 128 x 128 tiled buffer whose columns past the layer's width stay 0.
+// Bias gradients are summed in FP32 (shared-memory atomics) before the BF16 rounding.
+constexpr int Zw = 128;  // dZ buffer width
+
+struct Train_tc_smem {
+    Net_smem      net;
+    __nv_bfloat16 a0[Tile * Inputs];
+    __nv_bfloat16 a[4][Tile * Width];
+    __nv_bfloat16 z[2][Tile * Zw];
+    float         out[Tile * Out_stride];
+    float         gb[Bias_count];
+    uint64_t      mbar;
+    uint32_t      tmem_slot;
+};
+
+constexpr uint32_t Train_tmem_columns = 128;  // [0, 64): dA and forward; [64, 128): dW
+
+// Issues dW (and dA when with_da) for layer l; thread 0 only.
+template <int K, int N>
+__device__ inline void backward_mma(uint32_t tmem, __nv_bfloat16 const* z, __nv_bfloat16 const* act,
+                                    __nv_bfloat16 const* w, bool with_da, uint32_t mbar) {
+    constexpr int P = (N + 15) & ~15;
+    tc_fence_after();
+    uint32_t const zs = smem_u32(z), as = smem_u32(act), ws = smem_u32(w);
+    // dW[n][k] = sum_r dZ[r][n] A[r][k]: A operand dZ^T (MN-major: n groups 128 B apart, r groups
+    // Zw * 16 B apart), B operand A_l (MN-major: k groups 128 B, r groups K * 16 B).
+#pragma unroll
+    for (int s = 0; s < Tile / 16; ++s) {
+        umma_bf16(tmem + 64u, operand_desc(zs + 2u * Zw * 16u * s, Zw * 16u, 128u),
+                  operand_desc(as + 2u * K * 16u * s, K * 16u, 128u), instr_desc(Tile, K, true, true), s > 0);
+    }
+    if (with_da) {
+        // dA[r][k] = sum_n dZ[r][n] W[n][k]: A operand dZ (K-major over n), B operand W_l
+        // (MN-major: k groups 128 B, n groups K * 16 B).
+#pragma unroll
+        for (int s = 0; s < P / 16; ++s) {
+            umma_bf16(tmem, operand_desc(zs + 256u * s, 128u, Zw * 16u),
+                      operand_desc(ws + 2u * K * 16u * s, K * 16u, 128u), instr_desc(Tile, K, false, true), s > 0);
+        }
+    }
+    umma_commit(mbar);
+}
+
+__global__ void __launch_bounds__(Block) k_gradients_tc(__nv_bfloat16 const* wbf, float const* params,
+                                                        float const* in, float const* dirs, float const* scale,
+                                                        uint64_t n, float* partial, uint32_t* error) {
     extern __shared__ __align__(16) unsigned char raw[];
-    Train_smem& s = *reinterpret_cast<Train_smem*>(raw);
+    Train_tc_smem& s = *reinterpret_cast<Train_tc_smem*>(raw);
     load_net(s.net, wbf, params);
     uint64_t const base = uint64_t(blockIdx.x) * Tile;
     load_inputs(s.a0, in, base, n);
+    for (int i = threadIdx.x; i < 2 * Tile * Zw / 8; i += Block) {
+        reinterpret_cast<uint4*>(s.z)[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    for (int i = threadIdx.x; i < Bias_count; i += Block) {
+        s.gb[i] = 0.f;
+    }
+    fence_async_smem();
+    // TMEM: 128 columns for this kernel (the forward uses the first 64)
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem_slot)),
+                     "r"(Train_tmem_columns));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s.mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
     __syncthreads();
+    tc_fence_after();
+    Tmem_tile tm{s.tmem_slot, smem_u32(&s.mbar), 0u, error};
+
     __nv_bfloat16* const acts[Layers] = {s.a0, s.a[0], s.a[1], s.a[2], s.a[3]};
-    forward(s.net, acts, s.zb);
+    forward_tc(s.net, acts, s.out, tm);
+
+    // Loss gradient at the outputs -> dZ_4 (BF16, columns 0..39; 40..47 stay 0), bias grads.
+    int const r = threadIdx.x & (Tile - 1);
     if (threadIdx.x < Tile) {
-        int const      r = threadIdx.x;
         uint64_t const g = base + r;
-        float*         o = s.za + r * Out_stride;
+        float          gr[Outputs];
         if (g < n) {
-            output_gradient(s.zb + r * Out_stride,
-                            shading::v3(dirs[3 * g], dirs[3 * g + 1], dirs[3 * g + 2]), scale[g], o);
+            output_gradient(s.out + r * Out_stride, shading::v3(dirs[3 * g], dirs[3 * g + 1], dirs[3 * g + 2]),
+                            scale[g], gr);
         } else {
             for (int j = 0; j < Outputs; ++j) {
-                o[j] = 0.f;
+                gr[j] = 0.f;
             }
         }
+        for (int j = 0; j < Outputs; ++j) {
+            s.z[0][tiled(r, j, Zw)] = __float2bfloat16(gr[j]);
+            atomicAdd(&s.gb[bias_slot(4) + j], gr[j]);
+        }
     }
+    fence_async_smem();
+    tc_fence_before();
     __syncthreads();
-    float* const p = partial + uint64_t(blockIdx.x) * Parameters;
-    Net_smem const& net = s.net;
-    layer_backward<Width, Outputs>(acts[4], net.w + weight_tile_offset(4), s.za, s.zb,
-                                   p + weight_offset(4), p + bias_offset(4));
-    __syncthreads();
-    layer_backward<Width, Width>(acts[3], net.w + weight_tile_offset(3), s.zb, s.za,
-                                 p + weight_offset(3), p + bias_offset(3));
-    __syncthreads();
-    layer_backward<Width, Width>(acts[2], net.w + weight_tile_offset(2), s.za, s.zb,
-                                 p + weight_offset(2), p + bias_offset(2));
-    __syncthreads();
-    layer_backward<Width, Width>(acts[1], net.w + weight_tile_offset(1), s.zb, s.za,
-                                 p + weight_offset(1), p + bias_offset(1));
-    __syncthreads();
-    layer_backward<Inputs, Width>(acts[0], net.w + weight_tile_offset(0), s.za, nullptr,
-                                  p + weight_offset(0), p + bias_offset(0));
+
+    float* const   pout   = partial + uint64_t(blockIdx.x) * Parameters;
+    int const      warp   = threadIdx.x >> 5;
+    uint32_t const lanes  = uint32_t(32 * (warp & 3)) << 16;
+    int            cur    = 0;  // dZ buffer of the current layer
+#pragma unroll 1
+    for (int l = Layers - 1; l >= 0; --l) {
+        int const K = in_dim(l), N = out_dim(l);
+        if (threadIdx.x == 0) {
+            __nv_bfloat16 const* w = s.net.w + weight_tile_offset(l);
+            if (l == 4) {
+                backward_mma<Width, Outputs>(tm.tmem, s.z[cur], acts[l], w, true, tm.mbar);
+            } else if (l > 0) {
+                backward_mma<Width, Width>(tm.tmem, s.z[cur], acts[l], w, true, tm.mbar);
+            } else {
+                backward_mma<Inputs, Width>(tm.tmem, s.z[cur], acts[l], w, false, tm.mbar);
+            }
+        }
+        if (!mbar_wait(tm.mbar, tm.phase)) {
+            *tm.error = 1u;
+        }
+        tm.phase ^= 1u;
+        tc_fence_after();
+        // dW: thread (row n = t % 128, half t / 128) reads K / 2 columns of the dW accumulator.
+        {
+            int const   n  = r;
+            int const   k0 = (threadIdx.x >> 7) * (K / 2);
+            float       v[32];
+            if (K == Width) {
+                tmem_ld32(tm.tmem + lanes + 64u + uint32_t(k0), v);
+            } else {
+                float v8[8];
+                tmem_ld8(tm.tmem + lanes + 64u + uint32_t(k0), v8);
+                float v8b[8];
+                tmem_ld8(tm.tmem + lanes + 64u + uint32_t(k0) + 8u, v8b);
+                for (int i = 0; i < 8; ++i) {
+                    v[i]     = v8[i];
+                    v[8 + i] = v8b[i];
+                }
+            }
+            if (n < N) {
+                float* const dst = pout + weight_offset(l) + n * K + k0;
+                for (int i = 0; i < K / 2; ++i) {
+                    dst[i] = v[i];
+                }
+            }
+        }
+        if (l > 0) {
+            // dZ_{l-1} = dA masked by the ReLU of layer l's input; bias gradients of layer l - 1.
+            int const nxt = cur ^ 1;
+            int const k0  = (threadIdx.x >> 7) * (K / 2);  // K = 64 here
+            float     v[32];
+            tmem_ld32(tm.tmem + lanes + uint32_t(k0), v);
+            for (int i = 0; i < 32; ++i) {
+                int const   k  = k0 + i;
+                float const dz = __bfloat162float(acts[l][tiled(r, k, K)]) > 0.f ? v[i] : 0.f;
+                s.z[nxt][tiled(r, k, Zw)] = __float2bfloat16(dz);
+                atomicAdd(&s.gb[bias_slot(l - 1) + k], dz);
+            }
+            fence_async_smem();
+            cur = nxt;
+        }
+        tc_fence_before();
+        __syncthreads();
+    }
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm.tmem), "r"(Train_tmem_columns));
+    }
+    for (int l = 0; l < Layers; ++l) {
+        for (int i = threadIdx.x; i < out_dim(l); i += Block) {
+            pout[bias_offset(l) + i] = s.gb[bias_slot(l) + i];
+        }
+    }
 }
 
 // grads[p] = sum over blocks of partial[b][p], in block order (deterministic).
@@ -184,7 +316,8 @@ int set_kernel_attributes() {
         int const bytes = int(tile_smem_bytes());
         cudaError_t e   = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         if (e == cudaSuccess) {
-            e = cudaFuncSetAttribute(k_gradients, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            e = cudaFuncSetAttribute(k_gradients_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(sizeof(Train_tc_smem)));
         }
         return int(e);
     }();
@@ -245,6 +378,14 @@ int Network::set_parameters(float const* host) {
     return cudaGetLastError();
 }
 
+bool Network::timed_out() const {
+    uint32_t flag = 0;
+    if (error_) {
+        cudaMemcpy(&flag, error_, sizeof(flag), cudaMemcpyDeviceToHost);
+    }
+    return flag != 0;
+}
+
 int Network::get_parameters(float* host) const {
     return cudaMemcpy(host, params_, Parameters * sizeof(float), cudaMemcpyDeviceToHost);
 }
@@ -288,8 +429,16 @@ int Network::gradients(float const* inputs, float const* dirs, float const* scal
         }
         partial_blocks_ = blocks;
     }
-    k_gradients<<<unsigned(blocks), Block, tile_smem_bytes(), stream>>>(wbf_, params_, inputs, dirs, scale, n,
-                                                                        partial_);
+    if (!error_) {
+        if (cudaError_t const e = cudaMalloc(&error_, sizeof(uint32_t))) {
+            return e;
+        }
+        if (cudaError_t const e = cudaMemset(error_, 0, sizeof(uint32_t))) {
+            return e;
+        }
+    }
+    k_gradients_tc<<<unsigned(blocks), Block, sizeof(Train_tc_smem), stream>>>(wbf_, params_, inputs, dirs, scale,
+                                                                               n, partial_, error_);
     k_reduce<<<(Parameters + 255) / 256, 256, 0, stream>>>(partial_, uint32_t(blocks), grads_);
     return cudaGetLastError();
 }
@@ -383,6 +532,9 @@ SPB_API int32_t spb_guide_gradients(float const* params, float const* inputs, fl
     }
     if (e == 0) {
         e = cudaMemcpy(gradient, net.gradient(), Parameters * sizeof(float), cudaMemcpyDeviceToHost);
+    }
+    if (e == 0 && net.timed_out()) {
+        return spb::fail(SPB_ERROR_CUDA, "spb_guide_gradients: a tensor-core completion wait ran out");
     }
     return cuda_status(e, "spb_guide_gradients");
 }

@@ -36,6 +36,9 @@ class Network {
     int adam(float lr, cudaStream_t stream);
 
     float const*         gradient() const { return grads_; }
+    // True once a tensor-core completion wait of forward() or gradients() ran out.
+    bool                 timed_out() const;
+    uint32_t*            error_flag() const { return error_; }
     __nv_bfloat16 const* weights() const { return wbf_; }
     float const*         parameters() const { return params_; }
 
