@@ -59,6 +59,8 @@ def parse_args():
                    help="skip the 1920x1080 many-instances, many-lights render measurement")
     p.add_argument("--no-volume", action="store_true",
                    help="skip the 64-view heterogeneous-volume render measurement")
+    p.add_argument("--no-guiding", action="store_true",
+                   help="skip the doorway time-to-relMSE measurement (plain MIS against path guiding)")
     return p.parse_args()
 
 
@@ -236,7 +238,8 @@ def run_reference_arm(args, world, rank):
 def measure_render(args, with_cpu):
     """Plain MIS path tracing through the su_* C API: the Cornell scene (512x512, 64 spp, with
     time to relMSE 0.01), the many-instances, many-lights scene (1920x1080, 256 spp, depth 12;
-    one warm-up frame, one timed frame) and the heterogeneous volume (64 views, 128 spp)."""
+    one warm-up frame, one timed frame), the heterogeneous volume (64 views, 128 spp) and the
+    doorway interior's time to relMSE 0.01, plain MIS against learned guiding (1280x720)."""
     from sprout_b200 import render_bench
 
     out = {"cornell": render_bench.measure("cornell", spp=args.render_spp, frames=3, convergence=True,
@@ -245,6 +248,8 @@ def measure_render(args, with_cpu):
         out["wavefront"] = render_bench.measure("wavefront", frames=1, cpu_reference=with_cpu)
     if not args.no_volume:
         out["volume"] = render_bench.measure_volume(views=64, spp=128, cpu_reference=with_cpu)
+    if not args.no_guiding:
+        out["guiding"] = render_bench.measure_guiding()
     return out
 
 

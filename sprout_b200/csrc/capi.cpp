@@ -595,6 +595,9 @@ SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
         if (pt) {
             s.min_bounces = uint32_t(spb::json::number_or(pt->find("min_bounces"), s.min_bounces));
             s.max_bounces = uint32_t(spb::json::number_or(pt->find("max_bounces"), s.max_bounces));
+            // "seed": the sample streams' seed (this renderer's extension, default 0), for
+            // statistically independent renders of one scene
+            s.seed = uint32_t(spb::json::number_or(pt->find("seed"), s.seed));
             // "guiding": true, or an object of the Settings guide fields (this renderer's
             // extension; the reference ignores the key)
             if (spb::json::Value const* g = pt->find("guiding")) {
@@ -607,6 +610,8 @@ SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
                     s.record_depth   = uint32_t(spb::json::number_or(g->find("record_depth"), s.record_depth));
                     s.guide_seed     = uint32_t(spb::json::number_or(g->find("seed"), s.guide_seed));
                     s.guide_pass_spp = uint32_t(spb::json::number_or(g->find("pass_spp"), s.guide_pass_spp));
+                    s.guide_train_spp = uint32_t(spb::json::number_or(g->find("train_spp"), s.guide_train_spp));
+                    s.guide_depth     = uint32_t(spb::json::number_or(g->find("depth"), s.guide_depth));
                 }
                 s.guide_fraction = std::clamp(s.guide_fraction, 0.f, 0.95f);
                 s.record_depth   = std::clamp(s.record_depth, 1u, 8u);

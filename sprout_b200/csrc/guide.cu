@@ -5,6 +5,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -63,13 +64,15 @@ __global__ void __launch_bounds__(Block) k_forward(__nv_bfloat16 const* wbf, flo
     }
 }
 
-// ---- training tile on the tensor cores ----
-// Forward as in inference (keeping every layer's input), the loss gradient at the outputs, then
-// per layer l from the last: dW_l = dZ_l^T A_l (M = 128 over the neurons, padded with zero
-// rows; both operands MN-major) and dA_l = dZ_l W_l (M = 128 over the samples; dZ K-major, W
-// MN-major) into two TMEM accumulators, committed together; dZ_{l-1} = dA_l masked by ReLU.
-// dZ is held as BF16 in a 128 x 128 tiled buffer whose columns past the layer's width stay 0.
-// Bias gradients are summed in FP32 (shared-memory atomics) before the BF16 rounding.
+// ---- training on the tensor cores ----
+// A persistent kernel: one block per SM walks tiles of 128 samples.  Per tile: forward as in
+// inference (keeping every layer's input), the loss gradient at the outputs, then per layer l
+// from the last: dW_l += dZ_l^T A_l (M = 128 over the neurons, padded with zero rows; both
+// operands MN-major) and dA_l = dZ_l W_l (M = 128 over the samples; dZ K-major, W MN-major),
+// committed together; dZ_{l-1} = dA_l masked by ReLU.  Every layer's dW accumulator stays in
+// tensor memory across the block's tiles and is written out once, as the block's partial sum.
+// dZ is held as BF16 in a 128 x 128 tiled buffer whose columns past the layer's width stay 0;
+// bias gradients are summed in FP32 before the rounding (warp reductions, then shared memory).
 constexpr int Zw = 128;  // dZ buffer width
 
 struct Train_tc_smem {
@@ -79,25 +82,48 @@ struct Train_tc_smem {
     __nv_bfloat16 z[2][Tile * Zw];
     float         out[Tile * Out_stride];
     float         gb[Bias_count];
+    float         red[2][8][32];  // per-warp column sums, alternating between layers
     uint64_t      mbar;
     uint32_t      tmem_slot;
 };
 
-constexpr uint32_t Train_tmem_columns = 128;  // [0, 64): dA and forward; [64, 128): dW
+// TMEM columns: [0, 64) the forward / dA accumulator; then each layer's dW accumulator.
+constexpr uint32_t Train_tmem_columns = 512;
+__host__ __device__ constexpr uint32_t dw_column(int l) {
+    return l == 0 ? 64u : 96u + 64u * uint32_t(l - 1);  // 64 (32 wide), 96, 160, 224, 288 (64 wide)
+}
 
-// Issues dW (and dA when with_da) for layer l; thread 0 only.
+// Sum over a warp's 32 lanes (rows) of each of its 32 registers (columns), by recursive halving:
+// afterwards v[0] of lane j holds the total of column j.
+__device__ inline float warp_column_sums(float v[32]) {
+    int const lane = threadIdx.x & 31;
+#pragma unroll
+    for (int w = 16; w >= 1; w >>= 1) {
+        bool const upper = lane & w;
+#pragma unroll
+        for (int i = 0; i < w; ++i) {
+            float const send = upper ? v[i] : v[i + w];
+            float const keep = upper ? v[i + w] : v[i];
+            v[i]             = keep + __shfl_xor_sync(0xFFFFFFFFu, send, w);
+        }
+    }
+    return v[0];
+}
+
+// Issues the layer's dW (accumulating unless `fresh`) and, when with_da, its dA; thread 0.
 template <int K, int N>
-__device__ inline void backward_mma(uint32_t tmem, __nv_bfloat16 const* z, __nv_bfloat16 const* act,
-                                    __nv_bfloat16 const* w, bool with_da, uint32_t mbar) {
+__device__ inline void backward_mma(uint32_t tmem, uint32_t dw_col, __nv_bfloat16 const* z, __nv_bfloat16 const* act,
+                                    __nv_bfloat16 const* w, bool with_da, bool fresh, uint32_t mbar) {
     constexpr int P = (N + 15) & ~15;
     tc_fence_after();
     uint32_t const zs = smem_u32(z), as = smem_u32(act), ws = smem_u32(w);
-    // dW[n][k] = sum_r dZ[r][n] A[r][k]: A operand dZ^T (MN-major: n groups 128 B apart, r groups
+    // dW[n][k] += sum_r dZ[r][n] A[r][k]: A operand dZ^T (MN-major: n groups 128 B apart, r groups
     // Zw * 16 B apart), B operand A_l (MN-major: k groups 128 B, r groups K * 16 B).
 #pragma unroll
     for (int s = 0; s < Tile / 16; ++s) {
-        umma_bf16(tmem + 64u, operand_desc(zs + 2u * Zw * 16u * s, Zw * 16u, 128u),
-                  operand_desc(as + 2u * K * 16u * s, K * 16u, 128u), instr_desc(Tile, K, true, true), s > 0);
+        umma_bf16(tmem + dw_col, operand_desc(zs + 2u * Zw * 16u * s, Zw * 16u, 128u),
+                  operand_desc(as + 2u * K * 16u * s, K * 16u, 128u), instr_desc(Tile, K, true, true),
+                  (fresh && s == 0) ? 0u : 1u);
     }
     if (with_da) {
         // dA[r][k] = sum_n dZ[r][n] W[n][k]: A operand dZ (K-major over n), B operand W_l
@@ -113,20 +139,16 @@ __device__ inline void backward_mma(uint32_t tmem, __nv_bfloat16 const* z, __nv_
 
 __global__ void __launch_bounds__(Block) k_gradients_tc(__nv_bfloat16 const* wbf, float const* params,
                                                         float const* in, float const* dirs, float const* scale,
-                                                        uint64_t n, float* partial, uint32_t* error) {
+                                                        uint64_t n, uint32_t tiles, float* partial, uint32_t* error) {
     extern __shared__ __align__(16) unsigned char raw[];
     Train_tc_smem& s = *reinterpret_cast<Train_tc_smem*>(raw);
     load_net(s.net, wbf, params);
-    uint64_t const base = uint64_t(blockIdx.x) * Tile;
-    load_inputs(s.a0, in, base, n);
     for (int i = threadIdx.x; i < 2 * Tile * Zw / 8; i += Block) {
         reinterpret_cast<uint4*>(s.z)[i] = make_uint4(0u, 0u, 0u, 0u);
     }
     for (int i = threadIdx.x; i < Bias_count; i += Block) {
         s.gb[i] = 0.f;
     }
-    fence_async_smem();
-    // TMEM: 128 columns for this kernel (the forward uses the first 64)
     if (threadIdx.x < 32) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem_slot)),
                      "r"(Train_tmem_columns));
@@ -142,101 +164,142 @@ __global__ void __launch_bounds__(Block) k_gradients_tc(__nv_bfloat16 const* wbf
     Tmem_tile tm{s.tmem_slot, smem_u32(&s.mbar), 0u, error};
 
     __nv_bfloat16* const acts[Layers] = {s.a0, s.a[0], s.a[1], s.a[2], s.a[3]};
-    forward_tc(s.net, acts, s.out, tm);
-
-    // Loss gradient at the outputs -> dZ_4 (BF16, columns 0..39; 40..47 stay 0), bias grads.
-    int const r = threadIdx.x & (Tile - 1);
-    if (threadIdx.x < Tile) {
-        uint64_t const g = base + r;
-        float          gr[Outputs];
-        if (g < n) {
-            output_gradient(s.out + r * Out_stride, shading::v3(dirs[3 * g], dirs[3 * g + 1], dirs[3 * g + 2]),
-                            scale[g], gr);
-        } else {
-            for (int j = 0; j < Outputs; ++j) {
-                gr[j] = 0.f;
-            }
-        }
-        for (int j = 0; j < Outputs; ++j) {
-            s.z[0][tiled(r, j, Zw)] = __float2bfloat16(gr[j]);
-            atomicAdd(&s.gb[bias_slot(4) + j], gr[j]);
-        }
-    }
-    fence_async_smem();
-    tc_fence_before();
-    __syncthreads();
-
-    float* const   pout   = partial + uint64_t(blockIdx.x) * Parameters;
-    int const      warp   = threadIdx.x >> 5;
-    uint32_t const lanes  = uint32_t(32 * (warp & 3)) << 16;
-    int            cur    = 0;  // dZ buffer of the current layer
+    int const            r     = threadIdx.x & (Tile - 1);
+    int const            warp  = threadIdx.x >> 5;
+    int const            lane  = threadIdx.x & 31;
+    uint32_t const       lanes = uint32_t(32 * (warp & 3)) << 16;
+    bool                 fresh = true;  // no dW accumulated yet
 #pragma unroll 1
-    for (int l = Layers - 1; l >= 0; --l) {
-        int const K = in_dim(l), N = out_dim(l);
-        if (threadIdx.x == 0) {
-            __nv_bfloat16 const* w = s.net.w + weight_tile_offset(l);
-            if (l == 4) {
-                backward_mma<Width, Outputs>(tm.tmem, s.z[cur], acts[l], w, true, tm.mbar);
-            } else if (l > 0) {
-                backward_mma<Width, Width>(tm.tmem, s.z[cur], acts[l], w, true, tm.mbar);
-            } else {
-                backward_mma<Inputs, Width>(tm.tmem, s.z[cur], acts[l], w, false, tm.mbar);
-            }
-        }
-        if (!mbar_wait(tm.mbar, tm.phase)) {
-            *tm.error = 1u;
-        }
-        tm.phase ^= 1u;
-        tc_fence_after();
-        // dW: thread (row n = t % 128, half t / 128) reads K / 2 columns of the dW accumulator.
-        {
-            int const   n  = r;
-            int const   k0 = (threadIdx.x >> 7) * (K / 2);
-            float       v[32];
-            if (K == Width) {
-                tmem_ld32(tm.tmem + lanes + 64u + uint32_t(k0), v);
-            } else {
-                float v8[8];
-                tmem_ld8(tm.tmem + lanes + 64u + uint32_t(k0), v8);
-                float v8b[8];
-                tmem_ld8(tm.tmem + lanes + 64u + uint32_t(k0) + 8u, v8b);
-                for (int i = 0; i < 8; ++i) {
-                    v[i]     = v8[i];
-                    v[8 + i] = v8b[i];
-                }
-            }
-            if (n < N) {
-                float* const dst = pout + weight_offset(l) + n * K + k0;
-                for (int i = 0; i < K / 2; ++i) {
-                    dst[i] = v[i];
-                }
-            }
-        }
-        if (l > 0) {
-            // dZ_{l-1} = dA masked by the ReLU of layer l's input; bias gradients of layer l - 1.
-            int const nxt = cur ^ 1;
-            int const k0  = (threadIdx.x >> 7) * (K / 2);  // K = 64 here
-            float     v[32];
-            tmem_ld32(tm.tmem + lanes + uint32_t(k0), v);
-            for (int i = 0; i < 32; ++i) {
-                int const   k  = k0 + i;
-                float const dz = __bfloat162float(acts[l][tiled(r, k, K)]) > 0.f ? v[i] : 0.f;
-                s.z[nxt][tiled(r, k, Zw)] = __float2bfloat16(dz);
-                atomicAdd(&s.gb[bias_slot(l - 1) + k], dz);
-            }
-            fence_async_smem();
-            cur = nxt;
-        }
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        uint64_t const base = uint64_t(tile) * Tile;
+        load_inputs(s.a0, in, base, n);
+        fence_async_smem();
         tc_fence_before();
         __syncthreads();
+        forward_tc(s.net, acts, s.out, tm);
+
+        // Loss gradient at the outputs -> dZ_4 (BF16, columns 0..39; 40..47 stay 0) and, in FP32,
+        // into `out` for the bias gradient.
+        if (threadIdx.x < Tile) {
+            uint64_t const g = base + r;
+            float          gr[Outputs];
+            if (g < n) {
+                output_gradient(s.out + r * Out_stride,
+                                shading::v3(dirs[3 * g], dirs[3 * g + 1], dirs[3 * g + 2]), scale[g], gr);
+            } else {
+                for (int j = 0; j < Outputs; ++j) {
+                    gr[j] = 0.f;
+                }
+            }
+            for (int j = 0; j < Outputs; ++j) {
+                s.z[0][tiled(r, j, Zw)]  = __float2bfloat16(gr[j]);
+                s.out[r * Out_stride + j] = gr[j];
+            }
+            // columns the previous tile's hidden-layer dZ left behind
+            for (int j = Outputs; j < Width; ++j) {
+                s.z[0][tiled(r, j, Zw)] = __float2bfloat16(0.f);
+            }
+        }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+
+        int cur = 0;  // dZ buffer of the current layer
+#pragma unroll 1
+        for (int l = Layers - 1; l >= 0; --l) {
+            if (threadIdx.x == 0) {
+                __nv_bfloat16 const* w = s.net.w + weight_tile_offset(l);
+                if (l == 4) {
+                    backward_mma<Width, Outputs>(tm.tmem, dw_column(l), s.z[cur], acts[l], w, true, fresh, tm.mbar);
+                } else if (l > 0) {
+                    backward_mma<Width, Width>(tm.tmem, dw_column(l), s.z[cur], acts[l], w, true, fresh, tm.mbar);
+                } else {
+                    backward_mma<Inputs, Width>(tm.tmem, dw_column(l), s.z[cur], acts[l], w, false, fresh, tm.mbar);
+                }
+            }
+            if (l == Layers - 1 && threadIdx.x < Outputs) {
+                // output bias gradient, while the tensor cores work
+                float acc = 0.f;
+                for (int q = 0; q < Tile; ++q) {
+                    acc += s.out[q * Out_stride + threadIdx.x];
+                }
+                s.gb[bias_slot(4) + threadIdx.x] += acc;
+            }
+            if (!mbar_wait(tm.mbar, tm.phase)) {
+                *tm.error = 1u;
+            }
+            tm.phase ^= 1u;
+            tc_fence_after();
+            if (l > 0) {
+                // dZ_{l-1} = dA masked by the ReLU of layer l's input (K = 64 columns: thread
+                // row r, half t / 128).
+                int const nxt = cur ^ 1;
+                int const k0  = (threadIdx.x >> 7) * (Width / 2);
+                float     v[32];
+                tmem_ld32(tm.tmem + lanes + uint32_t(k0), v);
+#pragma unroll
+                for (int j = 0; j < 32; j += 8) {
+                    __nv_bfloat162 h[4];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        if (!(__bfloat162float(acts[l][tiled(r, k0 + j + q, Width)]) > 0.f)) {
+                            v[j + q] = 0.f;
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        h[q] = __floats2bfloat162_rn(v[j + 2 * q], v[j + 2 * q + 1]);
+                    }
+                    *reinterpret_cast<uint4*>(&s.z[nxt][tiled(r, k0 + j, Zw)]) = *reinterpret_cast<uint4*>(h);
+                }
+                fence_async_smem();
+                s.red[l & 1][warp][lane] = warp_column_sums(v);
+                cur = nxt;
+            }
+            tc_fence_before();
+            __syncthreads();
+            if (l > 0 && threadIdx.x < Width) {
+                // bias gradient of layer l - 1: column c = t, from the four warps on its half
+                int const c = threadIdx.x, h = c >> 5;
+                float const(&red)[8][32] = s.red[l & 1];
+                s.gb[bias_slot(l - 1) + c] += red[4 * h][c & 31] + red[4 * h + 1][c & 31] + red[4 * h + 2][c & 31] +
+                                              red[4 * h + 3][c & 31];
+            }
+        }
+        fresh = false;
     }
-    if (threadIdx.x < 32) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm.tmem), "r"(Train_tmem_columns));
+
+    // The block's partial sums: dW from tensor memory (thread row n, half of the columns),
+    // biases from shared memory.
+    float* const pout = partial + uint64_t(blockIdx.x) * Parameters;
+    __syncthreads();
+#pragma unroll 1
+    for (int l = 0; l < Layers; ++l) {
+        int const K  = in_dim(l), N = out_dim(l);
+        int const k0 = (threadIdx.x >> 7) * (K / 2);
+        float     v[32];
+        if (K == Width) {
+            tmem_ld32(tm.tmem + lanes + dw_column(l) + uint32_t(k0), v);
+        } else {
+            tmem_ld8(tm.tmem + lanes + dw_column(l) + uint32_t(k0), v);
+            tmem_ld8(tm.tmem + lanes + dw_column(l) + uint32_t(k0) + 8u, v + 8);
+        }
+        if (r < N) {
+            float* const dst = pout + weight_offset(l) + r * K + k0;
+            for (int i = 0; i < K / 2; ++i) {
+                dst[i] = fresh ? 0.f : v[i];
+            }
+        }
     }
     for (int l = 0; l < Layers; ++l) {
         for (int i = threadIdx.x; i < out_dim(l); i += Block) {
             pout[bias_offset(l) + i] = s.gb[bias_slot(l) + i];
         }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm.tmem), "r"(Train_tmem_columns));
     }
 }
 
@@ -437,9 +500,17 @@ int Network::gradients(float const* inputs, float const* dirs, float const* scal
             return e;
         }
     }
-    k_gradients_tc<<<unsigned(blocks), Block, sizeof(Train_tc_smem), stream>>>(wbf_, params_, inputs, dirs, scale,
-                                                                               n, partial_, error_);
-    k_reduce<<<(Parameters + 255) / 256, 256, 0, stream>>>(partial_, uint32_t(blocks), grads_);
+    // one persistent block per SM (at most one per tile)
+    static int const sms = [] {
+        int dev = 0, count = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+        return std::max(count, 1);
+    }();
+    uint32_t const grid = uint32_t(std::min<uint64_t>(blocks, uint64_t(sms)));
+    k_gradients_tc<<<grid, Block, sizeof(Train_tc_smem), stream>>>(wbf_, params_, inputs, dirs, scale, n,
+                                                                   uint32_t(blocks), partial_, error_);
+    k_reduce<<<(Parameters + 255) / 256, 256, 0, stream>>>(partial_, grid, grads_);
     return cudaGetLastError();
 }
 

@@ -173,12 +173,24 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float v[8]) {
     }
 }
 
+// Stores the 40 outputs of sample r into shared memory (Out_stride floats per sample).
+struct Smem_outputs {
+    float* out;
+    __device__ void operator()(int r, float const (&v)[Outputs]) const {
+#pragma unroll
+        for (int n = 0; n < Outputs; ++n) {
+            out[r * Out_stride + n] = v[n];
+        }
+    }
+};
+
 // One layer on the tensor cores.  Precondition: A and W are in shared memory, every writer
 // fenced its stores for the async proxy, and a block barrier (after tc_fence_before) followed.
-// Ends with the results stored and a barrier.
-template <int K, int N, bool Last>
+// Ends with the results stored (the last layer: store(r, outputs) by thread r < Tile) and a
+// barrier.
+template <int K, int N, bool Last, class Store = Smem_outputs>
 __device__ inline void layer_forward_tc(__nv_bfloat16 const* A, __nv_bfloat16 const* W, float const* b,
-                                        __nv_bfloat16* act, float* out, Tmem_tile& tm) {
+                                        __nv_bfloat16* act, Store const& store, Tmem_tile& tm) {
     constexpr int P = (N + 15) & ~15;
     if (threadIdx.x == 0) {
         tc_fence_after();
@@ -199,15 +211,16 @@ __device__ inline void layer_forward_tc(__nv_bfloat16 const* A, __nv_bfloat16 co
     int const      warp  = threadIdx.x >> 5;
     int const      r     = threadIdx.x & (Tile - 1);
     uint32_t const lanes = uint32_t(32 * (warp & 3)) << 16;
-    if (Last) {
+    if constexpr (Last) {
         if (threadIdx.x < Tile) {
-            float v[40];
+            float v[Outputs];
             tmem_ld32(tm.tmem + lanes, v);
             tmem_ld8(tm.tmem + lanes + 32u, v + 32);
 #pragma unroll
-            for (int n = 0; n < N; ++n) {
-                out[r * Out_stride + n] = v[n] + b[n];
+            for (int n = 0; n < Outputs; ++n) {
+                v[n] += b[n];
             }
+            store(r, v);
         }
     } else {
         int const n0 = (threadIdx.x >> 7) * (N / 2);  // N = 64: 32 columns per thread
@@ -230,14 +243,21 @@ __device__ inline void layer_forward_tc(__nv_bfloat16 const* A, __nv_bfloat16 co
 }
 
 // Forward through all layers: acts[0] holds the tile's inputs (128 x 32, tiled); acts[1..4]
-// receive the hidden activations (acts may alternate between two buffers), out the 40 outputs
-// per sample (128 rows of Out_stride floats).  Same entry conditions as layer_forward_tc.
+// receive the hidden activations (acts may alternate between two buffers); store(r, outputs)
+// takes each sample's 40 outputs.  Same entry conditions as layer_forward_tc.
+template <class Store>
+__device__ inline void forward_tc(Net_smem const& s, __nv_bfloat16* const acts[Layers], Store const& store,
+                                  Tmem_tile& tm) {
+    layer_forward_tc<Inputs, Width, false>(acts[0], s.w + weight_tile_offset(0), s.b + bias_slot(0), acts[1], store, tm);
+    layer_forward_tc<Width, Width, false>(acts[1], s.w + weight_tile_offset(1), s.b + bias_slot(1), acts[2], store, tm);
+    layer_forward_tc<Width, Width, false>(acts[2], s.w + weight_tile_offset(2), s.b + bias_slot(2), acts[3], store, tm);
+    layer_forward_tc<Width, Width, false>(acts[3], s.w + weight_tile_offset(3), s.b + bias_slot(3), acts[4], store, tm);
+    layer_forward_tc<Width, Outputs, true>(acts[4], s.w + weight_tile_offset(4), s.b + bias_slot(4), nullptr, store, tm);
+}
+
+// The same with the outputs stored in shared memory (128 rows of Out_stride floats).
 __device__ inline void forward_tc(Net_smem const& s, __nv_bfloat16* const acts[Layers], float* out, Tmem_tile& tm) {
-    layer_forward_tc<Inputs, Width, false>(acts[0], s.w + weight_tile_offset(0), s.b + bias_slot(0), acts[1], nullptr, tm);
-    layer_forward_tc<Width, Width, false>(acts[1], s.w + weight_tile_offset(1), s.b + bias_slot(1), acts[2], nullptr, tm);
-    layer_forward_tc<Width, Width, false>(acts[2], s.w + weight_tile_offset(2), s.b + bias_slot(2), acts[3], nullptr, tm);
-    layer_forward_tc<Width, Width, false>(acts[3], s.w + weight_tile_offset(3), s.b + bias_slot(3), acts[4], nullptr, tm);
-    layer_forward_tc<Width, Outputs, true>(acts[4], s.w + weight_tile_offset(4), s.b + bias_slot(4), nullptr, out, tm);
+    forward_tc(s, acts, Smem_outputs{out}, tm);
 }
 
 // TMEM columns for one accumulator tile (64 FP32 columns, a power of two >= 32).

@@ -114,10 +114,14 @@ struct Paths {
     float4*   sh2_d;
     float4*   sh2_L;
     float4*   L2;
-    // Path guiding: the network's 40 outputs for the path's current vertex (guide_ok: valid),
-    // the training records of its first record_depth vertices (5 float4 each: position and
-    // normal x | normal yz, wo xy | wo z, wi | throughput | radiance mark, w = 1 once marked)
-    // and the record awaiting its radiance mark.
+    // Path guiding, indexed by position in the current extension queue: the network inputs as
+    // BF16 tiles of 128 entries in the tensor cores' operand order (guide_in), the predicted
+    // mixture (guide_out: 8 float4 of unit mean and concentration, then the 8 weights) and
+    // whether the entry is guided (guide_ok).  Indexed by path: the training records of its
+    // first record_depth vertices (5 float4 each: position and normal x | normal yz, wo xy |
+    // wo z, wi | throughput | radiance mark, w = 1 once marked) and the record awaiting its
+    // radiance mark.
+    __nv_bfloat16* guide_in;
     float*    guide_out;
     uint8_t*  guide_ok;
     float4*   rec;
@@ -147,6 +151,7 @@ struct Wave {
     uint32_t guiding;         // 1: sample the guide's mixture at surface vertices
     float    guide_fraction;  // its share of continuation directions
     uint32_t record_depth;    // vertices per path recorded for training (0: none)
+    uint32_t guide_depth;     // vertices of depth below this are guided
     float4   bounds_lo;       // scene box, for the guide's position encoding
     float4   bounds_inv;      // 1 / its extent
 };
@@ -230,6 +235,12 @@ __device__ __forceinline__ uint32_t append(uint32_t* counter, bool want) {
     return base + __popc(mask & ((1u << lane) - 1u));
 }
 
+// Samples are taken over the image plus a border of the filter's integer radius, whose
+// filtered contributions reach the edge pixels (the reference's tile queue extends the edge
+// tiles by filter_radius_int, tile_queue.cpp:54-68; sample streams per bordered pixel as in
+// rendering_worker.cpp:93-104).
+constexpr int Film_border = 1;
+
 // ---- generate: camera rays (Perspective::generate_ray, camera_perspective.cpp:47-80) ----
 __global__ void k_generate(Cam cam, Wave wave, Paths p, uint32_t* queue, uint32_t* counters,
                            uint32_t num_paths) {
@@ -240,11 +251,12 @@ __global__ void k_generate(Cam cam, Wave wave, Paths p, uint32_t* queue, uint32_
     if (i >= num_paths) {
         return;
     }
-    uint32_t const pixels = cam.w * cam.h;
+    uint32_t const bw     = cam.w + 2 * Film_border;
+    uint32_t const pixels = bw * (cam.h + 2 * Film_border);
     uint32_t const pixel  = i % pixels;
     uint32_t const slot   = i / pixels;
-    uint32_t const x      = pixel % cam.w;
-    uint32_t const y      = pixel / cam.w;
+    int const      x      = int(pixel % bw) - Film_border;
+    int const      y      = int(pixel / bw) - Film_border;
 
     Rng rng;
     rng.start(wave.seed, uint64_t(pixel) + uint64_t(wave.first_sample + slot) * pixels);
@@ -940,17 +952,15 @@ __device__ __forceinline__ void store_shadow(Paths const& p, uint32_t path, bool
 }
 
 // ---- guide: the network's mixture for every queued surface hit (before shading) ----
-// One tile of 128 queue entries per block: encodes the hit (position in the scene box,
-// geometric normal facing the ray's origin, outgoing direction), runs the network
-// (guide_mlp.cuh) and stores its 40 outputs for k_shade.  Hits on other than Substitute
-// surfaces are marked invalid.
+// Two kernels per bounce.  k_guide_encode, one thread per queue entry, encodes the hit
+// (position in the scene box, geometric normal facing the ray's origin, outgoing direction)
+// into guide_in and marks the entry guided (a Substitute surface below the guided depth).
+// k_guide streams those tiles through the network on the tensor cores (guide_mlp.cuh) and
+// stores each entry's mixture at its queue position, where k_shade reads it.
 struct Infer_smem {
     guide::Net_smem net;
-    __nv_bfloat16   a0[guide::Tile * guide::Inputs];
     __nv_bfloat16   x[guide::Tile * guide::Width];
-    __nv_bfloat16   y[guide::Tile * guide::Width];
-    float           out[guide::Tile * guide::Out_stride];
-    uint32_t        path[guide::Tile];
+    __nv_bfloat16   y[guide::Tile * guide::Width];  // its first 8 KB also take the tile's inputs
     uint64_t        mbar;       // tensor-core completion barrier
     uint32_t        tmem_slot;  // accumulator address from tcgen05.alloc
 };
@@ -976,52 +986,105 @@ __device__ __forceinline__ V3 box_coordinates(Wave const& wave, V3 pos) {
               (pos.z - wave.bounds_lo.z) * wave.bounds_inv.z);
 }
 
-__global__ void __launch_bounds__(guide::Block)
-    k_guide(Scene_gpu s, Wave wave, Paths p, uint32_t const* __restrict__ queue,
-            uint32_t const* __restrict__ count, __nv_bfloat16 const* __restrict__ wbf,
+// One queue entry per thread: its inputs as row q % 128 of tile q / 128 (entries past the
+// queue's end, up to the tile boundary, get zeros).
+__global__ void __launch_bounds__(256)
+    k_guide_encode(Scene_gpu s, Wave wave, Paths p, uint32_t const* __restrict__ queue,
+                   uint32_t const* __restrict__ count) {
+    uint32_t const q   = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t const num = *count;
+    if (q >= (num + guide::Tile - 1) / guide::Tile * guide::Tile) {
+        return;
+    }
+    float in[guide::Inputs];
+    bool  ok = false;
+    if (q < num) {
+        uint32_t const path  = queue[q];
+        uint32_t const id    = p.hit_id[path];
+        uint32_t const depth = (p.info[path] >> 8) & 0xFFu;
+        if (id != gpu::Miss && depth < wave.guide_depth &&
+            s.materials[s.tri_info[id].w].type == shading::Type_substitute) {
+            V3 pos, geo_n, wo;
+            hit_frame(s, p, path, id, pos, geo_n, wo);
+            guide::encode(box_coordinates(wave, pos), geo_n, wo, in);
+            ok = true;
+        }
+        p.guide_ok[q] = ok ? 1 : 0;
+    }
+    __nv_bfloat16* const tile = p.guide_in + size_t(q / guide::Tile) * guide::Tile * guide::Inputs;
+    int const            r    = int(q % guide::Tile);
+#pragma unroll
+    for (int k = 0; k < guide::Inputs; k += 8) {
+        __nv_bfloat162 h[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            h[j] = __floats2bfloat162_rn(ok ? in[k + 2 * j] : 0.f, ok ? in[k + 2 * j + 1] : 0.f);
+        }
+        *reinterpret_cast<uint4*>(tile + guide::tiled(r, k, guide::Inputs)) = *reinterpret_cast<uint4*>(h);
+    }
+}
+
+// Stores entry base + r's mixture (guide::mixture of the 40 outputs) at its queue position:
+// 8 float4 (unit mean, concentration), then the 8 weights; consecutive rows are consecutive
+// 160-byte records, so a warp's stores are contiguous.
+struct Guide_outputs {
+    float*   guide_out;
+    uint32_t base;
+    uint32_t num;
+    __device__ void operator()(int r, float const (&v)[guide::Outputs]) const {
+        uint32_t const q = base + uint32_t(r);
+        if (q >= num) {
+            return;
+        }
+        guide::Lobe lobes[guide::Lobes];
+        guide::mixture(v, lobes);
+        float4* const dst = reinterpret_cast<float4*>(guide_out + size_t(q) * guide::Outputs);
+#pragma unroll
+        for (int j = 0; j < guide::Lobes; ++j) {
+            dst[j] = make_float4(lobes[j].mu.x, lobes[j].mu.y, lobes[j].mu.z, lobes[j].kappa);
+        }
+        dst[8] = make_float4(lobes[0].weight, lobes[1].weight, lobes[2].weight, lobes[3].weight);
+        dst[9] = make_float4(lobes[4].weight, lobes[5].weight, lobes[6].weight, lobes[7].weight);
+    }
+};
+
+// Persistent: each block loads the network once, then walks tiles, reading the next tile's
+// 8 KB of inputs into registers while the current one is on the tensor cores.
+__global__ void __launch_bounds__(guide::Block, 3)
+    k_guide(Paths p, uint32_t const* __restrict__ count, __nv_bfloat16 const* __restrict__ wbf,
             float const* __restrict__ params, uint32_t* error) {
     extern __shared__ __align__(16) unsigned char raw[];
-    Infer_smem&    m    = *reinterpret_cast<Infer_smem*>(raw);
-    uint32_t const num  = *count;
-    uint32_t const base = blockIdx.x * guide::Tile;
-    if (base >= num) {
+    Infer_smem&    m     = *reinterpret_cast<Infer_smem*>(raw);
+    uint32_t const num   = *count;
+    uint32_t const tiles = (num + guide::Tile - 1) / guide::Tile;
+    if (blockIdx.x >= tiles) {
         return;  // the whole block: no barrier is skipped by only some threads
     }
+    constexpr int Tile_uint4 = guide::Tile * guide::Inputs * 2 / 16;  // 512
+    static_assert(Tile_uint4 == 2 * guide::Block, "two 16-byte loads per thread per tile");
+    uint4 const* const src = reinterpret_cast<uint4 const*>(p.guide_in);
+    uint4 n0 = src[size_t(blockIdx.x) * Tile_uint4 + threadIdx.x];
+    uint4 n1 = src[size_t(blockIdx.x) * Tile_uint4 + guide::Block + threadIdx.x];
     guide::load_net(m.net, wbf, params);
-    if (threadIdx.x < guide::Tile) {
-        uint32_t const q    = base + threadIdx.x;
-        uint32_t       path = 0xFFFFFFFFu;
-        float          in[guide::Inputs];
-        bool           ok = false;
-        if (q < num) {
-            path              = queue[q];
-            uint32_t const id = p.hit_id[path];
-            if (id != gpu::Miss && s.materials[s.tri_info[id].w].type == shading::Type_substitute) {
-                V3 pos, geo_n, wo;
-                hit_frame(s, p, path, id, pos, geo_n, wo);
-                guide::encode(box_coordinates(wave, pos), geo_n, wo, in);
-                ok = true;
-            }
-            p.guide_ok[path] = ok ? 1 : 0;
-        }
-        for (int k = 0; k < guide::Inputs; ++k) {
-            m.a0[guide::tiled(threadIdx.x, k, guide::Inputs)] = __float2bfloat16(ok ? in[k] : 0.f);
-        }
-        m.path[threadIdx.x] = ok ? path : 0xFFFFFFFFu;
-    }
-    guide::fence_async_smem();
     guide::Tmem_tile tm = guide::tc_setup(&m.tmem_slot, &m.mbar, error);
-    __nv_bfloat16* const acts[guide::Layers] = {m.a0, m.x, m.y, m.x, m.y};
-    guide::forward_tc(m.net, acts, m.out, tm);
-    guide::tc_teardown(tm);
-    for (int i = threadIdx.x; i < guide::Tile * guide::Outputs; i += guide::Block) {
-        int const      r    = i / guide::Outputs;
-        int const      j    = i % guide::Outputs;
-        uint32_t const path = m.path[r];
-        if (path != 0xFFFFFFFFu) {
-            p.guide_out[size_t(path) * guide::Outputs + j] = m.out[r * guide::Out_stride + j];
+    __nv_bfloat16* const acts[guide::Layers] = {m.y, m.x, m.y, m.x, m.y};
+    uint4* const         a0 = reinterpret_cast<uint4*>(m.y);
+#pragma unroll 1
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        a0[threadIdx.x]               = n0;
+        a0[guide::Block + threadIdx.x] = n1;
+        uint32_t const next = tile + gridDim.x;
+        if (next < tiles) {
+            n0 = src[size_t(next) * Tile_uint4 + threadIdx.x];
+            n1 = src[size_t(next) * Tile_uint4 + guide::Block + threadIdx.x];
         }
+        guide::fence_async_smem();
+        guide::tc_fence_before();
+        __syncthreads();
+        // ends with a barrier, after which y may take the next inputs
+        guide::forward_tc(m.net, acts, Guide_outputs{p.guide_out, tile * guide::Tile, num}, tm);
     }
+    guide::tc_teardown(tm);
 }
 
 // ---- shade: one path vertex ----
@@ -1234,20 +1297,26 @@ __global__ void __launch_bounds__(Shade_block)
                 // The guide's mixture for this vertex (k_guide); continuation directions come
                 // from it with probability gf, else from the BSDF, and every pdf the MIS
                 // weights use is the combination of both.
-                bool const  guided = wave.guiding && p.guide_ok[path];
+                bool const  guided = wave.guiding && depth < wave.guide_depth && p.guide_ok[i];
                 float const gf     = guided ? wave.guide_fraction : 0.f;
                 guide::Lobe lobes[guide::Lobes];
                 if (guided) {
-                    float        o[guide::Outputs];
-                    float4 const* src = reinterpret_cast<float4 const*>(p.guide_out + size_t(path) * guide::Outputs);
-                    for (int k = 0; k < guide::Outputs / 4; ++k) {
-                        float4 const v = src[k];
-                        o[4 * k]       = v.x;
-                        o[4 * k + 1]   = v.y;
-                        o[4 * k + 2]   = v.z;
-                        o[4 * k + 3]   = v.w;
+                    float4 const* src = reinterpret_cast<float4 const*>(p.guide_out + size_t(i) * guide::Outputs);
+#pragma unroll
+                    for (int j = 0; j < guide::Lobes; ++j) {
+                        float4 const v = src[j];
+                        lobes[j].mu    = v3(v.x, v.y, v.z);
+                        lobes[j].kappa = v.w;
                     }
-                    guide::mixture(o, lobes);
+                    float4 const w0 = src[8], w1 = src[9];
+                    lobes[0].weight = w0.x;
+                    lobes[1].weight = w0.y;
+                    lobes[2].weight = w0.z;
+                    lobes[3].weight = w0.w;
+                    lobes[4].weight = w1.x;
+                    lobes[5].weight = w1.y;
+                    lobes[6].weight = w1.z;
+                    lobes[7].weight = w1.w;
                 }
 
                 // Next-event estimation (sample_lights / evaluate_light, pathtracer_mis.cpp:281-347).
@@ -1440,22 +1509,17 @@ __global__ void k_gather(Paths p, uint32_t w, uint32_t h, uint32_t samples, floa
     if (q >= w * h) {
         return;
     }
-    int const x = int(q % w);
-    int const y = int(q / w);
-    float4    acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    int const      x      = int(q % w);
+    int const      y      = int(q / w);
+    uint32_t const bw     = w + 2 * Film_border;
+    uint32_t const traced = bw * (h + 2 * Film_border);  // bordered pixels per sample slot
+    float4         acc    = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int dy = -1; dy <= 1; ++dy) {
-        int const sy = y - dy;
-        if (sy < 0 || sy >= int(h)) {
-            continue;
-        }
+        uint32_t const sy = uint32_t(y - dy + Film_border);  // bordered row, always inside
         for (int dx = -1; dx <= 1; ++dx) {
-            int const sx = x - dx;
-            if (sx < 0 || sx >= int(w)) {
-                continue;
-            }
-            uint32_t const src = uint32_t(sy) * w + uint32_t(sx);
+            uint32_t const src = sy * bw + uint32_t(x - dx + Film_border);
             for (uint32_t k = 0; k < samples; ++k) {
-                uint32_t const path = k * w * h + src;
+                uint32_t const path = k * traced + src;
                 float2 const   uv   = p.puv[path];
                 float const    wt   = filter_weight(uv.x - 0.5f - float(dx)) *
                                  filter_weight(uv.y - 0.5f - float(dy));
@@ -1585,6 +1649,7 @@ struct Renderer::Device {
     // path guiding
     guide::Network     net;
     bool               net_ready     = false;
+    uint32_t           guide_grid    = 1;      // k_guide blocks (persistent)
     uint32_t           guide_paths   = 0;  // paths the guide buffers hold
     uint32_t           guide_records = 0;  // record depth they were sized for
     uint32_t           train_capacity = 0;
@@ -1755,6 +1820,7 @@ Renderer::~Renderer() {
     free_ptr(p.sh2_d);
     free_ptr(p.sh2_L);
     free_ptr(p.L2);
+    free_ptr(p.guide_in);
     free_ptr(p.guide_out);
     free_ptr(p.guide_ok);
     free_ptr(p.rec);
@@ -2012,6 +2078,7 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     free_ptr(p.sh2_d);
     free_ptr(p.sh2_L);
     free_ptr(p.L2);
+    free_ptr(p.guide_in);
     free_ptr(p.guide_out);
     free_ptr(p.guide_ok);
     free_ptr(p.rec);
@@ -2058,11 +2125,14 @@ int32_t Renderer::ensure_guide(uint32_t paths) {
     Paths&         p  = d_->paths;
     uint32_t const rd = settings_.record_depth;
     if (d_->guide_paths < paths || d_->guide_records != rd) {
+        free_ptr(p.guide_in);
         free_ptr(p.guide_out);
         free_ptr(p.guide_ok);
         free_ptr(p.rec);
         free_ptr(p.open_record);
         size_t const n = d_->capacity;
+        size_t const tiled_entries = (n + guide::Tile - 1) / guide::Tile * guide::Tile;
+        SPB_RCUDA(cudaMalloc(&p.guide_in, tiled_entries * guide::Inputs * sizeof(__nv_bfloat16)));
         SPB_RCUDA(cudaMalloc(&p.guide_out, n * guide::Outputs * sizeof(float)));
         SPB_RCUDA(cudaMalloc(&p.guide_ok, n));
         SPB_RCUDA(cudaMalloc(&p.rec, n * rd * Record_float4 * sizeof(float4)));
@@ -2088,6 +2158,22 @@ int32_t Renderer::ensure_guide(uint32_t paths) {
         SPB_RCUDA(cudaError_t(d_->net.init(settings_.guide_seed)));
         SPB_RCUDA(cudaFuncSetAttribute(k_guide, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(sizeof(Infer_smem))));
+        // Persistent inference: as many blocks as fit on the SMs at once, from the SM's shared
+        // memory and registers (the blocks are independent, so any count is correct).
+        SPB_RCUDA(cudaFuncSetAttribute(k_guide, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       int(cudaSharedmemCarveoutMaxShared)));
+        int dev = 0, sms = 0, smem_sm = 0, reserved = 0, regs_sm = 0;
+        SPB_RCUDA(cudaGetDevice(&dev));
+        SPB_RCUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        SPB_RCUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+        SPB_RCUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+        SPB_RCUDA(cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev));
+        cudaFuncAttributes fa{};
+        SPB_RCUDA(cudaFuncGetAttributes(&fa, k_guide));
+        int const warp_regs = (fa.numRegs * 32 + 255) / 256 * 256;  // allocated per warp in 256s
+        int const per_sm    = std::min({smem_sm / (int(sizeof(Infer_smem)) + reserved),
+                                        regs_sm / std::max(1, warp_regs * (guide::Block / 32)), 2048 / guide::Block});
+        d_->guide_grid = uint32_t(std::max(1, sms * std::max(1, per_sm)));
         d_->net_ready = true;
         d_->pass      = 0;
     }
@@ -2125,12 +2211,12 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         error_ = "max_bounces too large";
         return SPB_ERROR_ARGUMENT;
     }
-    uint32_t const pixels = camera_.width * camera_.height;
+    // camera samples per sample slot: the image and its filter border
+    uint32_t const pixels = (camera_.width + 2 * Film_border) * (camera_.height + 2 * Film_border);
     // k samples per pixel per wave, up to about 4M paths per wave.
-    uint32_t per_wave = std::max(1u, std::min(num_samples, (1u << 22) / std::max(1u, pixels)));
-    if (settings_.guiding) {
-        per_wave = std::max(1u, std::min(per_wave, settings_.guide_pass_spp));  // train between passes
-    }
+    uint32_t const per_wave = std::max(1u, std::min(num_samples, (1u << 22) / std::max(1u, pixels)));
+    // while the guide trains, passes of guide_pass_spp with training steps in between
+    uint32_t const train_wave = std::max(1u, std::min(per_wave, settings_.guide_pass_spp));
     if (int32_t const st = ensure_buffers(per_wave * pixels)) {
         return st;
     }
@@ -2183,13 +2269,16 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     std::vector<uint32_t> host_ctr(Counter_words);
     SPB_RCUDA(cudaEventRecord(d_->ev0, st));
     for (uint32_t done = 0; done < num_samples;) {
-        uint32_t const k     = std::min(per_wave, num_samples - done);
+        bool const training = settings_.guiding &&
+                              (settings_.guide_train_spp == 0 || first_sample + done < settings_.guide_train_spp);
+        uint32_t const k     = std::min(training ? train_wave : per_wave, num_samples - done);
         uint32_t const paths = k * pixels;
         Wave           wave{first_sample + done, k, settings_.seed, settings_.min_bounces,
                   settings_.max_bounces};
         wave.guiding        = settings_.guiding ? 1u : 0u;
         wave.guide_fraction = settings_.guide_fraction;
-        wave.record_depth   = settings_.guiding ? settings_.record_depth : 0u;
+        wave.guide_depth    = settings_.guide_depth;
+        wave.record_depth   = training ? settings_.record_depth : 0u;
         wave.bounds_lo      = d_->bounds_lo;
         wave.bounds_inv     = d_->bounds_inv;
         SPB_RCUDA(cudaMemsetAsync(ctr, 0, Counter_words * sizeof(uint32_t), st));
@@ -2211,10 +2300,11 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             uint32_t* const c = ctr + Counter_stride * b;
             k_trace<false><<<d_->trace_grid, Trace_block, 0, st>>>(sg, d_->paths, q_in, c, c + 2,
                                                                    ctr + Overflow_slot);
-            if (settings_.guiding) {
-                k_guide<<<(paths + guide::Tile - 1) / guide::Tile, guide::Block, sizeof(Infer_smem), st>>>(
-                    sg, wave, d_->paths, q_in, c, d_->net.weights(), d_->net.parameters(),
-                    ctr + Overflow_slot + 1);
+            // (without media a vertex's depth is the iteration; with media it can be less)
+            if (settings_.guiding && (d_->has_media || b < settings_.guide_depth)) {
+                k_guide_encode<<<(paths + 255) / 256, 256, 0, st>>>(sg, wave, d_->paths, q_in, c);
+                k_guide<<<d_->guide_grid, guide::Block, sizeof(Infer_smem), st>>>(
+                    d_->paths, c, d_->net.weights(), d_->net.parameters(), ctr + Overflow_slot + 1);
             }
             k_shade<<<(paths + Shade_block - 1) / Shade_block, Shade_block, 0, st>>>(
                 sg, wave, d_->paths, q_in, c, q_out, c + Counter_stride, d_->shadow_queue, c + 1);
@@ -2229,13 +2319,13 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
                     sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot);
             }
         }
-        if (settings_.guiding) {
+        if (training) {
             if (int32_t const e = train_guide(paths, &wave)) {
                 return e;
             }
         }
-        k_gather<<<(pixels + 255) / 256, 256, 0, st>>>(d_->paths, camera_.width, camera_.height, k,
-                                                      d_->film, d_->comp);
+        k_gather<<<(camera_.width * camera_.height + 255) / 256, 256, 0, st>>>(
+            d_->paths, camera_.width, camera_.height, k, d_->film, d_->comp);
         SPB_RCUDA(cudaGetLastError());
         SPB_RCUDA(cudaMemcpyAsync(host_ctr.data(), ctr, Counter_words * sizeof(uint32_t),
                                   cudaMemcpyDeviceToHost, st));

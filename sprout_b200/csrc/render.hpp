@@ -54,16 +54,19 @@ struct Settings {
     // Learned path guiding (no counterpart in the reference): at surface vertices the
     // continuation direction comes from the network's vMF mixture with probability
     // guide_fraction, else from the BSDF (one-sample MIS of the two).  The network is trained
-    // online, guide_steps Adam steps (learning rate guide_lr) on guide_batch samples after each
-    // pass of samples, from the first record_depth vertices of every path.
-    bool     guiding        = false;
-    float    guide_fraction = 0.5f;
-    uint32_t guide_batch    = 1u << 18;
-    uint32_t guide_steps    = 1;
-    float    guide_lr       = 1e-3f;
-    uint32_t record_depth   = 2;
-    uint32_t guide_seed     = 7;
-    uint32_t guide_pass_spp = 4;  // samples per pixel between training steps
+    // online: guide_steps Adam steps (learning rate guide_lr) on batches of guide_batch records
+    // after each pass of guide_pass_spp samples per pixel, from the first record_depth vertices
+    // of every path, until guide_train_spp samples per pixel have been rendered.
+    bool     guiding         = false;
+    float    guide_fraction  = 0.5f;
+    uint32_t guide_batch     = 1u << 16;
+    uint32_t guide_steps     = 64;
+    float    guide_lr        = 1e-2f;
+    uint32_t record_depth    = 2;
+    uint32_t guide_seed      = 7;
+    uint32_t guide_pass_spp  = 4;   // samples per pixel between training steps
+    uint32_t guide_train_spp = 32;  // samples per pixel after which training stops (0: never)
+    uint32_t guide_depth     = 255;  // vertices of depth below this are guided
 };
 
 struct Stats {

@@ -1,4 +1,4 @@
-"""Path-tracer measurement through the su_* C API, timed on the device.  Three workloads:
+"""Path-tracer measurement through the su_* C API, timed on the device.  Four workloads:
 
 * cornell: the Cornell scene (sprout_b200.scenes.cornell), 512x512, 64 spp, max depth 8;
 * wavefront: 400 instances of a 5,000-triangle displaced sphere (2,000,000 triangles) lit by
@@ -6,9 +6,11 @@
   256 spp, max depth 12;
 * volume: a 2 m cube of 256^3 fBm density lit by a sphere light and the environment
   (sprout_b200.scenes.volume), a few of 64 seeded views of 256..1024 px, 128 spp, max depth
-  32.
+  32;
+* guiding: the doorway interior (sprout_b200.scenes.doorway), 1280x720: sample count and
+  device time to relMSE 0.01 for plain MIS and for learned path guiding.
 
-    python -m sprout_b200.render_bench [--scene cornell] [--width 512] [--height 512] [--spp 64]
+    python -m sprout_b200.render_bench [--scene cornell|wavefront|volume|guiding] [--width 512] [--height 512] [--spp 64]
                                        [--frames 3] [--convergence] [--cpu-reference]
 
 Prints one JSON object: samples/s and rays/s (closest-hit + shadow) per frame, the end-to-end
@@ -166,9 +168,91 @@ def measure_volume(views=4, spp=128, cpu_reference=False):
     return out
 
 
+GUIDING_CONFIG = ("doorway interior (sprout_b200.scenes.doorway): 6 x 6 x 3 m room lit only through a 1 x 2 m "
+                  "doorway by a uniform environment of radiance 5; 96 icospheres (491,520 tris) and 160 boxes, 70 % "
+                  "diffuse / 30 % GGX conductors alpha U[0.1, 0.6]; PTMIS max depth 8 (Russian roulette from 4)")
+
+
+def doorway_frame(width, height, spp, guiding=None, seed=0):
+    """One frame of the doorway interior through the su_* API: (RGB image as float64, device
+    seconds of the render, wall seconds of su_render_frame + su_postprocess + framebuffer copy).
+    The scene is built and uploaded before the timed frame (su_start_render_frame); a guided
+    frame starts from an untrained network all the same (the first frame of the engine)."""
+    lib = _lib.load()
+    stats = _lib.RenderStats()
+    su = capi.SuLibrary()
+    assert su.su_init(False) == 0
+    try:
+        scenes.doorway(su, width, height, spp, guiding=guiding, render_seed=seed)
+        assert su.su_start_render_frame(0) == 0, su.messages  # scene flattening, BVH build, upload
+        t0 = time.perf_counter()
+        assert su.su_render_frame(0) == 0, su.messages
+        assert su.su_postprocess() == 0
+        img = su.framebuffer(width, height)[0][:, :, :3].astype(np.float64)
+        wall = time.perf_counter() - t0
+        assert lib.spb_render_last_stats(ctypes.byref(stats)) == 0
+        return img, stats.device_seconds, wall
+    finally:
+        su.su_release()
+
+
+def measure_guiding(width=1280, height=720, reference_spp=4096, target=0.01, guiding=True):
+    """Time to relMSE `target` on the doorway interior, plain MIS against learned guiding.
+
+    relMSE is mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2) with both images scaled so
+    that the reference's mean is 0.5.  The reference r is a plain render of reference_spp samples
+    per pixel with an independent seed; its own noise adds to every measurement, in expectation
+    by c = v / R (v: the plain estimator's relative variance per sample), which a plain render
+    at s spp also measures (E[e] = v / s + v / R).  Each reported relMSE has c subtracted.  For
+    each integrator: a probe render gives the sample count expected to reach the target (relMSE
+    falls as 1/spp), then renders at that count (raised until the target is met) give the
+    reported sample count and device time of one frame."""
+    ref, ref_s, _ = doorway_frame(width, height, reference_spp, None, seed=1000)
+    k = 0.5 / ref.mean()
+
+    def raw(img):
+        return float(np.mean((k * img - k * ref) ** 2 / ((k * ref) ** 2 + 1e-2)))
+
+    probe = 512
+    img, _, _ = doorway_frame(width, height, probe)
+    e = raw(img)
+    c = e * probe / (reference_spp + probe)
+    out = {"workload": "doorway", "config": f"{GUIDING_CONFIG}, {width}x{height}",
+           "rel_mse": "mean (x - r)^2 / (r^2 + 0.01), images scaled so that mean(r) = 0.5, minus the "
+                      "reference's own share",
+           "reference": {"spp": reference_spp, "integrator": "plain MIS, independent seed",
+                         "device_seconds": round(ref_s, 3), "rel_mse_share": round(c, 6)},
+           "target": target}
+
+    def reach(first, guided):
+        spp, runs = first, []
+        for _ in range(4):
+            img, dev, wall = doorway_frame(width, height, spp, guiding if guided else None)
+            err = raw(img) - c
+            runs.append({"spp": spp, "rel_mse": round(err, 5), "device_seconds": round(dev, 4),
+                         "wall_seconds": round(wall, 3)})
+            if err <= target:
+                break
+            spp = int(np.ceil(spp * err / target / 8.0)) * 8 + 8
+        return runs
+
+    plain_v = (e - c) * probe
+    plain = reach(int(np.ceil(plain_v / target / 8.0)) * 8, False)
+    probe_img, _, _ = doorway_frame(width, height, 256, guiding)
+    guided_v = (raw(probe_img) - c) * 256
+    guided = reach(int(np.ceil(guided_v / target / 8.0)) * 8, True)
+    out["plain"] = plain[-1]
+    out["guided"] = guided[-1]
+    out["runs"] = {"plain": plain, "guided": guided}
+    if plain[-1]["rel_mse"] <= target and guided[-1]["rel_mse"] <= target:
+        out["guided_over_plain_device_time"] = round(guided[-1]["device_seconds"] / plain[-1]["device_seconds"], 4)
+        out["guided_over_plain_wall_time"] = round(guided[-1]["wall_seconds"] / plain[-1]["wall_seconds"], 4)
+    return out
+
+
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("--scene", choices=sorted(SCENES) + ["volume"], default="cornell")
+    p.add_argument("--scene", choices=sorted(SCENES) + ["volume", "guiding"], default="cornell")
     p.add_argument("--views", type=int, default=4, help="volume workload: number of views")
     p.add_argument("--width", type=int)
     p.add_argument("--height", type=int)
@@ -179,6 +263,8 @@ def main():
     a = p.parse_args()
     if a.scene == "volume":
         print(json.dumps(measure_volume(a.views, a.spp or 128, a.cpu_reference)))
+    elif a.scene == "guiding":
+        print(json.dumps(measure_guiding(a.width or 1280, a.height or 720)))
     else:
         print(json.dumps(measure(a.scene, a.width, a.height, a.spp, a.frames, a.convergence, a.cpu_reference)))
 
