@@ -80,9 +80,9 @@ struct Train_tc_smem {
     __nv_bfloat16 a0[Tile * Inputs];
     __nv_bfloat16 a[4][Tile * Width];
     __nv_bfloat16 z[2][Tile * Zw];
-    float         out[Tile * Out_stride];
     float         gb[Bias_count];
     float         red[2][8][32];  // per-warp column sums, alternating between layers
+    float         qpart[2][Tile];  // each half's share of the mixture density per sample
     uint64_t      mbar;
     uint32_t      tmem_slot;
 };
@@ -108,6 +108,109 @@ __device__ inline float warp_column_sums(float v[32]) {
         }
     }
     return v[0];
+}
+
+// The output layer of a training tile, by all threads, after its MMA was issued: thread t
+// takes sample r = t % 128 and lobes 4h..4h+3 (h = t / 128).  From the accumulator plus bias it
+// forms the mixture (softmax weights of all lobes; unit mean and concentration of its own),
+// adds its lobes' share of q(d) = sum_j w_j vMF_j(d), exchanges it with the other half, and
+// writes the gradient of scale * (-log q(d)) with respect to its 20 outputs (guide_mlp.cuh's
+// output_gradient, split in two) as BF16 dZ columns; columns 40..63 are cleared.  The per-warp
+// column sums of the FP32 gradient go to red (the output bias gradient).  Ends with a barrier.
+__device__ inline void finish_output_gradient(Train_tc_smem& s, float const* b, shading::V3 d, float scale,
+                                              float (&red)[8][32], Tmem_tile& tm) {
+    if (!mbar_wait(tm.mbar, tm.phase)) {
+        *tm.error = 1u;
+    }
+    tm.phase ^= 1u;
+    tc_fence_after();
+    int const      warp  = threadIdx.x >> 5;
+    int const      r     = threadIdx.x & (Tile - 1);
+    int const      h     = threadIdx.x >> 7;
+    uint32_t const lanes = uint32_t(32 * (warp & 3)) << 16;
+    float          o[16], logit[Lobes];
+    tmem_ld16(tm.tmem + lanes + uint32_t(16 * h), o);
+    tmem_ld8(tm.tmem + lanes + 32u, logit);
+    float mx = -3.4e38f;
+#pragma unroll
+    for (int j = 0; j < Lobes; ++j) {
+        logit[j] += b[32 + j];
+        mx = fmaxf(mx, logit[j]);
+    }
+    float sum = 0.f, w[4];
+#pragma unroll
+    for (int j = 0; j < Lobes; ++j) {
+        float const e = expf(logit[j] - mx);
+        sum += e;
+        if (j / 4 == h) {
+            w[j % 4] = e;
+        }
+    }
+    float mu[4][3], kappa[4], c[4], v[4], q = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            o[4 * j + k] += b[16 * h + 4 * j + k];
+        }
+        w[j] /= sum;
+        float const l2  = o[4 * j] * o[4 * j] + o[4 * j + 1] * o[4 * j + 1] + o[4 * j + 2] * o[4 * j + 2];
+        float const inv = l2 > 1e-20f ? 1.f / sqrtf(l2) : 0.f;
+        mu[j][0]        = l2 > 1e-20f ? inv * o[4 * j] : 0.f;
+        mu[j][1]        = l2 > 1e-20f ? inv * o[4 * j + 1] : 0.f;
+        mu[j][2]        = l2 > 1e-20f ? inv * o[4 * j + 2] : 1.f;
+        kappa[j]        = expf(fminf(fmaxf(o[4 * j + 3], Log_kappa_min), Log_kappa_max));
+        c[j]            = mu[j][0] * d.x + mu[j][1] * d.y + mu[j][2] * d.z;
+        float const nrm = kappa[j] / (2.f * 3.14159265358979f * -expm1f(-2.f * kappa[j]));
+        v[j]            = nrm * expf(kappa[j] * (c[j] - 1.f));
+        q += w[j] * v[j];
+    }
+    s.qpart[h][r] = q;
+    __syncthreads();
+    q = fmaxf(s.qpart[0][r] + s.qpart[1][r], 1e-30f);
+    float g[32];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float const rj = w[j] * v[j] / q;
+        g[16 + j]      = scale * (w[j] - rj);
+        float const lk = o[4 * j + 3];
+        if (lk > Log_kappa_min && lk < Log_kappa_max) {
+            float const x2 = 2.f * kappa[j];
+            g[4 * j + 3]   = -scale * rj * (1.f - x2 / expm1f(x2) + kappa[j] * (c[j] - 1.f));
+        } else {
+            g[4 * j + 3] = 0.f;
+        }
+        float const l2 = o[4 * j] * o[4 * j] + o[4 * j + 1] * o[4 * j + 1] + o[4 * j + 2] * o[4 * j + 2];
+        float const f  = l2 > 1e-20f ? -scale * rj * kappa[j] * rsqrtf(l2) : 0.f;
+        g[4 * j]       = f * (d.x - mu[j][0] * c[j]);
+        g[4 * j + 1]   = f * (d.y - mu[j][1] * c[j]);
+        g[4 * j + 2]   = f * (d.z - mu[j][2] * c[j]);
+    }
+    // dZ row r: lobe columns 16h..16h+15, logit columns 32+4h..32+4h+3, zeros in 40..63
+    __nv_bfloat162 hv[8];
+#pragma unroll
+    for (int q2 = 0; q2 < 8; ++q2) {
+        hv[q2] = __floats2bfloat162_rn(g[2 * q2], g[2 * q2 + 1]);
+    }
+    *reinterpret_cast<uint4*>(&s.z[0][tiled(r, 16 * h, Zw)])     = *reinterpret_cast<uint4*>(hv);
+    *reinterpret_cast<uint4*>(&s.z[0][tiled(r, 16 * h + 8, Zw)]) = *reinterpret_cast<uint4*>(hv + 4);
+    __nv_bfloat162 const lg[2] = {__floats2bfloat162_rn(g[16], g[17]), __floats2bfloat162_rn(g[18], g[19])};
+    *reinterpret_cast<uint2*>(&s.z[0][tiled(r, 32 + 4 * h, Zw)]) = *reinterpret_cast<uint2 const*>(lg);
+    uint4 const zero = make_uint4(0u, 0u, 0u, 0u);
+    if (h == 0) {
+        *reinterpret_cast<uint4*>(&s.z[0][tiled(r, 40, Zw)]) = zero;
+        *reinterpret_cast<uint4*>(&s.z[0][tiled(r, 48, Zw)]) = zero;
+    } else {
+        *reinterpret_cast<uint4*>(&s.z[0][tiled(r, 56, Zw)]) = zero;
+    }
+    fence_async_smem();
+#pragma unroll
+    for (int k = 20; k < 32; ++k) {
+        g[k] = 0.f;
+    }
+    red[warp][threadIdx.x & 31] = warp_column_sums(g);
+    tc_fence_before();
+    __syncthreads();
 }
 
 // Issues the layer's dW (accumulating unless `fresh`) and, when with_da, its dA; thread 0.
@@ -137,8 +240,11 @@ __device__ inline void backward_mma(uint32_t tmem, uint32_t dw_col, __nv_bfloat1
     umma_commit(mbar);
 }
 
+// Inputs: Tiled_inputs, BF16 tiles of 128 samples in operand order (8 KB each); else FP32,
+// 32 per sample.
+template <bool Tiled_inputs>
 __global__ void __launch_bounds__(Block) k_gradients_tc(__nv_bfloat16 const* wbf, float const* params,
-                                                        float const* in, float const* dirs, float const* scale,
+                                                        void const* in, float const* dirs, float const* scale,
                                                         uint64_t n, uint32_t tiles, float* partial, uint32_t* error) {
     extern __shared__ __align__(16) unsigned char raw[];
     Train_tc_smem& s = *reinterpret_cast<Train_tc_smem*>(raw);
@@ -172,37 +278,39 @@ __global__ void __launch_bounds__(Block) k_gradients_tc(__nv_bfloat16 const* wbf
 #pragma unroll 1
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         uint64_t const base = uint64_t(tile) * Tile;
-        load_inputs(s.a0, in, base, n);
-        fence_async_smem();
-        tc_fence_before();
-        __syncthreads();
-        forward_tc(s.net, acts, s.out, tm);
-
-        // Loss gradient at the outputs -> dZ_4 (BF16, columns 0..39; 40..47 stay 0) and, in FP32,
-        // into `out` for the bias gradient.
-        if (threadIdx.x < Tile) {
-            uint64_t const g = base + r;
-            float          gr[Outputs];
-            if (g < n) {
-                output_gradient(s.out + r * Out_stride,
-                                shading::v3(dirs[3 * g], dirs[3 * g + 1], dirs[3 * g + 2]), scale[g], gr);
-            } else {
-                for (int j = 0; j < Outputs; ++j) {
-                    gr[j] = 0.f;
-                }
-            }
-            for (int j = 0; j < Outputs; ++j) {
-                s.z[0][tiled(r, j, Zw)]  = __float2bfloat16(gr[j]);
-                s.out[r * Out_stride + j] = gr[j];
-            }
-            // columns the previous tile's hidden-layer dZ left behind
-            for (int j = Outputs; j < Width; ++j) {
-                s.z[0][tiled(r, j, Zw)] = __float2bfloat16(0.f);
-            }
+        if constexpr (Tiled_inputs) {
+            uint4 const* const src = static_cast<uint4 const*>(in) + uint64_t(tile) * (Tile * Inputs / 8);
+            uint4* const       dst = reinterpret_cast<uint4*>(s.a0);
+            dst[threadIdx.x]         = src[threadIdx.x];
+            dst[Block + threadIdx.x] = src[Block + threadIdx.x];
+        } else {
+            load_inputs(s.a0, static_cast<float const*>(in), base, n);
         }
+        uint64_t const   g     = base + r;
+        float const      sc    = g < n ? scale[g] : 0.f;
+        shading::V3 const d    = g < n ? shading::v3(dirs[3 * g], dirs[3 * g + 1], dirs[3 * g + 2])
+                                       : shading::v3(0.f, 0.f, 1.f);
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
+        // forward (hidden layers), then the output layer and the loss gradient -> dZ_4
+        layer_forward_tc<Inputs, Width, false>(acts[0], s.net.w + weight_tile_offset(0), s.net.b + bias_slot(0),
+                                               acts[1], Smem_outputs{nullptr}, tm);
+#pragma unroll
+        for (int l = 1; l < Layers - 1; ++l) {
+            layer_forward_tc<Width, Width, false>(acts[l], s.net.w + weight_tile_offset(l), s.net.b + bias_slot(l),
+                                                  acts[l + 1], Smem_outputs{nullptr}, tm);
+        }
+        issue_layer<Width, Outputs>(acts[4], s.net.w + weight_tile_offset(4), tm);
+        finish_output_gradient(s, s.net.b + bias_slot(4), d, sc, s.red[1], tm);
+        if (threadIdx.x < Outputs) {
+            // output bias gradient: column c lies in half h at local column lc
+            int const c  = threadIdx.x;
+            int const h  = c < 32 ? c / 16 : (c - 32) / 4;
+            int const lc = c < 32 ? c % 16 : 16 + (c - 32) % 4;
+            s.gb[bias_slot(4) + c] += s.red[1][4 * h][lc] + s.red[1][4 * h + 1][lc] + s.red[1][4 * h + 2][lc] +
+                                      s.red[1][4 * h + 3][lc];
+        }
 
         int cur = 0;  // dZ buffer of the current layer
 #pragma unroll 1
@@ -216,14 +324,6 @@ __global__ void __launch_bounds__(Block) k_gradients_tc(__nv_bfloat16 const* wbf
                 } else {
                     backward_mma<Inputs, Width>(tm.tmem, dw_column(l), s.z[cur], acts[l], w, false, fresh, tm.mbar);
                 }
-            }
-            if (l == Layers - 1 && threadIdx.x < Outputs) {
-                // output bias gradient, while the tensor cores work
-                float acc = 0.f;
-                for (int q = 0; q < Tile; ++q) {
-                    acc += s.out[q * Out_stride + threadIdx.x];
-                }
-                s.gb[bias_slot(4) + threadIdx.x] += acc;
             }
             if (!mbar_wait(tm.mbar, tm.phase)) {
                 *tm.error = 1u;
@@ -240,9 +340,11 @@ __global__ void __launch_bounds__(Block) k_gradients_tc(__nv_bfloat16 const* wbf
 #pragma unroll
                 for (int j = 0; j < 32; j += 8) {
                     __nv_bfloat162 h[4];
+                    uint4 const    in8 = *reinterpret_cast<uint4 const*>(&acts[l][tiled(r, k0 + j, Width)]);
+                    __nv_bfloat16 const* a8 = reinterpret_cast<__nv_bfloat16 const*>(&in8);
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
-                        if (!(__bfloat162float(acts[l][tiled(r, k0 + j + q, Width)]) > 0.f)) {
+                        if (!(__bfloat162float(a8[q]) > 0.f)) {
                             v[j + q] = 0.f;
                         }
                     }
@@ -303,8 +405,27 @@ __global__ void __launch_bounds__(Block) k_gradients_tc(__nv_bfloat16 const* wbf
     }
 }
 
-// grads[p] = sum over blocks of partial[b][p], in block order (deterministic).
-__global__ void k_reduce(float const* partial, uint32_t blocks, float* grads) {
+// grads[p] = sum over blocks of partial[b][p], in block order (deterministic); divided by the
+// total of weight_parts when given (the batch's loss weights, summed in a fixed order).
+__global__ void k_reduce(float const* partial, uint32_t blocks, float const* weight_parts, uint32_t num_parts,
+                         float* grads) {
+    __shared__ float total;
+    if (threadIdx.x < 32) {
+        float acc = 0.f;
+        if (weight_parts) {
+            for (uint32_t i = threadIdx.x; i < num_parts; i += 32) {
+                acc += weight_parts[i];
+            }
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+        }
+        if (threadIdx.x == 0) {
+            total = acc;
+        }
+    }
+    __syncthreads();
     uint32_t const p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= uint32_t(Parameters)) {
         return;
@@ -313,7 +434,7 @@ __global__ void k_reduce(float const* partial, uint32_t blocks, float* grads) {
     for (uint32_t b = 0; b < blocks; ++b) {
         acc += partial[uint64_t(b) * Parameters + p];
     }
-    grads[p] = acc;
+    grads[p] = !weight_parts ? acc : (total > 0.f ? acc / total : 0.f);
 }
 
 // Index of parameter p in the BF16 weight array, or -1 for a bias.
@@ -379,7 +500,11 @@ int set_kernel_attributes() {
         int const bytes = int(tile_smem_bytes());
         cudaError_t e   = cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         if (e == cudaSuccess) {
-            e = cudaFuncSetAttribute(k_gradients_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            e = cudaFuncSetAttribute(k_gradients_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(sizeof(Train_tc_smem)));
+        }
+        if (e == cudaSuccess) {
+            e = cudaFuncSetAttribute(k_gradients_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      int(sizeof(Train_tc_smem)));
         }
         return int(e);
@@ -480,25 +605,19 @@ int Network::forward(float const* inputs, uint64_t n, float* outputs, cudaStream
 
 int Network::gradients(float const* inputs, float const* dirs, float const* scale, uint64_t n,
                        cudaStream_t stream) {
+    return run_gradients(inputs, false, dirs, scale, n, nullptr, 0, stream);
+}
+
+int Network::gradients_tiled(__nv_bfloat16 const* tiles, float const* dirs, float const* weights, uint64_t n,
+                             float const* weight_parts, uint32_t num_parts, cudaStream_t stream) {
+    return run_gradients(tiles, true, dirs, weights, n, weight_parts, num_parts, stream);
+}
+
+int Network::run_gradients(void const* inputs, bool tiled, float const* dirs, float const* scale, uint64_t n,
+                           float const* weight_parts, uint32_t num_parts, cudaStream_t stream) {
     uint64_t const blocks = (n + Tile - 1) / Tile;
     if (blocks == 0) {
         return cudaMemsetAsync(grads_, 0, Parameters * sizeof(float), stream);
-    }
-    if (blocks > partial_blocks_) {
-        release(partial_);
-        if (cudaError_t const e = cudaMalloc(&partial_, blocks * Parameters * sizeof(float))) {
-            partial_blocks_ = 0;
-            return e;
-        }
-        partial_blocks_ = blocks;
-    }
-    if (!error_) {
-        if (cudaError_t const e = cudaMalloc(&error_, sizeof(uint32_t))) {
-            return e;
-        }
-        if (cudaError_t const e = cudaMemset(error_, 0, sizeof(uint32_t))) {
-            return e;
-        }
     }
     // one persistent block per SM (at most one per tile)
     static int const sms = [] {
@@ -508,9 +627,30 @@ int Network::gradients(float const* inputs, float const* dirs, float const* scal
         return std::max(count, 1);
     }();
     uint32_t const grid = uint32_t(std::min<uint64_t>(blocks, uint64_t(sms)));
-    k_gradients_tc<<<grid, Block, sizeof(Train_tc_smem), stream>>>(wbf_, params_, inputs, dirs, scale, n,
-                                                                   uint32_t(blocks), partial_, error_);
-    k_reduce<<<(Parameters + 255) / 256, 256, 0, stream>>>(partial_, grid, grads_);
+    if (grid > partial_blocks_) {
+        release(partial_);
+        if (cudaError_t const e = cudaMalloc(&partial_, size_t(grid) * Parameters * sizeof(float))) {
+            partial_blocks_ = 0;
+            return e;
+        }
+        partial_blocks_ = grid;
+    }
+    if (!error_) {
+        if (cudaError_t const e = cudaMalloc(&error_, sizeof(uint32_t))) {
+            return e;
+        }
+        if (cudaError_t const e = cudaMemset(error_, 0, sizeof(uint32_t))) {
+            return e;
+        }
+    }
+    if (tiled) {
+        k_gradients_tc<true><<<grid, Block, sizeof(Train_tc_smem), stream>>>(wbf_, params_, inputs, dirs, scale, n,
+                                                                             uint32_t(blocks), partial_, error_);
+    } else {
+        k_gradients_tc<false><<<grid, Block, sizeof(Train_tc_smem), stream>>>(wbf_, params_, inputs, dirs, scale, n,
+                                                                              uint32_t(blocks), partial_, error_);
+    }
+    k_reduce<<<(Parameters + 255) / 256, 256, 0, stream>>>(partial_, grid, weight_parts, num_parts, grads_);
     return cudaGetLastError();
 }
 

@@ -29,9 +29,13 @@ class Network {
     // Forward pass over n encoded inputs (device, n x 32 FP32) into n x 40 device outputs, on
     // the tensor cores; waits for completion.
     int forward(float const* inputs, uint64_t n, float* outputs, cudaStream_t stream);
-    // Gradient of (1/n) sum scale_i * (-log q(d_i | x_i)) into the device gradient buffer
-    // (`scale` already holds the 1/n).
+    // Gradient of sum_i scale_i * (-log q(d_i | x_i)) into the device gradient buffer.
     int gradients(float const* inputs, float const* dirs, float const* scale, uint64_t n, cudaStream_t stream);
+    // The same for the renderer's batches: inputs as BF16 tiles of 128 samples in the tensor
+    // cores' operand order (zero rows past n), and the loss sum_i w_i (-log q) / sum_i w_i with
+    // sum_i w_i the total of weight_parts (num_parts partial sums).
+    int gradients_tiled(__nv_bfloat16 const* tiles, float const* dirs, float const* weights, uint64_t n,
+                        float const* weight_parts, uint32_t num_parts, cudaStream_t stream);
     // One Adam step with the current gradient.
     int adam(float lr, cudaStream_t stream);
 
@@ -43,6 +47,9 @@ class Network {
     float const*         parameters() const { return params_; }
 
   private:
+    int run_gradients(void const* inputs, bool tiled, float const* dirs, float const* scale, uint64_t n,
+                      float const* weight_parts, uint32_t num_parts, cudaStream_t stream);
+
     float*         params_  = nullptr;
     float*         m_       = nullptr;
     float*         v_       = nullptr;

@@ -43,12 +43,16 @@ struct Net_smem {
 __device__ inline void load_net(Net_smem& s, __nv_bfloat16 const* __restrict__ wbf,
                                 float const* __restrict__ params) {
     int src = 0;
+#pragma unroll
     for (int l = 0; l < Layers; ++l) {
-        int const K = in_dim(l), N = out_dim(l), P = padded_out(l);
-        __nv_bfloat16* dst = s.w + weight_tile_offset(l);
-        for (int i = threadIdx.x; i < P * K; i += Block) {
-            int const n = i / K, k = i % K;
-            dst[tiled(n, k, K)] = n < N ? wbf[src + n * K + k] : __float2bfloat16(0.f);
+        // 16-byte chunks: 8 consecutive inputs of one output row, one core-matrix row
+        constexpr uint4 zero = {0u, 0u, 0u, 0u};
+        int const       K = in_dim(l), N = out_dim(l), P = padded_out(l);
+        __nv_bfloat16*  dst = s.w + weight_tile_offset(l);
+        for (int i = threadIdx.x; i < P * K / 8; i += Block) {
+            int const n = i / (K / 8), k = 8 * (i % (K / 8));
+            *reinterpret_cast<uint4*>(dst + tiled(n, k, K)) =
+                n < N ? *reinterpret_cast<uint4 const*>(wbf + src + n * K + k) : zero;
         }
         src += N * K;
     }
@@ -125,21 +129,28 @@ __device__ __forceinline__ void fence_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// Waits (bounded) for the mbarrier to complete the given phase; false if it never did.
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t phase) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(done)
+        : "r"(mbar), "r"(phase)
+        : "memory");
+    return done != 0;
+}
+
+// Waits (bounded) for the mbarrier to complete the given phase; false if it never did.  Called
+// by whole warps: lane 0 polls, then every lane observes the completed phase itself.
 __device__ inline bool mbar_wait(uint32_t mbar, uint32_t phase) {
-    for (uint32_t i = 0; i < (1u << 22); ++i) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, P1;\n\t}"
-            : "=r"(done)
-            : "r"(mbar), "r"(phase)
-            : "memory");
-        if (done) {
-            return true;
+    bool done = false;
+    if ((threadIdx.x & 31) == 0) {
+        for (uint32_t i = 0; i < (1u << 22) && !done; ++i) {
+            done = mbar_try_wait(mbar, phase);
         }
     }
-    return false;
+    __syncwarp();
+    return mbar_try_wait(mbar, phase);
 }
 
 // 32 / 8 consecutive FP32 columns of this thread's TMEM lane.
@@ -157,6 +168,21 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float v[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
+        v[i] = __uint_as_float(r[i]);
+    }
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
         v[i] = __uint_as_float(r[i]);
     }
 }
@@ -184,13 +210,14 @@ struct Smem_outputs {
     }
 };
 
-// One layer on the tensor cores.  Precondition: A and W are in shared memory, every writer
-// fenced its stores for the async proxy, and a block barrier (after tc_fence_before) followed.
-// Ends with the results stored (the last layer: store(r, outputs) by thread r < Tile) and a
-// barrier.
-template <int K, int N, bool Last, class Store = Smem_outputs>
-__device__ inline void layer_forward_tc(__nv_bfloat16 const* A, __nv_bfloat16 const* W, float const* b,
-                                        __nv_bfloat16* act, Store const& store, Tmem_tile& tm) {
+// One layer on the tensor cores, in two halves.  issue_layer (thread 0): the layer's MMAs into
+// the tile's accumulator and a commit to its mbarrier; precondition: A and W are in shared
+// memory, every writer fenced its stores for the async proxy, and a block barrier (after
+// tc_fence_before) followed.  finish_layer (all threads): waits for the commit, adds the bias,
+// applies ReLU and stores the BF16 activations (the last layer: store(r, outputs) by thread
+// r < Tile), then fences and ends with a barrier, after which the next layer may be issued.
+template <int K, int N>
+__device__ inline void issue_layer(__nv_bfloat16 const* A, __nv_bfloat16 const* W, Tmem_tile const& tm) {
     constexpr int P = (N + 15) & ~15;
     if (threadIdx.x == 0) {
         tc_fence_after();
@@ -203,6 +230,10 @@ __device__ inline void layer_forward_tc(__nv_bfloat16 const* A, __nv_bfloat16 co
         }
         umma_commit(tm.mbar);
     }
+}
+
+template <int N, bool Last, class Store>
+__device__ inline void finish_layer(float const* b, __nv_bfloat16* act, Store const& store, Tmem_tile& tm) {
     if (!mbar_wait(tm.mbar, tm.phase)) {
         *tm.error = 1u;
     }
@@ -240,6 +271,14 @@ __device__ inline void layer_forward_tc(__nv_bfloat16 const* A, __nv_bfloat16 co
     }
     tc_fence_before();
     __syncthreads();
+}
+
+// Both halves: one layer, results stored, ending with a barrier.
+template <int K, int N, bool Last, class Store = Smem_outputs>
+__device__ inline void layer_forward_tc(__nv_bfloat16 const* A, __nv_bfloat16 const* W, float const* b,
+                                        __nv_bfloat16* act, Store const& store, Tmem_tile& tm) {
+    issue_layer<K, N>(A, W, tm);
+    finish_layer<N, Last>(b, act, store, tm);
 }
 
 // Forward through all layers: acts[0] holds the tile's inputs (128 x 32, tiled); acts[1..4]

@@ -116,11 +116,10 @@ struct Paths {
     float4*   L2;
     // Path guiding, indexed by position in the current extension queue: the network inputs as
     // BF16 tiles of 128 entries in the tensor cores' operand order (guide_in), the predicted
-    // mixture (guide_out: 8 float4 of unit mean and concentration, then the 8 weights) and
-    // whether the entry is guided (guide_ok).  Indexed by path: the training records of its
-    // first record_depth vertices (5 float4 each: position and normal x | normal yz, wo xy |
-    // wo z, wi | throughput | radiance mark, w = 1 once marked) and the record awaiting its
-    // radiance mark.
+    // mixture (guide_out, Mixture_floats per entry) and whether the entry is guided (guide_ok).
+    // Indexed by path: the training records of its first record_depth vertices (5 float4 each:
+    // position and normal x | normal yz, wo xy | wo z, wi | throughput | radiance mark, w = 1
+    // once marked) and the record awaiting its radiance mark.
     __nv_bfloat16* guide_in;
     float*    guide_out;
     uint8_t*  guide_ok;
@@ -129,6 +128,11 @@ struct Paths {
 };
 
 constexpr int Record_float4 = 5;
+
+// The guide's mixture per queue entry: 8 float4 of unit mean and concentration, the 8 lobe
+// weights, then the 8 weights times their lobes' vMF normalisation
+// kappa / (2 pi (1 - e^{-2 kappa})), so that a density evaluation takes one exponential per lobe.
+constexpr int Mixture_floats = 48;
 
 // Shadow-queue entries are path indices; this bit marks the vertex's second shadow ray.
 constexpr uint32_t Second_shadow = 0x80000000u;
@@ -959,11 +963,14 @@ __device__ __forceinline__ void store_shadow(Paths const& p, uint32_t path, bool
 // stores each entry's mixture at its queue position, where k_shade reads it.
 struct Infer_smem {
     guide::Net_smem net;
-    __nv_bfloat16   x[guide::Tile * guide::Width];
-    __nv_bfloat16   y[guide::Tile * guide::Width];  // its first 8 KB also take the tile's inputs
-    uint64_t        mbar;       // tensor-core completion barrier
-    uint32_t        tmem_slot;  // accumulator address from tcgen05.alloc
+    // Per tile of the pair being processed: two activation buffers (the second's first 8 KB
+    // also take the tile's inputs); after the last layer the 32 KB hold its 128 output rows.
+    __nv_bfloat16 act[2][2][guide::Tile * guide::Width];
+    uint64_t      mbar[2];    // tensor-core completion barriers
+    uint32_t      tmem_slot;  // accumulator address from tcgen05.alloc
 };
+static_assert(sizeof(float) * 48 * guide::Tile <= sizeof(__nv_bfloat16) * 2 * guide::Tile * guide::Width,
+              "a tile's mixture rows fit its activation buffers");
 
 // Position, geometric normal (facing -dir) and outgoing direction of a path's hit.
 __device__ __forceinline__ void hit_frame(Scene_gpu const& s, Paths const& p, uint32_t path, uint32_t id,
@@ -1024,67 +1031,196 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// Stores entry base + r's mixture (guide::mixture of the 40 outputs) at its queue position:
-// 8 float4 (unit mean, concentration), then the 8 weights; consecutive rows are consecutive
-// 160-byte records, so a warp's stores are contiguous.
-struct Guide_outputs {
-    float*   guide_out;
-    uint32_t base;
-    uint32_t num;
-    __device__ void operator()(int r, float const (&v)[guide::Outputs]) const {
-        uint32_t const q = base + uint32_t(r);
-        if (q >= num) {
-            return;
-        }
-        guide::Lobe lobes[guide::Lobes];
-        guide::mixture(v, lobes);
-        float4* const dst = reinterpret_cast<float4*>(guide_out + size_t(q) * guide::Outputs);
-#pragma unroll
-        for (int j = 0; j < guide::Lobes; ++j) {
-            dst[j] = make_float4(lobes[j].mu.x, lobes[j].mu.y, lobes[j].mu.z, lobes[j].kappa);
-        }
-        dst[8] = make_float4(lobes[0].weight, lobes[1].weight, lobes[2].weight, lobes[3].weight);
-        dst[9] = make_float4(lobes[4].weight, lobes[5].weight, lobes[6].weight, lobes[7].weight);
+// The last layer of one tile, by all threads: thread t takes row t % 128 and lobes 4h..4h+3
+// (h = t / 128) of it -- their 16 outputs and the 8 mixture logits from the accumulator plus
+// bias -- and writes them as guide::mixture does (unit mean, concentration, softmax weight),
+// with the hardware exponential, into `rows` in the Mixture_floats form.
+__device__ __forceinline__ void finish_mixture(float const* b, float4* rows, guide::Tmem_tile& tm) {
+    if (!guide::mbar_wait(tm.mbar, tm.phase)) {
+        *tm.error = 1u;
     }
-};
+    tm.phase ^= 1u;
+    guide::tc_fence_after();
+    int const      warp  = threadIdx.x >> 5;
+    int const      r     = threadIdx.x & (guide::Tile - 1);
+    int const      h     = threadIdx.x >> 7;
+    uint32_t const lanes = uint32_t(32 * (warp & 3)) << 16;
+    float          m[16], logit[8];
+    guide::tmem_ld16(tm.tmem + lanes + uint32_t(16 * h), m);
+    guide::tmem_ld8(tm.tmem + lanes + 32u, logit);
+    float mx = -3.4e38f;
+#pragma unroll
+    for (int j = 0; j < guide::Lobes; ++j) {
+        logit[j] += b[32 + j];
+        mx = fmaxf(mx, logit[j]);
+    }
+    float sum = 0.f, mine[4];
+#pragma unroll
+    for (int j = 0; j < guide::Lobes; ++j) {
+        float const e = __expf(logit[j] - mx);
+        sum += e;
+        if (j / 4 == h) {
+            mine[j % 4] = e;
+        }
+    }
+    float const inv = 1.f / sum;
+    float4* const row = rows + r * (Mixture_floats / 4);
+    float         norm[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        int const   o  = 16 * h + 4 * j;
+        float const x  = m[4 * j] + b[o];
+        float const y  = m[4 * j + 1] + b[o + 1];
+        float const z  = m[4 * j + 2] + b[o + 2];
+        float const lk = m[4 * j + 3] + b[o + 3];
+        float const l2 = x * x + y * y + z * z;
+        float const s  = l2 > 1e-20f ? rsqrtf(l2) : 0.f;
+        float const k  = __expf(fminf(fmaxf(lk, guide::Log_kappa_min), guide::Log_kappa_max));
+        row[4 * h + j] = l2 > 1e-20f ? make_float4(s * x, s * y, s * z, k) : make_float4(0.f, 0.f, 1.f, k);
+        norm[j]        = k / (2.f * 3.14159265358979f * -expm1f(-2.f * k));
+        mine[j] *= inv;
+    }
+    row[8 + h]  = make_float4(mine[0], mine[1], mine[2], mine[3]);
+    row[10 + h] = make_float4(mine[0] * norm[0], mine[1] * norm[1], mine[2] * norm[2], mine[3] * norm[3]);
+}
 
-// Persistent: each block loads the network once, then walks tiles, reading the next tile's
-// 8 KB of inputs into registers while the current one is on the tensor cores.
-__global__ void __launch_bounds__(guide::Block, 3)
+// Persistent: each block loads the network once, then walks pairs of tiles, the two
+// interleaved layer by layer so that one tile's MMAs run while the other's results are stored;
+// the next pair's 16 KB of inputs are read into registers meanwhile.  The mixture rows, staged
+// in shared memory, are written to guide_out (entry q at q * Mixture_floats) as contiguous
+// 16-byte stores.
+constexpr uint32_t Infer_tmem_columns = 2 * guide::Tmem_columns;
+
+__global__ void __launch_bounds__(guide::Block, 2)
     k_guide(Paths p, uint32_t const* __restrict__ count, __nv_bfloat16 const* __restrict__ wbf,
             float const* __restrict__ params, uint32_t* error) {
     extern __shared__ __align__(16) unsigned char raw[];
     Infer_smem&    m     = *reinterpret_cast<Infer_smem*>(raw);
     uint32_t const num   = *count;
     uint32_t const tiles = (num + guide::Tile - 1) / guide::Tile;
-    if (blockIdx.x >= tiles) {
+    uint32_t const pairs = (tiles + 1) / 2;
+    if (blockIdx.x >= pairs) {
         return;  // the whole block: no barrier is skipped by only some threads
     }
     constexpr int Tile_uint4 = guide::Tile * guide::Inputs * 2 / 16;  // 512
     static_assert(Tile_uint4 == 2 * guide::Block, "two 16-byte loads per thread per tile");
-    uint4 const* const src = reinterpret_cast<uint4 const*>(p.guide_in);
-    uint4 n0 = src[size_t(blockIdx.x) * Tile_uint4 + threadIdx.x];
-    uint4 n1 = src[size_t(blockIdx.x) * Tile_uint4 + guide::Block + threadIdx.x];
+    uint4 const* const src  = reinterpret_cast<uint4 const*>(p.guide_in);
+    uint4 const        zero = make_uint4(0u, 0u, 0u, 0u);
+    auto const         load = [&](uint32_t tile, int half) {
+        return tile < tiles ? src[size_t(tile) * Tile_uint4 + half * guide::Block + threadIdx.x] : zero;
+    };
+    uint4 n[4] = {load(2 * blockIdx.x, 0), load(2 * blockIdx.x, 1), load(2 * blockIdx.x + 1, 0),
+                  load(2 * blockIdx.x + 1, 1)};
     guide::load_net(m.net, wbf, params);
-    guide::Tmem_tile tm = guide::tc_setup(&m.tmem_slot, &m.mbar, error);
-    __nv_bfloat16* const acts[guide::Layers] = {m.y, m.x, m.y, m.x, m.y};
-    uint4* const         a0 = reinterpret_cast<uint4*>(m.y);
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         guide::smem_u32(&m.tmem_slot)),
+                     "r"(Infer_tmem_columns));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        for (int t = 0; t < 2; ++t) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(guide::smem_u32(&m.mbar[t])), "r"(1));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    guide::tc_fence_before();
+    __syncthreads();
+    guide::tc_fence_after();
+    guide::Tmem_tile tm[2] = {{m.tmem_slot, guide::smem_u32(&m.mbar[0]), 0u, error},
+                              {m.tmem_slot + guide::Tmem_columns, guide::smem_u32(&m.mbar[1]), 0u, error}};
+    guide::Smem_outputs const unused{nullptr};
+    float const* const        b = m.net.b;
 #pragma unroll 1
-    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        a0[threadIdx.x]               = n0;
-        a0[guide::Block + threadIdx.x] = n1;
-        uint32_t const next = tile + gridDim.x;
-        if (next < tiles) {
-            n0 = src[size_t(next) * Tile_uint4 + threadIdx.x];
-            n1 = src[size_t(next) * Tile_uint4 + guide::Block + threadIdx.x];
+    for (uint32_t pair = blockIdx.x; pair < pairs; pair += gridDim.x) {
+        for (int t = 0; t < 2; ++t) {
+            uint4* const in = reinterpret_cast<uint4*>(m.act[t][1]);
+            in[threadIdx.x]                = n[2 * t];
+            in[guide::Block + threadIdx.x] = n[2 * t + 1];
+        }
+        uint32_t const next = pair + gridDim.x;
+        if (next < pairs) {
+            n[0] = load(2 * next, 0);
+            n[1] = load(2 * next, 1);
+            n[2] = load(2 * next + 1, 0);
+            n[3] = load(2 * next + 1, 1);
         }
         guide::fence_async_smem();
         guide::tc_fence_before();
         __syncthreads();
-        // ends with a barrier, after which y may take the next inputs
-        guide::forward_tc(m.net, acts, Guide_outputs{p.guide_out, tile * guide::Tile, num}, tm);
+        // layer l reads act[t][(l + 1) & 1] and writes act[t][l & 1]
+        guide::issue_layer<guide::Inputs, guide::Width>(m.act[0][1], m.net.w + guide::weight_tile_offset(0), tm[0]);
+        guide::issue_layer<guide::Inputs, guide::Width>(m.act[1][1], m.net.w + guide::weight_tile_offset(0), tm[1]);
+#pragma unroll
+        for (int l = 0; l < guide::Layers - 1; ++l) {
+            __nv_bfloat16 const* w_next = m.net.w + guide::weight_tile_offset(l + 1);
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                guide::finish_layer<guide::Width, false>(b + guide::bias_slot(l), m.act[t][l & 1], unused, tm[t]);
+                if (l + 1 < guide::Layers - 1) {
+                    guide::issue_layer<guide::Width, guide::Width>(m.act[t][l & 1], w_next, tm[t]);
+                } else {
+                    guide::issue_layer<guide::Width, guide::Outputs>(m.act[t][l & 1], w_next, tm[t]);
+                }
+            }
+        }
+        // Last layer: both tiles' rows into their (now free) activation buffers, then out.
+        for (int t = 0; t < 2; ++t) {
+            finish_mixture(b + guide::bias_slot(guide::Layers - 1), reinterpret_cast<float4*>(m.act[t]), tm[t]);
+        }
+        guide::tc_fence_before();
+        __syncthreads();
+        for (int t = 0; t < 2; ++t) {
+            uint32_t const base = (2 * pair + uint32_t(t)) * guide::Tile;
+            uint32_t const rows = base < num ? min(uint32_t(guide::Tile), num - base) : 0u;
+            uint4 const*   from = reinterpret_cast<uint4 const*>(m.act[t]);
+            uint4* const   to   = reinterpret_cast<uint4*>(p.guide_out + size_t(base) * Mixture_floats);
+            for (uint32_t i = threadIdx.x; i < rows * (Mixture_floats / 4); i += guide::Block) {
+                to[i] = from[i];
+            }
+        }
+        __syncthreads();  // the rows are read before the next pair's inputs replace them
     }
-    guide::tc_teardown(tm);
+    if (threadIdx.x < 32) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm[0].tmem), "r"(Infer_tmem_columns));
+    }
+}
+
+// ---- the guide's mixture as k_guide stores it per queue entry ----
+// (Mixture_floats per entry; read through L1 by each use.)
+
+__device__ __forceinline__ float mixture_pdf_at(float4 const* __restrict__ row, V3 w) {
+    float4 const c0 = row[10], c1 = row[11];
+    float const  c[guide::Lobes] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    float        q = 0.f;
+#pragma unroll
+    for (int j = 0; j < guide::Lobes; ++j) {
+        float4 const l = row[j];
+        q += c[j] * __expf(l.w * (l.x * w.x + l.y * w.y + l.z * w.z - 1.f));
+    }
+    return q;
+}
+
+// guide::mixture_sample on the stored form.
+__device__ __forceinline__ V3 mixture_sample_at(float4 const* __restrict__ row, float u0, float u1, float u2) {
+    float4 const w0 = row[8], w1 = row[9];
+    float const  w[guide::Lobes] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+    int          j   = guide::Lobes - 1;
+    float        acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < guide::Lobes - 1; ++k) {
+        acc += w[k];
+        if (u0 < acc) {
+            j = k;
+            break;
+        }
+    }
+    float4 const l = row[j];
+    guide::Lobe  lobe;
+    lobe.mu     = v3(l.x, l.y, l.z);
+    lobe.kappa  = l.w;
+    lobe.weight = 1.f;
+    return guide::mixture_sample(&lobe, 0.f, u1, u2);
 }
 
 // ---- shade: one path vertex ----
@@ -1299,25 +1435,7 @@ __global__ void __launch_bounds__(Shade_block)
                 // weights use is the combination of both.
                 bool const  guided = wave.guiding && depth < wave.guide_depth && p.guide_ok[i];
                 float const gf     = guided ? wave.guide_fraction : 0.f;
-                guide::Lobe lobes[guide::Lobes];
-                if (guided) {
-                    float4 const* src = reinterpret_cast<float4 const*>(p.guide_out + size_t(i) * guide::Outputs);
-#pragma unroll
-                    for (int j = 0; j < guide::Lobes; ++j) {
-                        float4 const v = src[j];
-                        lobes[j].mu    = v3(v.x, v.y, v.z);
-                        lobes[j].kappa = v.w;
-                    }
-                    float4 const w0 = src[8], w1 = src[9];
-                    lobes[0].weight = w0.x;
-                    lobes[1].weight = w0.y;
-                    lobes[2].weight = w0.z;
-                    lobes[3].weight = w0.w;
-                    lobes[4].weight = w1.x;
-                    lobes[5].weight = w1.y;
-                    lobes[6].weight = w1.z;
-                    lobes[7].weight = w1.w;
-                }
+                float4 const* const mix = reinterpret_cast<float4 const*>(p.guide_out + size_t(i) * Mixture_floats);
 
                 // Next-event estimation (sample_lights / evaluate_light, pathtracer_mis.cpp:281-347).
                 int const samples = num_light_samples(s, depth);
@@ -1330,7 +1448,7 @@ __global__ void __launch_bounds__(Shade_block)
                     if (sample_light(s, ps, geo_n, false, r, r1, r2, ls, light_mode(samples, k))) {
                         shading::Bxdf const f =
                             shading::substitute_evaluate(mat, s.e_table, ctx, ls.dir);
-                        float const pc = guided ? gf * guide::mixture_pdf(lobes, ls.dir) + (1.f - gf) * f.pdf
+                        float const pc = guided ? gf * mixture_pdf_at(mix, ls.dir) + (1.f - gf) * f.pdf
                                                 : f.pdf;
                         float const w  = ls.pdf / (ls.pdf * ls.pdf + pc * pc);
                         V3 const contrib = w * (T * (ls.radiance * f.reflection));
@@ -1348,7 +1466,7 @@ __global__ void __launch_bounds__(Shade_block)
                     float const g0 = rng.uniform();
                     float const g1 = rng.uniform();
                     float const g2 = rng.uniform();
-                    smp.wi       = guide::mixture_sample(lobes, g0, g1, g2);
+                    smp.wi       = mixture_sample_at(mix, g0, g1, g2);
                     smp.specular = false;
                     if (shading::dot(smp.wi, geo_n) > 0.f) {
                         shading::Bxdf const f = shading::substitute_evaluate(mat, s.e_table, ctx, smp.wi);
@@ -1365,7 +1483,7 @@ __global__ void __launch_bounds__(Shade_block)
                 }
                 if (smp.pdf > 0.f) {
                     float const pdf = guided && !smp.specular
-                                          ? gf * guide::mixture_pdf(lobes, smp.wi) + (1.f - gf) * smp.pdf
+                                          ? gf * mixture_pdf_at(mix, smp.wi) + (1.f - gf) * smp.pdf
                                           : smp.pdf;
                     if (guided && depth < wave.record_depth) {
                         // training record of this vertex (its radiance mark comes at the next)
@@ -1546,67 +1664,64 @@ __global__ void k_gather(Paths p, uint32_t w, uint32_t h, uint32_t samples, floa
 // Batch entry i takes record hash(i, pass) of the wave; a finished record (radiance mark set)
 // gives the input encoding, the continuation direction and the weight
 // luminance((L_final - L_mark) / T): the continuation's radiance times f cos / pdf at the
-// vertex, the target of the product-guiding loss.  Other records give weight 0.
-__global__ void k_train_gather(Paths p, Wave wave, uint32_t records, uint32_t batch, uint32_t pass,
-                               float* in, float* dir, float* weight) {
-    uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= batch) {
-        return;
+// vertex, the target of the product-guiding loss.  Other records, and rows past the batch up to
+// the tile boundary, give weight 0 and zero inputs.  The inputs are written as the training
+// kernel reads them (BF16 tiles of 128 rows); each block adds its weights in a fixed order into
+// parts[block] (the loss is normalised by their total).
+__global__ void __launch_bounds__(256)
+    k_train_gather(Paths p, Wave wave, uint32_t records, uint32_t batch, uint32_t pass, __nv_bfloat16* in,
+                   float* dir, float* weight, float* parts) {
+    __shared__ float part[256];
+    uint32_t const   i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t const   rows = (batch + guide::Tile - 1) / guide::Tile * guide::Tile;
+    float            w    = 0.f;
+    float            enc[guide::Inputs];
+    if (i < batch) {
+        uint64_t const h = (uint64_t(i) * 0x9E3779B97F4A7C15ull) ^ (uint64_t(pass + 1) * 0xD1B54A32D192ED03ull);
+        uint32_t const r = uint32_t(((h ^ (h >> 29)) * 0xBF58476D1CE4E5B9ull >> 32) % records);
+        float4 const*  d = p.rec + size_t(r) * Record_float4;
+        float4 const   mark = d[4];
+        float4 const   a = d[0], b = d[1], c = d[2], t = d[3];
+        if (mark.w == 1.f) {
+            uint32_t const path = r / wave.record_depth;
+            float4 const   l    = p.L[path];
+            float4 const   l2   = p.L2[path];
+            float const    cx   = t.x > 0.f ? (l.x + l2.x - mark.x) / t.x : 0.f;
+            float const    cy   = t.y > 0.f ? (l.y + l2.y - mark.y) / t.y : 0.f;
+            float const    cz   = t.z > 0.f ? (l.z + l2.z - mark.z) / t.z : 0.f;
+            // AP1 (ACEScg) luminance
+            float const lum = 0.2722287f * cx + 0.6740818f * cy + 0.0536895f * cz;
+            w               = (lum > 0.f && lum < 1e30f) ? lum : 0.f;
+        }
+        guide::encode(box_coordinates(wave, v3(a.x, a.y, a.z)), v3(a.w, b.x, b.y), v3(b.z, b.w, c.x), enc);
+        dir[3 * size_t(i)]     = w > 0.f ? c.y : 0.f;
+        dir[3 * size_t(i) + 1] = w > 0.f ? c.z : 0.f;
+        dir[3 * size_t(i) + 2] = w > 0.f ? c.w : 1.f;
+        weight[i]              = w;
     }
-    uint64_t const h = (uint64_t(i) * 0x9E3779B97F4A7C15ull) ^ (uint64_t(pass + 1) * 0xD1B54A32D192ED03ull);
-    uint32_t const r = uint32_t(((h ^ (h >> 29)) * 0xBF58476D1CE4E5B9ull >> 32) % records);
-    float4 const*  d = p.rec + size_t(r) * Record_float4;
-    float4 const   mark = d[4];
-    float          w    = 0.f;
-    float4 const   a = d[0], b = d[1], c = d[2], t = d[3];
-    if (mark.w == 1.f) {
-        uint32_t const path = r / wave.record_depth;
-        float4 const   l    = p.L[path];
-        float4 const   l2   = p.L2[path];
-        float const    cx   = t.x > 0.f ? (l.x + l2.x - mark.x) / t.x : 0.f;
-        float const    cy   = t.y > 0.f ? (l.y + l2.y - mark.y) / t.y : 0.f;
-        float const    cz   = t.z > 0.f ? (l.z + l2.z - mark.z) / t.z : 0.f;
-        // AP1 (ACEScg) luminance
-        float const lum = 0.2722287f * cx + 0.6740818f * cy + 0.0536895f * cz;
-        w               = (lum > 0.f && lum < 1e30f) ? lum : 0.f;
+    if (i < rows) {
+        __nv_bfloat16* const tile = in + size_t(i / guide::Tile) * guide::Tile * guide::Inputs;
+        int const            r    = int(i % guide::Tile);
+#pragma unroll
+        for (int k = 0; k < guide::Inputs; k += 8) {
+            __nv_bfloat162 h[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                h[j] = __floats2bfloat162_rn(w > 0.f ? enc[k + 2 * j] : 0.f, w > 0.f ? enc[k + 2 * j + 1] : 0.f);
+            }
+            *reinterpret_cast<uint4*>(tile + guide::tiled(r, k, guide::Inputs)) = *reinterpret_cast<uint4*>(h);
+        }
     }
-    float enc[guide::Inputs];
-    guide::encode(box_coordinates(wave, v3(a.x, a.y, a.z)), v3(a.w, b.x, b.y), v3(b.z, b.w, c.x), enc);
-    for (int k = 0; k < guide::Inputs; ++k) {
-        in[size_t(i) * guide::Inputs + k] = w > 0.f ? enc[k] : 0.f;
-    }
-    dir[3 * size_t(i)]     = w > 0.f ? c.y : 0.f;
-    dir[3 * size_t(i) + 1] = w > 0.f ? c.z : 0.f;
-    dir[3 * size_t(i) + 2] = w > 0.f ? c.w : 1.f;
-    weight[i]              = w;
-}
-
-// sum = the weights' total, in a fixed order (one block of 1024 threads).
-__global__ void __launch_bounds__(1024) k_sum_weights(float const* weight, uint32_t n, float* sum) {
-    __shared__ float part[1024];
-    float            acc = 0.f;
-    for (uint32_t i = threadIdx.x; i < n; i += 1024) {
-        acc += weight[i];
-    }
-    part[threadIdx.x] = acc;
+    part[threadIdx.x] = w;
     __syncthreads();
-    for (int w = 512; w > 0; w >>= 1) {
-        if (threadIdx.x < w) {
-            part[threadIdx.x] += part[threadIdx.x + w];
+    for (int o = 128; o > 0; o >>= 1) {
+        if (int(threadIdx.x) < o) {
+            part[threadIdx.x] += part[threadIdx.x + o];
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        *sum = part[0];
-    }
-}
-
-// scale_i = weight_i / sum: the batch loss becomes the weighted mean of -log q.
-__global__ void k_scale_weights(float const* weight, float const* sum, uint32_t n, float* scale) {
-    uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        float const s = *sum;
-        scale[i]      = s > 0.f ? weight[i] / s : 0.f;
+        parts[blockIdx.x] = part[0];
     }
 }
 
@@ -1653,11 +1768,10 @@ struct Renderer::Device {
     uint32_t           guide_paths   = 0;  // paths the guide buffers hold
     uint32_t           guide_records = 0;  // record depth they were sized for
     uint32_t           train_capacity = 0;
-    float*             train_in    = nullptr;
+    __nv_bfloat16*     train_in    = nullptr;  // the batch's inputs, BF16 tiles of 128
     float*             train_dir   = nullptr;
     float*             train_w     = nullptr;
-    float*             train_scale = nullptr;
-    float*             train_sum   = nullptr;
+    float*             train_parts = nullptr;  // per gather block: its weights' sum
     uint32_t           pass        = 0;  // training passes since the scene was set
     // paths
     uint32_t  capacity = 0;
@@ -1787,8 +1901,7 @@ Renderer::~Renderer() {
     free_ptr(d_->train_in);
     free_ptr(d_->train_dir);
     free_ptr(d_->train_w);
-    free_ptr(d_->train_scale);
-    free_ptr(d_->train_sum);
+    free_ptr(d_->train_parts);
     free_ptr(d_->nodes);
     free_ptr(d_->tris);
     free_ptr(d_->tri_info);
@@ -2133,7 +2246,7 @@ int32_t Renderer::ensure_guide(uint32_t paths) {
         size_t const n = d_->capacity;
         size_t const tiled_entries = (n + guide::Tile - 1) / guide::Tile * guide::Tile;
         SPB_RCUDA(cudaMalloc(&p.guide_in, tiled_entries * guide::Inputs * sizeof(__nv_bfloat16)));
-        SPB_RCUDA(cudaMalloc(&p.guide_out, n * guide::Outputs * sizeof(float)));
+        SPB_RCUDA(cudaMalloc(&p.guide_out, n * Mixture_floats * sizeof(float)));
         SPB_RCUDA(cudaMalloc(&p.guide_ok, n));
         SPB_RCUDA(cudaMalloc(&p.rec, n * rd * Record_float4 * sizeof(float4)));
         SPB_RCUDA(cudaMalloc(&p.open_record, n * sizeof(uint32_t)));
@@ -2145,13 +2258,12 @@ int32_t Renderer::ensure_guide(uint32_t paths) {
         free_ptr(d_->train_in);
         free_ptr(d_->train_dir);
         free_ptr(d_->train_w);
-        free_ptr(d_->train_scale);
-        free_ptr(d_->train_sum);
-        SPB_RCUDA(cudaMalloc(&d_->train_in, size_t(batch) * guide::Inputs * sizeof(float)));
+        free_ptr(d_->train_parts);
+        size_t const rows = (size_t(batch) + guide::Tile - 1) / guide::Tile * guide::Tile;
+        SPB_RCUDA(cudaMalloc(&d_->train_in, rows * guide::Inputs * sizeof(__nv_bfloat16)));
         SPB_RCUDA(cudaMalloc(&d_->train_dir, size_t(batch) * 3 * sizeof(float)));
         SPB_RCUDA(cudaMalloc(&d_->train_w, size_t(batch) * sizeof(float)));
-        SPB_RCUDA(cudaMalloc(&d_->train_scale, size_t(batch) * sizeof(float)));
-        SPB_RCUDA(cudaMalloc(&d_->train_sum, sizeof(float)));
+        SPB_RCUDA(cudaMalloc(&d_->train_parts, (rows + 255) / 256 * sizeof(float)));
         d_->train_capacity = batch;
     }
     if (!d_->net_ready) {
@@ -2186,13 +2298,13 @@ int32_t Renderer::train_guide(uint32_t paths, void const* wave_ptr) {
     cudaStream_t   st      = d_->stream;
     uint32_t const batch   = settings_.guide_batch;
     uint32_t const records = paths * settings_.record_depth;
+    // one thread per batch row, the last tile's rows past the batch included
+    uint32_t const gather_blocks = ((batch + guide::Tile - 1) / guide::Tile * guide::Tile + 255) / 256;
     for (uint32_t step = 0; step < settings_.guide_steps; ++step) {
-        k_train_gather<<<(batch + 255) / 256, 256, 0, st>>>(d_->paths, wave, records, batch, d_->pass++,
-                                                            d_->train_in, d_->train_dir, d_->train_w);
-        k_sum_weights<<<1, 1024, 0, st>>>(d_->train_w, batch, d_->train_sum);
-        k_scale_weights<<<(batch + 255) / 256, 256, 0, st>>>(d_->train_w, d_->train_sum, batch,
-                                                             d_->train_scale);
-        SPB_RCUDA(cudaError_t(d_->net.gradients(d_->train_in, d_->train_dir, d_->train_scale, batch, st)));
+        k_train_gather<<<gather_blocks, 256, 0, st>>>(d_->paths, wave, records, batch, d_->pass++, d_->train_in,
+                                                      d_->train_dir, d_->train_w, d_->train_parts);
+        SPB_RCUDA(cudaError_t(d_->net.gradients_tiled(d_->train_in, d_->train_dir, d_->train_w, batch,
+                                                      d_->train_parts, gather_blocks, st)));
         SPB_RCUDA(cudaError_t(d_->net.adam(settings_.guide_lr, st)));
     }
     return SPB_OK;

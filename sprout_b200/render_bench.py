@@ -233,7 +233,7 @@ def measure_guiding(width=1280, height=720, reference_spp=4096, target=0.01, gui
                          "wall_seconds": round(wall, 3)})
             if err <= target:
                 break
-            spp = int(np.ceil(spp * err / target / 8.0)) * 8 + 8
+            spp = max(spp + 8, int(np.ceil(spp * err / target / 8.0)) * 8)
         return runs
 
     plain_v = (e - c) * probe
