@@ -60,11 +60,11 @@ struct Settings {
     bool     guiding         = false;
     float    guide_fraction  = 0.5f;
     uint32_t guide_batch     = 1u << 16;
-    uint32_t guide_steps     = 64;
+    uint32_t guide_steps     = 32;
     float    guide_lr        = 1e-2f;
     uint32_t record_depth    = 2;
     uint32_t guide_seed      = 7;
-    uint32_t guide_pass_spp  = 4;   // samples per pixel between training steps
+    uint32_t guide_pass_spp  = 2;   // samples per pixel between training steps
     uint32_t guide_train_spp = 32;  // samples per pixel after which training stops (0: never)
     uint32_t guide_depth     = 255;  // vertices of depth below this are guided
 };
