@@ -168,8 +168,11 @@ SPB_API int32_t spb_intersect_host_static(spb_tree* tree, float const* rays, uin
  * Counters of the path tracer's last su_render / su_render_frame / su_render_iteration call
  * (the su_* engine of include/sprout.h): camera samples traced, closest-hit rays (camera and
  * continuation), any-hit (shadow) rays, and the device time between the first and last
- * kernel.  No counterpart in the reference (it logs wall-clock phases only,
- * rendering_driver.cpp:99-136).  SPB_ERROR_ARGUMENT if there is no engine.
+ * kernel.  With path guiding: the vertices the network was evaluated for and the device time
+ * of that inference (input encoding included), and the training samples (Adam steps x batch)
+ * and the device time of training (batch gathering, gradients, Adam).  No counterpart in the
+ * reference (it logs wall-clock phases only, rendering_driver.cpp:99-136).
+ * SPB_ERROR_ARGUMENT if there is no engine.
  */
 typedef struct spb_render_stats {
     uint64_t paths;
@@ -177,6 +180,10 @@ typedef struct spb_render_stats {
     uint64_t shadow_rays;
     double   device_seconds;
     uint32_t overflow;
+    uint64_t guide_vertices;
+    double   guide_inference_seconds;
+    uint64_t guide_training_samples;
+    double   guide_training_seconds;
 } spb_render_stats;
 SPB_API int32_t spb_render_last_stats(spb_render_stats* out);
 

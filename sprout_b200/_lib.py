@@ -44,6 +44,10 @@ class RenderStats(ctypes.Structure):
         ("shadow_rays", c_u64),
         ("device_seconds", ctypes.c_double),
         ("overflow", c_u32),
+        ("guide_vertices", c_u64),
+        ("guide_inference_seconds", ctypes.c_double),
+        ("guide_training_samples", c_u64),
+        ("guide_training_seconds", ctypes.c_double),
     ]
 
 

@@ -1112,6 +1112,10 @@ SPB_API int32_t spb_render_last_stats(spb_render_stats* out) {
     out->shadow_rays    = st.shadow_rays;
     out->device_seconds = st.seconds;
     out->overflow       = st.overflow;
+    out->guide_vertices          = st.guide_vertices;
+    out->guide_inference_seconds = st.guide_inference_seconds;
+    out->guide_training_samples  = st.guide_training_samples;
+    out->guide_training_seconds  = st.guide_training_seconds;
     return SPB_OK;
 }
 

@@ -1765,6 +1765,8 @@ struct Renderer::Device {
     guide::Network     net;
     bool               net_ready     = false;
     uint32_t           guide_grid    = 1;      // k_guide blocks (persistent)
+    // event pairs around the guide's inference and training launches of one render call
+    std::vector<cudaEvent_t> guide_events;
     uint32_t           guide_paths   = 0;  // paths the guide buffers hold
     uint32_t           guide_records = 0;  // record depth they were sized for
     uint32_t           train_capacity = 0;
@@ -1955,6 +1957,9 @@ Renderer::~Renderer() {
     }
     cudaEventDestroy(d_->ev0);
     cudaEventDestroy(d_->ev1);
+    for (cudaEvent_t e : d_->guide_events) {
+        cudaEventDestroy(e);
+    }
     delete d_;
 }
 
@@ -2379,6 +2384,19 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
 
     stats_ = Stats();
     std::vector<uint32_t> host_ctr(Counter_words);
+    // Device time of the guide's stages: event pairs (inference after each trace, training
+    // after each pass), summed once the call is done.
+    size_t              events_used = 0;
+    std::vector<size_t> train_pairs;
+    std::vector<bool>   guided_bounce(Max_bounce_slots, false);
+    auto const          guide_event = [&](size_t i) {
+        while (d_->guide_events.size() <= i) {
+            cudaEvent_t e = nullptr;
+            cudaEventCreate(&e);
+            d_->guide_events.push_back(e);
+        }
+        return d_->guide_events[i];
+    };
     SPB_RCUDA(cudaEventRecord(d_->ev0, st));
     for (uint32_t done = 0; done < num_samples;) {
         bool const training = settings_.guiding &&
@@ -2414,9 +2432,12 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
                                                                    ctr + Overflow_slot);
             // (without media a vertex's depth is the iteration; with media it can be less)
             if (settings_.guiding && (d_->has_media || b < settings_.guide_depth)) {
+                SPB_RCUDA(cudaEventRecord(guide_event(events_used++), st));
                 k_guide_encode<<<(paths + 255) / 256, 256, 0, st>>>(sg, wave, d_->paths, q_in, c);
                 k_guide<<<d_->guide_grid, guide::Block, sizeof(Infer_smem), st>>>(
                     d_->paths, c, d_->net.weights(), d_->net.parameters(), ctr + Overflow_slot + 1);
+                SPB_RCUDA(cudaEventRecord(guide_event(events_used++), st));
+                guided_bounce[b] = true;
             }
             k_shade<<<(paths + Shade_block - 1) / Shade_block, Shade_block, 0, st>>>(
                 sg, wave, d_->paths, q_in, c, q_out, c + Counter_stride, d_->shadow_queue, c + 1);
@@ -2432,9 +2453,13 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             }
         }
         if (training) {
+            SPB_RCUDA(cudaEventRecord(guide_event(events_used++), st));
             if (int32_t const e = train_guide(paths, &wave)) {
                 return e;
             }
+            SPB_RCUDA(cudaEventRecord(guide_event(events_used++), st));
+            train_pairs.push_back(events_used - 2);
+            stats_.guide_training_samples += uint64_t(settings_.guide_steps) * settings_.guide_batch;
         }
         k_gather<<<(camera_.width * camera_.height + 255) / 256, 256, 0, st>>>(
             d_->paths, camera_.width, camera_.height, k, d_->film, d_->comp);
@@ -2445,6 +2470,10 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         for (uint32_t b = 0; b < iterations; ++b) {
             stats_.extension_rays += host_ctr[Counter_stride * b];
             stats_.shadow_rays += host_ctr[Counter_stride * b + 1];
+            if (guided_bounce[b]) {
+                stats_.guide_vertices += host_ctr[Counter_stride * b];
+                guided_bounce[b] = false;
+            }
         }
         stats_.overflow += host_ctr[Overflow_slot];
         if (host_ctr[Overflow_slot + 1]) {
@@ -2459,6 +2488,13 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, d_->ev0, d_->ev1);
     stats_.seconds = double(ms) * 1e-3;
+    for (size_t i = 0, t = 0; i + 1 < events_used; i += 2) {
+        float pair_ms = 0.f;
+        cudaEventElapsedTime(&pair_ms, d_->guide_events[i], d_->guide_events[i + 1]);
+        bool const train = t < train_pairs.size() && train_pairs[t] == i;
+        (train ? stats_.guide_training_seconds : stats_.guide_inference_seconds) += double(pair_ms) * 1e-3;
+        t += train ? 1 : 0;
+    }
     return SPB_OK;
 }
 

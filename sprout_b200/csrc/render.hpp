@@ -75,6 +75,10 @@ struct Stats {
     uint64_t shadow_rays    = 0;  // any-hit rays
     double   seconds        = 0.0;  // device time of the last render call
     uint32_t overflow       = 0;  // rays dropped by the traversal stack guard (0 expected)
+    uint64_t guide_vertices          = 0;    // queue entries the guide network was run for
+    double   guide_inference_seconds = 0.0;  // device time of encoding + inference
+    uint64_t guide_training_samples  = 0;    // Adam steps x batch
+    double   guide_training_seconds  = 0.0;  // device time of training
 };
 
 class Renderer {

@@ -173,11 +173,12 @@ GUIDING_CONFIG = ("doorway interior (sprout_b200.scenes.doorway): 6 x 6 x 3 m ro
                   "diffuse / 30 % GGX conductors alpha U[0.1, 0.6]; PTMIS max depth 8 (Russian roulette from 4)")
 
 
-def doorway_frame(width, height, spp, guiding=None, seed=0):
+def doorway_frame(width, height, spp, guiding=None, seed=0, stats_out=None):
     """One frame of the doorway interior through the su_* API: (RGB image as float64, device
     seconds of the render, wall seconds of su_render_frame + su_postprocess + framebuffer copy).
     The scene is built and uploaded before the timed frame (su_start_render_frame); a guided
-    frame starts from an untrained network all the same (the first frame of the engine)."""
+    frame starts from an untrained network all the same (the first frame of the engine).
+    stats_out (a dict), when given, receives the frame's spb_render_stats fields."""
     lib = _lib.load()
     stats = _lib.RenderStats()
     su = capi.SuLibrary()
@@ -191,9 +192,43 @@ def doorway_frame(width, height, spp, guiding=None, seed=0):
         img = su.framebuffer(width, height)[0][:, :, :3].astype(np.float64)
         wall = time.perf_counter() - t0
         assert lib.spb_render_last_stats(ctypes.byref(stats)) == 0
+        if stats_out is not None:
+            stats_out.update({name: getattr(stats, name) for name, _ in stats._fields_})
         return img, stats.device_seconds, wall
     finally:
         su.su_release()
+
+
+# Algorithmic FLOPs of the guiding network (32 -> 64 x 4 -> 40): forward per vertex; a training
+# sample adds dW of every layer (as many again) and dA of layers 1..4.
+GUIDE_FORWARD_FLOP = 2 * (32 * 64 + 3 * 64 * 64 + 64 * 40)  # 33,792
+GUIDE_TRAIN_FLOP = 2 * GUIDE_FORWARD_FLOP + 2 * (3 * 64 * 64 + 64 * 40)  # 97,280
+
+
+def network_roofline(stats):
+    """The network's share of a guided frame against the tensor-core roofline: achieved
+    algorithmic TFLOP/s of inference (input encoding included) and of training (batch gathering
+    and Adam included) over their device time, as a fraction of the measured sustained BF16
+    GEMM rate (MEASURED_PEAKS.json; the fallback figure when the file is absent)."""
+    import pathlib
+
+    peaks = pathlib.Path(__file__).resolve().parent.parent / "MEASURED_PEAKS.json"
+    peak, kind = 1400.0, "fallback"
+    if peaks.exists():
+        peak, kind = float(json.loads(peaks.read_text())["bf16_tflops_sustained"]), "measured"
+    out = {"peak_tflops": peak, "peak_kind": f"{kind}, sustained bf16", "unit": "TFLOP/s",
+           "flop_per_vertex": GUIDE_FORWARD_FLOP, "flop_per_training_sample": GUIDE_TRAIN_FLOP}
+    if stats.get("guide_inference_seconds", 0) > 0:
+        a = stats["guide_vertices"] * GUIDE_FORWARD_FLOP / stats["guide_inference_seconds"] / 1e12
+        out["inference"] = {"vertices": stats["guide_vertices"],
+                            "seconds": round(stats["guide_inference_seconds"], 4),
+                            "achieved": round(a, 2), "frac": round(a / peak, 4)}
+    if stats.get("guide_training_seconds", 0) > 0:
+        a = stats["guide_training_samples"] * GUIDE_TRAIN_FLOP / stats["guide_training_seconds"] / 1e12
+        out["training"] = {"samples": stats["guide_training_samples"],
+                           "seconds": round(stats["guide_training_seconds"], 4),
+                           "achieved": round(a, 2), "frac": round(a / peak, 4)}
+    return out
 
 
 def measure_guiding(width=1280, height=720, reference_spp=4096, target=0.01, guiding=True):
@@ -224,10 +259,12 @@ def measure_guiding(width=1280, height=720, reference_spp=4096, target=0.01, gui
                          "device_seconds": round(ref_s, 3), "rel_mse_share": round(c, 6)},
            "target": target}
 
+    last_stats = {}
+
     def reach(first, guided):
         spp, runs = first, []
         for _ in range(4):
-            img, dev, wall = doorway_frame(width, height, spp, guiding if guided else None)
+            img, dev, wall = doorway_frame(width, height, spp, guiding if guided else None, stats_out=last_stats)
             err = raw(img) - c
             runs.append({"spp": spp, "rel_mse": round(err, 5), "device_seconds": round(dev, 4),
                          "wall_seconds": round(wall, 3)})
@@ -243,6 +280,7 @@ def measure_guiding(width=1280, height=720, reference_spp=4096, target=0.01, gui
     guided = reach(int(np.ceil(guided_v / target / 8.0)) * 8, True)
     out["plain"] = plain[-1]
     out["guided"] = guided[-1]
+    out["network"] = network_roofline(last_stats)
     out["runs"] = {"plain": plain, "guided": guided}
     if plain[-1]["rel_mse"] <= target and guided[-1]["rel_mse"] <= target:
         out["guided_over_plain_device_time"] = round(guided[-1]["device_seconds"] / plain[-1]["device_seconds"], 4)
@@ -252,7 +290,9 @@ def measure_guiding(width=1280, height=720, reference_spp=4096, target=0.01, gui
 
 def main():
     p = argparse.ArgumentParser()
-    p.add_argument("--scene", choices=sorted(SCENES) + ["volume", "guiding"], default="cornell")
+    p.add_argument("--scene", choices=sorted(SCENES) + ["volume", "guiding", "doorway"], default="cornell",
+                   help="doorway: one frame of the guiding workload (plain MIS, or --guided)")
+    p.add_argument("--guided", action="store_true", help="doorway: learned path guiding")
     p.add_argument("--views", type=int, default=4, help="volume workload: number of views")
     p.add_argument("--width", type=int)
     p.add_argument("--height", type=int)
@@ -265,6 +305,14 @@ def main():
         print(json.dumps(measure_volume(a.views, a.spp or 128, a.cpu_reference)))
     elif a.scene == "guiding":
         print(json.dumps(measure_guiding(a.width or 1280, a.height or 720)))
+    elif a.scene == "doorway":
+        w, h, spp = a.width or 1280, a.height or 720, a.spp or 64
+        st = {}
+        img, dev, wall = doorway_frame(w, h, spp, True if a.guided else None, stats_out=st)
+        print(json.dumps({"workload": "doorway", "guided": a.guided, "config": f"{GUIDING_CONFIG}, {w}x{h}, {spp} spp",
+                          "device_seconds": round(dev, 4), "wall_seconds": round(wall, 4),
+                          "msamples_s": round(w * h * spp / dev / 1e6, 3), "mean": float(img.mean()),
+                          "stats": st, "network": network_roofline(st) if a.guided else None}))
     else:
         print(json.dumps(measure(a.scene, a.width, a.height, a.spp, a.frames, a.convergence, a.cpu_reference)))
 

@@ -50,6 +50,25 @@ def test_guided_converges_to_plain(reference):
     assert worst < 0.03, f"worst 16x16 block deviation {worst:.4f}"
 
 
+def test_guided_matches_reference_image():
+    """The guided integrator against the reference renderer's own converged image of the
+    doorway interior (plain MIS, 8,192 spp; tests/golden/cornell_reference.npz), with the
+    statistical bounds of the plain parity test."""
+    import json
+    import pathlib
+
+    data = np.load(pathlib.Path(__file__).resolve().parent / "golden" / "cornell_reference.npz")
+    meta = json.loads(bytes(data["meta"]).decode())["cases"]["doorway96"]
+    ref = data["doorway96"].astype(np.float64)
+    img, _, _ = doorway_frame(meta["width"], meta["height"], 4 * meta["spp"], True)
+    m_ref, m_img = ref.mean(axis=(0, 1)), img.mean(axis=(0, 1))
+    assert np.all(np.abs(m_img - m_ref) <= 0.005 * m_ref), (m_img, m_ref)
+    b = meta["block"]
+    bi, br = block_means(img, b), block_means(ref, b)
+    worst = np.max(np.abs(bi - br) / (np.abs(br) + 0.01))
+    assert worst < 0.02, f"worst {b}x{b} block deviation {worst:.4f}"
+
+
 def test_guiding_settings_are_parsed():
     """The integrator's "guiding" object: explicit settings render, and training can stop
     early (train_spp) with the rest of the frame sampled by the frozen network."""
