@@ -48,6 +48,8 @@ class RenderStats(ctypes.Structure):
         ("guide_inference_seconds", ctypes.c_double),
         ("guide_training_samples", c_u64),
         ("guide_training_seconds", ctypes.c_double),
+        ("wave_paths", c_u32),
+        ("trace_blocks_per_sm", c_u32),
     ]
 
 

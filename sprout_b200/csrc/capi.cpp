@@ -598,6 +598,11 @@ SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
             // "seed": the sample streams' seed (this renderer's extension, default 0), for
             // statistically independent renders of one scene
             s.seed = uint32_t(spb::json::number_or(pt->find("seed"), s.seed));
+            // "wave_paths", "trace_blocks_per_sm": fixed launch shapes instead of the autotuner's
+            // (this renderer's extension)
+            s.wave_paths          = uint32_t(spb::json::number_or(pt->find("wave_paths"), 0.0));
+            s.trace_blocks_per_sm = uint32_t(spb::json::number_or(pt->find("trace_blocks_per_sm"), 0.0));
+            s.wave_paths          = s.wave_paths ? std::clamp(s.wave_paths, 1u << 16, 1u << 24) : 0u;
             // "guiding": true, or an object of the Settings guide fields (this renderer's
             // extension; the reference ignores the key)
             if (spb::json::Value const* g = pt->find("guiding")) {
@@ -1116,6 +1121,8 @@ SPB_API int32_t spb_render_last_stats(spb_render_stats* out) {
     out->guide_inference_seconds = st.guide_inference_seconds;
     out->guide_training_samples  = st.guide_training_samples;
     out->guide_training_seconds  = st.guide_training_seconds;
+    out->wave_paths              = st.wave_paths;
+    out->trace_blocks_per_sm     = st.trace_blocks_per_sm;
     return SPB_OK;
 }
 

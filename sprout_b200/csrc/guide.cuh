@@ -106,9 +106,18 @@ SPB_HD float mixture_pdf(Lobe const lobes[Lobes], shading::V3 w) {
     return p;
 }
 
-// Samples the mixture with three uniform numbers: a lobe by weight, then its cosine to the
-// mean by the inverse CDF of the vMF (Wenzel Jakob, "Numerically stable sampling of the von
-// Mises Fisher distribution on S2", 2012), then the azimuth.
+// Samples one lobe with two uniform numbers: the cosine to the mean by the inverse CDF of the
+// vMF (Wenzel Jakob, "Numerically stable sampling of the von Mises Fisher distribution on S2",
+// 2012), clamped to [-1, 1], then the azimuth.
+SPB_HD shading::V3 vmf_sample(Lobe const& l, float u1, float u2) {
+    float const c = fminf(fmaxf(1.f + logf(u1 + (1.f - u1) * expf(-2.f * l.kappa)) / l.kappa, -1.f), 1.f);
+    float const s = sqrtf(fmaxf(0.f, 1.f - c * c));
+    float const phi = 2.f * 3.14159265358979f * u2;
+    shading::Frame const f = shading::make_frame(l.mu);
+    return (s * cosf(phi)) * f.t + (s * sinf(phi)) * f.b + c * f.n;
+}
+
+// Samples the mixture with three uniform numbers: a lobe by weight, then vmf_sample.
 SPB_HD shading::V3 mixture_sample(Lobe const lobes[Lobes], float u0, float u1, float u2) {
     int   j   = Lobes - 1;
     float acc = 0.f;
@@ -119,12 +128,7 @@ SPB_HD shading::V3 mixture_sample(Lobe const lobes[Lobes], float u0, float u1, f
             break;
         }
     }
-    Lobe const& l = lobes[j];
-    float const c = 1.f + logf(u1 + (1.f - u1) * expf(-2.f * l.kappa)) / l.kappa;
-    float const s = sqrtf(fmaxf(0.f, 1.f - c * c));
-    float const phi = 2.f * 3.14159265358979f * u2;
-    shading::Frame const f = shading::make_frame(l.mu);
-    return (s * cosf(phi)) * f.t + (s * sinf(phi)) * f.b + c * f.n;
+    return vmf_sample(lobes[j], u1, u2);
 }
 
 }  // namespace spb::guide

@@ -58,6 +58,63 @@ constexpr uint32_t Class_boundary   = 2;  // ... of participating-medium boundar
 // Counter block (uint32): per bounce b, [8b] extension count, [8b+1] shadow count,
 // [8b+2] extend fetch, [8b+3] shadow fetch, [8b+4] transmittance count; then the overflow
 // counter.
+// Online autotuner of the wave size (paths per wave) and the traversal kernels' grid (blocks
+// per SM).  The waves of a frame try the candidates in turn -- wave sizes at the largest
+// occupancy first, then lower occupancies at the best size -- each timed with CUDA events
+// (device time per path of the whole wave); the best is kept for the rest of the frame and for
+// later frames of the scene.  Which samples are drawn does not depend on the wave size (each
+// sample's stream is fixed by its pixel and sample index), so tuning renders no extra work.
+struct Tuner {
+    static constexpr uint32_t Wave_sizes[5] = {1u << 20, 1u << 21, 1u << 22, 1u << 23, 1u << 24};
+    static constexpr uint32_t Sizes          = 5;
+    static constexpr uint32_t Max_wave_paths = 1u << 24;
+    uint32_t max_per_sm = 1;   // most traversal blocks an SM holds
+    uint32_t stage      = 0;   // 0: wave sizes, 1: occupancies, 2: done
+    uint32_t candidate  = 0;
+    uint32_t wave_paths = 1u << 22;
+    uint32_t per_sm     = 1;
+    double   best_ns    = 1e300;  // device ns per path of the best candidate so far
+    uint32_t best_wave  = 1u << 22;
+    uint32_t best_sm    = 1;
+
+    void reset(uint32_t max_blocks) {
+        *this      = Tuner();
+        max_per_sm = std::max(1u, max_blocks);
+        per_sm     = max_per_sm;
+        best_sm    = max_per_sm;
+        wave_paths = Wave_sizes[0];
+    }
+    bool     done() const { return stage == 2; }
+    uint32_t occupancy(uint32_t i) const {  // 3/4 and 1/2 of the largest
+        return std::max(1u, i == 0 ? max_per_sm * 3 / 4 : max_per_sm / 2);
+    }
+    // Result of a full wave of the current candidate.
+    void report(double ns_per_path) {
+        if (ns_per_path < best_ns) {
+            best_ns   = ns_per_path;
+            best_wave = wave_paths;
+            best_sm   = per_sm;
+        }
+        if (stage == 0 && ++candidate < Sizes) {
+            wave_paths = Wave_sizes[candidate];
+            return;
+        }
+        if (stage == 0) {
+            stage = 1;
+            candidate = 0;
+        } else {
+            ++candidate;
+        }
+        wave_paths = best_wave;
+        if (candidate < 2 && occupancy(candidate) < max_per_sm) {
+            per_sm = occupancy(candidate);
+        } else {
+            stage  = 2;
+            per_sm = best_sm;
+        }
+    }
+};
+
 constexpr uint32_t Counter_stride = 8;
 constexpr uint32_t Counter_words  = Counter_stride * Max_bounce_slots + 4;
 constexpr uint32_t Overflow_slot  = Counter_stride * Max_bounce_slots;
@@ -1220,7 +1277,17 @@ __device__ __forceinline__ V3 mixture_sample_at(float4 const* __restrict__ row, 
     lobe.mu     = v3(l.x, l.y, l.z);
     lobe.kappa  = l.w;
     lobe.weight = 1.f;
-    return guide::mixture_sample(&lobe, 0.f, u1, u2);
+    return guide::vmf_sample(lobe, u1, u2);
+}
+
+// Russian roulette's continuation probability (russian_roulette, integrator_helper.hpp:42-52):
+// the throughput's largest component.  The reference does not clamp it to 1 -- a throughput
+// above 1 then scales the path down, a bias it never meets with its BSDF sampling alone
+// (f cos / pdf stays below 1), and plain MIS here mirrors it.  Guided paths, whose throughput
+// f cos / (mixed pdf) can exceed 1, use the clamped, unbiased probability.
+__device__ __forceinline__ float continuation_probability(Wave const& wave, V3 T) {
+    float const q = shading::max_component(T);
+    return wave.guiding ? fminf(q, 1.f) : q;
 }
 
 // ---- shade: one path vertex ----
@@ -1308,7 +1375,7 @@ __global__ void __launch_bounds__(Shade_block)
             if (depth >= wave.max_bounces) {
                 done = true;
             } else if (depth >= wave.min_bounces) {
-                float const q = shading::max_component(T);
+                float const q = continuation_probability(wave, T);
                 if (rng.uniform() > q) {
                     done = true;
                 } else {
@@ -1394,7 +1461,7 @@ __global__ void __launch_bounds__(Shade_block)
                 } else if (depth >= wave.max_bounces) {
                     done = true;
                 } else if (depth >= wave.min_bounces) {
-                    float const q = shading::max_component(T);
+                    float const q = continuation_probability(wave, T);
                     if (rng.uniform() > q) {
                         done = true;
                     } else {
@@ -1460,21 +1527,20 @@ __global__ void __launch_bounds__(Shade_block)
                 }
 
                 // Continuation direction: the BSDF sample (pathtracer_mis.cpp:153-201), or with
-                // probability gf the guide's (no reflection below the surface).
+                // probability gf the guide's.  A guide direction gets the BSDF value and pdf the
+                // BSDF sampler would give it -- below the geometric surface too, where the
+                // Substitute BSDF (its cosines clamped to a small positive minimum) is not zero;
+                // dropping those directions would bias the one-sample MIS estimate low.
                 shading::Sampled smp;
                 if (guided && rng.uniform() < gf) {
                     float const g0 = rng.uniform();
                     float const g1 = rng.uniform();
                     float const g2 = rng.uniform();
-                    smp.wi       = mixture_sample_at(mix, g0, g1, g2);
-                    smp.specular = false;
-                    if (shading::dot(smp.wi, geo_n) > 0.f) {
-                        shading::Bxdf const f = shading::substitute_evaluate(mat, s.e_table, ctx, smp.wi);
-                        smp.reflection        = f.reflection;
-                        smp.pdf               = f.pdf;
-                    } else {
-                        smp.pdf = 0.f;
-                    }
+                    smp.wi                = mixture_sample_at(mix, g0, g1, g2);
+                    smp.specular          = false;
+                    shading::Bxdf const f = shading::substitute_evaluate(mat, s.e_table, ctx, smp.wi);
+                    smp.reflection        = f.reflection;
+                    smp.pdf               = f.pdf;
                 } else {
                     float const xl = rng.uniform();
                     float const x0 = rng.uniform();
@@ -1765,6 +1831,9 @@ struct Renderer::Device {
     guide::Network     net;
     bool               net_ready     = false;
     uint32_t           guide_grid    = 1;      // k_guide blocks (persistent)
+    Tuner              tuner;
+    uint32_t           sms           = 1;
+    cudaEvent_t        wave_ev[2]    = {nullptr, nullptr};
     // event pairs around the guide's inference and training launches of one render call
     std::vector<cudaEvent_t> guide_events;
     uint32_t           guide_paths   = 0;  // paths the guide buffers hold
@@ -1797,10 +1866,39 @@ struct Renderer::Device {
 
 namespace {
 
+// The renderer's device buffers come from the device's default stream-ordered memory pool,
+// set to keep the memory it gets back (release threshold: unlimited): an engine created after
+// another was released, or a wave larger than the last, reuses that memory instead of having
+// the driver map (and, on release, unmap) gigabytes anew -- which took up to half a second per
+// frame.  Allocation and release are ordered on the legacy default stream and completed before
+// they return, so the buffers behave as cudaMalloc'd ones for every stream.
+cudaError_t pool_malloc(void** p, size_t bytes) {
+    static bool const keep = [] {
+        int           dev  = 0;
+        cudaMemPool_t pool = nullptr;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t threshold = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+        }
+        return true;
+    }();
+    (void)keep;
+    cudaError_t const e = cudaMallocAsync(p, bytes, 0);
+    return e == cudaSuccess ? cudaStreamSynchronize(0) : e;
+}
+
+template <typename T>
+cudaError_t dev_malloc(T** p, size_t bytes) {
+    return pool_malloc(reinterpret_cast<void**>(p), bytes);
+}
+
+// Returns a buffer to the pool once the device is idle (no kernel may still use it).
 template <typename T>
 void free_ptr(T*& p) {
     if (p) {
-        cudaFree(p);
+        cudaDeviceSynchronize();
+        cudaFreeAsync(p, 0);
+        cudaStreamSynchronize(0);
         p = nullptr;
     }
 }
@@ -1808,7 +1906,7 @@ void free_ptr(T*& p) {
 template <typename T>
 cudaError_t upload(T*& dst, void const* src, size_t bytes) {
     free_ptr(dst);
-    cudaError_t e = cudaMalloc(&dst, std::max<size_t>(bytes, 16));
+    cudaError_t e = dev_malloc(&dst, std::max<size_t>(bytes, 16));
     if (e != cudaSuccess) {
         return e;
     }
@@ -1893,6 +1991,10 @@ Renderer::Renderer() : d_(new Device) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<false>, Trace_block, 0);
     d_->trace_grid = std::max(1, per_sm) * std::max(1, sms);
+    d_->sms        = uint32_t(std::max(1, sms));
+    d_->tuner.reset(uint32_t(std::max(1, per_sm)));
+    cudaEventCreate(&d_->wave_ev[0]);
+    cudaEventCreate(&d_->wave_ev[1]);
 }
 
 Renderer::~Renderer() {
@@ -1960,6 +2062,8 @@ Renderer::~Renderer() {
     for (cudaEvent_t e : d_->guide_events) {
         cudaEventDestroy(e);
     }
+    cudaEventDestroy(d_->wave_ev[0]);
+    cudaEventDestroy(d_->wave_ev[1]);
     delete d_;
 }
 
@@ -1985,6 +2089,7 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     }
     // Triangles of medium boundaries get their own class so shadow rays can pass them.
     std::vector<uint32_t> tri_class(nt, Class_surface);
+    d_->tuner.reset(d_->tuner.max_per_sm);  // a new scene is tuned anew
     d_->has_media = false;
     for (uint32_t t = 0; t < nt; ++t) {
         if (scene.materials[scene.tri_material[t]].type == shading::Type_volume) {
@@ -2154,9 +2259,9 @@ int32_t Renderer::set_camera(Camera_desc const& camera) {
         free_ptr(d_->film);
         free_ptr(d_->comp);
         free_ptr(d_->out);
-        SPB_RCUDA(cudaMalloc(&d_->film, pixels * sizeof(float4)));
-        SPB_RCUDA(cudaMalloc(&d_->comp, pixels * sizeof(float4)));
-        SPB_RCUDA(cudaMalloc(&d_->out, pixels * sizeof(float4)));
+        SPB_RCUDA(dev_malloc(&d_->film, pixels * sizeof(float4)));
+        SPB_RCUDA(dev_malloc(&d_->comp, pixels * sizeof(float4)));
+        SPB_RCUDA(dev_malloc(&d_->out, pixels * sizeof(float4)));
         d_->film_pixels = pixels;
     }
     camera_ready_ = true;
@@ -2207,31 +2312,31 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     free_ptr(d_->shadow_queue);
     free_ptr(d_->transmit_queue);
     size_t const n = paths;
-    SPB_RCUDA(cudaMalloc(&p.ray_o, n * sizeof(float4)));
-    SPB_RCUDA(cudaMalloc(&p.ray_d, n * sizeof(float4)));
-    SPB_RCUDA(cudaMalloc(&p.hit_id, n * sizeof(uint32_t)));
-    SPB_RCUDA(cudaMalloc(&p.hit_t, n * sizeof(float)));
-    SPB_RCUDA(cudaMalloc(&p.hit_uv, n * sizeof(float2)));
-    SPB_RCUDA(cudaMalloc(&p.T, n * sizeof(float4)));
-    SPB_RCUDA(cudaMalloc(&p.L, n * sizeof(float4)));
-    SPB_RCUDA(cudaMalloc(&p.puv, n * sizeof(float2)));
-    SPB_RCUDA(cudaMalloc(&p.rng, n * sizeof(uint4)));
-    SPB_RCUDA(cudaMalloc(&p.info, n * sizeof(uint32_t)));
-    SPB_RCUDA(cudaMalloc(&p.sh_o, n * sizeof(float4)));
-    SPB_RCUDA(cudaMalloc(&p.sh_d, n * sizeof(float4)));
-    SPB_RCUDA(cudaMalloc(&p.sh_L, n * sizeof(float4)));
-    SPB_RCUDA(cudaMalloc(&p.prev_n, n * sizeof(float4)));
-    SPB_RCUDA(cudaMalloc(&p.sh2_o, n * sizeof(float4)));
-    SPB_RCUDA(cudaMalloc(&p.sh2_d, n * sizeof(float4)));
-    SPB_RCUDA(cudaMalloc(&p.sh2_L, n * sizeof(float4)));
-    SPB_RCUDA(cudaMalloc(&p.L2, n * sizeof(float4)));
-    SPB_RCUDA(cudaMalloc(&d_->queue[0], n * sizeof(uint32_t)));
-    SPB_RCUDA(cudaMalloc(&d_->queue[1], n * sizeof(uint32_t)));
+    SPB_RCUDA(dev_malloc(&p.ray_o, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.ray_d, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.hit_id, n * sizeof(uint32_t)));
+    SPB_RCUDA(dev_malloc(&p.hit_t, n * sizeof(float)));
+    SPB_RCUDA(dev_malloc(&p.hit_uv, n * sizeof(float2)));
+    SPB_RCUDA(dev_malloc(&p.T, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.L, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.puv, n * sizeof(float2)));
+    SPB_RCUDA(dev_malloc(&p.rng, n * sizeof(uint4)));
+    SPB_RCUDA(dev_malloc(&p.info, n * sizeof(uint32_t)));
+    SPB_RCUDA(dev_malloc(&p.sh_o, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.sh_d, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.sh_L, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.prev_n, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.sh2_o, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.sh2_d, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.sh2_L, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.L2, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&d_->queue[0], n * sizeof(uint32_t)));
+    SPB_RCUDA(dev_malloc(&d_->queue[1], n * sizeof(uint32_t)));
     // up to two shadow rays per path vertex (split light selection)
-    SPB_RCUDA(cudaMalloc(&d_->shadow_queue, 2 * n * sizeof(uint32_t)));
-    SPB_RCUDA(cudaMalloc(&d_->transmit_queue, 2 * n * sizeof(uint32_t)));
+    SPB_RCUDA(dev_malloc(&d_->shadow_queue, 2 * n * sizeof(uint32_t)));
+    SPB_RCUDA(dev_malloc(&d_->transmit_queue, 2 * n * sizeof(uint32_t)));
     if (!d_->counters) {
-        SPB_RCUDA(cudaMalloc(&d_->counters, Counter_words * sizeof(uint32_t)));
+        SPB_RCUDA(dev_malloc(&d_->counters, Counter_words * sizeof(uint32_t)));
     }
     d_->capacity = paths;
     return SPB_OK;
@@ -2250,11 +2355,11 @@ int32_t Renderer::ensure_guide(uint32_t paths) {
         free_ptr(p.open_record);
         size_t const n = d_->capacity;
         size_t const tiled_entries = (n + guide::Tile - 1) / guide::Tile * guide::Tile;
-        SPB_RCUDA(cudaMalloc(&p.guide_in, tiled_entries * guide::Inputs * sizeof(__nv_bfloat16)));
-        SPB_RCUDA(cudaMalloc(&p.guide_out, n * Mixture_floats * sizeof(float)));
-        SPB_RCUDA(cudaMalloc(&p.guide_ok, n));
-        SPB_RCUDA(cudaMalloc(&p.rec, n * rd * Record_float4 * sizeof(float4)));
-        SPB_RCUDA(cudaMalloc(&p.open_record, n * sizeof(uint32_t)));
+        SPB_RCUDA(dev_malloc(&p.guide_in, tiled_entries * guide::Inputs * sizeof(__nv_bfloat16)));
+        SPB_RCUDA(dev_malloc(&p.guide_out, n * Mixture_floats * sizeof(float)));
+        SPB_RCUDA(dev_malloc(&p.guide_ok, n));
+        SPB_RCUDA(dev_malloc(&p.rec, n * rd * Record_float4 * sizeof(float4)));
+        SPB_RCUDA(dev_malloc(&p.open_record, n * sizeof(uint32_t)));
         d_->guide_paths   = uint32_t(n);
         d_->guide_records = rd;
     }
@@ -2265,10 +2370,10 @@ int32_t Renderer::ensure_guide(uint32_t paths) {
         free_ptr(d_->train_w);
         free_ptr(d_->train_parts);
         size_t const rows = (size_t(batch) + guide::Tile - 1) / guide::Tile * guide::Tile;
-        SPB_RCUDA(cudaMalloc(&d_->train_in, rows * guide::Inputs * sizeof(__nv_bfloat16)));
-        SPB_RCUDA(cudaMalloc(&d_->train_dir, size_t(batch) * 3 * sizeof(float)));
-        SPB_RCUDA(cudaMalloc(&d_->train_w, size_t(batch) * sizeof(float)));
-        SPB_RCUDA(cudaMalloc(&d_->train_parts, (rows + 255) / 256 * sizeof(float)));
+        SPB_RCUDA(dev_malloc(&d_->train_in, rows * guide::Inputs * sizeof(__nv_bfloat16)));
+        SPB_RCUDA(dev_malloc(&d_->train_dir, size_t(batch) * 3 * sizeof(float)));
+        SPB_RCUDA(dev_malloc(&d_->train_w, size_t(batch) * sizeof(float)));
+        SPB_RCUDA(dev_malloc(&d_->train_parts, (rows + 255) / 256 * sizeof(float)));
         d_->train_capacity = batch;
     }
     if (!d_->net_ready) {
@@ -2330,15 +2435,21 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     }
     // camera samples per sample slot: the image and its filter border
     uint32_t const pixels = (camera_.width + 2 * Film_border) * (camera_.height + 2 * Film_border);
-    // k samples per pixel per wave, up to about 4M paths per wave.
-    uint32_t const per_wave = std::max(1u, std::min(num_samples, (1u << 22) / std::max(1u, pixels)));
+    // Wave size: k samples per pixel per wave, k = paths per wave / pixels (at least 1), the
+    // paths per wave from the settings or the autotuner; buffers hold the largest candidate.
+    bool const     tuning     = settings_.wave_paths == 0 || settings_.trace_blocks_per_sm == 0;
+    uint32_t const max_paths  = settings_.wave_paths ? settings_.wave_paths : Tuner::Max_wave_paths;
+    auto const     wave_spp   = [&](uint32_t paths_per_wave) {
+        return std::max(1u, std::min(num_samples, paths_per_wave / std::max(1u, pixels)));
+    };
+    uint32_t const max_wave = wave_spp(max_paths);
     // while the guide trains, passes of guide_pass_spp with training steps in between
-    uint32_t const train_wave = std::max(1u, std::min(per_wave, settings_.guide_pass_spp));
-    if (int32_t const st = ensure_buffers(per_wave * pixels)) {
+    uint32_t const train_wave = std::max(1u, std::min(max_wave, settings_.guide_pass_spp));
+    if (int32_t const st = ensure_buffers(max_wave * pixels)) {
         return st;
     }
     if (settings_.guiding) {
-        if (int32_t const st = ensure_guide(per_wave * pixels)) {
+        if (int32_t const st = ensure_guide(max_wave * pixels)) {
             return st;
         }
     }
@@ -2401,8 +2512,22 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     for (uint32_t done = 0; done < num_samples;) {
         bool const training = settings_.guiding &&
                               (settings_.guide_train_spp == 0 || first_sample + done < settings_.guide_train_spp);
-        uint32_t const k     = std::min(training ? train_wave : per_wave, num_samples - done);
-        uint32_t const paths = k * pixels;
+        // this wave's configuration: tuned, the tuner's current candidate, or the settings
+        Tuner const&   tn          = d_->tuner;
+        bool const     probe       = tuning && !training && !tn.done();
+        uint32_t const wave_paths  = settings_.wave_paths ? settings_.wave_paths
+                                                          : (tn.done() ? tn.best_wave : tn.wave_paths);
+        uint32_t const blocks_sm   = settings_.trace_blocks_per_sm
+                                         ? std::min(settings_.trace_blocks_per_sm, tn.max_per_sm)
+                                         : (tn.done() ? tn.best_sm : (training ? tn.max_per_sm : tn.per_sm));
+        uint32_t const trace_grid  = blocks_sm * d_->sms;
+        uint32_t const full_k      = training ? train_wave : wave_spp(wave_paths);
+        uint32_t const k           = std::min(full_k, num_samples - done);
+        bool const     measured    = probe && k == full_k;  // a full wave of the candidate
+        uint32_t const paths       = k * pixels;
+        if (measured) {
+            SPB_RCUDA(cudaEventRecord(d_->wave_ev[0], st));
+        }
         Wave           wave{first_sample + done, k, settings_.seed, settings_.min_bounces,
                   settings_.max_bounces};
         wave.guiding        = settings_.guiding ? 1u : 0u;
@@ -2428,7 +2553,7 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             uint32_t* const q_in  = d_->queue[b & 1];
             uint32_t* const q_out = d_->queue[(b + 1) & 1];
             uint32_t* const c = ctr + Counter_stride * b;
-            k_trace<false><<<d_->trace_grid, Trace_block, 0, st>>>(sg, d_->paths, q_in, c, c + 2,
+            k_trace<false><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, q_in, c, c + 2,
                                                                    ctr + Overflow_slot);
             // (without media a vertex's depth is the iteration; with media it can be less)
             if (settings_.guiding && (d_->has_media || b < settings_.guide_depth)) {
@@ -2442,13 +2567,13 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             k_shade<<<(paths + Shade_block - 1) / Shade_block, Shade_block, 0, st>>>(
                 sg, wave, d_->paths, q_in, c, q_out, c + Counter_stride, d_->shadow_queue, c + 1);
             if (d_->has_media) {
-                k_trace<true, true><<<d_->trace_grid, Trace_block, 0, st>>>(
+                k_trace<true, true><<<trace_grid, Trace_block, 0, st>>>(
                     sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot,
                     d_->transmit_queue, c + 4);
                 k_transmit<<<(2 * paths + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
                     sg, d_->paths, d_->transmit_queue, c + 4, ctr + Overflow_slot);
             } else {
-                k_trace<true><<<d_->trace_grid, Trace_block, 0, st>>>(
+                k_trace<true><<<trace_grid, Trace_block, 0, st>>>(
                     sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot);
             }
         }
@@ -2464,9 +2589,17 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         k_gather<<<(camera_.width * camera_.height + 255) / 256, 256, 0, st>>>(
             d_->paths, camera_.width, camera_.height, k, d_->film, d_->comp);
         SPB_RCUDA(cudaGetLastError());
+        if (measured) {
+            SPB_RCUDA(cudaEventRecord(d_->wave_ev[1], st));
+        }
         SPB_RCUDA(cudaMemcpyAsync(host_ctr.data(), ctr, Counter_words * sizeof(uint32_t),
                                   cudaMemcpyDeviceToHost, st));
         SPB_RCUDA(cudaStreamSynchronize(st));
+        if (measured) {
+            float wave_ms = 0.f;
+            SPB_RCUDA(cudaEventElapsedTime(&wave_ms, d_->wave_ev[0], d_->wave_ev[1]));
+            d_->tuner.report(double(wave_ms) * 1e6 / double(paths));
+        }
         for (uint32_t b = 0; b < iterations; ++b) {
             stats_.extension_rays += host_ctr[Counter_stride * b];
             stats_.shadow_rays += host_ctr[Counter_stride * b + 1];
@@ -2481,6 +2614,8 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             return SPB_ERROR_CUDA;
         }
         stats_.paths += paths;
+        stats_.wave_paths          = std::max(stats_.wave_paths, paths);
+        stats_.trace_blocks_per_sm = blocks_sm;
         done += k;
     }
     SPB_RCUDA(cudaEventRecord(d_->ev1, st));

@@ -67,6 +67,9 @@ struct Settings {
     uint32_t guide_pass_spp  = 2;   // samples per pixel between training steps
     uint32_t guide_train_spp = 32;  // samples per pixel after which training stops (0: never)
     uint32_t guide_depth     = 255;  // vertices of depth below this are guided
+    // Paths per wave and traversal blocks per SM; 0: chosen by the online autotuner.
+    uint32_t wave_paths          = 0;
+    uint32_t trace_blocks_per_sm = 0;
 };
 
 struct Stats {
@@ -79,6 +82,8 @@ struct Stats {
     double   guide_inference_seconds = 0.0;  // device time of encoding + inference
     uint64_t guide_training_samples  = 0;    // Adam steps x batch
     double   guide_training_seconds  = 0.0;  // device time of training
+    uint32_t wave_paths              = 0;    // largest wave of the call (paths)
+    uint32_t trace_blocks_per_sm     = 0;    // traversal blocks per SM of its last wave
 };
 
 class Renderer {

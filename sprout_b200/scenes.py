@@ -541,7 +541,7 @@ def _box_mesh(lo, hi):
 
 def doorway(su, width: int = 1280, height: int = 720, spp: int = 64, seed: int = 3, spheres: int = 96,
             boxes: int = 160, sphere_subdivisions: int = 4, max_bounces: int = 8, min_bounces: int = 4,
-            environment: float = 5.0, guiding=None, render_seed: int = 0):
+            environment: float = 5.0, guiding=None, render_seed: int = 0, integrator=None):
     """A 6 x 6 x 3 m room (x, z in [-3, 3], y in [0, 3]) whose only opening is a 1 x 2 m doorway
     in the wall z = 3, outside a uniform environment of radiance `environment` (an
     Infinite_sphere light).  Inside: `spheres` icospheres (20 * 4^subdivisions triangles each:
@@ -551,7 +551,8 @@ def doorway(su, width: int = 1280, height: int = 720, spp: int = 64, seed: int =
     in the room's far corner looks towards the doorway with a 60 degree field of view.
     guiding: None for plain MIS, else True or a dict of guide settings (this renderer's
     "guiding" integrator key; the reference ignores it).  render_seed: the sample streams' seed
-    (this renderer's "seed" integrator key), for independent renders."""
+    (this renderer's "seed" integrator key), for independent renders.  integrator: further
+    PTMIS keys (e.g. this renderer's fixed launch shapes "wave_paths", "trace_blocks_per_sm")."""
     rng = np.random.default_rng(seed)
     eye = np.array([-2.4, 1.5, -2.7])
     cam = su.su_create_camera_perspective(width, height, math.radians(60.0))
@@ -561,6 +562,7 @@ def doorway(su, width: int = 1280, height: int = 720, spp: int = 64, seed: int =
         ptmis["guiding"] = guiding
     if render_seed:
         ptmis["seed"] = render_seed
+    ptmis.update(integrator or {})
 
     def clear(c, r):
         """Keeps objects off the camera and out of the doorway."""

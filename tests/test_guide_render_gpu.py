@@ -41,13 +41,19 @@ def test_guided_error_below_plain_at_equal_samples(reference):
     assert e_guided < 0.7 * e_plain, (e_guided, e_plain)
 
 
-def test_guided_converges_to_plain(reference):
-    guided, _, _ = doorway_frame(W, H, 2048, True, seed=7)
-    m_ref, m_img = reference.mean(axis=(0, 1)), guided.mean(axis=(0, 1))
-    assert np.all(np.abs(m_img - m_ref) <= 0.005 * m_ref), (m_img, m_ref)
-    bi, br = block_means(guided, 16), block_means(reference, 16)
+def test_guided_converges_to_plain():
+    """Guided and plain MIS estimate the same image: at 96x54, 32,768 guided spp against 131,072
+    plain spp, the image means agree within 0.3 % and 16x16-block means within 1.2 %
+    (independent plain renders at these counts agree within 0.5 %; a guided estimator that
+    lost the throughput above 1 to Russian roulette was 1.5 % dark in dim blocks)."""
+    w, h = 96, 54
+    plain, _, _ = doorway_frame(w, h, 131072, None, seed=1000)
+    guided, _, _ = doorway_frame(w, h, 32768, True, seed=7)
+    m_ref, m_img = plain.mean(axis=(0, 1)), guided.mean(axis=(0, 1))
+    assert np.all(np.abs(m_img - m_ref) <= 0.003 * m_ref), (m_img, m_ref)
+    bi, br = block_means(guided, 16), block_means(plain, 16)
     worst = np.max(np.abs(bi - br) / (np.abs(br) + 0.01))
-    assert worst < 0.03, f"worst 16x16 block deviation {worst:.4f}"
+    assert worst < 0.012, f"worst 16x16 block deviation {worst:.4f}"
 
 
 def test_guided_matches_reference_image():
