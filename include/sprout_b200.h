@@ -172,7 +172,8 @@ SPB_API int32_t spb_intersect_host_static(spb_tree* tree, float const* rays, uin
  * of that inference (input encoding included), and the training samples (Adam steps x batch)
  * and the device time of training (batch gathering, gradients, Adam).  Launch shapes: the
  * largest wave (paths) and the traversal blocks per SM of the last wave, as the autotuner (or
- * the integrator's "wave_paths" / "trace_blocks_per_sm" keys) set them.  No counterpart in the
+ * the integrator's "wave_paths" / "trace_blocks_per_sm" keys) set them, and the waves replayed
+ * from captured CUDA graphs (the "cuda_graphs" key turns them off).  No counterpart in the
  * reference (it logs wall-clock phases only, rendering_driver.cpp:99-136).
  * SPB_ERROR_ARGUMENT if there is no engine.
  */
@@ -188,6 +189,7 @@ typedef struct spb_render_stats {
     double   guide_training_seconds;
     uint32_t wave_paths;
     uint32_t trace_blocks_per_sm;
+    uint32_t graph_waves;
 } spb_render_stats;
 SPB_API int32_t spb_render_last_stats(spb_render_stats* out);
 

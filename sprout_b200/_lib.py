@@ -50,6 +50,7 @@ class RenderStats(ctypes.Structure):
         ("guide_training_seconds", ctypes.c_double),
         ("wave_paths", c_u32),
         ("trace_blocks_per_sm", c_u32),
+        ("graph_waves", c_u32),
     ]
 
 

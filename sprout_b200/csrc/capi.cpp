@@ -603,6 +603,8 @@ SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
             s.wave_paths          = uint32_t(spb::json::number_or(pt->find("wave_paths"), 0.0));
             s.trace_blocks_per_sm = uint32_t(spb::json::number_or(pt->find("trace_blocks_per_sm"), 0.0));
             s.wave_paths          = s.wave_paths ? std::clamp(s.wave_paths, 1u << 16, 1u << 24) : 0u;
+            // "cuda_graphs": false launches every wave's kernels one by one
+            s.cuda_graphs = spb::json::bool_or(pt->find("cuda_graphs"), true);
             // "guiding": true, or an object of the Settings guide fields (this renderer's
             // extension; the reference ignores the key)
             if (spb::json::Value const* g = pt->find("guiding")) {
@@ -1123,6 +1125,7 @@ SPB_API int32_t spb_render_last_stats(spb_render_stats* out) {
     out->guide_training_seconds  = st.guide_training_seconds;
     out->wave_paths              = st.wave_paths;
     out->trace_blocks_per_sm     = st.trace_blocks_per_sm;
+    out->graph_waves             = st.graph_waves;
     return SPB_OK;
 }
 

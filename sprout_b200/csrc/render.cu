@@ -116,6 +116,7 @@ struct Tuner {
 };
 
 constexpr uint32_t Counter_stride = 8;
+constexpr uint32_t Graph_max_paths = 1u << 21;  // largest wave replayed from a CUDA graph
 constexpr uint32_t Counter_words  = Counter_stride * Max_bounce_slots + 4;
 constexpr uint32_t Overflow_slot  = Counter_stride * Max_bounce_slots;
 
@@ -217,6 +218,14 @@ struct Wave {
     float4   bounds_inv;      // 1 / its extent
 };
 
+// A wave's launch parameters, which the kernels read from device memory: the host writes them
+// (pinned) and copies them before each wave, so that one captured CUDA graph replays every wave
+// of the same shape.
+struct Launch {
+    Cam  cam;
+    Wave wave;
+};
+
 // ---- PCG32 (O'Neill 2014), seeded as rnd::Generator::start (base/random/generator.inl) ----
 __device__ __forceinline__ uint32_t pcg_next(uint64_t& state, uint64_t inc) {
     uint64_t const old = state;
@@ -303,9 +312,11 @@ __device__ __forceinline__ uint32_t append(uint32_t* counter, bool want) {
 constexpr int Film_border = 1;
 
 // ---- generate: camera rays (Perspective::generate_ray, camera_perspective.cpp:47-80) ----
-__global__ void k_generate(Cam cam, Wave wave, Paths p, uint32_t* queue, uint32_t* counters,
+__global__ void k_generate(Launch const* __restrict__ launch, Paths p, uint32_t* queue, uint32_t* counters,
                            uint32_t num_paths) {
-    uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
+    Cam const      cam  = launch->cam;
+    Wave const     wave = launch->wave;
+    uint32_t const i    = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         counters[0] = num_paths;
     }
@@ -1053,8 +1064,9 @@ __device__ __forceinline__ V3 box_coordinates(Wave const& wave, V3 pos) {
 // One queue entry per thread: its inputs as row q % 128 of tile q / 128 (entries past the
 // queue's end, up to the tile boundary, get zeros).
 __global__ void __launch_bounds__(256)
-    k_guide_encode(Scene_gpu s, Wave wave, Paths p, uint32_t const* __restrict__ queue,
+    k_guide_encode(Scene_gpu s, Launch const* __restrict__ launch, Paths p, uint32_t const* __restrict__ queue,
                    uint32_t const* __restrict__ count) {
+    Wave const&    wave = launch->wave;
     uint32_t const q   = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t const num = *count;
     if (q >= (num + guide::Tile - 1) / guide::Tile * guide::Tile) {
@@ -1292,9 +1304,10 @@ __device__ __forceinline__ float continuation_probability(Wave const& wave, V3 T
 
 // ---- shade: one path vertex ----
 __global__ void __launch_bounds__(Shade_block)
-    k_shade(Scene_gpu s, Wave wave, Paths p, uint32_t const* __restrict__ q_in,
+    k_shade(Scene_gpu s, Launch const* __restrict__ launch, Paths p, uint32_t const* __restrict__ q_in,
             uint32_t const* __restrict__ count_in, uint32_t* q_out, uint32_t* count_out,
             uint32_t* sq, uint32_t* count_shadow) {
+    Wave const&    wave = launch->wave;
     uint32_t const i   = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t const num = *count_in;
 
@@ -1735,8 +1748,9 @@ __global__ void k_gather(Paths p, uint32_t w, uint32_t h, uint32_t samples, floa
 // kernel reads them (BF16 tiles of 128 rows); each block adds its weights in a fixed order into
 // parts[block] (the loss is normalised by their total).
 __global__ void __launch_bounds__(256)
-    k_train_gather(Paths p, Wave wave, uint32_t records, uint32_t batch, uint32_t pass, __nv_bfloat16* in,
-                   float* dir, float* weight, float* parts) {
+    k_train_gather(Paths p, Launch const* __restrict__ launch, uint32_t records, uint32_t batch, uint32_t pass,
+                   __nv_bfloat16* in, float* dir, float* weight, float* parts) {
+    Wave const&      wave = launch->wave;
     __shared__ float part[256];
     uint32_t const   i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t const   rows = (batch + guide::Tile - 1) / guide::Tile * guide::Tile;
@@ -1833,6 +1847,14 @@ struct Renderer::Device {
     uint32_t           guide_grid    = 1;      // k_guide blocks (persistent)
     Tuner              tuner;
     uint32_t           sms           = 1;
+    // per-wave launch block (pinned host copy, device copy) and the captured wave graphs
+    Launch*            launch_host   = nullptr;
+    Launch*            launch_dev    = nullptr;
+    struct Wave_graph {
+        uint32_t        k, trace_grid, iterations, events;
+        cudaGraphExec_t exec;  // nullptr: seen once, not captured yet
+    };
+    std::vector<Wave_graph> graphs;
     cudaEvent_t        wave_ev[2]    = {nullptr, nullptr};
     // event pairs around the guide's inference and training launches of one render call
     std::vector<cudaEvent_t> guide_events;
@@ -2064,6 +2086,15 @@ Renderer::~Renderer() {
     }
     cudaEventDestroy(d_->wave_ev[0]);
     cudaEventDestroy(d_->wave_ev[1]);
+    for (auto const& g : d_->graphs) {
+        if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+        }
+    }
+    free_ptr(d_->launch_dev);
+    if (d_->launch_host) {
+        cudaFreeHost(d_->launch_host);
+    }
     delete d_;
 }
 
@@ -2081,6 +2112,7 @@ int32_t Renderer::fail_cuda(char const* what, int code) {
     } while (0)
 
 int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
+    clear_graphs();
     uint32_t const nv = uint32_t(scene.positions.size() / 3);
     uint32_t const nt = uint32_t(scene.indices.size() / 3);
     if (nt == 0) {
@@ -2249,6 +2281,7 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
 }
 
 int32_t Renderer::set_camera(Camera_desc const& camera) {
+    clear_graphs();
     if (camera.width == 0 || camera.height == 0 || !(camera.fov > 0.f)) {
         error_ = "camera needs a resolution and a field of view";
         return SPB_ERROR_ARGUMENT;
@@ -2282,6 +2315,7 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     if (paths <= d_->capacity) {
         return SPB_OK;
     }
+    clear_graphs();
     Paths& p = d_->paths;
     free_ptr(p.ray_o);
     free_ptr(p.ray_d);
@@ -2348,6 +2382,7 @@ int32_t Renderer::ensure_guide(uint32_t paths) {
     Paths&         p  = d_->paths;
     uint32_t const rd = settings_.record_depth;
     if (d_->guide_paths < paths || d_->guide_records != rd) {
+        clear_graphs();
         free_ptr(p.guide_in);
         free_ptr(p.guide_out);
         free_ptr(p.guide_ok);
@@ -2377,6 +2412,7 @@ int32_t Renderer::ensure_guide(uint32_t paths) {
         d_->train_capacity = batch;
     }
     if (!d_->net_ready) {
+        clear_graphs();
         SPB_RCUDA(cudaError_t(d_->net.init(settings_.guide_seed)));
         SPB_RCUDA(cudaFuncSetAttribute(k_guide, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(sizeof(Infer_smem))));
@@ -2402,16 +2438,25 @@ int32_t Renderer::ensure_guide(uint32_t paths) {
     return SPB_OK;
 }
 
+// Drops the captured wave graphs (their kernels hold buffer and scene pointers).
+void Renderer::clear_graphs() {
+    for (auto const& g : d_->graphs) {
+        if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+        }
+    }
+    d_->graphs.clear();
+}
+
 // Training after a pass: guide_steps Adam steps, each on a fresh batch of the pass's records.
-int32_t Renderer::train_guide(uint32_t paths, void const* wave_ptr) {
-    Wave const&    wave    = *static_cast<Wave const*>(wave_ptr);
+int32_t Renderer::train_guide(uint32_t paths) {
     cudaStream_t   st      = d_->stream;
     uint32_t const batch   = settings_.guide_batch;
     uint32_t const records = paths * settings_.record_depth;
     // one thread per batch row, the last tile's rows past the batch included
     uint32_t const gather_blocks = ((batch + guide::Tile - 1) / guide::Tile * guide::Tile + 255) / 256;
     for (uint32_t step = 0; step < settings_.guide_steps; ++step) {
-        k_train_gather<<<gather_blocks, 256, 0, st>>>(d_->paths, wave, records, batch, d_->pass++, d_->train_in,
+        k_train_gather<<<gather_blocks, 256, 0, st>>>(d_->paths, d_->launch_dev, records, batch, d_->pass++, d_->train_in,
                                                       d_->train_dir, d_->train_w, d_->train_parts);
         SPB_RCUDA(cudaError_t(d_->net.gradients_tiled(d_->train_in, d_->train_dir, d_->train_w, batch,
                                                       d_->train_parts, gather_blocks, st)));
@@ -2496,11 +2541,8 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     stats_ = Stats();
     std::vector<uint32_t> host_ctr(Counter_words);
     // Device time of the guide's stages: event pairs (inference after each trace, training
-    // after each pass), summed once the call is done.
-    size_t              events_used = 0;
-    std::vector<size_t> train_pairs;
-    std::vector<bool>   guided_bounce(Max_bounce_slots, false);
-    auto const          guide_event = [&](size_t i) {
+    // after each pass), summed after each wave.
+    auto const guide_event = [&](size_t i) {
         while (d_->guide_events.size() <= i) {
             cudaEvent_t e = nullptr;
             cudaEventCreate(&e);
@@ -2508,6 +2550,75 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         }
         return d_->guide_events[i];
     };
+    if (!d_->launch_dev) {
+        SPB_RCUDA(dev_malloc(&d_->launch_dev, sizeof(Launch)));
+        SPB_RCUDA(cudaMallocHost(&d_->launch_host, sizeof(Launch)));
+    }
+    auto const record = [&](cudaEvent_t e, bool capture) {
+        return capture ? cudaEventRecordWithFlags(e, st, cudaEventRecordExternal) : cudaEventRecord(e, st);
+    };
+    bool const guide_at_all = settings_.guiding;
+    auto const guided_at    = [&](uint32_t b) { return guide_at_all && (d_->has_media || b < settings_.guide_depth); };
+
+    // Enqueues one wave's kernels (its launch block already copied to the device): generate,
+    // then per vertex extend / guide / shade / shadow, the guide's training after a training
+    // pass, and the film gather.  With media the bounce loop checks the extension queue on the
+    // host, so such waves are never captured into a graph.
+    auto const enqueue_wave = [&](uint32_t k, uint32_t paths, uint32_t trace_grid, bool training, bool capture,
+                                  uint32_t& iterations, size_t& events) -> int32_t {
+        SPB_RCUDA(cudaMemsetAsync(ctr, 0, Counter_words * sizeof(uint32_t), st));
+        k_generate<<<(paths + 255) / 256, 256, 0, st>>>(d_->launch_dev, d_->paths, d_->queue[0], ctr, paths);
+        iterations = 0;
+        for (uint32_t b = 0; b < max_iterations; ++b) {
+            if (b >= bounce_iterations) {
+                SPB_RCUDA(cudaMemcpyAsync(d_->pinned_count, ctr + Counter_stride * b, sizeof(uint32_t),
+                                          cudaMemcpyDeviceToHost, st));
+                SPB_RCUDA(cudaStreamSynchronize(st));
+                if (*d_->pinned_count == 0) {
+                    break;
+                }
+            }
+            iterations               = b + 1;
+            uint32_t* const q_in  = d_->queue[b & 1];
+            uint32_t* const q_out = d_->queue[(b + 1) & 1];
+            uint32_t* const c     = ctr + Counter_stride * b;
+            k_trace<false><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, q_in, c, c + 2, ctr + Overflow_slot);
+            // (without media a vertex's depth is the iteration; with media it can be less)
+            if (guided_at(b)) {
+                SPB_RCUDA(record(guide_event(events++), capture));
+                k_guide_encode<<<(paths + 255) / 256, 256, 0, st>>>(sg, d_->launch_dev, d_->paths, q_in, c);
+                k_guide<<<d_->guide_grid, guide::Block, sizeof(Infer_smem), st>>>(
+                    d_->paths, c, d_->net.weights(), d_->net.parameters(), ctr + Overflow_slot + 1);
+                SPB_RCUDA(record(guide_event(events++), capture));
+            }
+            k_shade<<<(paths + Shade_block - 1) / Shade_block, Shade_block, 0, st>>>(
+                sg, d_->launch_dev, d_->paths, q_in, c, q_out, c + Counter_stride, d_->shadow_queue, c + 1);
+            if (d_->has_media) {
+                k_trace<true, true><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->shadow_queue, c + 1, c + 3,
+                                                                       ctr + Overflow_slot, d_->transmit_queue, c + 4);
+                k_transmit<<<(2 * paths + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
+                    sg, d_->paths, d_->transmit_queue, c + 4, ctr + Overflow_slot);
+            } else {
+                k_trace<true><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->shadow_queue, c + 1, c + 3,
+                                                                  ctr + Overflow_slot);
+            }
+        }
+        if (training) {
+            SPB_RCUDA(record(guide_event(events++), capture));
+            if (int32_t const e = train_guide(paths)) {
+                return e;
+            }
+            SPB_RCUDA(record(guide_event(events++), capture));
+        }
+        k_gather<<<(camera_.width * camera_.height + 255) / 256, 256, 0, st>>>(d_->paths, camera_.width,
+                                                                              camera_.height, k, d_->film, d_->comp);
+        SPB_RCUDA(cudaGetLastError());
+        return SPB_OK;
+    };
+
+    if (settings_.guiding) {
+        guide_event(2 * Max_bounce_slots + 2);  // every event a wave can use, created before any capture
+    }
     SPB_RCUDA(cudaEventRecord(d_->ev0, st));
     for (uint32_t done = 0; done < num_samples;) {
         bool const training = settings_.guiding &&
@@ -2525,9 +2636,6 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         uint32_t const k           = std::min(full_k, num_samples - done);
         bool const     measured    = probe && k == full_k;  // a full wave of the candidate
         uint32_t const paths       = k * pixels;
-        if (measured) {
-            SPB_RCUDA(cudaEventRecord(d_->wave_ev[0], st));
-        }
         Wave           wave{first_sample + done, k, settings_.seed, settings_.min_bounces,
                   settings_.max_bounces};
         wave.guiding        = settings_.guiding ? 1u : 0u;
@@ -2536,59 +2644,55 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         wave.record_depth   = training ? settings_.record_depth : 0u;
         wave.bounds_lo      = d_->bounds_lo;
         wave.bounds_inv     = d_->bounds_inv;
-        SPB_RCUDA(cudaMemsetAsync(ctr, 0, Counter_words * sizeof(uint32_t), st));
-        k_generate<<<(paths + 255) / 256, 256, 0, st>>>(cam, wave, d_->paths, d_->queue[0], ctr,
-                                                         paths);
+        // The previous wave has completed (synchronized below), so the pinned block is free.
+        d_->launch_host->cam  = cam;
+        d_->launch_host->wave = wave;
+        if (measured) {
+            SPB_RCUDA(cudaEventRecord(d_->wave_ev[0], st));
+        }
+        SPB_RCUDA(cudaMemcpyAsync(d_->launch_dev, d_->launch_host, sizeof(Launch), cudaMemcpyHostToDevice, st));
         uint32_t iterations = 0;
-        for (uint32_t b = 0; b < max_iterations; ++b) {
-            if (b >= bounce_iterations) {
-                SPB_RCUDA(cudaMemcpyAsync(d_->pinned_count, ctr + Counter_stride * b,
-                                          sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-                SPB_RCUDA(cudaStreamSynchronize(st));
-                if (*d_->pinned_count == 0) {
-                    break;
+        size_t   events     = 0;
+        // Graphs pay where launches are a visible share of a wave (at most Graph_max_paths
+        // paths) and for wave shapes that recur: a shape is captured when it comes the second
+        // time, then replayed.
+        Device::Wave_graph* g = nullptr;
+        bool const graphable = settings_.cuda_graphs && !d_->has_media && !training && paths <= Graph_max_paths;
+        if (graphable) {
+            for (auto& e : d_->graphs) {
+                if (e.k == k && e.trace_grid == trace_grid) {
+                    g = &e;
                 }
             }
-            iterations = b + 1;
-            uint32_t* const q_in  = d_->queue[b & 1];
-            uint32_t* const q_out = d_->queue[(b + 1) & 1];
-            uint32_t* const c = ctr + Counter_stride * b;
-            k_trace<false><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, q_in, c, c + 2,
-                                                                   ctr + Overflow_slot);
-            // (without media a vertex's depth is the iteration; with media it can be less)
-            if (settings_.guiding && (d_->has_media || b < settings_.guide_depth)) {
-                SPB_RCUDA(cudaEventRecord(guide_event(events_used++), st));
-                k_guide_encode<<<(paths + 255) / 256, 256, 0, st>>>(sg, wave, d_->paths, q_in, c);
-                k_guide<<<d_->guide_grid, guide::Block, sizeof(Infer_smem), st>>>(
-                    d_->paths, c, d_->net.weights(), d_->net.parameters(), ctr + Overflow_slot + 1);
-                SPB_RCUDA(cudaEventRecord(guide_event(events_used++), st));
-                guided_bounce[b] = true;
-            }
-            k_shade<<<(paths + Shade_block - 1) / Shade_block, Shade_block, 0, st>>>(
-                sg, wave, d_->paths, q_in, c, q_out, c + Counter_stride, d_->shadow_queue, c + 1);
-            if (d_->has_media) {
-                k_trace<true, true><<<trace_grid, Trace_block, 0, st>>>(
-                    sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot,
-                    d_->transmit_queue, c + 4);
-                k_transmit<<<(2 * paths + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
-                    sg, d_->paths, d_->transmit_queue, c + 4, ctr + Overflow_slot);
-            } else {
-                k_trace<true><<<trace_grid, Trace_block, 0, st>>>(
-                    sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot);
+            if (!g) {
+                d_->graphs.push_back({k, trace_grid, 0, 0, nullptr});  // first sighting
             }
         }
-        if (training) {
-            SPB_RCUDA(cudaEventRecord(guide_event(events_used++), st));
-            if (int32_t const e = train_guide(paths, &wave)) {
-                return e;
+        if (g) {
+            if (!g->exec) {
+                SPB_RCUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                int32_t const     e     = enqueue_wave(k, paths, trace_grid, false, true, iterations, events);
+                cudaGraph_t       graph = nullptr;
+                cudaError_t const ce    = cudaStreamEndCapture(st, &graph);
+                if (e != SPB_OK || ce != cudaSuccess) {
+                    if (graph) {
+                        cudaGraphDestroy(graph);
+                    }
+                    return e != SPB_OK ? e : fail_cuda("cudaStreamEndCapture", int(ce));
+                }
+                cudaGraphExec_t   exec = nullptr;
+                cudaError_t const ie   = cudaGraphInstantiate(&exec, graph, 0);
+                cudaGraphDestroy(graph);
+                SPB_RCUDA(ie);
+                *g = Device::Wave_graph{k, trace_grid, iterations, uint32_t(events), exec};
             }
-            SPB_RCUDA(cudaEventRecord(guide_event(events_used++), st));
-            train_pairs.push_back(events_used - 2);
-            stats_.guide_training_samples += uint64_t(settings_.guide_steps) * settings_.guide_batch;
+            SPB_RCUDA(cudaGraphLaunch(g->exec, st));
+            iterations = g->iterations;
+            events     = g->events;
+            ++stats_.graph_waves;
+        } else if (int32_t const e = enqueue_wave(k, paths, trace_grid, training, false, iterations, events)) {
+            return e;
         }
-        k_gather<<<(camera_.width * camera_.height + 255) / 256, 256, 0, st>>>(
-            d_->paths, camera_.width, camera_.height, k, d_->film, d_->comp);
-        SPB_RCUDA(cudaGetLastError());
         if (measured) {
             SPB_RCUDA(cudaEventRecord(d_->wave_ev[1], st));
         }
@@ -2600,12 +2704,21 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             SPB_RCUDA(cudaEventElapsedTime(&wave_ms, d_->wave_ev[0], d_->wave_ev[1]));
             d_->tuner.report(double(wave_ms) * 1e6 / double(paths));
         }
+        // the guide's stages of this wave: inference pairs, then the training pair
+        for (size_t i = 0; i + 1 < events; i += 2) {
+            float pair_ms = 0.f;
+            cudaEventElapsedTime(&pair_ms, d_->guide_events[i], d_->guide_events[i + 1]);
+            bool const train = training && i + 2 == events;
+            (train ? stats_.guide_training_seconds : stats_.guide_inference_seconds) += double(pair_ms) * 1e-3;
+        }
+        if (training) {
+            stats_.guide_training_samples += uint64_t(settings_.guide_steps) * settings_.guide_batch;
+        }
         for (uint32_t b = 0; b < iterations; ++b) {
             stats_.extension_rays += host_ctr[Counter_stride * b];
             stats_.shadow_rays += host_ctr[Counter_stride * b + 1];
-            if (guided_bounce[b]) {
+            if (guided_at(b)) {
                 stats_.guide_vertices += host_ctr[Counter_stride * b];
-                guided_bounce[b] = false;
             }
         }
         stats_.overflow += host_ctr[Overflow_slot];
@@ -2623,13 +2736,6 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, d_->ev0, d_->ev1);
     stats_.seconds = double(ms) * 1e-3;
-    for (size_t i = 0, t = 0; i + 1 < events_used; i += 2) {
-        float pair_ms = 0.f;
-        cudaEventElapsedTime(&pair_ms, d_->guide_events[i], d_->guide_events[i + 1]);
-        bool const train = t < train_pairs.size() && train_pairs[t] == i;
-        (train ? stats_.guide_training_seconds : stats_.guide_inference_seconds) += double(pair_ms) * 1e-3;
-        t += train ? 1 : 0;
-    }
     return SPB_OK;
 }
 

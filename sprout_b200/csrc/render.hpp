@@ -70,6 +70,8 @@ struct Settings {
     // Paths per wave and traversal blocks per SM; 0: chosen by the online autotuner.
     uint32_t wave_paths          = 0;
     uint32_t trace_blocks_per_sm = 0;
+    // Waves without media or training are captured once per shape as a CUDA graph and replayed.
+    bool cuda_graphs = true;
 };
 
 struct Stats {
@@ -84,6 +86,7 @@ struct Stats {
     double   guide_training_seconds  = 0.0;  // device time of training
     uint32_t wave_paths              = 0;    // largest wave of the call (paths)
     uint32_t trace_blocks_per_sm     = 0;    // traversal blocks per SM of its last wave
+    uint32_t graph_waves             = 0;    // waves replayed from a captured CUDA graph
 };
 
 class Renderer {
@@ -123,7 +126,8 @@ class Renderer {
 
     int32_t ensure_buffers(uint32_t paths);
     int32_t ensure_guide(uint32_t paths);
-    int32_t train_guide(uint32_t paths, void const* wave);
+    int32_t train_guide(uint32_t paths);
+    void    clear_graphs();
     void    free_grids();
     int32_t fail_cuda(char const* what, int code);
 };
