@@ -166,6 +166,26 @@ class ClockSampler:
                 "reasons": seen, "samples": len(samples), "source": "NVML in a separate process, 2 ms period"}
 
 
+def rank_rays(rank: int, count: int) -> np.ndarray:
+    """This rank's share of the workload: rays rank*count .. rank*count+count-1 of the seeded
+    stream (every ray's stream depends only on its index, so N ranks together cast the first
+    N*count rays of one sequence -- weak scaling with disjoint ranges)."""
+    import sprout_b200 as sb
+
+    return sb.random_rays(count, seed=SEED, first=rank * count)
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """The slowest rank's time (the job's time); value itself without a process group."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -279,7 +299,7 @@ def main():
         torch.cuda.synchronize()
 
     pos, idx = sb.sphere_mesh(args.mesh_n, 0.1, SEED)
-    rays_host = sb.random_rays(args.rays, seed=SEED, first=rank * args.rays)
+    rays_host = rank_rays(rank, args.rays)
 
     tree = sb.Tree()
     tree.build(pos, idx)
@@ -309,12 +329,8 @@ def main():
         t_end.record(stream)
         barrier()
         clocks.mark_end()
-    elapsed = t_begin.elapsed_time(t_end) / 1e3
+    elapsed = max_over_ranks(t_begin.elapsed_time(t_end) / 1e3, dist, "cuda")
     kernel_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    if dist is not None:
-        tt = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed = float(tt.item())
     assert tree.status() == 0
 
     hit_fraction = float((d_ids != -1).float().mean().item())
@@ -347,11 +363,7 @@ def main():
         t0 = time.perf_counter()
         for _ in range(e_steps):
             tree.intersect(rays_np, out=out)
-        e_el = time.perf_counter() - t0
-        if dist is not None:
-            tt = torch.tensor([e_el], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e_el = float(tt.item())
+        e_el = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
         e2e = {"value": round(world * args.rays * e_steps / e_el / 1e6, 3), "unit": "Mrays/s",
                "h2d_bytes_per_step": 32 * args.rays, "d2h_bytes_per_step": 8 * args.rays,
                "steps": e_steps, "path": "spb_intersect_host (pinned host buffers, 2-stream chunked copies)"}

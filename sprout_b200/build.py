@@ -24,7 +24,7 @@ REFERENCE = pathlib.Path(os.environ.get("SPROUT_REFERENCE", "/root/reference"))
 
 SOURCES = ["common.cpp", "synth.cpp", "bvh8.cpp", "ggx_table.cpp", "light_tree.cpp", "cast.cu", "guide.cu", "render.cu", "capi.cpp"]
 HEADERS = ["common.hpp", "bvh8.hpp", "traverse.cuh", "material.cuh", "render.hpp", "json.hpp", "ggx_table.hpp",
-           "light_tree.hpp", "guide.cuh", "guide_mlp.cuh", "guide.hpp"]
+           "light_tree.hpp", "guide.cuh", "guide_mlp.cuh", "guide.hpp", "tuner.hpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
