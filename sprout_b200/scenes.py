@@ -178,7 +178,7 @@ def translation(x, y, z):
 
 def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounces: int = 8,
             min_bounces: int = 4, fov_degrees: float = 40.0, camera_position=(0.0, 1.0, -3.4),
-            spp: int = 64, tonemap: bool = False, medium=None, density=None, many_lights=False):
+            spp: int = 64, tonemap: bool = False, medium=None, density=None, many_lights=False, guiding=None):
     """Issues the scene's su_* calls on an initialised engine; returns the camera entity.
 
     medium: optional dict of Volumetric material parameters (e.g. color, attenuation_distance,
@@ -187,11 +187,15 @@ def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounc
     cube of grid_box_transformation() filled with this density grid.
     many_lights: the ceiling light is replaced by light_panel(): 66 emitters of different
     radiance, two of them two-sided (a light-tree test).
+    guiding: None for plain MIS, else True or a dict of guide settings (this renderer's
+    "guiding" integrator key).
     """
     cam = su.su_create_camera_perspective(width, height, math.radians(fov_degrees))
     su.set_transformation(cam, translation(*camera_position))
-    su.su_create_integrators(json.dumps({"surface": {"PTMIS": {"min_bounces": min_bounces,
-                                                              "max_bounces": max_bounces}}}).encode())
+    ptmis = {"min_bounces": min_bounces, "max_bounces": max_bounces}
+    if guiding is not None:
+        ptmis["guiding"] = guiding
+    su.su_create_integrators(json.dumps({"surface": {"PTMIS": ptmis}}).encode())
     su.su_create_sampler(spp)
     if tonemap:
         su.su_create_defaults()

@@ -75,6 +75,38 @@ def test_guided_matches_reference_image():
     assert worst < 0.02, f"worst {b}x{b} block deviation {worst:.4f}"
 
 
+@pytest.mark.parametrize("case", ["cornell64_sub3", "cornell64_lights"])
+def test_guided_cornell_matches_reference_image(case):
+    """Guiding on the Cornell box (a GGX conductor sphere; one area light, or 66 emitters picked
+    through the light tree) against the reference renderer's image, with the plain parity
+    test's bounds (image means within 0.5 %, 8x8 blocks within 2 %)."""
+    import json
+    import pathlib
+
+    from sprout_b200 import capi, scenes
+
+    data = np.load(pathlib.Path(__file__).resolve().parent / "golden" / "cornell_reference.npz")
+    meta = json.loads(bytes(data["meta"]).decode())["cases"][case]
+    ref = data[case].astype(np.float64)
+    w, h = meta["width"], meta["height"]
+    su = capi.SuLibrary()
+    assert su.su_init(False) == 0
+    try:
+        scene = dict(meta["scene"])
+        scene.pop("scene", None)
+        scenes.cornell(su, w, h, tonemap=True, spp=4 * meta["spp"], guiding=True, **scene)
+        assert su.su_render_frame(0) == 0, su.messages
+        assert su.su_postprocess() == 0
+        img = su.framebuffer(w, h)[0][:, :, :3].astype(np.float64)
+    finally:
+        su.su_release()
+    m_ref, m_img = ref.mean(axis=(0, 1)), img.mean(axis=(0, 1))
+    assert np.all(np.abs(m_img - m_ref) <= 0.005 * m_ref), (m_img, m_ref)
+    bi, br = block_means(img, 8), block_means(ref, 8)
+    worst = np.max(np.abs(bi - br) / (np.abs(br) + 0.01))
+    assert worst < 0.02, f"worst 8x8 block deviation {worst:.4f}"
+
+
 def test_guiding_settings_are_parsed():
     """The integrator's "guiding" object: explicit settings render, and training can stop
     early (train_spp) with the rest of the frame sampled by the frozen network."""
