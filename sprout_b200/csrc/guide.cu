@@ -114,9 +114,10 @@ __device__ inline float warp_column_sums(float v[32]) {
 // takes sample r = t % 128 and lobes 4h..4h+3 (h = t / 128).  From the accumulator plus bias it
 // forms the mixture (softmax weights of all lobes; unit mean and concentration of its own),
 // adds its lobes' share of q(d) = sum_j w_j vMF_j(d), exchanges it with the other half, and
-// writes the gradient of scale * (-log q(d)) with respect to its 20 outputs (guide_mlp.cuh's
-// output_gradient, split in two) as BF16 dZ columns; columns 40..63 are cleared.  The per-warp
-// column sums of the FP32 gradient go to red (the output bias gradient).  Ends with a barrier.
+// writes the gradient of scale * (-log q(d)) with respect to its 20 outputs as BF16 dZ
+// columns (columns 40..63 are cleared); the log-concentration has zero gradient where it is
+// clamped.  The per-warp column sums of the FP32 gradient go to red (the output bias
+// gradient).  Ends with a barrier.
 __device__ inline void finish_output_gradient(Train_tc_smem& s, float const* b, shading::V3 d, float scale,
                                               float (&red)[8][32], Tmem_tile& tm) {
     if (!mbar_wait(tm.mbar, tm.phase)) {

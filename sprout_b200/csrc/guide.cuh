@@ -98,14 +98,6 @@ SPB_HD float vmf_pdf(Lobe const& l, shading::V3 w) {
     return norm * expf(l.kappa * (shading::dot(l.mu, w) - 1.f));
 }
 
-SPB_HD float mixture_pdf(Lobe const lobes[Lobes], shading::V3 w) {
-    float p = 0.f;
-    for (int j = 0; j < Lobes; ++j) {
-        p += lobes[j].weight * vmf_pdf(lobes[j], w);
-    }
-    return p;
-}
-
 // Samples one lobe with two uniform numbers: the cosine to the mean by the inverse CDF of the
 // vMF (Wenzel Jakob, "Numerically stable sampling of the von Mises Fisher distribution on S2",
 // 2012), clamped to [-1, 1], then the azimuth.
@@ -115,20 +107,6 @@ SPB_HD shading::V3 vmf_sample(Lobe const& l, float u1, float u2) {
     float const phi = 2.f * 3.14159265358979f * u2;
     shading::Frame const f = shading::make_frame(l.mu);
     return (s * cosf(phi)) * f.t + (s * sinf(phi)) * f.b + c * f.n;
-}
-
-// Samples the mixture with three uniform numbers: a lobe by weight, then vmf_sample.
-SPB_HD shading::V3 mixture_sample(Lobe const lobes[Lobes], float u0, float u1, float u2) {
-    int   j   = Lobes - 1;
-    float acc = 0.f;
-    for (int k = 0; k < Lobes - 1; ++k) {
-        acc += lobes[k].weight;
-        if (u0 < acc) {
-            j = k;
-            break;
-        }
-    }
-    return vmf_sample(lobes[j], u1, u2);
 }
 
 }  // namespace spb::guide

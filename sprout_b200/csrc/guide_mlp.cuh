@@ -327,38 +327,4 @@ __device__ inline void tc_teardown(Tmem_tile const& tm) {
     }
 }
 
-// Gradient of scale * (-log q(d)) with respect to one sample's 40 outputs o (mixture from
-// guide.cuh; the log-concentration has zero gradient where it is clamped).
-__device__ inline void output_gradient(float const* o, shading::V3 d, float scale, float* g) {
-    Lobe lobes[Lobes];
-    mixture(o, lobes);
-    float v[Lobes];
-    float q = 0.f;
-    for (int j = 0; j < Lobes; ++j) {
-        v[j] = vmf_pdf(lobes[j], d);
-        q += lobes[j].weight * v[j];
-    }
-    q = fmaxf(q, 1e-30f);
-    for (int j = 0; j < Lobes; ++j) {
-        float const r     = lobes[j].weight * v[j] / q;
-        float const kappa = lobes[j].kappa;
-        float const c     = shading::dot(lobes[j].mu, d);
-        g[32 + j]         = scale * (lobes[j].weight - r);
-        float const lk    = o[4 * j + 3];
-        if (lk > Log_kappa_min && lk < Log_kappa_max) {
-            float const x2   = 2.f * kappa;
-            float const dlog = 1.f - x2 / expm1f(x2) + kappa * (c - 1.f);
-            g[4 * j + 3]     = -scale * r * dlog;
-        } else {
-            g[4 * j + 3] = 0.f;
-        }
-        float const m0 = o[4 * j], m1 = o[4 * j + 1], m2 = o[4 * j + 2];
-        float const l2 = m0 * m0 + m1 * m1 + m2 * m2;
-        float const f  = l2 > 1e-20f ? -scale * r * kappa * rsqrtf(l2) : 0.f;
-        g[4 * j]       = f * (d.x - lobes[j].mu.x * c);
-        g[4 * j + 1]   = f * (d.y - lobes[j].mu.y * c);
-        g[4 * j + 2]   = f * (d.z - lobes[j].mu.z * c);
-    }
-}
-
 }  // namespace spb::guide

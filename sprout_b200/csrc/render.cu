@@ -1214,7 +1214,7 @@ __device__ __forceinline__ float mixture_pdf_at(float4 const* __restrict__ row, 
     return q;
 }
 
-// guide::mixture_sample on the stored form.
+// Samples the stored mixture with three uniform numbers: a lobe by weight, then its vMF.
 __device__ __forceinline__ V3 mixture_sample_at(float4 const* __restrict__ row, float u0, float u1, float u2) {
     float4 const w0 = row[8], w1 = row[9];
     float const  w[guide::Lobes] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
