@@ -164,6 +164,15 @@ class ScriptRecorder:
         self.lines.append("defaults")
         return 0
 
+    def su_mount(self, folder):
+        self.lines.append(f"mount {folder.decode() if isinstance(folder, bytes) else folder}")
+        return 0
+
+    def load_take(self, path, width, height):
+        """su_load_take of a take file whose camera renders width x height."""
+        self.lines.append(f"take {int(width)} {int(height)} {path}")
+        return 0
+
     def su_create_material(self, desc):
         self.lines.append("material " + (desc.decode() if isinstance(desc, bytes) else desc))
         self.n["material"] += 1

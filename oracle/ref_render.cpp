@@ -21,6 +21,8 @@
 //          [<num parts> <byte offset of the parts: (first index, index count, material slot)>]
 //     prop <mesh handle or built-in shape id (< 8)> <num materials> <material handles...>
 //     light <prop handle>
+//     mount <folder>   (su_mount; the folder name without spaces)
+//     take <width> <height> <take file>   (su_load_take; the take's resolution, for the readback)
 //     progressive <iterations>
 //     frame <frame>
 //   Handles: the n-th camera/material/mesh/prop command creates handle 4000/1000+n/2000+n/3000+n.
@@ -78,6 +80,12 @@ int main(int argc, char** argv) {
             int p = 0;
             std::sscanf(rest, "%d", &p);
             status |= su_init(p != 0);
+            // the reference's warnings and errors go to stderr
+            su_register_log([](uint32_t type, char const* text) {
+                if (type == SU_LOG_WARNING || type == SU_LOG_ERROR) {
+                    std::fprintf(stderr, "reference log %u: %s\n", type, text);
+                }
+            });
         } else if (c == "camera") {
             float fov = 0.f;
             std::sscanf(rest, "%u %u %f", &width, &height, &fov);
@@ -89,6 +97,14 @@ int main(int argc, char** argv) {
                         &m[1], &m[2], &m[3], &m[4], &m[5], &m[6], &m[7], &m[8], &m[9], &m[10],
                         &m[11], &m[12], &m[13], &m[14], &m[15]);
             status |= su_entity_set_transformation(handles[h], m);
+        } else if (c == "mount") {
+            char folder[4096] = {};
+            std::sscanf(rest, " %4095s", folder);
+            status |= su_mount(folder);
+        } else if (c == "take") {
+            char path[4096] = {};
+            std::sscanf(rest, "%u %u %4095s", &width, &height, path);
+            status |= su_load_take(path);
         } else if (c == "integrators") {
             su_create_integrators(rest);
         } else if (c == "sampler") {

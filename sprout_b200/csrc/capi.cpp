@@ -86,6 +86,7 @@ struct Engine {
     bool                  tonemap_linear = false;  // su_create_defaults: Linear tonemapper
     uint32_t              iteration     = 0;
     std::vector<float>    target;  // resolved rgba
+    std::vector<std::string> mounts;  // su_mount folders, searched last mounted first
 };
 
 Engine* engine = nullptr;
@@ -433,6 +434,361 @@ int32_t render_samples(uint32_t first, uint32_t count) {
     return 0;
 }
 
+// ---- take and scene files (take::Loader::load, take_loader.cpp:98-197; scene::Loader,
+// scene_loader.cpp) -- the subset this renderer draws: a Perspective camera, the sampler's
+// sample count, the surface integrator, and a scene of named materials and Prop / Light
+// entities whose shapes are built-in shapes or triangle-mesh JSON files.  Each part is handed
+// to the matching su_* entry point, so a take builds exactly the scene those calls would.
+
+// Reads a whole file; false if it cannot be opened.
+bool read_text(std::string const& path, std::string& out) {
+    std::FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) {
+        return false;
+    }
+    out.clear();
+    char buf[1 << 16];
+    for (size_t n; (n = std::fread(buf, 1, sizeof(buf), f)) > 0;) {
+        out.append(buf, n);
+    }
+    std::fclose(f);
+    return true;
+}
+
+bool file_exists(std::string const& path) {
+    std::FILE* f = std::fopen(path.c_str(), "rb");
+    if (f) {
+        std::fclose(f);
+    }
+    return f != nullptr;
+}
+
+std::string directory_of(std::string const& path) {
+    size_t const slash = path.find_last_of('/');
+    return slash == std::string::npos ? std::string() : path.substr(0, slash + 1);
+}
+
+// A file named in a take or scene: under the mounted folders (last mounted first), then
+// beside the file that names it, then as given.
+std::string resolve(std::string const& name, std::string const& base) {
+    if (!name.empty() && name[0] == '/') {
+        return name;
+    }
+    for (auto m = engine->mounts.rbegin(); m != engine->mounts.rend(); ++m) {
+        std::string dir = *m;
+        if (!dir.empty() && dir.back() != '/') {
+            dir += '/';
+        }
+        if (file_exists(dir + name)) {
+            return dir + name;
+        }
+    }
+    if (!base.empty() && file_exists(base + name)) {
+        return base + name;
+    }
+    return name;
+}
+
+bool read_vec3(spb::json::Value const* v, double out[3]) {
+    if (!v || !v->is_array() || v->array.size() < 3) {
+        return false;
+    }
+    for (int k = 0; k < 3; ++k) {
+        out[k] = v->array[k].number;
+    }
+    return true;
+}
+
+// Row-major object-to-world matrix of a "transformation" object, as json::read_transformation
+// (json.cpp:252-296) reads it: 16 numbers, or position / scale / rotation (Euler degrees, the
+// basis Rz * Rx * Ry of json.cpp:216-227 with the rotation matrices of matrix3x3.inl:61-104)
+// / look_at and up (basis rows: -cross(dir, up), up, dir); rows 0-2 are the basis rows times
+// the scale, row 3 the position (compose, matrix4x4.inl:27-34).
+bool transformation_matrix(spb::json::Value const& v, float m[16]) {
+    if (v.is_array()) {
+        if (v.array.size() != 16) {
+            return false;
+        }
+        for (int i = 0; i < 16; ++i) {
+            m[i] = float(v.array[i].number);
+        }
+        return true;
+    }
+    if (!v.is_object()) {
+        return false;
+    }
+    double pos[3] = {0, 0, 0}, scale[3] = {1, 1, 1}, rot[3] = {0, 0, 0}, up[3] = {0, 1, 0}, at[3] = {0, 0, 1};
+    read_vec3(v.find("position"), pos);
+    read_vec3(v.find("scale"), scale);
+    read_vec3(v.find("rotation"), rot);
+    read_vec3(v.find("up"), up);
+    bool const look = read_vec3(v.find("look_at"), at);
+    double b[3][3];
+    if (look) {
+        double d[3] = {at[0] - pos[0], at[1] - pos[1], at[2] - pos[2]};
+        double const l = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        for (double& x : d) {
+            x /= l;
+        }
+        double const right[3] = {-(d[1] * up[2] - d[2] * up[1]), -(d[2] * up[0] - d[0] * up[2]),
+                                 -(d[0] * up[1] - d[1] * up[0])};
+        for (int k = 0; k < 3; ++k) {
+            b[0][k] = right[k];
+            b[1][k] = up[k];
+            b[2][k] = d[k];
+        }
+    } else {
+        double const d2r = 3.14159265358979323846 / 180.0;
+        double const cx = std::cos(rot[0] * d2r), sx = std::sin(rot[0] * d2r);
+        double const cy = std::cos(rot[1] * d2r), sy = std::sin(rot[1] * d2r);
+        double const cz = std::cos(rot[2] * d2r), sz = std::sin(rot[2] * d2r);
+        double const rx[3][3] = {{1, 0, 0}, {0, cx, -sx}, {0, sx, cx}};
+        double const ry[3][3] = {{cy, 0, sy}, {0, 1, 0}, {-sy, 0, cy}};
+        double const rz[3][3] = {{cz, -sz, 0}, {sz, cz, 0}, {0, 0, 1}};
+        double zx[3][3];
+        for (int i = 0; i < 3; ++i) {
+            for (int j = 0; j < 3; ++j) {
+                zx[i][j] = rz[i][0] * rx[0][j] + rz[i][1] * rx[1][j] + rz[i][2] * rx[2][j];
+            }
+        }
+        for (int i = 0; i < 3; ++i) {
+            for (int j = 0; j < 3; ++j) {
+                b[i][j] = zx[i][0] * ry[0][j] + zx[i][1] * ry[1][j] + zx[i][2] * ry[2][j];
+            }
+        }
+    }
+    // The rotation is kept as a quaternion (quaternion::create, quaternion.inl:12-35) and
+    // turned back into a basis (create_matrix3x3, quaternion.inl:64-86); for the look_at basis,
+    // whose up is not made orthogonal to the direction, this round trip changes the matrix.
+    float r[3][3];
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) {
+            r[i][j] = float(b[i][j]);
+        }
+    }
+    float q[4];  // x, y, z, w
+    float t;
+    if (r[2][2] < 0.f) {
+        if (r[0][0] > r[1][1]) {
+            t = 1.f + r[0][0] - r[1][1] - r[2][2];
+            float const v[4] = {t, r[0][1] + r[1][0], r[2][0] + r[0][2], r[2][1] - r[1][2]};
+            std::copy(v, v + 4, q);
+        } else {
+            t = 1.f - r[0][0] + r[1][1] - r[2][2];
+            float const v[4] = {r[0][1] + r[1][0], t, r[1][2] + r[2][1], r[0][2] - r[2][0]};
+            std::copy(v, v + 4, q);
+        }
+    } else {
+        if (r[0][0] < -r[1][1]) {
+            t = 1.f - r[0][0] - r[1][1] + r[2][2];
+            float const v[4] = {r[2][0] + r[0][2], r[1][2] + r[2][1], t, r[1][0] - r[0][1]};
+            std::copy(v, v + 4, q);
+        } else {
+            t = 1.f + r[0][0] + r[1][1] + r[2][2];
+            float const v[4] = {r[2][1] - r[1][2], r[0][2] - r[2][0], r[1][0] - r[0][1], t};
+            std::copy(v, v + 4, q);
+        }
+    }
+    float const f = 0.5f / std::sqrt(t);
+    float const x = f * q[0], y = f * q[1], z = f * q[2], w = f * q[3];
+    float const basis[3][3] = {{1.f - (2.f * y * y + 2.f * z * z), 2.f * x * y - 2.f * z * w, 2.f * x * z + 2.f * y * w},
+                               {2.f * x * y + 2.f * z * w, 1.f - (2.f * x * x + 2.f * z * z), 2.f * y * z - 2.f * x * w},
+                               {2.f * x * z - 2.f * y * w, 2.f * y * z + 2.f * x * w, 1.f - (2.f * x * x + 2.f * y * y)}};
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) {
+            m[4 * i + j] = float(basis[i][j] * scale[i]);
+        }
+        m[4 * i + 3] = 0.f;
+        m[12 + i]    = float(pos[i]);
+    }
+    m[15] = 1.f;
+    return true;
+}
+
+// A triangle-mesh JSON file ({"geometry": {"parts", "vertices": {"positions", "normals"},
+// "indices"}}, triangle_mesh_provider.cpp) through su_create_triangle_mesh_async.
+uint32_t load_mesh_file(std::string const& path) {
+    std::string text;
+    spb::json::Value root;
+    if (!read_text(path, text) || !spb::json::parse(text.c_str(), root)) {
+        log(SU_LOG_ERROR, "su_load_take: cannot read mesh file " + path);
+        return Null;
+    }
+    spb::json::Value const* g = root.find("geometry");
+    spb::json::Value const* verts = g ? g->find("vertices") : nullptr;
+    spb::json::Value const* pos = verts ? verts->find("positions") : nullptr;
+    spb::json::Value const* nrm = verts ? verts->find("normals") : nullptr;
+    spb::json::Value const* idx = g ? g->find("indices") : nullptr;
+    if (!pos || !pos->is_array() || !nrm || !nrm->is_array() || !idx || !idx->is_array() ||
+        pos->array.size() % 3 || nrm->array.size() != pos->array.size() || idx->array.size() % 3) {
+        log(SU_LOG_ERROR, "su_load_take: mesh file " + path + " needs positions, normals and triangle indices");
+        return Null;
+    }
+    std::string const topology = spb::json::string_or(g->find("primitive_topology"), "triangle_list");
+    if (topology != "triangle_list") {
+        log(SU_LOG_ERROR, "su_load_take: " + path + ": only triangle_list topology is supported");
+        return Null;
+    }
+    std::vector<float> p(pos->array.size()), n(nrm->array.size());
+    for (size_t i = 0; i < p.size(); ++i) {
+        p[i] = float(pos->array[i].number);
+        n[i] = float(nrm->array[i].number);
+    }
+    std::vector<uint32_t> ind(idx->array.size());
+    for (size_t i = 0; i < ind.size(); ++i) {
+        ind[i] = uint32_t(idx->array[i].number);
+    }
+    std::vector<uint32_t> parts;
+    if (spb::json::Value const* pv = g->find("parts"); pv && pv->is_array()) {
+        for (auto const& part : pv->array) {
+            parts.push_back(uint32_t(spb::json::number_or(part.find("start_index"), 0)));
+            parts.push_back(uint32_t(spb::json::number_or(part.find("num_indices"), 0)));
+            parts.push_back(uint32_t(spb::json::number_or(part.find("material_index"), 0)));
+        }
+    }
+    return su_create_triangle_mesh_async(uint32_t(ind.size() / 3), uint32_t(p.size() / 3), 3, p.data(), 3, n.data(),
+                                         0, nullptr, 0, nullptr, ind.data(), uint32_t(parts.size() / 3),
+                                         parts.empty() ? nullptr : parts.data());
+}
+
+// Built-in shape names (sprout.h's SU_SHAPE_* ids).
+uint32_t builtin_shape(std::string const& type) {
+    static std::map<std::string, uint32_t> const ids = {
+        {"Canopy", 0}, {"Cube", 1}, {"Disk", 2}, {"Distant_sphere", 3}, {"Infinite_sphere", 4},
+        {"Plane", 5}, {"Rectangle", 6}, {"Sphere", 7}};
+    auto const it = ids.find(type);
+    return it == ids.end() ? Null : it->second;
+}
+
+int32_t load_scene(std::string const& path) {
+    std::string text;
+    spb::json::Value root;
+    if (!read_text(path, text) || !spb::json::parse(text.c_str(), root)) {
+        log(SU_LOG_ERROR, "su_load_take: cannot read scene " + path);
+        return -2;
+    }
+    std::string const base = directory_of(path);
+    std::map<std::string, uint32_t> materials;
+    if (spb::json::Value const* mv = root.find("materials"); mv && mv->is_array()) {
+        for (auto const& m : mv->array) {
+            std::string const name = spb::json::string_or(m.find("name"), "");
+            uint32_t const id = su_create_material(spb::json::dump(m).c_str());
+            if (id == Null) {
+                log(SU_LOG_ERROR, "su_load_take: material \"" + name + "\" not supported");
+                return -2;
+            }
+            materials[name] = id;
+        }
+    }
+    std::map<std::string, uint32_t> meshes;
+    spb::json::Value const* ev = root.find("entities");
+    if (!ev || !ev->is_array()) {
+        log(SU_LOG_ERROR, "su_load_take: scene " + path + " has no entities");
+        return -2;
+    }
+    for (auto const& e : ev->array) {
+        std::string const type = spb::json::string_or(e.find("type"), "");
+        if (type != "Prop" && type != "Light") {
+            log(SU_LOG_WARNING, "su_load_take: entity type \"" + type + "\" skipped");
+            continue;
+        }
+        spb::json::Value const* sv = e.find("shape");
+        uint32_t shape = Null;
+        if (sv && sv->find("file")) {
+            std::string const file = resolve(spb::json::string_or(sv->find("file"), ""), base);
+            auto const it = meshes.find(file);
+            shape = it != meshes.end() ? it->second : (meshes[file] = load_mesh_file(file));
+        } else if (sv) {
+            shape = builtin_shape(spb::json::string_or(sv->find("type"), ""));
+        }
+        if (shape == Null) {
+            log(SU_LOG_ERROR, "su_load_take: entity shape not supported");
+            return -2;
+        }
+        std::vector<uint32_t> mats;
+        if (spb::json::Value const* names = e.find("materials"); names && names->is_array()) {
+            for (auto const& n : names->array) {
+                auto const it = materials.find(n.string);
+                if (it == materials.end()) {
+                    log(SU_LOG_ERROR, "su_load_take: unknown material \"" + n.string + "\"");
+                    return -2;
+                }
+                mats.push_back(it->second);
+            }
+        }
+        uint32_t const prop = su_create_prop(shape, uint32_t(mats.size()), mats.data());
+        if (prop == Null) {
+            return -2;
+        }
+        if (spb::json::Value const* tv = e.find("transformation")) {
+            float m[16];
+            if (!transformation_matrix(*tv, m) || su_entity_set_transformation(prop, m) != 0) {
+                log(SU_LOG_ERROR, "su_load_take: bad transformation");
+                return -2;
+            }
+        }
+        if (type == "Light" && su_create_light(prop) != 0) {
+            return -2;
+        }
+    }
+    return 0;
+}
+
+// su_load_take: a take given as JSON text or as a file name.
+int32_t load_take(std::string const& string) {
+    size_t const first = string.find_first_not_of(" \t\r\n");
+    bool const   is_json = first != std::string::npos && string[first] == '{';
+    std::string  text, base;
+    if (is_json) {
+        text = string;
+    } else {
+        std::string const path = resolve(string, "");
+        if (!read_text(path, text)) {
+            log(SU_LOG_ERROR, "su_load_take: cannot read " + string);
+            return -2;
+        }
+        base = directory_of(path);
+    }
+    spb::json::Value take;
+    if (!spb::json::parse(text.c_str(), take) || !take.is_object()) {
+        log(SU_LOG_ERROR, "su_load_take: take JSON parse error");
+        return -2;
+    }
+    if (spb::json::Value const* cam = take.find("camera")) {
+        if (su_create_camera(spb::json::dump(*cam).c_str()) == Null) {
+            return -2;
+        }
+        spb::json::Value const* persp = cam->find("Perspective");
+        if (spb::json::Value const* tv = persp ? persp->find("transformation") : nullptr) {
+            float m[16];
+            if (!transformation_matrix(*tv, m) || su_entity_set_transformation(engine->camera_entity, m) != 0) {
+                log(SU_LOG_ERROR, "su_load_take: bad camera transformation");
+                return -2;
+            }
+        }
+        // The sensor filter here is Gaussian, radius 1, alpha 1.8 (the C API's); other filters
+        // (the take default is radius 2) are drawn with it.
+        spb::json::Value const* sensor = persp ? persp->find("sensor") : nullptr;
+        spb::json::Value const* filter = sensor ? sensor->find("filter") : nullptr;
+        spb::json::Value const* gauss  = filter ? filter->find("Gaussian") : nullptr;
+        if (!gauss || spb::json::number_or(gauss->find("radius"), 2.0) != 1.0 ||
+            spb::json::number_or(gauss->find("alpha"), 1.8) != 1.8) {
+            log(SU_LOG_WARNING, "su_load_take: the sensor filter is drawn as Gaussian (radius 1, alpha 1.8)");
+        }
+    }
+    if (spb::json::Value const* sampler = take.find("sampler"); sampler && sampler->is_object() &&
+                                                                !sampler->object.empty()) {
+        su_create_sampler(uint32_t(spb::json::number_or(sampler->object[0].second.find("samples_per_pixel"), 1.0)));
+    }
+    if (spb::json::Value const* integrator = take.find("integrator")) {
+        su_create_integrators(spb::json::dump(*integrator).c_str());
+    }
+    if (spb::json::Value const* scene = take.find("scene"); scene && scene->is_string()) {
+        return load_scene(resolve(scene->string, base));
+    }
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -459,7 +815,9 @@ SU_LIBRARY_API int32_t su_mount(char const* folder) {
     if (!engine) {
         return -1;
     }
-    (void)folder;
+    if (folder) {
+        engine->mounts.emplace_back(folder);
+    }
     return 0;
 }
 
@@ -482,9 +840,7 @@ SU_LIBRARY_API int32_t su_load_take(char const* string) {
     if (!engine) {
         return -1;
     }
-    (void)string;
-    log(SU_LOG_ERROR, "su_load_take: take files are not supported by this renderer");
-    return -2;
+    return load_take(string ? string : "");
 }
 
 SU_LIBRARY_API int32_t su_create_defaults(void) {

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cctype>
+#include <cstdio>
 #include <cstdlib>
 #include <map>
 #include <memory>
@@ -219,6 +220,63 @@ inline double number_or(Value const* v, double fallback) {
 
 inline bool bool_or(Value const* v, bool fallback) {
     return (v && v->kind == Value::Kind::Bool) ? v->boolean : fallback;
+}
+
+inline std::string string_or(Value const* v, std::string const& fallback) {
+    return (v && v->kind == Value::Kind::String) ? v->string : fallback;
+}
+
+// The value as JSON text (numbers with 17 significant digits), for handing a parsed
+// sub-object to an entry point that takes a JSON string.
+inline void dump(Value const& v, std::string& out) {
+    switch (v.kind) {
+        case Value::Kind::Null:
+            out += "null";
+            break;
+        case Value::Kind::Bool:
+            out += v.boolean ? "true" : "false";
+            break;
+        case Value::Kind::Number: {
+            char buf[32];
+            std::snprintf(buf, sizeof(buf), "%.17g", v.number);
+            out += buf;
+            break;
+        }
+        case Value::Kind::String:
+            out += '"';
+            for (char const c : v.string) {
+                if (c == '"' || c == '\\') {
+                    out += '\\';
+                }
+                out += c;
+            }
+            out += '"';
+            break;
+        case Value::Kind::Array:
+            out += '[';
+            for (size_t i = 0; i < v.array.size(); ++i) {
+                out += i ? "," : "";
+                dump(v.array[i], out);
+            }
+            out += ']';
+            break;
+        case Value::Kind::Object:
+            out += '{';
+            for (size_t i = 0; i < v.object.size(); ++i) {
+                out += i ? "," : "";
+                dump(Value{Value::Kind::String, false, 0.0, v.object[i].first, {}, {}}, out);
+                out += ':';
+                dump(v.object[i].second, out);
+            }
+            out += '}';
+            break;
+    }
+}
+
+inline std::string dump(Value const& v) {
+    std::string out;
+    dump(v, out);
+    return out;
 }
 
 }  // namespace spb::json

@@ -55,7 +55,13 @@ CASES = {
     "volume64": (64, 64, 2048, {"scene": "volume"}, scenes.fbm_density(32)),
     # the guiding workload's room (plain MIS): lit only through a doorway by the environment
     "doorway96": (96, 54, 8192, {"scene": "doorway"}, None),
+    # a take file (tests/golden/takes/room.take, written for these tests in the reference's take
+    # and scene format) loaded by su_load_take: panels of a mesh file rotated by Euler angles,
+    # built-in Sphere and Cube props, a Sphere lamp, a look_at camera; the sample count is set
+    # after the take
+    "take_room96": (96, 72, 4096, {"scene": "take", "take": "room.take"}, None),
 }
+TAKES = HERE / "takes"
 PATH = HERE / "cornell_reference.npz"
 # Block size of the block-mean comparison where 8 is too small: many small, bright emitters
 # leave the 2048-spp reference image with 4 % noise in single 8x8 blocks (its 1024- and
@@ -78,6 +84,11 @@ def build(su, w, h, spp, kwargs, density=None):
         return scenes.volume(su, w, h, spp, density, **kwargs)
     if name == "doorway":
         return scenes.doorway(su, w, h, spp, **kwargs)
+    if name == "take":
+        su.su_mount(str(TAKES) + "/")
+        su.load_take(str(TAKES / kwargs["take"]), w, h)
+        su.su_create_sampler(spp)
+        return su.su_create_defaults()
     return scenes.cornell(su, w, h, tonemap=True, spp=spp, density=density, **kwargs)
 
 

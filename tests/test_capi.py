@@ -190,3 +190,33 @@ def test_builtin_shapes_accepted():
             assert su.su_create_prop(shape, 1, ids.ctypes.data) == capi.SU_RESOURCE_NULL, shape
     finally:
         assert su.su_release() == 0
+
+
+def test_take_files_load(tmp_path):
+    """su_load_take reads a take and its scene (tests/golden/takes: a take written in the
+    reference's format) on the host, resolving names through su_mount folders; unreadable
+    files, unknown material names and bad transformations give -2."""
+    import json
+
+    from sprout_b200 import capi
+
+    takes = pathlib.Path(__file__).resolve().parent / "golden" / "takes"
+    su = capi.SuLibrary()
+    assert su.su_init(False) == 0
+    try:
+        assert su.su_load_take(b"room.take") == -2  # not found before the folder is mounted
+        assert su.su_mount((str(takes) + "/").encode()) == 0
+        assert su.su_load_take(b"room.take") == 0
+        assert su.su_load_take(b"missing.take") == -2
+        assert su.su_load_take(b'{"scene": "missing.scene"}') == -2
+        assert su.su_load_take(b"{not json") == -2
+        scene = json.loads((takes / "room.scene").read_text())
+        scene["entities"][0]["materials"] = ["no_such_material"]
+        (tmp_path / "bad.scene").write_text(json.dumps(scene))
+        assert su.su_load_take(json.dumps({"scene": str(tmp_path / "bad.scene")}).encode()) == -2
+        scene = json.loads((takes / "room.scene").read_text())
+        scene["entities"][0]["transformation"] = [1, 0, 0]
+        (tmp_path / "bad_trafo.scene").write_text(json.dumps(scene))
+        assert su.su_load_take(json.dumps({"scene": str(tmp_path / "bad_trafo.scene")}).encode()) == -2
+    finally:
+        assert su.su_release() == 0

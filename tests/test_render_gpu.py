@@ -48,6 +48,12 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
             scenes.volume(su, width, height, spp, density, **scene)
         elif name == "doorway":
             scenes.doorway(su, width, height, spp, **scene)
+        elif name == "take":
+            takes = GOLDEN.parent / "takes"
+            assert su.su_mount((str(takes) + "/").encode()) == 0
+            assert su.su_load_take(str(takes / scene["take"]).encode()) == 0, su.messages
+            assert su.su_create_sampler(spp) == 0
+            assert su.su_create_defaults() == 0
         else:
             scenes.cornell(su, width, height, tonemap=True, spp=spp, density=density, **scene)
         if progressive:
@@ -66,7 +72,7 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
 
 CASES = ["cornell64_sub3", "cornell128_sub6", "cornell64_medium", "cornell64_thin_direct", "cornell64_grid",
          "cornell64_lights", "wavefront96", "builtins96", "builtins96_backdrop", "volume64",
-         "doorway96"]
+         "doorway96", "take_room96"]
 
 
 @pytest.mark.parametrize("name", CASES)
