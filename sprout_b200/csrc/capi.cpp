@@ -734,6 +734,89 @@ int32_t load_scene(std::string const& path) {
     return 0;
 }
 
+// A 3-D image in the reference's SUB format (image::encoding::sub::Reader::read,
+// sub_image_reader.cpp:35-224): "SUB\0", a uint64 header length, a JSON header (image
+// description: dimensions, Byte1 or Float1; pixels and, for sparse images, a topology bitfield
+// as offsets into the binary part), then the binary part.  A topology marks the stored voxels
+// (32-bit words, bit i at the word's bit 31 - i % 32), whose values follow in order; the others
+// are 0.  Bytes become value / 255.  Returns the new image's id, or Null.
+uint32_t load_sub_image(std::string const& path) {
+    std::string data;
+    if (!read_text(path, data) || data.size() < 12 || data.compare(0, 3, "SUB") != 0) {
+        log(SU_LOG_ERROR, "cannot read SUB image " + path);
+        return Null;
+    }
+    uint64_t header = 0;
+    std::memcpy(&header, data.data() + 4, sizeof(header));
+    spb::json::Value root;
+    if (12 + header > data.size() || !spb::json::parse(data.substr(12, header).c_str(), root)) {
+        log(SU_LOG_ERROR, "bad SUB header in " + path);
+        return Null;
+    }
+    uint64_t const           start = 12 + header;
+    spb::json::Value const* image  = root.find("image");
+    spb::json::Value const* desc   = image ? image->find("description") : nullptr;
+    spb::json::Value const* dims   = desc ? desc->find("dimensions") : nullptr;
+    std::string const       type   = desc ? spb::json::string_or(desc->find("type"), "") : "";
+    spb::json::Value const* pixels = image ? image->find("pixels") : nullptr;
+    spb::json::Value const* pbin   = pixels ? pixels->find("binary") : nullptr;
+    if (!dims || !dims->is_array() || dims->array.size() != 3 || !pbin || (type != "Byte1" && type != "Float1")) {
+        log(SU_LOG_ERROR, "SUB image " + path + ": need dimensions, a Byte1 or Float1 type and pixels");
+        return Null;
+    }
+    Image img;
+    uint64_t voxels = 1;
+    for (int k = 0; k < 3; ++k) {
+        img.dims[k] = uint32_t(dims->array[k].number);
+        voxels *= img.dims[k];
+    }
+    img.channels = 1;
+    img.pixels.assign(voxels, 0.f);
+    uint64_t const bytes  = type == "Byte1" ? 1 : 4;
+    uint64_t       cursor = start + uint64_t(spb::json::number_or(pbin->find("offset"), 0.0));
+    auto const     value  = [&](uint64_t at, float& v) {
+        if (at + bytes > data.size()) {
+            return false;
+        }
+        if (bytes == 1) {
+            v = float(uint8_t(data[at])) * (1.f / 255.f);
+        } else {
+            std::memcpy(&v, data.data() + at, 4);
+        }
+        return true;
+    };
+    spb::json::Value const* topo = image->find("topology");
+    spb::json::Value const* tbin = topo ? topo->find("binary") : nullptr;
+    if (tbin) {
+        uint64_t const words = (voxels + 31) / 32;
+        uint64_t const field = start + uint64_t(spb::json::number_or(tbin->find("offset"), 0.0));
+        if (field + 4 * words > data.size()) {
+            log(SU_LOG_ERROR, "SUB image " + path + ": truncated topology");
+            return Null;
+        }
+        for (uint64_t i = 0; i < voxels; ++i) {
+            uint32_t word;
+            std::memcpy(&word, data.data() + field + 4 * (i >> 5), 4);
+            if (word & (0x80000000u >> (i % 32))) {
+                if (!value(cursor, img.pixels[i])) {
+                    log(SU_LOG_ERROR, "SUB image " + path + ": truncated pixels");
+                    return Null;
+                }
+                cursor += bytes;
+            }
+        }
+    } else {
+        for (uint64_t i = 0; i < voxels; ++i, cursor += bytes) {
+            if (!value(cursor, img.pixels[i])) {
+                log(SU_LOG_ERROR, "SUB image " + path + ": truncated pixels");
+                return Null;
+            }
+        }
+    }
+    engine->images.push_back(std::move(img));
+    return uint32_t(engine->images.size() - 1);
+}
+
 // su_load_take: a take given as JSON text or as a file name.
 int32_t load_take(std::string const& string) {
     size_t const first = string.find_first_not_of(" \t\r\n");
@@ -1084,10 +1167,13 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
         // and subsurface colours default to it, distance 1, anisotropy clamped to +-0.999;
         // coefficients from attenuation() (collision_coefficients.inl:50-71).
         if (spb::json::Value const* density = desc.find("density")) {
-            // "density": {"id": image} or {"file": ...} (read_texture_description,
-            // material_provider.cpp:895-946); only in-memory images are supported here.
-            spb::json::Value const* id = density->is_object() ? density->find("id") : nullptr;
-            uint32_t const image = id && id->is_number() ? uint32_t(id->number) : Null;
+            // "density": {"id": image} or {"file": a SUB image} (read_texture_description,
+            // material_provider.cpp:895-946); files resolve under the su_mount folders.
+            spb::json::Value const* id   = density->is_object() ? density->find("id") : nullptr;
+            spb::json::Value const* file = density->is_object() ? density->find("file") : nullptr;
+            uint32_t const image = id && id->is_number() ? uint32_t(id->number)
+                                   : (file && file->is_string() ? load_sub_image(resolve(file->string, ""))
+                                                                : Null);
             if (image >= engine->images.size() || engine->images[image].channels != 1) {
                 log(SU_LOG_ERROR, "su_create_material: density must name a one-channel image id");
                 return Null;

@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import json
 import math
+import pathlib
 
 import numpy as np
 
@@ -183,8 +184,9 @@ def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounc
 
     medium: optional dict of Volumetric material parameters (e.g. color, attenuation_distance,
     anisotropy); the sphere then becomes a homogeneous participating medium instead of metal.
-    density: optional (nz, ny, nx) float array; with medium, the sphere is replaced by the
-    cube of grid_box_transformation() filled with this density grid.
+    density: optional (nz, ny, nx) float array, or the name of a SUB image file (sub.write_sub);
+    with medium, the sphere is replaced by the cube of grid_box_transformation() filled with
+    this density grid.
     many_lights: the ceiling light is replaced by light_panel(): 66 emitters of different
     radiance, two of them two-sided (a light-tree test).
     guiding: None for plain MIS, else True or a dict of guide settings (this renderer's
@@ -207,6 +209,8 @@ def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounc
         metal = _material(su, "Substitute", color=[0.95, 0.64, 0.54], roughness=math.sqrt(0.3), metallic=1.0)
     elif density is None:
         metal = _material(su, "Volumetric", **medium)
+    elif isinstance(density, (str, pathlib.Path)):
+        metal = _material(su, "Volumetric", density={"file": str(density)}, **medium)
     else:
         image = su.image(density)
         metal = _material(su, "Volumetric", density={"id": int(image)}, **medium)

@@ -220,3 +220,36 @@ def test_take_files_load(tmp_path):
         assert su.su_load_take(json.dumps({"scene": str(tmp_path / "bad_trafo.scene")}).encode()) == -2
     finally:
         assert su.su_release() == 0
+
+
+def test_density_from_sub_files(tmp_path):
+    """A Volumetric material's "density": {"file": ...} reads the reference's SUB format
+    (dense or sparse, Float1 or Byte1; sprout_b200.sub.write_sub), resolved under su_mount
+    folders; missing, foreign or truncated files give SU_RESOURCE_NULL."""
+    import json
+
+    from sprout_b200 import capi, scenes
+    from sprout_b200.sub import write_sub
+
+    dens = scenes.density_grid(8, 6, 5)
+    for name, kw in {"dense.sub": {}, "sparse.sub": {"sparse": True}, "bytes.sub": {"byte": True},
+                     "sparse_bytes.sub": {"byte": True, "sparse": True}}.items():
+        write_sub(tmp_path / name, dens, **kw)
+    (tmp_path / "truncated.sub").write_bytes((tmp_path / "dense.sub").read_bytes()[:-7])
+    (tmp_path / "foreign.sub").write_bytes(b"PNG\0" + b"\0" * 64)
+
+    su = capi.SuLibrary()
+    assert su.su_init(False) == 0
+    try:
+        def volumetric(file):
+            return su.su_create_material(json.dumps({"rendering": {"Volumetric": {"density": {"file": file}}}}).encode())
+
+        assert volumetric(str(tmp_path / "dense.sub")) != capi.SU_RESOURCE_NULL
+        assert volumetric("sparse.sub") == capi.SU_RESOURCE_NULL  # not mounted yet
+        assert su.su_mount(str(tmp_path).encode()) == 0
+        for name in ("sparse.sub", "bytes.sub", "sparse_bytes.sub"):
+            assert volumetric(name) != capi.SU_RESOURCE_NULL, name
+        for name in ("missing.sub", "truncated.sub", "foreign.sub"):
+            assert volumetric(name) == capi.SU_RESOURCE_NULL, name
+    finally:
+        assert su.su_release() == 0

@@ -139,3 +139,19 @@ def test_graph_replay_matches_direct_launches():
             su.su_release()
     assert graph_waves[0] > 0 and graph_waves[1] == 0
     assert np.array_equal(images[0], images[1])
+
+
+def test_density_file_renders_like_the_image(tmp_path):
+    """The density grid read from a SUB file (dense, and sparse behind a topology) renders the
+    image the same grid given as an in-memory image renders, bit for bit."""
+    from sprout_b200.sub import write_sub
+
+    dens = scenes.density_grid()
+    write_sub(tmp_path / "dense.sub", dens)
+    write_sub(tmp_path / "sparse.sub", dens, sparse=True)
+    medium = {"color": [0.9, 0.6, 0.4], "attenuation_distance": 0.03, "anisotropy": 0.3}
+    kw = {"sphere_subdivisions": 2, "medium": medium}
+    ref = render(48, 48, 64, density=dens, **kw)
+    for name in ("dense.sub", "sparse.sub"):
+        img = render(48, 48, 64, density=str(tmp_path / name), **kw)
+        assert np.array_equal(img, ref), name
