@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -817,6 +818,77 @@ uint32_t load_sub_image(std::string const& path) {
     return uint32_t(engine->images.size() - 1);
 }
 
+// An 8-bit RGB PNG (the reference's default exporter, encoding::png::Writer, writes this from
+// the postprocessed frame): one IHDR, the rows (filter byte 0 each) as a zlib stream of stored
+// deflate blocks in one IDAT, IEND; CRC-32 per chunk, Adler-32 over the rows.
+bool write_png(std::string const& path, uint32_t w, uint32_t h, uint8_t const* rgb) {
+    static uint32_t const* const crc_table = [] {
+        static uint32_t t[256];
+        for (uint32_t n = 0; n < 256; ++n) {
+            uint32_t c = n;
+            for (int k = 0; k < 8; ++k) {
+                c = (c & 1) ? 0xEDB88320u ^ (c >> 1) : c >> 1;
+            }
+            t[n] = c;
+        }
+        return t;
+    }();
+    auto const be32 = [](std::string& out, uint32_t v) {
+        for (int k = 3; k >= 0; --k) {
+            out += char((v >> (8 * k)) & 0xFF);
+        }
+    };
+    auto const chunk = [&](std::string& out, char const* type, std::string const& data) {
+        be32(out, uint32_t(data.size()));
+        std::string const body = std::string(type, 4) + data;
+        uint32_t          crc  = 0xFFFFFFFFu;
+        for (unsigned char const c : body) {
+            crc = crc_table[(crc ^ c) & 0xFF] ^ (crc >> 8);
+        }
+        out += body;
+        be32(out, crc ^ 0xFFFFFFFFu);
+    };
+    std::string raw;
+    raw.reserve(size_t(h) * (3 * size_t(w) + 1));
+    for (uint32_t y = 0; y < h; ++y) {
+        raw += char(0);
+        raw.append(reinterpret_cast<char const*>(rgb) + size_t(y) * 3 * w, 3 * size_t(w));
+    }
+    std::string z = "\x78\x01";
+    for (size_t at = 0; at < raw.size() || at == 0; at += 65535) {
+        size_t const n = std::min<size_t>(65535, raw.size() - at);
+        z += char(at + n >= raw.size() ? 1 : 0);
+        z += char(n & 0xFF);
+        z += char(n >> 8);
+        z += char(~n & 0xFF);
+        z += char((~n >> 8) & 0xFF);
+        z.append(raw, at, n);
+        if (raw.empty()) {
+            break;
+        }
+    }
+    uint32_t a = 1, b = 0;
+    for (unsigned char const c : raw) {
+        a = (a + c) % 65521;
+        b = (b + a) % 65521;
+    }
+    be32(z, (b << 16) | a);
+    std::string ihdr;
+    be32(ihdr, w);
+    be32(ihdr, h);
+    ihdr += std::string("\x08\x02\x00\x00\x00", 5);  // 8 bits, RGB, deflate, no filter, no interlace
+    std::string png = "\x89PNG\r\n\x1a\n";
+    chunk(png, "IHDR", ihdr);
+    chunk(png, "IDAT", z);
+    chunk(png, "IEND", "");
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) {
+        return false;
+    }
+    bool const ok = std::fwrite(png.data(), 1, png.size(), f) == png.size();
+    return std::fclose(f) == 0 && ok;
+}
+
 // su_load_take: a take given as JSON text or as a file name.
 int32_t load_take(std::string const& string) {
     size_t const first = string.find_first_not_of(" \t\r\n");
@@ -1480,14 +1552,32 @@ SU_LIBRARY_API int32_t su_render_frame(uint32_t frame) {
 }
 
 SU_LIBRARY_API int32_t su_render(void) {
-    return su_render_frame(0);
+    // render frame 0, then export it (capi.cpp:565-580)
+    if (int32_t const s = su_render_frame(0)) {
+        return s;
+    }
+    return su_export_frame(0);
 }
 
+// The reference's default exporter (take_loader.cpp set_default_exporter): the postprocessed
+// frame as an 8-bit sRGB PNG named output_<frame, 6 digits>.png in the working directory.
 SU_LIBRARY_API int32_t su_export_frame(uint32_t frame) {
     if (!engine) {
         return -1;
     }
-    (void)frame;
+    if (su_postprocess() != 0 && engine->target.empty()) {  // the current film, resolved
+        log(SU_LOG_WARNING, "su_export_frame: no rendered frame to export");
+        return 0;
+    }
+    std::vector<uint8_t> rgb(size_t(engine->width) * engine->height * 3);
+    if (su_copy_framebuffer(SU_UINT8, engine->width, engine->height, 3, rgb.data()) != 0) {
+        return 0;
+    }
+    char name[32];
+    std::snprintf(name, sizeof(name), "output_%06u.png", frame);
+    if (!write_png(name, engine->width, engine->height, rgb.data())) {
+        log(SU_LOG_ERROR, std::string("su_export_frame: cannot write ") + name);
+    }
     return 0;
 }
 

@@ -155,3 +155,24 @@ def test_density_file_renders_like_the_image(tmp_path):
     for name in ("dense.sub", "sparse.sub"):
         img = render(48, 48, 64, density=str(tmp_path / name), **kw)
         assert np.array_equal(img, ref), name
+
+
+def test_render_exports_png(tmp_path, monkeypatch):
+    """su_render renders frame 0 and exports it as the reference's default exporter does:
+    output_000000.png, the 8-bit sRGB framebuffer."""
+    from PIL import Image
+
+    monkeypatch.chdir(tmp_path)
+    su = capi.SuLibrary()
+    assert su.su_init(False) == 0
+    try:
+        scenes.cornell(su, 40, 30, sphere_subdivisions=2, tonemap=True, spp=16)
+        assert su.su_render() == 0, su.messages
+        rgb = np.zeros((30, 40, 3), np.uint8)
+        assert su.su_copy_framebuffer(capi.SU_UINT8, 40, 30, 3, rgb.ctypes.data) == 0
+        assert su.su_export_frame(3) == 0
+    finally:
+        su.su_release()
+    png = np.asarray(Image.open(tmp_path / "output_000000.png"))
+    assert png.shape == (30, 40, 3) and np.array_equal(png, rgb)
+    assert np.array_equal(np.asarray(Image.open(tmp_path / "output_000003.png")), rgb)
