@@ -10,6 +10,8 @@
 
 #include <cuda_bf16.h>
 
+#include <cstring>
+
 #include "guide.cuh"
 
 namespace spb::guide {
@@ -199,6 +201,15 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float v[8]) {
     }
 }
 
+// (max(x, 0), max(y, 0)) rounded to BF16 (x in the low half), in one conversion instruction.
+__device__ __forceinline__ __nv_bfloat162 relu_bf16x2(float x, float y) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(y), "f"(x));
+    __nv_bfloat162 h;
+    std::memcpy(&h, &r, sizeof(r));
+    return h;
+}
+
 // Stores the 40 outputs of sample r into shared memory (Out_stride floats per sample).
 struct Smem_outputs {
     float* out;
@@ -262,8 +273,7 @@ __device__ inline void finish_layer(float const* b, __nv_bfloat16* act, Store co
             __nv_bfloat162 h[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                h[q] = __floats2bfloat162_rn(fmaxf(v[j + 2 * q] + b[n0 + j + 2 * q], 0.f),
-                                             fmaxf(v[j + 2 * q + 1] + b[n0 + j + 2 * q + 1], 0.f));
+                h[q] = relu_bf16x2(v[j + 2 * q] + b[n0 + j + 2 * q], v[j + 2 * q + 1] + b[n0 + j + 2 * q + 1]);
             }
             *reinterpret_cast<uint4*>(act + tiled(r, n0 + j, N)) = *reinterpret_cast<uint4*>(h);
         }
