@@ -1879,48 +1879,44 @@ cudaError_t upload(T*& dst, void const* src, size_t bytes) {
     return bytes ? cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
 }
 
-// Majorant cells of a density grid: (min, max) density over each Cell_dim^3 block of voxels
-// plus one voxel on every side (wrapped for the repeat address mode, clipped otherwise), the
-// minimum starting at 1 as in Octree_builder::Splitter::split
+// Majorant cells of a density grid, one thread per cell: (min, max) density over its
+// Cell_dim^3 block of voxels plus one voxel on every side (wrapped for the repeat address mode,
+// clipped otherwise), the minimum starting at 1 as in Octree_builder::Splitter::split
 // (volumetric_octree_builder.cpp:170-186).
-std::vector<float2> majorant_cells(Density_grid const& g, bool repeat, int const cells[3]) {
-    int const           n[3] = {int(g.dims[0]), int(g.dims[1]), int(g.dims[2])};
-    int const           dim  = 1 << Cell_log2;
-    std::vector<float2> out(size_t(cells[0]) * cells[1] * cells[2]);
-    auto wrap = [&](int v, int axis) { return ((v % n[axis]) + n[axis]) % n[axis]; };
-    for (int cz = 0; cz < cells[2]; ++cz) {
-        for (int cy = 0; cy < cells[1]; ++cy) {
-            for (int cx = 0; cx < cells[0]; ++cx) {
-                int const c[3] = {cx, cy, cz};
-                int       lo[3];
-                int       hi[3];
-                for (int a = 0; a < 3; ++a) {
-                    lo[a] = c[a] * dim - 1;
-                    hi[a] = std::min((c[a] + 1) * dim + 1, n[a] + (repeat ? 1 : 0));
-                    if (!repeat) {
-                        lo[a] = std::max(lo[a], 0);
-                    }
-                }
-                float mn = 1.f;
-                float mx = 0.f;
-                for (int z = lo[2]; z < hi[2]; ++z) {
-                    for (int y = lo[1]; y < hi[1]; ++y) {
-                        size_t const row = (size_t(wrap(z, 2)) * n[1] + wrap(y, 1)) * n[0];
-                        for (int x = lo[0]; x < hi[0]; ++x) {
-                            float const v = g.density[row + wrap(x, 0)];
-                            mn            = std::min(mn, v);
-                            mx            = std::max(mx, v);
-                        }
-                    }
-                }
-                if (mn > mx) {
-                    mn = mx = 0.f;
-                }
-                out[(size_t(cz) * cells[1] + cy) * cells[0] + cx] = make_float2(mn, mx);
+__global__ void k_majorant_cells(float const* __restrict__ density, int nx, int ny, int nz, int cx, int cy, int cz,
+                                 bool repeat, float2* cells) {
+    int const i = int(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= cx * cy * cz) {
+        return;
+    }
+    int const n[3] = {nx, ny, nz};
+    int const c[3] = {i % cx, (i / cx) % cy, i / (cx * cy)};
+    int const dim  = 1 << Cell_log2;
+    int       lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = c[a] * dim - 1;
+        hi[a] = min((c[a] + 1) * dim + 1, n[a] + (repeat ? 1 : 0));
+        if (!repeat) {
+            lo[a] = max(lo[a], 0);
+        }
+    }
+    auto const wrap = [&](int v, int axis) { return ((v % n[axis]) + n[axis]) % n[axis]; };
+    float      mn   = 1.f;
+    float      mx   = 0.f;
+    for (int z = lo[2]; z < hi[2]; ++z) {
+        for (int y = lo[1]; y < hi[1]; ++y) {
+            size_t const row = (size_t(wrap(z, 2)) * n[1] + wrap(y, 1)) * n[0];
+            for (int x = lo[0]; x < hi[0]; ++x) {
+                float const v = __ldg(density + row + wrap(x, 0));
+                mn            = fminf(mn, v);
+                mx            = fmaxf(mx, v);
             }
         }
     }
-    return out;
+    if (mn > mx) {
+        mn = mx = 0.f;
+    }
+    cells[i] = make_float2(mn, mx);
 }
 
 }  // namespace
@@ -2214,8 +2210,14 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
         mg.cy    = cells[1];
         mg.cz    = cells[2];
         mg.flags = (gm.nearest ? 1u : 0u) | (gm.repeat ? 2u : 0u);
-        std::vector<float2> const cm = majorant_cells(g, gm.repeat, cells);
-        SPB_RCUDA(upload(d_->grid_cells[k], cm.data(), cm.size() * sizeof(float2)));
+        int const num_cells = cells[0] * cells[1] * cells[2];
+        free_ptr(d_->grid_cells[k]);
+        SPB_RCUDA(dev_malloc(&d_->grid_cells[k], size_t(num_cells) * sizeof(float2)));
+        k_majorant_cells<<<(num_cells + 127) / 128, 128, 0, d_->stream>>>(mg.density, mg.nx, mg.ny, mg.nz, cells[0],
+                                                                          cells[1], cells[2], gm.repeat,
+                                                                          d_->grid_cells[k]);
+        SPB_RCUDA(cudaGetLastError());
+        SPB_RCUDA(cudaStreamSynchronize(d_->stream));
         mg.cells = d_->grid_cells[k];
         media.push_back(mg);
     }
