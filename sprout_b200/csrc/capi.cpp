@@ -84,6 +84,7 @@ struct Engine {
     spb::render::Renderer renderer;
     bool                  frame_started = false;
     bool                  scene_dirty    = true;   // host scene changed since the last upload
+    bool                  camera_dirty   = false;  // only the camera changed since then
     bool                  tonemap_linear = false;  // su_create_defaults: Linear tonemapper
     uint32_t              iteration     = 0;
     std::vector<float>    target;  // resolved rgba
@@ -301,6 +302,8 @@ void texture_space(float const* m, Mesh const& mesh, float out[12]) {
     }
 }
 
+int32_t apply_camera();
+
 int32_t compile_scene() {
     spb::render::Scene_desc scene;
     scene.materials = engine->materials;
@@ -406,6 +409,12 @@ int32_t compile_scene() {
         log(SU_LOG_ERROR, engine->renderer.error());
         return s == SPB_ERROR_CUDA ? -2 : -1;
     }
+    return apply_camera();
+}
+
+// The camera entity's transformation, resolution and field of view, and the integrator
+// settings, into the renderer (without touching the uploaded scene).
+int32_t apply_camera() {
     spb::render::Camera_desc cam;
     cam.width  = engine->width;
     cam.height = engine->height;
@@ -1074,7 +1083,7 @@ SU_LIBRARY_API int32_t su_camera_set_resolution(uint32_t width, uint32_t height)
     engine->width         = width;
     engine->height        = height;
     engine->frame_started = false;
-    engine->scene_dirty   = true;
+    engine->camera_dirty  = true;
     return 0;
 }
 
@@ -1472,7 +1481,8 @@ SU_LIBRARY_API int32_t su_entity_set_transformation(uint32_t entity, float const
     }
     std::memcpy(engine->entities[entity].trafo, trafo, sizeof(float) * 16);
     engine->frame_started = false;
-    engine->scene_dirty   = true;
+    // moving the camera re-applies the camera only; moving a prop rebuilds the scene
+    (entity == engine->camera_entity ? engine->camera_dirty : engine->scene_dirty) = true;
     return 0;
 }
 
@@ -1496,12 +1506,19 @@ SU_LIBRARY_API int32_t su_start_render_frame(uint32_t frame) {
     if (!ready()) {
         return -2;
     }
-    // The scene is flattened, its BVH built and uploaded only when something changed.
+    // The scene is flattened, its BVH built and uploaded only when something changed; a moved
+    // camera or a new resolution only re-applies the camera.
     if (engine->scene_dirty) {
         if (int32_t const s = compile_scene()) {
             return s;
         }
-        engine->scene_dirty = false;
+        engine->scene_dirty  = false;
+        engine->camera_dirty = false;
+    } else if (engine->camera_dirty) {
+        if (int32_t const s = apply_camera()) {
+            return s;
+        }
+        engine->camera_dirty = false;
     }
     if (engine->renderer.start_frame()) {
         log(SU_LOG_ERROR, engine->renderer.error());

@@ -176,3 +176,34 @@ def test_render_exports_png(tmp_path, monkeypatch):
     png = np.asarray(Image.open(tmp_path / "output_000000.png"))
     assert png.shape == (30, 40, 3) and np.array_equal(png, rgb)
     assert np.array_equal(np.asarray(Image.open(tmp_path / "output_000003.png")), rgb)
+
+
+def test_camera_move_renders_like_a_fresh_scene():
+    """Moving the camera and changing the resolution between frames re-applies the camera
+    without rebuilding the scene; the frame equals the one a freshly built scene with that
+    camera renders, bit for bit."""
+    def fresh(w, h, position):
+        su = capi.SuLibrary()
+        assert su.su_init(False) == 0
+        try:
+            cam = scenes.cornell(su, w, h, sphere_subdivisions=2, tonemap=True, spp=16)
+            su.set_transformation(cam, scenes.translation(*position))
+            assert su.su_render_frame(0) == 0
+            assert su.su_postprocess() == 0
+            return su.framebuffer(w, h)[0][:, :, :3].copy()
+        finally:
+            su.su_release()
+
+    su = capi.SuLibrary()
+    assert su.su_init(False) == 0
+    try:
+        cam = scenes.cornell(su, 48, 40, sphere_subdivisions=2, tonemap=True, spp=16)
+        assert su.su_render_frame(0) == 0
+        assert su.su_camera_set_resolution(40, 32) == 0
+        su.set_transformation(cam, scenes.translation(0.2, 1.1, -3.0))
+        assert su.su_render_frame(0) == 0
+        assert su.su_postprocess() == 0
+        moved = su.framebuffer(40, 32)[0][:, :, :3].copy()
+    finally:
+        su.su_release()
+    assert np.array_equal(moved, fresh(40, 32, (0.2, 1.1, -3.0)))
