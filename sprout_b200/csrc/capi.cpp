@@ -1131,6 +1131,7 @@ SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
                 s.guiding = g->is_object() || spb::json::bool_or(g, false);
                 if (g->is_object()) {
                     s.guide_fraction = float(spb::json::number_or(g->find("fraction"), s.guide_fraction));
+                    s.metal_fraction = float(spb::json::number_or(g->find("metal_fraction"), s.metal_fraction));
                     s.guide_batch    = uint32_t(spb::json::number_or(g->find("batch"), s.guide_batch));
                     s.guide_steps    = uint32_t(spb::json::number_or(g->find("steps"), s.guide_steps));
                     s.guide_lr       = float(spb::json::number_or(g->find("learning_rate"), s.guide_lr));
@@ -1141,6 +1142,7 @@ SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
                     s.guide_depth     = uint32_t(spb::json::number_or(g->find("depth"), s.guide_depth));
                 }
                 s.guide_fraction = std::clamp(s.guide_fraction, 0.f, 0.95f);
+                s.metal_fraction = s.metal_fraction < 0.f ? -1.f : std::min(s.metal_fraction, 0.95f);
                 s.record_depth   = std::clamp(s.record_depth, 1u, 8u);
                 s.guide_batch    = std::clamp(s.guide_batch, 128u, 1u << 22);
             }

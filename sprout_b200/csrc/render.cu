@@ -156,6 +156,7 @@ struct Wave {
     uint32_t max_bounces;
     uint32_t guiding;         // 1: sample the guide's mixture at surface vertices
     float    guide_fraction;  // its share of continuation directions
+    float    metal_fraction;  // the same at metallic (pure GGX) surfaces
     uint32_t record_depth;    // vertices per path recorded for training (0: none)
     uint32_t guide_depth;     // vertices of depth below this are guided
     float4   bounds_lo;       // scene box, for the guide's position encoding
@@ -1458,7 +1459,7 @@ __global__ void __launch_bounds__(Shade_block)
                 // from it with probability gf, else from the BSDF, and every pdf the MIS
                 // weights use is the combination of both.
                 bool const  guided = wave.guiding && depth < wave.guide_depth && p.guide_ok[i];
-                float const gf     = guided ? wave.guide_fraction : 0.f;
+                float const gf     = !guided ? 0.f : (mat.metallic == 1.f ? wave.metal_fraction : wave.guide_fraction);
                 float4 const* const mix = reinterpret_cast<float4 const*>(p.guide_out + size_t(i) * Mixture_floats);
 
                 // Next-event estimation (sample_lights / evaluate_light, pathtracer_mis.cpp:281-347).
@@ -2586,6 +2587,7 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
                   settings_.max_bounces};
         wave.guiding        = settings_.guiding ? 1u : 0u;
         wave.guide_fraction = settings_.guide_fraction;
+        wave.metal_fraction = settings_.metal_fraction < 0.f ? settings_.guide_fraction : settings_.metal_fraction;
         wave.guide_depth    = settings_.guide_depth;
         wave.record_depth   = training ? settings_.record_depth : 0u;
         wave.bounds_lo      = d_->bounds_lo;

@@ -59,6 +59,7 @@ struct Settings {
     // of every path, until guide_train_spp samples per pixel have been rendered.
     bool     guiding         = false;
     float    guide_fraction  = 0.5f;
+    float    metal_fraction  = -1.f;  // at metallic surfaces; negative: guide_fraction
     uint32_t guide_batch     = 1u << 16;
     uint32_t guide_steps     = 32;
     float    guide_lr        = 1e-2f;
