@@ -409,7 +409,10 @@ __global__ void __launch_bounds__(Block) k_gradients_tc(__nv_bfloat16 const* wbf
 // grads[p] = sum over blocks of partial[b][p], in block order (deterministic); divided by the
 // total of weight_parts when given (the batch's loss weights, summed in a fixed order).
 __global__ void k_reduce(float const* partial, uint32_t blocks, float const* weight_parts, uint32_t num_parts,
-                         float* grads) {
+                         float* grads, uint32_t* step_counter) {
+    if (step_counter && blockIdx.x == 0 && threadIdx.x == 0) {
+        ++*step_counter;  // the Adam step that follows (k_adam_counted reads it)
+    }
     __shared__ float total;
     if (threadIdx.x < 32) {
         float acc = 0.f;
@@ -480,6 +483,34 @@ __global__ void k_adam(float* params, float* m, float* v, float const* grads, fl
     }
 }
 
+// Adam with its step count in device memory (counted by k_reduce), so that training steps can
+// be replayed from a captured graph; block 0 also advances `advance` (the caller's batch
+// counter) when given, after every reader of it has run.
+__global__ void k_adam_counted(float* params, float* m, float* v, float const* grads, float lr,
+                               uint32_t const* step_counter, uint32_t* advance, __nv_bfloat16* wbf) {
+    int const p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (advance && p == 0) {
+        ++*advance;
+    }
+    if (p >= Parameters) {
+        return;
+    }
+    float const step = float(max(*step_counter, 1u));
+    float const c1   = 1.f / (1.f - powf(0.9f, step));
+    float const c2   = 1.f / (1.f - powf(0.999f, step));
+    float const g    = grads[p];
+    float const mm   = 0.9f * m[p] + 0.1f * g;
+    float const vv   = 0.999f * v[p] + 0.001f * g * g;
+    m[p]             = mm;
+    v[p]             = vv;
+    float const w    = params[p] - lr * (mm * c1) / (sqrtf(vv * c2) + 1e-8f);
+    params[p]        = w;
+    int const i      = bf16_index(p);
+    if (i >= 0) {
+        wbf[i] = __float2bfloat16(w);
+    }
+}
+
 }  // namespace
 
 size_t tile_smem_bytes() {
@@ -523,6 +554,7 @@ Network::~Network() {
     release(wbf_);
     release(partial_);
     release(error_);
+    release(step_dev_);
 }
 
 int Network::init(uint32_t seed) {
@@ -555,10 +587,16 @@ int Network::set_parameters(float const* host) {
             return e;
         }
     }
+    if (!step_dev_) {
+        if (cudaError_t const e = cudaMalloc(&step_dev_, sizeof(uint32_t))) {
+            return e;
+        }
+    }
     cudaError_t e = cudaMemcpy(params_, host, bytes, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(m_, 0, bytes);
     if (e == cudaSuccess) e = cudaMemset(v_, 0, bytes);
     if (e == cudaSuccess) e = cudaMemset(grads_, 0, bytes);
+    if (e == cudaSuccess) e = cudaMemset(step_dev_, 0, sizeof(uint32_t));
     if (e != cudaSuccess) {
         return e;
     }
@@ -620,14 +658,37 @@ int Network::run_gradients(void const* inputs, bool tiled, float const* dirs, fl
     if (blocks == 0) {
         return cudaMemsetAsync(grads_, 0, Parameters * sizeof(float), stream);
     }
+    if (int const e = prepare_gradients(n)) {
+        return e;
+    }
     // one persistent block per SM (at most one per tile)
+    uint32_t const grid = uint32_t(std::min<uint64_t>(blocks, partial_blocks_));
+    if (tiled) {
+        k_gradients_tc<true><<<grid, Block, sizeof(Train_tc_smem), stream>>>(wbf_, params_, inputs, dirs, scale, n,
+                                                                             uint32_t(blocks), partial_, error_);
+    } else {
+        k_gradients_tc<false><<<grid, Block, sizeof(Train_tc_smem), stream>>>(wbf_, params_, inputs, dirs, scale, n,
+                                                                              uint32_t(blocks), partial_, error_);
+    }
+    k_reduce<<<(Parameters + 255) / 256, 256, 0, stream>>>(partial_, grid, weight_parts, num_parts, grads_,
+                                                           tiled ? step_dev_ : nullptr);
+    return cudaGetLastError();
+}
+
+int Network::adam_counted(float lr, uint32_t* advance, cudaStream_t stream) {
+    k_adam_counted<<<(Parameters + 255) / 256, 256, 0, stream>>>(params_, m_, v_, grads_, lr, step_dev_, advance,
+                                                                 wbf_);
+    return cudaGetLastError();
+}
+
+int Network::prepare_gradients(uint64_t n) {
     static int const sms = [] {
         int dev = 0, count = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
         return std::max(count, 1);
     }();
-    uint32_t const grid = uint32_t(std::min<uint64_t>(blocks, uint64_t(sms)));
+    uint64_t const grid = std::min<uint64_t>((n + Tile - 1) / Tile, uint64_t(sms));
     if (grid > partial_blocks_) {
         release(partial_);
         if (cudaError_t const e = cudaMalloc(&partial_, size_t(grid) * Parameters * sizeof(float))) {
@@ -644,15 +705,7 @@ int Network::run_gradients(void const* inputs, bool tiled, float const* dirs, fl
             return e;
         }
     }
-    if (tiled) {
-        k_gradients_tc<true><<<grid, Block, sizeof(Train_tc_smem), stream>>>(wbf_, params_, inputs, dirs, scale, n,
-                                                                             uint32_t(blocks), partial_, error_);
-    } else {
-        k_gradients_tc<false><<<grid, Block, sizeof(Train_tc_smem), stream>>>(wbf_, params_, inputs, dirs, scale, n,
-                                                                              uint32_t(blocks), partial_, error_);
-    }
-    k_reduce<<<(Parameters + 255) / 256, 256, 0, stream>>>(partial_, grid, weight_parts, num_parts, grads_);
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
 int Network::adam(float lr, cudaStream_t stream) {

@@ -38,6 +38,13 @@ class Network {
                         float const* weight_parts, uint32_t num_parts, cudaStream_t stream);
     // One Adam step with the current gradient.
     int adam(float lr, cudaStream_t stream);
+    // One Adam step after gradients_tiled(), with the step count kept in device memory (each
+    // gradients_tiled() call counts one), so that the pair can be replayed from a captured
+    // graph; increments *advance (if given) once the step has run.
+    int adam_counted(float lr, uint32_t* advance, cudaStream_t stream);
+    // Allocates what gradients_tiled() on n samples needs, so that no allocation happens while
+    // a stream is being captured.
+    int prepare_gradients(uint64_t n);
 
     float const*         gradient() const { return grads_; }
     // True once a tensor-core completion wait of forward() or gradients() ran out.
@@ -59,6 +66,7 @@ class Network {
     uint64_t       partial_blocks_ = 0;
     uint32_t       step_    = 0;
     uint32_t*      error_   = nullptr;  // set by a tensor-core wait that ran out
+    uint32_t*      step_dev_ = nullptr;  // Adam steps taken through gradients_tiled()
 };
 
 }  // namespace spb::guide

@@ -1693,9 +1693,11 @@ __global__ void k_gather(Paths p, uint32_t w, uint32_t h, uint32_t samples, floa
 // kernel reads them (BF16 tiles of 128 rows); each block adds its weights in a fixed order into
 // parts[block] (the loss is normalised by their total).
 __global__ void __launch_bounds__(256)
-    k_train_gather(Paths p, Launch const* __restrict__ launch, uint32_t records, uint32_t batch, uint32_t pass,
-                   __nv_bfloat16* in, float* dir, float* weight, float* parts) {
+    k_train_gather(Paths p, Launch const* __restrict__ launch, uint32_t records, uint32_t batch,
+                   uint32_t const* __restrict__ pass_counter, __nv_bfloat16* in, float* dir, float* weight,
+                   float* parts) {
     Wave const&      wave = launch->wave;
+    uint32_t const   pass = *pass_counter;
     __shared__ float part[256];
     uint32_t const   i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t const   rows = (batch + guide::Tile - 1) / guide::Tile * guide::Tile;
@@ -1810,7 +1812,14 @@ struct Renderer::Device {
     float*             train_dir   = nullptr;
     float*             train_w     = nullptr;
     float*             train_parts = nullptr;  // per gather block: its weights' sum
-    uint32_t           pass        = 0;  // training passes since the scene was set
+    uint32_t*          pass_counter = nullptr;  // training batches drawn since the network was set
+    // one captured training pass (guide_steps x [gather, gradients, Adam]) and its shape
+    struct Train_graph {
+        uint32_t        records, batch, steps;
+        float           lr;
+        cudaGraphExec_t exec;
+    };
+    Train_graph        train_graph{0, 0, 0, 0.f, nullptr};
     // paths
     uint32_t  capacity = 0;
     Paths     paths{};
@@ -1969,6 +1978,7 @@ Renderer::~Renderer() {
     free_ptr(d_->train_dir);
     free_ptr(d_->train_w);
     free_ptr(d_->train_parts);
+    free_ptr(d_->pass_counter);
     free_ptr(d_->nodes);
     free_ptr(d_->tris);
     free_ptr(d_->tri_info);
@@ -2357,6 +2367,12 @@ int32_t Renderer::ensure_guide(uint32_t paths) {
         SPB_RCUDA(dev_malloc(&d_->train_w, size_t(batch) * sizeof(float)));
         SPB_RCUDA(dev_malloc(&d_->train_parts, (rows + 255) / 256 * sizeof(float)));
         d_->train_capacity = batch;
+        clear_graphs();
+        SPB_RCUDA(cudaError_t(d_->net.prepare_gradients(batch)));
+    }
+    if (!d_->pass_counter) {
+        SPB_RCUDA(dev_malloc(&d_->pass_counter, sizeof(uint32_t)));
+        d_->net_ready = false;
     }
     if (!d_->net_ready) {
         clear_graphs();
@@ -2379,8 +2395,8 @@ int32_t Renderer::ensure_guide(uint32_t paths) {
         int const per_sm    = std::min({smem_sm / (int(sizeof(Infer_smem)) + reserved),
                                         regs_sm / std::max(1, warp_regs * (guide::Block / 32)), 2048 / guide::Block});
         d_->guide_grid = uint32_t(std::max(1, sms * std::max(1, per_sm)));
+        SPB_RCUDA(cudaMemset(d_->pass_counter, 0, sizeof(uint32_t)));
         d_->net_ready = true;
-        d_->pass      = 0;
     }
     return SPB_OK;
 }
@@ -2393,22 +2409,59 @@ void Renderer::clear_graphs() {
         }
     }
     d_->graphs.clear();
+    if (d_->train_graph.exec) {
+        cudaGraphExecDestroy(d_->train_graph.exec);
+    }
+    d_->train_graph = Device::Train_graph{0, 0, 0, 0.f, nullptr};
 }
 
 // Training after a pass: guide_steps Adam steps, each on a fresh batch of the pass's records.
+// The batch counter and Adam's step count live in device memory, so a pass of a recurring shape
+// is captured once as a graph and replayed (no host launch gaps between its ~100 launches).
 int32_t Renderer::train_guide(uint32_t paths) {
     cudaStream_t   st      = d_->stream;
     uint32_t const batch   = settings_.guide_batch;
     uint32_t const records = paths * settings_.record_depth;
+    uint32_t const steps   = settings_.guide_steps;
+    float const    lr      = settings_.guide_lr;
     // one thread per batch row, the last tile's rows past the batch included
     uint32_t const gather_blocks = ((batch + guide::Tile - 1) / guide::Tile * guide::Tile + 255) / 256;
-    for (uint32_t step = 0; step < settings_.guide_steps; ++step) {
-        k_train_gather<<<gather_blocks, 256, 0, st>>>(d_->paths, d_->launch_dev, records, batch, d_->pass++, d_->train_in,
-                                                      d_->train_dir, d_->train_w, d_->train_parts);
-        SPB_RCUDA(cudaError_t(d_->net.gradients_tiled(d_->train_in, d_->train_dir, d_->train_w, batch,
-                                                      d_->train_parts, gather_blocks, st)));
-        SPB_RCUDA(cudaError_t(d_->net.adam(settings_.guide_lr, st)));
+    auto const     enqueue_pass  = [&]() -> int32_t {
+        for (uint32_t step = 0; step < steps; ++step) {
+            k_train_gather<<<gather_blocks, 256, 0, st>>>(d_->paths, d_->launch_dev, records, batch, d_->pass_counter,
+                                                          d_->train_in, d_->train_dir, d_->train_w, d_->train_parts);
+            SPB_RCUDA(cudaError_t(d_->net.gradients_tiled(d_->train_in, d_->train_dir, d_->train_w, batch,
+                                                          d_->train_parts, gather_blocks, st)));
+            SPB_RCUDA(cudaError_t(d_->net.adam_counted(lr, d_->pass_counter, st)));
+        }
+        return SPB_OK;
+    };
+    if (!settings_.cuda_graphs) {
+        return enqueue_pass();
     }
+    Device::Train_graph& g = d_->train_graph;
+    if (!g.exec || g.records != records || g.batch != batch || g.steps != steps || g.lr != lr) {
+        if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
+        SPB_RCUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int32_t const     e     = enqueue_pass();
+        cudaGraph_t       graph = nullptr;
+        cudaError_t const ce    = cudaStreamEndCapture(st, &graph);
+        if (e != SPB_OK || ce != cudaSuccess) {
+            if (graph) {
+                cudaGraphDestroy(graph);
+            }
+            return e != SPB_OK ? e : fail_cuda("cudaStreamEndCapture", int(ce));
+        }
+        cudaGraphExec_t   exec = nullptr;
+        cudaError_t const ie   = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        SPB_RCUDA(ie);
+        g = Device::Train_graph{records, batch, steps, lr, exec};
+    }
+    SPB_RCUDA(cudaGraphLaunch(g.exec, st));
     return SPB_OK;
 }
 

@@ -246,7 +246,9 @@ def measure_guiding(width=1280, height=720, reference_spp=4096, target=0.01, gui
     at s spp also measures (E[e] = v / s + v / R).  Each reported relMSE has c subtracted.  For
     each integrator: a probe render gives the sample count expected to reach the target (relMSE
     falls as 1/spp), then renders at that count (raised until the target is met) give the
-    reported sample count and device time of one frame."""
+    reported sample count; the frame at that count is rendered three times (the same image) and
+    its median device and wall times are reported, so that one host stall on a shared machine
+    does not set the ratio."""
     ref, ref_s, _ = doorway_frame(width, height, reference_spp, None, seed=1000)
     k = 0.5 / ref.mean()
 
@@ -276,6 +278,14 @@ def measure_guiding(width=1280, height=720, reference_spp=4096, target=0.01, gui
             if err <= target:
                 break
             spp = max(spp + 8, int(np.ceil(spp * err / target / 8.0)) * 8)
+        last = runs[-1]
+        devs, walls = [last["device_seconds"]], [last["wall_seconds"]]
+        for _ in range(2):
+            _, dev, wall = doorway_frame(width, height, spp, guiding if guided else None, stats_out=last_stats)
+            devs.append(round(dev, 4))
+            walls.append(round(wall, 3))
+        last["device_seconds"], last["wall_seconds"] = float(np.median(devs)), float(np.median(walls))
+        last["device_seconds_frames"], last["wall_seconds_frames"] = devs, walls
         return runs
 
     plain_v = (e - c) * probe
