@@ -1267,11 +1267,16 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
             log(SU_LOG_ERROR, "su_create_material: temperature grids are not supported");
             return Null;
         }
+        // "emission" (material_provider.cpp:805-806): a homogeneous medium's emitted radiance per
+        // unit absorption (Material::collision_coefficients_emission, material.cpp:87-89)
         V3 emission{0.f, 0.f, 0.f};
         if (read_color(desc.find("emission"), emission) &&
             (emission.x > 0.f || emission.y > 0.f || emission.z > 0.f)) {
-            log(SU_LOG_ERROR, "su_create_material: emissive media are not supported");
-            return Null;
+            if (grid.image != Null) {
+                log(SU_LOG_ERROR, "su_create_material: emissive density grids are not supported");
+                return Null;
+            }
+            m.emission = emission;
         }
         if (spb::json::Value const* sampler = desc.find("sampler")) {
             // read_sampler_settings, material_provider.cpp:866-892; 3-D lookups use address_u

@@ -662,6 +662,56 @@ __device__ __forceinline__ bool track_homogeneous(shading::Material const& m, fl
     return false;
 }
 
+// Tracking in an emissive homogeneous medium (Tracking::tracking with emission,
+// tracking.cpp:473-540): absorption is sampled as an event beside scattering and null
+// collisions, each with probability proportional to its coefficient times the path weight;
+// returns 2 on absorption (li the emitted radiance, lw zero), 1 on scattering at t_out, 0 when
+// the segment is passed.
+__device__ __forceinline__ int track_homogeneous_emissive(shading::Material const& m, float t, float d,
+                                                          Rng& rng, float& t_out, V3& lw, V3& li) {
+    V3 const    mu_t = m.mu_a + m.mu_s;
+    float const mt   = shading::max_component(mu_t);
+    lw               = v3(1.f, 1.f, 1.f);
+    li               = v3(0.f, 0.f, 0.f);
+    if (!(mt > 1e-10f)) {
+        return 0;
+    }
+    float const imt  = 1.f / mt;
+    V3 const    mu_n = v3(mt - mu_t.x, mt - mu_t.y, mt - mu_t.z);
+    for (int step = 0; step < 4096; ++step) {
+        float const r0 = rng.uniform();
+        t -= logf(1.f - r0) * imt;
+        if (t > d) {
+            return 0;
+        }
+        float const ma = ((m.mu_a.x * lw.x) + (m.mu_a.y * lw.y) + (m.mu_a.z * lw.z)) * (1.f / 3.f);
+        float const ms = ((m.mu_s.x * lw.x) + (m.mu_s.y * lw.y) + (m.mu_s.z * lw.z)) * (1.f / 3.f);
+        float const mn = ((mu_n.x * lw.x) + (mu_n.y * lw.y) + (mu_n.z * lw.z)) * (1.f / 3.f);
+        float const mc = ma + ms + mn;
+        if (mc < 1e-10f) {
+            return 0;
+        }
+        float const c  = 1.f / mc;
+        float const pa = ma * c;
+        float const ps = ms * c;
+        float const pn = mn * c;
+        float const r1 = rng.uniform();
+        if (r1 < pa) {
+            li    = lw * ((1.f / (mt * pa)) * m.mu_a) * m.emission;
+            lw    = v3(0.f, 0.f, 0.f);
+            t_out = t;
+            return 2;
+        }
+        if ((r1 <= 1.f - pn) & (ps > 0.f)) {
+            lw    = lw * ((1.f / (mt * ps)) * m.mu_s);
+            t_out = t;
+            return 1;
+        }
+        lw = lw * ((1.f / (mt * pn)) * mu_n);
+    }
+    return 0;
+}
+
 // ---- heterogeneous media: density grids (Grid material, volumetric_grid.cpp) ----
 // Majorants: the grid is cut into cells of Cell_dim^3 voxels; each cell stores the minimum and
 // maximum density over the voxels that trilinear filtering inside it can read (the cell plus
@@ -1319,6 +1369,16 @@ __global__ void __launch_bounds__(Shade_block)
                 float const srs = shading::similarity_relation_scale(m.g, depth);
                 scatter = track_grid(s.media[m.medium - 1], m, srs, f3v(ro), dir_in, ro.w,
                                      p.hit_t[path], rng, t_sc, lw);
+            } else if (m.emission.x > 0.f || m.emission.y > 0.f || m.emission.z > 0.f) {
+                // An emissive medium that is not a light: its emission reaches the camera
+                // segment only (pathtracer_mis.cpp:220-229 with connect_light_volume returning
+                // 0 for a non-light, pathtracer_mis.cpp:382-387).
+                V3        li;
+                int const ev = track_homogeneous_emissive(m, ro.w, p.hit_t[path], rng, t_sc, lw, li);
+                if (ev == 2 && depth == 0) {
+                    L = L + T * li;
+                }
+                scatter = ev == 1;
             } else {
                 scatter = track_homogeneous(m, ro.w, p.hit_t[path], rng, t_sc, lw);
             }

@@ -33,6 +33,12 @@ THIN_MEDIUM = {"color": [0.8, 0.8, 0.8], "attenuation_distance": 0.5, "anisotrop
 # colour-dependent attenuation so that spectral MIS matters.
 GRID_MEDIUM = {"color": [0.9, 0.6, 0.4], "attenuation_distance": 0.03, "anisotropy": 0.3}
 
+# An emissive homogeneous sphere that is not a light: the camera sees its emission (absorption
+# events, each adding the emitted radiance), its scattered light stays dark beyond the camera
+# segment, and it absorbs and scatters the room's light.
+EMISSIVE_MEDIUM = {"color": [0.8, 0.8, 0.8], "subsurface_color": [0.3, 0.3, 0.3], "attenuation_distance": 0.1,
+                   "anisotropy": 0.3, "emission": [6.0, 3.0, 1.0]}
+
 # name -> (width, height, spp, scenes.cornell keyword arguments, density grid or None)
 CASES = {
     "cornell64_sub3": (64, 64, 4096, {"sphere_subdivisions": 3}, None),
@@ -40,6 +46,7 @@ CASES = {
     "cornell64_medium": (64, 64, 4096, {"sphere_subdivisions": 4, "medium": MEDIUM}, None),
     "cornell64_thin_direct": (64, 64, 4096, {"sphere_subdivisions": 4, "medium": THIN_MEDIUM,
                                              "max_bounces": 1, "min_bounces": 1}, None),
+    "cornell64_emissive": (64, 64, 4096, {"sphere_subdivisions": 4, "medium": EMISSIVE_MEDIUM}, None),
     "cornell64_grid": (64, 64, 4096, {"sphere_subdivisions": 2, "medium": GRID_MEDIUM},
                        scenes.density_grid()),
     # 66 emitters of different radiance and orientation, two of them two-sided (light tree)

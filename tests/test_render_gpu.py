@@ -70,7 +70,8 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
         su.su_release()
 
 
-CASES = ["cornell64_sub3", "cornell128_sub6", "cornell64_medium", "cornell64_thin_direct", "cornell64_grid",
+CASES = ["cornell64_sub3", "cornell128_sub6", "cornell64_medium", "cornell64_emissive", "cornell64_thin_direct",
+         "cornell64_grid",
          "cornell64_lights", "wavefront96", "builtins96", "builtins96_backdrop", "volume64",
          "doorway96", "take_room96"]
 
