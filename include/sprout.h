@@ -9,11 +9,14 @@
  * callback.
  *
  * Scope of this implementation (the rendering hot path): perspective camera, triangle meshes
- * (indexed, with normals, optional parts), the Substitute (Disney + GGX) and Light (constant
- * emission) materials, mesh lights, the PTMIS integrator, progressive and batch rendering, and
- * framebuffer readout.  Entry points for take/scene files, images, built-in analytic shapes
- * and animation frames return -2 / SU_RESOURCE_NULL with a logged reason.  Each declaration
- * below cites the reference function it replaces.
+ * (indexed, with normals, optional parts; in memory or from mesh JSON files), the built-in
+ * Cube, Disk, Rectangle, Sphere and Infinite_sphere shapes, the Substitute (Disney + GGX),
+ * Light (constant emission) and Volumetric (homogeneous or density-grid) materials, mesh and
+ * environment lights, one-channel images as density grids, take and scene files through
+ * su_load_take / su_mount, the PTMIS integrator (with optional path guiding), progressive and
+ * batch rendering, framebuffer readout and the default PNG export.  The Canopy,
+ * Distant_sphere and Plane shapes and animation frames return -2 / SU_RESOURCE_NULL with a
+ * logged reason.  Each declaration below cites the reference function it replaces.
  *
  * Deviation: su_copy_framebuffer(SU_FLOAT32, ..., 4, ...) returns 0 after copying; the
  * reference copies and then returns -2 (capi.cpp:704-714).
@@ -59,11 +62,12 @@ SU_LIBRARY_API char const* su_platform_revision(void);
 SU_LIBRARY_API int32_t su_init(bool progressive);
 /* capi.cpp:149-154 */
 SU_LIBRARY_API int32_t su_release(void);
-/* capi.cpp:156-162: file mounts (take/scene files are out of scope; accepted and ignored) */
+/* capi.cpp:156-162: folders searched (last mounted first) for files named by takes, scenes and the *_from_file calls */
 SU_LIBRARY_API int32_t su_mount(char const* folder);
 /* capi.cpp:164-173 */
 SU_LIBRARY_API int32_t su_clear(void);
-/* capi.cpp:175-206: take files are out of scope here: returns -2 */
+/* capi.cpp:175-206: a take as JSON text or a file name (camera, sampler, integrator, scene file with
+   materials and Prop / Light entities); -2 if it cannot be read or names something unsupported */
 SU_LIBRARY_API int32_t su_load_take(char const* string);
 /* capi.cpp:208-229 */
 SU_LIBRARY_API int32_t su_create_defaults(void);
@@ -77,13 +81,14 @@ SU_LIBRARY_API int32_t su_camera_set_resolution(uint32_t width, uint32_t height)
 SU_LIBRARY_API int32_t su_create_sampler(uint32_t num_samples);
 /* capi.cpp:314-326: {"surface": {"PTMIS": {"min_bounces", "max_bounces"}}} */
 SU_LIBRARY_API int32_t su_create_integrators(char const* string);
-/* capi.cpp:328-345: images are out of scope here: returns SU_RESOURCE_NULL */
+/* capi.cpp:328-345: one-channel float or byte images (2-D or 3-D), used as density grids by Volumetric
+   materials; other channel counts return SU_RESOURCE_NULL */
 SU_LIBRARY_API uint32_t su_create_image(uint32_t pixel_type, uint32_t num_channels, uint32_t width,
                                         uint32_t height, uint32_t depth, uint32_t num_elements,
                                         uint32_t stride, char const* data);
-/* capi.cpp:347-365: {"rendering": {"Substitute": {...}}} or {"rendering": {"Light": {...}}} */
+/* capi.cpp:347-365: {"rendering": {"Substitute" | "Light" | "Volumetric": {...}}} */
 SU_LIBRARY_API uint32_t su_create_material(char const* string);
-/* capi.cpp:367-376: returns SU_RESOURCE_NULL (files out of scope) */
+/* capi.cpp:367-376: a material JSON file (as su_create_material), under the mounted folders first */
 SU_LIBRARY_API uint32_t su_create_material_from_file(char const* filename);
 /* capi.cpp:378-406 (the mesh is copied at call time) */
 SU_LIBRARY_API uint32_t su_create_triangle_mesh_async(
@@ -91,7 +96,7 @@ SU_LIBRARY_API uint32_t su_create_triangle_mesh_async(
     float const* positions, uint32_t normals_stride, float const* normals, uint32_t tangents_stride,
     float const* tangents, uint32_t uvs_stride, float const* uvs, uint32_t const* indices,
     uint32_t num_parts, uint32_t const* parts);
-/* capi.cpp:408-418: returns SU_RESOURCE_NULL (files out of scope) */
+/* capi.cpp:408-418: a triangle-mesh JSON file, under the mounted folders first */
 SU_LIBRARY_API uint32_t su_create_triangle_mesh_from_file(char const* filename);
 /* capi.cpp:420-451 */
 SU_LIBRARY_API uint32_t su_create_prop(uint32_t shape, uint32_t num_materials,
@@ -115,7 +120,7 @@ SU_LIBRARY_API int32_t su_entity_set_transformation_frame(uint32_t entity, uint3
 SU_LIBRARY_API int32_t su_render(void);
 /* capi.cpp:582-596 */
 SU_LIBRARY_API int32_t su_render_frame(uint32_t frame);
-/* capi.cpp:598-604 (no exporters: no-op) */
+/* capi.cpp:598-604: writes output_NNNNNN.png (8-bit sRGB) into the working directory */
 SU_LIBRARY_API int32_t su_export_frame(uint32_t frame);
 /* capi.cpp:606-624 */
 SU_LIBRARY_API int32_t su_start_render_frame(uint32_t frame);

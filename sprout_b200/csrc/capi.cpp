@@ -1333,9 +1333,14 @@ SU_LIBRARY_API uint32_t su_create_material_from_file(char const* filename) {
     if (!engine) {
         return Null;
     }
-    (void)filename;
-    log(SU_LOG_ERROR, "su_create_material_from_file: files are not supported by this renderer");
-    return Null;
+    // A material file holds the same JSON su_create_material takes ({"rendering": {...}},
+    // material_provider.cpp:115-146); it is found under the mounted folders, then as given.
+    std::string text;
+    if (!filename || !read_text(resolve(filename, ""), text)) {
+        log(SU_LOG_ERROR, std::string("su_create_material_from_file: cannot read ") + (filename ? filename : "(null)"));
+        return Null;
+    }
+    return su_create_material(text.c_str());
 }
 
 SU_LIBRARY_API uint32_t su_create_triangle_mesh_async(
@@ -1396,9 +1401,12 @@ SU_LIBRARY_API uint32_t su_create_triangle_mesh_from_file(char const* filename) 
     if (!engine) {
         return Null;
     }
-    (void)filename;
-    log(SU_LOG_ERROR, "su_create_triangle_mesh_from_file: files are not supported by this renderer");
-    return Null;
+    // A triangle-mesh JSON file (the format scene files name), under the mounted folders first.
+    if (!filename) {
+        log(SU_LOG_ERROR, "su_create_triangle_mesh_from_file: no file name");
+        return Null;
+    }
+    return load_mesh_file(resolve(filename, ""));
 }
 
 SU_LIBRARY_API uint32_t su_create_prop(uint32_t shape, uint32_t num_materials,

@@ -107,7 +107,7 @@ def test_api_errors_and_lifecycle():
     try:
         assert su.su_init(True) == -1          # one engine only
         assert su.su_render_iteration() == -2  # nothing to render yet
-        assert su.su_create_prop(3, 0, None) == capi.SU_RESOURCE_NULL  # built-in shapes unsupported
+        assert su.su_create_prop(3, 0, None) == capi.SU_RESOURCE_NULL  # Distant_sphere is not supported
         assert su.su_create_material(b"{not json") == capi.SU_RESOURCE_NULL
         assert su.su_load_take(b"x.take") == -2
     finally:
