@@ -193,14 +193,20 @@ def dist_setup():
     return world, rank, local
 
 
-def reference_run(mesh_path, rays_path, steps, warmup):
+def reference_run(mesh_path, rays_path, steps, warmup, num_rays=None):
+    """Times the reference's Builder_SAH + Tree::intersect (oracle/_ref/ref_cast) on all host
+    threads over warmup + steps passes; with num_rays also returns its ids and t (last pass)."""
     import oracle
 
     with tempfile.TemporaryDirectory() as tmp:
         out = os.path.join(tmp, "out.bin")
         res = subprocess.run([str(oracle.REF_CAST), mesh_path, rays_path, out, "0", "hit", str(steps + warmup)],
                              capture_output=True, text=True, check=True)
-    return json.loads(res.stdout.strip().splitlines()[-1])
+        timing = json.loads(res.stdout.strip().splitlines()[-1])
+        if num_rays is None:
+            return timing
+        raw = np.fromfile(out, np.uint8, count=8 * num_rays)
+    return timing, raw[: 4 * num_rays].view(np.uint32), raw[4 * num_rays:].view(np.float32)
 
 
 def write_inputs(tmp, pos, idx, rays):
@@ -213,6 +219,44 @@ def write_inputs(tmp, pos, idx, rays):
     return mesh_path, rays_path
 
 
+def workload_config(rays: int, triangles: int, world: int) -> dict:
+    """The config object both arms print (same keys and values for the same workload)."""
+    return {"workload": WORKLOAD, "rays_per_step_per_gpu": rays, "triangles": triangles,
+            "parallelism": f"replicas x{world} (independent ray ranges)",
+            "l2": "inputs (rays, 512 MiB) larger than L2; no flush"}
+
+
+def l2_copy_bandwidth(torch) -> float:
+    """L2-resident copy bandwidth in GB/s (bytes read + written): torch copy_ between two
+    32 MiB buffers (together well inside the 126 MB L2), 64 copies replayed from one CUDA
+    graph, best of 5 replays timed with CUDA events."""
+    n = (32 << 20) // 4
+    a = torch.ones(n, dtype=torch.float32, device="cuda")
+    b = torch.empty_like(a)
+    reps = 64
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(3):
+            b.copy_(a)
+    torch.cuda.current_stream().wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        for _ in range(reps):
+            b.copy_(a)
+    best = float("inf")
+    for _ in range(6):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        graph.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del graph
+    return 2 * 4 * n * reps / best / 1e9
+
+
 def cpu_lscpu():
     try:
         out = subprocess.run(["lscpu"], capture_output=True, text=True).stdout
@@ -223,18 +267,21 @@ def cpu_lscpu():
 
 
 def run_reference_arm(args, world, rank):
+    """The reference's own CPU traversal (Builder_SAH(16,64,4) + Tree::intersect, compiled
+    from its sources into oracle/_ref/ref_cast) on all host threads.  The inputs come from the
+    oracle's C restatement of the benchmark synthesis, so this arm loads no product code."""
     if rank != 0:
         return
     import oracle
-    import sprout_b200 as sb
 
     if not oracle.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_cast not built"}))
         return
-    pos, idx = sb.sphere_mesh(args.mesh_n, 0.1, SEED)
-    rays = sb.random_rays(args.rays, seed=SEED)
+    pos, idx = oracle.synth_sphere_mesh(args.mesh_n, 0.1, SEED)
+    rays = oracle.synth_rays(args.rays, seed=SEED)
     with tempfile.TemporaryDirectory() as tmp:
         mesh_path, rays_path = write_inputs(tmp, pos, idx, rays)
+        del rays
         timing = reference_run(mesh_path, rays_path, args.steps, args.warmup)
     times = timing["hit_s_list"][args.warmup:]
     total = sum(times)
@@ -244,12 +291,12 @@ def run_reference_arm(args, world, rank):
         "n_gpus": world, "steps": len(times), "warmup": args.warmup,
         "ms_per_step": round(1e3 * total / len(times), 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "rays_per_step": args.rays, "triangles": int(idx.shape[0]),
-                   "l2": "inputs (rays, 512 MiB) larger than L2"},
+        "config": workload_config(args.rays, int(idx.shape[0]), world),
         "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": timing["threads"],
                          "kind": "reference", "cpu": cpu_lscpu(),
                          "sample": f"full workload ({args.rays} rays) per step, reference Builder_SAH(16,64,4) "
-                                   f"tree (build {timing['build_s']:.3f} s, untimed) + Tree::intersect"},
+                                   f"tree (build {timing['build_s']:.3f} s, untimed) + Tree::intersect; inputs "
+                                   f"from the oracle's restatement of the benchmark synthesis"},
         "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -334,6 +381,12 @@ def main():
     assert tree.status() == 0
 
     hit_fraction = float((d_ids != -1).float().mean().item())
+    gpu_ids = d_ids.cpu().numpy().view(np.uint32)
+    gpu_t = d_t.cpu().numpy()
+
+    # Work per ray (untimed counting pass) and the L2-resident copy bandwidth it is held against.
+    steps_count = tree.traversal_stats(d_rays)
+    l2_peak = l2_copy_bandwidth(torch)
 
     # any-hit throughput (reported beside the headline)
     d_occ = torch.empty(args.rays, dtype=torch.uint8, device="cuda")
@@ -374,19 +427,29 @@ def main():
     achieved = ALGO_BYTES_PER_RAY * args.rays / mean_kernel_s / 1e9
     traffic_per_ray = profiled_traffic()
 
+    fetched_per_ray = (80.0 * steps_count["node_steps"] + 48.0 * steps_count["triangle_steps"]) / args.rays
+    l2_achieved = fetched_per_ray * args.rays / mean_kernel_s / 1e9
+
     cpu_baseline = None
+    id_parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
 
         if oracle.reference_available():
             with tempfile.TemporaryDirectory() as tmp:
                 mesh_path, rays_path = write_inputs(tmp, pos, idx, rays_host)
-                timing = reference_run(mesh_path, rays_path, 2, 1)
+                timing, ref_ids, ref_t = reference_run(mesh_path, rays_path, 2, 1, num_rays=args.rays)
             t_cpu = statistics.mean(timing["hit_s_list"][1:])
             cpu_baseline = {"value": round(args.rays / t_cpu / 1e6, 3), "unit": "Mrays/s",
                             "cores": timing["threads"], "kind": "reference", "cpu": cpu_lscpu(),
                             "sample": f"full workload ({args.rays} rays), reference Builder_SAH(16,64,4) + "
-                                      f"Tree::intersect on all host threads, mean of 2 passes"}
+                                      f"Tree::intersect on all host threads, mean of 2 passes (tree build "
+                                      f"{timing['build_s']:.3f} s excluded)"}
+            # Every ray of the timed cast against the reference's own answer for it.
+            id_parity = oracle.id_parity(pos, idx, rays_host, ref_ids, ref_t, gpu_ids, gpu_t)
+            id_parity["against"] = ("reference Builder_SAH(16,64,4) + Tree::intersect (oracle/_ref/ref_cast), "
+                                    "every ray of the timed step")
+            id_parity["explained_fraction"] = round(id_parity["explained_edge_tie"] / args.rays, 9)
 
     render = None
     if rank == 0 and not args.no_render:
@@ -398,18 +461,27 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * elapsed / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "rays_per_step_per_gpu": args.rays,
-                       "triangles": info["num_triangles"], "bvh_nodes": info["num_nodes"],
-                       "bvh_depth": info["max_depth"], "build_s": round(info["build_seconds"], 3),
-                       "parallelism": f"replicas x{world} (independent ray ranges)",
-                       "l2": "inputs (rays, 512 MiB) larger than L2; no flush",
-                       "hit_fraction": round(hit_fraction, 5)},
+            "config": workload_config(args.rays, info["num_triangles"], world),
+            "tree": {"bvh_nodes": info["num_nodes"], "bvh_depth": info["max_depth"],
+                     "build_s": round(info["build_seconds"], 3), "hit_fraction": round(hit_fraction, 5)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 5), "peak_kind": peak_kind,
                          "algorithmic_bytes_per_ray": ALGO_BYTES_PER_RAY,
                          "kernel_ms_mean": round(1e3 * mean_kernel_s, 4),
                          "traffic": (round(traffic_per_ray * args.rays) if traffic_per_ray else None),
-                         "note": "traversal is L1/L2-latency bound; HBM carries only rays and results"},
+                         "note": "HBM carries only rays and results; the bound that matters is the "
+                                 "node and triangle fetch below",
+                         "l2": {"bound": "l2", "unit": "GB/s",
+                                "achieved": round(l2_achieved, 1), "peak": round(l2_peak, 1),
+                                "frac": round(l2_achieved / l2_peak, 4),
+                                "peak_kind": "measured in this run: L2-resident copy bandwidth (torch copy_ "
+                                             "of 2 x 32 MiB, graph-replayed, read + write bytes)",
+                                "fetched_bytes_per_ray": round(fetched_per_ray, 2),
+                                "nodes_per_ray": round(steps_count["node_steps"] / args.rays, 4),
+                                "triangles_per_ray": round(steps_count["triangle_steps"] / args.rays, 4),
+                                "bytes": "80 B per 8-wide node visited + 48 B per triangle tested, "
+                                         "counted by spb_cast_stats_device over the same rays"}},
+            "id_parity": id_parity,
             "any_hit_mrays_s": round(world * any_hit_mrays, 3),
             "render": render,
             "e2e": e2e,

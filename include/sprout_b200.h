@@ -117,9 +117,23 @@ SPB_API int32_t spb_intersect_p_host(spb_tree* tree, float const* rays, uint64_t
                                      uint8_t* occluded);
 
 /*
- * Device-side status of the last cast on this tree: number of rays whose traversal
- * stack would have overflowed (always 0 for trees this library builds; the kernel checks
- * and drops such rays instead of writing out of bounds).  Synchronizes the tree's stream.
+ * Closest hit (device pointers, as spb_intersect_device) that also counts the traversal's
+ * work: node_steps receives the 8-wide nodes visited and triangle_steps the triangles tested,
+ * summed over all rays of the batch.  Synchronizes the stream before returning the counts.
+ * For measurement (bytes fetched per ray: nodes x 80 + triangles x 48); the counting costs
+ * a few percent, so timed casts use spb_intersect_device.  The reference counts nothing of
+ * the kind; its Tree::intersect (source/core/scene/shape/triangle/bvh/triangle_bvh_tree.cpp:41-90)
+ * visits nodes and tests triangles in the same sense.
+ */
+SPB_API int32_t spb_cast_stats_device(spb_tree* tree, float const* rays, uint64_t num_rays,
+                                      uint32_t* ids, float* ts, void* stream,
+                                      uint64_t* node_steps, uint64_t* triangle_steps);
+
+/*
+ * Device-side status of the casts on this tree: number of rays whose traversal stack would
+ * have overflowed, counted over every cast entry point since the tree was created (always 0
+ * for trees this library builds; the kernel checks and drops such rays as misses instead of
+ * writing out of bounds).  Synchronizes the device.
  */
 SPB_API int32_t spb_tree_status(spb_tree* tree, uint32_t* overflowed_rays);
 
@@ -155,9 +169,12 @@ SPB_API int32_t spb_synth_rays(uint64_t first, uint64_t count, uint32_t seed, fl
  * SPB_ERROR_ARGUMENT); the fixed array (SPB_STATIC_MAX_RAYS * 40 bytes + 256 bytes, about
  * 2.5 MiB) stays allocated on every GPU that loads the library until the process exits.
  * The first call on a device looks up the array's device address (once per device).
+ * The address is looked up again in a new CUDA context (after a cudaDeviceReset, say).
  * All calls share the one array, so calls that overlap on the GPU -- from several host
  * threads, or on several trees at once -- race and must be serialized by the caller.
- * Results are identical to spb_intersect_host.  Uses the legacy default stream and returns
+ * Results are identical to spb_intersect_host, and so is the error behaviour: rays that
+ * would overflow the traversal stack (none for trees this library builds) end as misses and
+ * are counted where spb_tree_status reports them.  Uses the legacy default stream and returns
  * when the results are in host memory.
  */
 #define SPB_STATIC_MAX_RAYS 65536ull

@@ -3,6 +3,10 @@
 * :func:`restated_cast` -- the C restatement in ``cast_oracle.c`` (libcast_oracle.so).
 * :func:`reference_cast` -- the reference's own Builder_SAH + Tree::intersect/intersect_p,
   compiled from the reference sources into ``_ref/ref_cast`` by ``Makefile``.
+* :func:`synth_sphere_mesh`, :func:`synth_rays` -- the cast benchmark's inputs, restated in C
+  (``synth_oracle.c``), so the reference can be timed without loading the product library.
+* :func:`classify_mismatches` -- sorts closest-hit disagreements into rounding-level
+  edge/tie cases and unexplained ones.
 
 Only tests, the smoke check and the bench's CPU-baseline leg use this package.
 """
@@ -41,6 +45,12 @@ def _load():
                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int32]
         lib.oracle_triangle_test.restype = ctypes.c_int32
         lib.oracle_triangle_test.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_float, ctypes.c_void_p]
+        lib.oracle_synth_sphere_mesh.restype = ctypes.c_int32
+        lib.oracle_synth_sphere_mesh.argtypes = [ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32,
+                                                 ctypes.c_void_p, ctypes.c_void_p]
+        lib.oracle_synth_rays.restype = ctypes.c_int32
+        lib.oracle_synth_rays.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_float,
+                                          ctypes.c_void_p, ctypes.c_uint32]
         _lib = lib
     return _lib
 
@@ -82,6 +92,25 @@ def restated_cast(positions, indices, rays, closest=True, any_hit=True, brute=Fa
     return out
 
 
+def synth_sphere_mesh(n: int, amplitude: float = 0.1, seed: int = 1):
+    """The cast benchmark's displaced tetra-sphere, restated in C (synth_oracle.c)."""
+    lib = _load()
+    pos = np.empty((2 * n * n + 2, 3), np.float32)
+    idx = np.empty((4 * n * n, 3), np.uint32)
+    if lib.oracle_synth_sphere_mesh(n, amplitude, seed, pos.ctypes.data, idx.ctypes.data) != 0:
+        raise ValueError("oracle_synth_sphere_mesh rejected its arguments")
+    return pos, idx
+
+
+def synth_rays(count: int, seed: int = 1, first: int = 0, extent: float = 2.0, threads: int = 0):
+    """The cast benchmark's rays, restated in C (synth_oracle.c): (count, 8) float32."""
+    lib = _load()
+    rays = np.empty((count, 8), np.float32)
+    if lib.oracle_synth_rays(first, count, seed, extent, rays.ctypes.data, threads or os.cpu_count() or 1) != 0:
+        raise ValueError("oracle_synth_rays rejected its arguments")
+    return rays
+
+
 def reference_available() -> bool:
     return REF_CAST.exists()
 
@@ -121,6 +150,61 @@ def reference_cast(positions, indices, rays, threads=0, mode="both", workdir=Non
     ts = raw[4 * n: 8 * n].view(np.float32)
     occ = raw[8 * n: 9 * n]
     return {"ids": ids.copy(), "t": ts.copy(), "occluded": occ.copy(), "timing": timing}
+
+
+MISS = 0xFFFFFFFF
+
+
+def classify_mismatches(positions, indices, rays, ids_a, t_a, ids_b, t_b, test=None):
+    """Splits the rays on which two closest-hit results disagree into those explained by
+    rounding at a triangle edge or an equal-t tie and the unexplained rest.  ``test(ray, a, b,
+    c)`` is the restated triangle test returning (pass, t, u, v) (default: :func:`triangle_test`).
+    Returns (explained, unexplained) lists of ray indices."""
+    test = test or triangle_test
+    pos = np.asarray(positions, np.float32)
+    idx = np.asarray(indices, np.uint32)
+    explained, unexplained = [], []
+    for i in np.nonzero(np.asarray(ids_a) != np.asarray(ids_b))[0]:
+        ray = rays[i]
+        ok = True
+        tvals = []
+        for tid in (ids_a[i], ids_b[i]):
+            if tid == MISS:
+                continue
+            a, b, c = pos[idx[tid, 0]], pos[idx[tid, 1]], pos[idx[tid, 2]]
+            _, t, u, v = test(ray, a, b, c)
+            margin = min(u, 1.0 - u, v, 1.0 - u - v)
+            if not np.isfinite(t) or margin < -1e-5:
+                ok = False
+            tvals.append(t)
+        if len(tvals) == 2 and abs(tvals[0] - tvals[1]) > 1e-5 * max(1.0, abs(tvals[0])):
+            ok = False
+        if len(tvals) == 1:
+            # one side missed: the other's hit must sit on an edge
+            tid = ids_a[i] if ids_a[i] != MISS else ids_b[i]
+            a, b, c = pos[idx[tid, 0]], pos[idx[tid, 1]], pos[idx[tid, 2]]
+            _, t, u, v = test(ray, a, b, c)
+            if min(abs(u), abs(1 - u), abs(v), abs(1 - u - v)) > 1e-5:
+                ok = False
+        (explained if ok else unexplained).append(int(i))
+    return explained, unexplained
+
+
+def id_parity(positions, indices, rays, ref_ids, ref_t, ids, t):
+    """Summary of a closest-hit result against the reference's on the same rays: mismatching
+    ids, split into edge/tie cases and unexplained ones, and the largest t difference in ulps
+    where the ids agree (on hits)."""
+    ref_ids = np.asarray(ref_ids, np.uint32)
+    ids = np.asarray(ids, np.uint32)
+    explained, unexplained = classify_mismatches(positions, indices, rays, ref_ids, ref_t, ids, t)
+    same = (ref_ids == ids) & (ids != MISS)
+    ulps = np.abs(np.asarray(ref_t, np.float32)[same].view(np.int32).astype(np.int64)
+                  - np.asarray(t, np.float32)[same].view(np.int32).astype(np.int64))
+    return {"rays": int(ids.size), "hits": int((ids != MISS).sum()),
+            "mismatches": len(explained) + len(unexplained),
+            "explained_edge_tie": len(explained), "unexplained": len(unexplained),
+            "unexplained_rays": unexplained[:16],
+            "t_max_ulp_on_equal_ids": int(ulps.max()) if ulps.size else 0}
 
 
 # ---- renderer oracle: the reference's C API in its own process ----------------------------

@@ -76,6 +76,8 @@ PROTOTYPES = {
     "spb_guide_forward": (c_i32, [c_vp, c_vp, ctypes.c_uint64, c_vp]),
     "spb_guide_gradients": (c_i32, [c_vp, c_vp, c_vp, c_vp, ctypes.c_uint64, c_vp]),
     "spb_intersect_host_static": (c_i32, [c_vp, c_vp, c_u64, c_vp, c_vp]),
+    "spb_cast_stats_device": (c_i32, [c_vp, c_vp, c_u64, c_vp, c_vp, c_vp, ctypes.POINTER(c_u64),
+                                      ctypes.POINTER(c_u64)]),
 }
 
 _lib = None

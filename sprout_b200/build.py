@@ -72,9 +72,9 @@ def build_library(force: bool = False, verbose: bool = False, ptxas_info: bool =
 
 def build_oracle(force: bool = False, verbose: bool = False) -> pathlib.Path:
     """Compile the CPU restatement; also the reference build when its sources are here."""
-    src = ORACLE / "cast_oracle.c"
-    if force or _stale(ORACLE_LIB, [src]):
-        cmd = ["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-pthread", str(src),
+    srcs = [ORACLE / "cast_oracle.c", ORACLE / "synth_oracle.c"]
+    if force or _stale(ORACLE_LIB, srcs):
+        cmd = ["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-pthread"] + [str(s) for s in srcs] + [
                "-o", str(ORACLE_LIB), "-lm"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:

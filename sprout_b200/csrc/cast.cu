@@ -6,6 +6,7 @@
 //    with one atomicAdd on the launch's work counter, so lanes stay busy although ray costs
 //    differ by orders of magnitude (most rays of the benchmark leave the root box at once).
 //  * Traversal, triangle test and hit definition: traverse.cuh.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,12 +31,15 @@ constexpr uint32_t Full_mask        = 0xFFFFFFFFu;
 // entry points, slots 1 and 2 the two streams of the host pipeline.
 constexpr uint32_t Num_counter_slots = 3;
 
-template <bool Any_hit>
+// Stats: also count, per ray, the node and triangle steps of its traversal (summed per warp
+// into stats[0] and stats[1]); the counting variant is only launched by spb_cast_stats_device.
+template <bool Any_hit, bool Stats = false>
 __global__ void __launch_bounds__(Block)
     cast_kernel(uint4 const* __restrict__ nodes, float4 const* __restrict__ triangles,
                 float4 const* __restrict__ rays, uint32_t num_rays, uint32_t* __restrict__ ids,
                 float* __restrict__ ts, float2* __restrict__ uvs, uint8_t* __restrict__ occluded,
-                uint32_t* __restrict__ counters, float hit_margin) {
+                uint32_t* __restrict__ work, uint32_t* __restrict__ overflow, float hit_margin,
+                unsigned long long* __restrict__ stats) {
     uint32_t const lane = threadIdx.x & 31u;
     uint32_t const lt   = (1u << lane) - 1u;
 
@@ -45,6 +49,8 @@ __global__ void __launch_bounds__(Block)
     uint32_t       ray       = 0;
     bool           active    = false;
     bool           exhausted = false;
+    uint32_t       node_steps = 0;
+    uint32_t       tri_steps  = 0;
 
     while (true) {
         uint32_t const idle = __ballot_sync(Full_mask, !active);
@@ -56,7 +62,7 @@ __global__ void __launch_bounds__(Block)
             uint32_t const leader = __ffs(idle) - 1;
             uint32_t       base   = 0;
             if (lane == leader) {
-                base = atomicAdd(counters, count);
+                base = atomicAdd(work, count);
             }
             base = __shfl_sync(Full_mask, base, leader);
             if (uint64_t(base) + count >= num_rays) {
@@ -66,8 +72,10 @@ __global__ void __launch_bounds__(Block)
                 uint32_t const mine = base + __popc(idle & lt);
                 if (mine < num_rays) {
                     ray = mine;
-                    gpu::start_ray(r, tv, __ldg(rays + 2 * size_t(mine)),
-                                   __ldg(rays + 2 * size_t(mine) + 1));
+                    // Rays are read once: evict-first loads keep them from displacing the
+                    // tree's nodes and triangles in L2.
+                    gpu::start_ray(r, tv, __ldcs(rays + 2 * size_t(mine)),
+                                   __ldcs(rays + 2 * size_t(mine) + 1));
                     active = true;
                 }
             }
@@ -77,17 +85,36 @@ __global__ void __launch_bounds__(Block)
             continue;
         }
 
-        if (gpu::traversal_step<Any_hit>(r, tv, stack, nodes, triangles, hit_margin, counters + 1)) {
+        if constexpr (Stats) {
+            if (tv.tri_group.y != 0) {
+                ++tri_steps;
+            } else if ((tv.group.y & 0xFF000000u) || tv.sp > 0) {
+                ++node_steps;
+            }
+        }
+        if (gpu::traversal_step<Any_hit>(r, tv, stack, nodes, triangles, hit_margin, overflow)) {
             if (Any_hit) {
-                occluded[ray] = r.best_id != gpu::Miss ? 1 : 0;
+                __stcs(occluded + ray, uint8_t(r.best_id != gpu::Miss ? 1 : 0));
             } else {
-                ids[ray] = r.best_id;
-                ts[ray]  = r.tbest;
+                __stcs(ids + ray, r.best_id);
+                __stcs(ts + ray, r.tbest);
                 if (uvs) {
-                    uvs[ray] = make_float2(r.u, r.v);
+                    __stcs(uvs + ray, make_float2(r.u, r.v));
                 }
             }
             active = false;
+        }
+    }
+    if constexpr (Stats) {
+        unsigned long long n = node_steps;
+        unsigned long long t = tri_steps;
+        for (int o = 16; o > 0; o >>= 1) {
+            n += __shfl_down_sync(Full_mask, n, o);
+            t += __shfl_down_sync(Full_mask, t, o);
+        }
+        if (lane == 0) {
+            atomicAdd(stats + 0, n);
+            atomicAdd(stats + 1, t);
         }
     }
 }
@@ -114,6 +141,7 @@ struct spb_tree {
     uint4*        d_nodes    = nullptr;
     float4*       d_tris     = nullptr;
     uint32_t*     d_counters = nullptr;
+    unsigned long long* d_stats = nullptr;  // node steps, triangle steps (spb_cast_stats_device)
     bool          built      = false;
     float         hit_margin = 0.f;
     spb_tree_info info{};
@@ -196,11 +224,11 @@ int32_t launch(spb_tree* tree, bool any_hit, uint32_t slot, float4 const* rays, 
     if (any_hit) {
         cast_kernel<true><<<grid, Block, 0, stream>>>(
             reinterpret_cast<uint4 const*>(tree->d_nodes), tree->d_tris, rays, n, nullptr,
-            nullptr, nullptr, occ, counters, tree->hit_margin);
+            nullptr, nullptr, occ, counters, counters + 1, tree->hit_margin, nullptr);
     } else {
         cast_kernel<false><<<grid, Block, 0, stream>>>(
             reinterpret_cast<uint4 const*>(tree->d_nodes), tree->d_tris, rays, n, ids, ts, uvs,
-            nullptr, counters, tree->hit_margin);
+            nullptr, counters, counters + 1, tree->hit_margin, nullptr);
     }
     SPB_CUDA(cudaGetLastError());
     return SPB_OK;
@@ -243,7 +271,11 @@ extern "C" SPB_API int32_t spb_tree_create(spb_tree** out) {
     if (e == cudaSuccess) {
         e = cudaMemset(tree->d_counters, 0, 2 * Num_counter_slots * sizeof(uint32_t));
     }
+    if (e == cudaSuccess) {
+        e = cudaMalloc(&tree->d_stats, 2 * sizeof(unsigned long long));
+    }
     if (e != cudaSuccess) {
+        cudaFree(tree->d_stats);
         cudaFree(tree->d_counters);
         delete tree;
         return cuda_fail(e, "spb_tree_create");
@@ -265,6 +297,7 @@ extern "C" SPB_API int32_t spb_tree_release(spb_tree* tree) {
         release_device(tree);
         free_pipeline(tree->pipe);
         cudaFree(tree->d_counters);
+        cudaFree(tree->d_stats);
     }
     delete tree;
     return SPB_OK;
@@ -377,6 +410,44 @@ extern "C" SPB_API int32_t spb_intersect_p_device(spb_tree* tree, float const* r
                   nullptr, nullptr, nullptr, occluded, tree->last_stream);
 }
 
+extern "C" SPB_API int32_t spb_cast_stats_device(spb_tree* tree, float const* rays,
+                                                 uint64_t num_rays, uint32_t* ids, float* ts,
+                                                 void* stream, uint64_t* node_steps,
+                                                 uint64_t* triangle_steps) {
+    spb::clear_error();
+    if (int32_t const s = check_cast(tree, rays, num_rays, ids && ts && node_steps && triangle_steps,
+                                     "spb_cast_stats_device")) {
+        return s;
+    }
+    if (!node_steps || !triangle_steps) {
+        return spb::fail(SPB_ERROR_ARGUMENT, "spb_cast_stats_device: null counter");
+    }
+    *node_steps     = 0;
+    *triangle_steps = 0;
+    if (num_rays == 0) {
+        return SPB_OK;
+    }
+    Device_scope       scope(tree->device);
+    cudaStream_t const st = static_cast<cudaStream_t>(stream);
+    tree->last_stream     = st;
+    uint32_t* counters    = tree->d_counters;
+    SPB_CUDA(cudaMemsetAsync(counters, 0, sizeof(uint32_t), st));
+    SPB_CUDA(cudaMemsetAsync(tree->d_stats, 0, 2 * sizeof(unsigned long long), st));
+    uint32_t const n    = uint32_t(num_rays);
+    int const      grid = std::max(1, std::min(tree->grid_hit, int((uint64_t(n) + Block - 1) / Block)));
+    cast_kernel<false, true><<<grid, Block, 0, st>>>(
+        reinterpret_cast<uint4 const*>(tree->d_nodes), tree->d_tris,
+        reinterpret_cast<float4 const*>(rays), n, ids, ts, nullptr, nullptr, counters,
+        counters + 1, tree->hit_margin, tree->d_stats);
+    SPB_CUDA(cudaGetLastError());
+    unsigned long long host[2] = {0, 0};
+    SPB_CUDA(cudaMemcpyAsync(host, tree->d_stats, sizeof(host), cudaMemcpyDeviceToHost, st));
+    SPB_CUDA(cudaStreamSynchronize(st));
+    *node_steps     = host[0];
+    *triangle_steps = host[1];
+    return SPB_OK;
+}
+
 namespace {
 
 int32_t cast_host(spb_tree* tree, bool any_hit, float const* rays, uint64_t n, uint32_t* ids,
@@ -469,32 +540,71 @@ extern "C" SPB_API int32_t spb_tree_status(spb_tree* tree, uint32_t* overflowed_
 namespace {
 
 constexpr uint64_t Static_max_rays      = SPB_STATIC_MAX_RAYS;
-constexpr size_t   Static_counter_bytes = 256;  // work counter + overflow counter, padded
+constexpr size_t   Static_counter_bytes = 256;  // work counter, padded
 constexpr size_t   Static_scratch_bytes = Static_counter_bytes + Static_max_rays * (32 + 4 + 4);
 constexpr int      Static_max_devices   = 64;
 
 __device__ __align__(256) unsigned char g_static_scratch[Static_scratch_bytes];
 
-std::mutex     g_static_mutex;
-unsigned char* g_static_address[Static_max_devices] = {};
+// The array's device address per device, with the id of the CUDA context it was looked up in:
+// a context created after a cudaDeviceReset may place the array elsewhere, so the address is
+// looked up again whenever the current context's id differs from the cached one.
+struct Static_address {
+    unsigned char*     address    = nullptr;
+    unsigned long long context_id = 0;
+};
 
-// Device address of g_static_scratch on the current device (set up once per device; the
-// host-side symbol g_static_scratch itself is not a device address).
+std::mutex     g_static_mutex;
+Static_address g_static_address[Static_max_devices];
+
+using Ctx_get_current = CUresult(CUDAAPI*)(CUcontext*);
+using Ctx_get_id      = CUresult(CUDAAPI*)(CUcontext, unsigned long long*);
+
+// Id of the calling thread's current context (0 if the driver cannot tell, in which case the
+// address is looked up on every call).
+unsigned long long current_context_id() {
+    static Ctx_get_current get_current = nullptr;
+    static Ctx_get_id      get_id      = nullptr;
+    static bool const      resolved    = [] {
+        void* a = nullptr;
+        void* b = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault) == cudaSuccess) {
+            get_current = reinterpret_cast<Ctx_get_current>(a);
+            get_id      = reinterpret_cast<Ctx_get_id>(b);
+        }
+        return true;
+    }();
+    (void)resolved;
+    CUcontext          ctx = nullptr;
+    unsigned long long id  = 0;
+    if (get_current && get_id && get_current(&ctx) == CUDA_SUCCESS && ctx &&
+        get_id(ctx, &id) == CUDA_SUCCESS) {
+        return id;
+    }
+    return 0;
+}
+
+// Device address of g_static_scratch on the current device, looked up once per device and
+// context (the host-side symbol g_static_scratch itself is not a device address).
 int32_t static_scratch(int device, unsigned char** out) {
     if (device < 0 || device >= Static_max_devices) {
         return spb::fail(SPB_ERROR_STATE, "spb_intersect_host_static: device %d not supported",
                          device);
     }
+    unsigned long long const    context = current_context_id();
     std::lock_guard<std::mutex> lock(g_static_mutex);
-    if (!g_static_address[device]) {
+    Static_address&             cached = g_static_address[device];
+    if (!cached.address || context == 0 || cached.context_id != context) {
         void*             ptr = nullptr;
         cudaError_t const e   = cudaGetSymbolAddress(&ptr, g_static_scratch);
         if (e != cudaSuccess) {
             return cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
         }
-        g_static_address[device] = static_cast<unsigned char*>(ptr);
+        cached.address    = static_cast<unsigned char*>(ptr);
+        cached.context_id = context;
     }
-    *out = g_static_address[device];
+    *out = cached.address;
     return SPB_OK;
 }
 
@@ -522,29 +632,25 @@ extern "C" SPB_API int32_t spb_intersect_host_static(spb_tree* tree, float const
     if (int32_t const s = static_scratch(tree->device, &base)) {
         return s;
     }
-    auto* counters = reinterpret_cast<uint32_t*>(base);
-    auto* d_rays   = reinterpret_cast<float4*>(base + Static_counter_bytes);
-    auto* d_ids    = reinterpret_cast<uint32_t*>(base + Static_counter_bytes + Static_max_rays * 32);
-    auto* d_ts     = reinterpret_cast<float*>(base + Static_counter_bytes + Static_max_rays * 36);
+    auto* work   = reinterpret_cast<uint32_t*>(base);
+    auto* d_rays = reinterpret_cast<float4*>(base + Static_counter_bytes);
+    auto* d_ids  = reinterpret_cast<uint32_t*>(base + Static_counter_bytes + Static_max_rays * 32);
+    auto* d_ts   = reinterpret_cast<float*>(base + Static_counter_bytes + Static_max_rays * 36);
     uint32_t const n = uint32_t(num_rays);
 
-    // The array keeps the previous call's contents: both counters must start at zero.
-    SPB_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(uint32_t), nullptr));
+    // The array keeps the previous call's contents: the work counter must start at zero.
+    // Stack overflows (none for trees this library builds) are counted in the tree's own
+    // counter, as spb_intersect_host counts them, and reported by spb_tree_status.
+    SPB_CUDA(cudaMemsetAsync(work, 0, sizeof(uint32_t), nullptr));
     SPB_CUDA(cudaMemcpyAsync(d_rays, rays, size_t(n) * 32, cudaMemcpyHostToDevice, nullptr));
     int const grid = std::max(1, std::min(tree->grid_hit, int((n + Block - 1) / Block)));
     cast_kernel<false><<<grid, Block, 0, nullptr>>>(reinterpret_cast<uint4 const*>(tree->d_nodes),
                                                     tree->d_tris, d_rays, n, d_ids, d_ts, nullptr,
-                                                    nullptr, counters, tree->hit_margin);
+                                                    nullptr, work, tree->d_counters + 1,
+                                                    tree->hit_margin, nullptr);
     SPB_CUDA(cudaGetLastError());
     SPB_CUDA(cudaMemcpyAsync(ids, d_ids, size_t(n) * 4, cudaMemcpyDeviceToHost, nullptr));
     SPB_CUDA(cudaMemcpyAsync(ts, d_ts, size_t(n) * 4, cudaMemcpyDeviceToHost, nullptr));
-    uint32_t overflow = 0;
-    SPB_CUDA(cudaMemcpyAsync(&overflow, counters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                             nullptr));
     SPB_CUDA(cudaStreamSynchronize(nullptr));
-    if (overflow != 0) {
-        return spb::fail(SPB_ERROR_STATE, "spb_intersect_host_static: %u rays overflowed the stack",
-                         overflow);
-    }
     return SPB_OK;
 }

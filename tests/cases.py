@@ -52,32 +52,7 @@ def edge_rays(positions, indices):
 
 def classify_mismatches(positions, indices, rays, ids_a, t_a, ids_b, t_b, test):
     """Counts disagreements between two closest-hit results that are NOT explained by
-    rounding at a triangle edge or an equal-t tie.  ``test(ray, a, b, c)`` is the restated
-    triangle test returning (pass, t, u, v).  Returns (explained, unexplained) index lists."""
-    pos = np.asarray(positions, np.float32)
-    idx = np.asarray(indices, np.uint32)
-    explained, unexplained = [], []
-    for i in np.nonzero(ids_a != ids_b)[0]:
-        ray = rays[i]
-        ok = True
-        tvals = []
-        for tid in (ids_a[i], ids_b[i]):
-            if tid == MISS:
-                continue
-            a, b, c = pos[idx[tid, 0]], pos[idx[tid, 1]], pos[idx[tid, 2]]
-            _, t, u, v = test(ray, a, b, c)
-            margin = min(u, 1.0 - u, v, 1.0 - u - v)
-            if not np.isfinite(t) or margin < -1e-5:
-                ok = False
-            tvals.append(t)
-        if len(tvals) == 2 and abs(tvals[0] - tvals[1]) > 1e-5 * max(1.0, abs(tvals[0])):
-            ok = False
-        if len(tvals) == 1:
-            # one side missed: the other's hit must sit on an edge
-            tid = ids_a[i] if ids_a[i] != MISS else ids_b[i]
-            a, b, c = pos[idx[tid, 0]], pos[idx[tid, 1]], pos[idx[tid, 2]]
-            _, t, u, v = test(ray, a, b, c)
-            if min(abs(u), abs(1 - u), abs(v), abs(1 - u - v)) > 1e-5:
-                ok = False
-        (explained if ok else unexplained).append(int(i))
-    return explained, unexplained
+    rounding at a triangle edge or an equal-t tie (the checker lives in the oracle package)."""
+    import oracle
+
+    return oracle.classify_mismatches(positions, indices, rays, ids_a, t_a, ids_b, t_b, test)

@@ -137,6 +137,32 @@ def test_benchmark_size_properties(torch_cuda):
     assert np.array_equal(occ[sample], want["occluded"])
 
 
+def test_benchmark_ids_against_the_reference_at_full_size(torch_cuda):
+    """The benchmark's own workload (1,048,576 triangles, all 16,777,216 rays): every closest
+    hit of the GPU cast against the compiled reference's Builder_SAH(16,64,4) + Tree::intersect.
+    Disagreements must all be rounding-level edge/tie cases (the reference's rcpss reciprocal
+    and last-tested tie rule), at most 1e-4 of the rays; t within 2 ulp where the ids agree."""
+    if not oracle.reference_available():
+        pytest.skip("oracle/_ref/ref_cast not built")
+    torch = torch_cuda
+    pos, idx = sb.sphere_mesh(512, 0.1, 1)
+    n = 1 << 24
+    rays = sb.random_rays(n, seed=1)
+    with sb.Tree() as tree:
+        tree.build(pos, idx)
+        ids, t = tree.intersect(torch.from_numpy(rays).cuda())
+        torch.cuda.synchronize()
+        assert tree.status() == 0
+    ids = ids.cpu().numpy().view(np.uint32)
+    t = t.cpu().numpy()
+    ref = oracle.reference_cast(pos, idx, rays, mode="hit")
+    summary = oracle.id_parity(pos, idx, rays, ref["ids"], ref["t"], ids, t)
+    print("full-size id parity against the reference:", summary)
+    assert summary["unexplained"] == 0, summary
+    assert summary["explained_edge_tie"] <= 1e-4 * n
+    assert summary["t_max_ulp_on_equal_ids"] <= 2
+
+
 def test_empty_batch_and_state_errors():
     pos, idx = sb.sphere_mesh(4, 0.1, 1)
     with sb.Tree() as tree:

@@ -125,3 +125,21 @@ def test_tree_independence_on_degenerate_mesh():
     assert np.array_equal(a["ids"], b["ids"])
     assert np.array_equal(a["t"].view(np.uint32), b["t"].view(np.uint32))
     assert np.array_equal(a["occluded"], b["occluded"])
+
+
+@pytest.mark.parametrize("n", [1, 7, 64, 512])
+def test_synthesis_restatement_matches_the_product(n):
+    """The bench's reference arm makes the benchmark mesh and rays with the oracle's C
+    restatement (so that it loads no product code); both must be the product's bit for bit."""
+    want_pos, want_idx = sb.sphere_mesh(n, 0.1, 1)
+    pos, idx = oracle.synth_sphere_mesh(n, 0.1, 1)
+    assert np.array_equal(idx, want_idx)
+    assert np.array_equal(pos.view(np.uint32), want_pos.view(np.uint32))
+
+
+@pytest.mark.parametrize("first,count,seed,extent", [(0, 200000, 1, 2.0), ((1 << 24) - 5000, 10000, 1, 2.0),
+                                                     (12345, 3000, 9, 3.0)])
+def test_ray_synthesis_restatement_matches_the_product(first, count, seed, extent):
+    want = sb.random_rays(count, seed=seed, first=first, extent=extent)
+    got = oracle.synth_rays(count, seed=seed, first=first, extent=extent)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
