@@ -200,11 +200,13 @@ def id_parity(positions, indices, rays, ref_ids, ref_t, ids, t):
     same = (ref_ids == ids) & (ids != MISS)
     ulps = np.abs(np.asarray(ref_t, np.float32)[same].view(np.int32).astype(np.int64)
                   - np.asarray(t, np.float32)[same].view(np.int32).astype(np.int64))
+    hist = np.bincount(np.minimum(ulps, 4), minlength=5) if ulps.size else np.zeros(5, np.int64)
     return {"rays": int(ids.size), "hits": int((ids != MISS).sum()),
             "mismatches": len(explained) + len(unexplained),
             "explained_edge_tie": len(explained), "unexplained": len(unexplained),
             "unexplained_rays": unexplained[:16],
-            "t_max_ulp_on_equal_ids": int(ulps.max()) if ulps.size else 0}
+            "t_max_ulp_on_equal_ids": int(ulps.max()) if ulps.size else 0,
+            "t_ulp_histogram_0_1_2_3_4plus": [int(x) for x in hist]}
 
 
 # ---- renderer oracle: the reference's C API in its own process ----------------------------
@@ -295,15 +297,17 @@ class ScriptRecorder:
         return 0
 
 
-def reference_render(build_scene, width, height, iterations, progressive=True, workdir=None):
+def reference_render(build_scene, width, height, iterations, progressive=True, workdir=None, prepare=False):
     """Renders with the compiled reference: build_scene(recorder) issues the scene's calls.
-    Returns (rgb image (H, W, 3) float32, timing dict)."""
+    With prepare (batch mode), su_start_render_frame runs first and is timed apart
+    (timing["prepare_s"]): it joins the asynchronous mesh BVH builds and compiles the scene, so
+    timing["render_s"] covers the frame itself.  Returns (rgb image (H, W, 3) float32, timing)."""
     if not REF_RENDER.exists():
         raise FileNotFoundError(f"{REF_RENDER} missing: build it with `make -C oracle`")
     rec = ScriptRecorder()
     build_scene(rec)
     head = [f"init {1 if progressive else 0}"]
-    tail = [f"progressive {iterations}"] if progressive else ["frame 0"]
+    tail = [f"progressive {iterations}"] if progressive else (["prepare", "frame 0"] if prepare else ["frame 0"])
     with tempfile.TemporaryDirectory(dir=workdir) as tmp:
         sp, dp, op = (os.path.join(tmp, n) for n in ("script.txt", "data.bin", "out.bin"))
         with open(sp, "w") as f:

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <deque>
@@ -75,6 +76,14 @@ struct Binary_node {
 constexpr uint32_t Num_bins             = 32;
 constexpr uint32_t Parallel_threshold   = 1u << 15;
 constexpr uint32_t Max_leaf_triangles   = 3;
+// The collapse does not open a child holding at most Keep_leaf triangles: it stays one leaf
+// slot of up to Keep_leaf triangles (0: every binary child with more than one triangle can be
+// opened to fill the node).
+#ifndef SPB_BVH_KEEP_LEAF
+#define SPB_BVH_KEEP_LEAF 0
+#endif
+constexpr uint32_t Keep_leaf = SPB_BVH_KEEP_LEAF;
+static_assert(Keep_leaf <= Max_leaf_triangles, "a kept leaf must fit one slot");
 
 class Binary_builder {
   public:
@@ -295,6 +304,10 @@ float round_down(double x) {
 
 }  // namespace
 
+double scene_box_pad(double extent, double magnitude) {
+    return std::max(std::ldexp(std::max(extent, magnitude), -10), double(FLT_MIN));
+}
+
 float hit_margin_for(double extent, double magnitude) {
     float const m = float(std::ldexp(std::max(extent, magnitude), -17));
     return m > std::numeric_limits<float>::min() ? m : std::numeric_limits<float>::min();
@@ -358,6 +371,11 @@ bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* 
     // leaves hit_margin of room for the rounding of the traversal's slab arithmetic.
     out.hit_margin   = hit_margin_for(extent, magnitude);
     double const pad = 2.0 * double(out.hit_margin);
+    double const scene_pad = scene_box_pad(extent, magnitude);
+    for (int a = 0; a < 3; ++a) {
+        out.scene_lo[a] = std::nextafter(float(double(root_box.lo[a]) - scene_pad), -INFINITY);
+        out.scene_hi[a] = std::nextafter(float(double(root_box.hi[a]) + scene_pad), INFINITY);
+    }
 
     double const root_area = std::max(double(root_box.area()), 1e-30);
 
@@ -405,7 +423,7 @@ bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* 
                 float best_area = -1.f;
                 for (size_t i = 0; i < kids.size(); ++i) {
                     Binary_node const& k = bnodes[kids[i]];
-                    if (k.leaf) {
+                    if (k.leaf || k.count <= Keep_leaf) {
                         continue;
                     }
                     float const a = k.box.area();

@@ -51,7 +51,16 @@ struct Wide_bvh {
     uint32_t                   max_depth  = 0;
     double                     sah_cost   = 0.;
     float                      hit_margin = 0.f;  // see hit_margin_for
+    // Bounds of all triangles widened by 2^-10 of the scene size (rounded outward): a ray that
+    // misses this box cannot hit a triangle (scene_box_pad).
+    float                      scene_lo[3] = {0.f, 0.f, 0.f};
+    float                      scene_hi[3] = {0.f, 0.f, 0.f};
 };
+
+// Padding of the scene box a ray is first tested against: 2^-10 * max(scene extent, largest
+// coordinate magnitude), 128 times the hit margin, so that no ray whose hit point the
+// traversal accepts (within the hit margin of a triangle) falls outside it.
+double scene_box_pad(double extent, double magnitude);
 
 // Margin around a triangle's bounds within which a hit point must lie:
 // 2^-17 * max(scene extent, largest coordinate magnitude), at least FLT_MIN.  extent and

@@ -4,7 +4,12 @@
 //  * Persistent warps with dynamic ray fetch: each warp keeps 32 rays in flight; whenever
 //    at least Refill_threshold lanes have finished, the warp takes that many new ray indices
 //    with one atomicAdd on the launch's work counter, so lanes stay busy although ray costs
-//    differ by orders of magnitude (most rays of the benchmark leave the root box at once).
+//    differ by orders of magnitude.
+//  * A fetched ray is first tested against the tree's padded scene box (gpu::enters_box, in
+//    double precision); one that misses it (72 % of the benchmark's rays) is answered as a
+//    miss at once, without the 8-child test of the root node.
+//  * Rays are loaded with evict-first hints and results stored with streaming stores, so the
+//    512 MiB of benchmark rays do not push the tree (63 MiB) out of L2.
 //  * Traversal, triangle test and hit definition: traverse.cuh.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -23,8 +28,23 @@ namespace {
 
 using namespace spb;
 
+// Launch shape: 128-thread blocks, registers bounded so that SPB_CAST_MIN_BLOCKS blocks fit on
+// an SM (9: 56 registers, 36 warps; measured 3 % faster than the unbounded 64 registers and
+// 6 % faster than 48 registers at 10 blocks); a warp refills once Refill_threshold of its lanes
+// are idle (8 measured best against 4, 12 and 16).
+#ifndef SPB_CAST_REFILL
+#define SPB_CAST_REFILL 8
+#endif
+#ifndef SPB_CAST_MIN_BLOCKS
+#define SPB_CAST_MIN_BLOCKS 9
+#endif
 constexpr int      Block            = 128;
-constexpr uint32_t Refill_threshold = 8;
+constexpr uint32_t Refill_threshold = SPB_CAST_REFILL;
+#if SPB_CAST_MIN_BLOCKS > 0
+#define SPB_CAST_BOUNDS __launch_bounds__(Block, SPB_CAST_MIN_BLOCKS)
+#else
+#define SPB_CAST_BOUNDS __launch_bounds__(Block)
+#endif
 constexpr uint32_t Full_mask        = 0xFFFFFFFFu;
 
 // Counter slots (2 words each: work counter, overflow count).  Slot 0 serves the device
@@ -34,12 +54,12 @@ constexpr uint32_t Num_counter_slots = 3;
 // Stats: also count, per ray, the node and triangle steps of its traversal (summed per warp
 // into stats[0] and stats[1]); the counting variant is only launched by spb_cast_stats_device.
 template <bool Any_hit, bool Stats = false>
-__global__ void __launch_bounds__(Block)
+__global__ void SPB_CAST_BOUNDS
     cast_kernel(uint4 const* __restrict__ nodes, float4 const* __restrict__ triangles,
                 float4 const* __restrict__ rays, uint32_t num_rays, uint32_t* __restrict__ ids,
                 float* __restrict__ ts, float2* __restrict__ uvs, uint8_t* __restrict__ occluded,
                 uint32_t* __restrict__ work, uint32_t* __restrict__ overflow, float hit_margin,
-                unsigned long long* __restrict__ stats) {
+                float3 scene_lo, float3 scene_hi, unsigned long long* __restrict__ stats) {
     uint32_t const lane = threadIdx.x & 31u;
     uint32_t const lt   = (1u << lane) - 1u;
 
@@ -53,11 +73,13 @@ __global__ void __launch_bounds__(Block)
     uint32_t       tri_steps  = 0;
 
     while (true) {
-        uint32_t const idle = __ballot_sync(Full_mask, !active);
+        uint32_t idle = __ballot_sync(Full_mask, !active);
         if (exhausted && idle == Full_mask) {
             break;
         }
-        if (!exhausted && __popc(idle) >= int(Refill_threshold)) {
+        // Refill while enough lanes are idle.  A fetched ray that misses the scene box is
+        // answered at once (a miss) and its lane stays idle for the next round of the loop.
+        while (!exhausted && __popc(idle) >= int(Refill_threshold)) {
             uint32_t const count  = __popc(idle);
             uint32_t const leader = __ffs(idle) - 1;
             uint32_t       base   = 0;
@@ -71,14 +93,25 @@ __global__ void __launch_bounds__(Block)
             if (!active) {
                 uint32_t const mine = base + __popc(idle & lt);
                 if (mine < num_rays) {
-                    ray = mine;
                     // Rays are read once: evict-first loads keep them from displacing the
                     // tree's nodes and triangles in L2.
                     gpu::start_ray(r, tv, __ldcs(rays + 2 * size_t(mine)),
                                    __ldcs(rays + 2 * size_t(mine) + 1));
-                    active = true;
+                    if (gpu::enters_box(r, scene_lo, scene_hi)) {
+                        ray    = mine;
+                        active = true;
+                    } else if (Any_hit) {
+                        __stcs(occluded + mine, uint8_t(0));
+                    } else {
+                        __stcs(ids + mine, gpu::Miss);
+                        __stcs(ts + mine, r.tbest);
+                        if (uvs) {
+                            __stcs(uvs + mine, make_float2(0.f, 0.f));
+                        }
+                    }
                 }
             }
+            idle = __ballot_sync(Full_mask, !active);
         }
 
         if (!active) {
@@ -144,6 +177,8 @@ struct spb_tree {
     unsigned long long* d_stats = nullptr;  // node steps, triangle steps (spb_cast_stats_device)
     bool          built      = false;
     float         hit_margin = 0.f;
+    float3        scene_lo   = {0.f, 0.f, 0.f};  // Wide_bvh::scene_lo / scene_hi
+    float3        scene_hi   = {0.f, 0.f, 0.f};
     spb_tree_info info{};
     Pipeline      pipe;
     cudaStream_t  last_stream = nullptr;
@@ -224,11 +259,11 @@ int32_t launch(spb_tree* tree, bool any_hit, uint32_t slot, float4 const* rays, 
     if (any_hit) {
         cast_kernel<true><<<grid, Block, 0, stream>>>(
             reinterpret_cast<uint4 const*>(tree->d_nodes), tree->d_tris, rays, n, nullptr,
-            nullptr, nullptr, occ, counters, counters + 1, tree->hit_margin, nullptr);
+            nullptr, nullptr, occ, counters, counters + 1, tree->hit_margin, tree->scene_lo, tree->scene_hi, nullptr);
     } else {
         cast_kernel<false><<<grid, Block, 0, stream>>>(
             reinterpret_cast<uint4 const*>(tree->d_nodes), tree->d_tris, rays, n, ids, ts, uvs,
-            nullptr, counters, counters + 1, tree->hit_margin, nullptr);
+            nullptr, counters, counters + 1, tree->hit_margin, tree->scene_lo, tree->scene_hi, nullptr);
     }
     SPB_CUDA(cudaGetLastError());
     return SPB_OK;
@@ -342,6 +377,8 @@ extern "C" SPB_API int32_t spb_tree_build(spb_tree* tree, uint32_t num_vertices,
     tree->info.build_seconds = std::chrono::duration<double>(t1 - t0).count();
     tree->info.sah_cost      = bvh.sah_cost;
     tree->hit_margin         = bvh.hit_margin;
+    tree->scene_lo           = make_float3(bvh.scene_lo[0], bvh.scene_lo[1], bvh.scene_lo[2]);
+    tree->scene_hi           = make_float3(bvh.scene_hi[0], bvh.scene_hi[1], bvh.scene_hi[2]);
     tree->built              = true;
     return SPB_OK;
 }
@@ -438,7 +475,7 @@ extern "C" SPB_API int32_t spb_cast_stats_device(spb_tree* tree, float const* ra
     cast_kernel<false, true><<<grid, Block, 0, st>>>(
         reinterpret_cast<uint4 const*>(tree->d_nodes), tree->d_tris,
         reinterpret_cast<float4 const*>(rays), n, ids, ts, nullptr, nullptr, counters,
-        counters + 1, tree->hit_margin, tree->d_stats);
+        counters + 1, tree->hit_margin, tree->scene_lo, tree->scene_hi, tree->d_stats);
     SPB_CUDA(cudaGetLastError());
     unsigned long long host[2] = {0, 0};
     SPB_CUDA(cudaMemcpyAsync(host, tree->d_stats, sizeof(host), cudaMemcpyDeviceToHost, st));
@@ -647,7 +684,7 @@ extern "C" SPB_API int32_t spb_intersect_host_static(spb_tree* tree, float const
     cast_kernel<false><<<grid, Block, 0, nullptr>>>(reinterpret_cast<uint4 const*>(tree->d_nodes),
                                                     tree->d_tris, d_rays, n, d_ids, d_ts, nullptr,
                                                     nullptr, work, tree->d_counters + 1,
-                                                    tree->hit_margin, nullptr);
+                                                    tree->hit_margin, tree->scene_lo, tree->scene_hi, nullptr);
     SPB_CUDA(cudaGetLastError());
     SPB_CUDA(cudaMemcpyAsync(ids, d_ids, size_t(n) * 4, cudaMemcpyDeviceToHost, nullptr));
     SPB_CUDA(cudaMemcpyAsync(ts, d_ts, size_t(n) * 4, cudaMemcpyDeviceToHost, nullptr));

@@ -190,6 +190,34 @@ __device__ __forceinline__ uint32_t node_test(Ray_state const& r, uint4 const* _
 }
 
 
+// Whether the ray's [min_t, max_t] overlaps the box [lo, hi]: a slab test in double precision
+// whose reciprocals are the ray's slab reciprocals (start_ray) refined by one Newton step, so
+// that rounding cannot reject a ray that passes through the box by more than about 1e-14 of
+// its distance to it.  A NaN anywhere makes the test pass (fmin and fmax ignore NaN), leaving
+// such rays to the traversal.  Used with the tree's scene box (Wide_bvh::scene_lo/hi), which
+// is padded by 128 hit margins: every ray it rejects ends as a miss of the full traversal too.
+__device__ __forceinline__ bool enters_box(Ray_state const& r, float3 lo, float3 hi) {
+    float const o[3]   = {r.ox, r.oy, r.oz};
+    float const d[3]   = {r.dx, r.dy, r.dz};
+    float const inv[3] = {r.ix, r.iy, r.iz};
+    float const l[3]   = {lo.x, lo.y, lo.z};
+    float const h[3]   = {hi.x, hi.y, hi.z};
+    double      tn     = r.tmin;
+    double      tf     = r.tbest;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float const  tiny = 8.27180613e-25f;  // 2^-80, as safe_rcp
+        double const m    = fabsf(d[k]) < tiny ? copysignf(tiny, d[k]) : d[k];
+        double       i    = inv[k];
+        i                 = i * fma(-m, i, 2.0);
+        double const a    = (double(l[k]) - double(o[k])) * i;
+        double const b    = (double(h[k]) - double(o[k])) * i;
+        tn                = fmax(tn, fmin(a, b));
+        tf                = fmin(tf, fmax(a, b));
+    }
+    return tn <= tf;
+}
+
 // Per-lane traversal state kept in registers; the node-group stack itself is a separate
 // array (local memory), so that dynamic indexing into it does not pull these scalars out of
 // registers.

@@ -141,7 +141,9 @@ def test_benchmark_ids_against_the_reference_at_full_size(torch_cuda):
     """The benchmark's own workload (1,048,576 triangles, all 16,777,216 rays): every closest
     hit of the GPU cast against the compiled reference's Builder_SAH(16,64,4) + Tree::intersect.
     Disagreements must all be rounding-level edge/tie cases (the reference's rcpss reciprocal
-    and last-tested tie rule), at most 1e-4 of the rays; t within 2 ulp where the ids agree."""
+    and last-tested tie rule), at most 1e-4 of the rays; where the ids agree, t within 4 ulp
+    (the reference's 1/det is rcpss plus one Newton step, good to about 2 ulp, which t = e2.q / det
+    inherits; the IEEE quotient here is good to half an ulp)."""
     if not oracle.reference_available():
         pytest.skip("oracle/_ref/ref_cast not built")
     torch = torch_cuda
@@ -160,7 +162,7 @@ def test_benchmark_ids_against_the_reference_at_full_size(torch_cuda):
     print("full-size id parity against the reference:", summary)
     assert summary["unexplained"] == 0, summary
     assert summary["explained_edge_tie"] <= 1e-4 * n
-    assert summary["t_max_ulp_on_equal_ids"] <= 2
+    assert summary["t_max_ulp_on_equal_ids"] <= 4
 
 
 def test_empty_batch_and_state_errors():
