@@ -24,11 +24,13 @@
 //     mount <folder>   (su_mount; the folder name without spaces)
 //     take <width> <height> <take file>   (su_load_take; the take's resolution, for the readback)
 //     progressive <iterations>
+//     prepare   (su_start_render_frame(0), timed apart as prepare_s: joins the asynchronous mesh
+//               BVH builds and compiles the scene, so that a later "frame" times the render)
 //     frame <frame>
 //   Handles: the n-th camera/material/mesh/prop command creates handle 4000/1000+n/2000+n/3000+n.
 //   DATA: raw little-endian arrays referenced by byte offset.
 //   OUT: float32 RGBA framebuffer (width * height * 4).
-// Prints one JSON line: render seconds and the su_* status codes.
+// Prints one JSON line: render and preparation seconds and the su_* status codes.
 #include "capi/sprout.h"
 
 #include <chrono>
@@ -65,6 +67,7 @@ int main(int argc, char** argv) {
     uint32_t n_mat = 0, n_mesh = 0, n_prop = 0, n_image = 0;
     uint32_t width = 0, height = 0;
     double   render_s = 0.0;
+    double   prepare_s = 0.0;
     int32_t  status   = 0;
 
     char line[1 << 16];
@@ -164,6 +167,10 @@ int main(int argc, char** argv) {
                 status |= su_render_iteration();
             }
             render_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        } else if (c == "prepare") {
+            auto const t0 = std::chrono::steady_clock::now();
+            status |= su_start_render_frame(0);
+            prepare_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         } else if (c == "frame") {
             uint32_t f = 0;
             std::sscanf(rest, "%u", &f);
@@ -185,6 +192,7 @@ int main(int argc, char** argv) {
     std::fwrite(fb.data(), sizeof(float), fb.size(), of);
     std::fclose(of);
     su_release();
-    std::printf("{\"render_s\": %.6f, \"status\": %d}\n", render_s, status);
+    std::printf("{\"render_s\": %.6f, \"prepare_s\": %.6f, \"status\": %d}\n", render_s, prepare_s,
+                status);
     return 0;
 }

@@ -16,8 +16,9 @@
 Prints one JSON object: samples/s and rays/s (closest-hit + shadow) per frame, the end-to-end
 frame rate seen by the caller (render + postprocess + framebuffer copy to host), optionally
 the sample count and device time to reach relMSE 0.01 against a 4096-spp image of this
-renderer, and optionally the reference renderer's rate on the host cores (the whole frame for
-cornell; a 480x270, 32-spp frame of the same scene for wavefront).
+renderer (the doorway against its 65,536-spp image), and optionally the reference renderer's rate on the host cores (the whole frame for
+cornell; a 960x540, 16-spp frame of the same scene for wavefront), its scene preparation timed
+apart.
 """
 
 from __future__ import annotations
@@ -26,6 +27,7 @@ import argparse
 import ctypes
 import json
 import os
+import pathlib
 import statistics
 import time
 
@@ -42,7 +44,7 @@ SCENES = {
                   "metallic Bernoulli(0.3)), 4,096 emissive tris of log-uniform radiance [0.1, 100] via the light "
                   "tree, PTMIS max depth 12 (Russian roulette from depth 4)",
                   lambda su, w, h, spp: scenes.wavefront(su, w, h, spp),
-                  (1920, 1080, 256), (480, 270, 32)),
+                  (1920, 1080, 256), (960, 540, 16)),
 }
 
 
@@ -105,13 +107,16 @@ def measure(scene="cornell", width=None, height=None, spp=None, frames=3, conver
 
         if oracle.REF_RENDER.exists():
             cw, ch, cspp = cpu_frame or (width, height, spp)
-            _, timing = oracle.reference_render(lambda r: build(r, cw, ch, cspp), cw, ch, 0, progressive=False)
+            _, timing = oracle.reference_render(lambda r: build(r, cw, ch, cspp), cw, ch, 0, progressive=False,
+                                                prepare=True)
             what = "full frame" if cpu_frame is None else f"{cw}x{ch}, {cspp} spp frame of the same scene"
             out["cpu_baseline"] = {"msamples_s": round(cw * ch * cspp / timing["render_s"] / 1e6, 4),
                                    "seconds": round(timing["render_s"], 3), "cores": os.cpu_count(),
+                                   "prepare_seconds": round(timing["prepare_s"], 3),
                                    "kind": "reference",
-                                   "sample": f"{what}, the reference's su_render_frame (batch, scene build "
-                                             "included) on all host threads"}
+                                   "sample": f"{what}, the reference's su_render_frame (batch) on all host "
+                                             "threads; its mesh BVH builds and first scene compile run before, "
+                                             "timed apart (prepare_seconds)"}
     return out
 
 
@@ -162,14 +167,18 @@ def measure_volume(views=4, spp=128, cpu_reference=False):
 
         if oracle.REF_RENDER.exists():
             position, _ = chosen[0]
-            cw, cspp = 128, 8
+            cw, cspp = 256, 32
             _, timing = oracle.reference_render(
-                lambda r: scenes.volume(r, cw, cw, cspp, density, position=position), cw, cw, 0, progressive=False)
+                lambda r: scenes.volume(r, cw, cw, cspp, density, position=position), cw, cw, 0, progressive=False,
+                prepare=True)
             out["cpu_baseline"] = {"msamples_s": round(cw * cw * cspp / timing["render_s"] / 1e6, 4),
                                    "seconds": round(timing["render_s"], 3), "cores": os.cpu_count(),
+                                   "prepare_seconds": round(timing["prepare_s"], 3),
                                    "kind": "reference",
                                    "sample": f"first view at {cw}x{cw}, {cspp} spp, the reference's su_render_frame "
-                                             "(batch, scene and majorant-tree build included) on all host threads"}
+                                             "(batch) on all host threads; the majorant tree (built when the "
+                                             "material is created), the mesh BVH builds and the first scene compile "
+                                             "run before it, timed apart (prepare_seconds)"}
     return out
 
 
@@ -236,43 +245,54 @@ def network_roofline(stats):
     return out
 
 
-def measure_guiding(width=1280, height=720, reference_spp=4096, target=0.01, guiding=True):
-    """Time to relMSE `target` on the doorway interior, plain MIS against learned guiding.
+REFERENCE_64K = pathlib.Path(__file__).resolve().parent.parent / "tests" / "golden" / "doorway_reference_64k.npz"
 
-    relMSE is mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2) with both images scaled so
-    that the reference's mean is 0.5.  The reference r is a plain render of reference_spp samples
-    per pixel with an independent seed; its own noise adds to every measurement, in expectation
-    by c = v / R (v: the plain estimator's relative variance per sample), which a plain render
-    at s spp also measures (E[e] = v / s + v / R).  Each reported relMSE has c subtracted.  For
-    each integrator: a probe render gives the sample count expected to reach the target (relMSE
-    falls as 1/spp), then renders at that count (raised until the target is met) give the
-    reported sample count; the frame at that count is rendered three times (the same image) and
-    its median device and wall times are reported, so that one host stall on a shared machine
-    does not set the ratio."""
-    ref, ref_s, _ = doorway_frame(width, height, reference_spp, None, seed=1000)
-    k = 0.5 / ref.mean()
+# Training schedules of the guided integrator ("guiding" key of the PTMIS integrator): this
+# renderer's defaults (passes of 2 spp, 32 Adam steps of 65,536 records, learning rate 1e-2,
+# training until 32 spp), and the configuration's own (batches of 2^18 records, learning rate
+# 1e-3, the rest as the defaults).
+GUIDING_SCHEDULES = {
+    "tuned": True,
+    "config": {"batch": 1 << 18, "learning_rate": 1e-3},
+}
 
-    def raw(img):
-        return float(np.mean((k * img - k * ref) ** 2 / ((k * ref) ** 2 + 1e-2)))
 
-    probe = 512
-    img, _, _ = doorway_frame(width, height, probe)
-    e = raw(img)
-    c = e * probe / (reference_spp + probe)
+def measure_guiding(width=1280, height=720, target=0.01):
+    """Time to relMSE `target` on the doorway interior: plain MIS against learned guiding under
+    each training schedule.
+
+    relMSE is the mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2), r the converged
+    image tests/golden/doorway_reference_64k.npz (65,536 spp of plain MIS at 1280x720, summed in
+    float64 over 64 frames of independent seeds; tests/golden/make_doorway_reference.py), with no
+    rescaling and nothing subtracted (its own error adds about 0.01 * s / 65536 at s spp).  For
+    each integrator a probe render predicts the sample count that reaches the target (relMSE
+    falls as 1 / spp), renders at that count (raised until the target is met) give the reported
+    count, and the frame at that count is rendered three times; the median device and wall
+    times are reported, so that one host stall on a shared machine does not set the ratio."""
+    if not REFERENCE_64K.exists():
+        raise FileNotFoundError(f"{REFERENCE_64K} missing: make it with tests/golden/make_doorway_reference.py")
+    data = np.load(REFERENCE_64K)
+    ref = data["image"].astype(np.float64)
+    meta = json.loads(bytes(data["meta"]).decode())
+    assert ref.shape == (height, width, 3), ref.shape
+
+    def rel(img):
+        return float(np.mean((img - ref) ** 2 / (ref * ref + 1e-2)))
+
     out = {"workload": "doorway", "config": f"{GUIDING_CONFIG}, {width}x{height}",
-           "rel_mse": "mean (x - r)^2 / (r^2 + 0.01), images scaled so that mean(r) = 0.5, minus the "
-                      "reference's own share",
-           "reference": {"spp": reference_spp, "integrator": "plain MIS, independent seed",
-                         "device_seconds": round(ref_s, 3), "rel_mse_share": round(c, 6)},
+           "rel_mse": "mean over pixels and channels of (x - r)^2 / (r^2 + 0.01), no rescaling",
+           "reference": {"spp": meta["spp"], "integrator": "plain MIS, float64 sum of 64 frames of independent "
+                                                           "seeds (tests/golden/doorway_reference_64k.npz)",
+                         "mean": [round(x, 6) for x in meta["mean"]]},
            "target": target}
 
     last_stats = {}
 
-    def reach(first, guided):
+    def reach(first, guiding):
         spp, runs = first, []
-        for _ in range(4):
-            img, dev, wall = doorway_frame(width, height, spp, guiding if guided else None, stats_out=last_stats)
-            err = raw(img) - c
+        for _ in range(5):
+            img, dev, wall = doorway_frame(width, height, spp, guiding, stats_out=last_stats)
+            err = rel(img)
             runs.append({"spp": spp, "rel_mse": round(err, 5), "device_seconds": round(dev, 4),
                          "wall_seconds": round(wall, 3)})
             if err <= target:
@@ -281,25 +301,35 @@ def measure_guiding(width=1280, height=720, reference_spp=4096, target=0.01, gui
         last = runs[-1]
         devs, walls = [last["device_seconds"]], [last["wall_seconds"]]
         for _ in range(2):
-            _, dev, wall = doorway_frame(width, height, spp, guiding if guided else None, stats_out=last_stats)
+            _, dev, wall = doorway_frame(width, height, spp, guiding, stats_out=last_stats)
             devs.append(round(dev, 4))
             walls.append(round(wall, 3))
         last["device_seconds"], last["wall_seconds"] = float(np.median(devs)), float(np.median(walls))
         last["device_seconds_frames"], last["wall_seconds_frames"] = devs, walls
         return runs
 
-    plain_v = (e - c) * probe
-    plain = reach(int(np.ceil(plain_v / target / 8.0)) * 8, False)
-    probe_img, _, _ = doorway_frame(width, height, 256, guiding)
-    guided_v = (raw(probe_img) - c) * 256
-    guided = reach(int(np.ceil(guided_v / target / 8.0)) * 8, True)
+    def predicted(guiding, probe):
+        img, _, _ = doorway_frame(width, height, probe, guiding)
+        return max(8, int(np.ceil(probe * rel(img) / target / 8.0)) * 8)
+
+    plain = reach(predicted(None, 256), None)
     out["plain"] = plain[-1]
-    out["guided"] = guided[-1]
-    out["network"] = network_roofline(last_stats)
-    out["runs"] = {"plain": plain, "guided": guided}
-    if plain[-1]["rel_mse"] <= target and guided[-1]["rel_mse"] <= target:
-        out["guided_over_plain_device_time"] = round(guided[-1]["device_seconds"] / plain[-1]["device_seconds"], 4)
-        out["guided_over_plain_wall_time"] = round(guided[-1]["wall_seconds"] / plain[-1]["wall_seconds"], 4)
+    out["runs"] = {"plain": plain}
+    out["schedules"] = {}
+    for name, guiding in GUIDING_SCHEDULES.items():
+        runs = reach(predicted(guiding, 128), guiding)
+        entry = {"guiding": guiding, "result": runs[-1], "network": network_roofline(last_stats)}
+        if plain[-1]["rel_mse"] <= target and runs[-1]["rel_mse"] <= target:
+            entry["guided_over_plain_device_time"] = round(runs[-1]["device_seconds"] / plain[-1]["device_seconds"], 4)
+            entry["guided_over_plain_wall_time"] = round(runs[-1]["wall_seconds"] / plain[-1]["wall_seconds"], 4)
+        out["schedules"][name] = entry
+        out["runs"][name] = runs
+    tuned = out["schedules"]["tuned"]
+    out["guided"] = tuned["result"]
+    out["network"] = tuned["network"]
+    for key in ("guided_over_plain_device_time", "guided_over_plain_wall_time"):
+        if key in tuned:
+            out[key] = tuned[key]
     return out
 
 

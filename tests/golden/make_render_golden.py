@@ -67,14 +67,21 @@ CASES = {
     # built-in Sphere and Cube props, a Sphere lamp, a look_at camera; the sample count is set
     # after the take
     "take_room96": (96, 72, 4096, {"scene": "take", "take": "room.take"}, None),
+    # the Cornell workload at its configured size: 512x512, the 81,920-triangle sphere
+    "cornell512": (512, 512, 2048, {"sphere_subdivisions": 6}, None),
+    # the guiding workload's room at 320x180 (plain MIS), the image the guided integrator is
+    # compared with at a size where its network sees realistic training passes
+    "doorway320": (320, 180, 4096, {"scene": "doorway"}, None),
 }
+# Cases stored as float16 (the large images; the tests' bounds are far above its rounding).
+HALF = {"cornell512", "doorway320"}
 TAKES = HERE / "takes"
 PATH = HERE / "cornell_reference.npz"
 # Block size of the block-mean comparison where 8 is too small: many small, bright emitters
 # leave the 2048-spp reference image with 4 % noise in single 8x8 blocks (its 1024- and
 # 2048-spp images differ by that much), 1.6 % in 16x16 blocks; the dense medium 1.7 % and
 # 0.6 %.
-BLOCK = {"wavefront96": 16, "volume64": 16, "doorway96": 16}
+BLOCK = {"wavefront96": 16, "volume64": 16, "doorway96": 16, "doorway320": 20}
 
 
 def build(su, w, h, spp, kwargs, density=None):
@@ -111,7 +118,7 @@ def main(names):
                                               progressive=False)
         if timing["status"] != 0:
             raise RuntimeError(f"{name}: reference status {timing['status']}")
-        out[name] = img.astype(np.float32)
+        out[name] = img.astype(np.float16 if name in HALF else np.float32)
         if density is not None:
             out[name + "_density"] = density
         meta["cases"][name] = {"width": w, "height": h, "spp": spp, "scene": kwargs,

@@ -63,16 +63,17 @@ def test_guided_converges_to_plain():
     assert worst < 0.012, f"worst 16x16 block deviation {worst:.4f}"
 
 
-def test_guided_matches_reference_image():
+@pytest.mark.parametrize("case", ["doorway96", "doorway320"])
+def test_guided_matches_reference_image(case):
     """The guided integrator against the reference renderer's own converged image of the
-    doorway interior (plain MIS, 8,192 spp; tests/golden/cornell_reference.npz), with the
-    statistical bounds of the plain parity test."""
+    doorway interior (plain MIS; 96x54 at 8,192 spp and 320x180 at 4,096 spp;
+    tests/golden/cornell_reference.npz), with the statistical bounds of the plain parity test."""
     import json
     import pathlib
 
     data = np.load(pathlib.Path(__file__).resolve().parent / "golden" / "cornell_reference.npz")
-    meta = json.loads(bytes(data["meta"]).decode())["cases"]["doorway96"]
-    ref = data["doorway96"].astype(np.float64)
+    meta = json.loads(bytes(data["meta"]).decode())["cases"][case]
+    ref = data[case].astype(np.float64)
     img, _, _ = doorway_frame(meta["width"], meta["height"], 4 * meta["spp"], True)
     m_ref, m_img = ref.mean(axis=(0, 1)), img.mean(axis=(0, 1))
     assert np.all(np.abs(m_img - m_ref) <= 0.005 * m_ref), (m_img, m_ref)

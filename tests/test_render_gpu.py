@@ -73,14 +73,14 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
 CASES = ["cornell64_sub3", "cornell128_sub6", "cornell64_medium", "cornell64_emissive", "cornell64_thin_direct",
          "cornell64_grid",
          "cornell64_lights", "wavefront96", "builtins96", "builtins96_backdrop", "volume64",
-         "doorway96", "take_room96"]
+         "doorway96", "take_room96", "cornell512", "doorway320"]
 
 
 @pytest.mark.parametrize("name", CASES)
 def test_converged_image_matches_reference(name):
     data = np.load(GOLDEN)
     meta = json.loads(bytes(data["meta"]).decode())["cases"][name]
-    ref = data[name]
+    ref = data[name].astype(np.float32)
     density = data[meta["density"]] if meta.get("density") else None
     img = render(meta["width"], meta["height"], 4 * meta["spp"], density=density, **meta["scene"])
     assert np.all(np.isfinite(img))
