@@ -190,7 +190,10 @@ SPB_API int32_t spb_intersect_host_static(spb_tree* tree, float const* rays, uin
  * and the device time of training (batch gathering, gradients, Adam).  Launch shapes: the
  * largest wave (paths) and the traversal blocks per SM of the last wave, as the autotuner (or
  * the integrator's "wave_paths" / "trace_blocks_per_sm" keys) set them, and the waves replayed
- * from captured CUDA graphs (the "cuda_graphs" key turns them off).  No counterpart in the
+ * from captured CUDA graphs (the "cuda_graphs" key turns them off).  Scene: the props kept
+ * as instances of shared per-mesh trees under a top-level tree (the "instancing" key; 0 when
+ * every prop was flattened into one tree), the triangles the uploaded trees hold, and the
+ * medium tracking segments that reached the 65,536-collision cap.  No counterpart in the
  * reference (it logs wall-clock phases only, rendering_driver.cpp:99-136).
  * SPB_ERROR_ARGUMENT if there is no engine.
  */
@@ -207,6 +210,9 @@ typedef struct spb_render_stats {
     uint32_t wave_paths;
     uint32_t trace_blocks_per_sm;
     uint32_t graph_waves;
+    uint32_t instances;         /* props under a top-level tree (0: the scene was flattened) */
+    uint32_t tracking_capped;   /* medium tracking segments cut at the step cap (0 expected) */
+    uint64_t device_triangles;  /* triangles in the uploaded trees */
 } spb_render_stats;
 SPB_API int32_t spb_render_last_stats(spb_render_stats* out);
 

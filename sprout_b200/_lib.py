@@ -51,6 +51,9 @@ class RenderStats(ctypes.Structure):
         ("wave_paths", c_u32),
         ("trace_blocks_per_sm", c_u32),
         ("graph_waves", c_u32),
+        ("instances", c_u32),
+        ("tracking_capped", c_u32),
+        ("device_triangles", c_u64),
     ]
 
 

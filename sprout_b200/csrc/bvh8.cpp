@@ -313,46 +313,11 @@ float hit_margin_for(double extent, double magnitude) {
     return m > std::numeric_limits<float>::min() ? m : std::numeric_limits<float>::min();
 }
 
-bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* positions,
-                    uint32_t const* indices, uint32_t num_threads, Wide_bvh& out,
-                    std::string& error, uint32_t const* tri_class) {
-    out = Wide_bvh();
-
-    if (num_triangles == 0) {
-        error = "mesh has no triangles";
-        return false;
-    }
-    for (uint64_t i = 0; i < uint64_t(num_triangles) * 3; ++i) {
-        if (indices[i] >= num_vertices) {
-            error = "triangle index out of range";
-            return false;
-        }
-    }
-
-    std::vector<Box>   boxes(num_triangles);
-    std::vector<float> centroids(size_t(num_triangles) * 3);
-    parallel_ranges(num_triangles, num_threads, [&](uint32_t, uint64_t begin, uint64_t end) {
-        for (uint64_t t = begin; t < end; ++t) {
-            Box b;
-            for (int k = 0; k < 3; ++k) {
-                b.grow(positions + 3 * size_t(indices[3 * t + k]));
-            }
-            boxes[t] = b;
-            for (int a = 0; a < 3; ++a) {
-                centroids[3 * t + a] = 0.5f * (b.lo[a] + b.hi[a]);
-            }
-        }
-    });
-
-    for (uint32_t t = 0; t < num_triangles; ++t) {
-        for (int a = 0; a < 3; ++a) {
-            if (!std::isfinite(boxes[t].lo[a]) || !std::isfinite(boxes[t].hi[a])) {
-                error = "mesh has non-finite vertex positions";
-                return false;
-            }
-        }
-    }
-
+// Binary SAH tree over the primitives' boxes, collapsed to 8-wide nodes; emit(p, record)
+// fills the leaf record of primitive p.
+template <typename Emit>
+bool collapse_tree(std::vector<Box> const& boxes, std::vector<float> const& centroids,
+                   uint32_t num_threads, Wide_bvh& out, std::string& error, Emit&& emit) {
     Binary_builder builder(boxes, centroids, num_threads);
     builder.build();
     auto&       bnodes = builder.nodes();
@@ -547,16 +512,7 @@ bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* 
                 for (uint32_t t : tris) {
                     Wide_triangle wt;
                     std::memset(&wt, 0, sizeof(wt));
-                    float const* pa = positions + 3 * size_t(indices[3 * size_t(t) + 0]);
-                    float const* pb = positions + 3 * size_t(indices[3 * size_t(t) + 1]);
-                    float const* pc2 = positions + 3 * size_t(indices[3 * size_t(t) + 2]);
-                    for (int a = 0; a < 3; ++a) {
-                        wt.a[a]  = pa[a];
-                        wt.e1[a] = pb[a] - pa[a];
-                        wt.e2[a] = pc2[a] - pa[a];
-                    }
-                    wt.id        = t;
-                    wt.tri_class = tri_class ? tri_class[t] : 0u;
+                    emit(t, wt);
                     out.triangles.push_back(wt);
                 }
                 tri_offset += cnt;
@@ -585,5 +541,88 @@ bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* 
     }
     return true;
 }
+
+bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* positions,
+                    uint32_t const* indices, uint32_t num_threads, Wide_bvh& out,
+                    std::string& error, uint32_t const* tri_class) {
+    out = Wide_bvh();
+
+    if (num_triangles == 0) {
+        error = "mesh has no triangles";
+        return false;
+    }
+    for (uint64_t i = 0; i < uint64_t(num_triangles) * 3; ++i) {
+        if (indices[i] >= num_vertices) {
+            error = "triangle index out of range";
+            return false;
+        }
+    }
+
+    std::vector<Box>   boxes(num_triangles);
+    std::vector<float> centroids(size_t(num_triangles) * 3);
+    parallel_ranges(num_triangles, num_threads, [&](uint32_t, uint64_t begin, uint64_t end) {
+        for (uint64_t t = begin; t < end; ++t) {
+            Box b;
+            for (int k = 0; k < 3; ++k) {
+                b.grow(positions + 3 * size_t(indices[3 * t + k]));
+            }
+            boxes[t] = b;
+            for (int a = 0; a < 3; ++a) {
+                centroids[3 * t + a] = 0.5f * (b.lo[a] + b.hi[a]);
+            }
+        }
+    });
+
+    for (uint32_t t = 0; t < num_triangles; ++t) {
+        for (int a = 0; a < 3; ++a) {
+            if (!std::isfinite(boxes[t].lo[a]) || !std::isfinite(boxes[t].hi[a])) {
+                error = "mesh has non-finite vertex positions";
+                return false;
+            }
+        }
+    }
+
+    return collapse_tree(boxes, centroids, num_threads, out, error,
+                         [&](uint32_t t, Wide_triangle& wt) {
+                             float const* pa = positions + 3 * size_t(indices[3 * size_t(t) + 0]);
+                             float const* pb = positions + 3 * size_t(indices[3 * size_t(t) + 1]);
+                             float const* pc = positions + 3 * size_t(indices[3 * size_t(t) + 2]);
+                             for (int a = 0; a < 3; ++a) {
+                                 wt.a[a]  = pa[a];
+                                 wt.e1[a] = pb[a] - pa[a];
+                                 wt.e2[a] = pc[a] - pa[a];
+                             }
+                             wt.id        = t;
+                             wt.tri_class = tri_class ? tri_class[t] : 0u;
+                         });
+}
+
+bool build_wide_instances(uint32_t num_instances, float const* boxes_lo_hi, uint32_t instance_class,
+                          uint32_t num_threads, Wide_bvh& out, std::string& error) {
+    out = Wide_bvh();
+    if (num_instances == 0) {
+        error = "no instances";
+        return false;
+    }
+    std::vector<Box>   boxes(num_instances);
+    std::vector<float> centroids(size_t(num_instances) * 3);
+    for (uint32_t i = 0; i < num_instances; ++i) {
+        boxes[i].grow(boxes_lo_hi + 6 * size_t(i));
+        boxes[i].grow(boxes_lo_hi + 6 * size_t(i) + 3);
+        for (int a = 0; a < 3; ++a) {
+            if (!std::isfinite(boxes[i].lo[a]) || !std::isfinite(boxes[i].hi[a])) {
+                error = "instance with non-finite bounds";
+                return false;
+            }
+            centroids[3 * size_t(i) + a] = 0.5f * (boxes[i].lo[a] + boxes[i].hi[a]);
+        }
+    }
+    return collapse_tree(boxes, centroids, num_threads, out, error,
+                         [&](uint32_t i, Wide_triangle& wt) {
+                             wt.id        = i;
+                             wt.tri_class = instance_class;
+                         });
+}
+
 
 }  // namespace spb

@@ -76,4 +76,10 @@ bool build_wide_bvh(uint32_t num_vertices, uint32_t num_triangles, float const* 
                     uint32_t const* indices, uint32_t num_threads, Wide_bvh& out,
                     std::string& error, uint32_t const* tri_class = nullptr);
 
+// Builds a top-level 8-wide tree over instance boxes (6 floats each: lo.xyz, hi.xyz).  Its leaf
+// records carry the instance index in Wide_triangle::id and instance_class in tri_class; their
+// vertex fields are unused.
+bool build_wide_instances(uint32_t num_instances, float const* boxes_lo_hi, uint32_t instance_class,
+                          uint32_t num_threads, Wide_bvh& out, std::string& error);
+
 }  // namespace spb

@@ -86,6 +86,8 @@ struct Engine {
     bool                  scene_dirty    = true;   // host scene changed since the last upload
     bool                  camera_dirty   = false;  // only the camera changed since then
     bool                  tonemap_linear = false;  // su_create_defaults: Linear tonemapper
+    int                   instancing     = -1;     // PTMIS "instancing": -1 auto, 0 off, 1 on
+    bool                  sampler_golden = true;   // a take's "Random" sampler turns it off
     uint32_t              iteration     = 0;
     std::vector<float>    target;  // resolved rgba
     std::vector<std::string> mounts;  // su_mount folders, searched last mounted first
@@ -306,7 +308,8 @@ int32_t apply_camera();
 
 int32_t compile_scene() {
     spb::render::Scene_desc scene;
-    scene.materials = engine->materials;
+    scene.instancing = engine->instancing;
+    scene.materials  = engine->materials;
     // fallback material for unassigned slots: grey Substitute
     Material fallback{};
     fallback.type     = spb::shading::Type_substitute;
@@ -317,6 +320,7 @@ int32_t compile_scene() {
     uint32_t const fallback_id = uint32_t(scene.materials.size());
     scene.materials.push_back(fallback);
     std::vector<uint32_t> grid_images;  // image id of each scene.grids entry
+    std::map<uint32_t, uint32_t> scene_mesh;  // engine shape id -> scene mesh index
 
     for (Entity const& e : engine->entities) {
         if (e.camera || e.shape == Null) {
@@ -338,43 +342,43 @@ int32_t compile_scene() {
         }
         Mesh const& mesh =
             e.shape < First_mesh_id ? engine->builtin[e.shape] : engine->meshes[e.shape - First_mesh_id];
-        uint32_t const base = uint32_t(scene.positions.size() / 3);
-        float const*   m    = e.trafo;
-        float          rot[9];
-        float          pos[3];
-        decompose(m, rot, pos);
-        for (size_t v = 0; v < mesh.positions.size() / 3; ++v) {
-            float const x = mesh.positions[3 * v];
-            float const y = mesh.positions[3 * v + 1];
-            float const z = mesh.positions[3 * v + 2];
-            // row vector times matrix: p' = x * row0 + y * row1 + z * row2 + row3
-            scene.positions.push_back(x * m[0] + y * m[4] + z * m[8] + m[12]);
-            scene.positions.push_back(x * m[1] + y * m[5] + z * m[9] + m[13]);
-            scene.positions.push_back(x * m[2] + y * m[6] + z * m[10] + m[14]);
-            float const nx = mesh.normals[3 * v];
-            float const ny = mesh.normals[3 * v + 1];
-            float const nz = mesh.normals[3 * v + 2];
-            scene.normals.push_back(nx * rot[0] + ny * rot[3] + nz * rot[6]);
-            scene.normals.push_back(nx * rot[1] + ny * rot[4] + nz * rot[7]);
-            scene.normals.push_back(nx * rot[2] + ny * rot[5] + nz * rot[8]);
+        auto it = scene_mesh.find(e.shape);
+        if (it == scene_mesh.end()) {
+            spb::render::Mesh_desc md;
+            md.positions = mesh.positions;
+            md.normals   = mesh.normals;
+            md.indices   = mesh.indices;
+            md.tri_slot.resize(mesh.indices.size() / 3);
+            for (size_t t = 0; t < md.tri_slot.size(); ++t) {
+                md.tri_slot[t] = mesh.part_slot[mesh.part_of[t]];
+            }
+            it = scene_mesh.emplace(e.shape, uint32_t(scene.meshes.size())).first;
+            scene.meshes.push_back(std::move(md));
         }
+        spb::render::Instance_desc inst;
+        inst.mesh     = it->second;
+        inst.fallback = fallback_id;
+        inst.light    = e.light;
+        std::copy(e.trafo, e.trafo + 16, inst.trafo);
+        float pos[3];
+        decompose(e.trafo, inst.rotation, pos);
         // A density-grid medium samples its grid in the prop's texture space, so each prop gets
         // its own copy of such a material (one per slot), pointing at its own medium record.
-        std::vector<uint32_t> slot_material(e.materials.size(), fallback_id);
+        inst.materials.assign(e.materials.size(), fallback_id);
         for (size_t k = 0; k < e.materials.size(); ++k) {
             uint32_t const mat = e.materials[k];
             if (mat >= engine->materials.size()) {
                 continue;
             }
-            slot_material[k] = mat;
+            inst.materials[k] = mat;
             Grid_ref const& gr = engine->material_grids[mat];
             if (gr.image == Null) {
                 continue;
             }
             spb::render::Grid_medium gm;
-            auto const it = std::find(grid_images.begin(), grid_images.end(), gr.image);
-            gm.grid = uint32_t(it - grid_images.begin());
-            if (it == grid_images.end()) {
+            auto const gi = std::find(grid_images.begin(), grid_images.end(), gr.image);
+            gm.grid = uint32_t(gi - grid_images.begin());
+            if (gi == grid_images.end()) {
                 Image const&             img = engine->images[gr.image];
                 spb::render::Density_grid g;
                 std::copy(img.dims, img.dims + 3, g.dims);
@@ -384,24 +388,16 @@ int32_t compile_scene() {
             }
             gm.nearest = gr.nearest;
             gm.repeat  = gr.repeat;
-            texture_space(m, mesh, gm.world_to_uvw);
+            texture_space(e.trafo, mesh, gm.world_to_uvw);
             scene.media.push_back(gm);
             Material copy = engine->materials[mat];
             copy.medium   = uint32_t(scene.media.size());
-            slot_material[k] = uint32_t(scene.materials.size());
+            inst.materials[k] = uint32_t(scene.materials.size());
             scene.materials.push_back(copy);
         }
-        for (size_t t = 0; t < mesh.indices.size() / 3; ++t) {
-            for (int k = 0; k < 3; ++k) {
-                scene.indices.push_back(base + mesh.indices[3 * t + k]);
-            }
-            uint32_t const slot = mesh.part_slot[mesh.part_of[t]];
-            scene.tri_material.push_back(slot < slot_material.size() ? slot_material[slot]
-                                                                     : fallback_id);
-            scene.tri_light.push_back(e.light ? 1 : 0);
-        }
+        scene.instances.push_back(std::move(inst));
     }
-    if (scene.indices.empty()) {
+    if (scene.instances.empty()) {
         log(SU_LOG_ERROR, "scene has no triangles");
         return -2;
     }
@@ -424,7 +420,12 @@ int32_t apply_camera() {
         log(SU_LOG_ERROR, engine->renderer.error());
         return -2;
     }
-    engine->renderer.set_settings(engine->settings);
+    // Batch rendering samples with golden ratio sequences, progressive rendering with
+    // independent random numbers (su_create_sampler, capi.cpp:295-312; load_sampler_pool,
+    // take_loader.cpp:531-556).
+    spb::render::Settings settings = engine->settings;
+    settings.golden_ratio          = !engine->progressive && engine->sampler_golden;
+    engine->renderer.set_settings(settings);
     return 0;
 }
 
@@ -940,9 +941,14 @@ int32_t load_take(std::string const& string) {
             log(SU_LOG_WARNING, "su_load_take: the sensor filter is drawn as Gaussian (radius 1, alpha 1.8)");
         }
     }
+    engine->sampler_golden = false;  // a take without a sampler samples randomly (take_loader.cpp:150-157)
     if (spb::json::Value const* sampler = take.find("sampler"); sampler && sampler->is_object() &&
                                                                 !sampler->object.empty()) {
         su_create_sampler(uint32_t(spb::json::number_or(sampler->object[0].second.find("samples_per_pixel"), 1.0)));
+        // "Golden_ratio" (and su_create_sampler) sample batch frames with golden ratio
+        // sequences; "Random" (and the reference's "RD", whose sequence this renderer does not
+        // have) with independent random numbers
+        engine->sampler_golden = sampler->object[0].first == "Golden_ratio";
     }
     if (spb::json::Value const* integrator = take.find("integrator")) {
         su_create_integrators(spb::json::dump(*integrator).c_str());
@@ -1125,6 +1131,14 @@ SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
             s.wave_paths          = s.wave_paths ? std::clamp(s.wave_paths, 1u << 16, 1u << 24) : 0u;
             // "cuda_graphs": false launches every wave's kernels one by one
             s.cuda_graphs = spb::json::bool_or(pt->find("cuda_graphs"), true);
+            // "instancing": true keeps one tree per mesh under a top-level tree over the props,
+            // false flattens every prop into one world-space tree; absent or "auto": two
+            // levels when flattening would multiply the distinct meshes' triangles by more
+            // than four and exceed a million (this renderer's extension)
+            engine->instancing = -1;
+            if (spb::json::Value const* inst = pt->find("instancing"); inst && !inst->is_string()) {
+                engine->instancing = spb::json::bool_or(inst, false) ? 1 : 0;
+            }
             // "guiding": true, or an object of the Settings guide fields (this renderer's
             // extension; the reference ignores the key)
             if (spb::json::Value const* g = pt->find("guiding")) {
@@ -1690,6 +1704,9 @@ SPB_API int32_t spb_render_last_stats(spb_render_stats* out) {
     out->wave_paths              = st.wave_paths;
     out->trace_blocks_per_sm     = st.trace_blocks_per_sm;
     out->graph_waves             = st.graph_waves;
+    out->instances               = st.instances;
+    out->tracking_capped         = st.tracking_capped;
+    out->device_triangles        = st.device_triangles;
     return SPB_OK;
 }
 

@@ -275,10 +275,10 @@ struct Builder {
 
 }  // namespace
 
-void build_light_tree(std::vector<Light_input> const& lights, uint32_t num_triangles,
+void build_light_tree(std::vector<Light_input> const& lights, uint32_t num_slots,
                       Light_tree& out) {
     out = Light_tree();
-    out.order.assign(num_triangles, 0xFFFFFFFFu);
+    out.order.assign(num_slots, 0xFFFFFFFFu);
     if (lights.empty()) {
         return;
     }
@@ -332,8 +332,8 @@ void build_light_tree(std::vector<Light_input> const& lights, uint32_t num_trian
         b.put_float4(out.tris, in.a[0], in.a[1], in.a[2], it.area);
         b.put_float4(out.tris, in.b[0] - in.a[0], in.b[1] - in.a[1], in.b[2] - in.a[2], 0.0);
         b.put_float4(out.tris, in.c[0] - in.a[0], in.c[1] - in.a[1], in.c[2] - in.a[2], 0.0);
-        out.tris.back() = Builder::bits(in.tri);
-        out.order[in.tri] = o;
+        out.tris.back() = Builder::bits(in.material);
+        out.order[in.slot] = o;
     }
 }
 

@@ -20,7 +20,8 @@ struct Light_input {
     double   a[3], b[3], c[3];
     double   power = 0.0;  // area * mean radiance (twice that for two-sided emitters)
     bool     two_sided = false;
-    uint32_t tri       = 0;  // scene triangle index
+    uint32_t slot      = 0;  // index of its entry in Light_tree::order
+    uint32_t material  = 0;  // its material (stored with it for the renderer's light sampling)
 };
 
 // Device-ready arrays, 4 floats per float4.
@@ -30,8 +31,8 @@ struct Light_input {
 //           middle (left child: order < middle).  Leaves hold lights first .. first+count-1.
 //   cones:  3 float4 per light in tree order: (centre, radius), (normal, cos spread),
 //           (power, 0, 0, 0)
-//   tris:   3 float4 per light in tree order: (a, area), (b - a, 0), (c - a, triangle id bits)
-//   order:  per scene triangle, its position in tree order, or 0xFFFFFFFF
+//   tris:   3 float4 per light in tree order: (a, area), (b - a, 0), (c - a, material index bits)
+//   order:  per light slot (Light_input::slot), its position in tree order, or 0xFFFFFFFF
 struct Light_tree {
     std::vector<float>    nodes;
     std::vector<float>    cones;
@@ -44,7 +45,7 @@ struct Light_tree {
 
 constexpr uint32_t Light_leaf_size = 4;
 
-void build_light_tree(std::vector<Light_input> const& lights, uint32_t num_triangles,
+void build_light_tree(std::vector<Light_input> const& lights, uint32_t num_slots,
                       Light_tree& out);
 
 }  // namespace spb::render

@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 
 #include "bvh8.hpp"
 #include "common.hpp"
@@ -46,6 +47,10 @@ namespace {
 using shading::V3;
 using shading::v3;
 
+__device__ __forceinline__ V3 f3v(float4 a) {
+    return v3(a.x, a.y, a.z);
+}
+
 constexpr uint32_t Full_mask        = 0xFFFFFFFFu;
 constexpr int      Trace_block      = 128;
 constexpr int      Shade_block      = 256;
@@ -55,6 +60,7 @@ constexpr int      Filter_samples   = 30;
 constexpr uint32_t Max_bounce_slots = 64;
 constexpr uint32_t Class_surface    = 1;  // Wide_triangle::tri_class of ordinary surfaces
 constexpr uint32_t Class_boundary   = 2;  // ... of participating-medium boundaries
+constexpr uint32_t Class_instance   = 4;  // ... of top-level leaves (instances)
 
 // Counter block (uint32): per bounce b, [8b] extension count, [8b+1] shadow count,
 // [8b+2] extend fetch, [8b+3] shadow fetch, [8b+4] transmittance count; then the overflow
@@ -92,12 +98,69 @@ struct Scene_gpu {
     float4                    env;  // uniform environment radiance; w: its pick probability in NEE
     float const*              e_table;
     Medium_gpu const*         media;  // Material::medium - 1 indexes this
+    // Instances: what the traversal reads (two-level trees only) and what shading reads (also
+    // the single identity instance of a flattened scene).
+    gpu::Instance_trace const* inst_trace;
+    struct Instance_shade const* inst_shade;
+    uint32_t const*           inst_materials;  // per instance slot: index into materials
+    uint32_t                  instanced;       // 1: two-level trees, hit records name instances
+    uint32_t*                 tracking_capped;  // counts tracking segments that reached their step cap
 };
+
+// What shading reads of an instance: its object-to-world map (rows: world_k =
+// dot(row_k.xyz, object) + row_k.w), the rotation of its normals (rows), its mesh's first entry
+// in tri_info, its first material slot in inst_materials, and its first entry in light_order
+// (0xFFFFFFFF if it is not a light).  A flattened scene has one instance: the identity.
+struct Instance_shade {
+    float4   o2w[3];
+    float4   nrm[3];
+    uint32_t tri_base;
+    uint32_t mat_base;
+    uint32_t light_base;
+    uint32_t pad;
+};
+
+__device__ __forceinline__ V3 map_point(float4 const* rows, V3 p) {
+    return v3(fmaf(rows[0].x, p.x, fmaf(rows[0].y, p.y, fmaf(rows[0].z, p.z, rows[0].w))),
+              fmaf(rows[1].x, p.x, fmaf(rows[1].y, p.y, fmaf(rows[1].z, p.z, rows[1].w))),
+              fmaf(rows[2].x, p.x, fmaf(rows[2].y, p.y, fmaf(rows[2].z, p.z, rows[2].w))));
+}
+
+// A hit triangle in world space: vertices, the shading normals at them (not normalised) and
+// its material; tri: its tri_info entry.
+struct World_tri {
+    V3       a, b, c;
+    uint32_t material;
+    uint4    tri;
+};
+
+// Triangle id of instance inst (a closest-hit record) in world space; with_normals also gives
+// the vertex normals.
+__device__ __forceinline__ World_tri world_triangle(Scene_gpu const& s, uint32_t inst, uint32_t id,
+                                                    V3* normals = nullptr) {
+    Instance_shade const& in = s.inst_shade[inst];
+    float4 const o2w[3] = {in.o2w[0], in.o2w[1], in.o2w[2]};
+    World_tri    w;
+    w.tri      = s.tri_info[in.tri_base + id];
+    w.a        = map_point(o2w, f3v(s.positions[w.tri.x]));
+    w.b        = map_point(o2w, f3v(s.positions[w.tri.y]));
+    w.c        = map_point(o2w, f3v(s.positions[w.tri.z]));
+    w.material = s.inst_materials[in.mat_base + w.tri.w];
+    if (normals) {
+        float4 const rows[3] = {in.nrm[0], in.nrm[1], in.nrm[2]};  // w = 0: no translation
+        normals[0] = map_point(rows, f3v(s.normals[w.tri.x]));
+        normals[1] = map_point(rows, f3v(s.normals[w.tri.y]));
+        normals[2] = map_point(rows, f3v(s.normals[w.tri.z]));
+    }
+    return w;
+}
+
 
 struct Paths {
     float4*   ray_o;  // origin, min_t
     float4*   ray_d;  // direction, max_t
     uint32_t* hit_id;
+    uint32_t* hit_inst;  // instance of the hit (two-level trees only)
     float*    hit_t;
     float2*   hit_uv;
     float4*   T;      // throughput, w: pdf of the last BSDF sample
@@ -129,6 +192,11 @@ struct Paths {
     uint32_t* open_record;
 };
 
+// The instance of a path's closest hit (the only instance of a flattened scene).
+__device__ __forceinline__ uint32_t hit_instance(Scene_gpu const& s, Paths const& p, uint32_t path) {
+    return s.instanced ? p.hit_inst[path] : 0u;
+}
+
 constexpr int Record_float4 = 5;
 
 // The guide's mixture per queue entry: 8 float4 of unit mean and concentration, the 8 lobe
@@ -154,6 +222,11 @@ struct Wave {
     uint32_t seed;
     uint32_t min_bounces;
     uint32_t max_bounces;
+    // Golden ratio sampling of the camera and the first Golden_bounces vertices (see
+    // golden_1d): the frame's samples per pixel (0: independent random samples) and the sorted
+    // table of frac(j / phi) * 2^32, j < golden_n.
+    uint32_t        golden_n;
+    uint32_t const* golden_sorted;
     uint32_t guiding;         // 1: sample the guide's mixture at surface vertices
     float    guide_fraction;  // its share of continuation directions
     float    metal_fraction;  // the same at metallic (pure GGX) surfaces
@@ -207,9 +280,101 @@ struct Rng {
     }
 };
 
-__device__ __forceinline__ V3 f3v(float4 a) {
-    return v3(a.x, a.y, a.z);
+
+// ---- golden ratio sampling (sampler::Golden_ratio, sampler_golden_ratio.cpp:21-73) ----
+// In batch rendering the reference samples the camera and, at the first three vertices of a
+// path, light selection, light points and BSDF directions from golden ratio sequences
+// (Pathtracer_MIS::material_sampler / light_sampler, pathtracer_mis.cpp:403-417): per pixel and
+// dimension the frame's n samples are frac(r + j / phi), j < n, with a random offset r, put in
+// a random order; 2-D dimensions pair the same sequence, sorted, with a second one
+// (golden_ratio in sample_distribution.inl, after Schretter, Kobbelt and Dehaye 2012).  Every
+// sample of a pixel thus lands in its own stratum of each dimension.  Here any sample is
+// computed directly from its index: in 32-bit fixed point (2^32 / phi rounds to 2654435769),
+// with a keyed bijection of [0, n) as the per-pixel shuffle (the reference shuffles with its
+// pixel's random stream) and, for the sorted first coordinates, a table of the sequence
+// without offset in ascending order, which the offset rotates.
+constexpr uint32_t Golden_step    = 2654435769u;
+constexpr uint32_t Golden_bounces = 3;  // Pathtracer_MIS::Num_dedicated_samplers
+
+// A bijection of [0, n) chosen by key: an invertible mix of the bits below n's next power of
+// two (odd multiplications, xor-shifts and additions, each a bijection of that range),
+// repeated until the value falls below n (cycle walking).
+__device__ __forceinline__ uint32_t permute(uint32_t i, uint32_t n, uint32_t key) {
+    uint32_t mask = n - 1u;
+    mask |= mask >> 1;
+    mask |= mask >> 2;
+    mask |= mask >> 4;
+    mask |= mask >> 8;
+    mask |= mask >> 16;
+    uint32_t const m1 = (key * 2u + 1u) | 1u;
+    uint32_t const a1 = key >> 11;
+    do {
+        i = ((i ^ (key >> 5)) * m1) & mask;
+        i ^= i >> 3;
+        i = (i + a1) & mask;
+        i = (i * 0x2C9277B5u) & mask;
+        i ^= (i & mask) >> 5;
+        i = ((i ^ (key >> 19)) * 0x85EBCA77u) & mask;
+        i ^= i >> 2;
+    } while (i >= n);
+    return i;
 }
+
+// Offset and shuffle key of a pixel's golden ratio dimension (its own PCG32 stream).
+__device__ __forceinline__ void golden_stream(uint32_t seed, uint32_t pixel, uint32_t dim, uint32_t& off0,
+                                              uint32_t& off1, uint32_t& key) {
+    uint64_t       state = 0;
+    uint64_t const inc   = ((uint64_t(pixel) << 6 | dim) << 1) | 1u;
+    pcg_next(state, inc);
+    state += uint64_t(seed) ^ 0x9E3779B97F4A7C15ull;
+    pcg_next(state, inc);
+    off0 = pcg_next(state, inc);
+    off1 = pcg_next(state, inc);
+    key  = pcg_next(state, inc);
+}
+
+__device__ __forceinline__ float fixed_to_unit(uint32_t x) {
+    return float(x >> 8) * (1.f / 16777216.f);
+}
+
+// Sample s of 1-D dimension dim of a pixel.
+__device__ __forceinline__ float golden_1d(Wave const& w, uint32_t pixel, uint32_t s, uint32_t dim) {
+    uint32_t off0, off1, key;
+    golden_stream(w.seed, pixel, dim, off0, off1, key);
+    uint32_t const j = permute(s, w.golden_n, key);
+    return fixed_to_unit(off0 + j * Golden_step);
+}
+
+// Sample s of 2-D dimension dim of a pixel.
+__device__ __forceinline__ float2 golden_2d(Wave const& w, uint32_t pixel, uint32_t s, uint32_t dim) {
+    uint32_t off0, off1, key;
+    golden_stream(w.seed, pixel, dim, off0, off1, key);
+    uint32_t const n = w.golden_n;
+    uint32_t const i = permute(s, n, key);
+    // First coordinate: the i-th smallest of frac(off0 + j / phi), j < n -- the sorted table
+    // rotated to start at c, the first entry that wraps past 1 when off0 is added.
+    uint64_t const wrap = (1ull << 32) - off0;
+    uint32_t       lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t const mid = (lo + hi) >> 1;
+        if (uint64_t(__ldg(w.golden_sorted + mid)) < wrap) {
+            lo = mid + 1;
+        } else {
+            hi = mid;
+        }
+    }
+    uint32_t k = lo + i;
+    k      = k >= n ? k - n : k;
+    return make_float2(fixed_to_unit(__ldg(w.golden_sorted + k) + off0), fixed_to_unit(off1 + i * Golden_step));
+}
+
+// Golden ratio dimensions: 2-D 0 the pixel position, 1 + 4 d + k the light point of light
+// sample k at vertex depth d, 1 + 4 d + 3 the BSDF direction; 1-D 16 + 4 d + k the light
+// selection of light sample k, 16 + 4 d + 3 the BSDF lobe.
+__device__ __forceinline__ uint32_t golden_light_2d(uint32_t depth, int k) { return 1u + 4u * depth + uint32_t(k); }
+__device__ __forceinline__ uint32_t golden_bsdf_2d(uint32_t depth) { return 1u + 4u * depth + 3u; }
+__device__ __forceinline__ uint32_t golden_light_1d(uint32_t depth, int k) { return 16u + 4u * depth + uint32_t(k); }
+__device__ __forceinline__ uint32_t golden_bsdf_1d(uint32_t depth) { return 16u + 4u * depth + 3u; }
 
 // Ray origin offset off a surface (Waechter and Binder, "A Fast and Robust Method for
 // Avoiding Self-Intersection", Ray Tracing Gems 2019, ch. 6), n pointing to the side the ray
@@ -277,8 +442,13 @@ __global__ void k_generate(Launch const* __restrict__ launch, Paths p, uint32_t*
 
     Rng rng;
     rng.start(wave.seed, uint64_t(pixel) + uint64_t(wave.first_sample + slot) * pixels);
-    float const u = rng.uniform();
-    float const v = rng.uniform();
+    float u = rng.uniform();
+    float v = rng.uniform();
+    if (wave.golden_n) {
+        float2 const g = golden_2d(wave, pixel, wave.first_sample + slot, 0);
+        u              = g.x;
+        v              = g.y;
+    }
 
     float const cx = float(x) + u;
     float const cy = float(y) + v;
@@ -314,7 +484,8 @@ __global__ void k_generate(Launch const* __restrict__ launch, Paths p, uint32_t*
 // Any_hit: shadow rays.  Media: the scene has participating media -- shadow rays ignore
 // medium boundaries and unoccluded ones go to the transmittance queue instead of adding
 // their contribution directly.
-template <bool Any_hit, bool Media = false>
+// Instances: the scene is a top-level tree over instances of per-mesh trees.
+template <bool Any_hit, bool Media = false, bool Instances = false>
 __global__ void __launch_bounds__(Trace_block)
     k_trace(Scene_gpu s, Paths p, uint32_t const* __restrict__ queue,
             uint32_t const* __restrict__ count, uint32_t* fetch, uint32_t* overflow,
@@ -323,9 +494,10 @@ __global__ void __launch_bounds__(Trace_block)
     uint32_t const lane = threadIdx.x & 31u;
     uint32_t const lt   = (1u << lane) - 1u;
 
-    gpu::Ray_state r;
-    gpu::Traversal tv;
-    uint2          stack[gpu::Stack_size];
+    gpu::Ray_state      r;
+    gpu::Traversal      tv;
+    gpu::Instance_state is;
+    uint2               stack[gpu::Stack_size];
     uint32_t       path      = 0;
     bool           active    = false;
     bool           exhausted = false;
@@ -358,6 +530,9 @@ __global__ void __launch_bounds__(Trace_block)
                     } else {
                         gpu::start_ray(r, tv, p.ray_o[path], p.ray_d[path]);
                     }
+                    if constexpr (Instances) {
+                        gpu::start_instances(r, is);
+                    }
                     active = true;
                 }
             }
@@ -365,8 +540,9 @@ __global__ void __launch_bounds__(Trace_block)
         if (!active) {
             continue;
         }
-        if (gpu::traversal_step<Any_hit, Media>(r, tv, stack, s.nodes, s.tris, s.hit_margin,
-                                                 overflow, Class_boundary)) {
+        if (gpu::traversal_step<Any_hit, Media, Instances>(r, tv, stack, s.nodes, s.tris, s.hit_margin,
+                                                            overflow, Class_boundary, &is,
+                                                            s.inst_trace)) {
             if (Any_hit) {
                 if (r.best_id == gpu::Miss) {
                     if (Media) {
@@ -386,6 +562,9 @@ __global__ void __launch_bounds__(Trace_block)
                 p.hit_id[path] = r.best_id;
                 p.hit_t[path]  = r.tbest;
                 p.hit_uv[path] = make_float2(r.u, r.v);
+                if constexpr (Instances) {
+                    p.hit_inst[path] = is.best_inst;
+                }
             }
             active = false;
         }
@@ -601,11 +780,11 @@ __device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, V3 n, bo
     float4 const   la   = s.light_tris[3 * l + 0];
     float4 const   le1  = s.light_tris[3 * l + 1];
     float4 const   le2  = s.light_tris[3 * l + 2];
-    uint32_t const ltri = __float_as_uint(le2.w);
+    uint32_t const lmat_id = __float_as_uint(le2.w);  // the emitter's material
     float const    sq   = sqrtf(r1);
     V3 const       q    = f3v(la) + (sq * (1.f - r2)) * f3v(le1) + (sq * r2) * f3v(le2);
     V3             ln   = shading::normalize(shading::cross(f3v(le1), f3v(le2)));
-    shading::Material const lmat = s.materials[s.tri_info[ltri].w];
+    shading::Material const lmat = s.materials[lmat_id];
     if (lmat.two_sided && shading::dot(ln, q - ps) > 0.f) {
         ln = -ln;
     }
@@ -624,11 +803,17 @@ __device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, V3 n, bo
     return true;
 }
 
+// Collisions one tracking segment may take (the reference loops until the segment ends,
+// tracking.cpp:286-349,473-540).  A segment that reaches the cap -- in practice only one of
+// optical thickness in the tens of thousands -- ends with the weight built up so far and is
+// counted (capped, Stats::tracking_capped), so that a render can show it never happened.
+constexpr int Max_tracking_steps = 1 << 16;
+
 // Homogeneous-medium tracking over [t, d] with spectral MIS (Tracking::tracking for a
 // homogeneous medium, tracking.cpp:425-470): returns true on a scattering event at t_out;
 // lw receives the path weight either way.
 __device__ __forceinline__ bool track_homogeneous(shading::Material const& m, float t, float d,
-                                                  Rng& rng, float& t_out, V3& lw) {
+                                                  Rng& rng, float& t_out, V3& lw, uint32_t* capped) {
     V3 const    mu_t = m.mu_a + m.mu_s;
     float const mt   = shading::max_component(mu_t);
     lw               = v3(1.f, 1.f, 1.f);
@@ -637,7 +822,7 @@ __device__ __forceinline__ bool track_homogeneous(shading::Material const& m, fl
     }
     float const imt  = 1.f / mt;
     V3 const    mu_n = v3(mt - mu_t.x, mt - mu_t.y, mt - mu_t.z);
-    for (int step = 0; step < 4096; ++step) {
+    for (int step = 0; step < Max_tracking_steps; ++step) {
         float const r0 = rng.uniform();
         t -= logf(1.f - r0) * imt;
         if (t > d) {
@@ -659,6 +844,7 @@ __device__ __forceinline__ bool track_homogeneous(shading::Material const& m, fl
         }
         lw = lw * ((1.f / (mt * pn)) * mu_n);
     }
+    atomicAdd(capped, 1u);
     return false;
 }
 
@@ -668,7 +854,8 @@ __device__ __forceinline__ bool track_homogeneous(shading::Material const& m, fl
 // returns 2 on absorption (li the emitted radiance, lw zero), 1 on scattering at t_out, 0 when
 // the segment is passed.
 __device__ __forceinline__ int track_homogeneous_emissive(shading::Material const& m, float t, float d,
-                                                          Rng& rng, float& t_out, V3& lw, V3& li) {
+                                                          Rng& rng, float& t_out, V3& lw, V3& li,
+                                                          uint32_t* capped) {
     V3 const    mu_t = m.mu_a + m.mu_s;
     float const mt   = shading::max_component(mu_t);
     lw               = v3(1.f, 1.f, 1.f);
@@ -678,7 +865,7 @@ __device__ __forceinline__ int track_homogeneous_emissive(shading::Material cons
     }
     float const imt  = 1.f / mt;
     V3 const    mu_n = v3(mt - mu_t.x, mt - mu_t.y, mt - mu_t.z);
-    for (int step = 0; step < 4096; ++step) {
+    for (int step = 0; step < Max_tracking_steps; ++step) {
         float const r0 = rng.uniform();
         t -= logf(1.f - r0) * imt;
         if (t > d) {
@@ -709,6 +896,7 @@ __device__ __forceinline__ int track_homogeneous_emissive(shading::Material cons
         }
         lw = lw * ((1.f / (mt * pn)) * mu_n);
     }
+    atomicAdd(capped, 1u);
     return 0;
 }
 
@@ -870,7 +1058,6 @@ __device__ bool walk_cells(Medium_gpu const& g, V3 o, V3 d, float t0, float t1, 
     return false;
 }
 
-constexpr int Max_tracking_steps = 1 << 16;
 
 // Delta tracking with spectral MIS through a density grid over the world ray (ro, rd) for t in
 // [t0, t1] (Tracking_multi::integrate heterogeneous branch, tracking_multi.cpp:98-164, with
@@ -878,7 +1065,7 @@ constexpr int Max_tracking_steps = 1 << 16;
 // coefficient (similarity relation).  Returns true on a scattering event at t_out; lw receives
 // the path weight either way.
 __device__ bool track_grid(Medium_gpu const& g, shading::Material const& m, float srs, V3 ro,
-                           V3 rd, float t0, float t1, Rng& rng, float& t_out, V3& lw) {
+                           V3 rd, float t0, float t1, Rng& rng, float& t_out, V3& lw, uint32_t* capped) {
     V3 const    o     = to_texture(g, ro);
     V3 const    d     = to_texture_dir(g, rd);
     V3 const    mu_s  = srs * m.mu_s;
@@ -920,6 +1107,9 @@ __device__ bool track_grid(Medium_gpu const& g, shading::Material const& m, floa
         }
         return true;
     });
+    if (steps >= Max_tracking_steps) {
+        atomicAdd(capped, 1u);
+    }
     return scattered;
 }
 
@@ -933,7 +1123,7 @@ __device__ __forceinline__ bool all_below_abort(V3 w) {
 // multiplied by the estimate; returns false when it falls below Abort_epsilon (the shadow
 // ray counts as blocked, Tracking::transmittance, tracking.cpp:143-180).
 __device__ bool transmit_grid(Medium_gpu const& g, shading::Material const& m, float srs, V3 ro,
-                              V3 rd, float t0, float t1, Rng& rng, V3& w) {
+                              V3 rd, float t0, float t1, Rng& rng, V3& w, uint32_t* capped) {
     V3 const    o     = to_texture(g, ro);
     V3 const    d     = to_texture_dir(g, rd);
     V3 const    mu_s  = srs * m.mu_s;
@@ -977,6 +1167,9 @@ __device__ bool transmit_grid(Medium_gpu const& g, shading::Material const& m, f
         }
         return false;
     });
+    if (steps >= Max_tracking_steps) {
+        atomicAdd(capped, 1u);
+    }
     return !blocked;
 }
 
@@ -1038,13 +1231,10 @@ static_assert(sizeof(float) * 48 * guide::Tile <= sizeof(__nv_bfloat16) * 2 * gu
 // Position, geometric normal (facing -dir) and outgoing direction of a path's hit.
 __device__ __forceinline__ void hit_frame(Scene_gpu const& s, Paths const& p, uint32_t path, uint32_t id,
                                           V3& pos, V3& geo_n, V3& wo) {
-    uint4 const  tri = s.tri_info[id];
-    V3 const     a   = f3v(s.positions[tri.x]);
-    V3 const     b   = f3v(s.positions[tri.y]);
-    V3 const     c   = f3v(s.positions[tri.z]);
-    float2 const uv  = p.hit_uv[path];
-    pos              = (1.f - uv.x - uv.y) * a + uv.x * b + uv.y * c;
-    geo_n            = shading::normalize(shading::cross(b - a, c - a));
+    World_tri const w  = world_triangle(s, hit_instance(s, p, path), id);
+    float2 const    uv = p.hit_uv[path];
+    pos                = (1.f - uv.x - uv.y) * w.a + uv.x * w.b + uv.y * w.c;
+    geo_n              = shading::normalize(shading::cross(w.b - w.a, w.c - w.a));
     wo               = -f3v(p.ray_d[path]);
     if (shading::dot(geo_n, wo) < 0.f) {
         geo_n = -geo_n;
@@ -1074,7 +1264,8 @@ __global__ void __launch_bounds__(256)
         uint32_t const id    = p.hit_id[path];
         uint32_t const depth = (p.info[path] >> 8) & 0xFFu;
         if (id != gpu::Miss && depth < wave.guide_depth &&
-            s.materials[s.tri_info[id].w].type == shading::Type_substitute) {
+            s.materials[world_triangle(s, hit_instance(s, p, path), id).material].type ==
+                shading::Type_substitute) {
             V3 pos, geo_n, wo;
             hit_frame(s, p, path, id, pos, geo_n, wo);
             guide::encode(box_coordinates(wave, pos), geo_n, wo, in);
@@ -1368,19 +1559,20 @@ __global__ void __launch_bounds__(Shade_block)
             if (m.medium != 0) {
                 float const srs = shading::similarity_relation_scale(m.g, depth);
                 scatter = track_grid(s.media[m.medium - 1], m, srs, f3v(ro), dir_in, ro.w,
-                                     p.hit_t[path], rng, t_sc, lw);
+                                     p.hit_t[path], rng, t_sc, lw, s.tracking_capped);
             } else if (m.emission.x > 0.f || m.emission.y > 0.f || m.emission.z > 0.f) {
                 // An emissive medium that is not a light: its emission reaches the camera
                 // segment only (pathtracer_mis.cpp:220-229 with connect_light_volume returning
                 // 0 for a non-light, pathtracer_mis.cpp:382-387).
                 V3        li;
-                int const ev = track_homogeneous_emissive(m, ro.w, p.hit_t[path], rng, t_sc, lw, li);
+                int const ev = track_homogeneous_emissive(m, ro.w, p.hit_t[path], rng, t_sc, lw, li,
+                                                          s.tracking_capped);
                 if (ev == 2 && depth == 0) {
                     L = L + T * li;
                 }
                 scatter = ev == 1;
             } else {
-                scatter = track_homogeneous(m, ro.w, p.hit_t[path], rng, t_sc, lw);
+                scatter = track_homogeneous(m, ro.w, p.hit_t[path], rng, t_sc, lw, s.tracking_capped);
             }
             T = T * lw;
             if (!(lw.x >= Abort_epsilon || lw.y >= Abort_epsilon || lw.z >= Abort_epsilon)) {
@@ -1436,20 +1628,20 @@ __global__ void __launch_bounds__(Shade_block)
                 extend = true;
             }
         } else if (!done) {
-            uint4 const  tri = s.tri_info[id];
-            V3 const     a   = f3v(s.positions[tri.x]);
-            V3 const     b   = f3v(s.positions[tri.y]);
-            V3 const     c   = f3v(s.positions[tri.z]);
+            uint32_t const inst = hit_instance(s, p, path);
+            V3             vn[3];
+            World_tri const wt = world_triangle(s, inst, id, vn);
+            V3 const     a   = wt.a;
+            V3 const     b   = wt.b;
+            V3 const     c   = wt.c;
             float2 const uv  = p.hit_uv[path];
             float const  bw  = 1.f - uv.x - uv.y;
             V3 const     pos = bw * a + uv.x * b + uv.y * c;
             V3           geo_n = shading::normalize(shading::cross(b - a, c - a));
-            V3 const     na  = f3v(s.normals[tri.x]);
-            V3 const     nb  = f3v(s.normals[tri.y]);
-            V3 const     nc  = f3v(s.normals[tri.z]);
-            V3           ns  = shading::normalize(bw * na + uv.x * nb + uv.y * nc);
+            V3           ns  = shading::normalize(bw * vn[0] + uv.x * vn[1] + uv.y * vn[2]);
             V3 const     wo  = -dir_in;
-            shading::Material const mat = s.materials[tri.w];
+            uint32_t const mat_id = wt.material;
+            shading::Material const mat = s.materials[mat_id];
             float const  cos_o = shading::dot(geo_n, wo);
             bool const   front = cos_o > 0.f;
             bool const   emits = mat.type == shading::Type_light;
@@ -1460,7 +1652,8 @@ __global__ void __launch_bounds__(Shade_block)
                     if (front || mat.two_sided) {
                         // only emitters registered as lights (su_create_light) are reached by
                         // a continuation ray; others are seen from the camera only
-                        uint32_t const order = s.light_order[id];
+                        uint32_t const lb    = s.inst_shade[inst].light_base;
+                        uint32_t const order = lb != 0xFFFFFFFFu ? s.light_order[lb + id] : 0xFFFFFFFFu;
                         float          w     = order != 0xFFFFFFFFu ? 1.f : 0.f;
                         if (!singular && order != 0xFFFFFFFFu) {
                             // the light-tree pick from the previous vertex (connect_light,
@@ -1498,7 +1691,7 @@ __global__ void __launch_bounds__(Shade_block)
                 // Null boundary of a medium: the ray continues unchanged past the hit, the
                 // medium changes (interface_change), depth and MIS state are kept
                 // (pathtracer_mis.cpp:180-205, Straight_transmission).
-                medium        = front ? tri.w + 1 : 0;
+                medium        = front ? mat_id + 1 : 0;
                 p.ray_o[path] = make_float4(ro.x, ro.y, ro.z, offset_f(p.hit_t[path]));
                 p.ray_d[path] = make_float4(rd.x, rd.y, rd.z, Ray_max_t);
                 ++vtx;
@@ -1522,13 +1715,28 @@ __global__ void __launch_bounds__(Shade_block)
                 float const gf     = !guided ? 0.f : (mat.metallic == 1.f ? wave.metal_fraction : wave.guide_fraction);
                 float4 const* const mix = reinterpret_cast<float4 const*>(p.guide_out + size_t(i) * Mixture_floats);
 
+                // The first vertices sample from the pixel's golden ratio sequences (batch
+                // rendering), the others from the path's random stream.
+                bool const     golden  = wave.golden_n != 0 && depth < Golden_bounces;
+                uint32_t const pixels  = (launch->cam.w + 2 * Film_border) * (launch->cam.h + 2 * Film_border);
+                uint32_t const gpixel  = path % pixels;
+                uint32_t const gsample = wave.first_sample + path / pixels;
+
                 // Next-event estimation (sample_lights / evaluate_light, pathtracer_mis.cpp:281-347).
                 int const samples = num_light_samples(s, depth);
                 V3 const  ps      = offset_ray(pos, geo_n);
                 for (int k = 0; k < samples; ++k) {
-                    float const  r  = rng.uniform();
-                    float const  r1 = rng.uniform();
-                    float const  r2 = rng.uniform();
+                    float r, r1, r2;
+                    if (golden) {
+                        r               = golden_1d(wave, gpixel, gsample, golden_light_1d(depth, k));
+                        float2 const g2 = golden_2d(wave, gpixel, gsample, golden_light_2d(depth, k));
+                        r1              = g2.x;
+                        r2              = g2.y;
+                    } else {
+                        r  = rng.uniform();
+                        r1 = rng.uniform();
+                        r2 = rng.uniform();
+                    }
                     Light_sample ls;
                     if (sample_light(s, ps, geo_n, false, r, r1, r2, ls, light_mode(samples, k))) {
                         shading::Bxdf const f =
@@ -1559,6 +1767,10 @@ __global__ void __launch_bounds__(Shade_block)
                     shading::Bxdf const f = shading::substitute_evaluate(mat, s.e_table, ctx, smp.wi);
                     smp.reflection        = f.reflection;
                     smp.pdf               = f.pdf;
+                } else if (golden) {
+                    float const  xl = golden_1d(wave, gpixel, gsample, golden_bsdf_1d(depth));
+                    float2 const x2 = golden_2d(wave, gpixel, gsample, golden_bsdf_2d(depth));
+                    smp = shading::substitute_sample(mat, s.e_table, ctx, xl, x2.x, x2.y);
                 } else {
                     float const xl = rng.uniform();
                     float const x0 = rng.uniform();
@@ -1619,6 +1831,7 @@ __global__ void __launch_bounds__(Shade_block)
 // ray (closest hits on boundary triangles only).  Homogeneous segments add their optical depth;
 // density-grid segments multiply in a ratio-tracking estimate (which uses the path's random
 // stream).  The light contribution, times the transmittance, is added to the path's radiance.
+template <bool Instances = false>
 __global__ void __launch_bounds__(Trace_block)
     k_transmit(Scene_gpu s, Paths p, uint32_t const* __restrict__ queue,
                uint32_t const* __restrict__ count, uint32_t* overflow) {
@@ -1642,11 +1855,15 @@ __global__ void __launch_bounds__(Trace_block)
     Rng            rng;
     uint2          stack[gpu::Stack_size];
     for (int crossing = 0; crossing < 64; ++crossing) {
-        gpu::Ray_state r;
-        gpu::Traversal tv;
+        gpu::Ray_state      r;
+        gpu::Traversal      tv;
+        gpu::Instance_state is;
         gpu::start_ray(r, tv, make_float4(ro.x, ro.y, ro.z, t0), rd);
-        while (!gpu::traversal_step<false, true>(r, tv, stack, s.nodes, s.tris, s.hit_margin,
-                                                 overflow, Class_surface)) {
+        if constexpr (Instances) {
+            gpu::start_instances(r, is);
+        }
+        while (!gpu::traversal_step<false, true, Instances>(r, tv, stack, s.nodes, s.tris, s.hit_margin,
+                                                            overflow, Class_surface, &is, s.inst_trace)) {
         }
         bool const  hit = r.best_id != gpu::Miss;
         float const end = hit ? r.tbest : rd.w;
@@ -1662,7 +1879,7 @@ __global__ void __launch_bounds__(Trace_block)
                 }
                 float const srs = shading::similarity_relation_scale(m.g, depth);
                 if (!transmit_grid(s.media[m.medium - 1], m, srs, f3v(ro), f3v(rd), t0, end, rng,
-                                   w)) {
+                                   w, s.tracking_capped)) {
                     blocked = true;
                     break;
                 }
@@ -1674,10 +1891,9 @@ __global__ void __launch_bounds__(Trace_block)
         if (!hit) {
             break;
         }
-        uint4 const tri = s.tri_info[r.best_id];
-        V3 const    a   = f3v(s.positions[tri.x]);
-        V3 const    geo = shading::cross(f3v(s.positions[tri.y]) - a, f3v(s.positions[tri.z]) - a);
-        medium          = shading::dot(geo, v3(rd.x, rd.y, rd.z)) < 0.f ? tri.w + 1 : 0;
+        World_tri const wt  = world_triangle(s, Instances ? is.best_inst : 0u, r.best_id);
+        V3 const        geo = shading::cross(wt.b - wt.a, wt.c - wt.a);
+        medium              = shading::dot(geo, v3(rd.x, rd.y, rd.z)) < 0.f ? wt.material + 1 : 0;
         t0              = offset_f(r.tbest);
         if (t0 >= rd.w) {
             break;
@@ -1841,6 +2057,14 @@ struct Renderer::Device {
     uint32_t*          light_order = nullptr;
     float*             e_table    = nullptr;
     Medium_gpu*        media      = nullptr;
+    gpu::Instance_trace* inst_trace     = nullptr;
+    Instance_shade*      inst_shade     = nullptr;
+    uint32_t*            inst_materials = nullptr;
+    bool                 instanced      = false;  // two-level trees
+    uint32_t             per_sm_flat    = 1;      // traversal blocks per SM (occupancy), flat trees
+    uint32_t             per_sm_inst    = 1;      // ... two-level trees
+    uint32_t*            golden_sorted  = nullptr;  // frac(j / phi) * 2^32, j < golden_n, ascending
+    uint32_t             golden_n       = 0;
     std::vector<float*>  grid_density;  // one per density grid
     std::vector<float2*> grid_cells;
     uint32_t           num_lights = 0;
@@ -2022,6 +2246,10 @@ Renderer::Renderer() : d_(new Device) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace<false>, Trace_block, 0);
+    int per_sm_inst = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_inst, k_trace<false, false, true>, Trace_block, 0);
+    d_->per_sm_flat = uint32_t(std::max(1, per_sm));
+    d_->per_sm_inst = uint32_t(std::max(1, per_sm_inst));
     d_->trace_grid = std::max(1, per_sm) * std::max(1, sms);
     d_->sms        = uint32_t(std::max(1, sms));
     d_->tuner.reset(uint32_t(std::max(1, per_sm)));
@@ -2050,11 +2278,16 @@ Renderer::~Renderer() {
     free_ptr(d_->light_tris);
     free_ptr(d_->light_order);
     free_ptr(d_->e_table);
+    free_ptr(d_->inst_trace);
+    free_ptr(d_->inst_shade);
+    free_ptr(d_->inst_materials);
+    free_ptr(d_->golden_sorted);
     free_grids();
     Paths& p = d_->paths;
     free_ptr(p.ray_o);
     free_ptr(p.ray_d);
     free_ptr(p.hit_id);
+    free_ptr(p.hit_inst);
     free_ptr(p.hit_t);
     free_ptr(p.hit_uv);
     free_ptr(p.T);
@@ -2124,59 +2357,64 @@ int32_t Renderer::fail_cuda(char const* what, int code) {
 
 int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     clear_graphs();
-    uint32_t const nv = uint32_t(scene.positions.size() / 3);
-    uint32_t const nt = uint32_t(scene.indices.size() / 3);
-    if (nt == 0) {
+    if (scene.instances.empty()) {
         error_ = "scene has no triangles";
         return SPB_ERROR_STATE;
     }
-    // Triangles of medium boundaries get their own class so shadow rays can pass them.
-    std::vector<uint32_t> tri_class(nt, Class_surface);
-    d_->tuner.reset(d_->tuner.max_per_sm);  // a new scene is tuned anew
-    d_->has_media = false;
-    for (uint32_t t = 0; t < nt; ++t) {
-        if (scene.materials[scene.tri_material[t]].type == shading::Type_volume) {
-            tri_class[t]  = Class_boundary;
-            d_->has_media = true;
+    for (Instance_desc const& in : scene.instances) {
+        if (in.mesh >= scene.meshes.size() || scene.meshes[in.mesh].indices.empty()) {
+            error_ = "instance of a missing or empty mesh";
+            return SPB_ERROR_ARGUMENT;
         }
     }
-    Wide_bvh    bvh;
-    std::string err;
-    if (!build_wide_bvh(nv, nt, scene.positions.data(), scene.indices.data(), num_threads, bvh,
-                        err, tri_class.data())) {
-        error_ = "BVH build: " + err;
+    auto const material_of = [&](Instance_desc const& in, uint32_t slot) {
+        uint32_t const m = slot < in.materials.size() ? in.materials[slot] : in.fallback;
+        return m < scene.materials.size() ? m : in.fallback;
+    };
+    // Two levels when flattening would multiply the distinct meshes' triangles (unless the
+    // scene's "instancing" setting decides).
+    uint64_t              flat_tris = 0;
+    uint64_t              mesh_tris = 0;
+    std::vector<uint32_t> uses(scene.meshes.size(), 0);
+    for (Instance_desc const& in : scene.instances) {
+        flat_tris += scene.meshes[in.mesh].indices.size() / 3;
+        if (uses[in.mesh]++ == 0) {
+            mesh_tris += scene.meshes[in.mesh].indices.size() / 3;
+        }
+    }
+    bool const two_level = scene.instancing == 1 ||
+                           (scene.instancing < 0 && flat_tris > 4 * mesh_tris && flat_tris > (1u << 20));
+    if (flat_tris >= (1ull << 32)) {
+        error_ = "scene has too many triangles";
         return SPB_ERROR_ARGUMENT;
     }
-    cudaDeviceSynchronize();
-    SPB_RCUDA(upload(d_->nodes, bvh.nodes.data(), bvh.nodes.size() * sizeof(Wide_node)));
-    SPB_RCUDA(upload(d_->tris, bvh.triangles.data(), bvh.triangles.size() * sizeof(Wide_triangle)));
-    d_->hit_margin = bvh.hit_margin;
+    d_->instanced = two_level;
+    // A new scene is tuned anew, at the occupancy of the traversal it uses.
+    d_->tuner.reset(two_level ? d_->per_sm_inst : d_->per_sm_flat);
+    d_->has_media = false;
 
-    std::vector<uint4> info(nt);
-    for (uint32_t t = 0; t < nt; ++t) {
-        info[t] = make_uint4(scene.indices[3 * t], scene.indices[3 * t + 1], scene.indices[3 * t + 2],
-                             scene.tri_material[t]);
-    }
-    std::vector<float4> pos(nv), nrm(nv);
-    for (uint32_t v = 0; v < nv; ++v) {
-        pos[v] = make_float4(scene.positions[3 * v], scene.positions[3 * v + 1],
-                             scene.positions[3 * v + 2], 0.f);
-        nrm[v] = make_float4(scene.normals[3 * v], scene.normals[3 * v + 1], scene.normals[3 * v + 2],
-                             0.f);
-    }
+    std::vector<Wide_node>           nodes;
+    std::vector<Wide_triangle>       tris;
+    std::vector<uint4>               info;    // per triangle: vertices, material slot
+    std::vector<float4>              pos;     // object space (world space when flattened)
+    std::vector<float4>              nrm;
+    std::vector<uint32_t>            inst_materials;
+    std::vector<Instance_shade>      shade;
+    std::vector<gpu::Instance_trace> trace;
+    std::vector<Light_input>         emitters;
+    uint32_t                         light_slots = 0;
+    double                           lo[3] = {1e300, 1e300, 1e300};
+    double                           hi[3] = {-1e300, -1e300, -1e300};
+    uint64_t                         device_triangles = 0;
 
-    // Lights: every triangle of a light prop whose material emits, in a light tree.
-    std::vector<Light_input> emitters;
-    for (uint32_t t = 0; t < nt; ++t) {
-        shading::Material const& m = scene.materials[scene.tri_material[t]];
-        if (!scene.tri_light[t] || m.type != shading::Type_light) {
-            continue;
-        }
+    // An emissive triangle of a light prop, with its world-space vertices.
+    auto const add_emitter = [&](double const a[3], double const b[3], double const c[3],
+                                 shading::Material const& m, uint32_t slot, uint32_t material) {
         Light_input li;
         for (int k = 0; k < 3; ++k) {
-            li.a[k] = scene.positions[3 * scene.indices[3 * t] + k];
-            li.b[k] = scene.positions[3 * scene.indices[3 * t + 1] + k];
-            li.c[k] = scene.positions[3 * scene.indices[3 * t + 2] + k];
+            li.a[k] = a[k];
+            li.b[k] = b[k];
+            li.c[k] = c[k];
         }
         double const e1[3] = {li.b[0] - li.a[0], li.b[1] - li.a[1], li.b[2] - li.a[2]};
         double const e2[3] = {li.c[0] - li.a[0], li.c[1] - li.a[1], li.c[2] - li.a[2]};
@@ -2185,29 +2423,293 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
         double const cz    = e1[0] * e2[1] - e1[1] * e2[0];
         double const area  = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
         li.two_sided       = m.two_sided != 0;
-        li.power = area * (double(m.emission.x) + m.emission.y + m.emission.z) / 3.0 *
-                   (li.two_sided ? 2.0 : 1.0);
-        li.tri = t;
+        li.power = area * (double(m.emission.x) + m.emission.y + m.emission.z) / 3.0 * (li.two_sided ? 2.0 : 1.0);
+        li.slot     = slot;
+        li.material = material;
         if (area > 0.0 && li.power > 0.0) {
             emitters.push_back(li);
         }
+    };
+    auto const grow = [&](double const p[3]) {
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], p[k]);
+            hi[k] = std::max(hi[k], p[k]);
+        }
+    };
+
+    if (!two_level) {
+        // Every instance flattened into world space (one tree); shading sees one identity
+        // instance whose material slots are the materials themselves.
+        std::vector<float>    wpos;
+        std::vector<uint32_t> windex;
+        std::vector<uint32_t> tri_class;
+        for (Instance_desc const& in : scene.instances) {
+            Mesh_desc const& mesh = scene.meshes[in.mesh];
+            uint32_t const   base = uint32_t(wpos.size() / 3);
+            float const*     m    = in.trafo;
+            float const*     rot  = in.rotation;
+            for (size_t v = 0; v < mesh.positions.size() / 3; ++v) {
+                float const x = mesh.positions[3 * v];
+                float const y = mesh.positions[3 * v + 1];
+                float const z = mesh.positions[3 * v + 2];
+                // row vector times matrix: p' = x * row0 + y * row1 + z * row2 + row3
+                float const wx = x * m[0] + y * m[4] + z * m[8] + m[12];
+                float const wy = x * m[1] + y * m[5] + z * m[9] + m[13];
+                float const wz = x * m[2] + y * m[6] + z * m[10] + m[14];
+                wpos.push_back(wx);
+                wpos.push_back(wy);
+                wpos.push_back(wz);
+                pos.push_back(make_float4(wx, wy, wz, 0.f));
+                float const nx = mesh.normals[3 * v];
+                float const ny = mesh.normals[3 * v + 1];
+                float const nz = mesh.normals[3 * v + 2];
+                nrm.push_back(make_float4(nx * rot[0] + ny * rot[3] + nz * rot[6], nx * rot[1] + ny * rot[4] + nz * rot[7],
+                                          nx * rot[2] + ny * rot[5] + nz * rot[8], 0.f));
+                double const wp[3] = {wx, wy, wz};
+                grow(wp);
+            }
+            for (size_t t = 0; t < mesh.indices.size() / 3; ++t) {
+                uint32_t const mat = material_of(in, mesh.tri_slot[t]);
+                uint32_t const v[3] = {base + mesh.indices[3 * t], base + mesh.indices[3 * t + 1],
+                                       base + mesh.indices[3 * t + 2]};
+                uint32_t const global = uint32_t(info.size());
+                info.push_back(make_uint4(v[0], v[1], v[2], mat));
+                windex.insert(windex.end(), v, v + 3);
+                shading::Material const& sm = scene.materials[mat];
+                bool const volume = sm.type == shading::Type_volume;
+                d_->has_media |= volume;
+                tri_class.push_back(volume ? Class_boundary : Class_surface);
+                if (in.light && sm.type == shading::Type_light) {
+                    double a[3], b[3], c[3];
+                    for (int k = 0; k < 3; ++k) {
+                        a[k] = wpos[3 * size_t(v[0]) + k];
+                        b[k] = wpos[3 * size_t(v[1]) + k];
+                        c[k] = wpos[3 * size_t(v[2]) + k];
+                    }
+                    add_emitter(a, b, c, sm, global, mat);
+                }
+            }
+        }
+        Wide_bvh    bvh;
+        std::string err;
+        if (!build_wide_bvh(uint32_t(pos.size()), uint32_t(info.size()), wpos.data(), windex.data(), num_threads,
+                            bvh, err, tri_class.data())) {
+            error_ = "BVH build: " + err;
+            return SPB_ERROR_ARGUMENT;
+        }
+        nodes          = std::move(bvh.nodes);
+        tris           = std::move(bvh.triangles);
+        d_->hit_margin = bvh.hit_margin;
+        Instance_shade id{};
+        id.o2w[0] = make_float4(1.f, 0.f, 0.f, 0.f);
+        id.o2w[1] = make_float4(0.f, 1.f, 0.f, 0.f);
+        id.o2w[2] = make_float4(0.f, 0.f, 1.f, 0.f);
+        id.nrm[0] = id.o2w[0];
+        id.nrm[1] = id.o2w[1];
+        id.nrm[2] = id.o2w[2];
+        shade.push_back(id);
+        inst_materials.resize(scene.materials.size());
+        for (uint32_t k = 0; k < inst_materials.size(); ++k) {
+            inst_materials[k] = k;
+        }
+        light_slots      = uint32_t(info.size());
+        device_triangles = info.size();
+    } else {
+        // One tree per (mesh, per-triangle class) in object space, a top-level tree over the
+        // instances' world boxes.
+        struct Blas {
+            std::vector<Wide_node>     nodes;
+            std::vector<Wide_triangle> tris;
+            float                      margin;
+            uint32_t                   depth;
+            uint32_t                   node_off = 0;
+            uint32_t                   tri_off  = 0;
+        };
+        std::vector<Blas>                                      blases;
+        std::map<std::pair<uint32_t, std::vector<uint32_t>>, uint32_t> blas_of;
+        std::vector<uint32_t>                                  inst_blas(scene.instances.size());
+        std::vector<uint32_t>                                  mesh_vbase(scene.meshes.size(), 0xFFFFFFFFu);
+        std::vector<uint32_t>                                  mesh_tbase(scene.meshes.size(), 0);
+        std::vector<float>                                     boxes(6 * scene.instances.size());
+        for (size_t i = 0; i < scene.instances.size(); ++i) {
+            Instance_desc const& in   = scene.instances[i];
+            Mesh_desc const&     mesh = scene.meshes[in.mesh];
+            uint32_t const       nt   = uint32_t(mesh.indices.size() / 3);
+            if (mesh_vbase[in.mesh] == 0xFFFFFFFFu) {
+                mesh_vbase[in.mesh] = uint32_t(pos.size());
+                mesh_tbase[in.mesh] = uint32_t(info.size());
+                for (size_t v = 0; v < mesh.positions.size() / 3; ++v) {
+                    pos.push_back(make_float4(mesh.positions[3 * v], mesh.positions[3 * v + 1], mesh.positions[3 * v + 2], 0.f));
+                    nrm.push_back(make_float4(mesh.normals[3 * v], mesh.normals[3 * v + 1], mesh.normals[3 * v + 2], 0.f));
+                }
+                uint32_t const vb = mesh_vbase[in.mesh];
+                for (uint32_t t = 0; t < nt; ++t) {
+                    info.push_back(make_uint4(vb + mesh.indices[3 * t], vb + mesh.indices[3 * t + 1],
+                                              vb + mesh.indices[3 * t + 2], mesh.tri_slot[t]));
+                }
+            }
+            std::vector<uint32_t> cls(nt);
+            uint32_t              max_slot = 0;
+            for (uint32_t t = 0; t < nt; ++t) {
+                bool const volume = scene.materials[material_of(in, mesh.tri_slot[t])].type == shading::Type_volume;
+                d_->has_media |= volume;
+                cls[t]   = volume ? Class_boundary : Class_surface;
+                max_slot = std::max(max_slot, mesh.tri_slot[t]);
+            }
+            auto key = std::make_pair(in.mesh, cls);
+            auto it  = blas_of.find(key);
+            if (it == blas_of.end()) {
+                Wide_bvh    bvh;
+                std::string err;
+                if (!build_wide_bvh(uint32_t(mesh.positions.size() / 3), nt, mesh.positions.data(),
+                                    mesh.indices.data(), num_threads, bvh, err, cls.data())) {
+                    error_ = "BVH build: " + err;
+                    return SPB_ERROR_ARGUMENT;
+                }
+                Blas b;
+                b.nodes  = std::move(bvh.nodes);
+                b.tris   = std::move(bvh.triangles);
+                b.margin = bvh.hit_margin;
+                b.depth  = bvh.max_depth;
+                it       = blas_of.emplace(std::move(key), uint32_t(blases.size())).first;
+                blases.push_back(std::move(b));
+            }
+            inst_blas[i] = it->second;
+
+            // Maps: object -> world (row vectors times trafo), its inverse, the normals' rotation.
+            float const* m = in.trafo;
+            double       L[3][3], tr[3];
+            for (int r = 0; r < 3; ++r) {
+                for (int c = 0; c < 3; ++c) {
+                    L[r][c] = m[4 * r + c];
+                }
+                tr[r] = m[12 + r];
+            }
+            double const det = L[0][0] * (L[1][1] * L[2][2] - L[1][2] * L[2][1]) -
+                               L[0][1] * (L[1][0] * L[2][2] - L[1][2] * L[2][0]) +
+                               L[0][2] * (L[1][0] * L[2][1] - L[1][1] * L[2][0]);
+            if (!(std::fabs(det) > 1e-30)) {
+                error_ = "instance with a singular transformation";
+                return SPB_ERROR_ARGUMENT;
+            }
+            double Li[3][3];  // inverse of L
+            Li[0][0] = (L[1][1] * L[2][2] - L[1][2] * L[2][1]) / det;
+            Li[0][1] = (L[0][2] * L[2][1] - L[0][1] * L[2][2]) / det;
+            Li[0][2] = (L[0][1] * L[1][2] - L[0][2] * L[1][1]) / det;
+            Li[1][0] = (L[1][2] * L[2][0] - L[1][0] * L[2][2]) / det;
+            Li[1][1] = (L[0][0] * L[2][2] - L[0][2] * L[2][0]) / det;
+            Li[1][2] = (L[0][2] * L[1][0] - L[0][0] * L[1][2]) / det;
+            Li[2][0] = (L[1][0] * L[2][1] - L[1][1] * L[2][0]) / det;
+            Li[2][1] = (L[0][1] * L[2][0] - L[0][0] * L[2][1]) / det;
+            Li[2][2] = (L[0][0] * L[1][1] - L[0][1] * L[1][0]) / det;
+            // world_j = sum_i object_i L[i][j] + tr_j; object_k = sum_j Li[j][k] (world_j - tr_j)
+            gpu::Instance_trace it_rec{};
+            Instance_shade      sh{};
+            for (int k = 0; k < 3; ++k) {
+                double const off = -(Li[0][k] * tr[0] + Li[1][k] * tr[1] + Li[2][k] * tr[2]);
+                it_rec.w2o[k]    = make_float4(float(Li[0][k]), float(Li[1][k]), float(Li[2][k]), float(off));
+                sh.o2w[k]        = make_float4(m[k], m[4 + k], m[8 + k], m[12 + k]);
+                sh.nrm[k]        = make_float4(in.rotation[k], in.rotation[3 + k], in.rotation[6 + k], 0.f);
+            }
+            it_rec.hit_margin = blases[inst_blas[i]].margin;
+            trace.push_back(it_rec);
+            sh.tri_base = mesh_tbase[in.mesh];
+            sh.mat_base = uint32_t(inst_materials.size());
+            for (uint32_t k = 0; k <= max_slot; ++k) {
+                inst_materials.push_back(material_of(in, k));
+            }
+            sh.light_base = 0xFFFFFFFFu;
+            bool const emits = in.light && std::any_of(mesh.tri_slot.begin(), mesh.tri_slot.end(), [&](uint32_t k) {
+                                   return scene.materials[material_of(in, k)].type == shading::Type_light;
+                               });
+            if (emits) {
+                sh.light_base = light_slots;
+                light_slots += nt;
+            }
+            shade.push_back(sh);
+
+            // World box of the instance (its transformed vertices) and its emitters.
+            std::vector<double> wv(mesh.positions.size());
+            double blo[3] = {1e300, 1e300, 1e300}, bhi[3] = {-1e300, -1e300, -1e300};
+            for (size_t v = 0; v < mesh.positions.size() / 3; ++v) {
+                double const x = mesh.positions[3 * v], y = mesh.positions[3 * v + 1], z = mesh.positions[3 * v + 2];
+                for (int k = 0; k < 3; ++k) {
+                    wv[3 * v + k] = x * L[0][k] + y * L[1][k] + z * L[2][k] + tr[k];
+                    blo[k]        = std::min(blo[k], wv[3 * v + k]);
+                    bhi[k]        = std::max(bhi[k], wv[3 * v + k]);
+                }
+                grow(&wv[3 * v]);
+            }
+            for (int k = 0; k < 3; ++k) {
+                boxes[6 * i + k]     = std::nextafter(float(blo[k]), -INFINITY);
+                boxes[6 * i + 3 + k] = std::nextafter(float(bhi[k]), INFINITY);
+            }
+            if (emits) {
+                for (uint32_t t = 0; t < nt; ++t) {
+                    uint32_t const           mat = material_of(in, mesh.tri_slot[t]);
+                    shading::Material const& sm  = scene.materials[mat];
+                    if (sm.type == shading::Type_light) {
+                        add_emitter(&wv[3 * size_t(mesh.indices[3 * t])], &wv[3 * size_t(mesh.indices[3 * t + 1])],
+                                    &wv[3 * size_t(mesh.indices[3 * t + 2])], sm, sh.light_base + t, mat);
+                    }
+                }
+            }
+        }
+        Wide_bvh    top;
+        std::string err;
+        if (!build_wide_instances(uint32_t(scene.instances.size()), boxes.data(), Class_instance, num_threads, top,
+                                  err)) {
+            error_ = "top-level tree: " + err;
+            return SPB_ERROR_ARGUMENT;
+        }
+        uint32_t deepest = 0;
+        nodes            = std::move(top.nodes);
+        tris             = std::move(top.triangles);
+        for (Blas& b : blases) {
+            b.node_off = uint32_t(nodes.size());
+            b.tri_off  = uint32_t(tris.size());
+            for (Wide_node n : b.nodes) {
+                n.child_base += b.node_off;
+                n.tri_base += b.tri_off;
+                nodes.push_back(n);
+            }
+            tris.insert(tris.end(), b.tris.begin(), b.tris.end());
+            deepest = std::max(deepest, b.depth);
+            device_triangles += b.tris.size();
+        }
+        if (top.max_depth + deepest + 2 > Max_wide_depth) {
+            error_ = "top-level and instance trees together deeper than the traversal stack";
+            return SPB_ERROR_ARGUMENT;
+        }
+        for (size_t i = 0; i < scene.instances.size(); ++i) {
+            trace[i].root = blases[inst_blas[i]].node_off;
+        }
+        d_->hit_margin = top.hit_margin;
     }
+    stats_.instances        = two_level ? uint32_t(scene.instances.size()) : 0u;
+    stats_.device_triangles = device_triangles;
+    instances_        = stats_.instances;
+    device_triangles_ = device_triangles;
+
+    cudaDeviceSynchronize();
+    SPB_RCUDA(upload(d_->nodes, nodes.data(), nodes.size() * sizeof(Wide_node)));
+    SPB_RCUDA(upload(d_->tris, tris.data(), tris.size() * sizeof(Wide_triangle)));
+    SPB_RCUDA(upload(d_->inst_shade, shade.data(), shade.size() * sizeof(Instance_shade)));
+    SPB_RCUDA(upload(d_->inst_materials, inst_materials.data(), inst_materials.size() * sizeof(uint32_t)));
+    free_ptr(d_->inst_trace);
+    if (!trace.empty()) {
+        SPB_RCUDA(upload(d_->inst_trace, trace.data(), trace.size() * sizeof(gpu::Instance_trace)));
+    }
+
     Light_tree tree;
-    build_light_tree(emitters, nt, tree);
+    build_light_tree(emitters, std::max(light_slots, 1u), tree);
     d_->num_lights = tree.num_lights;
 
     // Scene box for the guide's position encoding; a new scene starts a new guide.
     {
-        float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
-        for (uint32_t v = 0; v < nv; ++v) {
-            for (int k = 0; k < 3; ++k) {
-                lo[k] = std::min(lo[k], scene.positions[3 * v + k]);
-                hi[k] = std::max(hi[k], scene.positions[3 * v + k]);
-            }
-        }
-        d_->bounds_lo  = make_float4(lo[0], lo[1], lo[2], 0.f);
-        d_->bounds_inv = make_float4(1.f / std::max(hi[0] - lo[0], 1e-6f), 1.f / std::max(hi[1] - lo[1], 1e-6f),
-                                     1.f / std::max(hi[2] - lo[2], 1e-6f), 0.f);
+        d_->bounds_lo  = make_float4(float(lo[0]), float(lo[1]), float(lo[2]), 0.f);
+        d_->bounds_inv = make_float4(1.f / std::max(float(hi[0] - lo[0]), 1e-6f), 1.f / std::max(float(hi[1] - lo[1]), 1e-6f),
+                                     1.f / std::max(float(hi[2] - lo[2]), 1e-6f), 0.f);
         d_->net_ready  = false;
     }
 
@@ -2217,13 +2719,6 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     float const* env = scene.environment;
     d_->env          = make_float4(env[0], env[1], env[2], 0.f);
     if (scene.environment_light && (env[0] > 0.f || env[1] > 0.f || env[2] > 0.f)) {
-        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-        for (uint32_t v = 0; v < nv; ++v) {
-            for (int k = 0; k < 3; ++k) {
-                lo[k] = std::min(lo[k], double(scene.positions[3 * v + k]));
-                hi[k] = std::max(hi[k], double(scene.positions[3 * v + k]));
-            }
-        }
         double ext2 = 0.0;
         for (int k = 0; k < 3; ++k) {
             ext2 += (hi[k] - lo[k]) * (hi[k] - lo[k]);
@@ -2337,6 +2832,7 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     free_ptr(p.ray_o);
     free_ptr(p.ray_d);
     free_ptr(p.hit_id);
+    free_ptr(p.hit_inst);
     free_ptr(p.hit_t);
     free_ptr(p.hit_uv);
     free_ptr(p.T);
@@ -2366,6 +2862,7 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     SPB_RCUDA(dev_malloc(&p.ray_o, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&p.ray_d, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&p.hit_id, n * sizeof(uint32_t)));
+    SPB_RCUDA(dev_malloc(&p.hit_inst, n * sizeof(uint32_t)));
     SPB_RCUDA(dev_malloc(&p.hit_t, n * sizeof(float)));
     SPB_RCUDA(dev_malloc(&p.hit_uv, n * sizeof(float2)));
     SPB_RCUDA(dev_malloc(&p.T, n * sizeof(float4)));
@@ -2550,6 +3047,17 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     uint32_t const max_wave = wave_spp(max_paths);
     // while the guide trains, passes of guide_pass_spp with training steps in between
     uint32_t const train_wave = std::max(1u, std::min(max_wave, settings_.guide_pass_spp));
+    // Golden ratio sequences over the frame's samples (first_sample + num_samples per pixel).
+    uint32_t const golden_n = settings_.golden_ratio ? first_sample + num_samples : 0u;
+    if (golden_n != 0 && golden_n != d_->golden_n) {
+        std::vector<uint32_t> sorted(golden_n);
+        for (uint32_t j = 0; j < golden_n; ++j) {
+            sorted[j] = j * 2654435769u;
+        }
+        std::sort(sorted.begin(), sorted.end());
+        SPB_RCUDA(upload(d_->golden_sorted, sorted.data(), sorted.size() * sizeof(uint32_t)));
+        d_->golden_n = golden_n;
+    }
     if (int32_t const st = ensure_buffers(max_wave * pixels)) {
         return st;
     }
@@ -2588,6 +3096,11 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     sg.env           = d_->env;
     sg.e_table       = d_->e_table;
     sg.media         = d_->media;
+    sg.inst_trace     = d_->inst_trace;
+    sg.inst_shade     = d_->inst_shade;
+    sg.inst_materials = d_->inst_materials;
+    sg.instanced      = d_->instanced ? 1u : 0u;
+    sg.tracking_capped = d_->counters + Overflow_slot + 2;
 
     cudaStream_t const st = d_->stream;
     uint32_t* const    ctr = d_->counters;
@@ -2598,7 +3111,9 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     uint32_t const bounce_iterations = settings_.max_bounces + 1;
     uint32_t const max_iterations = d_->has_media ? Max_bounce_slots - 1 : bounce_iterations;
 
-    stats_ = Stats();
+    stats_                  = Stats();
+    stats_.instances        = instances_;
+    stats_.device_triangles = device_triangles_;
     std::vector<uint32_t> host_ctr(Counter_words);
     // Device time of the guide's stages: event pairs (inference after each trace, training
     // after each pass), summed after each wave.
@@ -2642,7 +3157,12 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             uint32_t* const q_in  = d_->queue[b & 1];
             uint32_t* const q_out = d_->queue[(b + 1) & 1];
             uint32_t* const c     = ctr + Counter_stride * b;
-            k_trace<false><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, q_in, c, c + 2, ctr + Overflow_slot);
+            if (d_->instanced) {
+                k_trace<false, false, true><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, q_in, c, c + 2,
+                                                                               ctr + Overflow_slot);
+            } else {
+                k_trace<false><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, q_in, c, c + 2, ctr + Overflow_slot);
+            }
             // (without media a vertex's depth is the iteration; with media it can be less)
             if (guided_at(b)) {
                 SPB_RCUDA(record(guide_event(events++), capture));
@@ -2653,11 +3173,19 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             }
             k_shade<<<(paths + Shade_block - 1) / Shade_block, Shade_block, 0, st>>>(
                 sg, d_->launch_dev, d_->paths, q_in, c, q_out, c + Counter_stride, d_->shadow_queue, c + 1);
-            if (d_->has_media) {
+            if (d_->has_media && d_->instanced) {
+                k_trace<true, true, true><<<trace_grid, Trace_block, 0, st>>>(
+                    sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot, d_->transmit_queue, c + 4);
+                k_transmit<true><<<(2 * paths + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
+                    sg, d_->paths, d_->transmit_queue, c + 4, ctr + Overflow_slot);
+            } else if (d_->has_media) {
                 k_trace<true, true><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->shadow_queue, c + 1, c + 3,
                                                                        ctr + Overflow_slot, d_->transmit_queue, c + 4);
-                k_transmit<<<(2 * paths + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
+                k_transmit<false><<<(2 * paths + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
                     sg, d_->paths, d_->transmit_queue, c + 4, ctr + Overflow_slot);
+            } else if (d_->instanced) {
+                k_trace<true, false, true><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->shadow_queue, c + 1,
+                                                                              c + 3, ctr + Overflow_slot);
             } else {
                 k_trace<true><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->shadow_queue, c + 1, c + 3,
                                                                   ctr + Overflow_slot);
@@ -2705,6 +3233,8 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         wave.record_depth   = training ? settings_.record_depth : 0u;
         wave.bounds_lo      = d_->bounds_lo;
         wave.bounds_inv     = d_->bounds_inv;
+        wave.golden_n       = golden_n;
+        wave.golden_sorted  = d_->golden_sorted;
         // The previous wave has completed (synchronized below), so the pinned block is free.
         d_->launch_host->cam  = cam;
         d_->launch_host->wave = wave;
@@ -2783,6 +3313,7 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             }
         }
         stats_.overflow += host_ctr[Overflow_slot];
+        stats_.tracking_capped += host_ctr[Overflow_slot + 2];
         if (host_ctr[Overflow_slot + 1]) {
             error_ = "path guiding: a tensor-core completion wait ran out";
             return SPB_ERROR_CUDA;

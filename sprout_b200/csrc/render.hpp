@@ -25,18 +25,41 @@ struct Grid_medium {
     float    world_to_uvw[12] = {};   // rows: uvw_k = dot(row_k.xyz, p) + row_k.w
 };
 
-// World-space scene as the host engine flattens it (one BVH over all props' triangles).
+// A mesh in object space, shared by the instances that place it.
+struct Mesh_desc {
+    std::vector<float>    positions;  // 3 per vertex
+    std::vector<float>    normals;    // 3 per vertex (shading)
+    std::vector<uint32_t> indices;    // 3 per triangle
+    std::vector<uint32_t> tri_slot;   // material slot per triangle
+};
+
+// A prop: a mesh placed by a row-major object-to-world matrix (translation in the last row, as
+// su_entity_set_transformation takes it; points are row vectors times the matrix), the
+// rotation its normals turn by, its materials per slot, and whether it is a light.
+struct Instance_desc {
+    uint32_t              mesh      = 0;
+    float                 trafo[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+    float                 rotation[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};  // row-major, normals as row vectors
+    std::vector<uint32_t> materials;  // slot -> index into Scene_desc::materials
+    uint32_t              fallback  = 0;  // material of slots beyond `materials`
+    bool                  light     = false;
+};
+
+// The scene as the host engine collects it (prop_bvh_wrapper.cpp, prop.cpp: props placing
+// shapes).  The renderer either flattens every instance into one world-space tree, or -- when
+// props share meshes enough for it to pay -- keeps one tree per mesh in object space under a
+// top-level tree over the instances (instancing).
 struct Scene_desc {
-    std::vector<float>              positions;     // 3 per vertex, world space
-    std::vector<float>              normals;       // 3 per vertex, world space (shading)
-    std::vector<uint32_t>           indices;       // 3 per triangle
-    std::vector<uint32_t>           tri_material;  // per triangle, index into materials
-    std::vector<uint8_t>            tri_light;     // per triangle: 1 if it belongs to a light prop
+    std::vector<Mesh_desc>          meshes;
+    std::vector<Instance_desc>      instances;
     std::vector<shading::Material>  materials;    // Volume materials: medium = 1 + grid medium
     std::vector<Density_grid>       grids;
     std::vector<Grid_medium>        media;
     float                           environment[3] = {0.f, 0.f, 0.f};  // uniform radiance at infinity
     bool                            environment_light = false;  // also sampled by next-event estimation
+    // Two-level trees: -1 when flattening would hold more than four times the triangles of the
+    // distinct meshes and over a million triangles; 0 never; 1 always.
+    int                             instancing = -1;
 };
 
 struct Camera_desc {
@@ -51,6 +74,9 @@ struct Settings {
     uint32_t min_bounces = 4;   // Russian roulette starts here
     uint32_t max_bounces = 8;
     uint32_t seed        = 0;
+    // Golden ratio sequences for the camera and the first three vertices of a frame rendered in
+    // one call (the reference's batch mode); false: independent random samples (progressive).
+    bool     golden_ratio = false;
     // Learned path guiding (no counterpart in the reference): at surface vertices the
     // continuation direction comes from the network's vMF mixture with probability
     // guide_fraction, else from the BSDF (one-sample MIS of the two).  The network is trained
@@ -88,6 +114,9 @@ struct Stats {
     uint32_t wave_paths              = 0;    // largest wave of the call (paths)
     uint32_t trace_blocks_per_sm     = 0;    // traversal blocks per SM of its last wave
     uint32_t graph_waves             = 0;    // waves replayed from a captured CUDA graph
+    uint32_t instances               = 0;    // instances under a top-level tree (0: flattened)
+    uint64_t device_triangles        = 0;    // triangles in the uploaded trees
+    uint32_t tracking_capped         = 0;    // medium tracking segments cut at their step cap
 };
 
 class Renderer {
@@ -121,6 +150,8 @@ class Renderer {
     Settings    settings_;
     Camera_desc camera_;
     Stats       stats_;
+    uint32_t    instances_        = 0;  // of the uploaded scene (Stats::instances)
+    uint64_t    device_triangles_ = 0;
     bool        scene_ready_  = false;
     bool        camera_ready_ = false;
     std::string error_;

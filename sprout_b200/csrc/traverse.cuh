@@ -250,20 +250,94 @@ __device__ __forceinline__ void start_ray(Ray_state& r, Traversal& tv, float4 ro
     tv.sp            = 0;
 }
 
+// ---- two-level traversal (instancing) ----
+// The top-level tree's leaf records are instances (Wide_triangle::id = instance index).  A lane
+// reaching one pushes what is left of its top-level traversal (pending node group, then pending
+// leaves), transforms its ray into the instance's object space -- the direction by the linear
+// part only, not renormalised, so that t is the same parameter in both spaces and min_t,
+// the closest hit so far and every hit distance carry over -- and walks the instance's own tree
+// from its root.  When that tree is spent (the stack back at the depth where it began), the
+// world ray is restored and the top-level traversal resumes.  A stack entry whose top byte is
+// zero is a group of pending top-level leaves (node groups are pushed only while they still
+// have children to visit, in the top byte).
+
+// What the traversal reads of an instance: its world-to-object map (rows: object_k =
+// dot(row_k.xyz, world) + row_k.w), the root node of its tree and that tree's hit margin.
+struct Instance_trace {
+    float4   w2o[3];
+    uint32_t root;
+    float    hit_margin;
+    uint32_t pad[2];
+};
+static_assert(sizeof(Instance_trace) == 64, "Instance_trace is 64 bytes");
+
+// A lane's two-level state: the world-space ray, kept while the lane is inside an instance;
+// the instance it is in (Miss at the top level); the stack depth at which that instance's tree
+// began; the instance of the closest hit so far; the hit margin of the current tree.
+struct Instance_state {
+    float    wox, woy, woz;
+    float    wdx, wdy, wdz;
+    uint32_t inst;
+    uint32_t base_sp;
+    uint32_t best_inst;
+    float    margin;
+};
+
+__device__ __forceinline__ void start_instances(Ray_state const& r, Instance_state& is) {
+    is.wox       = r.ox;
+    is.woy       = r.oy;
+    is.woz       = r.oz;
+    is.wdx       = r.dx;
+    is.wdy       = r.dy;
+    is.wdz       = r.dz;
+    is.inst      = Miss;
+    is.base_sp   = 0;
+    is.best_inst = Miss;
+    is.margin    = 0.f;
+}
+
+// The ray's origin and direction replaced (slab reciprocals and octant recomputed).
+__device__ __forceinline__ void set_ray(Ray_state& r, float ox, float oy, float oz, float dx,
+                                        float dy, float dz) {
+    r.ox = ox;
+    r.oy = oy;
+    r.oz = oz;
+    r.dx = dx;
+    r.dy = dy;
+    r.dz = dz;
+    r.ix = safe_rcp(dx);
+    r.iy = safe_rcp(dy);
+    r.iz = safe_rcp(dz);
+    uint32_t const o = (r.ix < 0.f ? 1u : 0u) | (r.iy < 0.f ? 2u : 0u) | (r.iz < 0.f ? 4u : 0u);
+    r.oct_inv        = 7u - o;
+}
+
+__device__ __forceinline__ bool push_group(uint2* stack, Traversal& tv, uint2 group) {
+    if (tv.sp < Stack_size) {
+        stack[tv.sp++] = group;
+        return true;
+    }
+    return false;
+}
+
 // One traversal step: a triangle if the current triangle group has one pending, else the
 // next node (taking the next group from the stack when the current one is spent).
 // Returns true when the ray is finished (any hit found, or nothing left to visit).
 // overflow receives a count if the stack guard ever trips (it cannot for trees of depth
-// <= Max_wide_depth); the ray then ends as a miss instead of writing out of bounds.
+// <= Max_wide_depth, nor for two-level trees whose depths add up to at most that); the ray
+// then ends as a miss instead of writing out of bounds.
 // Filter: triangles whose class word (Wide_triangle::tri_class) shares a bit with skip_class
 // are ignored (the path tracer skips medium boundaries for shadow rays, and surfaces when it
 // walks the boundaries along a shadow ray).
-template <bool Any_hit, bool Filter = false>
+// Instances: two-level traversal (is, instances); the top-level tree's leaves are instances.
+template <bool Any_hit, bool Filter = false, bool Instances = false>
 __device__ __forceinline__ bool traversal_step(Ray_state& r, Traversal& tv, uint2* stack,
                                                uint4 const* __restrict__ nodes,
                                                float4 const* __restrict__ triangles,
                                                float hit_margin, uint32_t* overflow,
-                                               uint32_t skip_class = 0) {
+                                               uint32_t skip_class = 0,
+                                               Instance_state* is = nullptr,
+                                               Instance_trace const* __restrict__ instances = nullptr) {
     // Single exit (no early return): the place where the two branches rejoin decides where a
     // diverged warp reconverges, and keeping it at the end measured fastest.
     bool done = false;
@@ -272,39 +346,116 @@ __device__ __forceinline__ bool traversal_step(Ray_state& r, Traversal& tv, uint
         tv.tri_group.y &= tv.tri_group.y - 1;
         float4 const* tri = triangles + 3 * size_t(tv.tri_group.x + k);
         float4 const  a   = __ldg(tri + 0);
-        float4 const  e1  = __ldg(tri + 1);
-        float4 const  e2  = __ldg(tri + 2);
-        float         t, u, v;
-        bool const    candidate = !Filter || !(__float_as_uint(e1.w) & skip_class);
-        if (candidate && triangle_test(r, a, e1, e2, r.tbest, t, u, v) &&
-            within_bounds(r, a, e1, e2, t, hit_margin)) {
-            uint32_t const id = __float_as_uint(a.w);
-            if (Any_hit) {
-                r.best_id = id;
-                done      = true;
-            } else if (t < r.tbest || id < r.best_id) {
-                r.tbest   = t;
-                r.best_id = id;
-                r.u       = u;
-                r.v       = v;
+        bool          enter = false;
+        if constexpr (Instances) {
+            enter = is->inst == Miss;
+        }
+        if (enter) {
+            if constexpr (Instances) {
+                // A top-level leaf: keep the rest of the top-level traversal, enter the instance.
+                uint32_t const inst = __float_as_uint(a.w);
+                bool           ok   = true;
+                if (tv.group.y & 0xFF000000u) {
+                    ok = push_group(stack, tv, tv.group);
+                }
+                if (ok && tv.tri_group.y != 0) {
+                    ok = push_group(stack, tv, tv.tri_group);
+                }
+                if (!ok) {
+                    atomicAdd(overflow, 1u);
+                    r.best_id = Miss;
+                    done      = true;
+                } else {
+                    Instance_trace const& it = instances[inst];
+                    float4 const          m0 = __ldg(&it.w2o[0]);
+                    float4 const          m1 = __ldg(&it.w2o[1]);
+                    float4 const          m2 = __ldg(&it.w2o[2]);
+                    uint32_t const        root = __ldg(&it.root);
+                    is->margin  = __ldg(&it.hit_margin);
+                    is->inst    = inst;
+                    is->base_sp = tv.sp;
+                    set_ray(r, fmaf(m0.x, is->wox, fmaf(m0.y, is->woy, fmaf(m0.z, is->woz, m0.w))),
+                            fmaf(m1.x, is->wox, fmaf(m1.y, is->woy, fmaf(m1.z, is->woz, m1.w))),
+                            fmaf(m2.x, is->wox, fmaf(m2.y, is->woy, fmaf(m2.z, is->woz, m2.w))),
+                            fmaf(m0.x, is->wdx, fmaf(m0.y, is->wdy, m0.z * is->wdz)),
+                            fmaf(m1.x, is->wdx, fmaf(m1.y, is->wdy, m1.z * is->wdz)),
+                            fmaf(m2.x, is->wdx, fmaf(m2.y, is->wdy, m2.z * is->wdz)));
+                    tv.group     = make_uint2(root, 0x80000000u);
+                    tv.tri_group = make_uint2(0, 0);
+                }
+            }
+        } else {
+            float4 const e1 = __ldg(tri + 1);
+            float4 const e2 = __ldg(tri + 2);
+            float        t, u, v;
+            float        margin = hit_margin;
+            if constexpr (Instances) {
+                margin = is->margin;
+            }
+            bool const candidate = !Filter || !(__float_as_uint(e1.w) & skip_class);
+            if (candidate && triangle_test(r, a, e1, e2, r.tbest, t, u, v) &&
+                within_bounds(r, a, e1, e2, t, margin)) {
+                uint32_t const id = __float_as_uint(a.w);
+                if (Any_hit) {
+                    r.best_id = id;
+                    if constexpr (Instances) {
+                        is->best_inst = is->inst;
+                    }
+                    done = true;
+                } else {
+                    // t <= the closest t so far; equal distances go to the smaller
+                    // (instance, triangle) pair.
+                    bool closer = t < r.tbest;
+                    if constexpr (Instances) {
+                        closer = closer || is->inst < is->best_inst ||
+                                 (is->inst == is->best_inst && id < r.best_id);
+                    } else {
+                        closer = closer || id < r.best_id;
+                    }
+                    if (closer) {
+                        r.tbest   = t;
+                        r.best_id = id;
+                        r.u       = u;
+                        r.v       = v;
+                        if constexpr (Instances) {
+                            is->best_inst = is->inst;
+                        }
+                    }
+                }
             }
         }
     } else {
-        // A spent node group is replaced by the next one from the stack in the same step, so
-        // no step is spent on the pop alone.
-        if (!(tv.group.y & 0xFF000000u) && tv.sp > 0) {
-            tv.group = stack[--tv.sp];
+        bool leaves = false;  // a group of pending top-level leaves came off the stack
+        if (!(tv.group.y & 0xFF000000u)) {
+            if constexpr (Instances) {
+                if (is->inst != Miss && tv.sp == is->base_sp) {
+                    // The instance's tree is spent: back to the world ray.
+                    set_ray(r, is->wox, is->woy, is->woz, is->wdx, is->wdy, is->wdz);
+                    is->inst = Miss;
+                }
+            }
+            // A spent node group is replaced by the next one from the stack in the same step,
+            // so no step is spent on the pop alone.
+            if (tv.sp > 0) {
+                uint2 const e = stack[--tv.sp];
+                if (Instances && !(e.y & 0xFF000000u)) {
+                    tv.tri_group = e;
+                    leaves       = true;
+                } else {
+                    tv.group = e;
+                }
+            }
         }
-        if (tv.group.y & 0xFF000000u) {
+        if (leaves) {
+            // nothing more this step: the next one enters the first of those instances
+        } else if (tv.group.y & 0xFF000000u) {
             uint32_t const b = 31u - __clz(tv.group.y & 0xFF000000u);
             tv.group.y &= ~(1u << b);
             uint32_t const slot = (b - 24u) ^ r.oct_inv;
             uint32_t const rel  = __popc(tv.group.y & 0xFFu & ((1u << slot) - 1u));
             uint32_t const node = tv.group.x + rel;
             if (tv.group.y & 0xFF000000u) {
-                if (tv.sp < Stack_size) {
-                    stack[tv.sp++] = tv.group;
-                } else {
+                if (!push_group(stack, tv, tv.group)) {
                     atomicAdd(overflow, 1u);
                     r.best_id = Miss;
                     done      = true;

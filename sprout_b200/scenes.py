@@ -179,7 +179,8 @@ def translation(x, y, z):
 
 def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounces: int = 8,
             min_bounces: int = 4, fov_degrees: float = 40.0, camera_position=(0.0, 1.0, -3.4),
-            spp: int = 64, tonemap: bool = False, medium=None, density=None, many_lights=False, guiding=None):
+            spp: int = 64, tonemap: bool = False, medium=None, density=None, many_lights=False, guiding=None,
+            integrator=None):
     """Issues the scene's su_* calls on an initialised engine; returns the camera entity.
 
     medium: optional dict of Volumetric material parameters (e.g. color, attenuation_distance,
@@ -191,12 +192,14 @@ def cornell(su, width: int, height: int, sphere_subdivisions: int = 6, max_bounc
     radiance, two of them two-sided (a light-tree test).
     guiding: None for plain MIS, else True or a dict of guide settings (this renderer's
     "guiding" integrator key).
+    integrator: further PTMIS keys (e.g. this renderer's "instancing").
     """
     cam = su.su_create_camera_perspective(width, height, math.radians(fov_degrees))
     su.set_transformation(cam, translation(*camera_position))
     ptmis = {"min_bounces": min_bounces, "max_bounces": max_bounces}
     if guiding is not None:
         ptmis["guiding"] = guiding
+    ptmis.update(integrator or {})
     su.su_create_integrators(json.dumps({"surface": {"PTMIS": ptmis}}).encode())
     su.su_create_sampler(spp)
     if tonemap:
@@ -360,12 +363,13 @@ def emitter_cloud(count: int = 4096, seed: int = 2, size: float = 0.25):
 
 def wavefront(su, width: int = 1920, height: int = 1080, spp: int = 256, max_bounces: int = 12,
               min_bounces: int = 4, instances: int = 400, emitters: int = 4096, seed: int = 2,
-              tonemap: bool = True):
+              tonemap: bool = True, integrator=None):
     """The many-instances, many-lights scene: a ground plane; `instances` randomly placed,
     scaled and rotated copies of one 5,000-triangle displaced sphere (props sharing a mesh, so
     2,000,000 triangles for 400), each with a random Substitute material (roughness U[0.05, 1],
     metallic Bernoulli(0.3), colour U[0, 1]^3); `emitters` emissive triangles with their own
-    Light materials; PTMIS, max depth 12; a pinhole camera with a 60 degree field of view."""
+    Light materials; PTMIS, max depth 12; a pinhole camera with a 60 degree field of view.
+    integrator: further PTMIS keys (e.g. this renderer's "instancing")."""
     rng = np.random.default_rng(seed)
     cam = su.su_create_camera_perspective(width, height, math.radians(60.0))
     m = np.eye(4, dtype=np.float32)
@@ -373,8 +377,9 @@ def wavefront(su, width: int = 1920, height: int = 1080, spp: int = 256, max_bou
     m[1, 1], m[1, 2], m[2, 1], m[2, 2] = math.cos(0.25), math.sin(0.25), -math.sin(0.25), math.cos(0.25)
     m[3, :3] = (0.0, 6.0, -17.0)
     su.set_transformation(cam, m)
-    su.su_create_integrators(json.dumps({"surface": {"PTMIS": {"min_bounces": min_bounces,
-                                                              "max_bounces": max_bounces}}}).encode())
+    ptmis = {"min_bounces": min_bounces, "max_bounces": max_bounces}
+    ptmis.update(integrator or {})
+    su.su_create_integrators(json.dumps({"surface": {"PTMIS": ptmis}}).encode())
     su.su_create_sampler(spp)
     if tonemap:
         su.su_create_defaults()
@@ -513,15 +518,16 @@ def _look_at(position, target=(0.0, 0.0, 0.0)):
 
 
 def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -3.2),
-           max_bounces: int = 32, min_bounces: int = 4, environment=(0.3, 0.35, 0.4)):
+           max_bounces: int = 32, min_bounces: int = 4, environment=(0.3, 0.35, 0.4), integrator=None):
     """A 2 m Cube (built-in, [-1, 1]^3) filled with a density grid (VOLUME_MEDIUM), lit by a
     Sphere light of radius 0.25 (radiance 60) and a uniform Infinite_sphere environment; a
     pinhole camera at `position` looking at the centre with a 40 degree field of view; PTMIS
-    with max depth 32."""
+    with max depth 32.  integrator: further PTMIS keys (e.g. this renderer's "instancing")."""
     cam = su.su_create_camera_perspective(width, height, math.radians(40.0))
     su.set_transformation(cam, _look_at(position))
-    su.su_create_integrators(json.dumps({"surface": {"PTMIS": {"min_bounces": min_bounces,
-                                                              "max_bounces": max_bounces}}}).encode())
+    ptmis = {"min_bounces": min_bounces, "max_bounces": max_bounces}
+    ptmis.update(integrator or {})
+    su.su_create_integrators(json.dumps({"surface": {"PTMIS": ptmis}}).encode())
     su.su_create_sampler(spp)
     su.su_create_defaults()
     image = su.image(density)

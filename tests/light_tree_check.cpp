@@ -43,9 +43,9 @@ struct Checker {
 
     float const* node(uint32_t n) const { return &t.nodes[12 * size_t(n)]; }
 
-    // light (tree order) -> input index
+    // light (tree order) -> input (its stored material is 2 * slot + 5)
     Light_input const& light(uint32_t o) const {
-        return in[by_tri[u32(t.tris[12 * size_t(o) + 11])]];
+        return in[by_tri[(u32(t.tris[12 * size_t(o) + 11]) - 5u) / 2u]];
     }
 
     // returns the [begin, end) range of lights of the subtree, checks contents
@@ -126,7 +126,7 @@ bool check(std::vector<Light_input> const& in, uint32_t num_triangles, char cons
     }
     Checker k{t, in, std::vector<int>(in.size(), 0), std::vector<uint32_t>(num_triangles, 0)};
     for (size_t i = 0; i < in.size(); ++i) {
-        k.by_tri[in[i].tri] = uint32_t(i);
+        k.by_tri[in[i].slot] = uint32_t(i);
     }
     uint32_t b, e;
     double   p;
@@ -138,8 +138,10 @@ bool check(std::vector<Light_input> const& in, uint32_t num_triangles, char cons
         if (k.seen[o] != 1) {
             k.fail("light seen once", uint32_t(o));
         }
-        uint32_t const tri = u32(t.tris[12 * o + 11]);
-        if (t.order[tri] != o) {
+        // the light at tree position o carries its material; its slot maps back to o
+        uint32_t const material = u32(t.tris[12 * o + 11]);
+        uint32_t const slot     = (material - 5u) / 2u;
+        if (material != 2u * slot + 5u || slot >= num_triangles || t.order[slot] != o) {
             k.fail("order", uint32_t(o));
         }
     }
@@ -170,7 +172,8 @@ std::vector<Light_input> emitters(int n, int kind, uint32_t seed) {
         }
         l.power     = std::exp(4.0 * u(g));
         l.two_sided = (i % 7) == 3;
-        l.tri       = uint32_t(3 * i + 1);
+        l.slot      = uint32_t(3 * i + 1);
+        l.material  = 2u * l.slot + 5u;
         v.push_back(l);
     }
     return v;
