@@ -22,9 +22,10 @@ ORACLE = ROOT / "oracle"
 ORACLE_LIB = ORACLE / "libcast_oracle.so"
 REFERENCE = pathlib.Path(os.environ.get("SPROUT_REFERENCE", "/root/reference"))
 
-SOURCES = ["common.cpp", "synth.cpp", "bvh8.cpp", "ggx_table.cpp", "light_tree.cpp", "cast.cu", "guide.cu", "render.cu", "capi.cpp"]
+SOURCES = ["common.cpp", "synth.cpp", "bvh8.cpp", "ggx_table.cpp", "light_tree.cpp", "postprocess.cpp", "cast.cu",
+           "guide.cu", "render.cu", "capi.cpp"]
 HEADERS = ["common.hpp", "bvh8.hpp", "traverse.cuh", "material.cuh", "render.hpp", "json.hpp", "ggx_table.hpp",
-           "light_tree.hpp", "guide.cuh", "guide_mlp.cuh", "guide.hpp", "tuner.hpp"]
+           "light_tree.hpp", "guide.cuh", "guide_mlp.cuh", "guide.hpp", "tuner.hpp", "postprocess.hpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -54,7 +55,7 @@ def build_library(force: bool = False, verbose: bool = False, ptxas_info: bool =
     inputs = [CSRC / s for s in SOURCES] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "sprout_b200.h", ROOT / "include" / "sprout.h"]
     if not force and not _stale(LIBRARY, inputs):
         return LIBRARY
-    cmd = [_nvcc(), "-shared", "-o", str(LIBRARY)] + [str(CSRC / s) for s in SOURCES] + NVCC_FLAGS
+    cmd = [_nvcc(), "-shared", "-o", str(LIBRARY)] + [str(CSRC / s) for s in SOURCES] + NVCC_FLAGS + ["-lz"]
     if ptxas_info:
         cmd += ["-Xptxas", "-v"]
     tmp = LIBRARY.with_suffix(".so.tmp")

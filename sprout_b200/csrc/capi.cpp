@@ -19,6 +19,7 @@
 #include "../../include/sprout_b200.h"
 #include "common.hpp"
 #include "json.hpp"
+#include "postprocess.hpp"
 #include "render.hpp"
 
 namespace {
@@ -85,7 +86,8 @@ struct Engine {
     bool                  frame_started = false;
     bool                  scene_dirty    = true;   // host scene changed since the last upload
     bool                  camera_dirty   = false;  // only the camera changed since then
-    bool                  tonemap_linear = false;  // su_create_defaults: Linear tonemapper
+    std::vector<spb::post::Tonemapper> pipeline;  // applied in order by su_postprocess
+    std::vector<std::string>           exporters = {"PNG"};  // image formats su_export_frame writes
     int                   instancing     = -1;     // PTMIS "instancing": -1 auto, 0 off, 1 on
     bool                  sampler_golden = true;   // a take's "Random" sampler turns it off
     uint32_t              iteration     = 0;
@@ -900,6 +902,42 @@ bool write_png(std::string const& path, uint32_t w, uint32_t h, uint8_t const* r
 }
 
 // su_load_take: a take given as JSON text or as a file name.
+// A take's tonemapper object (load_tonemapper, take_loader.cpp:864-903).
+bool read_tonemapper(spb::json::Value const& v, spb::post::Tonemapper& t) {
+    if (!v.is_object() || v.object.empty()) {
+        return false;
+    }
+    auto const& [name, p] = v.object[0];
+    auto const  num       = [&](char const* key, float fallback) {
+        return float(spb::json::number_or(p.find(key), fallback));
+    };
+    t             = spb::post::Tonemapper();
+    t.auto_expose = spb::json::bool_or(p.find("auto_expose"), false);
+    t.exposure    = num("exposure", 0.f);
+    if (name == "Linear") {
+        t.kind = spb::post::Tonemapper::Kind::Linear;
+    } else if (name == "ACES") {
+        t.kind = spb::post::Tonemapper::Kind::Aces;
+    } else if (name == "Generic") {
+        t.kind     = spb::post::Tonemapper::Kind::Generic;
+        t.contrast = num("contrast", t.contrast);
+        t.shoulder = num("shoulder", t.shoulder);
+        t.mid_in   = num("mid_in", t.mid_in);
+        t.mid_out  = num("mid_out", t.mid_out);
+        t.hdr_max  = num("hdr_max", t.hdr_max);
+    } else if (name == "Piecewise") {
+        t.kind              = spb::post::Tonemapper::Kind::Piecewise;
+        t.toe_strength      = num("toe_strength", t.toe_strength);
+        t.toe_length        = num("toe_length", t.toe_length);
+        t.shoulder_strength = num("shoulder_strength", t.shoulder_strength);
+        t.shoulder_length   = num("shoulder_length", t.shoulder_length);
+        t.shoulder_angle    = num("shoulder_angle", t.shoulder_angle);
+    } else {
+        return false;
+    }
+    return true;
+}
+
 int32_t load_take(std::string const& string) {
     size_t const first = string.find_first_not_of(" \t\r\n");
     bool const   is_json = first != std::string::npos && string[first] == '{';
@@ -952,6 +990,37 @@ int32_t load_take(std::string const& string) {
     }
     if (spb::json::Value const* integrator = take.find("integrator")) {
         su_create_integrators(spb::json::dump(*integrator).c_str());
+    }
+    // "post": the postprocessors in order (Loader::load_postprocessors, take_loader.cpp:817-862);
+    // without it the Linear tonemapper (set_default_postprocessor, :965-978).
+    engine->pipeline.assign(1, spb::post::Tonemapper());
+    if (spb::json::Value const* post = take.find("post"); post && post->is_array()) {
+        engine->pipeline.clear();
+        for (auto const& pp : post->array) {
+            if (!pp.is_object() || pp.object.empty()) {
+                continue;
+            }
+            spb::json::Value const* tm = pp.find("tonemapper");
+            spb::post::Tonemapper   t;
+            if (!tm || !read_tonemapper(*tm, t)) {
+                log(SU_LOG_WARNING, "su_load_take: postprocessor \"" + pp.object[0].first + "\" is not supported; skipped");
+                continue;
+            }
+            engine->pipeline.push_back(t);
+        }
+    }
+    // "export": {"Image": {"format": "PNG" | "EXR" | "RGBE"}} (load_exporters, take_loader.cpp:907-951);
+    // without it the PNG writer (set_default_exporter, :980-994).
+    engine->exporters.assign(1, "PNG");
+    if (spb::json::Value const* ex = take.find("export"); ex && ex->is_object()) {
+        engine->exporters.clear();
+        for (auto const& [name, value] : ex->object) {
+            if (name == "Image") {
+                engine->exporters.push_back(spb::json::string_or(value.find("format"), "PNG"));
+            } else {
+                log(SU_LOG_WARNING, "su_load_take: exporter \"" + name + "\" is not supported; skipped");
+            }
+        }
     }
     if (spb::json::Value const* scene = take.find("scene"); scene && scene->is_string()) {
         return load_scene(resolve(scene->string, base));
@@ -1019,7 +1088,7 @@ SU_LIBRARY_API int32_t su_create_defaults(void) {
     }
     // take_loader.cpp:965-978: with ACEScg the default pipeline is the Linear tonemapper
     // (exposure 0), which maps the AP1 film to linear sRGB (tonemapping/linear.cpp:10-27).
-    engine->tonemap_linear = true;
+    engine->pipeline.assign(1, spb::post::Tonemapper());
     if (!engine->have_integrator) {
         engine->settings        = spb::render::Settings();
         engine->have_integrator = true;
@@ -1619,10 +1688,24 @@ SU_LIBRARY_API int32_t su_export_frame(uint32_t frame) {
     if (su_copy_framebuffer(SU_UINT8, engine->width, engine->height, 3, rgb.data()) != 0) {
         return 0;
     }
-    char name[32];
-    std::snprintf(name, sizeof(name), "output_%06u.png", frame);
-    if (!write_png(name, engine->width, engine->height, rgb.data())) {
-        log(SU_LOG_ERROR, std::string("su_export_frame: cannot write ") + name);
+    // Image_sequence("output_", writer) per exporter (take_loader.cpp:907-951): PNG of the
+    // 8-bit sRGB framebuffer, EXR (half) and RGBE of the postprocessed linear frame.
+    for (std::string const& format : engine->exporters) {
+        char name[40];
+        bool ok = false;
+        if (format == "EXR") {
+            std::snprintf(name, sizeof(name), "output_%06u.exr", frame);
+            ok = spb::post::write_exr(name, engine->width, engine->height, engine->target.data(), false);
+        } else if (format == "RGBE") {
+            std::snprintf(name, sizeof(name), "output_%06u.hdr", frame);
+            ok = spb::post::write_rgbe(name, engine->width, engine->height, engine->target.data());
+        } else {
+            std::snprintf(name, sizeof(name), "output_%06u.png", frame);
+            ok = write_png(name, engine->width, engine->height, rgb.data());
+        }
+        if (!ok) {
+            log(SU_LOG_ERROR, std::string("su_export_frame: cannot write ") + name);
+        }
     }
     return 0;
 }
@@ -1639,16 +1722,9 @@ SU_LIBRARY_API int32_t su_postprocess(void) {
         log(SU_LOG_ERROR, engine->renderer.error());
         return -2;
     }
-    if (engine->tonemap_linear) {
-        for (size_t i = 0; i < engine->target.size(); i += 4) {
-            float* c        = &engine->target[i];
-            float const r   = c[0];
-            float const g   = c[1];
-            float const b   = c[2];
-            c[0]            = 1.70505155f * r - 0.62179068f * g - 0.08325840f * b;
-            c[1]            = -0.13025714f * r + 1.14080289f * g - 0.01054853f * b;
-            c[2]            = -0.02400328f * r - 0.12896877f * g + 1.15297171f * b;
-        }
+    // The postprocessor pipeline (Pipeline::apply, postprocessor_pipeline.cpp:69-102).
+    for (spb::post::Tonemapper const& t : engine->pipeline) {
+        spb::post::apply(t, engine->target.data(), engine->target.size() / 4);
     }
     return 0;
 }

@@ -369,12 +369,14 @@ __device__ __forceinline__ float2 golden_2d(Wave const& w, uint32_t pixel, uint3
 }
 
 // Golden ratio dimensions: 2-D 0 the pixel position, 1 + 4 d + k the light point of light
-// sample k at vertex depth d, 1 + 4 d + 3 the BSDF direction; 1-D 16 + 4 d + k the light
-// selection of light sample k, 16 + 4 d + 3 the BSDF lobe.
+// sample k at vertex depth d, 1 + 4 d + 3 the BSDF (or guide) direction; 1-D 16 + 4 d + k the
+// light selection of light sample k, 16 + 4 d + 3 the BSDF lobe (or guide lobe), 32 + d the
+// choice between guide and BSDF.
 __device__ __forceinline__ uint32_t golden_light_2d(uint32_t depth, int k) { return 1u + 4u * depth + uint32_t(k); }
 __device__ __forceinline__ uint32_t golden_bsdf_2d(uint32_t depth) { return 1u + 4u * depth + 3u; }
 __device__ __forceinline__ uint32_t golden_light_1d(uint32_t depth, int k) { return 16u + 4u * depth + uint32_t(k); }
 __device__ __forceinline__ uint32_t golden_bsdf_1d(uint32_t depth) { return 16u + 4u * depth + 3u; }
+__device__ __forceinline__ uint32_t golden_choice_1d(uint32_t depth) { return 32u + depth; }
 
 // Ray origin offset off a surface (Waechter and Binder, "A Fast and Robust Method for
 // Avoiding Self-Intersection", Ray Tracing Gems 2019, ch. 6), n pointing to the side the ray
@@ -1758,10 +1760,24 @@ __global__ void __launch_bounds__(Shade_block)
                 // Substitute BSDF (its cosines clamped to a small positive minimum) is not zero;
                 // dropping those directions would bias the one-sample MIS estimate low.
                 shading::Sampled smp;
-                if (guided && rng.uniform() < gf) {
-                    float const g0 = rng.uniform();
-                    float const g1 = rng.uniform();
-                    float const g2 = rng.uniform();
+                // With golden ratio sampling, the choice between guide and BSDF has a dimension
+                // of its own, and the guide's lobe and direction use the BSDF's (one of the two
+                // samplers is used at a vertex).
+                float const choice = !guided ? 1.f
+                                             : (golden ? golden_1d(wave, gpixel, gsample, golden_choice_1d(depth))
+                                                       : rng.uniform());
+                if (guided && choice < gf) {
+                    float g0, g1, g2;
+                    if (golden) {
+                        g0              = golden_1d(wave, gpixel, gsample, golden_bsdf_1d(depth));
+                        float2 const g2d = golden_2d(wave, gpixel, gsample, golden_bsdf_2d(depth));
+                        g1              = g2d.x;
+                        g2              = g2d.y;
+                    } else {
+                        g0 = rng.uniform();
+                        g1 = rng.uniform();
+                        g2 = rng.uniform();
+                    }
                     smp.wi                = mixture_sample_at(mix, g0, g1, g2);
                     smp.specular          = false;
                     shading::Bxdf const f = shading::substitute_evaluate(mat, s.e_table, ctx, smp.wi);

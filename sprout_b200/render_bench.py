@@ -42,9 +42,14 @@ SCENES = {
                 (512, 512, 64), None),
     "wavefront": ("400 instances of a 5,000-tri displaced sphere (2,000,000 tris, Substitute roughness U[0.05,1], "
                   "metallic Bernoulli(0.3)), 4,096 emissive tris of log-uniform radiance [0.1, 100] via the light "
-                  "tree, PTMIS max depth 12 (Russian roulette from depth 4)",
+                  "tree, PTMIS max depth 12 (Russian roulette from depth 4); the props kept as instances of one "
+                  "mesh under a top-level tree",
                   lambda su, w, h, spp: scenes.wavefront(su, w, h, spp),
                   (1920, 1080, 256), (960, 540, 16)),
+    "wavefront_flat": ("the same scene with every prop flattened into one 2,004,098-triangle tree "
+                       "(\"instancing\": false)",
+                       lambda su, w, h, spp: scenes.wavefront(su, w, h, spp, integrator={"instancing": False}),
+                       (1920, 1080, 256), None),
 }
 
 
@@ -65,7 +70,9 @@ def measure(scene="cornell", width=None, height=None, spp=None, frames=3, conver
     try:
         build(su, width, height, spp)
         t0 = time.perf_counter()
-        assert su.su_render_frame(0) == 0, su.messages  # scene upload + BVH build + warm-up
+        assert su.su_start_render_frame(0) == 0, su.messages  # scene upload + BVH build
+        out["prepare_s"] = round(time.perf_counter() - t0, 3)
+        assert su.su_render_frame(0) == 0, su.messages  # warm-up (autotuner)
         out["first_frame_s"] = round(time.perf_counter() - t0, 3)
         dev, wall = [], []
         for _ in range(frames):
@@ -79,7 +86,8 @@ def measure(scene="cornell", width=None, height=None, spp=None, frames=3, conver
         dev_s = statistics.median(dev)
         rays = stats.extension_rays + stats.shadow_rays
         samples = width * height * spp
-        out.update({"msamples_s": round(samples / dev_s / 1e6, 3), "mrays_s": round(rays / dev_s / 1e6, 3),
+        out.update({"instances": stats.instances, "device_triangles": stats.device_triangles,
+                    "msamples_s": round(samples / dev_s / 1e6, 3), "mrays_s": round(rays / dev_s / 1e6, 3),
                     "ms_per_frame": round(1e3 * dev_s, 3), "rays_per_sample": round(rays / samples, 3),
                     "e2e_msamples_s": round(samples / statistics.median(wall) / 1e6, 3),
                     "e2e_note": "su_render_frame + su_postprocess + su_copy_framebuffer to host, wall clock"})
@@ -289,16 +297,26 @@ def measure_guiding(width=1280, height=720, target=0.01):
     last_stats = {}
 
     def reach(first, guiding):
+        """The smallest multiple of 8 spp whose frame meets the target: up from the prediction
+        until it is met, then down while it still is."""
         spp, runs = first, []
-        for _ in range(5):
+        met = None
+        for _ in range(12):
             img, dev, wall = doorway_frame(width, height, spp, guiding, stats_out=last_stats)
             err = rel(img)
             runs.append({"spp": spp, "rel_mse": round(err, 5), "device_seconds": round(dev, 4),
                          "wall_seconds": round(wall, 3)})
             if err <= target:
-                break
-            spp = max(spp + 8, int(np.ceil(spp * err / target / 8.0)) * 8)
-        last = runs[-1]
+                met = runs[-1]
+                if spp <= 8 or (len(runs) > 1 and runs[-2]["spp"] < spp):
+                    break  # came up to it: the count below missed
+                spp -= 8
+            elif met is not None:
+                break  # went down past it
+            else:
+                spp = max(spp + 8, int(np.ceil(spp * err / target / 8.0)) * 8)
+        last = met if met is not None else runs[-1]
+        spp  = last["spp"]
         devs, walls = [last["device_seconds"]], [last["wall_seconds"]]
         for _ in range(2):
             _, dev, wall = doorway_frame(width, height, spp, guiding, stats_out=last_stats)
@@ -306,6 +324,8 @@ def measure_guiding(width=1280, height=720, target=0.01):
             walls.append(round(wall, 3))
         last["device_seconds"], last["wall_seconds"] = float(np.median(devs)), float(np.median(walls))
         last["device_seconds_frames"], last["wall_seconds_frames"] = devs, walls
+        runs.remove(last)
+        runs.append(last)
         return runs
 
     def predicted(guiding, probe):

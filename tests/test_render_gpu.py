@@ -226,3 +226,53 @@ def test_golden_ratio_sampling_lowers_the_error():
         e_batch += rel_mse(batch, ref)
         e_random += rel_mse(random, ref)
     assert e_batch < 0.9 * e_random, (e_batch, e_random)
+
+
+def test_take_postprocessors_and_exporters(tmp_path, monkeypatch):
+    """A take's "post" pipeline and "export" writers (take_loader.cpp:817-951): frames rendered
+    with the Linear tonemapper and with ACES differ exactly by the tonemappers' curves (checked
+    here per pixel from the Linear frame, which is AP1 -> sRGB of the film), and the EXR and RGBE
+    exporters write output_000000.exr / .hdr holding the postprocessed frame."""
+    import json
+
+    takes = GOLDEN.parent / "takes"
+    base = json.loads((takes / "room.take").read_text())
+    base["sampler"] = {"Random": {"samples_per_pixel": 16}}
+
+    def frame(post=None, export=None):
+        take = dict(base)
+        if post is not None:
+            take["post"] = post
+        if export is not None:
+            take["export"] = export
+        path = tmp_path / "t.take"
+        path.write_text(json.dumps(take))
+        su = capi.SuLibrary()
+        assert su.su_init(False) == 0
+        try:
+            assert su.su_mount((str(takes) + "/").encode()) == 0
+            assert su.su_load_take(str(path).encode()) == 0, su.messages
+            assert su.su_render() == 0, su.messages
+            img, _ = su.framebuffer(96, 72)
+            return img[:, :, :3].astype(np.float64)
+        finally:
+            su.su_release()
+
+    monkeypatch.chdir(tmp_path)
+    linear = frame()
+    aces = frame(post=[{"tonemapper": {"ACES": {"exposure": 0.5}}}],
+                 export={"Image": {"format": "EXR"}})
+    assert (tmp_path / "output_000000.exr").exists()
+    # ACES of 2^0.5 * film, from the Linear frame (linear sRGB = AP1_to_sRGB(film))
+    to_ap1 = np.linalg.inv(np.array([[1.70505155, -0.62179068, -0.08325840],
+                                     [-0.13025714, 1.14080289, -0.01054853],
+                                     [-0.02400328, -0.12896877, 1.15297171]]))
+    film = linear @ to_ap1.T * 2 ** 0.5
+    rrt = film @ np.array([[0.970889, 0.026963, 0.002148], [0.010889, 0.986963, 0.002148],
+                           [0.010889, 0.026963, 0.962148]]).T
+    odt = (rrt * (rrt + 0.0245786) - 0.000090537) / (rrt * (0.983729 * rrt + 0.4329510) + 0.238081)
+    want = odt @ np.array([[1.60475, -0.53108, -0.07367], [-0.10208, 1.10813, -0.00605],
+                           [-0.00327, -0.07276, 1.07602]]).T
+    assert np.allclose(aces, want, rtol=1e-3, atol=1e-5)
+    frame(export={"Image": {"format": "RGBE"}})
+    assert (tmp_path / "output_000000.hdr").read_bytes().startswith(b"#?RADIANCE")
