@@ -313,6 +313,7 @@ def measure_render(args, with_cpu):
                                            cpu_reference=with_cpu)}
     if not args.no_wavefront:
         out["wavefront"] = render_bench.measure("wavefront", frames=1, cpu_reference=with_cpu)
+        out["wavefront_flat"] = render_bench.measure("wavefront_flat", frames=1)
     if not args.no_volume:
         out["volume"] = render_bench.measure_volume(views=64, spp=128, cpu_reference=with_cpu)
     if not args.no_guiding:

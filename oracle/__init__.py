@@ -274,15 +274,30 @@ class ScriptRecorder:
         self.n["image"] += 1
         return self.n["image"] - 1
 
-    def mesh(self, positions, normals, indices, parts=None):
+    def image2d(self, pixels):
+        """su_create_image of a 2-D image (height, width, channels), uint8 (Byte) or float32."""
+        a = np.ascontiguousarray(pixels)
+        h, w, c = a.shape
+        kind = 0 if a.dtype == np.uint8 else 2
+        a = a if a.dtype == np.uint8 else a.astype(np.float32)
+        self.lines.append(f"image {kind} {c} {w} {h} 1 {self._blob(a)}")
+        self.n["image"] += 1
+        return self.n["image"] - 1
+
+    def mesh(self, positions, normals, indices, parts=None, uvs=None):
         pos = np.asarray(positions, np.float32).reshape(-1, 3)
         nrm = np.asarray(normals, np.float32).reshape(-1, 3)
         idx = np.asarray(indices, np.uint32).reshape(-1, 3)
         op, on, oi = self._blob(pos), self._blob(nrm), self._blob(idx)
         line = f"mesh {idx.shape[0]} {pos.shape[0]} {op} {on} {oi}"
-        if parts is not None:
-            prt = np.asarray(parts, np.uint32).reshape(-1, 3)
-            line += f" {prt.shape[0]} {self._blob(prt)}"
+        if parts is not None or uvs is not None:
+            if parts is not None:
+                prt = np.asarray(parts, np.uint32).reshape(-1, 3)
+                line += f" {prt.shape[0]} {self._blob(prt)}"
+            else:
+                line += " 0 0"
+        if uvs is not None:
+            line += f" {self._blob(np.asarray(uvs, np.float32).reshape(-1, 2))}"
         self.lines.append(line)
         self.n["mesh"] += 1
         return 2000 + self.n["mesh"] - 1

@@ -18,7 +18,8 @@
 //       (su_create_image, tightly packed; the created image id must equal the number of images
 //       created before it, which the recorded material JSON refers to)
 //     mesh <num_triangles> <num_vertices> <byte offset of positions> <of normals> <of indices>
-//          [<num parts> <byte offset of the parts: (first index, index count, material slot)>]
+//          [<num parts> <byte offset of the parts: (first index, index count, material slot)>
+//           [<byte offset of the texture coordinates, 2 floats per vertex>]]
 //     prop <mesh handle or built-in shape id (< 8)> <num materials> <material handles...>
 //     light <prop handle>
 //     mount <folder>   (su_mount; the folder name without spaces)
@@ -130,14 +131,16 @@ int main(int argc, char** argv) {
             }
         } else if (c == "mesh") {
             uint32_t nt = 0, nv = 0, np = 0;
-            size_t   op = 0, on = 0, oi = 0, opart = 0;
-            std::sscanf(rest, "%u %u %zu %zu %zu %u %zu", &nt, &nv, &op, &on, &oi, &np, &opart);
+            size_t   op = 0, on = 0, oi = 0, opart = 0, ouv = 0;
+            int const fields = std::sscanf(rest, "%u %u %zu %zu %zu %u %zu %zu", &nt, &nv, &op, &on, &oi, &np,
+                                           &opart, &ouv);
             auto const* pos = reinterpret_cast<float const*>(data.data() + op);
             auto const* nrm = reinterpret_cast<float const*>(data.data() + on);
             auto const* idx = reinterpret_cast<uint32_t const*>(data.data() + oi);
             auto const* prt = np ? reinterpret_cast<uint32_t const*>(data.data() + opart) : nullptr;
+            auto const* uvs = fields == 8 ? reinterpret_cast<float const*>(data.data() + ouv) : nullptr;
             handles[2000 + n_mesh++] = su_create_triangle_mesh_async(
-                nt, nv, 3, pos, 3, nrm, 0, nullptr, 0, nullptr, idx, np, prt);
+                nt, nv, 3, pos, 3, nrm, 0, nullptr, uvs ? 2 : 0, uvs, idx, np, prt);
         } else if (c == "prop") {
             uint32_t mesh = 0, nm = 0;
             int      off  = 0;

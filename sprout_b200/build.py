@@ -22,10 +22,11 @@ ORACLE = ROOT / "oracle"
 ORACLE_LIB = ORACLE / "libcast_oracle.so"
 REFERENCE = pathlib.Path(os.environ.get("SPROUT_REFERENCE", "/root/reference"))
 
-SOURCES = ["common.cpp", "synth.cpp", "bvh8.cpp", "ggx_table.cpp", "light_tree.cpp", "postprocess.cpp", "cast.cu",
+SOURCES = ["common.cpp", "synth.cpp", "bvh8.cpp", "ggx_table.cpp", "light_tree.cpp", "postprocess.cpp", "image_io.cpp",
+           "cast.cu",
            "guide.cu", "render.cu", "capi.cpp"]
 HEADERS = ["common.hpp", "bvh8.hpp", "traverse.cuh", "material.cuh", "render.hpp", "json.hpp", "ggx_table.hpp",
-           "light_tree.hpp", "guide.cuh", "guide_mlp.cuh", "guide.hpp", "tuner.hpp", "postprocess.hpp"]
+           "light_tree.hpp", "guide.cuh", "guide_mlp.cuh", "guide.hpp", "tuner.hpp", "postprocess.hpp", "image_io.hpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -82,14 +82,16 @@ class SuLibrary:
     def __getattr__(self, name):
         return getattr(self.lib, name)
 
-    def mesh(self, positions, normals, indices, parts=None):
+    def mesh(self, positions, normals, indices, parts=None, uvs=None):
         pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
         nrm = np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
         idx = np.ascontiguousarray(indices, np.uint32).reshape(-1, 3)
         prt = None if parts is None else np.ascontiguousarray(parts, np.uint32).reshape(-1, 3)
-        self._keep += [pos, nrm, idx, prt]
+        tex = None if uvs is None else np.ascontiguousarray(uvs, np.float32).reshape(-1, 2)
+        self._keep += [pos, nrm, idx, prt, tex]
         return self.lib.su_create_triangle_mesh_async(
-            idx.shape[0], pos.shape[0], 3, pos.ctypes.data, 3, nrm.ctypes.data, 0, None, 0, None,
+            idx.shape[0], pos.shape[0], 3, pos.ctypes.data, 3, nrm.ctypes.data, 0, None,
+            0 if tex is None else 2, None if tex is None else tex.ctypes.data,
             idx.ctypes.data, 0 if prt is None else prt.shape[0], None if prt is None else prt.ctypes.data)
 
     def image(self, pixels):
@@ -97,6 +99,16 @@ class SuLibrary:
         a = np.ascontiguousarray(pixels, np.float32)
         d, h, w = a.shape if a.ndim == 3 else (1,) + a.shape
         return self.lib.su_create_image(2, 1, w, h, d, 0, 4, a.ctypes.data)
+
+    def image2d(self, pixels):
+        """su_create_image of a 2-D image (height, width, channels): uint8 pixels as Byte (sRGB
+        encoded where used as colour), float32 pixels as Float."""
+        a = np.ascontiguousarray(pixels)
+        h, w, c = a.shape
+        kind, size = (0, 1) if a.dtype == np.uint8 else (2, 4)
+        a = a if a.dtype == np.uint8 else a.astype(np.float32)
+        self._keep.append(a)
+        return self.lib.su_create_image(kind, c, w, h, 1, 0, size * c, a.ctypes.data)
 
     def prop(self, shape, materials):
         mats = np.ascontiguousarray(materials, np.uint32)

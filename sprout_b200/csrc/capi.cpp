@@ -12,12 +12,14 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <tuple>
 #include <utility>
 #include <vector>
 
 #include "../../include/sprout.h"
 #include "../../include/sprout_b200.h"
 #include "common.hpp"
+#include "image_io.hpp"
 #include "json.hpp"
 #include "postprocess.hpp"
 #include "render.hpp"
@@ -38,6 +40,7 @@ constexpr uint32_t Shape_sphere          = 7;
 struct Mesh {
     std::vector<float>    positions;  // 3 per vertex
     std::vector<float>    normals;    // 3 per vertex
+    std::vector<float>    uvs;        // 2 per vertex (texture coordinates; zero when not given)
     std::vector<uint32_t> indices;    // 3 per triangle
     std::vector<uint32_t> part_of;    // part per triangle
     std::vector<uint32_t> part_slot;  // material slot per part
@@ -47,7 +50,22 @@ struct Mesh {
 struct Image {
     uint32_t           dims[3]  = {0, 0, 0};
     uint32_t           channels = 0;
-    std::vector<float> pixels;  // channels per pixel, x fastest
+    std::vector<float> pixels;         // channels per pixel, x fastest
+    bool               encoded_bytes = false;  // from 8- or 16-bit data: sRGB where used as colour
+};
+
+// Texture maps of a Substitute material (Material_base::set_sample,
+// substitute_base_material.inl:36-96): colour, and surface (roughness, and metallic from a
+// second channel) or roughness alone; images by id, sampled with the material's sampler
+// settings and the texture's uv scale.
+struct Material_maps {
+    uint32_t color          = Null;  // image ids
+    uint32_t surface        = Null;
+    uint32_t surface_usage  = 0;     // 2: Surface (roughness, metallic), 1: Roughness
+    float    color_scale[2] = {1.f, 1.f};
+    float    surface_scale[2] = {1.f, 1.f};
+    bool     nearest        = false;
+    bool     clamp          = false;
 };
 
 // Host-side part of a Volumetric material with a density grid (Grid, volumetric_grid.cpp).
@@ -73,6 +91,7 @@ struct Engine {
     Mesh                  builtin[First_mesh_id];  // tessellated built-in shapes, made on first use
     std::vector<Material> materials;
     std::vector<Grid_ref> material_grids;  // parallel to materials
+    std::vector<Material_maps> material_maps;  // parallel to materials
     std::vector<Image>    images;
     std::vector<Entity>   entities;
     uint32_t              camera_entity = Null;
@@ -142,24 +161,29 @@ bool read_color(spb::json::Value const* v, V3& out) {
 // exact areas, so emitters built from them carry the analytic shape's power.
 Mesh make_builtin(uint32_t shape) {
     Mesh m;
-    auto vertex = [&m](double x, double y, double z, double nx, double ny, double nz) {
+    // Texture coordinates as the analytic shapes report them: planar shapes (0.5 (x + 1),
+    // 0.5 (1 - y)) in their plane (rectangle.cpp:38-58, disk.cpp:50-58), the sphere
+    // (phi / 2 pi, theta / pi) (sphere.cpp:55-60).
+    auto vertex = [&m](double x, double y, double z, double nx, double ny, double nz, double u = 0.0,
+                       double v = 0.0) {
         m.positions.insert(m.positions.end(), {float(x), float(y), float(z)});
         m.normals.insert(m.normals.end(), {float(nx), float(ny), float(nz)});
+        m.uvs.insert(m.uvs.end(), {float(u), float(v)});
         return uint32_t(m.positions.size() / 3 - 1);
     };
     if (shape == Shape_rectangle) {
         for (auto [x, y] : {std::pair{-1, -1}, {1, -1}, {1, 1}, {-1, 1}}) {
-            vertex(x, y, 0, 0, 0, 1);
+            vertex(x, y, 0, 0, 0, 1, 0.5 * (x + 1), 0.5 * (1 - y));
         }
         m.indices = {0, 1, 2, 0, 2, 3};
     } else if (shape == Shape_disk) {
         int const    n = 256;
         double const r = std::sqrt(3.14159265358979323846 /
                                    (0.5 * n * std::sin(2.0 * 3.14159265358979323846 / n)));
-        vertex(0, 0, 0, 0, 0, 1);
+        vertex(0, 0, 0, 0, 0, 1, 0.5, 0.5);
         for (int i = 0; i < n; ++i) {
             double const a = 2.0 * 3.14159265358979323846 * i / n;
-            vertex(r * std::cos(a), r * std::sin(a), 0, 0, 0, 1);
+            vertex(r * std::cos(a), r * std::sin(a), 0, 0, 0, 1, 0.5 * (std::cos(a) + 1), 0.5 * (1 - std::sin(a)));
         }
         for (uint32_t i = 0; i < uint32_t(n); ++i) {
             m.indices.insert(m.indices.end(), {0u, 1 + i, 1 + (i + 1) % n});
@@ -175,7 +199,7 @@ Mesh make_builtin(uint32_t shape) {
                     p[u]     = a;
                     p[v]     = b;
                     nn[axis] = sign;
-                    vertex(p[0], p[1], p[2], nn[0], nn[1], nn[2]);
+                    vertex(p[0], p[1], p[2], nn[0], nn[1], nn[2], 0.5 * (a + 1), 0.5 * (1 - b));
                 }
                 // (u, v, axis) is right-handed: counter-clockwise in (u, v) faces +axis
                 if (sign > 0) {
@@ -228,8 +252,11 @@ Mesh make_builtin(uint32_t shape) {
             area += 0.5 * std::sqrt(x * x + y * y + z * z);
         }
         double const s = std::sqrt(4.0 * 3.14159265358979323846 / area);
+        double const pi = 3.14159265358979323846;
         for (auto const& p : v) {
-            vertex(s * p[0], s * p[1], s * p[2], p[0], p[1], p[2]);
+            // per vertex; triangles across the u seam interpolate between 1 and 0
+            vertex(s * p[0], s * p[1], s * p[2], p[0], p[1], p[2], (-std::atan2(p[0], p[2]) + pi) / (2.0 * pi),
+                   std::acos(std::clamp(p[1], -1.0, 1.0)) / pi);
         }
         for (auto const& [a, b, c] : f) {
             m.indices.insert(m.indices.end(), {a, b, c});
@@ -324,6 +351,68 @@ int32_t compile_scene() {
     std::vector<uint32_t> grid_images;  // image id of each scene.grids entry
     std::map<uint32_t, uint32_t> scene_mesh;  // engine shape id -> scene mesh index
 
+    // Texture maps: each (image, use, sampler, scale) once, its texels decoded for the use.
+    std::map<std::tuple<uint32_t, uint32_t, bool, bool, float, float>, uint32_t> textures;
+    auto const texture = [&](uint32_t image, uint32_t use, Material_maps const& mm, float const scale[2]) {
+        auto const key = std::make_tuple(image, use, mm.nearest, mm.clamp, scale[0], scale[1]);
+        auto const it  = textures.find(key);
+        if (it != textures.end()) {
+            return it->second;
+        }
+        Image const&              img = engine->images[image];
+        spb::render::Texture_desc t;
+        t.width    = img.dims[0];
+        t.height   = img.dims[1];
+        t.nearest  = mm.nearest;
+        t.clamp    = mm.clamp;
+        t.scale[0] = scale[0];
+        t.scale[1] = scale[1];
+        size_t const texels = size_t(t.width) * t.height;
+        uint32_t const c    = img.channels;
+        if (use == 0) {
+            // colour (Byte3_sRGB / Float3, texture.cpp:60-110): sRGB-encoded bytes to linear, then
+            // sRGB -> AP1; one-channel images as grey
+            t.channels = 3;
+            t.texels.resize(3 * texels);
+            for (size_t i = 0; i < texels; ++i) {
+                float rgb[3];
+                for (int k = 0; k < 3; ++k) {
+                    float v = img.pixels[i * c + std::min<uint32_t>(k, c - 1)];
+                    if (img.encoded_bytes) {
+                        v = v <= 0.04045f ? v / 12.92f : std::pow((v + 0.055f) / 1.055f, 2.4f);
+                    }
+                    rgb[k] = v;
+                }
+                V3 const ap1 = img.encoded_bytes ? srgb_to_ap1(V3{rgb[0], rgb[1], rgb[2]}) : V3{rgb[0], rgb[1], rgb[2]};
+                t.texels[3 * i]     = ap1.x;
+                t.texels[3 * i + 1] = ap1.y;
+                t.texels[3 * i + 2] = ap1.z;
+            }
+        } else {
+            // surface: roughness (X) and, for the Surface use of a 2+ channel image, metallic (Y)
+            t.channels = (use == 2 && c >= 2) ? 2 : 1;
+            t.texels.resize(t.channels * texels);
+            for (size_t i = 0; i < texels; ++i) {
+                for (uint32_t k = 0; k < t.channels; ++k) {
+                    t.texels[t.channels * i + k] = img.pixels[i * c + k];
+                }
+            }
+        }
+        scene.textures.push_back(std::move(t));
+        return textures[key] = uint32_t(scene.textures.size());
+    };
+    for (size_t k = 0; k < engine->materials.size() && k < engine->material_maps.size(); ++k) {
+        Material_maps const& mm = engine->material_maps[k];
+        Material&            m  = scene.materials[k];
+        if (mm.color != Null && mm.color < engine->images.size()) {
+            m.color_map = texture(mm.color, 0, mm, mm.color_scale);
+        }
+        if (mm.surface != Null && mm.surface < engine->images.size()) {
+            m.surface_map      = texture(mm.surface, mm.surface_usage, mm, mm.surface_scale);
+            m.surface_channels = scene.textures[m.surface_map - 1].channels;
+        }
+    }
+
     for (Entity const& e : engine->entities) {
         if (e.camera || e.shape == Null) {
             continue;
@@ -349,6 +438,7 @@ int32_t compile_scene() {
             spb::render::Mesh_desc md;
             md.positions = mesh.positions;
             md.normals   = mesh.normals;
+            md.uvs       = mesh.uvs;
             md.indices   = mesh.indices;
             md.tri_slot.resize(mesh.indices.size() / 3);
             for (size_t t = 0; t < md.tri_slot.size(); ++t) {
@@ -512,6 +602,51 @@ bool read_vec3(spb::json::Value const* v, double out[3]) {
     return true;
 }
 
+// An image file (PNG or EXR) as a new image; Null (with a logged reason) if it cannot be read.
+uint32_t load_image_file(std::string const& path) {
+    spb::image_io::Pixels px;
+    std::string           error;
+    if (!spb::image_io::read_image(path, px, error)) {
+        log(SU_LOG_ERROR, "texture: " + error);
+        return Null;
+    }
+    Image img;
+    img.dims[0]       = px.width;
+    img.dims[1]       = px.height;
+    img.dims[2]       = 1;
+    img.channels      = px.channels;
+    img.pixels        = std::move(px.values);
+    img.encoded_bytes = px.encoded_bytes;
+    engine->images.push_back(std::move(img));
+    return uint32_t(engine->images.size() - 1);
+}
+
+// A texture description's image ({"id": image} or {"file": name}, read_texture_description,
+// material_provider.cpp:895-946) and its uv scale; false if it names none.
+bool texture_image(spb::json::Value const& v, uint32_t& image, float scale[2]) {
+    if (!v.is_object()) {
+        return false;
+    }
+    spb::json::Value const* id   = v.find("id");
+    spb::json::Value const* file = v.find("file");
+    if (id && id->is_number()) {
+        image = uint32_t(id->number);
+    } else if (file && file->is_string()) {
+        image = load_image_file(resolve(file->string, ""));
+    } else {
+        return false;
+    }
+    if (spb::json::Value const* sc = v.find("scale")) {
+        if (sc->is_array() && sc->array.size() >= 2) {
+            scale[0] = float(sc->array[0].number);
+            scale[1] = float(sc->array[1].number);
+        } else if (sc->is_number()) {
+            scale[0] = scale[1] = float(sc->number);
+        }
+    }
+    return true;
+}
+
 // Row-major object-to-world matrix of a "transformation" object, as json::read_transformation
 // (json.cpp:252-296) reads it: 16 numbers, or position / scale / rotation (Euler degrees, the
 // basis Rz * Rx * Ry of json.cpp:216-227 with the rotation matrices of matrix3x3.inl:61-104)
@@ -647,6 +782,15 @@ uint32_t load_mesh_file(std::string const& path) {
         p[i] = float(pos->array[i].number);
         n[i] = float(nrm->array[i].number);
     }
+    // "texture_coordinates_0": two per vertex (triangle_json_handler.cpp:189-199)
+    std::vector<float>      uv;
+    spb::json::Value const* tc = verts->find("texture_coordinates_0");
+    if (tc && tc->is_array() && tc->array.size() == 2 * (p.size() / 3)) {
+        uv.resize(tc->array.size());
+        for (size_t i = 0; i < uv.size(); ++i) {
+            uv[i] = float(tc->array[i].number);
+        }
+    }
     std::vector<uint32_t> ind(idx->array.size());
     for (size_t i = 0; i < ind.size(); ++i) {
         ind[i] = uint32_t(idx->array[i].number);
@@ -660,8 +804,8 @@ uint32_t load_mesh_file(std::string const& path) {
         }
     }
     return su_create_triangle_mesh_async(uint32_t(ind.size() / 3), uint32_t(p.size() / 3), 3, p.data(), 3, n.data(),
-                                         0, nullptr, 0, nullptr, ind.data(), uint32_t(parts.size() / 3),
-                                         parts.empty() ? nullptr : parts.data());
+                                         0, nullptr, uv.empty() ? 0 : 2, uv.empty() ? nullptr : uv.data(), ind.data(),
+                                         uint32_t(parts.size() / 3), parts.empty() ? nullptr : parts.data());
 }
 
 // Built-in shape names (sprout.h's SU_SHAPE_* ids).
@@ -1068,6 +1212,7 @@ SU_LIBRARY_API int32_t su_clear(void) {
     engine->meshes.clear();
     engine->materials.clear();
     engine->material_grids.clear();
+    engine->material_maps.clear();
     engine->images.clear();
     engine->camera_entity = Null;
     engine->frame_started = false;
@@ -1275,6 +1420,7 @@ SU_LIBRARY_API uint32_t su_create_image(uint32_t pixel_type, uint32_t num_channe
             img.pixels[i * num_channels + c] = v;
         }
     }
+    img.encoded_bytes = bytes == 1;
     engine->images.push_back(std::move(img));
     engine->scene_dirty = true;
     return uint32_t(engine->images.size() - 1);
@@ -1297,8 +1443,9 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
     std::string const&      type = rendering->object.front().first;
     spb::json::Value const& desc = rendering->object.front().second;
 
-    Material m{};
-    Grid_ref grid;
+    Material      m{};
+    Grid_ref      grid;
+    Material_maps maps;
     m.two_sided = spb::json::bool_or(desc.find("two_sided"), false) ? 1u : 0u;
     if (type == "Light") {
         // material_provider.cpp:298-364: "emission" is a radiance, default 10
@@ -1327,6 +1474,70 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
         if (read_color(desc.find("emission"), emission) &&
             (emission.x > 0.f || emission.y > 0.f || emission.z > 0.f)) {
             log(SU_LOG_WARNING, "su_create_material: Substitute emission is ignored by this renderer");
+        }
+        m.color = color;
+        m.f0d   = f0d;
+        // Texture maps (load_substitute, material_provider.cpp:483-600): "color" and
+        // "roughness" as texture descriptions (with an optional constant "value"), "surface"
+        // (roughness and metallic), or a "textures" array with a "usage" per entry.
+        auto const bad_image = [&](uint32_t image) {
+            return image >= engine->images.size() || engine->images[image].dims[2] != 1;
+        };
+        if (spb::json::Value const* c = desc.find("color"); c && c->is_object()) {
+            if (texture_image(*c, maps.color, maps.color_scale) && bad_image(maps.color)) {
+                log(SU_LOG_ERROR, "su_create_material: colour texture names no 2-D image");
+                return Null;
+            }
+        }
+        if (spb::json::Value const* rv = desc.find("roughness"); rv && rv->is_object()) {
+            float const value = float(spb::json::number_or(rv->find("value"), 0.8));
+            float const rr    = std::max(value, spb::shading::Min_roughness);
+            m.alpha           = rr * rr;
+            if (texture_image(*rv, maps.surface, maps.surface_scale)) {
+                maps.surface_usage = 1;
+            }
+        }
+        if (spb::json::Value const* sv = desc.find("surface"); sv && sv->is_object()) {
+            if (texture_image(*sv, maps.surface, maps.surface_scale)) {
+                maps.surface_usage = 2;
+            }
+        }
+        if (spb::json::Value const* tv = desc.find("textures"); tv && tv->is_array()) {
+            for (auto const& t : tv->array) {
+                std::string const usage = spb::json::string_or(t.find("usage"), "");
+                uint32_t          image = Null;
+                float             scale[2] = {1.f, 1.f};
+                if ((usage != "Color" && usage != "Surface" && usage != "Roughness") ||
+                    !texture_image(t, image, scale)) {
+                    log(SU_LOG_WARNING, "su_create_material: texture usage \"" + usage + "\" is not supported");
+                    continue;
+                }
+                if (usage == "Color") {
+                    maps.color = image;
+                    std::copy(scale, scale + 2, maps.color_scale);
+                } else {
+                    maps.surface       = image;
+                    maps.surface_usage = usage == "Surface" ? 2 : 1;
+                    std::copy(scale, scale + 2, maps.surface_scale);
+                }
+            }
+        }
+        if ((maps.color != Null && bad_image(maps.color)) || (maps.surface != Null && bad_image(maps.surface))) {
+            log(SU_LOG_ERROR, "su_create_material: texture names no 2-D image");
+            return Null;
+        }
+        if (spb::json::Value const* sampler = desc.find("sampler")) {
+            // read_sampler_settings, material_provider.cpp:866-892
+            if (spb::json::Value const* f = sampler->find("filter"); f && f->is_string()) {
+                maps.nearest = f->string == "Nearest";
+            }
+            spb::json::Value const* a = sampler->find("address");
+            if (a && a->is_array() && !a->array.empty()) {
+                a = &a->array[0];
+            }
+            if (a && a->is_string()) {
+                maps.clamp = a->string == "Clamp";
+            }
         }
     } else if (type == "Volumetric") {
         // material_provider.cpp:767-849 (homogeneous case): colour 0.5 by default, attenuation
@@ -1408,6 +1619,7 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
     }
     engine->materials.push_back(m);
     engine->material_grids.push_back(grid);
+    engine->material_maps.push_back(maps);
     engine->scene_dirty = true;
     return uint32_t(engine->materials.size() - 1);
 }
@@ -1429,7 +1641,7 @@ SU_LIBRARY_API uint32_t su_create_material_from_file(char const* filename) {
 SU_LIBRARY_API uint32_t su_create_triangle_mesh_async(
     uint32_t num_triangles, uint32_t num_vertices, uint32_t positions_stride,
     float const* positions, uint32_t normals_stride, float const* normals, uint32_t /*tangents_stride*/,
-    float const* /*tangents*/, uint32_t /*uvs_stride*/, float const* /*uvs*/, uint32_t const* indices,
+    float const* /*tangents*/, uint32_t uvs_stride, float const* uvs, uint32_t const* indices,
     uint32_t num_parts, uint32_t const* parts) {
     if (!engine) {
         return Null;
@@ -1447,6 +1659,14 @@ SU_LIBRARY_API uint32_t su_create_triangle_mesh_async(
         for (int k = 0; k < 3; ++k) {
             mesh.positions[3 * v + k] = positions[size_t(v) * positions_stride + k];
             mesh.normals[3 * v + k]   = normals[size_t(v) * normals_stride + k];
+        }
+    }
+    // texture coordinates (optional; zero without them)
+    mesh.uvs.assign(2 * size_t(num_vertices), 0.f);
+    if (uvs && uvs_stride >= 2) {
+        for (uint32_t v = 0; v < num_vertices; ++v) {
+            mesh.uvs[2 * v]     = uvs[size_t(v) * uvs_stride];
+            mesh.uvs[2 * v + 1] = uvs[size_t(v) * uvs_stride + 1];
         }
     }
     mesh.indices.resize(3 * size_t(num_triangles));

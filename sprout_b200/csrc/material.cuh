@@ -136,6 +136,15 @@ struct Material {
     V3       mu_s;       // scattering coefficient per metre (Volume)
     uint32_t medium;     // Volume: 0 homogeneous, else 1 + index of the density-grid medium
     uint32_t pad;
+    // Substitute texture maps: the base colour and the dielectric F0 the per-hit parameters are
+    // rebuilt from, and 1 + the index of the colour and surface textures (0: none); the surface
+    // texture holds roughness, and metallic too when surface_channels is 2.
+    V3       color;
+    float    f0d;
+    uint32_t color_map;
+    uint32_t surface_map;
+    uint32_t surface_channels;
+    uint32_t pad2;
 };
 
 constexpr uint32_t Type_substitute = 0;

@@ -82,6 +82,15 @@ struct Medium_gpu {
     uint32_t      pad;
 };
 
+// A material texture (Texture_desc): texels as float4 (unused components 0), x fastest.
+struct Texture_gpu {
+    float4 const* texels;
+    int           w, h;
+    uint32_t      flags;  // bit 0: nearest filter; bit 1: clamp address mode (else repeat)
+    float         su, sv;  // uv scale
+    uint32_t      pad[2];
+};
+
 struct Scene_gpu {
     uint4 const*              nodes;
     float4 const*             tris;
@@ -105,6 +114,8 @@ struct Scene_gpu {
     uint32_t const*           inst_materials;  // per instance slot: index into materials
     uint32_t                  instanced;       // 1: two-level trees, hit records name instances
     uint32_t*                 tracking_capped;  // counts tracking segments that reached their step cap
+    float2 const*             uvs;       // per vertex, parallel to positions
+    Texture_gpu const*        textures;  // Material::color_map / surface_map - 1 index this
 };
 
 // What shading reads of an instance: its object-to-world map (rows: world_k =
@@ -984,6 +995,65 @@ __device__ float sample_density(Medium_gpu const& g, V3 uvw) {
     return (1.f - r) * b0 + r * b1;
 }
 
+// A material texture at uv (Nearest_2D / Linear_2D, texture_sampler.cpp:14-121): uv scaled,
+// wrapped or clamped, then the texel it falls in, or the bilinear blend of the four texels
+// around it (texel centres at half-integer positions).
+__device__ float4 sample_texture(Texture_gpu const& t, float2 uv) {
+    bool const  repeat = !(t.flags & 2u);
+    float const u      = address(uv.x * t.su, repeat);
+    float const v      = address(uv.y * t.sv, repeat);
+    if (t.flags & 1u) {
+        int const x = min(int(u * float(t.w)), t.w - 1);
+        int const y = min(int(v * float(t.h)), t.h - 1);
+        return __ldg(t.texels + size_t(y) * t.w + x);
+    }
+    float const fu = u * float(t.w) - 0.5f;
+    float const fv = v * float(t.h) - 0.5f;
+    float const x0 = floorf(fu);
+    float const y0 = floorf(fv);
+    int const   x  = int(x0);
+    int const   y  = int(y0);
+    int const   xa = lower_bound(x, t.w - 1, repeat);
+    int const   ya = lower_bound(y, t.h - 1, repeat);
+    int const   xb = increment(x, t.w - 1, repeat);
+    int const   yb = increment(y, t.h - 1, repeat);
+    float const a  = fu - x0;
+    float const b  = fv - y0;
+    float4 const c00 = __ldg(t.texels + size_t(ya) * t.w + xa);
+    float4 const c10 = __ldg(t.texels + size_t(ya) * t.w + xb);
+    float4 const c01 = __ldg(t.texels + size_t(yb) * t.w + xa);
+    float4 const c11 = __ldg(t.texels + size_t(yb) * t.w + xb);
+    float const  w00 = (1.f - a) * (1.f - b), w10 = a * (1.f - b), w01 = (1.f - a) * b, w11 = a * b;
+    return make_float4(w00 * c00.x + w10 * c10.x + w01 * c01.x + w11 * c11.x,
+                       w00 * c00.y + w10 * c10.y + w01 * c01.y + w11 * c11.y,
+                       w00 * c00.z + w10 * c10.z + w01 * c01.z + w11 * c11.z, 0.f);
+}
+
+// A Substitute material's parameters at a hit with texture coordinates uv
+// (Material_base::set_sample, substitute_base_material.inl:36-96): the colour map replaces the
+// colour; the surface map gives the roughness (mapped to [Min_roughness, 1], ggx.inl:47-49) and,
+// with two channels, the metallic value; albedo and F0 follow from them.
+__device__ void apply_texture_maps(Scene_gpu const& s, shading::Material& m, float2 uv) {
+    V3    color    = m.color;
+    float metallic = m.metallic;
+    if (m.color_map) {
+        float4 const c = sample_texture(s.textures[m.color_map - 1], uv);
+        color          = v3(c.x, c.y, c.z);
+    }
+    if (m.surface_map) {
+        float4 const c = sample_texture(s.textures[m.surface_map - 1], uv);
+        float const  r = c.x * (1.f - shading::Min_roughness) + shading::Min_roughness;
+        m.alpha        = r * r;
+        if (m.surface_channels >= 2) {
+            metallic = c.y;
+        }
+    }
+    m.metallic = metallic;
+    m.albedo   = (1.f - metallic) * color;
+    m.f0       = v3(m.f0d + metallic * (color.x - m.f0d), m.f0d + metallic * (color.y - m.f0d),
+                    m.f0d + metallic * (color.z - m.f0d));
+}
+
 // Walks the majorant cells that the texture-space ray o + t d crosses for t in [t0, t1],
 // clipped to the grid's unit cube (outside it the medium is empty, as outside the reference's
 // Gridtree, volumetric_octree.cpp:64-75).  Calls visit(cell (min, max) density, ta, tb) for
@@ -1643,7 +1713,15 @@ __global__ void __launch_bounds__(Shade_block)
             V3           ns  = shading::normalize(bw * vn[0] + uv.x * vn[1] + uv.y * vn[2]);
             V3 const     wo  = -dir_in;
             uint32_t const mat_id = wt.material;
-            shading::Material const mat = s.materials[mat_id];
+            shading::Material mat = s.materials[mat_id];
+            if (mat.color_map | mat.surface_map) {
+                float2 const t0  = s.uvs[wt.tri.x];
+                float2 const t1  = s.uvs[wt.tri.y];
+                float2 const t2  = s.uvs[wt.tri.z];
+                float2 const tuv = make_float2(bw * t0.x + uv.x * t1.x + uv.y * t2.x,
+                                               bw * t0.y + uv.x * t1.y + uv.y * t2.y);
+                apply_texture_maps(s, mat, tuv);
+            }
             float const  cos_o = shading::dot(geo_n, wo);
             bool const   front = cos_o > 0.f;
             bool const   emits = mat.type == shading::Type_light;
@@ -2079,6 +2157,9 @@ struct Renderer::Device {
     bool                 instanced      = false;  // two-level trees
     uint32_t             per_sm_flat    = 1;      // traversal blocks per SM (occupancy), flat trees
     uint32_t             per_sm_inst    = 1;      // ... two-level trees
+    float2*              uvs            = nullptr;
+    Texture_gpu*         textures       = nullptr;
+    std::vector<float4*> texture_texels;
     uint32_t*            golden_sorted  = nullptr;  // frac(j / phi) * 2^32, j < golden_n, ascending
     uint32_t             golden_n       = 0;
     std::vector<float*>  grid_density;  // one per density grid
@@ -2298,6 +2379,11 @@ Renderer::~Renderer() {
     free_ptr(d_->inst_shade);
     free_ptr(d_->inst_materials);
     free_ptr(d_->golden_sorted);
+    free_ptr(d_->uvs);
+    free_ptr(d_->textures);
+    for (float4*& t : d_->texture_texels) {
+        free_ptr(t);
+    }
     free_grids();
     Paths& p = d_->paths;
     free_ptr(p.ray_o);
@@ -2414,6 +2500,7 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     std::vector<uint4>               info;    // per triangle: vertices, material slot
     std::vector<float4>              pos;     // object space (world space when flattened)
     std::vector<float4>              nrm;
+    std::vector<float2>              uv;      // texture coordinates, parallel to pos
     std::vector<uint32_t>            inst_materials;
     std::vector<Instance_shade>      shade;
     std::vector<gpu::Instance_trace> trace;
@@ -2476,6 +2563,8 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
                 wpos.push_back(wy);
                 wpos.push_back(wz);
                 pos.push_back(make_float4(wx, wy, wz, 0.f));
+                uv.push_back(mesh.uvs.size() >= 2 * (v + 1) ? make_float2(mesh.uvs[2 * v], mesh.uvs[2 * v + 1])
+                                                            : make_float2(0.f, 0.f));
                 float const nx = mesh.normals[3 * v];
                 float const ny = mesh.normals[3 * v + 1];
                 float const nz = mesh.normals[3 * v + 2];
@@ -2557,6 +2646,8 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
                 for (size_t v = 0; v < mesh.positions.size() / 3; ++v) {
                     pos.push_back(make_float4(mesh.positions[3 * v], mesh.positions[3 * v + 1], mesh.positions[3 * v + 2], 0.f));
                     nrm.push_back(make_float4(mesh.normals[3 * v], mesh.normals[3 * v + 1], mesh.normals[3 * v + 2], 0.f));
+                    uv.push_back(mesh.uvs.size() >= 2 * (v + 1) ? make_float2(mesh.uvs[2 * v], mesh.uvs[2 * v + 1])
+                                                                : make_float2(0.f, 0.f));
                 }
                 uint32_t const vb = mesh_vbase[in.mesh];
                 for (uint32_t t = 0; t < nt; ++t) {
@@ -2751,6 +2842,36 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     SPB_RCUDA(upload(d_->tri_info, info.data(), info.size() * sizeof(uint4)));
     SPB_RCUDA(upload(d_->positions, pos.data(), pos.size() * sizeof(float4)));
     SPB_RCUDA(upload(d_->normals, nrm.data(), nrm.size() * sizeof(float4)));
+    SPB_RCUDA(upload(d_->uvs, uv.data(), uv.size() * sizeof(float2)));
+    // Material textures, each as float4 texels.
+    for (float4*& t : d_->texture_texels) {
+        free_ptr(t);
+    }
+    d_->texture_texels.assign(scene.textures.size(), nullptr);
+    std::vector<Texture_gpu> tex_table(scene.textures.size());
+    for (size_t k = 0; k < scene.textures.size(); ++k) {
+        Texture_desc const& td = scene.textures[k];
+        size_t const        n  = size_t(td.width) * td.height;
+        if (td.channels < 1 || td.channels > 4 || td.texels.size() != n * td.channels) {
+            error_ = "texture with inconsistent texels";
+            return SPB_ERROR_ARGUMENT;
+        }
+        std::vector<float4> texels(n, make_float4(0.f, 0.f, 0.f, 0.f));
+        for (size_t i = 0; i < n; ++i) {
+            float v[4] = {0.f, 0.f, 0.f, 0.f};
+            for (uint32_t c = 0; c < td.channels; ++c) {
+                v[c] = td.texels[i * td.channels + c];
+            }
+            texels[i] = make_float4(v[0], v[1], v[2], v[3]);
+        }
+        SPB_RCUDA(upload(d_->texture_texels[k], texels.data(), texels.size() * sizeof(float4)));
+        tex_table[k] = Texture_gpu{d_->texture_texels[k], int(td.width), int(td.height),
+                                   (td.nearest ? 1u : 0u) | (td.clamp ? 2u : 0u), td.scale[0], td.scale[1], {0, 0}};
+    }
+    free_ptr(d_->textures);
+    if (!tex_table.empty()) {
+        SPB_RCUDA(upload(d_->textures, tex_table.data(), tex_table.size() * sizeof(Texture_gpu)));
+    }
     SPB_RCUDA(upload(d_->materials, scene.materials.data(),
                      scene.materials.size() * sizeof(shading::Material)));
     SPB_RCUDA(upload(d_->light_nodes, tree.nodes.data(), tree.nodes.size() * sizeof(float)));
@@ -3117,6 +3238,8 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     sg.inst_materials = d_->inst_materials;
     sg.instanced      = d_->instanced ? 1u : 0u;
     sg.tracking_capped = d_->counters + Overflow_slot + 2;
+    sg.uvs             = d_->uvs;
+    sg.textures        = d_->textures;
 
     cudaStream_t const st = d_->stream;
     uint32_t* const    ctr = d_->counters;

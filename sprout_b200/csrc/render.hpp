@@ -29,8 +29,22 @@ struct Grid_medium {
 struct Mesh_desc {
     std::vector<float>    positions;  // 3 per vertex
     std::vector<float>    normals;    // 3 per vertex (shading)
+    std::vector<float>    uvs;        // 2 per vertex (texture coordinates), or empty
     std::vector<uint32_t> indices;    // 3 per triangle
     std::vector<uint32_t> tri_slot;   // material slot per triangle
+};
+
+// A 2-D texture of a material, its texels already decoded for their use (colour: linear
+// ACEScg; surface: roughness, metallic), sampled bilinearly or nearest, repeating or clamped,
+// at the hit's texture coordinates times scale (texture_sampler.cpp Linear_2D / Nearest_2D).
+struct Texture_desc {
+    uint32_t           width    = 0;
+    uint32_t           height   = 0;
+    uint32_t           channels = 0;  // 1 to 3 values per texel in texels
+    std::vector<float> texels;
+    bool               nearest  = false;
+    bool               clamp    = false;
+    float              scale[2] = {1.f, 1.f};
 };
 
 // A prop: a mesh placed by a row-major object-to-world matrix (translation in the last row, as
@@ -55,6 +69,7 @@ struct Scene_desc {
     std::vector<shading::Material>  materials;    // Volume materials: medium = 1 + grid medium
     std::vector<Density_grid>       grids;
     std::vector<Grid_medium>        media;
+    std::vector<Texture_desc>       textures;     // Material::color_map / surface_map - 1 index this
     float                           environment[3] = {0.f, 0.f, 0.f};  // uniform radiance at infinity
     bool                            environment_light = false;  // also sampled by next-event estimation
     // Two-level trees: -1 when flattening would hold more than four times the triangles of the
@@ -87,12 +102,12 @@ struct Settings {
     float    guide_fraction  = 0.5f;
     float    metal_fraction  = -1.f;  // at metallic surfaces; negative: guide_fraction
     uint32_t guide_batch     = 1u << 16;
-    uint32_t guide_steps     = 32;
+    uint32_t guide_steps     = 16;
     float    guide_lr        = 1e-2f;
     uint32_t record_depth    = 2;
     uint32_t guide_seed      = 7;
-    uint32_t guide_pass_spp  = 2;   // samples per pixel between training steps
-    uint32_t guide_train_spp = 32;  // samples per pixel after which training stops (0: never)
+    uint32_t guide_pass_spp  = 1;   // samples per pixel between training steps
+    uint32_t guide_train_spp = 16;  // samples per pixel after which training stops (0: never)
     uint32_t guide_depth     = 255;  // vertices of depth below this are guided
     // Paths per wave and traversal blocks per SM; 0: chosen by the online autotuner.
     uint32_t wave_paths          = 0;

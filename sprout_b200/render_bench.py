@@ -256,8 +256,8 @@ def network_roofline(stats):
 REFERENCE_64K = pathlib.Path(__file__).resolve().parent.parent / "tests" / "golden" / "doorway_reference_64k.npz"
 
 # Training schedules of the guided integrator ("guiding" key of the PTMIS integrator): this
-# renderer's defaults (passes of 2 spp, 32 Adam steps of 65,536 records, learning rate 1e-2,
-# training until 32 spp), and the configuration's own (batches of 2^18 records, learning rate
+# renderer's defaults (passes of 1 spp, 16 Adam steps of 65,536 records, learning rate 1e-2,
+# training until 16 spp), and the configuration's own (batches of 2^18 records, learning rate
 # 1e-3, the rest as the defaults).
 GUIDING_SCHEDULES = {
     "tuned": True,

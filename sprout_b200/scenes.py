@@ -633,3 +633,68 @@ def doorway(su, width: int = 1280, height: int = 720, spp: int = 64, seed: int =
     su.set_transformation(prop, np.eye(4, dtype=np.float32))
     su.su_create_light(prop)
     return cam
+
+
+def checker_image(size: int = 64, checks: int = 8, colors=((200, 40, 30), (30, 60, 210))):
+    """A size x size RGB byte image of checks x checks squares of two colours."""
+    y, x = np.mgrid[0:size, 0:size]
+    odd = ((x * checks // size) + (y * checks // size)) % 2 == 1
+    img = np.empty((size, size, 3), np.uint8)
+    img[~odd] = colors[0]
+    img[odd] = colors[1]
+    return img
+
+
+def surface_image(size: int = 32, stripes: int = 4):
+    """A size x size two-channel byte image: roughness (X) in stripes of 0.1 and 0.9 along x,
+    metallic (Y) 1 in the lower half of the rows, else 0.  (Bytes, because the reference
+    renderer returns NaN for float images used as surface or roughness maps.)"""
+    y, x = np.mgrid[0:size, 0:size]
+    img = np.empty((size, size, 2), np.uint8)
+    img[..., 0] = np.where((x * stripes // size) % 2 == 0, 26, 230)
+    img[..., 1] = np.where(y >= size // 2, 255, 0)
+    return img
+
+
+def textured_room(su, width: int, height: int, spp: int, max_bounces: int = 8, integrator=None):
+    """The Cornell box with texture maps instead of the sphere's metal: the back wall's colour
+    from a checker image (byte sRGB, uv scale 2, so the image repeats twice), the floor's
+    roughness and metallic from a two-channel byte image (Surface use), and a rotated block
+    whose colour comes from the checker image through a "textures" entry, sampled with the
+    Nearest filter; every quad carries texture coordinates over [0, 1]^2."""
+    cam = su.su_create_camera_perspective(width, height, math.radians(40.0))
+    su.set_transformation(cam, translation(0.0, 1.0, -3.4))
+    ptmis = {"min_bounces": 4, "max_bounces": max_bounces}
+    ptmis.update(integrator or {})
+    su.su_create_integrators(json.dumps({"surface": {"PTMIS": ptmis}}).encode())
+    su.su_create_sampler(spp)
+    su.su_create_defaults()
+    checker = su.image2d(checker_image())
+    surface = su.image2d(surface_image())
+    back = _material(su, "Substitute", color={"id": int(checker), "scale": 2.0}, roughness=1.0)
+    floor = _material(su, "Substitute", color=[0.8, 0.8, 0.75], surface={"id": int(surface)})
+    white = _material(su, "Substitute", color=[0.75, 0.75, 0.75], roughness=1.0, metallic=0.0)
+    red = _material(su, "Substitute", color=[0.75, 0.05, 0.05], roughness=1.0, metallic=0.0)
+    green = _material(su, "Substitute", color=[0.05, 0.75, 0.05], roughness=1.0, metallic=0.0)
+    block = _material(su, "Substitute", textures=[{"id": int(checker), "usage": "Color"}], roughness=0.6,
+                      sampler={"filter": "Nearest"})
+    light = _material(su, "Light", emission=[17.0, 17.0, 17.0])
+    geo = cornell_geometry(1)
+    del geo["sphere"]
+    quad_uv = np.array([[0, 1], [1, 1], [1, 0], [0, 0]], np.float32)
+    assign = {"floor": floor, "ceiling": white, "back": back, "left": red, "right": green, "light": light}
+    for name, (pos, nrm, idx) in geo.items():
+        prop = su.prop(su.mesh(pos, nrm, idx, uvs=quad_uv), [assign[name]])
+        su.set_transformation(prop, np.eye(4, dtype=np.float32))
+        if name == "light":
+            su.su_create_light(prop)
+    # a textured block: the unit box with per-face texture coordinates
+    pos, nrm, idx = box()
+    uv = np.tile(quad_uv, (len(pos) // 4, 1))
+    prop = su.prop(su.mesh(pos, nrm, idx, uvs=uv), [block])
+    m = np.diag([0.6, 0.6, 0.6, 1.0]).astype(np.float32)
+    c, sn = math.cos(0.4), math.sin(0.4)
+    m[:3, :3] = np.array([[0.6 * c, 0, -0.6 * sn], [0, 0.6, 0], [0.6 * sn, 0, 0.6 * c]], np.float32)
+    m[3, :3] = (0.2, 0.3, 0.2)
+    su.set_transformation(prop, m)
+    return cam

@@ -69,6 +69,9 @@ CASES = {
     "take_room96": (96, 72, 4096, {"scene": "take", "take": "room.take"}, None),
     # the Cornell workload at its configured size: 512x512, the 81,920-triangle sphere
     "cornell512": (512, 512, 2048, {"sphere_subdivisions": 6}, None),
+    # texture maps: a checker colour map repeated by uv scale 2, a roughness / metallic surface
+    # map, a nearest-filtered colour map on a rotated block (byte and float images by id)
+    "textured96": (96, 72, 4096, {"scene": "textured"}, None),
     # the guiding workload's room at 320x180 (plain MIS), the image the guided integrator is
     # compared with at a size where its network sees realistic training passes
     "doorway320": (320, 180, 4096, {"scene": "doorway"}, None),
@@ -98,6 +101,8 @@ def build(su, w, h, spp, kwargs, density=None):
         return scenes.volume(su, w, h, spp, density, **kwargs)
     if name == "doorway":
         return scenes.doorway(su, w, h, spp, **kwargs)
+    if name == "textured":
+        return scenes.textured_room(su, w, h, spp, **kwargs)
     if name == "take":
         su.su_mount(str(TAKES) + "/")
         su.load_take(str(TAKES / kwargs["take"]), w, h)

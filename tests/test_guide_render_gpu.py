@@ -33,15 +33,19 @@ def rel_mse(x, r):
     return float(np.mean((k * x - k * r) ** 2 / ((k * r) ** 2 + 1e-2)))
 
 
+# A schedule for this small image, whose training passes see few paths: 16 passes of 2 spp, 32
+# Adam steps each (the default schedule is tuned for the 1280x720 frame).
+SMALL_IMAGE_SCHEDULE = {"pass_spp": 2, "steps": 32, "train_spp": 32}
+
+
 def test_guided_error_below_plain_at_equal_samples(reference):
     """At 64 spp (16 training passes of 2 spp, then inference only), summed over three sample
     seeds: guided error is at most 0.75 x plain.  Single seeds measured 0.65-0.71 at this small
-    image (each training pass sees only 30 k paths); the bench's 1280x720 frame reaches relMSE
-    0.01 with a third of plain's samples."""
+    image (each training pass sees only 30 k paths)."""
     e_plain = e_guided = 0.0
     for seed in range(3):
         plain, _, _ = doorway_frame(W, H, 64, None, seed=seed)
-        guided, _, _ = doorway_frame(W, H, 64, True, seed=seed)
+        guided, _, _ = doorway_frame(W, H, 64, SMALL_IMAGE_SCHEDULE, seed=seed)
         assert np.all(np.isfinite(guided))
         e_plain += rel_mse(plain, reference)
         e_guided += rel_mse(guided, reference)

@@ -48,6 +48,8 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
             scenes.volume(su, width, height, spp, density, **scene)
         elif name == "doorway":
             scenes.doorway(su, width, height, spp, **scene)
+        elif name == "textured":
+            scenes.textured_room(su, width, height, spp, **scene)
         elif name == "take":
             takes = GOLDEN.parent / "takes"
             assert su.su_mount((str(takes) + "/").encode()) == 0
@@ -73,7 +75,7 @@ def render(width, height, spp, progressive=False, iterations=0, **scene):
 CASES = ["cornell64_sub3", "cornell128_sub6", "cornell64_medium", "cornell64_emissive", "cornell64_thin_direct",
          "cornell64_grid",
          "cornell64_lights", "wavefront96", "builtins96", "builtins96_backdrop", "volume64",
-         "doorway96", "take_room96", "cornell512", "doorway320"]
+         "doorway96", "take_room96", "cornell512", "doorway320", "textured96"]
 
 
 @pytest.mark.parametrize("name", CASES)
