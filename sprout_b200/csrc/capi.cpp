@@ -1335,6 +1335,21 @@ SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
         if (pt) {
             s.min_bounces = uint32_t(spb::json::number_or(pt->find("min_bounces"), s.min_bounces));
             s.max_bounces = uint32_t(spb::json::number_or(pt->find("max_bounces"), s.max_bounces));
+            // "light_sampling": {"strategy": "Single" | "Adaptive", "splitting_threshold": t}
+            // (load_light_sampling, take_loader.cpp:995-1015; the threshold is used as t^4,
+            // Tree::set_splitting_threshold, light_tree.cpp:341-343)
+            if (spb::json::Value const* ls = pt->find("light_sampling"); ls && ls->is_object()) {
+                std::string const strategy = spb::json::string_or(ls->find("strategy"), "");
+                if (strategy == "Single") {
+                    s.light_split = false;
+                } else if (strategy == "Adaptive") {
+                    s.light_split = true;
+                }
+                if (spb::json::Value const* st = ls->find("splitting_threshold"); st && !st->is_string()) {
+                    float const t     = float(spb::json::number_or(st, 0.08));
+                    s.split_threshold = t * t * t * t;
+                }
+            }
             // "seed": the sample streams' seed (this renderer's extension, default 0), for
             // statistically independent renders of one scene
             s.seed = uint32_t(spb::json::number_or(pt->find("seed"), s.seed));

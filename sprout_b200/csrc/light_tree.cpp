@@ -127,19 +127,30 @@ struct Bin {
     Box    box;
     Cone   cone;
     double power = 0.0;
+    double power2 = 0.0;  // sum of squared powers (for the node's variance)
     int    count = 0;
 
     void add(Item const& it) {
         box.add(it.box);
         cone = merge(cone, it.cone);
         power += it.power;
+        power2 += it.power * it.power;
         ++count;
     }
     void add(Bin const& b) {
         box.add(b.box);
         cone = merge(cone, b.cone);
         power += b.power;
+        power2 += b.power2;
         count += b.count;
+    }
+    // Population variance of the powers (every light here has a positive power).
+    double variance() const {
+        if (count == 0) {
+            return 0.0;
+        }
+        double const mean = power / count;
+        return std::fabs(power2 / count - mean * mean);
     }
     double cost() const { return count ? power * box.area() * orientation_measure(cone) : 0.0; }
 };
@@ -163,7 +174,7 @@ struct Builder {
     }
 
     void write_node(uint32_t node, Bin const& b, uint32_t first, uint32_t count, uint32_t middle) {
-        float* n = &out.nodes[12 * size_t(node)];
+        float* n = &out.nodes[Light_node_floats * size_t(node)];
         double c[3], r2 = 0.0;
         for (int k = 0; k < 3; ++k) {
             c[k] = 0.5 * (b.box.lo[k] + b.box.hi[k]);
@@ -181,6 +192,11 @@ struct Builder {
         n[9]  = bits(first);
         n[10] = bits(count);
         n[11] = bits(middle);
+        double const mean = b.count ? b.power / b.count : 0.0;
+        n[12] = float(b.variance());
+        n[13] = bits(uint32_t(b.count));
+        n[14] = float(b.variance() + mean * mean);
+        n[15] = 0.f;
     }
 
     // Builds the subtree of index[begin, end) into node; returns its depth.
@@ -265,7 +281,7 @@ struct Builder {
         }
         uint32_t const child = out.num_nodes;
         out.num_nodes += 2;
-        out.nodes.resize(12 * size_t(out.num_nodes));
+        out.nodes.resize(Light_node_floats * size_t(out.num_nodes));
         write_node(node, all, child, 0, mid);
         uint32_t const d0 = build(child, begin, mid);
         uint32_t const d1 = build(child + 1, mid, end);
@@ -310,7 +326,7 @@ void build_light_tree(std::vector<Light_input> const& lights, uint32_t num_slots
     std::vector<uint32_t> index(lights.size());
     std::iota(index.begin(), index.end(), 0u);
     out.num_nodes = 1;
-    out.nodes.resize(12);
+    out.nodes.resize(Light_node_floats);
     Builder b{items, index, out};
     out.depth      = b.build(0, 0, uint32_t(lights.size()));
     out.num_lights = uint32_t(lights.size());
@@ -335,6 +351,32 @@ void build_light_tree(std::vector<Light_input> const& lights, uint32_t num_slots
         out.tris.back() = Builder::bits(in.material);
         out.order[in.slot] = o;
     }
+}
+
+uint32_t max_split_picks(Light_tree const& tree, uint32_t start) {
+    if (tree.num_nodes == 0) {
+        return 0;
+    }
+    struct Walk {
+        Light_tree const& t;
+        uint32_t          count(uint32_t node, uint32_t depth) const {
+            float const* n = &t.nodes[Light_node_floats * size_t(node)];
+            uint32_t     first, lights;
+            std::memcpy(&first, &n[9], 4);
+            std::memcpy(&lights, &n[10], 4);
+            if (lights != 0) {
+                return depth < Max_split_depth ? lights : 1u;
+            }
+            if (depth >= Max_split_depth) {
+                return 1u;
+            }
+            if (depth == Max_split_depth - 1) {
+                return 2u;
+            }
+            return count(first, depth + 1) + count(first + 1, depth + 1);
+        }
+    };
+    return Walk{tree}.count(0, start);
 }
 
 }  // namespace spb::render

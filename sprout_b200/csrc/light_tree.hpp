@@ -25,10 +25,15 @@ struct Light_input {
 };
 
 // Device-ready arrays, 4 floats per float4.
-//   nodes:  3 float4 per node: (centre, radius), (axis, cos spread), (power, first, count,
-//           middle) with first/count/middle stored as uint32 bits.  Inner nodes have count 0
-//           and their children at first and first + 1; lights of the subtree [b, e) split at
-//           middle (left child: order < middle).  Leaves hold lights first .. first+count-1.
+//   nodes:  4 float4 per node: (centre, radius), (axis, cos spread), (power, first, count,
+//           middle), (variance, lights, variance + mean^2, 0 -- the renderer's split radius^2)
+//           with first/count/middle/lights
+//           stored as uint32 bits.  Inner nodes have count 0 and their children at first and
+//           first + 1; lights of the subtree [b, e) split at middle (left child: order <
+//           middle).  Leaves hold lights first .. first+count-1.  variance and mean are the
+//           population variance and the mean of the subtree's light powers and lights their
+//           number (the inputs of the splitting decision, light_tree.cpp:197-224 and
+//           light_tree_builder.cpp:86-102).
 //   cones:  3 float4 per light in tree order: (centre, radius), (normal, cos spread),
 //           (power, 0, 0, 0)
 //   tris:   3 float4 per light in tree order: (a, area), (b - a, 0), (c - a, material index bits)
@@ -43,7 +48,19 @@ struct Light_tree {
     uint32_t              depth      = 0;
 };
 
-constexpr uint32_t Light_leaf_size = 4;
+constexpr uint32_t Light_leaf_size   = 4;
+constexpr uint32_t Light_node_floats = 16;
+// Splitting (Tree::random_light with split, light_tree.cpp:363-461): while a walk is above
+// this depth, a node whose split test passes sends the walk into both children, and a leaf
+// passes all its lights; at most Max_light_picks lights per walk (Tree::Max_lights).
+constexpr uint32_t Max_split_depth = 5;
+constexpr uint32_t Max_light_picks = 1u << (Max_split_depth + 1);
+
+// The most lights one splitting walk that starts at depth `start` can return
+// (Build_node::count_max_splits, light_tree.cpp:156-170, over this tree's shape): a leaf
+// reached above Max_split_depth gives all its lights, a node at Max_split_depth - 1 gives two
+// picks, a deeper node one.
+uint32_t max_split_picks(Light_tree const& tree, uint32_t start);
 
 void build_light_tree(std::vector<Light_input> const& lights, uint32_t num_slots,
                       Light_tree& out);

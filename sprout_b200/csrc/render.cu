@@ -63,10 +63,11 @@ constexpr uint32_t Class_boundary   = 2;  // ... of participating-medium boundar
 constexpr uint32_t Class_instance   = 4;  // ... of top-level leaves (instances)
 
 // Counter block (uint32): per bounce b, [8b] extension count, [8b+1] shadow count,
-// [8b+2] extend fetch, [8b+3] shadow fetch, [8b+4] transmittance count; then the overflow
-// counter.
+// [8b+2] extend fetch, [8b+3] shadow fetch, [8b+4] transmittance count, [8b+5] picks of split
+// light selections, [8b+6] split records; then the overflow counter.
 constexpr uint32_t Counter_stride = 8;
 constexpr uint32_t Graph_max_paths = 1u << 21;  // largest wave replayed from a CUDA graph
+constexpr uint64_t Pick_budget     = 24ull << 30;  // bytes of picks a wave may hold
 constexpr uint32_t Counter_words  = Counter_stride * Max_bounce_slots + 4;
 constexpr uint32_t Overflow_slot  = Counter_stride * Max_bounce_slots;
 
@@ -99,7 +100,7 @@ struct Scene_gpu {
     float4 const*             positions;
     float4 const*             normals;
     shading::Material const*  materials;
-    float4 const*             light_nodes;  // light tree (light_tree.hpp): 3 per node
+    float4 const*             light_nodes;  // light tree (light_tree.hpp): 4 per node
     float4 const*             light_cones;  // 3 per light in tree order: bounds for importance
     float4 const*             light_tris;   // 3 per light in tree order: (a, area), e1, (e2, tri)
     uint32_t const*           light_order;  // per triangle: tree order, 0xFFFFFFFF if no light
@@ -116,6 +117,11 @@ struct Scene_gpu {
     uint32_t*                 tracking_capped;  // counts tracking segments that reached their step cap
     float2 const*             uvs;       // per vertex, parallel to positions
     Texture_gpu const*        textures;  // Material::color_map / surface_map - 1 index this
+    // Light selection splits at vertices of depth below split_bounces (0: never, Single light
+    // sampling); the split tree walk starts at depth split_depth_bias.
+    uint32_t                  split_bounces;
+    uint32_t                  split_depth_bias;
+    float                     split_scale;  // 3 (1 / t - 1)^2 for the splitting threshold t (split_node)
 };
 
 // What shading reads of an instance: its object-to-world map (rows: world_k =
@@ -183,12 +189,16 @@ struct Paths {
     float4*   sh_d;
     float4*   sh_L;
     float4*   prev_n;  // geometric normal at the last scattering vertex; w 1: medium vertex
-    // Second shadow ray of a vertex whose light selection is split (the environment and one
-    // emitter, see Split_bounces); its contributions accumulate in L2 (added to L by gather),
-    // so that no two kernel threads ever add to the same radiance.
-    float4*   sh2_o;
-    float4*   sh2_d;
-    float4*   sh2_L;
+    // Vertices whose light selection splits into several lights (select_lights): one record per
+    // vertex per bounce -- (shadow-ray origin, path) and (first pick, picks, depth, 0) -- and
+    // per selected light a pick: (direction, distance) and (contribution, record).  Shadow rays
+    // zero the contributions of occluded picks (and scale those through media); k_pick_sum
+    // then adds each record's picks in order to L2 (added to L by gather), so that no two
+    // kernel threads ever add to the same radiance and the sum does not depend on scheduling.
+    float4*   split_o;
+    uint4*    split_m;
+    float4*   pick_d;
+    float4*   pick_c;
     float4*   L2;
     // Path guiding, indexed by position in the current extension queue: the network inputs as
     // BF16 tiles of 128 entries in the tensor cores' operand order (guide_in), the predicted
@@ -215,8 +225,9 @@ constexpr int Record_float4 = 5;
 // kappa / (2 pi (1 - e^{-2 kappa})), so that a density evaluation takes one exponential per lobe.
 constexpr int Mixture_floats = 48;
 
-// Shadow-queue entries are path indices; this bit marks the vertex's second shadow ray.
-constexpr uint32_t Second_shadow = 0x80000000u;
+// Shadow-queue entries are path indices (the path's shadow slot) or, with this bit, pick
+// indices (a light of a split selection).
+constexpr uint32_t Pick_shadow = 0x80000000u;
 
 struct Cam {
     float3   left_top;
@@ -379,11 +390,14 @@ __device__ __forceinline__ float2 golden_2d(Wave const& w, uint32_t pixel, uint3
     return make_float2(fixed_to_unit(__ldg(w.golden_sorted + k) + off0), fixed_to_unit(off1 + i * Golden_step));
 }
 
-// Golden ratio dimensions: 2-D 0 the pixel position, 1 + 4 d + k the light point of light
-// sample k at vertex depth d, 1 + 4 d + 3 the BSDF (or guide) direction; 1-D 16 + 4 d + k the
-// light selection of light sample k, 16 + 4 d + 3 the BSDF lobe (or guide lobe), 32 + d the
-// choice between guide and BSDF.
-__device__ __forceinline__ uint32_t golden_light_2d(uint32_t depth, int k) { return 1u + 4u * depth + uint32_t(k); }
+// Golden ratio dimensions: 2-D 0 the pixel position, the light point of the l-th selected light
+// at vertex depth d 1 + 4 d + l for l < 3 and 64 + 64 d + l beyond (the reference gives each
+// light of a split selection its own dimension, pathtracer_mis.cpp:298-318), 1 + 4 d + 3 the
+// BSDF (or guide) direction; 1-D 16 + 4 d the light selection, 16 + 4 d + 3 the BSDF lobe (or
+// guide lobe), 32 + d the choice between guide and BSDF.
+__device__ __forceinline__ uint32_t golden_light_2d(uint32_t depth, uint32_t l) {
+    return l < 3u ? 1u + 4u * depth + l : 64u + 64u * depth + l;
+}
 __device__ __forceinline__ uint32_t golden_bsdf_2d(uint32_t depth) { return 1u + 4u * depth + 3u; }
 __device__ __forceinline__ uint32_t golden_light_1d(uint32_t depth, int k) { return 16u + 4u * depth + uint32_t(k); }
 __device__ __forceinline__ uint32_t golden_bsdf_1d(uint32_t depth) { return 16u + 4u * depth + 3u; }
@@ -536,10 +550,14 @@ __global__ void __launch_bounds__(Trace_block)
                 if (mine < num) {
                     path = queue[mine];
                     if (Any_hit) {
-                        uint32_t const pi     = path & ~Second_shadow;
-                        bool const     second = path & Second_shadow;
-                        gpu::start_ray(r, tv, second ? p.sh2_o[pi] : p.sh_o[pi],
-                                       second ? p.sh2_d[pi] : p.sh_d[pi]);
+                        if (path & Pick_shadow) {
+                            uint32_t const pk  = path & ~Pick_shadow;
+                            uint32_t const rec = __float_as_uint(p.pick_c[pk].w);
+                            float4 const   o   = p.split_o[rec];
+                            gpu::start_ray(r, tv, make_float4(o.x, o.y, o.z, 0.f), p.pick_d[pk]);
+                        } else {
+                            gpu::start_ray(r, tv, p.sh_o[path], p.sh_d[path]);
+                        }
                     } else {
                         gpu::start_ray(r, tv, p.ray_o[path], p.ray_d[path]);
                     }
@@ -560,16 +578,20 @@ __global__ void __launch_bounds__(Trace_block)
                 if (r.best_id == gpu::Miss) {
                     if (Media) {
                         transmit_queue[atomicAdd(transmit_count, 1u)] = path;
-                    } else {
-                        uint32_t const pi = path & ~Second_shadow;
-                        float4* const  Lp = (path & Second_shadow) ? p.L2 : p.L;
-                        float4 const   c  = (path & Second_shadow) ? p.sh2_L[pi] : p.sh_L[pi];
-                        float4         l  = Lp[pi];
+                    } else if (!(path & Pick_shadow)) {
+                        float4 const c = p.sh_L[path];
+                        float4       l = p.L[path];
                         l.x += c.x;
                         l.y += c.y;
                         l.z += c.z;
-                        Lp[pi] = l;
+                        p.L[path] = l;
                     }
+                } else if (path & Pick_shadow) {
+                    // occluded: the pick adds nothing
+                    float* const c = reinterpret_cast<float*>(p.pick_c + (path & ~Pick_shadow));
+                    c[0] = 0.f;
+                    c[1] = 0.f;
+                    c[2] = 0.f;
                 }
             } else {
                 p.hit_id[path] = r.best_id;
@@ -640,103 +662,210 @@ __device__ float light_importance(float4 sphere, float4 cone, float power, V3 p,
     return fmaxf(power * ce * cr / dist, 1e-30f);
 }
 
-// Picks a light (tree order) by walking the tree from the root with the random number r;
-// returns its index and sets pick to its probability.
-__device__ uint32_t pick_light(Scene_gpu const& s, V3 p, V3 n, bool total_sphere, float r,
-                               float& pick) {
-    float    pdf  = 1.f;
-    uint32_t node = 0;
-    for (int level = 0; level < 64; ++level) {
-        float4 const   meta  = s.light_nodes[3 * node + 2];
-        uint32_t const first = __float_as_uint(meta.y);
-        uint32_t const count = __float_as_uint(meta.z);
-        if (count != 0) {
-            float w[Light_leaf_size];
-            float sum = 0.f;
-            for (uint32_t k = 0; k < Light_leaf_size; ++k) {
-                w[k] = 0.f;
-                if (k < count) {
-                    uint32_t const l = first + k;
-                    w[k] = light_importance(s.light_cones[3 * l], s.light_cones[3 * l + 1],
-                                            s.light_cones[3 * l + 2].x, p, n, total_sphere);
-                    sum += w[k];
-                }
-            }
-            float    acc    = 0.f;
-            uint32_t chosen = count - 1;
-            for (uint32_t k = 0; k + 1 < count; ++k) {
-                acc += w[k];
-                if (r * sum < acc) {
-                    chosen = k;
-                    break;
-                }
-            }
-            pick = pdf * (w[chosen] / sum);
-            return first + chosen;
-        }
-        uint32_t const c0 = first;
-        float const    w0 = light_importance(s.light_nodes[3 * c0], s.light_nodes[3 * c0 + 1],
-                                             s.light_nodes[3 * c0 + 2].x, p, n, total_sphere);
-        float const    w1 = light_importance(s.light_nodes[3 * c0 + 3], s.light_nodes[3 * c0 + 4],
-                                             s.light_nodes[3 * c0 + 5].x, p, n, total_sphere);
-        float const    p0 = w0 / (w0 + w1);
-        if (r < p0) {
-            node = c0;
-            pdf *= p0;
-            r = fminf(r / p0, 0x1.fffffep-1f);
-        } else {
-            node = c0 + 1;
-            pdf *= 1.f - p0;
-            r = fminf((r - p0) / (1.f - p0), 0x1.fffffep-1f);
-        }
-    }
-    pick = 0.f;
-    return 0;
+// Light-tree nodes: 4 float4 each (light_tree.hpp): (centre, radius), (axis, cos spread),
+// (power, first, count, middle), (variance, lights, 0, 0).
+constexpr uint32_t Light_node_stride = 4;
+constexpr uint32_t Env_pick          = 0xFFFFFFFFu;  // a pick of the environment
+
+__device__ __forceinline__ float node_importance(Scene_gpu const& s, uint32_t node, V3 p, V3 n,
+                                                 bool total_sphere) {
+    float4 const* nd = s.light_nodes + Light_node_stride * node;
+    return light_importance(nd[0], nd[1], nd[2].x, p, n, total_sphere);
 }
 
-// Probability that pick_light from (p, n) returns the light at tree position order
-// (Tree::pdf, light_tree.cpp:564-640): the same importances along the path to its leaf.
-__device__ float light_pick_pdf(Scene_gpu const& s, V3 p, V3 n, bool total_sphere,
-                                uint32_t order) {
-    float    pdf  = 1.f;
-    uint32_t node = 0;
-    for (int level = 0; level < 64; ++level) {
-        float4 const   meta  = s.light_nodes[3 * node + 2];
-        uint32_t const first = __float_as_uint(meta.y);
-        uint32_t const count = __float_as_uint(meta.z);
+__device__ __forceinline__ float emitter_importance(Scene_gpu const& s, uint32_t l, V3 p, V3 n,
+                                                    bool total_sphere) {
+    return light_importance(s.light_cones[3 * l], s.light_cones[3 * l + 1], s.light_cones[3 * l + 2].x,
+                            p, n, total_sphere);
+}
+
+// Whether light selection at p descends into both children of a node (Node::split,
+// light_tree.cpp:197-224; Estevez and Kulla 2018, sec. 5).  With g = 1 / x^2 for x uniform
+// between the near and far side of the node's bounding sphere, a = max(d - r, 0.001) and
+// b = d + r: E[g] = 1 / (a b), E[g^2] = (b^3 - a^3) / (3 (b - a) a^3 b^3), V[g] = E[g^2] - E[g]^2;
+// with the variance ve and mean ee of the node's light powers, the estimate's variance is
+// s2 = ve V[g] + ve E[g]^2 + ee^2 V[g], and the node splits when 1 / (1 + sqrt(s2)) falls to
+// the threshold t, i.e. s2 >= S = (1 / t - 1)^2.  Multiplied by 3 (b - a) a^3 b^3 > 0 (under
+// which V[g] becomes (b - a)^3 and E[g]^2 becomes 3 (b - a) a b) and divided by b - a, the
+// test needs no division: (ve + ee^2) (b - a)^2 + 3 ve a b >= 3 S a^3 b^3.  b = a (a point
+// light at a distance) does not split, as the reference's undefined V[g] does not.
+// The host stores with each node the squared distance from its centre beyond which the test
+// cannot pass (0: nowhere; split_radius2), which most shading points are beyond.
+__device__ __forceinline__ bool split_node(Scene_gpu const& s, uint32_t node, V3 p) {
+    float4 const* nd  = s.light_nodes + Light_node_stride * node;
+    float4 const  var = nd[3];  // (ve, lights, ve + ee^2, split radius^2)
+    if (!(var.w > 0.f)) {
+        return false;
+    }
+    float4 const sph = nd[0];
+    V3 const     v   = v3(p.x - sph.x, p.y - sph.y, p.z - sph.z);
+    float const  d2  = shading::dot(v, v);
+    if (d2 >= var.w) {
+        return false;
+    }
+    float const   d   = fminf(sqrtf(d2), 1e6f);
+    float const   a   = fmaxf(d - sph.w, 0.001f);
+    float const   b   = d + sph.w;
+    float const   ab  = a * b;
+    float const   bma = b - a;
+    return bma > 0.f && var.z * bma * bma + 3.f * var.x * ab >= s.split_scale * (ab * ab * ab);
+}
+
+// One light of a selection: its tree-order index (or Env_pick) and the probability with which
+// the selection contains it.
+struct Light_pick {
+    uint32_t light;
+    float    pdf;
+};
+
+// Chooses a leaf light in proportion to the importances of the leaf's lights.
+__device__ __forceinline__ Light_pick pick_in_leaf(Scene_gpu const& s, uint32_t first, uint32_t count,
+                                                   V3 p, V3 n, bool total_sphere, float r) {
+    float w[Light_leaf_size];
+    float sum = 0.f;
+    for (uint32_t k = 0; k < Light_leaf_size; ++k) {
+        w[k] = k < count ? emitter_importance(s, first + k, p, n, total_sphere) : 0.f;
+        sum += w[k];
+    }
+    float    acc    = 0.f;
+    uint32_t chosen = count - 1;
+    for (uint32_t k = 0; k + 1 < count; ++k) {
+        acc += w[k];
+        if (r * sum < acc) {
+            chosen = k;
+            break;
+        }
+    }
+    return {first + chosen, w[chosen] / sum};
+}
+
+// Light selection at p (normal n; total_sphere for medium vertices) with the random number r:
+// Tree::random_light (light_tree.cpp:363-461).  Without splitting one light: the environment
+// with probability env.w, else an emitter found by walking the tree, each step choosing a child
+// in proportion to its importance.  With splitting (the first vertices of Adaptive light
+// sampling): the environment with probability 1, and the tree walked from depth
+// split_depth_bias, descending into both children of every node that split_node passes while
+// above Max_split_depth (a leaf so reached gives all its lights); below the first node that does
+// not split, the walk chooses as before, with the random number it carried.  Fills out (at most
+// Max_light_picks entries, the host having bounded the tree's picks so) and returns the count.
+__device__ uint32_t select_lights(Scene_gpu const& s, V3 p, V3 n, bool total_sphere, float r, bool split,
+                                  Light_pick* out) {
+    uint32_t m     = 0;
+    float    ip    = 0.f;
+    uint32_t depth = Max_split_depth;
+    if (split) {
+        depth = s.split_depth_bias;
+        if (s.env.w > 0.f) {
+            out[m++] = {Env_pick, 1.f};
+        }
+    } else {
+        ip = s.env.w;
+        if (r < ip) {
+            out[m++] = {Env_pick, ip};
+            return m;
+        }
+    }
+    if (s.num_lights == 0) {
+        return m;
+    }
+    struct Walk {
+        uint32_t node;
+        uint32_t depth;
+        float    pdf;
+        float    r;
+    };
+    Walk     stack[Max_split_depth + 1];
+    uint32_t top = 0;
+    Walk     t{0u, depth, 1.f - ip, fminf((r - ip) / (1.f - ip), 0x1.fffffep-1f)};
+    for (int step = 0; step < 4096; ++step) {
+        float4 const   meta     = s.light_nodes[Light_node_stride * t.node + 2];
+        uint32_t const first    = __float_as_uint(meta.y);
+        uint32_t const count    = __float_as_uint(meta.z);
+        bool const     do_split = t.depth < Max_split_depth && split_node(s, t.node, p);
+        if (count == 0) {
+            if (do_split) {
+                if (top < Max_split_depth + 1) {
+                    stack[top++] = {first + 1, t.depth + 1, t.pdf, t.r};
+                }
+                t.node = first;
+                ++t.depth;
+            } else {
+                float const w0 = node_importance(s, first, p, n, total_sphere);
+                float const w1 = node_importance(s, first + 1, p, n, total_sphere);
+                float const p0 = w0 / (w0 + w1);
+                if (t.r < p0) {
+                    t.node = first;
+                    t.pdf *= p0;
+                    t.r = fminf(t.r / p0, 0x1.fffffep-1f);
+                } else {
+                    t.node = first + 1;
+                    t.pdf *= 1.f - p0;
+                    t.r = fminf((t.r - p0) / (1.f - p0), 0x1.fffffep-1f);
+                }
+                t.depth = Max_split_depth;
+            }
+            continue;
+        }
+        if (do_split) {
+            for (uint32_t k = 0; k < count && m < Max_light_picks; ++k) {
+                out[m++] = {first + k, t.pdf};
+            }
+        } else if (m < Max_light_picks) {
+            Light_pick const pk = pick_in_leaf(s, first, count, p, n, total_sphere, t.r);
+            out[m++]            = {pk.light, pk.pdf * t.pdf};
+        }
+        if (top == 0) {
+            break;
+        }
+        t = stack[--top];
+    }
+    return m;
+}
+
+// Probability that select_lights from (p, n) includes the light at tree position order
+// (Tree::pdf, light_tree.cpp:564-640): 1 through every split, the children's importances
+// below.
+__device__ float light_pick_pdf(Scene_gpu const& s, V3 p, V3 n, bool total_sphere, uint32_t order,
+                                bool split) {
+    float    pdf   = split ? 1.f : 1.f - s.env.w;
+    uint32_t node  = 0;
+    uint32_t depth = split ? s.split_depth_bias : Max_split_depth;
+    for (int level = 0; level < 64; ++level, ++depth) {
+        float4 const   meta     = s.light_nodes[Light_node_stride * node + 2];
+        uint32_t const first    = __float_as_uint(meta.y);
+        uint32_t const count    = __float_as_uint(meta.z);
+        bool const     do_split = depth < Max_split_depth && split_node(s, node, p);
         if (count != 0) {
-            float sum = 0.f;
+            if (do_split) {
+                return pdf;
+            }
+            float sum  = 0.f;
             float mine = 0.f;
             for (uint32_t k = 0; k < count && k < Light_leaf_size; ++k) {
                 uint32_t const l = first + k;
-                float const    w = light_importance(s.light_cones[3 * l], s.light_cones[3 * l + 1],
-                                                    s.light_cones[3 * l + 2].x, p, n, total_sphere);
+                float const    w = emitter_importance(s, l, p, n, total_sphere);
                 sum += w;
                 mine = l == order ? w : mine;
             }
             return pdf * (mine / sum);
         }
-        uint32_t const c0 = first;
-        float const    w0 = light_importance(s.light_nodes[3 * c0], s.light_nodes[3 * c0 + 1],
-                                             s.light_nodes[3 * c0 + 2].x, p, n, total_sphere);
-        float const    w1 = light_importance(s.light_nodes[3 * c0 + 3], s.light_nodes[3 * c0 + 4],
-                                             s.light_nodes[3 * c0 + 5].x, p, n, total_sphere);
-        float const    p0 = w0 / (w0 + w1);
-        if (order < __float_as_uint(meta.w)) {
-            node = c0;
-            pdf *= p0;
-        } else {
-            node = c0 + 1;
-            pdf *= 1.f - p0;
+        bool const left = order < __float_as_uint(meta.w);
+        if (!do_split) {
+            float const w0 = node_importance(s, first, p, n, total_sphere);
+            float const w1 = node_importance(s, first + 1, p, n, total_sphere);
+            float const p0 = w0 / (w0 + w1);
+            pdf *= left ? p0 : 1.f - p0;
+            depth = Max_split_depth;
         }
+        node = left ? first : first + 1;
     }
     return 0.f;
 }
 
 // Light sample for next-event estimation seen from ps (normal n; total_sphere for medium
-// vertices): a light picked by the tree, a uniform point on it, the solid-angle pdf times the
-// pick probability.  False if the sample is unusable (grazing or behind a one-sided emitter,
-// Mesh::sample in triangle_mesh.cpp:462-516).
+// vertices) from a selected light: a uniform point on it (or a uniform direction for the
+// environment), the solid-angle pdf times the selection probability.  False if the sample is
+// unusable (grazing or behind a one-sided emitter, Mesh::sample in triangle_mesh.cpp:462-516).
 struct Light_sample {
     V3    dir;
     float dist;
@@ -744,29 +873,17 @@ struct Light_sample {
     V3    radiance;
 };
 
-// Light selection is split at the first Split_bounces vertices, as with the reference's
-// Adaptive light sampling (Pathtracer_MIS::splitting, pathtracer_mis.cpp:419-422;
-// Tree::random_light / pdf, light_tree.cpp:363-470, 564-640): there every infinite light is
-// sampled with probability 1 besides one emitter picked by the tree (so a vertex may send two
-// shadow rays).  The reference decides this from the depth at the vertex for next-event
+// Light selection splits at the first Split_bounces vertices with the reference's Adaptive
+// light sampling (Pathtracer_MIS::splitting, pathtracer_mis.cpp:419-422): the environment is
+// sampled with probability 1 there, beside the emitters the split tree walk selects, each with
+// a shadow ray.  The reference decides this from the depth at the vertex for next-event
 // estimation but from the depth after the bounce when it weighs the light hit (connect_light
-// runs after ++ray.depth), and this renderer does the same so that images agree.  The
-// reference's splitting of the emitter tree itself (several emitters per vertex) is not
-// mirrored: one emitter is picked.
+// runs after ++ray.depth), and this renderer does the same so that images agree.
 constexpr uint32_t Split_bounces = 3;  // Pathtracer_MIS::Num_dedicated_samplers
 
-// Which lights a sample may come from.
-enum Light_mode : int {
-    Any_light   = 0,  // the environment with probability env.w, else an emitter from the tree
-    Environment = 1,  // the environment, probability 1
-    Emitters    = 2,  // an emitter from the tree, probability 1 for the tree
-};
-
 __device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, V3 n, bool total_sphere,
-                                             float r, float r1, float r2, Light_sample& ls,
-                                             int mode = Any_light) {
-    float const env_p = mode == Any_light ? s.env.w : (mode == Environment ? 1.f : 0.f);
-    if (r < env_p) {
+                                             Light_pick pk, float r1, float r2, Light_sample& ls) {
+    if (pk.light == Env_pick) {
         // The environment: uniform directions over the hemisphere of n, or over the sphere at a
         // medium vertex (Infinite_sphere::sample, infinite_sphere.cpp:68-101).
         float const z   = total_sphere ? 1.f - 2.f * r1 : r1;
@@ -776,27 +893,21 @@ __device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, V3 n, bo
         shading::Frame const f = shading::make_frame(n);
         ls.dir      = (rad * cp) * f.t + (rad * sp) * f.b + z * f.n;
         ls.dist     = Ray_max_t;
-        ls.pdf      = env_p * (total_sphere ? 1.f / (4.f * shading::Pi) : 1.f / (2.f * shading::Pi));
+        ls.pdf      = pk.pdf * (total_sphere ? 1.f / (4.f * shading::Pi) : 1.f / (2.f * shading::Pi));
         ls.radiance = v3(s.env.x, s.env.y, s.env.z);
         return true;
     }
-    if (s.num_lights == 0) {
+    if (!(pk.pdf > 0.f)) {
         return false;
     }
-    r = fminf((r - env_p) / (1.f - env_p), 0x1.fffffep-1f);
-    float          pick;
-    uint32_t const l = pick_light(s, ps, n, total_sphere, r, pick);
-    pick *= 1.f - env_p;
-    if (!(pick > 0.f)) {
-        return false;
-    }
-    float4 const   la   = s.light_tris[3 * l + 0];
-    float4 const   le1  = s.light_tris[3 * l + 1];
-    float4 const   le2  = s.light_tris[3 * l + 2];
+    uint32_t const l       = pk.light;
+    float4 const   la      = s.light_tris[3 * l + 0];
+    float4 const   le1     = s.light_tris[3 * l + 1];
+    float4 const   le2     = s.light_tris[3 * l + 2];
     uint32_t const lmat_id = __float_as_uint(le2.w);  // the emitter's material
-    float const    sq   = sqrtf(r1);
-    V3 const       q    = f3v(la) + (sq * (1.f - r2)) * f3v(le1) + (sq * r2) * f3v(le2);
-    V3             ln   = shading::normalize(shading::cross(f3v(le1), f3v(le2)));
+    float const    sq      = sqrtf(r1);
+    V3 const       q       = f3v(la) + (sq * (1.f - r2)) * f3v(le1) + (sq * r2) * f3v(le2);
+    V3             ln      = shading::normalize(shading::cross(f3v(le1), f3v(le2)));
     shading::Material const lmat = s.materials[lmat_id];
     if (lmat.two_sided && shading::dot(ln, q - ps) > 0.f) {
         ln = -ln;
@@ -811,7 +922,7 @@ __device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, V3 n, bo
     }
     ls.dir      = dir;
     ls.dist     = d;
-    ls.pdf      = pick * d2 / (cl * la.w);
+    ls.pdf      = pk.pdf * d2 / (cl * la.w);
     ls.radiance = lmat.emission;
     return true;
 }
@@ -1247,39 +1358,121 @@ __device__ bool transmit_grid(Medium_gpu const& g, shading::Material const& m, f
 
 // Light samples at a vertex of the given depth: two (the environment, and an emitter) where
 // the selection is split and both kinds of light exist, else one (0 without lights).
-__device__ __forceinline__ int num_light_samples(Scene_gpu const& s, uint32_t depth) {
-    if (s.num_lights == 0 && !(s.env.w > 0.f)) {
-        return 0;
+// Whether light selection at a vertex of this depth splits (Pathtracer_MIS::splitting).
+__device__ __forceinline__ bool splits_at(Scene_gpu const& s, uint32_t depth) {
+    return depth < s.split_bounces;
+}
+
+__device__ __forceinline__ void store_shadow(Paths const& p, uint32_t path, V3 o, Light_sample const& ls,
+                                             V3 contrib, uint32_t depth) {
+    p.sh_o[path] = make_float4(o.x, o.y, o.z, 0.f);
+    p.sh_d[path] = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
+    p.sh_L[path] = make_float4(contrib.x, contrib.y, contrib.z, float(depth));
+}
+
+// The wave's queues and counters k_shade appends to.
+struct Shade_out {
+    uint32_t* q_out;          // extension queue of the next vertex
+    uint32_t* count_out;
+    uint32_t* sq;             // shadow queue
+    uint32_t* count_shadow;
+    uint32_t* count_picks;    // picks of split selections
+    uint32_t* count_records;  // split records
+};
+
+// Next-event estimation at a vertex (sample_lights / evaluate_light, pathtracer_mis.cpp:281-347):
+// the lights select_lights chooses with the random number `select`, a sample on each (the
+// pixel's golden ratio dimension of that light at the first vertices, else the path's random
+// stream), and each sample's contribution eval(ls).  A single light goes to the path's shadow
+// slot (returns true when it holds a ray); several get a split record and a pick each, their
+// contributions summed by k_pick_sum after the shadow rays.
+template <class Eval>
+__device__ __forceinline__ bool next_event(Scene_gpu const& s, Paths const& p, Wave const& wave,
+                                           Shade_out const& out, uint32_t path, V3 ps, V3 n,
+                                           bool total_sphere, uint32_t depth, float select, Rng& rng,
+                                           bool golden, uint32_t gpixel, uint32_t gsample, Eval const& eval) {
+    Light_pick     picks[Max_light_picks];
+    uint32_t const m     = select_lights(s, ps, n, total_sphere, select, splits_at(s, depth), picks);
+    auto const     point = [&](uint32_t l, float& r1, float& r2) {
+        if (golden) {
+            float2 const g = golden_2d(wave, gpixel, gsample, golden_light_2d(depth, l));
+            r1             = g.x;
+            r2             = g.y;
+        } else {
+            r1 = rng.uniform();
+            r2 = rng.uniform();
+        }
+    };
+    if (m == 0) {
+        return false;
     }
-    return depth < Split_bounces && s.env.w > 0.f && s.num_lights > 0 ? 2 : 1;
-}
-
-__device__ __forceinline__ int light_mode(int samples, int k) {
-    return samples == 1 ? Any_light : (k == 0 ? Environment : Emitters);
-}
-
-// Probability factor of the environment (or, with emitter = true, of the emitter tree) in the
-// light selection of the vertex whose continuation ray arrives with depth `depth`.
-__device__ __forceinline__ float selection_share(Scene_gpu const& s, uint32_t depth, bool emitter) {
-    if (depth < Split_bounces) {
-        return 1.f;
+    if (m == 1) {
+        float r1, r2;
+        point(0, r1, r2);
+        Light_sample ls;
+        if (sample_light(s, ps, n, total_sphere, picks[0], r1, r2, ls)) {
+            V3 const c = eval(ls);
+            if (shading::max_component(c) > 0.f) {
+                store_shadow(p, path, ps, ls, c, depth);
+                return true;
+            }
+        }
+        return false;
     }
-    return emitter ? 1.f - s.env.w : s.env.w;
+    uint32_t const base = atomicAdd(out.count_picks, m);
+    uint32_t const rec  = atomicAdd(out.count_records, 1u);
+    p.split_o[rec]      = make_float4(ps.x, ps.y, ps.z, __uint_as_float(path));
+    p.split_m[rec]      = make_uint4(base, m, depth, 0u);
+    uint64_t valid      = 0;
+    for (uint32_t l = 0; l < m; ++l) {
+        float r1, r2;
+        point(l, r1, r2);
+        Light_sample ls;
+        V3           c = v3(0.f, 0.f, 0.f);
+        float4       d = make_float4(0.f, 0.f, 1.f, 0.f);
+        if (sample_light(s, ps, n, total_sphere, picks[l], r1, r2, ls)) {
+            V3 const e = eval(ls);
+            if (shading::max_component(e) > 0.f) {
+                c = e;
+                d = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
+                valid |= 1ull << l;
+            }
+        }
+        p.pick_d[base + l] = d;
+        p.pick_c[base + l] = make_float4(c.x, c.y, c.z, __uint_as_float(rec));
+    }
+    if (valid != 0) {
+        uint32_t q = atomicAdd(out.count_shadow, uint32_t(__popcll(valid)));
+        for (uint32_t l = 0; l < m; ++l) {
+            if ((valid >> l) & 1u) {
+                out.sq[q++] = Pick_shadow | (base + l);
+            }
+        }
+    }
+    return false;
 }
 
-__device__ __forceinline__ void store_shadow(Paths const& p, uint32_t path, bool second, V3 o,
-                                             Light_sample const& ls, V3 contrib, uint32_t depth) {
-    float4 const ro = make_float4(o.x, o.y, o.z, 0.f);
-    float4 const rd = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
-    float4 const c  = make_float4(contrib.x, contrib.y, contrib.z, float(depth));
-    if (second) {
-        p.sh2_o[path] = ro;
-        p.sh2_d[path] = rd;
-        p.sh2_L[path] = c;
-    } else {
-        p.sh_o[path] = ro;
-        p.sh_d[path] = rd;
-        p.sh_L[path] = c;
+// Sums each split record's picks (in pick order) into its path's L2, after the bounce's shadow
+// rays have zeroed the occluded ones.
+__global__ void __launch_bounds__(256)
+    k_pick_sum(Paths p, uint32_t const* __restrict__ count) {
+    uint32_t const num = *count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < num; i += gridDim.x * blockDim.x) {
+        float4 const o = p.split_o[i];
+        uint4 const  m = p.split_m[i];
+        float        x = 0.f, y = 0.f, z = 0.f;
+        for (uint32_t l = 0; l < m.y; ++l) {
+            float4 const c = p.pick_c[m.x + l];
+            x += c.x;
+            y += c.y;
+            z += c.z;
+        }
+        uint32_t const path = __float_as_uint(o.w);
+        float4         l2   = p.L2[path];
+        l2.x += x;
+        l2.y += y;
+        l2.z += z;
+        p.L2[path] = l2;
     }
 }
 
@@ -1563,15 +1756,13 @@ __device__ __forceinline__ float continuation_probability(Wave const& wave, V3 T
 // ---- shade: one path vertex ----
 __global__ void __launch_bounds__(Shade_block)
     k_shade(Scene_gpu s, Launch const* __restrict__ launch, Paths p, uint32_t const* __restrict__ q_in,
-            uint32_t const* __restrict__ count_in, uint32_t* q_out, uint32_t* count_out,
-            uint32_t* sq, uint32_t* count_shadow) {
+            uint32_t const* __restrict__ count_in, Shade_out out) {
     Wave const&    wave = launch->wave;
     uint32_t const i   = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t const num = *count_in;
 
     bool     extend  = false;
-    bool     shadow  = false;
-    bool     shadow2 = false;  // the vertex's second light sample (split selection)
+    bool     shadow  = false;  // the path's shadow slot holds a ray
     uint32_t path    = 0;
 
     if (i < num) {
@@ -1617,7 +1808,7 @@ __global__ void __launch_bounds__(Shade_block)
                 float w = 1.f;
                 if (vtx > 0 && !singular) {
                     float4 const pn    = p.prev_n[path];
-                    float const  pdf_e = selection_share(s, depth, false) *
+                    float const  pdf_e = (splits_at(s, depth) ? 1.f : s.env.w) *
                                          (pn.w != 0.f ? 1.f / (4.f * shading::Pi)
                                                       : 1.f / (2.f * shading::Pi));
                     w = power_heuristic(bsdf_pdf, pdf_e);
@@ -1669,23 +1860,13 @@ __global__ void __launch_bounds__(Shade_block)
                 float const g   = shading::van_de_hulst_anisotropy(m.g, depth);
                 V3 const    pos = v3(ro.x + t_sc * rd.x, ro.y + t_sc * rd.y, ro.z + t_sc * rd.z);
                 V3 const    wo  = -dir_in;
-                int const samples = num_light_samples(s, depth);
-                for (int k = 0; k < samples; ++k) {
-                    float const  r  = rng.uniform();
-                    float const  r1 = rng.uniform();
-                    float const  r2 = rng.uniform();
-                    Light_sample ls;
-                    if (sample_light(s, pos, v3(0.f, 0.f, 1.f), true, r, r1, r2, ls,
-                                     light_mode(samples, k))) {
-                        float const f = shading::phase_hg(shading::dot(wo, ls.dir), g);
-                        float const w = ls.pdf / (ls.pdf * ls.pdf + f * f);
-                        V3 const contrib = (w * f) * (T * ls.radiance);
-                        if (shading::max_component(contrib) > 0.f) {
-                            store_shadow(p, path, k == 1, pos, ls, contrib, depth);
-                            (k == 1 ? shadow2 : shadow) = true;
-                        }
-                    }
-                }
+                float const select = rng.uniform();
+                shadow = next_event(s, p, wave, out, path, pos, v3(0.f, 0.f, 1.f), true, depth, select, rng,
+                                    false, 0u, 0u, [&](Light_sample const& ls) {
+                                        float const f = shading::phase_hg(shading::dot(wo, ls.dir), g);
+                                        float const w = ls.pdf / (ls.pdf * ls.pdf + f * f);
+                                        return (w * f) * (T * ls.radiance);
+                                    });
                 float const x0 = rng.uniform();
                 float const x1 = rng.uniform();
                 float       pdf;
@@ -1739,8 +1920,8 @@ __global__ void __launch_bounds__(Shade_block)
                             // the light-tree pick from the previous vertex (connect_light,
                             // pathtracer_mis.cpp:349-380)
                             float4 const pn    = p.prev_n[path];
-                            float const  pick  = selection_share(s, depth, true) *
-                                                light_pick_pdf(s, f3v(ro), f3v(pn), pn.w != 0.f, order);
+                            float const  pick  = light_pick_pdf(s, f3v(ro), f3v(pn), pn.w != 0.f, order,
+                                                                splits_at(s, depth));
                             float const  t     = p.hit_t[path];
                             float const  area  = s.light_tris[3 * order].w;
                             float const  pdf_l = pick * (t * t) / (fabsf(cos_o) * area);
@@ -1803,34 +1984,18 @@ __global__ void __launch_bounds__(Shade_block)
                 uint32_t const gsample = wave.first_sample + path / pixels;
 
                 // Next-event estimation (sample_lights / evaluate_light, pathtracer_mis.cpp:281-347).
-                int const samples = num_light_samples(s, depth);
-                V3 const  ps      = offset_ray(pos, geo_n);
-                for (int k = 0; k < samples; ++k) {
-                    float r, r1, r2;
-                    if (golden) {
-                        r               = golden_1d(wave, gpixel, gsample, golden_light_1d(depth, k));
-                        float2 const g2 = golden_2d(wave, gpixel, gsample, golden_light_2d(depth, k));
-                        r1              = g2.x;
-                        r2              = g2.y;
-                    } else {
-                        r  = rng.uniform();
-                        r1 = rng.uniform();
-                        r2 = rng.uniform();
-                    }
-                    Light_sample ls;
-                    if (sample_light(s, ps, geo_n, false, r, r1, r2, ls, light_mode(samples, k))) {
-                        shading::Bxdf const f =
-                            shading::substitute_evaluate(mat, s.e_table, ctx, ls.dir);
-                        float const pc = guided ? gf * mixture_pdf_at(mix, ls.dir) + (1.f - gf) * f.pdf
-                                                : f.pdf;
-                        float const w  = ls.pdf / (ls.pdf * ls.pdf + pc * pc);
-                        V3 const contrib = w * (T * (ls.radiance * f.reflection));
-                        if (shading::max_component(contrib) > 0.f) {
-                            store_shadow(p, path, k == 1, ps, ls, contrib, depth);
-                            (k == 1 ? shadow2 : shadow) = true;
-                        }
-                    }
-                }
+                V3 const    ps     = offset_ray(pos, geo_n);
+                float const select = golden ? golden_1d(wave, gpixel, gsample, golden_light_1d(depth, 0))
+                                            : rng.uniform();
+                shadow = next_event(s, p, wave, out, path, ps, geo_n, false, depth, select, rng, golden, gpixel,
+                                    gsample, [&](Light_sample const& ls) {
+                                        shading::Bxdf const f =
+                                            shading::substitute_evaluate(mat, s.e_table, ctx, ls.dir);
+                                        float const pc = guided ? gf * mixture_pdf_at(mix, ls.dir) + (1.f - gf) * f.pdf
+                                                                : f.pdf;
+                                        float const w  = ls.pdf / (ls.pdf * ls.pdf + pc * pc);
+                                        return w * (T * (ls.radiance * f.reflection));
+                                    });
 
                 // Continuation direction: the BSDF sample (pathtracer_mis.cpp:153-201), or with
                 // probability gf the guide's.  A guide direction gets the BSDF value and pdf the
@@ -1906,17 +2071,13 @@ __global__ void __launch_bounds__(Shade_block)
         p.info[path] = pack_info(vtx, depth, singular, medium);
     }
 
-    uint32_t const slot = append(count_out, extend);
+    uint32_t const slot = append(out.count_out, extend);
     if (extend) {
-        q_out[slot] = path;
+        out.q_out[slot] = path;
     }
-    uint32_t const sslot = append(count_shadow, shadow);
+    uint32_t const sslot = append(out.count_shadow, shadow);
     if (shadow) {
-        sq[sslot] = path;
-    }
-    uint32_t const sslot2 = append(count_shadow, shadow2);
-    if (shadow2) {
-        sq[sslot2] = path | Second_shadow;
+        out.sq[sslot] = path;
     }
 }
 
@@ -1929,79 +2090,98 @@ template <bool Instances = false>
 __global__ void __launch_bounds__(Trace_block)
     k_transmit(Scene_gpu s, Paths p, uint32_t const* __restrict__ queue,
                uint32_t const* __restrict__ count, uint32_t* overflow) {
-    uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= *count) {
-        return;
-    }
-    uint32_t const entry  = queue[i];
-    uint32_t const path   = entry & ~Second_shadow;
-    bool const     second = entry & Second_shadow;
-    uint32_t       medium = p.info[path] >> 17;
-    float4 const   ro     = second ? p.sh2_o[path] : p.sh_o[path];
-    float4 const   rd     = second ? p.sh2_d[path] : p.sh_d[path];
-    float4 const   c      = second ? p.sh2_L[path] : p.sh_L[path];
-    uint32_t const depth  = uint32_t(c.w);
-    float          t0     = ro.w;
-    V3             tau    = v3(0.f, 0.f, 0.f);
-    V3             w      = v3(1.f, 1.f, 1.f);
-    bool           random = false;  // this shadow ray's random stream was started
-    bool           blocked = false;
-    Rng            rng;
-    uint2          stack[gpu::Stack_size];
-    for (int crossing = 0; crossing < 64; ++crossing) {
-        gpu::Ray_state      r;
-        gpu::Traversal      tv;
-        gpu::Instance_state is;
-        gpu::start_ray(r, tv, make_float4(ro.x, ro.y, ro.z, t0), rd);
-        if constexpr (Instances) {
-            gpu::start_instances(r, is);
+    uint32_t const num = *count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < num; i += gridDim.x * blockDim.x) {
+        uint32_t const entry = queue[i];
+        bool const     pick  = entry & Pick_shadow;
+        uint32_t const pk    = entry & ~Pick_shadow;
+        // The ray and its contribution: the path's shadow slot, or a pick of a split selection
+        // (its origin, path and depth in the vertex's record).
+        uint32_t path, depth, stream;
+        float4   ro, rd, c;
+        if (pick) {
+            c                   = p.pick_c[pk];
+            rd                  = p.pick_d[pk];
+            uint32_t const rec  = __float_as_uint(c.w);
+            float4 const   o    = p.split_o[rec];
+            uint4 const    m    = p.split_m[rec];
+            ro                  = make_float4(o.x, o.y, o.z, 0.f);
+            path                = __float_as_uint(o.w);
+            depth               = m.z;
+            stream              = 1u + (pk - m.x);
+        } else {
+            path   = entry;
+            ro     = p.sh_o[path];
+            rd     = p.sh_d[path];
+            c      = p.sh_L[path];
+            depth  = uint32_t(c.w);
+            stream = 0u;
         }
-        while (!gpu::traversal_step<false, true, Instances>(r, tv, stack, s.nodes, s.tris, s.hit_margin,
-                                                            overflow, Class_surface, &is, s.inst_trace)) {
-        }
-        bool const  hit = r.best_id != gpu::Miss;
-        float const end = hit ? r.tbest : rd.w;
-        if (medium != 0) {
-            shading::Material const m = s.materials[medium - 1];
-            if (m.medium != 0) {
-                if (!random) {
-                    // A stream of its own, seeded from the path's state (which this kernel
-                    // only reads: a vertex's two shadow rays may be in flight together).
-                    uint4 const st = p.rng[path];
-                    rng.start((uint64_t(st.y) << 32) | st.x, (uint64_t(path) << 1) | (second ? 1u : 0u));
-                    random = true;
+        uint32_t medium  = p.info[path] >> 17;
+        float    t0      = ro.w;
+        V3       tau     = v3(0.f, 0.f, 0.f);
+        V3       w       = v3(1.f, 1.f, 1.f);
+        bool     random  = false;  // this shadow ray's random stream was started
+        bool     blocked = false;
+        Rng      rng;
+        uint2    stack[gpu::Stack_size];
+        for (int crossing = 0; crossing < 64; ++crossing) {
+            gpu::Ray_state      r;
+            gpu::Traversal      tv;
+            gpu::Instance_state is;
+            gpu::start_ray(r, tv, make_float4(ro.x, ro.y, ro.z, t0), rd);
+            if constexpr (Instances) {
+                gpu::start_instances(r, is);
+            }
+            while (!gpu::traversal_step<false, true, Instances>(r, tv, stack, s.nodes, s.tris, s.hit_margin,
+                                                                overflow, Class_surface, &is, s.inst_trace)) {
+            }
+            bool const  hit = r.best_id != gpu::Miss;
+            float const end = hit ? r.tbest : rd.w;
+            if (medium != 0) {
+                shading::Material const m = s.materials[medium - 1];
+                if (m.medium != 0) {
+                    if (!random) {
+                        // A stream of its own, seeded from the path's state (which this kernel
+                        // only reads: several shadow rays of a vertex may be in flight together).
+                        uint4 const st = p.rng[path];
+                        rng.start((uint64_t(st.y) << 32) | st.x, (uint64_t(path) << 7) | stream);
+                        random = true;
+                    }
+                    float const srs = shading::similarity_relation_scale(m.g, depth);
+                    if (!transmit_grid(s.media[m.medium - 1], m, srs, f3v(ro), f3v(rd), t0, end, rng,
+                                       w, s.tracking_capped)) {
+                        blocked = true;
+                        break;
+                    }
+                } else {
+                    float const len = fmaxf(end - t0, 0.f);
+                    tau = tau + len * (m.mu_a + m.mu_s);
                 }
-                float const srs = shading::similarity_relation_scale(m.g, depth);
-                if (!transmit_grid(s.media[m.medium - 1], m, srs, f3v(ro), f3v(rd), t0, end, rng,
-                                   w, s.tracking_capped)) {
-                    blocked = true;
-                    break;
-                }
-            } else {
-                float const len = fmaxf(end - t0, 0.f);
-                tau = tau + len * (m.mu_a + m.mu_s);
+            }
+            if (!hit) {
+                break;
+            }
+            World_tri const wt  = world_triangle(s, Instances ? is.best_inst : 0u, r.best_id);
+            V3 const        geo = shading::cross(wt.b - wt.a, wt.c - wt.a);
+            medium              = shading::dot(geo, v3(rd.x, rd.y, rd.z)) < 0.f ? wt.material + 1 : 0;
+            t0                  = offset_f(r.tbest);
+            if (t0 >= rd.w) {
+                break;
             }
         }
-        if (!hit) {
-            break;
-        }
-        World_tri const wt  = world_triangle(s, Instances ? is.best_inst : 0u, r.best_id);
-        V3 const        geo = shading::cross(wt.b - wt.a, wt.c - wt.a);
-        medium              = shading::dot(geo, v3(rd.x, rd.y, rd.z)) < 0.f ? wt.material + 1 : 0;
-        t0              = offset_f(r.tbest);
-        if (t0 >= rd.w) {
-            break;
+        V3 const tr = blocked ? v3(0.f, 0.f, 0.f)
+                              : v3(w.x * expf(-tau.x), w.y * expf(-tau.y), w.z * expf(-tau.z));
+        if (pick) {
+            p.pick_c[pk] = make_float4(tr.x * c.x, tr.y * c.y, tr.z * c.z, c.w);
+        } else if (!blocked) {
+            float4 l = p.L[path];
+            l.x += tr.x * c.x;
+            l.y += tr.y * c.y;
+            l.z += tr.z * c.z;
+            p.L[path] = l;
         }
     }
-    if (blocked) {
-        return;
-    }
-    float4* const Lp = second ? p.L2 : p.L;
-    float4        l  = Lp[path];
-    l.x += w.x * expf(-tau.x) * c.x;
-    l.y += w.y * expf(-tau.y) * c.y;
-    l.z += w.z * expf(-tau.z) * c.z;
-    Lp[path] = l;
 }
 
 // ---- film: Filtered_1p0::add_sample (sensor/filtered.inl:125-187) as a gather ----
@@ -2164,6 +2344,9 @@ struct Renderer::Device {
     uint32_t             golden_n       = 0;
     std::vector<float*>  grid_density;  // one per density grid
     std::vector<float2*> grid_cells;
+    // the light tree's nodes as uploaded, and the splitting threshold their split radii are for
+    std::vector<float>   light_tree_nodes;
+    float                split_radii_threshold = -1.f;
     uint32_t           num_lights = 0;
     float4             env        = {0.f, 0.f, 0.f, 0.f};
     float              hit_margin = 0.f;
@@ -2210,6 +2393,11 @@ struct Renderer::Device {
     uint32_t* counters       = nullptr;
     uint32_t* pinned_count   = nullptr;  // host-pinned word for the queue-length check
     bool      has_media      = false;
+    // split light selection: the most lights one selection returns in this scene, the depth
+    // the split walk starts at, and the picks the buffers hold
+    uint32_t  max_picks        = 1;
+    uint32_t  split_depth_bias = 0;
+    uint64_t  pick_capacity    = 0;
     // film
     float4*   film = nullptr;
     float4*   comp = nullptr;
@@ -2401,9 +2589,10 @@ Renderer::~Renderer() {
     free_ptr(p.sh_d);
     free_ptr(p.sh_L);
     free_ptr(p.prev_n);
-    free_ptr(p.sh2_o);
-    free_ptr(p.sh2_d);
-    free_ptr(p.sh2_L);
+    free_ptr(p.split_o);
+    free_ptr(p.split_m);
+    free_ptr(p.pick_d);
+    free_ptr(p.pick_c);
     free_ptr(p.L2);
     free_ptr(p.guide_in);
     free_ptr(p.guide_out);
@@ -2526,7 +2715,10 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
         double const cz    = e1[0] * e2[1] - e1[1] * e2[0];
         double const area  = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
         li.two_sided       = m.two_sided != 0;
-        li.power = area * (double(m.emission.x) + m.emission.y + m.emission.z) / 3.0 * (li.two_sided ? 2.0 : 1.0);
+        // Light::power (light.cpp:38-48) and Scene::light_power (scene.cpp:504): area times the
+        // largest radiance component, twice that for two-sided emitters.
+        li.power = area * std::max({double(m.emission.x), double(m.emission.y), double(m.emission.z)}) *
+                   (li.two_sided ? 2.0 : 1.0);
         li.slot     = slot;
         li.material = material;
         if (area > 0.0 && li.power > 0.0) {
@@ -2821,8 +3013,8 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     }
 
     // The environment's share of light picks: its power against the emitters', with the
-    // reference's power of an infinite light, squared scene extent x 4 pi x mean radiance
-    // (Light::power, light.cpp:38-48; Tree_builder, light_tree_builder.cpp:527-537).
+    // reference's power of an infinite light, squared scene extent x 4 pi x the largest radiance
+    // component (Light::power, light.cpp:38-48; Tree_builder, light_tree_builder.cpp:527-537).
     float const* env = scene.environment;
     d_->env          = make_float4(env[0], env[1], env[2], 0.f);
     if (scene.environment_light && (env[0] > 0.f || env[1] > 0.f || env[2] > 0.f)) {
@@ -2831,12 +3023,27 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
             ext2 += (hi[k] - lo[k]) * (hi[k] - lo[k]);
         }
         double const p_env = ext2 * 4.0 * 3.14159265358979323846 *
-                             (double(env[0]) + env[1] + env[2]) / 3.0;
+                             std::max({double(env[0]), double(env[1]), double(env[2])});
         double p_finite = 0.0;
         for (Light_input const& li : emitters) {
             p_finite += li.power;
         }
         d_->env.w = float(p_env / (p_env + p_finite));
+    }
+    // Split light selection: the depth the split walk starts at, so that the environment and
+    // the most emitters one walk can return fit Max_light_picks (Tree_builder,
+    // light_tree_builder.cpp:510-522), and that most.
+    {
+        uint32_t const infinite = d_->env.w > 0.f ? 1u : 0u;
+        uint32_t       bias     = 0;
+        if (infinite != 0 && tree.num_nodes != 0) {
+            uint32_t const left = Max_light_picks - max_split_picks(tree, 0);
+            if (left < infinite) {
+                bias = std::max(uint32_t(std::ceil(std::log2(double(infinite - left)))), 1u);
+            }
+        }
+        d_->split_depth_bias = bias;
+        d_->max_picks        = (tree.num_nodes != 0 ? max_split_picks(tree, bias) : 0u) + infinite;
     }
 
     SPB_RCUDA(upload(d_->tri_info, info.data(), info.size() * sizeof(uint4)));
@@ -2875,6 +3082,8 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     SPB_RCUDA(upload(d_->materials, scene.materials.data(),
                      scene.materials.size() * sizeof(shading::Material)));
     SPB_RCUDA(upload(d_->light_nodes, tree.nodes.data(), tree.nodes.size() * sizeof(float)));
+    d_->light_tree_nodes      = tree.nodes;
+    d_->split_radii_threshold = -1.f;  // split radii set at the first render
     SPB_RCUDA(upload(d_->light_cones, tree.cones.data(), tree.cones.size() * sizeof(float)));
     SPB_RCUDA(upload(d_->light_tris, tree.tris.data(), tree.tris.size() * sizeof(float)));
     SPB_RCUDA(upload(d_->light_order, tree.order.data(), tree.order.size() * sizeof(uint32_t)));
@@ -2960,8 +3169,9 @@ int32_t Renderer::start_frame() {
     return SPB_OK;
 }
 
-int32_t Renderer::ensure_buffers(uint32_t paths) {
-    if (paths <= d_->capacity) {
+int32_t Renderer::ensure_buffers(uint32_t paths, uint32_t picks_per_path) {
+    uint64_t const picks = uint64_t(paths) * picks_per_path;
+    if (paths <= d_->capacity && picks <= d_->pick_capacity) {
         return SPB_OK;
     }
     clear_graphs();
@@ -2981,9 +3191,10 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     free_ptr(p.sh_d);
     free_ptr(p.sh_L);
     free_ptr(p.prev_n);
-    free_ptr(p.sh2_o);
-    free_ptr(p.sh2_d);
-    free_ptr(p.sh2_L);
+    free_ptr(p.split_o);
+    free_ptr(p.split_m);
+    free_ptr(p.pick_d);
+    free_ptr(p.pick_c);
     free_ptr(p.L2);
     free_ptr(p.guide_in);
     free_ptr(p.guide_out);
@@ -3011,15 +3222,19 @@ int32_t Renderer::ensure_buffers(uint32_t paths) {
     SPB_RCUDA(dev_malloc(&p.sh_d, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&p.sh_L, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&p.prev_n, n * sizeof(float4)));
-    SPB_RCUDA(dev_malloc(&p.sh2_o, n * sizeof(float4)));
-    SPB_RCUDA(dev_malloc(&p.sh2_d, n * sizeof(float4)));
-    SPB_RCUDA(dev_malloc(&p.sh2_L, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&p.L2, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&d_->queue[0], n * sizeof(uint32_t)));
     SPB_RCUDA(dev_malloc(&d_->queue[1], n * sizeof(uint32_t)));
-    // up to two shadow rays per path vertex (split light selection)
-    SPB_RCUDA(dev_malloc(&d_->shadow_queue, 2 * n * sizeof(uint32_t)));
-    SPB_RCUDA(dev_malloc(&d_->transmit_queue, 2 * n * sizeof(uint32_t)));
+    // Split selections: a record per path and every light its selection can return.  Shadow
+    // rays: a path's slot and every pick.
+    size_t const np = std::max<size_t>(size_t(n) * picks_per_path, 1);
+    SPB_RCUDA(dev_malloc(&p.split_o, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.split_m, n * sizeof(uint4)));
+    SPB_RCUDA(dev_malloc(&p.pick_d, np * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.pick_c, np * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&d_->shadow_queue, (n + np) * sizeof(uint32_t)));
+    SPB_RCUDA(dev_malloc(&d_->transmit_queue, (n + np) * sizeof(uint32_t)));
+    d_->pick_capacity = uint64_t(n) * picks_per_path;
     if (!d_->counters) {
         SPB_RCUDA(dev_malloc(&d_->counters, Counter_words * sizeof(uint32_t)));
     }
@@ -3159,6 +3374,62 @@ int32_t Renderer::train_guide(uint32_t paths) {
     return SPB_OK;
 }
 
+// Squared distance from a light-tree node's centre beyond which split_node cannot pass for
+// the splitting measure S = (1 / t - 1)^2, or 0 if it passes nowhere.  The test is g >= 0 for
+// g = (ve + ee^2) (b - a)^2 + 3 ve a b - 3 S (a b)^3 with a = max(d - r, E), b = d + r, E = 0.001.
+// Beyond d = r + E, in x = d^2 - r^2, g = 4 r^2 (ve + ee^2) + 3 ve x - 3 S x^3 is concave, so it
+// is negative beyond its largest root, found by bisection.  Below (a = E, b = d + r in
+// [r, 2 r + E]) g is a cubic in b whose maximum lies at an end or a critical point; when that
+// maximum is clearly negative the node never splits.  The radius is widened by 1 % so that the
+// float test on the device never passes beyond it.
+static float split_radius2(double r, double ve, double vee, double S) {
+    if (S <= 0.0) {
+        return INFINITY;
+    }
+    double const E  = 0.001;
+    auto const   g2 = [&](double x) { return 4.0 * r * r * vee + 3.0 * ve * x - 3.0 * S * x * x * x; };
+    double const x0 = (r + E) * (r + E) - r * r;
+    double const xs = std::max(x0, ve > 0.0 ? std::sqrt(ve / (3.0 * S)) : x0);
+    double       dmax;
+    if (g2(xs) >= 0.0) {
+        double lo = xs, hi = std::max(2.0 * xs, 1e-12);
+        while (g2(hi) >= 0.0 && hi < 1e30) {
+            lo = hi;
+            hi *= 2.0;
+        }
+        for (int i = 0; i < 100; ++i) {
+            double const mid = 0.5 * (lo + hi);
+            (g2(mid) >= 0.0 ? lo : hi) = mid;
+        }
+        dmax = std::sqrt(hi + r * r);
+    } else {
+        auto const G = [&](double b) {
+            double const eb = E * b;
+            return vee * (b - E) * (b - E) + 3.0 * ve * eb - 3.0 * S * eb * eb * eb;
+        };
+        double       gmax = std::max(G(r), G(2.0 * r + E));
+        double const A    = 9.0 * S * E * E * E, B = -2.0 * vee, C = 2.0 * vee * E - 3.0 * ve * E;
+        double const disc = B * B - 4.0 * A * C;
+        if (disc >= 0.0) {
+            for (double const sgn : {1.0, -1.0}) {
+                double const b = (-B + sgn * std::sqrt(disc)) / (2.0 * A);
+                if (b >= r && b <= 2.0 * r + E) {
+                    gmax = std::max(gmax, G(b));
+                }
+            }
+        }
+        double const b1    = 2.0 * r + E;
+        double const scale = std::max({std::fabs(vee * 4.0 * r * r), std::fabs(3.0 * ve * E * b1),
+                                       std::fabs(3.0 * S * E * E * E * b1 * b1 * b1), 1e-300});
+        if (gmax < -1e-4 * scale) {
+            return 0.f;
+        }
+        dmax = r + E;
+    }
+    double const d = 1.01 * dmax + 1e-6;
+    return float(d * d);
+}
+
 int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     if (!ready()) {
         error_ = "render needs a scene and a camera";
@@ -3177,7 +3448,15 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     // Wave size: k samples per pixel per wave, k = paths per wave / pixels (at least 1), the
     // paths per wave from the settings or the autotuner; buffers hold the largest candidate.
     bool const     tuning     = settings_.wave_paths == 0 || settings_.trace_blocks_per_sm == 0;
-    uint32_t const max_paths  = settings_.wave_paths ? settings_.wave_paths : Tuner::Max_wave_paths;
+    // Split light selection: every path of a wave may select up to max_picks lights; waves are
+    // bounded so that their picks fit Pick_budget bytes.
+    uint32_t const picks_per_path = settings_.light_split && d_->max_picks > 1 ? d_->max_picks : 0u;
+    uint32_t const pick_paths =
+        picks_per_path ? uint32_t(std::min<uint64_t>(Tuner::Max_wave_paths,
+                                                      Pick_budget / (uint64_t(picks_per_path) * 2 * sizeof(float4))))
+                       : Tuner::Max_wave_paths;
+    uint32_t const max_paths =
+        std::min(settings_.wave_paths ? settings_.wave_paths : Tuner::Max_wave_paths, pick_paths);
     auto const     wave_spp   = [&](uint32_t paths_per_wave) {
         return std::max(1u, std::min(num_samples, paths_per_wave / std::max(1u, pixels)));
     };
@@ -3195,7 +3474,18 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         SPB_RCUDA(upload(d_->golden_sorted, sorted.data(), sorted.size() * sizeof(uint32_t)));
         d_->golden_n = golden_n;
     }
-    if (int32_t const st = ensure_buffers(max_wave * pixels)) {
+    if (settings_.light_split && d_->split_radii_threshold != settings_.split_threshold &&
+        !d_->light_tree_nodes.empty()) {
+        double const t = settings_.split_threshold;
+        double const S = t >= 1.0 ? 0.0 : (1.0 / t - 1.0) * (1.0 / t - 1.0);
+        std::vector<float>& nodes = d_->light_tree_nodes;
+        for (size_t n = 0; n + Light_node_floats <= nodes.size(); n += Light_node_floats) {
+            nodes[n + 15] = split_radius2(nodes[n + 3], nodes[n + 12], nodes[n + 14], S);
+        }
+        SPB_RCUDA(cudaMemcpy(d_->light_nodes, nodes.data(), nodes.size() * sizeof(float), cudaMemcpyHostToDevice));
+        d_->split_radii_threshold = settings_.split_threshold;
+    }
+    if (int32_t const st = ensure_buffers(max_wave * pixels, picks_per_path)) {
         return st;
     }
     if (settings_.guiding) {
@@ -3238,6 +3528,13 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     sg.inst_materials = d_->inst_materials;
     sg.instanced      = d_->instanced ? 1u : 0u;
     sg.tracking_capped = d_->counters + Overflow_slot + 2;
+    sg.split_bounces    = settings_.light_split ? Split_bounces : 0u;
+    sg.split_depth_bias = d_->split_depth_bias;
+    {
+        // t >= 1 splits every node the walk passes above Max_split_depth
+        double const t = settings_.split_threshold;
+        sg.split_scale = t >= 1.0 ? 0.f : float(3.0 * (1.0 / t - 1.0) * (1.0 / t - 1.0));
+    }
     sg.uvs             = d_->uvs;
     sg.textures        = d_->textures;
 
@@ -3281,6 +3578,9 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     auto const enqueue_wave = [&](uint32_t k, uint32_t paths, uint32_t trace_grid, bool training, bool capture,
                                   uint32_t& iterations, size_t& events) -> int32_t {
         SPB_RCUDA(cudaMemsetAsync(ctr, 0, Counter_words * sizeof(uint32_t), st));
+        // k_transmit loops over its queue: at most a slot and every pick per path
+        uint32_t const transmit_grid = uint32_t(std::min<uint64_t>(
+            (uint64_t(paths) * (1 + picks_per_path) + Trace_block - 1) / Trace_block, uint64_t(32) * d_->sms));
         k_generate<<<(paths + 255) / 256, 256, 0, st>>>(d_->launch_dev, d_->paths, d_->queue[0], ctr, paths);
         iterations = 0;
         for (uint32_t b = 0; b < max_iterations; ++b) {
@@ -3311,16 +3611,17 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
                 SPB_RCUDA(record(guide_event(events++), capture));
             }
             k_shade<<<(paths + Shade_block - 1) / Shade_block, Shade_block, 0, st>>>(
-                sg, d_->launch_dev, d_->paths, q_in, c, q_out, c + Counter_stride, d_->shadow_queue, c + 1);
+                sg, d_->launch_dev, d_->paths, q_in, c,
+                Shade_out{q_out, c + Counter_stride, d_->shadow_queue, c + 1, c + 5, c + 6});
             if (d_->has_media && d_->instanced) {
                 k_trace<true, true, true><<<trace_grid, Trace_block, 0, st>>>(
                     sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot, d_->transmit_queue, c + 4);
-                k_transmit<true><<<(2 * paths + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
+                k_transmit<true><<<transmit_grid, Trace_block, 0, st>>>(
                     sg, d_->paths, d_->transmit_queue, c + 4, ctr + Overflow_slot);
             } else if (d_->has_media) {
                 k_trace<true, true><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->shadow_queue, c + 1, c + 3,
                                                                        ctr + Overflow_slot, d_->transmit_queue, c + 4);
-                k_transmit<false><<<(2 * paths + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
+                k_transmit<false><<<transmit_grid, Trace_block, 0, st>>>(
                     sg, d_->paths, d_->transmit_queue, c + 4, ctr + Overflow_slot);
             } else if (d_->instanced) {
                 k_trace<true, false, true><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->shadow_queue, c + 1,
@@ -3328,6 +3629,9 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             } else {
                 k_trace<true><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->shadow_queue, c + 1, c + 3,
                                                                   ctr + Overflow_slot);
+            }
+            if (picks_per_path != 0) {
+                k_pick_sum<<<std::min((paths + 255) / 256, 8 * d_->sms), 256, 0, st>>>(d_->paths, c + 6);
             }
         }
         if (training) {
@@ -3353,8 +3657,9 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         // this wave's configuration: tuned, the tuner's current candidate, or the settings
         Tuner const&   tn          = d_->tuner;
         bool const     probe       = tuning && !training && !tn.done();
-        uint32_t const wave_paths  = settings_.wave_paths ? settings_.wave_paths
-                                                          : (tn.done() ? tn.best_wave : tn.wave_paths);
+        uint32_t const wave_paths  = std::min(settings_.wave_paths ? settings_.wave_paths
+                                                                   : (tn.done() ? tn.best_wave : tn.wave_paths),
+                                              max_paths);
         uint32_t const blocks_sm   = settings_.trace_blocks_per_sm
                                          ? std::min(settings_.trace_blocks_per_sm, tn.max_per_sm)
                                          : (tn.done() ? tn.best_sm : (training ? tn.max_per_sm : tn.per_sm));

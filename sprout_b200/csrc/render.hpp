@@ -89,6 +89,12 @@ struct Settings {
     uint32_t min_bounces = 4;   // Russian roulette starts here
     uint32_t max_bounces = 8;
     uint32_t seed        = 0;
+    // Light selection (the PTMIS "light_sampling" object): Adaptive splits the selection at the
+    // first three vertices (the environment with probability 1, and every light-tree node
+    // whose split test passes descended on both sides), Single picks one light everywhere;
+    // split_threshold is the reference's splitting_threshold to the fourth power.
+    bool     light_split     = true;
+    float    split_threshold = 4.096e-5f;
     // Golden ratio sequences for the camera and the first three vertices of a frame rendered in
     // one call (the reference's batch mode); false: independent random samples (progressive).
     bool     golden_ratio = false;
@@ -171,7 +177,7 @@ class Renderer {
     bool        camera_ready_ = false;
     std::string error_;
 
-    int32_t ensure_buffers(uint32_t paths);
+    int32_t ensure_buffers(uint32_t paths, uint32_t picks_per_path);
     int32_t ensure_guide(uint32_t paths);
     int32_t train_guide(uint32_t paths);
     void    clear_graphs();

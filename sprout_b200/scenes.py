@@ -422,19 +422,20 @@ def _trafo(scale, rows, position):
 
 def builtin_shapes(su, width: int = 64, height: int = 48, spp: int = 64, environment=(0.4, 0.5, 0.7),
                    environment_light: bool = True, max_bounces: int = 8, min_bounces: int = 4,
-                   lamp: bool = True):
+                   lamp: bool = True, integrator=None):
     """Built-in analytic shapes created by id (su_create_prop with SU_SHAPE_*): a Disk of
     radius 3 as the ground, a metal Sphere, a rotated Cube, a Rectangle light of 0.6 x 0.6
     facing down (radiance 20), and an Infinite_sphere of uniform radiance `environment` (a
     light unless environment_light is False, then only seen by the camera).  lamp=False leaves
-    the Rectangle light out."""
+    the Rectangle light out.  integrator: further PTMIS keys."""
     cam = su.su_create_camera_perspective(width, height, math.radians(45.0))
     m = np.eye(4, dtype=np.float32)
     m[1, 1], m[1, 2], m[2, 1], m[2, 2] = math.cos(0.25), math.sin(0.25), -math.sin(0.25), math.cos(0.25)
     m[3, :3] = (0.0, 1.5, -4.0)
     su.set_transformation(cam, m)
-    su.su_create_integrators(json.dumps({"surface": {"PTMIS": {"min_bounces": min_bounces,
-                                                              "max_bounces": max_bounces}}}).encode())
+    ptmis = {"min_bounces": min_bounces, "max_bounces": max_bounces}
+    ptmis.update(integrator or {})
+    su.su_create_integrators(json.dumps({"surface": {"PTMIS": ptmis}}).encode())
     su.su_create_sampler(spp)
     su.su_create_defaults()
     ground = _material(su, "Substitute", color=[0.7, 0.7, 0.7], roughness=0.8, metallic=0.0)

@@ -4,10 +4,13 @@
 //   - every light appears exactly once in tree order, and order[] inverts the mapping;
 //   - inner nodes' children are adjacent, leaves hold 1..4 lights, the lights of a subtree are
 //     a contiguous range split at `middle`;
-//   - node power is the sum of its lights' powers;
+//   - node power is the sum of its lights' powers, node variance their population variance
+//     (and variance + mean^2) and node light count their number;
+//   - a splitting walk returns at most Max_light_picks lights (max_split_picks);
 //   - a node's bounding sphere contains its lights' triangles and its cone contains their
 //     normals (cos spread -1 when a two-sided light is below).
-// Prints "ok <nodes> <depth>" per tree or the first violation, and exits non-zero on failure.
+// Prints "ok <name> <nodes> <depth> <most picks>" per tree or the first violation, and exits
+// non-zero on failure.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -41,7 +44,7 @@ struct Checker {
         ok = false;
     }
 
-    float const* node(uint32_t n) const { return &t.nodes[12 * size_t(n)]; }
+    float const* node(uint32_t n) const { return &t.nodes[spb::render::Light_node_floats * size_t(n)]; }
 
     // light (tree order) -> input (its stored material is 2 * slot + 5)
     Light_input const& light(uint32_t o) const {
@@ -50,6 +53,10 @@ struct Checker {
 
     // returns the [begin, end) range of lights of the subtree, checks contents
     void walk(uint32_t n, uint32_t& begin, uint32_t& end, double& power, int depth) {
+        double power2 = 0.0;
+        walk(n, begin, end, power, power2, depth);
+    }
+    void walk(uint32_t n, uint32_t& begin, uint32_t& end, double& power, double& power2, int depth) {
         if (depth > 64) {
             fail("depth", n);
             return;
@@ -62,12 +69,15 @@ struct Checker {
                 fail("leaf range", n);
                 return;
             }
-            begin = first;
-            end   = first + count;
-            power = 0.0;
+            begin  = first;
+            end    = first + count;
+            power  = 0.0;
+            power2 = 0.0;
             for (uint32_t o = first; o < end; ++o) {
                 ++seen[o];
-                power += t.cones[12 * size_t(o) + 8];
+                double const p = t.cones[12 * size_t(o) + 8];
+                power += p;
+                power2 += p * p;
             }
         } else {
             if (first + 1 >= t.num_nodes) {
@@ -75,18 +85,29 @@ struct Checker {
                 return;
             }
             uint32_t b0, e0, b1, e1;
-            double   p0, p1;
-            walk(first, b0, e0, p0, depth + 1);
-            walk(first + 1, b1, e1, p1, depth + 1);
+            double   p0, p1, q0, q1;
+            walk(first, b0, e0, p0, q0, depth + 1);
+            walk(first + 1, b1, e1, p1, q1, depth + 1);
             if (e0 != b1 || u32(nd[11]) != b1) {
                 fail("middle", n);
             }
-            begin = b0;
-            end   = e1;
-            power = p0 + p1;
+            begin  = b0;
+            end    = e1;
+            power  = p0 + p1;
+            power2 = q0 + q1;
         }
         if (std::fabs(power - nd[8]) > 1e-4 * std::fabs(power) + 1e-6) {
             fail("power", n);
+        }
+        uint32_t const lights = end - begin;
+        if (u32(nd[13]) != lights) {
+            fail("light count", n);
+        }
+        double const mean     = power / lights;
+        double const variance = std::fabs(power2 / lights - mean * mean);
+        if (std::fabs(variance - nd[12]) > 1e-3 * variance + 1e-3 * mean * mean + 1e-9 ||
+            std::fabs(variance + mean * mean - nd[14]) > 1e-4 * (variance + mean * mean) + 1e-9) {
+            fail("variance", n);
         }
         // bounds of every light below
         double const c[3] = {nd[0], nd[1], nd[2]};
@@ -145,8 +166,15 @@ bool check(std::vector<Light_input> const& in, uint32_t num_triangles, char cons
             k.fail("order", uint32_t(o));
         }
     }
+    uint32_t const picks = spb::render::max_split_picks(t, 0);
+    if (k.ok && (picks == 0 || picks > spb::render::Max_light_picks ||
+                 spb::render::max_split_picks(t, spb::render::Max_split_depth) != 1u ||
+                 (in.size() <= spb::render::Light_leaf_size && picks != in.size()))) {
+        std::printf("FAIL %s: max_split_picks %u\n", name, picks);
+        k.ok = false;
+    }
     if (k.ok) {
-        std::printf("ok %s %u %u\n", name, t.num_nodes, t.depth);
+        std::printf("ok %s %u %u %u\n", name, t.num_nodes, t.depth, picks);
     }
     return k.ok;
 }
