@@ -217,6 +217,29 @@ typedef struct spb_render_stats {
 SPB_API int32_t spb_render_last_stats(spb_render_stats* out);
 
 /*
+ * Several views of the engine's scene in one render: the scene the su_* calls built (uploaded
+ * first if it changed), the integrator, sampler kind and settings of the engine, and `count`
+ * cameras, each with its own resolution, horizontal field of view (radians) and row-major
+ * 4 x 4 camera-to-world transformation (as su_entity_set_transformation takes for the camera
+ * entity).  Every view gets samples_per_pixel samples; their paths share the renderer's waves,
+ * so small views fill the GPU together, and each view traces the same paths as when rendered
+ * alone.  rgba receives the resolved linear images one after another (view 0's
+ * width x height x 4 floats first), as su_copy_framebuffer(SU_FLOAT32, ...) would for each.
+ * No counterpart in the reference, which renders one camera per frame (rendering_driver.cpp);
+ * the engine's own camera is re-applied by its next su_* frame.
+ * SPB_ERROR_STATE without an engine or complete scene, SPB_ERROR_ARGUMENT for bad views
+ * (1 to 4096 of them, each with a positive resolution and field of view).
+ */
+typedef struct spb_view {
+    uint32_t width;
+    uint32_t height;
+    float    fov;
+    float    transformation[16];
+} spb_view;
+SPB_API int32_t spb_render_views(uint32_t count, spb_view const* views, uint32_t samples_per_pixel,
+                                 float* rgba);
+
+/*
  * The 32 x 32 GGX directional-albedo table the Substitute material's energy compensation
  * reads (row = alpha index, column = cos(theta_o) index, both i / 31), as computed by this
  * library.  Stands in for the reference's generated table E

@@ -57,6 +57,16 @@ class RenderStats(ctypes.Structure):
     ]
 
 
+class View(ctypes.Structure):
+    """spb_view: one camera of spb_render_views."""
+    _fields_ = [
+        ("width", c_u32),
+        ("height", c_u32),
+        ("fov", ctypes.c_float),
+        ("transformation", ctypes.c_float * 16),
+    ]
+
+
 # name -> (restype, argtypes); mirrors include/sprout_b200.h one to one.
 PROTOTYPES = {
     "spb_last_error": (ctypes.c_char_p, []),
@@ -75,6 +85,7 @@ PROTOTYPES = {
     "spb_synth_rays": (c_i32, [c_u64, c_u64, c_u32, c_f32, c_vp, c_u32]),
     "spb_ggx_albedo_table": (c_i32, [c_vp]),
     "spb_render_last_stats": (c_i32, [ctypes.POINTER(RenderStats)]),
+    "spb_render_views": (c_i32, [c_u32, ctypes.POINTER(View), c_u32, c_vp]),
     "spb_guide_parameter_count": (c_i32, [ctypes.POINTER(ctypes.c_uint32)]),
     "spb_guide_forward": (c_i32, [c_vp, c_vp, ctypes.c_uint64, c_vp]),
     "spb_guide_gradients": (c_i32, [c_vp, c_vp, c_vp, c_vp, ctypes.c_uint64, c_vp]),

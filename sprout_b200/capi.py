@@ -119,6 +119,24 @@ class SuLibrary:
         m = np.ascontiguousarray(matrix, np.float32).reshape(16)
         return self.lib.su_entity_set_transformation(entity, m.ctypes.data)
 
+    def render_views(self, views, spp):
+        """Renders the engine's scene from several cameras in one call (spb_render_views of the
+        sprout_b200 library): views are (width, height, fov_radians, 4x4 row-major
+        camera-to-world matrix) tuples; returns one (height, width, 4) float32 image per view."""
+        arr = (_lib.View * len(views))()
+        total = 0
+        for v, (w, h, fov, m) in zip(arr, views):
+            v.width, v.height, v.fov = int(w), int(h), float(fov)
+            v.transformation[:] = [float(x) for x in np.asarray(m, np.float32).reshape(16)]
+            total += int(w) * int(h)
+        out = np.zeros(total * 4, np.float32)
+        _lib.check(self.lib.spb_render_views(len(views), arr, int(spp), out.ctypes.data))
+        images, at = [], 0
+        for w, h, _, _ in views:
+            images.append(out[at * 4:(at + w * h) * 4].reshape(h, w, 4))
+            at += w * h
+        return images
+
     def framebuffer(self, width, height):
         out = np.zeros((height, width, 4), np.float32)
         status = self.lib.su_copy_framebuffer(SU_FLOAT32, width, height, 4, out.ctypes.data)

@@ -1998,6 +1998,50 @@ SU_LIBRARY_API int32_t su_copy_framebuffer(uint32_t type, uint32_t width, uint32
     return -2;
 }
 
+SPB_API int32_t spb_render_views(uint32_t count, spb_view const* views, uint32_t samples_per_pixel,
+                                 float* rgba) {
+    if (!engine) {
+        return SPB_ERROR_STATE;
+    }
+    if (!views || !rgba || count == 0 || count > spb::render::Max_views || samples_per_pixel == 0) {
+        return SPB_ERROR_ARGUMENT;
+    }
+    if (!ready()) {
+        return SPB_ERROR_STATE;
+    }
+    std::vector<spb::render::Camera_desc> cams(count);
+    for (uint32_t v = 0; v < count; ++v) {
+        cams[v].width  = views[v].width;
+        cams[v].height = views[v].height;
+        cams[v].fov    = views[v].fov;
+        decompose(views[v].transformation, cams[v].rotation, cams[v].position);
+    }
+    // the scene (if it changed) and the engine's settings; its camera entity comes back with
+    // its next frame
+    if (engine->scene_dirty) {
+        if (compile_scene() != 0) {
+            return SPB_ERROR_STATE;
+        }
+        engine->scene_dirty = false;
+    } else if (apply_camera() != 0) {
+        return SPB_ERROR_STATE;
+    }
+    engine->camera_dirty  = true;
+    engine->frame_started = false;
+    if (int32_t const s = engine->renderer.set_views(cams)) {
+        log(SU_LOG_ERROR, engine->renderer.error());
+        return s;
+    }
+    if (render_samples(0, samples_per_pixel) != 0) {
+        return SPB_ERROR_CUDA;
+    }
+    if (int32_t const s = engine->renderer.resolve(rgba)) {
+        log(SU_LOG_ERROR, engine->renderer.error());
+        return s;
+    }
+    return SPB_OK;
+}
+
 SPB_API int32_t spb_render_last_stats(spb_render_stats* out) {
     if (!engine || !out) {
         return SPB_ERROR_ARGUMENT;

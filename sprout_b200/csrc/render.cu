@@ -62,10 +62,11 @@ constexpr uint32_t Class_surface    = 1;  // Wide_triangle::tri_class of ordinar
 constexpr uint32_t Class_boundary   = 2;  // ... of participating-medium boundaries
 constexpr uint32_t Class_instance   = 4;  // ... of top-level leaves (instances)
 
-// Counter block (uint32): per bounce b, [8b] extension count, [8b+1] shadow count,
-// [8b+2] extend fetch, [8b+3] shadow fetch, [8b+4] transmittance count, [8b+5] picks of split
-// light selections, [8b+6] split records; then the overflow counter.
-constexpr uint32_t Counter_stride = 8;
+// Counter block (uint32): per bounce b, at Counter_stride * b + k: k = 0 extension count,
+// 1 shadow count, 2 extend fetch, 3 shadow fetch, 4 shadow slots through media (rays to
+// emitters), 5 picks of split light selections, 6 split records, 7 picks through media,
+// 8 shadow slots through media (rays to the environment); then the overflow counter.
+constexpr uint32_t Counter_stride = 16;
 constexpr uint32_t Graph_max_paths = 1u << 21;  // largest wave replayed from a CUDA graph
 constexpr uint64_t Pick_budget     = 24ull << 30;  // bytes of picks a wave may hold
 constexpr uint32_t Counter_words  = Counter_stride * Max_bounce_slots + 4;
@@ -189,6 +190,11 @@ struct Paths {
     float4*   sh_d;
     float4*   sh_L;
     float4*   prev_n;  // geometric normal at the last scattering vertex; w 1: medium vertex
+    // Second shadow slot: the environment's sample when light selection splits; its
+    // contribution accumulates in L2, so that no two kernel threads add to the same radiance.
+    float4*   sh2_o;
+    float4*   sh2_d;
+    float4*   sh2_L;
     // Vertices whose light selection splits into several lights (select_lights): one record per
     // vertex per bounce -- (shadow-ray origin, path) and (first pick, picks, depth, 0) -- and
     // per selected light a pick: (direction, distance) and (contribution, record).  Shadow rays
@@ -225,9 +231,12 @@ constexpr int Record_float4 = 5;
 // kappa / (2 pi (1 - e^{-2 kappa})), so that a density evaluation takes one exponential per lobe.
 constexpr int Mixture_floats = 48;
 
-// Shadow-queue entries are path indices (the path's shadow slot) or, with this bit, pick
-// indices (a light of a split selection).
-constexpr uint32_t Pick_shadow = 0x80000000u;
+// Shadow-queue entries are path indices (the path's first shadow slot), path indices with
+// Second_shadow (its second slot: the environment's sample of a split selection), or pick
+// indices with Pick_shadow (an emitter of a split selection that chose several).
+constexpr uint32_t Pick_shadow   = 0x80000000u;
+constexpr uint32_t Second_shadow = 0x40000000u;
+constexpr uint32_t Entry_index   = 0x3FFFFFFFu;
 
 struct Cam {
     float3   left_top;
@@ -261,10 +270,32 @@ struct Wave {
 // A wave's launch parameters, which the kernels read from device memory: the host writes them
 // (pinned) and copies them before each wave, so that one captured CUDA graph replays every wave
 // of the same shape.
+//
+// A render covers one or more views (cameras with their own resolution), their bordered pixel
+// ranges concatenated into one sample space of `pixels` entries: view v owns [view_offsets[v],
+// view_offsets[v + 1]) and its film pixels [film_offsets[v], film_offsets[v + 1]).
 struct Launch {
-    Cam  cam;
-    Wave wave;
+    Cam const*      cams;
+    uint32_t const* view_offsets;
+    uint32_t const* film_offsets;
+    uint32_t        num_views;
+    uint32_t        pixels;  // bordered pixels of all views
+    Wave            wave;
 };
+
+// The view owning entry x of a prefix table offsets[0 .. n] (offsets[0] = 0).
+__device__ __forceinline__ uint32_t view_of(uint32_t const* offsets, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, hi = n;  // offsets[lo] <= x < offsets[hi]
+    while (hi - lo > 1) {
+        uint32_t const mid = (lo + hi) >> 1;
+        if (__ldg(offsets + mid) <= x) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
 
 // ---- PCG32 (O'Neill 2014), seeded as rnd::Generator::start (base/random/generator.inl) ----
 __device__ __forceinline__ uint32_t pcg_next(uint64_t& state, uint64_t inc) {
@@ -451,7 +482,6 @@ constexpr int Film_border = 1;
 // ---- generate: camera rays (Perspective::generate_ray, camera_perspective.cpp:47-80) ----
 __global__ void k_generate(Launch const* __restrict__ launch, Paths p, uint32_t* queue, uint32_t* counters,
                            uint32_t num_paths) {
-    Cam const      cam  = launch->cam;
     Wave const     wave = launch->wave;
     uint32_t const i    = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
@@ -460,19 +490,25 @@ __global__ void k_generate(Launch const* __restrict__ launch, Paths p, uint32_t*
     if (i >= num_paths) {
         return;
     }
-    uint32_t const bw     = cam.w + 2 * Film_border;
-    uint32_t const pixels = bw * (cam.h + 2 * Film_border);
+    uint32_t const pixels = launch->pixels;
     uint32_t const pixel  = i % pixels;
     uint32_t const slot   = i / pixels;
-    int const      x      = int(pixel % bw) - Film_border;
-    int const      y      = int(pixel / bw) - Film_border;
+    uint32_t const view   = view_of(launch->view_offsets, launch->num_views, pixel);
+    Cam const      cam    = launch->cams[view];
+    uint32_t const local  = pixel - launch->view_offsets[view];
+    uint32_t const bw     = cam.w + 2 * Film_border;
+    int const      x      = int(local % bw) - Film_border;
+    int const      y      = int(local / bw) - Film_border;
 
-    Rng rng;
-    rng.start(wave.seed, uint64_t(pixel) + uint64_t(wave.first_sample + slot) * pixels);
+    // A view's sample streams depend on its own pixel index and size only, so that a view
+    // rendered with others traces the paths it would trace alone.
+    uint32_t const view_pixels = launch->view_offsets[view + 1] - launch->view_offsets[view];
+    Rng            rng;
+    rng.start(wave.seed, uint64_t(local) + uint64_t(wave.first_sample + slot) * view_pixels);
     float u = rng.uniform();
     float v = rng.uniform();
     if (wave.golden_n) {
-        float2 const g = golden_2d(wave, pixel, wave.first_sample + slot, 0);
+        float2 const g = golden_2d(wave, local, wave.first_sample + slot, 0);
         u              = g.x;
         v              = g.y;
     }
@@ -507,6 +543,19 @@ __global__ void k_generate(Launch const* __restrict__ launch, Paths p, uint32_t*
     }
 }
 
+// Where k_trace puts unoccluded shadow rays of a scene with media (for k_transmit): slot
+// entries into queue (rays to emitters from the front, counted by count; rays to the
+// environment from the back, entry capacity - 1 downwards, counted by env_count), picks into
+// pick_queue.
+struct Transmit_out {
+    uint32_t* queue;
+    uint32_t* count;
+    uint32_t* env_count;
+    uint32_t  capacity;
+    uint32_t* pick_queue;
+    uint32_t* pick_count;
+};
+
 // ---- extend / shadow: persistent traversal over a queue of path indices ----
 // Any_hit: shadow rays.  Media: the scene has participating media -- shadow rays ignore
 // medium boundaries and unoccluded ones go to the transmittance queue instead of adding
@@ -516,7 +565,7 @@ template <bool Any_hit, bool Media = false, bool Instances = false>
 __global__ void __launch_bounds__(Trace_block)
     k_trace(Scene_gpu s, Paths p, uint32_t const* __restrict__ queue,
             uint32_t const* __restrict__ count, uint32_t* fetch, uint32_t* overflow,
-            uint32_t* transmit_queue = nullptr, uint32_t* transmit_count = nullptr) {
+            Transmit_out tq = Transmit_out{}) {
     uint32_t const num  = *count;
     uint32_t const lane = threadIdx.x & 31u;
     uint32_t const lt   = (1u << lane) - 1u;
@@ -550,13 +599,15 @@ __global__ void __launch_bounds__(Trace_block)
                 if (mine < num) {
                     path = queue[mine];
                     if (Any_hit) {
+                        uint32_t const e = path & Entry_index;
                         if (path & Pick_shadow) {
-                            uint32_t const pk  = path & ~Pick_shadow;
-                            uint32_t const rec = __float_as_uint(p.pick_c[pk].w);
+                            uint32_t const rec = __float_as_uint(p.pick_c[e].w);
                             float4 const   o   = p.split_o[rec];
-                            gpu::start_ray(r, tv, make_float4(o.x, o.y, o.z, 0.f), p.pick_d[pk]);
+                            gpu::start_ray(r, tv, make_float4(o.x, o.y, o.z, 0.f), p.pick_d[e]);
+                        } else if (path & Second_shadow) {
+                            gpu::start_ray(r, tv, p.sh2_o[e], p.sh2_d[e]);
                         } else {
-                            gpu::start_ray(r, tv, p.sh_o[path], p.sh_d[path]);
+                            gpu::start_ray(r, tv, p.sh_o[e], p.sh_d[e]);
                         }
                     } else {
                         gpu::start_ray(r, tv, p.ray_o[path], p.ray_d[path]);
@@ -575,20 +626,33 @@ __global__ void __launch_bounds__(Trace_block)
                                                             overflow, Class_boundary, &is,
                                                             s.inst_trace)) {
             if (Any_hit) {
+                uint32_t const e = path & Entry_index;
                 if (r.best_id == gpu::Miss) {
                     if (Media) {
-                        transmit_queue[atomicAdd(transmit_count, 1u)] = path;
+                        // Through media: picks to their own queue; slot rays to the environment
+                        // fill the slot queue from its back, the others from its front, so that
+                        // k_transmit's warps walk rays of one kind (their lengths through a
+                        // medium differ widely).
+                        if (path & Pick_shadow) {
+                            tq.pick_queue[atomicAdd(tq.pick_count, 1u)] = path;
+                        } else if (((path & Second_shadow) ? p.sh2_d[e].w : p.sh_d[e].w) >= Ray_max_t) {
+                            tq.queue[tq.capacity - 1u - atomicAdd(tq.env_count, 1u)] = path;
+                        } else {
+                            tq.queue[atomicAdd(tq.count, 1u)] = path;
+                        }
                     } else if (!(path & Pick_shadow)) {
-                        float4 const c = p.sh_L[path];
-                        float4       l = p.L[path];
+                        bool const   second = path & Second_shadow;
+                        float4 const c      = second ? p.sh2_L[e] : p.sh_L[e];
+                        float4* const Lp    = second ? p.L2 : p.L;
+                        float4       l      = Lp[e];
                         l.x += c.x;
                         l.y += c.y;
                         l.z += c.z;
-                        p.L[path] = l;
+                        Lp[e] = l;
                     }
                 } else if (path & Pick_shadow) {
                     // occluded: the pick adds nothing
-                    float* const c = reinterpret_cast<float*>(p.pick_c + (path & ~Pick_shadow));
+                    float* const c = reinterpret_cast<float*>(p.pick_c + e);
                     c[0] = 0.f;
                     c[1] = 0.f;
                     c[2] = 0.f;
@@ -1363,11 +1427,20 @@ __device__ __forceinline__ bool splits_at(Scene_gpu const& s, uint32_t depth) {
     return depth < s.split_bounces;
 }
 
-__device__ __forceinline__ void store_shadow(Paths const& p, uint32_t path, V3 o, Light_sample const& ls,
-                                             V3 contrib, uint32_t depth) {
-    p.sh_o[path] = make_float4(o.x, o.y, o.z, 0.f);
-    p.sh_d[path] = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
-    p.sh_L[path] = make_float4(contrib.x, contrib.y, contrib.z, float(depth));
+__device__ __forceinline__ void store_shadow(Paths const& p, uint32_t path, bool second, V3 o,
+                                             Light_sample const& ls, V3 contrib, uint32_t depth) {
+    float4 const ro = make_float4(o.x, o.y, o.z, 0.f);
+    float4 const rd = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
+    float4 const c  = make_float4(contrib.x, contrib.y, contrib.z, float(depth));
+    if (second) {
+        p.sh2_o[path] = ro;
+        p.sh2_d[path] = rd;
+        p.sh2_L[path] = c;
+    } else {
+        p.sh_o[path] = ro;
+        p.sh_d[path] = rd;
+        p.sh_L[path] = c;
+    }
 }
 
 // The wave's queues and counters k_shade appends to.
@@ -1383,14 +1456,16 @@ struct Shade_out {
 // Next-event estimation at a vertex (sample_lights / evaluate_light, pathtracer_mis.cpp:281-347):
 // the lights select_lights chooses with the random number `select`, a sample on each (the
 // pixel's golden ratio dimension of that light at the first vertices, else the path's random
-// stream), and each sample's contribution eval(ls).  A single light goes to the path's shadow
-// slot (returns true when it holds a ray); several get a split record and a pick each, their
-// contributions summed by k_pick_sum after the shadow rays.
+// stream), and each sample's contribution eval(ls).  The environment of a split selection (its
+// first light) takes the path's second shadow slot; a single other light the first slot;
+// several emitters get a split record and a pick each, their contributions summed by
+// k_pick_sum after the shadow rays.  shadow / shadow2: the slots hold rays.
 template <class Eval>
-__device__ __forceinline__ bool next_event(Scene_gpu const& s, Paths const& p, Wave const& wave,
+__device__ __forceinline__ void next_event(Scene_gpu const& s, Paths const& p, Wave const& wave,
                                            Shade_out const& out, uint32_t path, V3 ps, V3 n,
                                            bool total_sphere, uint32_t depth, float select, Rng& rng,
-                                           bool golden, uint32_t gpixel, uint32_t gsample, Eval const& eval) {
+                                           bool golden, uint32_t gpixel, uint32_t gsample, Eval const& eval,
+                                           bool& shadow, bool& shadow2) {
     Light_pick     picks[Max_light_picks];
     uint32_t const m     = select_lights(s, ps, n, total_sphere, select, splits_at(s, depth), picks);
     auto const     point = [&](uint32_t l, float& r1, float& r2) {
@@ -1403,53 +1478,61 @@ __device__ __forceinline__ bool next_event(Scene_gpu const& s, Paths const& p, W
             r2 = rng.uniform();
         }
     };
-    if (m == 0) {
-        return false;
-    }
-    if (m == 1) {
+    auto const slot = [&](uint32_t l, bool second) {
         float r1, r2;
-        point(0, r1, r2);
+        point(l, r1, r2);
         Light_sample ls;
-        if (sample_light(s, ps, n, total_sphere, picks[0], r1, r2, ls)) {
+        if (sample_light(s, ps, n, total_sphere, picks[l], r1, r2, ls)) {
             V3 const c = eval(ls);
             if (shading::max_component(c) > 0.f) {
-                store_shadow(p, path, ps, ls, c, depth);
+                store_shadow(p, path, second, ps, ls, c, depth);
                 return true;
             }
         }
         return false;
+    };
+    uint32_t first = 0;
+    if (m > 1 && picks[0].light == Env_pick) {
+        shadow2 = slot(0, true);
+        first   = 1;
     }
-    uint32_t const base = atomicAdd(out.count_picks, m);
+    uint32_t const count = m - first;
+    if (count == 1) {
+        shadow = slot(first, false);
+    }
+    if (count < 2) {
+        return;
+    }
+    uint32_t const base = atomicAdd(out.count_picks, count);
     uint32_t const rec  = atomicAdd(out.count_records, 1u);
     p.split_o[rec]      = make_float4(ps.x, ps.y, ps.z, __uint_as_float(path));
-    p.split_m[rec]      = make_uint4(base, m, depth, 0u);
+    p.split_m[rec]      = make_uint4(base, count, depth, 0u);
     uint64_t valid      = 0;
-    for (uint32_t l = 0; l < m; ++l) {
+    for (uint32_t k = 0; k < count; ++k) {
         float r1, r2;
-        point(l, r1, r2);
+        point(first + k, r1, r2);
         Light_sample ls;
         V3           c = v3(0.f, 0.f, 0.f);
         float4       d = make_float4(0.f, 0.f, 1.f, 0.f);
-        if (sample_light(s, ps, n, total_sphere, picks[l], r1, r2, ls)) {
+        if (sample_light(s, ps, n, total_sphere, picks[first + k], r1, r2, ls)) {
             V3 const e = eval(ls);
             if (shading::max_component(e) > 0.f) {
                 c = e;
                 d = make_float4(ls.dir.x, ls.dir.y, ls.dir.z, ls.dist);
-                valid |= 1ull << l;
+                valid |= 1ull << k;
             }
         }
-        p.pick_d[base + l] = d;
-        p.pick_c[base + l] = make_float4(c.x, c.y, c.z, __uint_as_float(rec));
+        p.pick_d[base + k] = d;
+        p.pick_c[base + k] = make_float4(c.x, c.y, c.z, __uint_as_float(rec));
     }
     if (valid != 0) {
         uint32_t q = atomicAdd(out.count_shadow, uint32_t(__popcll(valid)));
-        for (uint32_t l = 0; l < m; ++l) {
-            if ((valid >> l) & 1u) {
-                out.sq[q++] = Pick_shadow | (base + l);
+        for (uint32_t k = 0; k < count; ++k) {
+            if ((valid >> k) & 1u) {
+                out.sq[q++] = Pick_shadow | (base + k);
             }
         }
     }
-    return false;
 }
 
 // Sums each split record's picks (in pick order) into its path's L2, after the bounce's shadow
@@ -1762,7 +1845,8 @@ __global__ void __launch_bounds__(Shade_block)
     uint32_t const num = *count_in;
 
     bool     extend  = false;
-    bool     shadow  = false;  // the path's shadow slot holds a ray
+    bool     shadow  = false;  // the path's first shadow slot holds a ray
+    bool     shadow2 = false;  // ... its second
     uint32_t path    = 0;
 
     if (i < num) {
@@ -1861,12 +1945,12 @@ __global__ void __launch_bounds__(Shade_block)
                 V3 const    pos = v3(ro.x + t_sc * rd.x, ro.y + t_sc * rd.y, ro.z + t_sc * rd.z);
                 V3 const    wo  = -dir_in;
                 float const select = rng.uniform();
-                shadow = next_event(s, p, wave, out, path, pos, v3(0.f, 0.f, 1.f), true, depth, select, rng,
-                                    false, 0u, 0u, [&](Light_sample const& ls) {
-                                        float const f = shading::phase_hg(shading::dot(wo, ls.dir), g);
-                                        float const w = ls.pdf / (ls.pdf * ls.pdf + f * f);
-                                        return (w * f) * (T * ls.radiance);
-                                    });
+                next_event(s, p, wave, out, path, pos, v3(0.f, 0.f, 1.f), true, depth, select, rng, false, 0u,
+                           0u, [&](Light_sample const& ls) {
+                               float const f = shading::phase_hg(shading::dot(wo, ls.dir), g);
+                               float const w = ls.pdf / (ls.pdf * ls.pdf + f * f);
+                               return (w * f) * (T * ls.radiance);
+                           }, shadow, shadow2);
                 float const x0 = rng.uniform();
                 float const x1 = rng.uniform();
                 float       pdf;
@@ -1979,23 +2063,23 @@ __global__ void __launch_bounds__(Shade_block)
                 // The first vertices sample from the pixel's golden ratio sequences (batch
                 // rendering), the others from the path's random stream.
                 bool const     golden  = wave.golden_n != 0 && depth < Golden_bounces;
-                uint32_t const pixels  = (launch->cam.w + 2 * Film_border) * (launch->cam.h + 2 * Film_border);
-                uint32_t const gpixel  = path % pixels;
+                uint32_t const pixels  = launch->pixels;
+                uint32_t const gview   = view_of(launch->view_offsets, launch->num_views, path % pixels);
+                uint32_t const gpixel  = path % pixels - launch->view_offsets[gview];  // within its view
                 uint32_t const gsample = wave.first_sample + path / pixels;
 
                 // Next-event estimation (sample_lights / evaluate_light, pathtracer_mis.cpp:281-347).
                 V3 const    ps     = offset_ray(pos, geo_n);
                 float const select = golden ? golden_1d(wave, gpixel, gsample, golden_light_1d(depth, 0))
                                             : rng.uniform();
-                shadow = next_event(s, p, wave, out, path, ps, geo_n, false, depth, select, rng, golden, gpixel,
-                                    gsample, [&](Light_sample const& ls) {
-                                        shading::Bxdf const f =
-                                            shading::substitute_evaluate(mat, s.e_table, ctx, ls.dir);
-                                        float const pc = guided ? gf * mixture_pdf_at(mix, ls.dir) + (1.f - gf) * f.pdf
-                                                                : f.pdf;
-                                        float const w  = ls.pdf / (ls.pdf * ls.pdf + pc * pc);
-                                        return w * (T * (ls.radiance * f.reflection));
-                                    });
+                next_event(s, p, wave, out, path, ps, geo_n, false, depth, select, rng, golden, gpixel, gsample,
+                           [&](Light_sample const& ls) {
+                               shading::Bxdf const f = shading::substitute_evaluate(mat, s.e_table, ctx, ls.dir);
+                               float const pc = guided ? gf * mixture_pdf_at(mix, ls.dir) + (1.f - gf) * f.pdf
+                                                       : f.pdf;
+                               float const w  = ls.pdf / (ls.pdf * ls.pdf + pc * pc);
+                               return w * (T * (ls.radiance * f.reflection));
+                           }, shadow, shadow2);
 
                 // Continuation direction: the BSDF sample (pathtracer_mis.cpp:153-201), or with
                 // probability gf the guide's.  A guide direction gets the BSDF value and pdf the
@@ -2079,109 +2163,127 @@ __global__ void __launch_bounds__(Shade_block)
     if (shadow) {
         out.sq[sslot] = path;
     }
+    uint32_t const sslot2 = append(out.count_shadow, shadow2);
+    if (shadow2) {
+        out.sq[sslot2] = path | Second_shadow;
+    }
 }
 
 // ---- shadow rays through media: Worker::transmittance (rendering_worker.cpp:209-267) ----
-// For each unoccluded shadow ray of a scene with media, walks the medium boundaries along the
-// ray (closest hits on boundary triangles only).  Homogeneous segments add their optical depth;
-// density-grid segments multiply in a ratio-tracking estimate (which uses the path's random
-// stream).  The light contribution, times the transmittance, is added to the path's radiance.
-template <bool Instances = false>
-__global__ void __launch_bounds__(Trace_block)
-    k_transmit(Scene_gpu s, Paths p, uint32_t const* __restrict__ queue,
-               uint32_t const* __restrict__ count, uint32_t* overflow) {
-    uint32_t const num = *count;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < num; i += gridDim.x * blockDim.x) {
-        uint32_t const entry = queue[i];
-        bool const     pick  = entry & Pick_shadow;
-        uint32_t const pk    = entry & ~Pick_shadow;
-        // The ray and its contribution: the path's shadow slot, or a pick of a split selection
-        // (its origin, path and depth in the vertex's record).
-        uint32_t path, depth, stream;
-        float4   ro, rd, c;
-        if (pick) {
-            c                   = p.pick_c[pk];
-            rd                  = p.pick_d[pk];
-            uint32_t const rec  = __float_as_uint(c.w);
-            float4 const   o    = p.split_o[rec];
-            uint4 const    m    = p.split_m[rec];
-            ro                  = make_float4(o.x, o.y, o.z, 0.f);
-            path                = __float_as_uint(o.w);
-            depth               = m.z;
-            stream              = 1u + (pk - m.x);
-        } else {
-            path   = entry;
-            ro     = p.sh_o[path];
-            rd     = p.sh_d[path];
-            c      = p.sh_L[path];
-            depth  = uint32_t(c.w);
-            stream = 0u;
+// One shadow ray's walk from its origin: medium boundaries found by closest hits on boundary
+// triangles, homogeneous segments adding their optical depth, density-grid segments
+// multiplying in a ratio-tracking estimate (on a stream of its own, seeded from the path's
+// state, which this kernel only reads: a vertex's shadow rays may be in flight together).
+// Returns false when the ray is blocked; tr receives the transmittance.
+template <bool Instances>
+__device__ __forceinline__ bool walk_shadow(Scene_gpu const& s, Paths const& p, uint32_t path, float4 ro, float4 rd,
+                                            uint32_t depth, uint32_t stream, uint32_t* overflow, V3& tr) {
+    uint32_t medium = p.info[path] >> 17;
+    float    t0     = ro.w;
+    V3       tau    = v3(0.f, 0.f, 0.f);
+    V3       w      = v3(1.f, 1.f, 1.f);
+    bool     random = false;
+    Rng      rng;
+    uint2    stack[gpu::Stack_size];
+    for (int crossing = 0; crossing < 64; ++crossing) {
+        gpu::Ray_state      r;
+        gpu::Traversal      tv;
+        gpu::Instance_state is;
+        gpu::start_ray(r, tv, make_float4(ro.x, ro.y, ro.z, t0), rd);
+        if constexpr (Instances) {
+            gpu::start_instances(r, is);
         }
-        uint32_t medium  = p.info[path] >> 17;
-        float    t0      = ro.w;
-        V3       tau     = v3(0.f, 0.f, 0.f);
-        V3       w       = v3(1.f, 1.f, 1.f);
-        bool     random  = false;  // this shadow ray's random stream was started
-        bool     blocked = false;
-        Rng      rng;
-        uint2    stack[gpu::Stack_size];
-        for (int crossing = 0; crossing < 64; ++crossing) {
-            gpu::Ray_state      r;
-            gpu::Traversal      tv;
-            gpu::Instance_state is;
-            gpu::start_ray(r, tv, make_float4(ro.x, ro.y, ro.z, t0), rd);
-            if constexpr (Instances) {
-                gpu::start_instances(r, is);
-            }
-            while (!gpu::traversal_step<false, true, Instances>(r, tv, stack, s.nodes, s.tris, s.hit_margin,
-                                                                overflow, Class_surface, &is, s.inst_trace)) {
-            }
-            bool const  hit = r.best_id != gpu::Miss;
-            float const end = hit ? r.tbest : rd.w;
-            if (medium != 0) {
-                shading::Material const m = s.materials[medium - 1];
-                if (m.medium != 0) {
-                    if (!random) {
-                        // A stream of its own, seeded from the path's state (which this kernel
-                        // only reads: several shadow rays of a vertex may be in flight together).
-                        uint4 const st = p.rng[path];
-                        rng.start((uint64_t(st.y) << 32) | st.x, (uint64_t(path) << 7) | stream);
-                        random = true;
-                    }
-                    float const srs = shading::similarity_relation_scale(m.g, depth);
-                    if (!transmit_grid(s.media[m.medium - 1], m, srs, f3v(ro), f3v(rd), t0, end, rng,
-                                       w, s.tracking_capped)) {
-                        blocked = true;
-                        break;
-                    }
-                } else {
-                    float const len = fmaxf(end - t0, 0.f);
-                    tau = tau + len * (m.mu_a + m.mu_s);
+        while (!gpu::traversal_step<false, true, Instances>(r, tv, stack, s.nodes, s.tris, s.hit_margin,
+                                                            overflow, Class_surface, &is, s.inst_trace)) {
+        }
+        bool const  hit = r.best_id != gpu::Miss;
+        float const end = hit ? r.tbest : rd.w;
+        if (medium != 0) {
+            shading::Material const m = s.materials[medium - 1];
+            if (m.medium != 0) {
+                if (!random) {
+                    uint4 const st = p.rng[path];
+                    rng.start((uint64_t(st.y) << 32) | st.x, (uint64_t(path) << 7) | stream);
+                    random = true;
                 }
-            }
-            if (!hit) {
-                break;
-            }
-            World_tri const wt  = world_triangle(s, Instances ? is.best_inst : 0u, r.best_id);
-            V3 const        geo = shading::cross(wt.b - wt.a, wt.c - wt.a);
-            medium              = shading::dot(geo, v3(rd.x, rd.y, rd.z)) < 0.f ? wt.material + 1 : 0;
-            t0                  = offset_f(r.tbest);
-            if (t0 >= rd.w) {
-                break;
+                float const srs = shading::similarity_relation_scale(m.g, depth);
+                if (!transmit_grid(s.media[m.medium - 1], m, srs, f3v(ro), f3v(rd), t0, end, rng,
+                                   w, s.tracking_capped)) {
+                    return false;
+                }
+            } else {
+                float const len = fmaxf(end - t0, 0.f);
+                tau = tau + len * (m.mu_a + m.mu_s);
             }
         }
-        V3 const tr = blocked ? v3(0.f, 0.f, 0.f)
-                              : v3(w.x * expf(-tau.x), w.y * expf(-tau.y), w.z * expf(-tau.z));
-        if (pick) {
-            p.pick_c[pk] = make_float4(tr.x * c.x, tr.y * c.y, tr.z * c.z, c.w);
-        } else if (!blocked) {
-            float4 l = p.L[path];
-            l.x += tr.x * c.x;
-            l.y += tr.y * c.y;
-            l.z += tr.z * c.z;
-            p.L[path] = l;
+        if (!hit) {
+            break;
+        }
+        World_tri const wt  = world_triangle(s, Instances ? is.best_inst : 0u, r.best_id);
+        V3 const        geo = shading::cross(wt.b - wt.a, wt.c - wt.a);
+        medium              = shading::dot(geo, v3(rd.x, rd.y, rd.z)) < 0.f ? wt.material + 1 : 0;
+        t0                  = offset_f(r.tbest);
+        if (t0 >= rd.w) {
+            break;
         }
     }
+    tr = v3(w.x * expf(-tau.x), w.y * expf(-tau.y), w.z * expf(-tau.z));
+    return true;
+}
+
+// Shadow slots through media, one thread per entry: the queue holds `count` rays to emitters
+// at its front and `env_count` rays to the environment at its back (entries capacity - 1
+// downwards).  The light contribution times the transmittance is added to the path's radiance
+// (L for the first slot, L2 for the second).  Picks take k_transmit_picks: a kernel of its own
+// keeps this one free of branches on the entry's kind, which cost most of its lanes.
+template <bool Instances = false>
+__global__ void __launch_bounds__(Trace_block)
+    k_transmit(Scene_gpu s, Paths p, uint32_t const* __restrict__ queue, uint32_t const* __restrict__ count,
+               uint32_t const* __restrict__ env_count, uint32_t capacity, uint32_t* overflow) {
+    uint32_t const j     = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t const front = *count;
+    if (j >= front + *env_count) {
+        return;
+    }
+    uint32_t const entry  = queue[j < front ? j : capacity - 1u - (j - front)];
+    uint32_t const path   = entry & Entry_index;
+    bool const     second = entry & Second_shadow;
+    float4 const   ro     = second ? p.sh2_o[path] : p.sh_o[path];
+    float4 const   rd     = second ? p.sh2_d[path] : p.sh_d[path];
+    float4 const   c      = second ? p.sh2_L[path] : p.sh_L[path];
+    V3             tr;
+    if (!walk_shadow<Instances>(s, p, path, ro, rd, uint32_t(c.w), second ? 1u : 0u, overflow, tr)) {
+        return;
+    }
+    float4* const Lp = second ? p.L2 : p.L;
+    float4        l  = Lp[path];
+    l.x += tr.x * c.x;
+    l.y += tr.y * c.y;
+    l.z += tr.z * c.z;
+    Lp[path] = l;
+}
+
+// Picks through media, one thread per entry: the pick's contribution is scaled by the
+// transmittance (zero when blocked) for k_pick_sum.
+template <bool Instances = false>
+__global__ void __launch_bounds__(Trace_block)
+    k_transmit_picks(Scene_gpu s, Paths p, uint32_t const* __restrict__ queue, uint32_t const* __restrict__ count,
+                     uint32_t* overflow) {
+    uint32_t const j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= *count) {
+        return;
+    }
+    uint32_t const pk  = queue[j] & Entry_index;
+    float4 const   c   = p.pick_c[pk];
+    uint32_t const rec = __float_as_uint(c.w);
+    float4 const   o   = p.split_o[rec];
+    uint4 const    m   = p.split_m[rec];
+    V3             tr  = v3(0.f, 0.f, 0.f);
+    if (!walk_shadow<Instances>(s, p, __float_as_uint(o.w), make_float4(o.x, o.y, o.z, 0.f), p.pick_d[pk], m.z,
+                                2u + (pk - m.x), overflow, tr)) {
+        tr = v3(0.f, 0.f, 0.f);
+    }
+    p.pick_c[pk] = make_float4(tr.x * c.x, tr.y * c.y, tr.z * c.z, c.w);
 }
 
 // ---- film: Filtered_1p0::add_sample (sensor/filtered.inl:125-187) as a gather ----
@@ -2195,21 +2297,25 @@ __device__ __forceinline__ float filter_weight(float d) {
     return c_filter[o] + t * (c_filter[o1] - c_filter[o]);
 }
 
-__global__ void k_gather(Paths p, uint32_t w, uint32_t h, uint32_t samples, float4* film,
-                         float4* comp) {
+__global__ void k_gather(Paths p, Launch const* __restrict__ launch, uint32_t film_pixels, uint32_t samples,
+                         float4* film, float4* comp) {
     uint32_t const q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= w * h) {
+    if (q >= film_pixels) {
         return;
     }
-    int const      x      = int(q % w);
-    int const      y      = int(q / w);
+    uint32_t const view   = view_of(launch->film_offsets, launch->num_views, q);
+    uint32_t const w      = launch->cams[view].w;
+    uint32_t const local  = q - launch->film_offsets[view];
+    int const      x      = int(local % w);
+    int const      y      = int(local / w);
     uint32_t const bw     = w + 2 * Film_border;
-    uint32_t const traced = bw * (h + 2 * Film_border);  // bordered pixels per sample slot
+    uint32_t const base   = launch->view_offsets[view];  // the view's first bordered pixel
+    uint32_t const traced = launch->pixels;               // bordered pixels per sample slot
     float4         acc    = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int dy = -1; dy <= 1; ++dy) {
         uint32_t const sy = uint32_t(y - dy + Film_border);  // bordered row, always inside
         for (int dx = -1; dx <= 1; ++dx) {
-            uint32_t const src = sy * bw + uint32_t(x - dx + Film_border);
+            uint32_t const src = base + sy * bw + uint32_t(x - dx + Film_border);
             for (uint32_t k = 0; k < samples; ++k) {
                 uint32_t const path = k * traced + src;
                 float2 const   uv   = p.puv[path];
@@ -2389,7 +2495,8 @@ struct Renderer::Device {
     Paths     paths{};
     uint32_t* queue[2] = {nullptr, nullptr};
     uint32_t* shadow_queue   = nullptr;
-    uint32_t* transmit_queue = nullptr;
+    uint32_t* transmit_queue      = nullptr;  // shadow slots through media (2 per path)
+    uint32_t* transmit_pick_queue = nullptr;  // picks through media
     uint32_t* counters       = nullptr;
     uint32_t* pinned_count   = nullptr;  // host-pinned word for the queue-length check
     bool      has_media      = false;
@@ -2402,7 +2509,13 @@ struct Renderer::Device {
     float4*   film = nullptr;
     float4*   comp = nullptr;
     float4*   out  = nullptr;
-    uint32_t  film_pixels = 0;
+    uint32_t  film_pixels = 0;    // film pixels of all views
+    // the views: cameras, prefix tables of their bordered (sampled) and film pixels
+    Cam*      cams          = nullptr;
+    uint32_t* view_offsets  = nullptr;
+    uint32_t* film_offsets  = nullptr;
+    uint32_t  num_views     = 0;
+    uint32_t  traced_pixels = 0;
     int       trace_grid  = 0;
     cudaStream_t stream   = nullptr;
     cudaEvent_t  ev0      = nullptr;
@@ -2590,6 +2703,9 @@ Renderer::~Renderer() {
     free_ptr(p.sh_L);
     free_ptr(p.prev_n);
     free_ptr(p.split_o);
+    free_ptr(p.sh2_o);
+    free_ptr(p.sh2_d);
+    free_ptr(p.sh2_L);
     free_ptr(p.split_m);
     free_ptr(p.pick_d);
     free_ptr(p.pick_c);
@@ -2604,6 +2720,7 @@ Renderer::~Renderer() {
     free_ptr(d_->queue[1]);
     free_ptr(d_->shadow_queue);
     free_ptr(d_->transmit_queue);
+    free_ptr(d_->transmit_pick_queue);
     free_ptr(d_->counters);
     if (d_->pinned_count) {
         cudaFreeHost(d_->pinned_count);
@@ -2611,6 +2728,9 @@ Renderer::~Renderer() {
     free_ptr(d_->film);
     free_ptr(d_->comp);
     free_ptr(d_->out);
+    free_ptr(d_->cams);
+    free_ptr(d_->view_offsets);
+    free_ptr(d_->film_offsets);
     if (d_->stream) {
         cudaStreamDestroy(d_->stream);
     }
@@ -3139,13 +3259,53 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
 }
 
 int32_t Renderer::set_camera(Camera_desc const& camera) {
+    return set_views(std::vector<Camera_desc>{camera});
+}
+
+int32_t Renderer::set_views(std::vector<Camera_desc> const& views) {
     clear_graphs();
-    if (camera.width == 0 || camera.height == 0 || !(camera.fov > 0.f)) {
-        error_ = "camera needs a resolution and a field of view";
+    if (views.empty() || views.size() > Max_views) {
+        error_ = "between 1 and " + std::to_string(Max_views) + " views";
         return SPB_ERROR_ARGUMENT;
     }
-    camera_ = camera;
-    uint32_t const pixels = camera.width * camera.height;
+    std::vector<Cam>      cams(views.size());
+    std::vector<uint32_t> traced(views.size() + 1, 0), film(views.size() + 1, 0);
+    for (size_t v = 0; v < views.size(); ++v) {
+        Camera_desc const& c = views[v];
+        if (c.width == 0 || c.height == 0 || !(c.fov > 0.f) || c.width > 65536 || c.height > 65536) {
+            error_ = "camera needs a resolution and a field of view";
+            return SPB_ERROR_ARGUMENT;
+        }
+        // Perspective::on_update (camera_perspective.cpp:203-224): image plane at distance
+        // 1 / tan(fov / 2), x in [-1, 1], y in [-h/w, h/w]
+        float const ratio = float(c.height) / float(c.width);
+        float const z     = 1.f / std::tan(0.5f * c.fov);
+        Cam&        cam   = cams[v];
+        cam.left_top      = make_float3(-1.f, ratio, z);
+        cam.d_x           = make_float3(2.f / float(c.width), 0.f, 0.f);
+        cam.d_y           = make_float3(0.f, -2.f * ratio / float(c.height), 0.f);
+        cam.r0            = make_float3(c.rotation[0], c.rotation[1], c.rotation[2]);
+        cam.r1            = make_float3(c.rotation[3], c.rotation[4], c.rotation[5]);
+        cam.r2            = make_float3(c.rotation[6], c.rotation[7], c.rotation[8]);
+        cam.pos           = make_float3(c.position[0], c.position[1], c.position[2]);
+        cam.w             = c.width;
+        cam.h             = c.height;
+        uint64_t const t  = uint64_t(traced[v]) + uint64_t(c.width + 2 * Film_border) * (c.height + 2 * Film_border);
+        uint64_t const f  = uint64_t(film[v]) + uint64_t(c.width) * c.height;
+        if (t >= (1ull << 31)) {
+            error_ = "views too large";
+            return SPB_ERROR_ARGUMENT;
+        }
+        traced[v + 1] = uint32_t(t);
+        film[v + 1]   = uint32_t(f);
+    }
+    views_ = views;
+    SPB_RCUDA(upload(d_->cams, cams.data(), cams.size() * sizeof(Cam)));
+    SPB_RCUDA(upload(d_->view_offsets, traced.data(), traced.size() * sizeof(uint32_t)));
+    SPB_RCUDA(upload(d_->film_offsets, film.data(), film.size() * sizeof(uint32_t)));
+    d_->num_views     = uint32_t(views.size());
+    d_->traced_pixels = traced.back();
+    uint32_t const pixels = film.back();
     if (pixels != d_->film_pixels) {
         free_ptr(d_->film);
         free_ptr(d_->comp);
@@ -3192,6 +3352,9 @@ int32_t Renderer::ensure_buffers(uint32_t paths, uint32_t picks_per_path) {
     free_ptr(p.sh_L);
     free_ptr(p.prev_n);
     free_ptr(p.split_o);
+    free_ptr(p.sh2_o);
+    free_ptr(p.sh2_d);
+    free_ptr(p.sh2_L);
     free_ptr(p.split_m);
     free_ptr(p.pick_d);
     free_ptr(p.pick_c);
@@ -3206,6 +3369,7 @@ int32_t Renderer::ensure_buffers(uint32_t paths, uint32_t picks_per_path) {
     free_ptr(d_->queue[1]);
     free_ptr(d_->shadow_queue);
     free_ptr(d_->transmit_queue);
+    free_ptr(d_->transmit_pick_queue);
     size_t const n = paths;
     SPB_RCUDA(dev_malloc(&p.ray_o, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&p.ray_d, n * sizeof(float4)));
@@ -3221,19 +3385,23 @@ int32_t Renderer::ensure_buffers(uint32_t paths, uint32_t picks_per_path) {
     SPB_RCUDA(dev_malloc(&p.sh_o, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&p.sh_d, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&p.sh_L, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.sh2_o, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.sh2_d, n * sizeof(float4)));
+    SPB_RCUDA(dev_malloc(&p.sh2_L, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&p.prev_n, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&p.L2, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&d_->queue[0], n * sizeof(uint32_t)));
     SPB_RCUDA(dev_malloc(&d_->queue[1], n * sizeof(uint32_t)));
     // Split selections: a record per path and every light its selection can return.  Shadow
-    // rays: a path's slot and every pick.
+    // rays: a path's two slots and every pick.
     size_t const np = std::max<size_t>(size_t(n) * picks_per_path, 1);
     SPB_RCUDA(dev_malloc(&p.split_o, n * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&p.split_m, n * sizeof(uint4)));
     SPB_RCUDA(dev_malloc(&p.pick_d, np * sizeof(float4)));
     SPB_RCUDA(dev_malloc(&p.pick_c, np * sizeof(float4)));
-    SPB_RCUDA(dev_malloc(&d_->shadow_queue, (n + np) * sizeof(uint32_t)));
-    SPB_RCUDA(dev_malloc(&d_->transmit_queue, (n + np) * sizeof(uint32_t)));
+    SPB_RCUDA(dev_malloc(&d_->shadow_queue, (2 * n + np) * sizeof(uint32_t)));
+    SPB_RCUDA(dev_malloc(&d_->transmit_queue, 2 * n * sizeof(uint32_t)));
+    SPB_RCUDA(dev_malloc(&d_->transmit_pick_queue, np * sizeof(uint32_t)));
     d_->pick_capacity = uint64_t(n) * picks_per_path;
     if (!d_->counters) {
         SPB_RCUDA(dev_malloc(&d_->counters, Counter_words * sizeof(uint32_t)));
@@ -3444,7 +3612,7 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         return SPB_ERROR_ARGUMENT;
     }
     // camera samples per sample slot: the image and its filter border
-    uint32_t const pixels = (camera_.width + 2 * Film_border) * (camera_.height + 2 * Film_border);
+    uint32_t const pixels = d_->traced_pixels;
     // Wave size: k samples per pixel per wave, k = paths per wave / pixels (at least 1), the
     // paths per wave from the settings or the autotuner; buffers hold the largest candidate.
     bool const     tuning     = settings_.wave_paths == 0 || settings_.trace_blocks_per_sm == 0;
@@ -3494,18 +3662,6 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         }
     }
 
-    float const ratio = float(camera_.height) / float(camera_.width);
-    float const z     = 1.f / std::tan(0.5f * camera_.fov);
-    Cam         cam;
-    cam.left_top = make_float3(-1.f, ratio, z);
-    cam.d_x      = make_float3(2.f / float(camera_.width), 0.f, 0.f);
-    cam.d_y      = make_float3(0.f, -2.f * ratio / float(camera_.height), 0.f);
-    cam.r0       = make_float3(camera_.rotation[0], camera_.rotation[1], camera_.rotation[2]);
-    cam.r1       = make_float3(camera_.rotation[3], camera_.rotation[4], camera_.rotation[5]);
-    cam.r2       = make_float3(camera_.rotation[6], camera_.rotation[7], camera_.rotation[8]);
-    cam.pos      = make_float3(camera_.position[0], camera_.position[1], camera_.position[2]);
-    cam.w        = camera_.width;
-    cam.h        = camera_.height;
 
     Scene_gpu sg;
     sg.nodes         = d_->nodes;
@@ -3578,9 +3734,8 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     auto const enqueue_wave = [&](uint32_t k, uint32_t paths, uint32_t trace_grid, bool training, bool capture,
                                   uint32_t& iterations, size_t& events) -> int32_t {
         SPB_RCUDA(cudaMemsetAsync(ctr, 0, Counter_words * sizeof(uint32_t), st));
-        // k_transmit loops over its queue: at most a slot and every pick per path
-        uint32_t const transmit_grid = uint32_t(std::min<uint64_t>(
-            (uint64_t(paths) * (1 + picks_per_path) + Trace_block - 1) / Trace_block, uint64_t(32) * d_->sms));
+        // k_transmit: one thread per shadow slot (at most two per path)
+        uint32_t const transmit_grid = (2 * paths + Trace_block - 1) / Trace_block;
         k_generate<<<(paths + 255) / 256, 256, 0, st>>>(d_->launch_dev, d_->paths, d_->queue[0], ctr, paths);
         iterations = 0;
         for (uint32_t b = 0; b < max_iterations; ++b) {
@@ -3613,16 +3768,33 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             k_shade<<<(paths + Shade_block - 1) / Shade_block, Shade_block, 0, st>>>(
                 sg, d_->launch_dev, d_->paths, q_in, c,
                 Shade_out{q_out, c + Counter_stride, d_->shadow_queue, c + 1, c + 5, c + 6});
-            if (d_->has_media && d_->instanced) {
-                k_trace<true, true, true><<<trace_grid, Trace_block, 0, st>>>(
-                    sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot, d_->transmit_queue, c + 4);
-                k_transmit<true><<<transmit_grid, Trace_block, 0, st>>>(
-                    sg, d_->paths, d_->transmit_queue, c + 4, ctr + Overflow_slot);
-            } else if (d_->has_media) {
-                k_trace<true, true><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->shadow_queue, c + 1, c + 3,
-                                                                       ctr + Overflow_slot, d_->transmit_queue, c + 4);
-                k_transmit<false><<<transmit_grid, Trace_block, 0, st>>>(
-                    sg, d_->paths, d_->transmit_queue, c + 4, ctr + Overflow_slot);
+            if (d_->has_media) {
+                Transmit_out const tq{d_->transmit_queue, c + 4, c + 8, 2 * paths, d_->transmit_pick_queue, c + 7};
+                if (d_->instanced) {
+                    k_trace<true, true, true><<<trace_grid, Trace_block, 0, st>>>(
+                        sg, d_->paths, d_->shadow_queue, c + 1, c + 3, ctr + Overflow_slot, tq);
+                    k_transmit<true><<<transmit_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->transmit_queue, c + 4,
+                                                                            c + 8, 2 * paths, ctr + Overflow_slot);
+                } else {
+                    k_trace<true, true><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->shadow_queue, c + 1,
+                                                                           c + 3, ctr + Overflow_slot, tq);
+                    k_transmit<false><<<transmit_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->transmit_queue, c + 4,
+                                                                             c + 8, 2 * paths, ctr + Overflow_slot);
+                }
+                if (picks_per_path != 0) {
+                    // picks through media, one thread each: their number sets the grid (waves
+                    // with media read counters on the host and are never captured)
+                    SPB_RCUDA(cudaMemcpyAsync(d_->pinned_count, c + 7, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+                    SPB_RCUDA(cudaStreamSynchronize(st));
+                    uint32_t const picked = *d_->pinned_count;
+                    if (picked != 0 && d_->instanced) {
+                        k_transmit_picks<true><<<(picked + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
+                            sg, d_->paths, d_->transmit_pick_queue, c + 7, ctr + Overflow_slot);
+                    } else if (picked != 0) {
+                        k_transmit_picks<false><<<(picked + Trace_block - 1) / Trace_block, Trace_block, 0, st>>>(
+                            sg, d_->paths, d_->transmit_pick_queue, c + 7, ctr + Overflow_slot);
+                    }
+                }
             } else if (d_->instanced) {
                 k_trace<true, false, true><<<trace_grid, Trace_block, 0, st>>>(sg, d_->paths, d_->shadow_queue, c + 1,
                                                                               c + 3, ctr + Overflow_slot);
@@ -3641,8 +3813,8 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
             }
             SPB_RCUDA(record(guide_event(events++), capture));
         }
-        k_gather<<<(camera_.width * camera_.height + 255) / 256, 256, 0, st>>>(d_->paths, camera_.width,
-                                                                              camera_.height, k, d_->film, d_->comp);
+        k_gather<<<(d_->film_pixels + 255) / 256, 256, 0, st>>>(d_->paths, d_->launch_dev, d_->film_pixels, k,
+                                                                d_->film, d_->comp);
         SPB_RCUDA(cudaGetLastError());
         return SPB_OK;
     };
@@ -3680,8 +3852,12 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         wave.golden_n       = golden_n;
         wave.golden_sorted  = d_->golden_sorted;
         // The previous wave has completed (synchronized below), so the pinned block is free.
-        d_->launch_host->cam  = cam;
-        d_->launch_host->wave = wave;
+        d_->launch_host->cams         = d_->cams;
+        d_->launch_host->view_offsets = d_->view_offsets;
+        d_->launch_host->film_offsets = d_->film_offsets;
+        d_->launch_host->num_views    = d_->num_views;
+        d_->launch_host->pixels       = pixels;
+        d_->launch_host->wave         = wave;
         if (measured) {
             SPB_RCUDA(cudaEventRecord(d_->wave_ev[0], st));
         }

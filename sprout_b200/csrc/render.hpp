@@ -77,6 +77,8 @@ struct Scene_desc {
     int                             instancing = -1;
 };
 
+constexpr uint32_t Max_views = 4096;
+
 struct Camera_desc {
     uint32_t width  = 0;
     uint32_t height = 0;
@@ -147,6 +149,10 @@ class Renderer {
 
     int32_t set_scene(Scene_desc const& scene, uint32_t num_threads);
     int32_t set_camera(Camera_desc const& camera);
+    // Several views rendered together: a render call traces every view's pixels in the same
+    // waves (the same samples per pixel), and resolve() returns their images one after another
+    // (view 0's width x height pixels first).  set_camera is the one-view case.
+    int32_t set_views(std::vector<Camera_desc> const& views);
     void    set_settings(Settings const& s) { settings_ = s; }
 
     // Clears the film (start of a frame).
@@ -156,7 +162,8 @@ class Renderer {
     // frame; sample i of a pixel always uses the same random stream.
     int32_t render(uint32_t first_sample, uint32_t num_samples);
 
-    // Film resolve: rgb / weight per pixel (ACEScg linear), alpha 1, into host rgba floats.
+    // Film resolve: rgb / weight per pixel (ACEScg linear), alpha 1, into host rgba floats
+    // (the views' images one after another).
     int32_t resolve(float* rgba);
 
     Stats const& stats() const { return stats_; }
@@ -169,7 +176,7 @@ class Renderer {
     struct Device;
     Device*     d_ = nullptr;
     Settings    settings_;
-    Camera_desc camera_;
+    std::vector<Camera_desc> views_;
     Stats       stats_;
     uint32_t    instances_        = 0;  // of the uploaded scene (Stats::instances)
     uint64_t    device_triangles_ = 0;

@@ -133,12 +133,14 @@ VOLUME_CONFIG = ("2 m cube of 256^3 fBm density (5 octaves, seed 4), mu_t 20 per
                  "RGB delta/ratio tracking (the reference's transport; no hero wavelengths)")
 
 
-def measure_volume(views=4, spp=128, cpu_reference=False):
+def measure_volume(views=4, spp=128, cpu_reference=False, batch=True):
     """The heterogeneous-volume workload: the first `views` of scenes.volume_views() (seeded
     camera positions, image sides U[256, 1024]) of one scene, built and uploaded once; each
     view moves the camera and sets its resolution, then renders one frame.  Samples/s over the
     device time of all views; the end-to-end rate includes, per view, su_render_frame +
-    su_postprocess + framebuffer copy, and the scene's one-time upload."""
+    su_postprocess + framebuffer copy, and the scene's one-time upload.  With batch, the same
+    views are also rendered together in one spb_render_views call (after one untimed call),
+    timed on the device and end to end (the call, with every view's image copied to the host)."""
     lib = _lib.load()
     stats = _lib.RenderStats()
     density = scenes.fbm_density(256)
@@ -161,6 +163,20 @@ def measure_volume(views=4, spp=128, cpu_reference=False):
             seconds += stats.device_seconds
             samples += side * side * spp
             rays += stats.extension_rays + stats.shadow_rays
+        if batch:
+            cams = [(side, side, scenes.VOLUME_FOV, scenes._look_at(position)) for position, side in chosen]
+            su.render_views(cams, spp)  # warm-up: the autotuner's probes
+            t0 = time.perf_counter()
+            su.render_views(cams, spp)
+            batch_wall = time.perf_counter() - t0
+            assert lib.spb_render_last_stats(ctypes.byref(stats)) == 0
+            batch_out = {"msamples_s": round(samples / stats.device_seconds / 1e6, 3),
+                         "mrays_s": round((stats.extension_rays + stats.shadow_rays) / stats.device_seconds / 1e6, 3),
+                         "device_seconds": round(stats.device_seconds, 3),
+                         "e2e_msamples_s": round(samples / batch_wall / 1e6, 3),
+                         "wave_paths": stats.wave_paths,
+                         "note": f"all {views} views in one spb_render_views call: their paths share the waves; "
+                                 "e2e = the call, every view's image copied to the host"}
     finally:
         su.su_release()
     out = {"workload": "volume", "config": f"{VOLUME_CONFIG}, {views} of 64 views (sides "
@@ -170,6 +186,8 @@ def measure_volume(views=4, spp=128, cpu_reference=False):
            "e2e_msamples_s": round(samples / wall / 1e6, 3),
            "e2e_note": "per view: camera move + su_render_frame + su_postprocess + su_copy_framebuffer to "
                        "host, wall clock (the scene's one-time upload and majorant build in the first view)"}
+    if batch:
+        out["batch"] = batch_out
     if cpu_reference:
         import oracle  # test/baseline infrastructure: times the reference renderer
 

@@ -468,6 +468,8 @@ def builtin_shapes(su, width: int = 64, height: int = 48, spp: int = 64, environ
 # mu_t = -ln(0.5) / 0.034657 = 20 per metre at density 1; subsurface colour 0.32297 gives a
 # single-scattering albedo of 0.9 at anisotropy 0.6 through the reference's scattering()
 # mapping (collision_coefficients.inl:50-71).
+VOLUME_FOV = math.radians(40.0)  # horizontal field of view of the volume views
+
 VOLUME_MEDIUM = {"attenuation_color": [0.5, 0.5, 0.5], "attenuation_distance": 0.0346574,
                  "subsurface_color": [0.322972, 0.322972, 0.322972], "anisotropy": 0.6}
 
@@ -524,7 +526,7 @@ def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -
     Sphere light of radius 0.25 (radiance 60) and a uniform Infinite_sphere environment; a
     pinhole camera at `position` looking at the centre with a 40 degree field of view; PTMIS
     with max depth 32.  integrator: further PTMIS keys (e.g. this renderer's "instancing")."""
-    cam = su.su_create_camera_perspective(width, height, math.radians(40.0))
+    cam = su.su_create_camera_perspective(width, height, VOLUME_FOV)
     su.set_transformation(cam, _look_at(position))
     ptmis = {"min_bounces": min_bounces, "max_bounces": max_bounces}
     ptmis.update(integrator or {})

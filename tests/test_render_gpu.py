@@ -318,3 +318,40 @@ def test_take_postprocessors_and_exporters(tmp_path, monkeypatch):
     assert np.allclose(aces, want, rtol=1e-3, atol=1e-5)
     frame(export={"Image": {"format": "RGBE"}})
     assert (tmp_path / "output_000000.hdr").read_bytes().startswith(b"#?RADIANCE")
+
+
+def test_views_render_together_as_alone():
+    """spb_render_views: three views of different sizes and positions rendered in one call.  A
+    view's sample streams depend on its own pixels only, so each traces the paths it traces when
+    rendered alone through su_render_frame; only the order in which the film sums the samples
+    differs (the waves group them differently), so the images agree to float rounding."""
+    import math
+
+    views = [(64, 48, scenes.translation(0.0, 1.0, -3.4)),
+             (40, 40, scenes.translation(0.3, 0.9, -3.0)),
+             (96, 24, scenes.translation(-0.2, 1.2, -3.6))]
+    fov = math.radians(40.0)
+    su = capi.SuLibrary()
+    assert su.su_init(False) == 0
+    try:
+        cam = scenes.cornell(su, 64, 48, sphere_subdivisions=3, spp=16)
+        assert su.su_render_frame(0) == 0, su.messages  # uploads the scene
+        batch = su.render_views([(w, h, fov, m) for w, h, m in views], 16)
+        st = _lib.RenderStats()
+        assert _lib.load().spb_render_last_stats(ctypes.byref(st)) == 0
+        assert st.paths == 16 * sum((w + 2) * (h + 2) for w, h, _ in views)
+        alone = []
+        for w, h, m in views:
+            assert su.su_camera_set_resolution(w, h) == 0
+            su.set_transformation(cam, m)
+            assert su.su_render_frame(0) == 0, su.messages
+            assert su.su_postprocess() == 0
+            img, status = su.framebuffer(w, h)
+            assert status == 0
+            alone.append(img.copy())
+    finally:
+        su.su_release()
+    for (w, h, _), b, a in zip(views, batch, alone):
+        assert b.shape == (h, w, 4) and np.all(np.isfinite(b))
+        assert a[:, :, :3].mean() > 0.05
+        np.testing.assert_allclose(b[:, :, :3], a[:, :, :3], rtol=1e-4, atol=1e-6)
