@@ -51,6 +51,11 @@ def _load():
         lib.oracle_synth_rays.restype = ctypes.c_int32
         lib.oracle_synth_rays.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_float,
                                           ctypes.c_void_p, ctypes.c_uint32]
+        lib.oracle_spectral_render.restype = ctypes.c_int32
+        lib.oracle_spectral_render.argtypes = (
+            [ctypes.c_uint32] + [ctypes.c_void_p] * 4 + [ctypes.c_uint32] * 3 + [ctypes.c_void_p] * 3 +
+            [ctypes.c_int32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p] +
+            [ctypes.c_uint32] * 3 + [ctypes.c_uint64] + [ctypes.c_void_p] * 4)
         _lib = lib
     return _lib
 
@@ -333,3 +338,70 @@ def reference_render(build_scene, width, height, iterations, progressive=True, w
         timing = json.loads(res.stdout.strip().splitlines()[-1])
         img = np.fromfile(op, np.float32).reshape(height, width, 4)
     return img[:, :, :3].copy(), timing
+
+
+# ---- the spectral mode's image (spectral_oracle.c) ----
+
+SRGB_TO_AP1 = np.array([[0.61309732, 0.33952285, 0.04737928],
+                        [0.07019422, 0.91635557, 0.01345259],
+                        [0.02061560, 0.10956983, 0.86981512]])
+
+
+def volumetric_coefficients(attenuation_color, attenuation_distance, subsurface_color, anisotropy):
+    """(mu_a, mu_s) in ACEScg of a Volumetric material as su_create_material reads it: colours
+    converted from sRGB, then the reference's attenuation() and scattering() mappings
+    (collision_coefficients.inl:50-71; the library's capi.cpp restates them the same way)."""
+    ac = SRGB_TO_AP1 @ np.asarray(attenuation_color, np.float64)
+    ssc = SRGB_TO_AP1 @ np.asarray(subsurface_color, np.float64)
+    g = float(np.clip(anisotropy, -0.999, 0.999))
+    mu_t = -np.log(np.clip(ac, 0.01, 0.991102)) / attenuation_distance
+    root = np.sqrt(9.59217 + 41.6808 * ssc + 17.7126 * ssc * ssc)
+    factor = np.clip(4.097125 + 4.20863 * ssc - root, 0.0, 1.0)
+    pss = (1.0 - factor * factor) / (1.0 - g * factor * factor)
+    mu_a = mu_t * (1.0 - pss)
+    return mu_a, mu_t - mu_a
+
+
+def spectral_render(scene, spp, seed=1, runs=None):
+    """The FP64 image (height, width, 3) of a scene described as sprout_b200.scenes.spectral_box
+    returns it: `runs` independent renders of spp / runs samples per pixel on parallel threads,
+    averaged."""
+    import concurrent.futures
+    import os
+
+    lib = _load()
+    tris = np.ascontiguousarray(scene["triangles"], np.float64)
+    roles = np.ascontiguousarray(scene["roles"], np.int32)  # 0 lamp, 1 medium boundary
+    mu_a, mu_s = volumetric_coefficients(**scene["medium"])
+    g = float(np.clip(scene["medium"]["anisotropy"], -0.999, 0.999))
+    emission = SRGB_TO_AP1 @ np.asarray(scene["emission"], np.float64)
+    mats = np.ascontiguousarray(np.array([list(emission) + [0.0] * 5,
+                                          list(mu_a) + list(mu_s) + [g, 1.0]], np.float64))
+    types = np.array([0, 1], np.int32)
+    density = np.ascontiguousarray(scene["density"], np.float64)
+    nz, ny, nx = density.shape
+    w2uvw = np.ascontiguousarray(scene["world_to_uvw"], np.float64)
+    env = np.ascontiguousarray(SRGB_TO_AP1 @ np.asarray(scene["environment"], np.float64))
+    cam = scene["camera"]
+    m = np.asarray(cam["matrix"], np.float64)
+    rot = np.ascontiguousarray(m[:3, :3] / np.linalg.norm(m[:3, :3], axis=1, keepdims=True))
+    pos = np.ascontiguousarray(m[3, :3])
+    w, h = cam["width"], cam["height"]
+    runs = runs or max(1, min(os.cpu_count() or 1, spp))
+    per = max(1, spp // runs)
+
+    def one(k):
+        out = np.zeros((h, w, 3), np.float64)
+        weight = np.zeros((h, w), np.float64)
+        light_tri = np.zeros(len(tris), np.uint32)
+        light_cdf = np.zeros(len(tris), np.float64)
+        lib.oracle_spectral_render(len(tris), tris.ctypes.data, roles.ctypes.data, types.ctypes.data,
+                                   mats.ctypes.data, nx, ny, nz, density.ctypes.data, w2uvw.ctypes.data,
+                                   env.ctypes.data, 1, w, h, float(cam["fov"]), rot.ctypes.data, pos.ctypes.data,
+                                   per, scene["min_bounces"], scene["max_bounces"], seed * 7919 + k,
+                                   light_tri.ctypes.data, light_cdf.ctypes.data, out.ctypes.data, weight.ctypes.data)
+        return out
+
+    with concurrent.futures.ThreadPoolExecutor(runs) as ex:
+        images = list(ex.map(one, range(runs)))
+    return np.mean(images, axis=0)

@@ -26,7 +26,8 @@ SOURCES = ["common.cpp", "synth.cpp", "bvh8.cpp", "ggx_table.cpp", "light_tree.c
            "cast.cu",
            "guide.cu", "render.cu", "capi.cpp"]
 HEADERS = ["common.hpp", "bvh8.hpp", "traverse.cuh", "material.cuh", "render.hpp", "json.hpp", "ggx_table.hpp",
-           "light_tree.hpp", "guide.cuh", "guide_mlp.cuh", "guide.hpp", "tuner.hpp", "postprocess.hpp", "image_io.hpp"]
+           "light_tree.hpp", "guide.cuh", "guide_mlp.cuh", "guide.hpp", "tuner.hpp", "postprocess.hpp", "image_io.hpp",
+           "spectral.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -74,7 +75,7 @@ def build_library(force: bool = False, verbose: bool = False, ptxas_info: bool =
 
 def build_oracle(force: bool = False, verbose: bool = False) -> pathlib.Path:
     """Compile the CPU restatement; also the reference build when its sources are here."""
-    srcs = [ORACLE / "cast_oracle.c", ORACLE / "synth_oracle.c"]
+    srcs = [ORACLE / "cast_oracle.c", ORACLE / "synth_oracle.c", ORACLE / "spectral_oracle.c"]
     if force or _stale(ORACLE_LIB, srcs):
         cmd = ["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-pthread"] + [str(s) for s in srcs] + [
                "-o", str(ORACLE_LIB), "-lm"]

@@ -1350,6 +1350,9 @@ SU_LIBRARY_API int32_t su_create_integrators(char const* string) {
                     s.split_threshold = t * t * t * t;
                 }
             }
+            // "spectral": hero-wavelength spectral transport (this renderer's extension; scenes of
+            // participating media, emitters and the environment)
+            s.spectral = spb::json::bool_or(pt->find("spectral"), false);
             // "seed": the sample streams' seed (this renderer's extension, default 0), for
             // statistically independent renders of one scene
             s.seed = uint32_t(spb::json::number_or(pt->find("seed"), s.seed));

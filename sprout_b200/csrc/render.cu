@@ -37,6 +37,7 @@
 #include "guide_mlp.cuh"
 #include "light_tree.hpp"
 #include "render.hpp"
+#include "spectral.cuh"
 #include "tuner.hpp"
 #include "traverse.cuh"
 
@@ -2408,6 +2409,419 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// ---- hero-wavelength spectral transport (spectral.cuh): one persistent launch ----
+// The renderer's spectral mode, for scenes of participating media, emitters and the
+// environment (the many-view volume workload): each thread takes (view, pixel, sample) work
+// items from a counter and traces the whole path carrying Hero_count wavelengths; every RGB
+// quantity (emission, medium coefficients) is upsampled at them.  Tracking is the RGB
+// renderer's spectral-MIS delta tracking over the carried wavelengths (majorants from the RGB
+// coefficients, which bound every upsampled value since the basis is a partition of unity);
+// light selection picks one light (no splitting); shadow rays walk their medium crossings
+// with ratio tracking and are blocked by any other triangle.  Each sample's radiance is read
+// out to ACEScg (c_spec_resp) and splatted with the film filter into its view's film with
+// atomics (so the film's summation order, unlike the wavefront renderer's, is not fixed).
+namespace spec = spb::spectral;
+constexpr int Spec_table = 341;  // readout at 1 nm steps over [Lambda_min, Lambda_max]
+__constant__ float c_spec_resp[3 * Spec_table];
+
+// The sample's film colour: sum over the carried wavelengths of radiance times the readout
+// (which includes the round-trip correction and Lambda_span / Hero_count).
+__device__ __forceinline__ V3 spec_readout(spec::V4 L, spec::V4 lambdas) {
+    V3 acc = v3(0.f, 0.f, 0.f);
+    for (int k = 0; k < spec::Hero_count; ++k) {
+        float const x = lambdas.v[k] - spec::Lambda_min;
+        int const   i = min(max(int(x), 0), Spec_table - 2);
+        float const f = x - float(i);
+        acc.x += L.v[k] * ((1.f - f) * c_spec_resp[3 * i] + f * c_spec_resp[3 * i + 3]);
+        acc.y += L.v[k] * ((1.f - f) * c_spec_resp[3 * i + 1] + f * c_spec_resp[3 * i + 4]);
+        acc.z += L.v[k] * ((1.f - f) * c_spec_resp[3 * i + 2] + f * c_spec_resp[3 * i + 5]);
+    }
+    return acc;
+}
+
+__device__ __forceinline__ spec::V4 spec_of(V3 c, spec::V4 lambdas) {
+    return spec::upsample(c.x, c.y, c.z, lambdas);
+}
+
+__device__ __forceinline__ bool spec_below_abort(spec::V4 w) {
+    return spec::maximum(w) < Abort_epsilon;
+}
+
+// Delta tracking with spectral MIS in a homogeneous medium (track_homogeneous over the
+// carried wavelengths).
+__device__ bool spec_track_homogeneous(spec::V4 mu_a, spec::V4 mu_s, float t, float d, Rng& rng, float& t_out,
+                                       spec::V4& lw, uint32_t* capped) {
+    spec::V4 const mu_t = spec::add(mu_a, mu_s);
+    float const    mt   = spec::maximum(mu_t);
+    lw                  = spec::splat(1.f);
+    if (!(mt > 1e-10f)) {
+        return false;
+    }
+    float const imt  = 1.f / mt;
+    spec::V4    mu_n = spec::add(spec::splat(mt), spec::scale(-1.f, mu_t));
+    for (int step = 0; step < Max_tracking_steps; ++step) {
+        t -= logf(1.f - rng.uniform()) * imt;
+        if (t > d) {
+            return false;
+        }
+        float const ms = spec::average(spec::mul(mu_s, lw));
+        float const mn = spec::average(spec::mul(mu_n, lw));
+        float const mc = ms + mn;
+        if (mc < 1e-10f) {
+            return false;
+        }
+        float const ps = ms / mc;
+        float const pn = mn / mc;
+        if ((rng.uniform() <= 1.f - pn) & (ps > 0.f)) {
+            lw    = spec::mul(lw, spec::scale(1.f / (mt * ps), mu_s));
+            t_out = t;
+            return true;
+        }
+        lw = spec::mul(lw, spec::scale(1.f / (mt * pn), mu_n));
+    }
+    atomicAdd(capped, 1u);
+    return false;
+}
+
+// Delta tracking with spectral MIS through a density grid (track_grid over the carried
+// wavelengths); maj_t bounds the coefficients at density 1 for every wavelength.
+__device__ bool spec_track_grid(Medium_gpu const& g, float maj_t, spec::V4 mu_a, spec::V4 mu_s, V3 ro, V3 rd,
+                                float t0, float t1, Rng& rng, float& t_out, spec::V4& lw, uint32_t* capped) {
+    V3 const o     = to_texture(g, ro);
+    V3 const d     = to_texture_dir(g, rd);
+    lw             = spec::splat(1.f);
+    int  steps     = 0;
+    bool scattered = false;
+    walk_cells(g, o, d, t0, t1, [&](float2 cell, float ta, float tb) {
+        float const mt = cell.y * maj_t;
+        if (mt < Min_mt) {
+            return false;
+        }
+        float const imt = 1.f / mt;
+        for (float t = ta; steps < Max_tracking_steps; ++steps) {
+            t -= logf(1.f - rng.uniform()) * imt;
+            if (t > tb) {
+                return false;
+            }
+            float const    den  = sample_density(g, o + t * d);
+            spec::V4 const ms3  = spec::scale(den, mu_s);
+            spec::V4 const mu_n = spec::add(spec::splat(mt), spec::scale(-den, spec::add(mu_a, mu_s)));
+            float const    ms   = spec::average(spec::mul(ms3, lw));
+            float const    mn   = spec::average(spec::mul(mu_n, lw));
+            float const    sum  = ms + mn;
+            if (!(sum > 0.f)) {
+                lw = spec::splat(0.f);
+                return true;
+            }
+            float const ps = ms / sum;
+            float const pn = mn / sum;
+            if ((rng.uniform() <= 1.f - pn) & (ps > 0.f)) {
+                lw        = spec::mul(lw, spec::scale(1.f / (mt * ps), ms3));
+                t_out     = t;
+                scattered = true;
+                return true;
+            }
+            lw = spec::mul(lw, spec::scale(1.f / (mt * pn), mu_n));
+        }
+        return true;
+    });
+    if (steps >= Max_tracking_steps) {
+        atomicAdd(capped, 1u);
+    }
+    return scattered;
+}
+
+// Ratio tracking through a density grid (transmit_grid over the carried wavelengths): w is
+// multiplied by the estimate; false when it falls below Abort_epsilon.
+__device__ bool spec_transmit_grid(Medium_gpu const& g, float maj_t, float min_t, spec::V4 mu_t, V3 ro, V3 rd,
+                                   float t0, float t1, Rng& rng, spec::V4& w, uint32_t* capped) {
+    V3 const o       = to_texture(g, ro);
+    V3 const d       = to_texture_dir(g, rd);
+    int      steps   = 0;
+    bool     blocked = false;
+    walk_cells(g, o, d, t0, t1, [&](float2 cell, float ta, float tb) {
+        float const mt = cell.y * maj_t;
+        if (mt < Min_mt) {
+            return false;
+        }
+        float const cm = fmaxf(cell.x * min_t, 0.f);
+        if (cm > 0.f) {
+            w = spec::scale(expf(-(tb - ta) * cm), w);
+            if (spec_below_abort(w)) {
+                blocked = true;
+                return true;
+            }
+        }
+        float const mr = mt - cm;
+        if (mr < Min_mt) {
+            return false;
+        }
+        float const imr = 1.f / mr;
+        for (float t = ta; steps < Max_tracking_steps; ++steps) {
+            t -= logf(1.f - rng.uniform()) * imr;
+            if (t > tb) {
+                return false;
+            }
+            float const den = sample_density(g, o + t * d);
+            for (int k = 0; k < spec::Hero_count; ++k) {
+                w.v[k] *= (mr - (den * mu_t.v[k] - cm)) * imr;
+            }
+            if (spec_below_abort(w)) {
+                blocked = true;
+                return true;
+            }
+        }
+        return false;
+    });
+    if (steps >= Max_tracking_steps) {
+        atomicAdd(capped, 1u);
+    }
+    return !blocked;
+}
+
+// The medium coefficients of material index + 1 `medium` at the carried wavelengths, with the
+// similarity-relation scale of scattering at depth (shading::similarity_relation_scale).
+struct Spec_medium {
+    spec::V4 mu_a, mu_s;
+    float    maj_t, min_t;  // bounds of mu_t at density 1 over every wavelength
+};
+
+__device__ __forceinline__ Spec_medium spec_medium(shading::Material const& m, uint32_t depth, spec::V4 lambdas) {
+    float const srs = shading::similarity_relation_scale(m.g, depth);
+    V3 const    ms  = srs * m.mu_s;
+    Spec_medium r;
+    r.mu_a  = spec_of(m.mu_a, lambdas);
+    r.mu_s  = spec_of(ms, lambdas);
+    r.maj_t = shading::max_component(m.mu_a) + shading::max_component(ms);
+    r.min_t = shading::min_component(m.mu_a) + shading::min_component(ms);
+    return r;
+}
+
+// Transmittance of a shadow ray from o along d up to dist, starting inside `medium`: medium
+// boundaries are crossed, any other triangle blocks it.
+__device__ bool spec_transmit(Scene_gpu const& s, V3 o, V3 d, float dist, uint32_t medium, uint32_t depth,
+                              spec::V4 lambdas, Rng& rng, uint2* stack, uint32_t* overflow, spec::V4& tr) {
+    tr       = spec::splat(1.f);
+    float t0 = 0.f;
+    for (int crossing = 0; crossing < 64; ++crossing) {
+        gpu::Ray_state r;
+        gpu::Traversal tv;
+        gpu::start_ray(r, tv, make_float4(o.x, o.y, o.z, t0), make_float4(d.x, d.y, d.z, dist));
+        while (!gpu::traversal_step<false>(r, tv, stack, s.nodes, s.tris, s.hit_margin, overflow)) {
+        }
+        bool const  hit = r.best_id != gpu::Miss;
+        float const end = hit ? r.tbest : dist;
+        if (medium != 0) {
+            shading::Material const m  = s.materials[medium - 1];
+            Spec_medium const       sm = spec_medium(m, depth, lambdas);
+            if (m.medium != 0) {
+                if (!spec_transmit_grid(s.media[m.medium - 1], sm.maj_t, sm.min_t, spec::add(sm.mu_a, sm.mu_s), o, d,
+                                        t0, end, rng, tr, s.tracking_capped)) {
+                    return false;
+                }
+            } else {
+                float const len = fmaxf(end - t0, 0.f);
+                for (int k = 0; k < spec::Hero_count; ++k) {
+                    tr.v[k] *= expf(-len * (sm.mu_a.v[k] + sm.mu_s.v[k]));
+                }
+            }
+        }
+        if (!hit) {
+            return true;
+        }
+        World_tri const wt = world_triangle(s, 0u, r.best_id);
+        if (s.materials[wt.material].type != shading::Type_volume) {
+            return false;
+        }
+        V3 const geo = shading::cross(wt.b - wt.a, wt.c - wt.a);
+        medium       = shading::dot(geo, d) < 0.f ? wt.material + 1 : 0;
+        t0           = offset_f(r.tbest);
+        if (t0 >= dist) {
+            return true;
+        }
+    }
+    return true;
+}
+
+// Adds a sample's colour to the film pixels its filter footprint covers (the splat form of
+// k_gather's gather: a sample of bordered pixel (sx, sy) at offset uv adds weight
+// f(u - 0.5 - dx) f(v - 0.5 - dy) to film pixel (sx + dx, sy + dy)).
+__device__ __forceinline__ void spec_splat(float4* film, uint32_t film_base, int w, int h, int sx, int sy, float u,
+                                           float v, V3 c) {
+    for (int dy = -1; dy <= 1; ++dy) {
+        int const fy = sy + dy;
+        if (fy < 0 || fy >= h) {
+            continue;
+        }
+        float const wy = filter_weight(v - 0.5f - float(dy));
+        for (int dx = -1; dx <= 1; ++dx) {
+            int const fx = sx + dx;
+            if (fx < 0 || fx >= w) {
+                continue;
+            }
+            float const  wt  = wy * filter_weight(u - 0.5f - float(dx));
+            float* const dst = reinterpret_cast<float*>(film + film_base + uint32_t(fy) * uint32_t(w) + uint32_t(fx));
+            atomicAdd(dst + 0, wt * c.x);
+            atomicAdd(dst + 1, wt * c.y);
+            atomicAdd(dst + 2, wt * c.z);
+            atomicAdd(dst + 3, wt);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(Trace_block)
+    k_spectral(Scene_gpu s, Launch const* __restrict__ launch, uint64_t total, unsigned long long* next, float4* film,
+               uint32_t* overflow, unsigned long long* counts) {
+    Wave const     wave   = launch->wave;
+    uint32_t const pixels = launch->pixels;
+    uint2          stack[gpu::Stack_size];
+    unsigned long long segments = 0, shadows = 0;
+    for (;;) {
+        unsigned long long const item = atomicAdd(next, 1ull);
+        if (item >= total) {
+            break;
+        }
+        uint32_t const pixel       = uint32_t(item % pixels);
+        uint32_t const slot        = uint32_t(item / pixels);
+        uint32_t const view        = view_of(launch->view_offsets, launch->num_views, pixel);
+        Cam const      cam         = launch->cams[view];
+        uint32_t const local       = pixel - launch->view_offsets[view];
+        uint32_t const view_pixels = launch->view_offsets[view + 1] - launch->view_offsets[view];
+        uint32_t const bw          = cam.w + 2 * Film_border;
+        int const      px          = int(local % bw) - Film_border;
+        int const      py          = int(local / bw) - Film_border;
+        Rng            rng;
+        rng.start(wave.seed, uint64_t(local) + uint64_t(wave.first_sample + slot) * view_pixels);
+        float const u  = rng.uniform();
+        float const v  = rng.uniform();
+        float const cx = float(px) + u;
+        float const cy = float(py) + v;
+        V3          d  = v3(cam.left_top.x + cx * cam.d_x.x + cy * cam.d_y.x, cam.left_top.y + cx * cam.d_x.y + cy * cam.d_y.y,
+                            cam.left_top.z + cx * cam.d_x.z + cy * cam.d_y.z);
+        d              = shading::normalize(d);
+        d = v3(d.x * cam.r0.x + d.y * cam.r1.x + d.z * cam.r2.x, d.x * cam.r0.y + d.y * cam.r1.y + d.z * cam.r2.y,
+               d.x * cam.r0.z + d.y * cam.r1.z + d.z * cam.r2.z);
+        spec::V4 const lambdas = spec::wavelengths(rng.uniform());
+        spec::V4       T       = spec::splat(1.f);
+        spec::V4       L       = spec::splat(0.f);
+        V3             o       = v3(cam.pos.x, cam.pos.y, cam.pos.z);
+        float          tmin    = 0.f;
+        uint32_t       medium  = 0;
+        uint32_t       depth   = 0;
+        bool           camera  = true;  // no scattering vertex yet
+        float          pdf_prev = 0.f;  // phase pdf of the last continuation
+        V3             prev_p   = o;    // its vertex
+        for (int seg = 0; seg < 1024; ++seg) {
+            ++segments;
+            gpu::Ray_state r;
+            gpu::Traversal tv;
+            gpu::start_ray(r, tv, make_float4(o.x, o.y, o.z, tmin), make_float4(d.x, d.y, d.z, Ray_max_t));
+            while (!gpu::traversal_step<false>(r, tv, stack, s.nodes, s.tris, s.hit_margin, overflow)) {
+            }
+            bool const  hit   = r.best_id != gpu::Miss;
+            float const t_hit = hit ? r.tbest : Ray_max_t;
+            bool        scattered = false;
+            float       t_sc      = 0.f;
+            if (medium != 0) {
+                shading::Material const m  = s.materials[medium - 1];
+                Spec_medium const       sm = spec_medium(m, depth, lambdas);
+                spec::V4                lw;
+                scattered = m.medium != 0 ? spec_track_grid(s.media[m.medium - 1], sm.maj_t, sm.mu_a, sm.mu_s, o, d,
+                                                             tmin, t_hit, rng, t_sc, lw, s.tracking_capped)
+                                          : spec_track_homogeneous(sm.mu_a, sm.mu_s, tmin, t_hit, rng, t_sc, lw,
+                                                                   s.tracking_capped);
+                T = spec::mul(T, lw);
+                if (spec_below_abort(lw)) {
+                    break;
+                }
+            }
+            if (scattered) {
+                // A scattering vertex in the medium (HG phase function).
+                if (depth >= wave.max_bounces) {
+                    break;
+                }
+                if (depth >= wave.min_bounces) {
+                    float const q = spec::maximum(T);
+                    if (rng.uniform() > q) {
+                        break;
+                    }
+                    T = spec::scale(1.f / q, T);
+                }
+                shading::Material const m   = s.materials[medium - 1];
+                float const             g   = shading::van_de_hulst_anisotropy(m.g, depth);
+                V3 const                pos = o + t_sc * d;
+                V3 const                wo  = -d;
+                float const             select = rng.uniform();
+                float const             r1     = rng.uniform();
+                float const             r2     = rng.uniform();
+                Light_pick              pick[1];
+                if (select_lights(s, pos, v3(0.f, 0.f, 1.f), true, select, false, pick) == 1) {
+                    Light_sample ls;
+                    if (sample_light(s, pos, v3(0.f, 0.f, 1.f), true, pick[0], r1, r2, ls)) {
+                        float const f = shading::phase_hg(shading::dot(wo, ls.dir), g);
+                        float const w = ls.pdf / (ls.pdf * ls.pdf + f * f);
+                        spec::V4    tr;
+                        ++shadows;
+                        if (spec_transmit(s, pos, ls.dir, ls.dist, medium, depth, lambdas, rng, stack, overflow, tr)) {
+                            L = spec::add(L, spec::mul(spec::scale(w * f, T), spec::mul(tr, spec_of(ls.radiance, lambdas))));
+                        }
+                    }
+                }
+                float    pdf;
+                V3 const wi = shading::sample_hg(wo, g, rng.uniform(), rng.uniform(), pdf);
+                o        = pos;
+                d        = wi;
+                tmin     = 0.f;
+                pdf_prev = pdf;
+                prev_p   = pos;
+                camera   = false;
+                ++depth;
+                continue;
+            }
+            if (!hit) {
+                // The environment: seen by the camera; by continuations when it is a light,
+                // weighted against its next-event pdf (the sphere of directions at a medium vertex).
+                if (medium == 0 && (camera || s.env.w > 0.f)) {
+                    float w = 1.f;
+                    if (!camera) {
+                        w = power_heuristic(pdf_prev, s.env.w * (1.f / (4.f * shading::Pi)));
+                    }
+                    L = spec::add(L, spec::scale(w, spec::mul(T, spec_of(v3(s.env.x, s.env.y, s.env.z), lambdas))));
+                }
+                break;
+            }
+            World_tri const         wt    = world_triangle(s, 0u, r.best_id);
+            shading::Material const mat   = s.materials[wt.material];
+            V3 const                geo   = shading::normalize(shading::cross(wt.b - wt.a, wt.c - wt.a));
+            float const             cos_o = -shading::dot(geo, d);
+            bool const              front = cos_o > 0.f;
+            if (mat.type == shading::Type_light) {
+                if (front || mat.two_sided) {
+                    uint32_t const lb    = s.inst_shade[0].light_base;
+                    uint32_t const order = lb != 0xFFFFFFFFu ? s.light_order[lb + r.best_id] : 0xFFFFFFFFu;
+                    float          w     = camera ? 1.f : (order != 0xFFFFFFFFu ? 1.f : 0.f);
+                    if (!camera && order != 0xFFFFFFFFu) {
+                        float const pick  = light_pick_pdf(s, prev_p, v3(0.f, 0.f, 1.f), true, order, false);
+                        float const area  = s.light_tris[3 * order].w;
+                        float const t     = r.tbest;  // the ray starts at the vertex prev_p
+                        float const pdf_l = pick * (t * t) / (fabsf(cos_o) * area);
+                        w                 = power_heuristic(pdf_prev, pdf_l);
+                    }
+                    L = spec::add(L, spec::scale(w, spec::mul(T, spec_of(mat.emission, lambdas))));
+                }
+                break;
+            }
+            // A medium boundary (the only other material of a spectral scene): the ray
+            // continues past it in the medium behind it.
+            medium = front ? wt.material + 1 : 0;
+            tmin   = offset_f(r.tbest);
+        }
+        spec_splat(film, launch->film_offsets[view], int(cam.w), int(cam.h), px, py, u, v, spec_readout(L, lambdas));
+    }
+    atomicAdd(counts, segments);
+    atomicAdd(counts + 1, shadows);
+}
+
 __global__ void k_resolve(float4 const* film, float4 const* comp, uint32_t n, float4* out) {
     uint32_t const q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) {
@@ -2503,6 +2917,11 @@ struct Renderer::Device {
     // split light selection: the most lights one selection returns in this scene, the depth
     // the split walk starts at, and the picks the buffers hold
     uint32_t  max_picks        = 1;
+    // spectral mode: the scene holds only emitters and non-emissive media; the readout table is
+    // uploaded; the work counter and the kernel's step counts
+    bool                spectral_scene = false;
+    bool                spectral_table = false;
+    unsigned long long* spectral_work  = nullptr;
     uint32_t  split_depth_bias = 0;
     uint64_t  pick_capacity    = 0;
     // film
@@ -2729,6 +3148,7 @@ Renderer::~Renderer() {
     free_ptr(d_->comp);
     free_ptr(d_->out);
     free_ptr(d_->cams);
+    free_ptr(d_->spectral_work);
     free_ptr(d_->view_offsets);
     free_ptr(d_->film_offsets);
     if (d_->stream) {
@@ -2802,7 +3222,8 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     d_->instanced = two_level;
     // A new scene is tuned anew, at the occupancy of the traversal it uses.
     d_->tuner.reset(two_level ? d_->per_sm_inst : d_->per_sm_flat);
-    d_->has_media = false;
+    d_->has_media      = false;
+    d_->spectral_scene = !two_level;
 
     std::vector<Wide_node>           nodes;
     std::vector<Wide_triangle>       tris;
@@ -2895,6 +3316,8 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
                 shading::Material const& sm = scene.materials[mat];
                 bool const volume = sm.type == shading::Type_volume;
                 d_->has_media |= volume;
+                d_->spectral_scene &= sm.type == shading::Type_light ||
+                                      (volume && !(sm.emission.x > 0.f || sm.emission.y > 0.f || sm.emission.z > 0.f));
                 tri_class.push_back(volume ? Class_boundary : Class_surface);
                 if (in.light && sm.type == shading::Type_light) {
                     double a[3], b[3], c[3];
@@ -3653,7 +4076,21 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         SPB_RCUDA(cudaMemcpy(d_->light_nodes, nodes.data(), nodes.size() * sizeof(float), cudaMemcpyHostToDevice));
         d_->split_radii_threshold = settings_.split_threshold;
     }
-    if (int32_t const st = ensure_buffers(max_wave * pixels, picks_per_path)) {
+    if (settings_.spectral) {
+        // the persistent spectral kernel keeps its paths in registers: no wave buffers
+        if (settings_.guiding) {
+            error_ = "spectral rendering has no path guiding";
+            return SPB_ERROR_ARGUMENT;
+        }
+        if (!d_->spectral_scene || d_->instanced) {
+            error_ = "spectral rendering takes scenes of participating media (not emissive), emitters and the "
+                     "environment, in one tree";
+            return SPB_ERROR_ARGUMENT;
+        }
+        if (!d_->counters) {
+            SPB_RCUDA(dev_malloc(&d_->counters, Counter_words * sizeof(uint32_t)));
+        }
+    } else if (int32_t const st = ensure_buffers(max_wave * pixels, picks_per_path)) {
         return st;
     }
     if (settings_.guiding) {
@@ -3706,6 +4143,9 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     stats_                  = Stats();
     stats_.instances        = instances_;
     stats_.device_triangles = device_triangles_;
+    if (settings_.spectral) {
+        return render_spectral(&sg, first_sample, num_samples);
+    }
     std::vector<uint32_t> host_ctr(Counter_words);
     // Device time of the guide's stages: event pairs (inference after each trace, training
     // after each pass), summed after each wave.
@@ -3948,6 +4388,73 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, d_->ev0, d_->ev1);
     stats_.seconds = double(ms) * 1e-3;
+    return SPB_OK;
+}
+
+// Spectral mode: one persistent launch over every (view, pixel, sample) of the call, its
+// samples splatted into the views' films (see k_spectral).
+int32_t Renderer::render_spectral(void const* scene, uint32_t first_sample, uint32_t num_samples) {
+    Scene_gpu const&   sg = *static_cast<Scene_gpu const*>(scene);
+    cudaStream_t const st = d_->stream;
+    if (!d_->spectral_table) {
+        double c[9];
+        double m[9];
+        for (int i = 0; i < 9; ++i) {
+            m[i] = spectral::Srgb_to_ap1[i];
+        }
+        spectral::readout_matrix(m, c);
+        std::vector<float> table(3 * Spec_table);
+        for (int i = 0; i < Spec_table; ++i) {
+            double resp[3];
+            spectral::response(spectral::Lambda_min + double(i), m, resp);
+            for (int k = 0; k < 3; ++k) {
+                table[3 * i + k] = float((c[3 * k] * resp[0] + c[3 * k + 1] * resp[1] + c[3 * k + 2] * resp[2]) *
+                                         double(spectral::Lambda_span) / spectral::Hero_count);
+            }
+        }
+        SPB_RCUDA(cudaMemcpyToSymbol(c_spec_resp, table.data(), table.size() * sizeof(float)));
+        d_->spectral_table = true;
+    }
+    if (!d_->spectral_work) {
+        SPB_RCUDA(dev_malloc(&d_->spectral_work, 4 * sizeof(unsigned long long)));
+    }
+    if (!d_->launch_dev) {
+        SPB_RCUDA(dev_malloc(&d_->launch_dev, sizeof(Launch)));
+        SPB_RCUDA(cudaMallocHost(&d_->launch_host, sizeof(Launch)));
+    }
+    Wave wave{first_sample, num_samples, settings_.seed, settings_.min_bounces, settings_.max_bounces};
+    d_->launch_host->cams         = d_->cams;
+    d_->launch_host->view_offsets = d_->view_offsets;
+    d_->launch_host->film_offsets = d_->film_offsets;
+    d_->launch_host->num_views    = d_->num_views;
+    d_->launch_host->pixels       = d_->traced_pixels;
+    d_->launch_host->wave         = wave;
+    SPB_RCUDA(cudaMemcpyAsync(d_->launch_dev, d_->launch_host, sizeof(Launch), cudaMemcpyHostToDevice, st));
+    SPB_RCUDA(cudaMemsetAsync(d_->spectral_work, 0, 4 * sizeof(unsigned long long), st));
+    SPB_RCUDA(cudaMemsetAsync(d_->counters, 0, Counter_words * sizeof(uint32_t), st));
+    uint64_t const total = uint64_t(d_->traced_pixels) * num_samples;
+    int            per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spectral, Trace_block, 0);
+    uint32_t const grid = uint32_t(std::max(1, per_sm)) * d_->sms;
+    SPB_RCUDA(cudaEventRecord(d_->ev0, st));
+    k_spectral<<<grid, Trace_block, 0, st>>>(sg, d_->launch_dev, total, d_->spectral_work, d_->film,
+                                              d_->counters + Overflow_slot, d_->spectral_work + 2);
+    SPB_RCUDA(cudaGetLastError());
+    SPB_RCUDA(cudaEventRecord(d_->ev1, st));
+    unsigned long long counts[4];
+    uint32_t           host_ctr[4];
+    SPB_RCUDA(cudaMemcpyAsync(counts, d_->spectral_work, sizeof(counts), cudaMemcpyDeviceToHost, st));
+    SPB_RCUDA(cudaMemcpyAsync(host_ctr, d_->counters + Overflow_slot, sizeof(host_ctr), cudaMemcpyDeviceToHost, st));
+    SPB_RCUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, d_->ev0, d_->ev1);
+    stats_.seconds         = double(ms) * 1e-3;
+    stats_.paths           = total;
+    stats_.extension_rays  = counts[2];
+    stats_.shadow_rays     = counts[3];
+    stats_.overflow        = host_ctr[0];
+    stats_.tracking_capped = host_ctr[2];
+    stats_.wave_paths      = uint32_t(std::min<uint64_t>(total, 0xFFFFFFFFu));
     return SPB_OK;
 }
 

@@ -122,6 +122,10 @@ struct Settings {
     uint32_t trace_blocks_per_sm = 0;
     // Waves without media or training are captured once per shape as a CUDA graph and replayed.
     bool cuda_graphs = true;
+    // Hero-wavelength spectral transport (no counterpart in the reference, which is RGB): each
+    // path carries four wavelengths in [380, 720] nm; one persistent launch renders every view
+    // and sample.  For scenes of participating media, emitters and the environment.
+    bool spectral = false;
 };
 
 struct Stats {
@@ -185,6 +189,8 @@ class Renderer {
     std::string error_;
 
     int32_t ensure_buffers(uint32_t paths, uint32_t picks_per_path);
+    // (scene: the kernels' scene parameters, a type private to render.cu)
+    int32_t render_spectral(void const* scene, uint32_t first_sample, uint32_t num_samples);
     int32_t ensure_guide(uint32_t paths);
     int32_t train_guide(uint32_t paths);
     void    clear_graphs();

@@ -133,14 +133,16 @@ VOLUME_CONFIG = ("2 m cube of 256^3 fBm density (5 octaves, seed 4), mu_t 20 per
                  "RGB delta/ratio tracking (the reference's transport; no hero wavelengths)")
 
 
-def measure_volume(views=4, spp=128, cpu_reference=False, batch=True):
+def measure_volume(views=4, spp=128, cpu_reference=False, batch=True, spectral=True):
     """The heterogeneous-volume workload: the first `views` of scenes.volume_views() (seeded
     camera positions, image sides U[256, 1024]) of one scene, built and uploaded once; each
     view moves the camera and sets its resolution, then renders one frame.  Samples/s over the
     device time of all views; the end-to-end rate includes, per view, su_render_frame +
     su_postprocess + framebuffer copy, and the scene's one-time upload.  With batch, the same
     views are also rendered together in one spb_render_views call (after one untimed call),
-    timed on the device and end to end (the call, with every view's image copied to the host)."""
+    timed on the device and end to end (the call, with every view's image copied to the host).
+    With spectral, the same batch once more in the hero-wavelength spectral mode (4 wavelengths
+    per path in [380, 720] nm; every view and sample in one persistent launch)."""
     lib = _lib.load()
     stats = _lib.RenderStats()
     density = scenes.fbm_density(256)
@@ -177,6 +179,21 @@ def measure_volume(views=4, spp=128, cpu_reference=False, batch=True):
                          "wave_paths": stats.wave_paths,
                          "note": f"all {views} views in one spb_render_views call: their paths share the waves; "
                                  "e2e = the call, every view's image copied to the host"}
+        if spectral:
+            assert su.su_create_integrators(json.dumps({"surface": {"PTMIS": {
+                "min_bounces": 4, "max_bounces": 32, "spectral": True}}}).encode()) == 0
+            su.render_views(cams, spp)  # warm-up
+            t0 = time.perf_counter()
+            su.render_views(cams, spp)
+            spectral_wall = time.perf_counter() - t0
+            assert lib.spb_render_last_stats(ctypes.byref(stats)) == 0
+            spectral_out = {"msamples_s": round(samples / stats.device_seconds / 1e6, 3),
+                            "device_seconds": round(stats.device_seconds, 3),
+                            "e2e_msamples_s": round(samples / spectral_wall / 1e6, 3),
+                            "segments_per_sample": round(stats.extension_rays / stats.paths, 3),
+                            "shadow_rays_per_sample": round(stats.shadow_rays / stats.paths, 3),
+                            "note": f"hero-wavelength spectral mode (4 wavelengths in [380, 720] nm per path), "
+                                    f"all {views} views and samples in one persistent launch"}
     finally:
         su.su_release()
     out = {"workload": "volume", "config": f"{VOLUME_CONFIG}, {views} of 64 views (sides "
@@ -188,6 +205,8 @@ def measure_volume(views=4, spp=128, cpu_reference=False, batch=True):
                        "host, wall clock (the scene's one-time upload and majorant build in the first view)"}
     if batch:
         out["batch"] = batch_out
+        if spectral:
+            out["spectral_batch"] = spectral_out
     if cpu_reference:
         import oracle  # test/baseline infrastructure: times the reference renderer
 

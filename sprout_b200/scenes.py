@@ -701,3 +701,53 @@ def textured_room(su, width: int, height: int, spp: int, max_bounces: int = 8, i
     m[3, :3] = (0.2, 0.3, 0.2)
     su.set_transformation(prop, m)
     return cam
+
+
+# ---- a chromatic medium for the spectral mode ----
+
+def spectral_box(su, width: int, height: int, spp: int, density, position=(2.6, 1.6, -3.0),
+                 max_bounces: int = 12, min_bounces: int = 4, integrator=None, medium=None, emission=None,
+                 environment=None):
+    """The spectral mode's check scene: a [-1, 1]^3 box (a mesh with outward faces) filled with
+    a density grid of a chromatic medium (attenuation colour [0.4, 0.6, 0.8] over 0.5 m,
+    subsurface colour 0.7, anisotropy 0.4), a sphere light of radius 0.3 (an icosphere mesh,
+    radiance [30, 22, 14]) beside it and a uniform environment [0.2, 0.3, 0.5]; PTMIS with the
+    renderer's "spectral" key.  Returns the camera entity and the scene as data (world-space
+    triangles, per-triangle roles, material parameters as given to su_create_material, the
+    density and its world-to-texture map, the camera), from which the oracle renders the same
+    image.  medium (Volumetric parameters), emission and environment replace the colours."""
+    fov = math.radians(45.0)
+    cam = su.su_create_camera_perspective(width, height, fov)
+    view = _look_at(position)
+    su.set_transformation(cam, view)
+    ptmis = {"min_bounces": min_bounces, "max_bounces": max_bounces, "spectral": True}
+    ptmis.update(integrator or {})
+    su.su_create_integrators(json.dumps({"surface": {"PTMIS": ptmis}}).encode())
+    su.su_create_sampler(spp)
+    medium = medium or {"attenuation_color": [0.4, 0.6, 0.8], "attenuation_distance": 0.5,
+                        "subsurface_color": [0.7, 0.7, 0.7], "anisotropy": 0.4}
+    emission = emission or [30.0, 22.0, 14.0]
+    environment = environment or [0.2, 0.3, 0.5]
+    image = su.image(density)
+    m_medium = _material(su, "Volumetric", density={"id": int(image)}, **medium)
+    m_lamp = _material(su, "Light", emission=emission)
+    m_sky = _material(su, "Light", emission=environment)
+    bp, bn, bi = _box_mesh((-1.0, -1.0, -1.0), (1.0, 1.0, 1.0))
+    v, f = icosphere(1)
+    lp = (0.3 * v + np.array([1.5, 1.4, -1.3], np.float32)).astype(np.float32)
+    box_prop = su.prop(su.mesh(bp, bn, bi), [m_medium])
+    su.set_transformation(box_prop, np.eye(4, dtype=np.float32))
+    lamp_prop = su.prop(su.mesh(lp, v, f), [m_lamp])
+    su.set_transformation(lamp_prop, np.eye(4, dtype=np.float32))
+    su.su_create_light(lamp_prop)
+    sky_prop = su.prop(SHAPE_INFINITE_SPHERE, [m_sky])
+    su.set_transformation(sky_prop, np.eye(4, dtype=np.float32))
+    su.su_create_light(sky_prop)
+    tris = np.concatenate([bp[bi].reshape(-1, 9), lp[f].reshape(-1, 9)]).astype(np.float64)
+    roles = np.concatenate([np.ones(len(bi), np.int32), np.zeros(len(f), np.int32)])
+    scene = {"triangles": tris, "roles": roles, "medium": medium, "emission": emission,
+             "environment": environment, "density": np.asarray(density, np.float64),
+             "world_to_uvw": [[0.5, 0.0, 0.0, 0.5], [0.0, 0.5, 0.0, 0.5], [0.0, 0.0, 0.5, 0.5]],
+             "camera": {"width": width, "height": height, "fov": fov, "matrix": view},
+             "min_bounces": min_bounces, "max_bounces": max_bounces}
+    return cam, scene
