@@ -811,22 +811,23 @@ __device__ __forceinline__ Light_pick pick_in_leaf(Scene_gpu const& s, uint32_t 
 // sampling): the environment with probability 1, and the tree walked from depth
 // split_depth_bias, descending into both children of every node that split_node passes while
 // above Max_split_depth (a leaf so reached gives all its lights); below the first node that does
-// not split, the walk chooses as before, with the random number it carried.  Fills out (at most
-// Max_light_picks entries, the host having bounded the tree's picks so) and returns the count.
-__device__ uint32_t select_lights(Scene_gpu const& s, V3 p, V3 n, bool total_sphere, float r, bool split,
-                                  Light_pick* out) {
+// not split, the walk chooses as before, with the random number it carried.  Hands each light to
+// emit(index, pick) (at most Max_light_picks, the host having bounded the tree's picks so),
+// stopping early when emit returns false, and returns the number emitted.
+template <class Emit>
+__device__ uint32_t walk_lights(Scene_gpu const& s, V3 p, V3 n, bool total_sphere, float r, bool split, Emit&& emit) {
     uint32_t m     = 0;
     float    ip    = 0.f;
     uint32_t depth = Max_split_depth;
     if (split) {
         depth = s.split_depth_bias;
-        if (s.env.w > 0.f) {
-            out[m++] = {Env_pick, 1.f};
+        if (s.env.w > 0.f && !emit(m++, Light_pick{Env_pick, 1.f})) {
+            return m;
         }
     } else {
         ip = s.env.w;
         if (r < ip) {
-            out[m++] = {Env_pick, ip};
+            emit(m++, Light_pick{Env_pick, ip});
             return m;
         }
     }
@@ -873,11 +874,15 @@ __device__ uint32_t select_lights(Scene_gpu const& s, V3 p, V3 n, bool total_sph
         }
         if (do_split) {
             for (uint32_t k = 0; k < count && m < Max_light_picks; ++k) {
-                out[m++] = {first + k, t.pdf};
+                if (!emit(m++, Light_pick{first + k, t.pdf})) {
+                    return m;
+                }
             }
         } else if (m < Max_light_picks) {
             Light_pick const pk = pick_in_leaf(s, first, count, p, n, total_sphere, t.r);
-            out[m++]            = {pk.light, pk.pdf * t.pdf};
+            if (!emit(m++, Light_pick{pk.light, pk.pdf * t.pdf})) {
+                return m;
+            }
         }
         if (top == 0) {
             break;
@@ -885,6 +890,15 @@ __device__ uint32_t select_lights(Scene_gpu const& s, V3 p, V3 n, bool total_sph
         t = stack[--top];
     }
     return m;
+}
+
+// select_lights into an array (at most Max_light_picks entries; one without splitting).
+__device__ __forceinline__ uint32_t select_lights(Scene_gpu const& s, V3 p, V3 n, bool total_sphere, float r,
+                                                  bool split, Light_pick* out) {
+    return walk_lights(s, p, n, total_sphere, r, split, [&](uint32_t k, Light_pick pk) {
+        out[k] = pk;
+        return true;
+    });
 }
 
 // Probability that select_lights from (p, n) includes the light at tree position order
@@ -1467,8 +1481,29 @@ __device__ __forceinline__ void next_event(Scene_gpu const& s, Paths const& p, W
                                            bool total_sphere, uint32_t depth, float select, Rng& rng,
                                            bool golden, uint32_t gpixel, uint32_t gsample, Eval const& eval,
                                            bool& shadow, bool& shadow2) {
-    Light_pick     picks[Max_light_picks];
-    uint32_t const m     = select_lights(s, ps, n, total_sphere, select, splits_at(s, depth), picks);
+    // One walk counts the selection and keeps its first two lights; a split selection of more
+    // (rare) walks again for each further light.
+    bool const split  = splits_at(s, depth);
+    Light_pick first0 = {0u, 0.f}, first1 = {0u, 0.f};
+    uint32_t const m  = walk_lights(s, ps, n, total_sphere, select, split, [&](uint32_t k, Light_pick pk) {
+        if (k == 0) {
+            first0 = pk;
+        } else if (k == 1) {
+            first1 = pk;
+        }
+        return true;
+    });
+    auto const pick_at = [&](uint32_t k) {
+        if (k < 2) {
+            return k == 0 ? first0 : first1;
+        }
+        Light_pick got = {0u, 0.f};
+        walk_lights(s, ps, n, total_sphere, select, split, [&](uint32_t i, Light_pick pk) {
+            got = pk;
+            return i < k;
+        });
+        return got;
+    };
     auto const     point = [&](uint32_t l, float& r1, float& r2) {
         if (golden) {
             float2 const g = golden_2d(wave, gpixel, gsample, golden_light_2d(depth, l));
@@ -1483,7 +1518,7 @@ __device__ __forceinline__ void next_event(Scene_gpu const& s, Paths const& p, W
         float r1, r2;
         point(l, r1, r2);
         Light_sample ls;
-        if (sample_light(s, ps, n, total_sphere, picks[l], r1, r2, ls)) {
+        if (sample_light(s, ps, n, total_sphere, pick_at(l), r1, r2, ls)) {
             V3 const c = eval(ls);
             if (shading::max_component(c) > 0.f) {
                 store_shadow(p, path, second, ps, ls, c, depth);
@@ -1493,7 +1528,7 @@ __device__ __forceinline__ void next_event(Scene_gpu const& s, Paths const& p, W
         return false;
     };
     uint32_t first = 0;
-    if (m > 1 && picks[0].light == Env_pick) {
+    if (m > 1 && first0.light == Env_pick) {
         shadow2 = slot(0, true);
         first   = 1;
     }
@@ -1515,7 +1550,7 @@ __device__ __forceinline__ void next_event(Scene_gpu const& s, Paths const& p, W
         Light_sample ls;
         V3           c = v3(0.f, 0.f, 0.f);
         float4       d = make_float4(0.f, 0.f, 1.f, 0.f);
-        if (sample_light(s, ps, n, total_sphere, picks[first + k], r1, r2, ls)) {
+        if (sample_light(s, ps, n, total_sphere, pick_at(first + k), r1, r2, ls)) {
             V3 const e = eval(ls);
             if (shading::max_component(e) > 0.f) {
                 c = e;
