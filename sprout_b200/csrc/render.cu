@@ -68,7 +68,7 @@ constexpr uint32_t Class_instance   = 4;  // ... of top-level leaves (instances)
 // emitters), 5 picks of split light selections, 6 split records, 7 picks through media,
 // 8 shadow slots through media (rays to the environment); then the overflow counter.
 constexpr uint32_t Counter_stride = 16;
-constexpr uint32_t Graph_max_paths = 1u << 21;  // largest wave replayed from a CUDA graph
+constexpr uint32_t Graph_max_paths = 1u << 25;  // largest wave replayed from a CUDA graph
 constexpr uint64_t Pick_budget     = 24ull << 30;  // bytes of picks a wave may hold
 constexpr uint32_t Counter_words  = Counter_stride * Max_bounce_slots + 4;
 constexpr uint32_t Overflow_slot  = Counter_stride * Max_bounce_slots;
@@ -4339,9 +4339,8 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         SPB_RCUDA(cudaMemcpyAsync(d_->launch_dev, d_->launch_host, sizeof(Launch), cudaMemcpyHostToDevice, st));
         uint32_t iterations = 0;
         size_t   events     = 0;
-        // Graphs pay where launches are a visible share of a wave (at most Graph_max_paths
-        // paths) and for wave shapes that recur: a shape is captured when it comes the second
-        // time, then replayed.
+        // Wave shapes that recur are replayed from graphs: a shape is captured when it comes the
+        // second time (waves without media or training, up to Graph_max_paths paths).
         Device::Wave_graph* g = nullptr;
         bool const graphable = settings_.cuda_graphs && !d_->has_media && !training && paths <= Graph_max_paths;
         if (graphable) {

@@ -38,17 +38,19 @@ from . import _lib, capi, scenes
 SCENES = {
     "cornell": ("Cornell box (5 walls, 0.25 m^2 light of radiance 17, 81,920-tri GGX conductor sphere alpha 0.3), "
                 "PTMIS max depth 8 (Russian roulette from depth 4)",
-                lambda su, w, h, spp: scenes.cornell(su, w, h, sphere_subdivisions=6, tonemap=True, spp=spp),
+                lambda su, w, h, spp, extra=None: scenes.cornell(su, w, h, sphere_subdivisions=6, tonemap=True, spp=spp,
+                                                                  integrator=extra),
                 (512, 512, 64), None),
     "wavefront": ("400 instances of a 5,000-tri displaced sphere (2,000,000 tris, Substitute roughness U[0.05,1], "
                   "metallic Bernoulli(0.3)), 4,096 emissive tris of log-uniform radiance [0.1, 100] via the light "
                   "tree, PTMIS max depth 12 (Russian roulette from depth 4); the props kept as instances of one "
                   "mesh under a top-level tree",
-                  lambda su, w, h, spp: scenes.wavefront(su, w, h, spp),
+                  lambda su, w, h, spp, extra=None: scenes.wavefront(su, w, h, spp, integrator=extra),
                   (1920, 1080, 256), (960, 540, 16)),
     "wavefront_flat": ("the same scene with every prop flattened into one 2,004,098-triangle tree "
                        "(\"instancing\": false)",
-                       lambda su, w, h, spp: scenes.wavefront(su, w, h, spp, integrator={"instancing": False}),
+                       lambda su, w, h, spp, extra=None: scenes.wavefront(su, w, h, spp,
+                                                                           integrator={"instancing": False, **(extra or {})}),
                        (1920, 1080, 256), None),
 }
 
@@ -59,7 +61,9 @@ def rel_mse(x, r):
 
 
 def measure(scene="cornell", width=None, height=None, spp=None, frames=3, convergence=False,
-            cpu_reference=False):
+            cpu_reference=False, tuning_frames=6, integrator=None):
+    """Times `frames` steady-state frames of a scene (device time from the renderer's events;
+    end to end by the wall clock).  integrator: further PTMIS keys (e.g. "cuda_graphs": false)."""
     config, build, (w0, h0, spp0), cpu_frame = SCENES[scene]
     width, height, spp = width or w0, height or h0, spp or spp0
     lib = _lib.load()
@@ -68,12 +72,24 @@ def measure(scene="cornell", width=None, height=None, spp=None, frames=3, conver
     out = {"workload": scene, "config": f"{config}, {width}x{height}, {spp} spp"}
     assert su.su_init(False) == 0
     try:
-        build(su, width, height, spp)
+        build(su, width, height, spp, integrator)
         t0 = time.perf_counter()
         assert su.su_start_render_frame(0) == 0, su.messages  # scene upload + BVH build
         out["prepare_s"] = round(time.perf_counter() - t0, 3)
         assert su.su_render_frame(0) == 0, su.messages  # warm-up (autotuner)
         out["first_frame_s"] = round(time.perf_counter() - t0, 3)
+        # The autotuner tries wave sizes, then lower occupancies, one full wave each, and keeps
+        # the best for later frames: warm up until two frames in a row end on the same launch
+        # shape (the tuned one), so that timed frames are steady-state frames.
+        shape = None
+        for _ in range(tuning_frames):
+            assert lib.spb_render_last_stats(ctypes.byref(stats)) == 0
+            now = (stats.wave_paths, stats.trace_blocks_per_sm)
+            if now == shape:
+                break
+            shape = now
+            assert su.su_render_frame(0) == 0, su.messages
+        out["launch_shape"] = {"wave_paths": stats.wave_paths, "trace_blocks_per_sm": stats.trace_blocks_per_sm}
         dev, wall = [], []
         for _ in range(frames):
             t0 = time.perf_counter()
@@ -87,6 +103,7 @@ def measure(scene="cornell", width=None, height=None, spp=None, frames=3, conver
         rays = stats.extension_rays + stats.shadow_rays
         samples = width * height * spp
         out.update({"instances": stats.instances, "device_triangles": stats.device_triangles,
+                    "graph_waves": stats.graph_waves,
                     "msamples_s": round(samples / dev_s / 1e6, 3), "mrays_s": round(rays / dev_s / 1e6, 3),
                     "ms_per_frame": round(1e3 * dev_s, 3), "rays_per_sample": round(rays / samples, 3),
                     "e2e_msamples_s": round(samples / statistics.median(wall) / 1e6, 3),
