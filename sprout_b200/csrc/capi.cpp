@@ -451,6 +451,7 @@ int32_t compile_scene() {
         inst.mesh     = it->second;
         inst.fallback = fallback_id;
         inst.light    = e.light;
+        inst.cube     = e.shape == Shape_cube;
         std::copy(e.trafo, e.trafo + 16, inst.trafo);
         float pos[3];
         decompose(e.trafo, inst.rotation, pos);
@@ -464,7 +465,15 @@ int32_t compile_scene() {
             }
             inst.materials[k] = mat;
             Grid_ref const& gr = engine->material_grids[mat];
+            Material const& em = engine->materials[mat];
+            bool const emitting_light = e.light && em.type == spb::shading::Type_volume &&
+                                        (em.emission.x > 0.f || em.emission.y > 0.f || em.emission.z > 0.f);
             if (gr.image == Null) {
+                if (emitting_light) {
+                    // the light of an emitting medium is named by its material: one per prop
+                    inst.materials[k] = uint32_t(scene.materials.size());
+                    scene.materials.push_back(em);
+                }
                 continue;
             }
             spb::render::Grid_medium gm;
@@ -1579,15 +1588,13 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
             log(SU_LOG_ERROR, "su_create_material: temperature grids are not supported");
             return Null;
         }
-        // "emission" (material_provider.cpp:805-806): a homogeneous medium's emitted radiance per
-        // unit absorption (Material::collision_coefficients_emission, material.cpp:87-89)
+        // "emission" (material_provider.cpp:805-806): the emitted radiance per unit absorption
+        // (Material::collision_coefficients_emission, material.cpp:87-89); with a density grid
+        // the material is a Grid_emission (material_provider.cpp:823-830), whose absorption
+        // scales with the density and whose emission does not (volumetric_grid.cpp:110-127).
         V3 emission{0.f, 0.f, 0.f};
         if (read_color(desc.find("emission"), emission) &&
             (emission.x > 0.f || emission.y > 0.f || emission.z > 0.f)) {
-            if (grid.image != Null) {
-                log(SU_LOG_ERROR, "su_create_material: emissive density grids are not supported");
-                return Null;
-            }
             m.emission = emission;
         }
         if (spb::json::Value const* sampler = desc.find("sampler")) {

@@ -305,6 +305,18 @@ void build_light_tree(std::vector<Light_input> const& lights, uint32_t num_slots
         it.box.add(in.a);
         it.box.add(in.b);
         it.box.add(in.c);
+        if (in.volume != 0) {
+            // an emitting medium: its box, radiating in every direction
+            for (int k = 0; k < 3; ++k) {
+                it.centroid[k]  = 0.5 * (in.a[k] + in.b[k]);
+                it.cone.axis[k] = k == 2 ? 1.0 : 0.0;
+            }
+            it.cone.theta = Pi;
+            it.power      = in.power;
+            it.area       = 0.0;
+            it.two_sided  = true;
+            continue;
+        }
         double e1[3], e2[3], n[3];
         for (int k = 0; k < 3; ++k) {
             it.centroid[k] = (in.a[k] + in.b[k] + in.c[k]) / 3.0;
@@ -345,6 +357,14 @@ void build_light_tree(std::vector<Light_input> const& lights, uint32_t num_slots
         b.put_float4(out.cones, it.cone.axis[0], it.cone.axis[1], it.cone.axis[2],
                      it.two_sided ? -1.0 : 1.0);
         b.put_float4(out.cones, it.power, 0.0, 0.0, 0.0);
+        if (in.volume != 0) {
+            b.put_float4(out.tris, c[0], c[1], c[2], -double(in.volume));
+            b.put_float4(out.tris, 0.0, 0.0, 0.0, 0.0);
+            b.put_float4(out.tris, 0.0, 0.0, 0.0, 0.0);
+            out.tris.back()    = Builder::bits(in.material);
+            out.order[in.slot] = o;
+            continue;
+        }
         b.put_float4(out.tris, in.a[0], in.a[1], in.a[2], it.area);
         b.put_float4(out.tris, in.b[0] - in.a[0], in.b[1] - in.a[1], in.b[2] - in.a[2], 0.0);
         b.put_float4(out.tris, in.c[0] - in.a[0], in.c[1] - in.a[1], in.c[2] - in.a[2], 0.0);

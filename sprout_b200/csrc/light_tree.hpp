@@ -15,13 +15,15 @@
 
 namespace spb::render {
 
-// One emissive triangle in world space.
+// One emissive triangle in world space, or an emitting medium (volume != 0) whose world box
+// runs from a to b (c its centre), emitting in all directions.
 struct Light_input {
     double   a[3], b[3], c[3];
     double   power = 0.0;  // area * mean radiance (twice that for two-sided emitters)
     bool     two_sided = false;
     uint32_t slot      = 0;  // index of its entry in Light_tree::order
     uint32_t material  = 0;  // its material (stored with it for the renderer's light sampling)
+    uint32_t volume    = 0;  // 1 + the renderer's index of an emitting medium's light; 0: a triangle
 };
 
 // Device-ready arrays, 4 floats per float4.
@@ -36,7 +38,8 @@ struct Light_input {
 //           light_tree_builder.cpp:86-102).
 //   cones:  3 float4 per light in tree order: (centre, radius), (normal, cos spread),
 //           (power, 0, 0, 0)
-//   tris:   3 float4 per light in tree order: (a, area), (b - a, 0), (c - a, material index bits)
+//   tris:   3 float4 per light in tree order: (a, area), (b - a, 0), (c - a, material index bits);
+//           for an emitting medium (centre, -volume), (0, 0), (0, material index bits)
 //   order:  per light slot (Light_input::slot), its position in tree order, or 0xFFFFFFFF
 struct Light_tree {
     std::vector<float>    nodes;

@@ -135,7 +135,10 @@ struct Material {
     V3       mu_a;       // absorption coefficient per metre (Volume)
     V3       mu_s;       // scattering coefficient per metre (Volume)
     uint32_t medium;     // Volume: 0 homogeneous, else 1 + index of the density-grid medium
-    uint32_t pad;
+    // Volume: 0 when its emission is not a light's; else 1 + its light's position in the light
+    // tree, or Volume_light_unsampled for a light whose shape next-event estimation cannot
+    // sample (its emission then counts with weight 1 on every segment).
+    uint32_t volume_light;
     // Substitute texture maps: the base colour and the dielectric F0 the per-hit parameters are
     // rebuilt from, and 1 + the index of the colour and surface textures (0: none); the surface
     // texture holds roughness, and metallic too when surface_channels is 2.
@@ -150,6 +153,7 @@ struct Material {
 constexpr uint32_t Type_substitute = 0;
 constexpr uint32_t Type_light      = 1;
 constexpr uint32_t Type_volume     = 2;  // participating medium inside a closed mesh
+constexpr uint32_t Volume_light_unsampled = 0xFFFFFFFFu;
 
 // Henyey-Greenstein phase function of c = dot(wo, wi) (material.inl:15-19).
 SPB_HD float phase_hg(float c, float g) {

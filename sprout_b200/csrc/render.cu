@@ -94,6 +94,33 @@ struct Texture_gpu {
     uint32_t      pad[2];
 };
 
+// A Cube prop whose emitting medium is a light (Light::Type::Volume and Volume_image,
+// light.cpp:101-134; the cube is [-1, 1]^3 in object space, cube.cpp:134-190): its
+// object-to-world map, world volume and material, and for a density grid the 3-D distribution
+// its points are drawn from with the grid's normalisation (Grid_emission, volumetric_grid.cpp).
+struct Volume_light_gpu {
+    float4   m0, m1, m2;  // rows: world_k = dot(row_k.xyz, object) + row_k.w
+    float    volume;
+    uint32_t material;
+    uint32_t dist;        // 0: uniform points (homogeneous medium); else 1 + index into emission_dists
+    uint32_t medium;      // the density-grid medium (index into media) when dist != 0
+    float    pdf_factor;  // voxels / largest absorption coefficient (Grid_emission::pdf_factor_)
+    V3       a_norm;      // largest absorption coefficient / absorption coefficient (a_norm_)
+};
+
+// The 3-D distribution of a density grid's emitted luminance (Grid_emission::prepare_sampling
+// with Distribution_3D, volumetric_grid.cpp:182-318, distribution_3d.cpp): per voxel its
+// probability, and cumulative sums over slices (z), over the rows of each slice and over the
+// voxels of each row, each running from 0 to 1.
+struct Emission_dist_gpu {
+    float const* prob;   // nx * ny * nz, x fastest
+    float const* cdf_z;  // nz + 1
+    float const* cdf_y;  // nz * (ny + 1)
+    float const* cdf_x;  // nz * ny * (nx + 1)
+    int          nx, ny, nz;
+    uint32_t     repeat;  // the grid's address mode (1: repeat, 0: clamp)
+};
+
 struct Scene_gpu {
     uint4 const*              nodes;
     float4 const*             tris;
@@ -124,6 +151,10 @@ struct Scene_gpu {
     uint32_t                  split_bounces;
     uint32_t                  split_depth_bias;
     float                     split_scale;  // 3 (1 / t - 1)^2 for the splitting threshold t (split_node)
+    // Emitting media that are lights: their light-tree entries (light_tris) hold -1 - index
+    // into volume_lights in the first float4's w.
+    Volume_light_gpu const*   volume_lights;
+    Emission_dist_gpu const*  emission_dists;
 };
 
 // What shading reads of an instance: its object-to-world map (rows: world_k =
@@ -960,8 +991,94 @@ struct Light_sample {
 // runs after ++ray.depth), and this renderer does the same so that images agree.
 constexpr uint32_t Split_bounces = 3;  // Pathtracer_MIS::Num_dedicated_samplers
 
+// Index i in [0, n) with cdf[i] <= r < cdf[i + 1] for r in [0, 1) (cdf[0] = 0, cdf[n] = 1),
+// and where r falls inside that bucket.
+__device__ __forceinline__ int cdf_bucket(float const* cdf, int n, float r, float& frac) {
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        int const mid = (lo + hi) >> 1;
+        if (__ldg(cdf + mid) <= r) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    float const c0 = __ldg(cdf + lo);
+    float const c1 = __ldg(cdf + lo + 1);
+    frac           = c1 > c0 ? fminf((r - c0) / (c1 - c0), 0.99999994f) : 0.5f;
+    return lo;
+}
+
+// A voxel drawn in proportion to its probability and a uniform point in it (slice, then row,
+// then voxel, as Distribution_3D::sample_continuous, distribution_3d.cpp:46-55); returns the
+// voxel's probability (0 if none can be drawn), its index and the point in texture space.
+__device__ float sample_emission(Emission_dist_gpu const& e, float r1, float r2, float r3, uint32_t& voxel,
+                                 V3& uvw) {
+    float      fz, fy, fx;
+    int const  z = cdf_bucket(e.cdf_z, e.nz, r3, fz);
+    int const  y = cdf_bucket(e.cdf_y + size_t(z) * (e.ny + 1), e.ny, r2, fy);
+    int const  x = cdf_bucket(e.cdf_x + (size_t(z) * e.ny + y) * (e.nx + 1), e.nx, r1, fx);
+    voxel        = uint32_t((size_t(z) * e.ny + y) * e.nx + x);
+    uvw          = v3((float(x) + fx) / float(e.nx), (float(y) + fy) / float(e.ny), (float(z) + fz) / float(e.nz));
+    return __ldg(e.prob + voxel);
+}
+
+// The probability of the voxel that texture-space point uvw falls in, under the grid's address
+// mode (Grid_emission::emission_pdf without its factor, volumetric_grid.cpp:104-108).
+__device__ __forceinline__ float emission_prob(Emission_dist_gpu const& e, V3 uvw) {
+    bool const  repeat = e.repeat != 0;
+    float const u      = repeat ? uvw.x - floorf(uvw.x) : __saturatef(uvw.x);
+    float const v      = repeat ? uvw.y - floorf(uvw.y) : __saturatef(uvw.y);
+    float const w      = repeat ? uvw.z - floorf(uvw.z) : __saturatef(uvw.z);
+    int const   x      = min(int(u * float(e.nx)), e.nx - 1);
+    int const   y      = min(int(v * float(e.ny)), e.ny - 1);
+    int const   z      = min(int(w * float(e.nz)), e.nz - 1);
+    return __ldg(e.prob + (size_t(z) * e.ny + y) * e.nx + x);
+}
+
+// Next-event sample of an emitting medium's light: a point inside the cube -- uniform for a
+// homogeneous medium (Cube::sample_volume, cube.cpp:134-151), from the emission distribution for
+// a density grid (volume_image_sample, light.cpp:112-134, and Cube::sample_volume with uvw,
+// cube.cpp:177-190) -- with pdf distance^2 / volume (times the voxel's probability times the
+// grid's factor); its radiance is the medium's absorption times emission
+// (Homogeneous::evaluate_radiance), or for a grid the nearest density times a_norm times the
+// emission (Grid_emission::evaluate_radiance with Filter::Nearest, Pathtracer_MIS::evaluate_light).
+__device__ bool sample_volume_light(Scene_gpu const& s, uint32_t index, V3 ps, V3 n, bool total_sphere,
+                                    float pick_pdf, float r1, float r2, float r3, Light_sample& ls) {
+    Volume_light_gpu const  vl   = s.volume_lights[index];
+    shading::Material const lmat = s.materials[vl.material];
+    V3                      uvw  = v3(r1, r2, r3);
+    float                   pdf  = 1.f;
+    V3                      rad  = lmat.mu_a * lmat.emission;
+    if (vl.dist != 0) {
+        uint32_t    voxel;
+        float const prob = sample_emission(s.emission_dists[vl.dist - 1], r1, r2, r3, voxel, uvw);
+        if (!(prob > 0.f)) {
+            return false;
+        }
+        pdf = prob * vl.pdf_factor;
+        rad = (__ldg(s.media[vl.medium].density + voxel) * vl.a_norm) * lmat.emission;
+    }
+    V3 const    o    = v3(2.f * uvw.x - 1.f, 2.f * uvw.y - 1.f, 2.f * uvw.z - 1.f);
+    V3 const    wp   = v3(vl.m0.x * o.x + vl.m0.y * o.y + vl.m0.z * o.z + vl.m0.w,
+                          vl.m1.x * o.x + vl.m1.y * o.y + vl.m1.z * o.z + vl.m1.w,
+                          vl.m2.x * o.x + vl.m2.y * o.y + vl.m2.z * o.z + vl.m2.w);
+    V3 const    axis = wp - ps;
+    float const d2   = shading::dot(axis, axis);
+    float const d    = sqrtf(d2);
+    V3 const    dir  = (1.f / d) * axis;
+    if (!(d > 0.f) || (!total_sphere && !(shading::dot(dir, n) > 0.f))) {
+        return false;
+    }
+    ls.dir      = dir;
+    ls.dist     = d;
+    ls.pdf      = pick_pdf * (d2 / vl.volume) * pdf;
+    ls.radiance = rad;
+    return true;
+}
+
 __device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, V3 n, bool total_sphere,
-                                             Light_pick pk, float r1, float r2, Light_sample& ls) {
+                                             Light_pick pk, float r1, float r2, Rng& rng, Light_sample& ls) {
     if (pk.light == Env_pick) {
         // The environment: uniform directions over the hemisphere of n, or over the sphere at a
         // medium vertex (Infinite_sphere::sample, infinite_sphere.cpp:68-101).
@@ -981,6 +1098,10 @@ __device__ __forceinline__ bool sample_light(Scene_gpu const& s, V3 ps, V3 n, bo
     }
     uint32_t const l       = pk.light;
     float4 const   la      = s.light_tris[3 * l + 0];
+    if (la.w < 0.f) {
+        return sample_volume_light(s, uint32_t(-1.f - la.w), ps, n, total_sphere, pk.pdf, r1, r2, rng.uniform(),
+                                   ls);
+    }
     float4 const   le1     = s.light_tris[3 * l + 1];
     float4 const   le2     = s.light_tris[3 * l + 2];
     uint32_t const lmat_id = __float_as_uint(le2.w);  // the emitter's material
@@ -1137,14 +1258,26 @@ __device__ __forceinline__ int increment(int v, int max, bool repeat) {
     return v >= max ? (repeat ? 0 : max) : v + 1;
 }
 
+// Texture filtering by depth (Pathtracer_MIS::integrate, pathtracer_mis.cpp:121, and
+// Sampler_cache::sampler_3D / sampler_2D, sampler_cache.cpp:40-64): a vertex of depth 0 or 1
+// samples its textures with their own filter, a deeper one with the nearest texel (keeping the
+// address mode); the segment after a vertex and its shadow rays track density grids with the
+// vertex's filter.  A path's depth after a bounce is the depth of the vertex it left plus one.
+__device__ __forceinline__ bool nearest_at_vertex(uint32_t depth) {
+    return depth >= 2;
+}
+__device__ __forceinline__ bool nearest_after_bounce(uint32_t depth) {
+    return depth >= 3;
+}
+
 // Density at texture-space point uvw: Linear_3D::sample_1 (texture_sampler.cpp:175-188,
-// map :256-283) or Nearest_3D (:124-172).
-__device__ float sample_density(Medium_gpu const& g, V3 uvw) {
+// map :256-283) or Nearest_3D (:124-172), the latter also where `nearest` overrides the filter.
+__device__ float sample_density(Medium_gpu const& g, V3 uvw, bool nearest = false) {
     bool const  repeat = g.flags & 2u;
     float const u      = address(uvw.x, repeat);
     float const v      = address(uvw.y, repeat);
     float const w      = address(uvw.z, repeat);
-    if (g.flags & 1u) {
+    if ((g.flags & 1u) || nearest) {
         int const x = min(int(u * float(g.nx)), g.nx - 1);
         int const y = min(int(v * float(g.ny)), g.ny - 1);
         int const z = min(int(w * float(g.nz)), g.nz - 1);
@@ -1187,12 +1320,12 @@ __device__ float sample_density(Medium_gpu const& g, V3 uvw) {
 
 // A material texture at uv (Nearest_2D / Linear_2D, texture_sampler.cpp:14-121): uv scaled,
 // wrapped or clamped, then the texel it falls in, or the bilinear blend of the four texels
-// around it (texel centres at half-integer positions).
-__device__ float4 sample_texture(Texture_gpu const& t, float2 uv) {
+// around it (texel centres at half-integer positions); nearest overrides the filter.
+__device__ float4 sample_texture(Texture_gpu const& t, float2 uv, bool nearest = false) {
     bool const  repeat = !(t.flags & 2u);
     float const u      = address(uv.x * t.su, repeat);
     float const v      = address(uv.y * t.sv, repeat);
-    if (t.flags & 1u) {
+    if ((t.flags & 1u) || nearest) {
         int const x = min(int(u * float(t.w)), t.w - 1);
         int const y = min(int(v * float(t.h)), t.h - 1);
         return __ldg(t.texels + size_t(y) * t.w + x);
@@ -1223,15 +1356,15 @@ __device__ float4 sample_texture(Texture_gpu const& t, float2 uv) {
 // (Material_base::set_sample, substitute_base_material.inl:36-96): the colour map replaces the
 // colour; the surface map gives the roughness (mapped to [Min_roughness, 1], ggx.inl:47-49) and,
 // with two channels, the metallic value; albedo and F0 follow from them.
-__device__ void apply_texture_maps(Scene_gpu const& s, shading::Material& m, float2 uv) {
+__device__ void apply_texture_maps(Scene_gpu const& s, shading::Material& m, float2 uv, bool nearest) {
     V3    color    = m.color;
     float metallic = m.metallic;
     if (m.color_map) {
-        float4 const c = sample_texture(s.textures[m.color_map - 1], uv);
+        float4 const c = sample_texture(s.textures[m.color_map - 1], uv, nearest);
         color          = v3(c.x, c.y, c.z);
     }
     if (m.surface_map) {
-        float4 const c = sample_texture(s.textures[m.surface_map - 1], uv);
+        float4 const c = sample_texture(s.textures[m.surface_map - 1], uv, nearest);
         float const  r = c.x * (1.f - shading::Min_roughness) + shading::Min_roughness;
         m.alpha        = r * r;
         if (m.surface_channels >= 2) {
@@ -1324,10 +1457,11 @@ __device__ bool walk_cells(Medium_gpu const& g, V3 o, V3 d, float t0, float t1, 
 // Delta tracking with spectral MIS through a density grid over the world ray (ro, rd) for t in
 // [t0, t1] (Tracking_multi::integrate heterogeneous branch, tracking_multi.cpp:98-164, with
 // Tracking::tracking over a majorant cell, tracking.cpp:286-349).  srs scales the scattering
-// coefficient (similarity relation).  Returns true on a scattering event at t_out; lw receives
-// the path weight either way.
+// coefficient (similarity relation); nearest overrides the grid's filter.  Returns true on a
+// scattering event at t_out; lw receives the path weight either way.
 __device__ bool track_grid(Medium_gpu const& g, shading::Material const& m, float srs, V3 ro,
-                           V3 rd, float t0, float t1, Rng& rng, float& t_out, V3& lw, uint32_t* capped) {
+                           V3 rd, float t0, float t1, bool nearest, Rng& rng, float& t_out, V3& lw,
+                           uint32_t* capped) {
     V3 const    o     = to_texture(g, ro);
     V3 const    d     = to_texture_dir(g, rd);
     V3 const    mu_s  = srs * m.mu_s;
@@ -1346,7 +1480,7 @@ __device__ bool track_grid(Medium_gpu const& g, shading::Material const& m, floa
             if (t > tb) {
                 return false;
             }
-            float const den  = sample_density(g, o + t * d);
+            float const den  = sample_density(g, o + t * d, nearest);
             V3 const    ma   = den * m.mu_a;
             V3 const    ms3  = den * mu_s;
             V3 const    mu_n = v3(mt - (ma.x + ms3.x), mt - (ma.y + ms3.y), mt - (ma.z + ms3.z));
@@ -1375,6 +1509,74 @@ __device__ bool track_grid(Medium_gpu const& g, shading::Material const& m, floa
     return scattered;
 }
 
+// Tracking through an emissive density grid (Grid_emission, volumetric_grid.cpp:110-127, with
+// the emissive Tracking::tracking over a majorant cell, tracking.cpp:351-423): absorption is an
+// event beside scattering and null collisions, each chosen in proportion to its coefficient
+// times the path weight; the absorbed path carries the emission (constant over the grid; the
+// density scales the absorption coefficient).  Returns 2 on absorption at t_out (li the
+// emitted radiance, lw zero), 1 on scattering at t_out, 0 when the segment is passed.
+__device__ int track_grid_emissive(Medium_gpu const& g, shading::Material const& m, float srs, V3 ro, V3 rd,
+                                   float t0, float t1, bool nearest, Rng& rng, float& t_out, V3& lw, V3& li,
+                                   uint32_t* capped) {
+    V3 const    o     = to_texture(g, ro);
+    V3 const    d     = to_texture_dir(g, rd);
+    V3 const    mu_s  = srs * m.mu_s;
+    float const maj_t = shading::max_component(m.mu_a) + shading::max_component(mu_s);
+    lw                = v3(1.f, 1.f, 1.f);
+    li                = v3(0.f, 0.f, 0.f);
+    int steps         = 0;
+    int event         = 0;
+    walk_cells(g, o, d, t0, t1, [&](float2 cell, float ta, float tb) {
+        float const mt = cell.y * maj_t;
+        if (mt < Min_mt) {
+            return false;
+        }
+        float const imt = 1.f / mt;
+        for (float t = ta; steps < Max_tracking_steps; ++steps) {
+            t -= logf(1.f - rng.uniform()) * imt;
+            if (t > tb) {
+                return false;
+            }
+            float const den  = sample_density(g, o + t * d, nearest);
+            V3 const    ma3  = den * m.mu_a;
+            V3 const    ms3  = den * mu_s;
+            V3 const    mu_n = v3(mt - (ma3.x + ms3.x), mt - (ma3.y + ms3.y), mt - (ma3.z + ms3.z));
+            float const ma   = ((ma3.x * lw.x) + (ma3.y * lw.y) + (ma3.z * lw.z)) * (1.f / 3.f);
+            float const ms   = ((ms3.x * lw.x) + (ms3.y * lw.y) + (ms3.z * lw.z)) * (1.f / 3.f);
+            float const mn   = ((mu_n.x * lw.x) + (mu_n.y * lw.y) + (mu_n.z * lw.z)) * (1.f / 3.f);
+            float const sum  = ma + ms + mn;
+            if (!(sum > 0.f)) {
+                lw = v3(0.f, 0.f, 0.f);
+                return true;
+            }
+            float const c  = 1.f / sum;
+            float const pa = ma * c;
+            float const ps = ms * c;
+            float const pn = mn * c;
+            float const r1 = rng.uniform();
+            if (r1 < pa) {
+                li    = lw * ((1.f / (mt * pa)) * ma3) * m.emission;
+                lw    = v3(0.f, 0.f, 0.f);
+                t_out = t;
+                event = 2;
+                return true;
+            }
+            if ((r1 <= 1.f - pn) & (ps > 0.f)) {
+                lw    = lw * ((1.f / (mt * ps)) * ms3);
+                t_out = t;
+                event = 1;
+                return true;
+            }
+            lw = lw * ((1.f / (mt * pn)) * mu_n);
+        }
+        return true;
+    });
+    if (steps >= Max_tracking_steps) {
+        atomicAdd(capped, 1u);
+    }
+    return event;
+}
+
 __device__ __forceinline__ bool all_below_abort(V3 w) {
     return w.x < Abort_epsilon && w.y < Abort_epsilon && w.z < Abort_epsilon;
 }
@@ -1383,9 +1585,10 @@ __device__ __forceinline__ bool all_below_abort(V3 w) {
 // majorant cell, residual ratio tracking against the cell's minorant where it is positive
 // (tracking_transmitted / residual_ratio_tracking_transmitted, tracking.cpp:32-140).  w is
 // multiplied by the estimate; returns false when it falls below Abort_epsilon (the shadow
-// ray counts as blocked, Tracking::transmittance, tracking.cpp:143-180).
+// ray counts as blocked, Tracking::transmittance, tracking.cpp:143-180).  nearest overrides the
+// grid's filter.
 __device__ bool transmit_grid(Medium_gpu const& g, shading::Material const& m, float srs, V3 ro,
-                              V3 rd, float t0, float t1, Rng& rng, V3& w, uint32_t* capped) {
+                              V3 rd, float t0, float t1, bool nearest, Rng& rng, V3& w, uint32_t* capped) {
     V3 const    o     = to_texture(g, ro);
     V3 const    d     = to_texture_dir(g, rd);
     V3 const    mu_s  = srs * m.mu_s;
@@ -1418,7 +1621,7 @@ __device__ bool transmit_grid(Medium_gpu const& g, shading::Material const& m, f
             if (t > tb) {
                 return false;
             }
-            float const den = sample_density(g, o + t * d);
+            float const den = sample_density(g, o + t * d, nearest);
             V3 const    mt3 = den * (m.mu_a + mu_s);
             w = v3(w.x * ((mr - (mt3.x - cm)) * imr), w.y * ((mr - (mt3.y - cm)) * imr),
                    w.z * ((mr - (mt3.z - cm)) * imr));
@@ -1518,7 +1721,7 @@ __device__ __forceinline__ void next_event(Scene_gpu const& s, Paths const& p, W
         float r1, r2;
         point(l, r1, r2);
         Light_sample ls;
-        if (sample_light(s, ps, n, total_sphere, pick_at(l), r1, r2, ls)) {
+        if (sample_light(s, ps, n, total_sphere, pick_at(l), r1, r2, rng, ls)) {
             V3 const c = eval(ls);
             if (shading::max_component(c) > 0.f) {
                 store_shadow(p, path, second, ps, ls, c, depth);
@@ -1550,7 +1753,7 @@ __device__ __forceinline__ void next_event(Scene_gpu const& s, Paths const& p, W
         Light_sample ls;
         V3           c = v3(0.f, 0.f, 0.f);
         float4       d = make_float4(0.f, 0.f, 1.f, 0.f);
-        if (sample_light(s, ps, n, total_sphere, pick_at(first + k), r1, r2, ls)) {
+        if (sample_light(s, ps, n, total_sphere, pick_at(first + k), r1, r2, rng, ls)) {
             V3 const e = eval(ls);
             if (shading::max_component(e) > 0.f) {
                 c = e;
@@ -1872,6 +2075,26 @@ __device__ __forceinline__ float continuation_probability(Wave const& wave, V3 T
     return wave.guiding ? fminf(q, 1.f) : q;
 }
 
+// The pdf with which next-event estimation from the previous vertex would have drawn the point
+// at distance t along the ray inside an emitting medium's light (connect_light_volume,
+// pathtracer_mis.cpp:382-400, with Light::pdf for Volume and Volume_image lights,
+// light.cpp:352-362): the light-tree pick from that vertex times distance^2 / volume, times the
+// voxel's probability and the grid's factor for a density grid.
+__device__ float volume_light_pdf(Scene_gpu const& s, Paths const& p, uint32_t path, shading::Material const& m,
+                                  V3 ro, V3 rd, float t, uint32_t depth) {
+    uint32_t const         order = m.volume_light - 1;
+    float4 const           pn    = p.prev_n[path];
+    float const            pick  = light_pick_pdf(s, ro, f3v(pn), pn.w != 0.f, order, splits_at(s, depth));
+    Volume_light_gpu const vl    = s.volume_lights[uint32_t(-1.f - s.light_tris[3 * order].w)];
+    float                  pdf   = pick * (t * t) / vl.volume;
+    if (vl.dist != 0) {
+        Medium_gpu const& g   = s.media[vl.medium];
+        V3 const          uvw = to_texture(g, ro + t * rd);
+        pdf *= emission_prob(s.emission_dists[vl.dist - 1], uvw) * vl.pdf_factor;
+    }
+    return pdf;
+}
+
 // ---- shade: one path vertex ----
 __global__ void __launch_bounds__(Shade_block)
     k_shade(Scene_gpu s, Launch const* __restrict__ launch, Paths p, uint32_t const* __restrict__ q_in,
@@ -1939,21 +2162,33 @@ __global__ void __launch_bounds__(Shade_block)
         } else if (medium != 0) {
             shading::Material const m = s.materials[medium - 1];
             V3 lw;
-            if (m.medium != 0) {
-                float const srs = shading::similarity_relation_scale(m.g, depth);
-                scatter = track_grid(s.media[m.medium - 1], m, srs, f3v(ro), dir_in, ro.w,
-                                     p.hit_t[path], rng, t_sc, lw, s.tracking_capped);
-            } else if (m.emission.x > 0.f || m.emission.y > 0.f || m.emission.z > 0.f) {
-                // An emissive medium that is not a light: its emission reaches the camera
-                // segment only (pathtracer_mis.cpp:220-229 with connect_light_volume returning
-                // 0 for a non-light, pathtracer_mis.cpp:382-387).
+            bool const emissive = m.emission.x > 0.f || m.emission.y > 0.f || m.emission.z > 0.f;
+            if (emissive) {
+                // An emitting medium: an absorption event ends the path with the emitted
+                // radiance (pathtracer_mis.cpp:214-231).  The camera segment takes all of it;
+                // later segments take it only from a light, weighed against next-event
+                // estimation of that light from the previous vertex (connect_light_volume,
+                // pathtracer_mis.cpp:382-400).
                 V3        li;
-                int const ev = track_homogeneous_emissive(m, ro.w, p.hit_t[path], rng, t_sc, lw, li,
-                                                          s.tracking_capped);
-                if (ev == 2 && depth == 0) {
-                    L = L + T * li;
+                int const ev = m.medium != 0
+                                   ? track_grid_emissive(s.media[m.medium - 1], m,
+                                                         shading::similarity_relation_scale(m.g, depth), f3v(ro),
+                                                         dir_in, ro.w, p.hit_t[path], nearest_after_bounce(depth),
+                                                         rng, t_sc, lw, li, s.tracking_capped)
+                                   : track_homogeneous_emissive(m, ro.w, p.hit_t[path], rng, t_sc, lw, li,
+                                                                s.tracking_capped);
+                if (ev == 2 && (depth == 0 || m.volume_light != 0)) {
+                    float w = 1.f;
+                    if (depth > 0 && !singular && m.volume_light != shading::Volume_light_unsampled) {
+                        w = power_heuristic(bsdf_pdf, volume_light_pdf(s, p, path, m, f3v(ro), dir_in, t_sc, depth));
+                    }
+                    L = L + w * (T * li);
                 }
                 scatter = ev == 1;
+            } else if (m.medium != 0) {
+                float const srs = shading::similarity_relation_scale(m.g, depth);
+                scatter = track_grid(s.media[m.medium - 1], m, srs, f3v(ro), dir_in, ro.w, p.hit_t[path],
+                                     nearest_after_bounce(depth), rng, t_sc, lw, s.tracking_capped);
             } else {
                 scatter = track_homogeneous(m, ro.w, p.hit_t[path], rng, t_sc, lw, s.tracking_capped);
             }
@@ -2021,7 +2256,7 @@ __global__ void __launch_bounds__(Shade_block)
                 float2 const t2  = s.uvs[wt.tri.z];
                 float2 const tuv = make_float2(bw * t0.x + uv.x * t1.x + uv.y * t2.x,
                                                bw * t0.y + uv.x * t1.y + uv.y * t2.y);
-                apply_texture_maps(s, mat, tuv);
+                apply_texture_maps(s, mat, tuv, nearest_at_vertex(depth));
             }
             float const  cos_o = shading::dot(geo_n, wo);
             bool const   front = cos_o > 0.f;
@@ -2243,8 +2478,8 @@ __device__ __forceinline__ bool walk_shadow(Scene_gpu const& s, Paths const& p, 
                     random = true;
                 }
                 float const srs = shading::similarity_relation_scale(m.g, depth);
-                if (!transmit_grid(s.media[m.medium - 1], m, srs, f3v(ro), f3v(rd), t0, end, rng,
-                                   w, s.tracking_capped)) {
+                if (!transmit_grid(s.media[m.medium - 1], m, srs, f3v(ro), f3v(rd), t0, end,
+                                   nearest_at_vertex(depth), rng, w, s.tracking_capped)) {
                     return false;
                 }
             } else {
@@ -2792,7 +3027,7 @@ __global__ void __launch_bounds__(Trace_block)
                 Light_pick              pick[1];
                 if (select_lights(s, pos, v3(0.f, 0.f, 1.f), true, select, false, pick) == 1) {
                     Light_sample ls;
-                    if (sample_light(s, pos, v3(0.f, 0.f, 1.f), true, pick[0], r1, r2, ls)) {
+                    if (sample_light(s, pos, v3(0.f, 0.f, 1.f), true, pick[0], r1, r2, rng, ls)) {
                         float const f = shading::phase_hg(shading::dot(wo, ls.dir), g);
                         float const w = ls.pdf / (ls.pdf * ls.pdf + f * f);
                         spec::V4    tr;
@@ -2899,6 +3134,9 @@ struct Renderer::Device {
     uint32_t             golden_n       = 0;
     std::vector<float*>  grid_density;  // one per density grid
     std::vector<float2*> grid_cells;
+    Volume_light_gpu*    volume_lights  = nullptr;  // emitting media that are lights
+    Emission_dist_gpu*   emission_dists = nullptr;
+    std::vector<float*>  dist_data;  // per emission distribution: prob, cdf_z, cdf_y, cdf_x
     // the light tree's nodes as uploaded, and the splitting threshold their split radii are for
     std::vector<float>   light_tree_nodes;
     float                split_radii_threshold = -1.f;
@@ -3065,6 +3303,81 @@ __global__ void k_majorant_cells(float const* __restrict__ density, int nx, int 
     cells[i] = make_float2(mn, mx);
 }
 
+// The emission distribution of a density grid whose voxels emit density x emission
+// (Grid_emission::prepare_sampling, volumetric_grid.cpp:182-318, built with
+// SU_IBL_MIS_COMPENSATION): voxel weights max(luminance - 0.6 average luminance, 0) (ACEScg
+// luminance) normalised to probabilities, with the cumulative sums over slices, rows and voxels
+// the device draws from (Distribution_3D over Distribution_2D over Distribution_1D).
+struct Emission_dist_host {
+    std::vector<float> data;  // prob (n), cdf_z (nz + 1), cdf_y (nz (ny + 1)), cdf_x (nz ny (nx + 1))
+    uint32_t           dims[3] = {0, 0, 0};
+    bool               repeat  = false;  // the grid's address mode
+    double             average[3] = {0.0, 0.0, 0.0};  // mean emitted radiance over the voxels
+    double             total      = 0.0;              // sum of the weights (0: nothing to draw)
+};
+
+Emission_dist_host emission_distribution(Density_grid const& g, V3 emission) {
+    size_t const nx = g.dims[0], ny = g.dims[1], nz = g.dims[2], n = nx * ny * nz;
+    auto const   lum = [](double r, double gg, double b) {
+        return 0.2722287168 * r + 0.6740817658 * gg + 0.0536895174 * b;
+    };
+    Emission_dist_host  out;
+    std::copy(g.dims, g.dims + 3, out.dims);
+    std::vector<double> w(n);
+    double              sum[3] = {0.0, 0.0, 0.0};
+    for (size_t v = 0; v < n; ++v) {
+        double const d = g.density[v];
+        sum[0] += d * emission.x;
+        sum[1] += d * emission.y;
+        sum[2] += d * emission.z;
+        w[v] = lum(d * emission.x, d * emission.y, d * emission.z);
+    }
+    for (int k = 0; k < 3; ++k) {
+        out.average[k] = sum[k] / double(n);
+    }
+    double const al = 0.6 * lum(out.average[0], out.average[1], out.average[2]);
+    for (double& x : w) {
+        x = std::max(x - al, 0.0);
+        out.total += x;
+    }
+    if (!(out.total > 0.0)) {
+        return out;
+    }
+    out.data.resize(n + (nz + 1) + nz * (ny + 1) + nz * ny * (nx + 1));
+    float* const prob  = out.data.data();
+    float* const cdf_z = prob + n;
+    float* const cdf_y = cdf_z + (nz + 1);
+    float* const cdf_x = cdf_y + nz * (ny + 1);
+    // A running sum normalised by its total, ending at exactly 1 (uniform where the total is 0;
+    // such a range is never drawn).
+    auto const cumulate = [](double const* x, size_t len, double total, float* cdf) {
+        double acc = 0.0;
+        cdf[0]     = 0.f;
+        for (size_t i = 0; i < len; ++i) {
+            acc += x[i];
+            cdf[i + 1] = total > 0.0 ? float(acc / total) : float(double(i + 1) / double(len));
+        }
+        cdf[len] = 1.f;
+    };
+    std::vector<double> slice(nz, 0.0), row(nz * ny, 0.0);
+    for (size_t z = 0; z < nz; ++z) {
+        for (size_t y = 0; y < ny; ++y) {
+            double const* r = &w[(z * ny + y) * nx];
+            double        s = 0.0;
+            for (size_t x = 0; x < nx; ++x) {
+                s += r[x];
+                prob[(z * ny + y) * nx + x] = float(r[x] / out.total);
+            }
+            row[z * ny + y] = s;
+            slice[z] += s;
+            cumulate(r, nx, s, cdf_x + (z * ny + y) * (nx + 1));
+        }
+        cumulate(&row[z * ny], ny, slice[z], cdf_y + z * (ny + 1));
+    }
+    cumulate(slice.data(), nz, out.total, cdf_z);
+    return out;
+}
+
 }  // namespace
 
 void Renderer::free_grids() {
@@ -3077,6 +3390,12 @@ void Renderer::free_grids() {
     d_->grid_density.clear();
     d_->grid_cells.clear();
     free_ptr(d_->media);
+    for (float*& e : d_->dist_data) {
+        free_ptr(e);
+    }
+    d_->dist_data.clear();
+    free_ptr(d_->volume_lights);
+    free_ptr(d_->emission_dists);
 }
 
 Renderer::Renderer() : d_(new Device) {
@@ -3578,9 +3897,105 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
         SPB_RCUDA(upload(d_->inst_trace, trace.data(), trace.size() * sizeof(gpu::Instance_trace)));
     }
 
+    // Emitting media of light props (Scene::create_light, scene.cpp:330-350).  The medium of a
+    // built-in Cube is a light that next-event estimation samples inside (Light::Type::Volume for
+    // a homogeneous medium, Volume_image for a density grid); another shape's medium cannot be
+    // sampled there (Shape::sample_volume fails and pdf_volume is 0 for it), so its emission
+    // counts with weight 1 on every segment, as does that of a light with nothing to draw.
+    std::vector<shading::Material>  materials = scene.materials;
+    std::vector<Volume_light_gpu>   volume_lights;
+    std::vector<Emission_dist_host> dists;
+    for (Instance_desc const& in : scene.instances) {
+        if (!in.light) {
+            continue;
+        }
+        std::vector<uint32_t> slots = scene.meshes[in.mesh].tri_slot;
+        std::sort(slots.begin(), slots.end());
+        slots.erase(std::unique(slots.begin(), slots.end()), slots.end());
+        for (uint32_t const slot : slots) {
+            uint32_t const     mat = material_of(in, slot);
+            shading::Material& m   = materials[mat];
+            if (m.type != shading::Type_volume || !(m.emission.x > 0.f || m.emission.y > 0.f || m.emission.z > 0.f)) {
+                continue;
+            }
+            if (m.volume_light != 0) {
+                error_ = "an emitting medium's material lights more than one prop (each needs its own)";
+                return SPB_ERROR_ARGUMENT;
+            }
+            m.volume_light = shading::Volume_light_unsampled;
+            if (!in.cube) {
+                continue;
+            }
+            float const*     t = in.trafo;
+            Volume_light_gpu vl{};
+            vl.m0 = make_float4(t[0], t[4], t[8], t[12]);
+            vl.m1 = make_float4(t[1], t[5], t[9], t[13]);
+            vl.m2 = make_float4(t[2], t[6], t[10], t[14]);
+            // Cube::volume (cube.cpp:229-232): the cube [-1, 1]^3 scaled
+            double const det = double(t[0]) * (double(t[5]) * t[10] - double(t[6]) * t[9]) -
+                               double(t[1]) * (double(t[4]) * t[10] - double(t[6]) * t[8]) +
+                               double(t[2]) * (double(t[4]) * t[9] - double(t[5]) * t[8]);
+            double const volume = 8.0 * std::fabs(det);
+            vl.volume           = float(volume);
+            vl.material         = mat;
+            // the average radiance its power is taken from (volumetric::Material::prepare_sampling,
+            // volumetric_material.cpp:40-44, or the grid's mean of density x emission)
+            double average[3] = {double(m.mu_a.x) * m.emission.x, double(m.mu_a.y) * m.emission.y,
+                                 double(m.mu_a.z) * m.emission.z};
+            if (m.medium != 0) {
+                Grid_medium const& gm = scene.media[m.medium - 1];
+                double const       maj_a = std::max({double(m.mu_a.x), double(m.mu_a.y), double(m.mu_a.z)});
+                if (!(maj_a > 0.0)) {
+                    continue;  // a medium that absorbs nothing emits nothing
+                }
+                Emission_dist_host d = emission_distribution(scene.grids[gm.grid], m.emission);
+                if (!(d.total > 0.0)) {
+                    continue;
+                }
+                d.repeat            = gm.repeat;
+                double const voxels = double(d.dims[0]) * d.dims[1] * d.dims[2];
+                vl.medium           = m.medium - 1;
+                vl.dist             = uint32_t(dists.size()) + 1;
+                vl.pdf_factor       = float(voxels / maj_a);
+                vl.a_norm = v3(m.mu_a.x > 0.f ? float(maj_a / m.mu_a.x) : 0.f, m.mu_a.y > 0.f ? float(maj_a / m.mu_a.y) : 0.f,
+                               m.mu_a.z > 0.f ? float(maj_a / m.mu_a.z) : 0.f);
+                std::copy(d.average, d.average + 3, average);
+                dists.push_back(std::move(d));
+            }
+            Light_input li;
+            for (int k = 0; k < 3; ++k) {
+                li.a[k] = 1e300;
+                li.b[k] = -1e300;
+            }
+            for (int c = 0; c < 8; ++c) {
+                double const o[3] = {c & 1 ? 1.0 : -1.0, c & 2 ? 1.0 : -1.0, c & 4 ? 1.0 : -1.0};
+                for (int k = 0; k < 3; ++k) {
+                    double const w = o[0] * t[k] + o[1] * t[4 + k] + o[2] * t[8 + k] + t[12 + k];
+                    li.a[k]        = std::min(li.a[k], w);
+                    li.b[k]        = std::max(li.b[k], w);
+                }
+            }
+            for (int k = 0; k < 3; ++k) {
+                li.c[k] = 0.5 * (li.a[k] + li.b[k]);
+            }
+            li.volume    = uint32_t(volume_lights.size()) + 1;
+            li.power     = volume * std::max({average[0], average[1], average[2]});
+            li.two_sided = true;
+            li.slot      = light_slots + uint32_t(volume_lights.size());
+            li.material  = mat;
+            if (volume > 0.0 && li.power > 0.0) {
+                emitters.push_back(li);
+                volume_lights.push_back(vl);
+            }
+        }
+    }
+
     Light_tree tree;
-    build_light_tree(emitters, std::max(light_slots, 1u), tree);
+    build_light_tree(emitters, std::max(light_slots + uint32_t(volume_lights.size()), 1u), tree);
     d_->num_lights = tree.num_lights;
+    for (size_t k = 0; k < volume_lights.size(); ++k) {
+        materials[volume_lights[k].material].volume_light = tree.order[light_slots + k] + 1;
+    }
 
     // Scene box for the guide's position encoding; a new scene starts a new guide.
     {
@@ -3657,8 +4072,7 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     if (!tex_table.empty()) {
         SPB_RCUDA(upload(d_->textures, tex_table.data(), tex_table.size() * sizeof(Texture_gpu)));
     }
-    SPB_RCUDA(upload(d_->materials, scene.materials.data(),
-                     scene.materials.size() * sizeof(shading::Material)));
+    SPB_RCUDA(upload(d_->materials, materials.data(), materials.size() * sizeof(shading::Material)));
     SPB_RCUDA(upload(d_->light_nodes, tree.nodes.data(), tree.nodes.size() * sizeof(float)));
     d_->light_tree_nodes      = tree.nodes;
     d_->split_radii_threshold = -1.f;  // split radii set at the first render
@@ -3712,6 +4126,25 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
         media.push_back(mg);
     }
     SPB_RCUDA(upload(d_->media, media.data(), media.size() * sizeof(Medium_gpu)));
+    // Emitting media that are lights, and the emission distributions of their grids.
+    std::vector<Emission_dist_gpu> dist_table;
+    for (Emission_dist_host const& d : dists) {
+        d_->dist_data.push_back(nullptr);
+        SPB_RCUDA(upload(d_->dist_data.back(), d.data.data(), d.data.size() * sizeof(float)));
+        size_t const      n = size_t(d.dims[0]) * d.dims[1] * d.dims[2];
+        Emission_dist_gpu e{};
+        e.prob   = d_->dist_data.back();
+        e.cdf_z  = e.prob + n;
+        e.cdf_y  = e.cdf_z + (d.dims[2] + 1);
+        e.cdf_x  = e.cdf_y + size_t(d.dims[2]) * (d.dims[1] + 1);
+        e.nx     = int(d.dims[0]);
+        e.ny     = int(d.dims[1]);
+        e.nz     = int(d.dims[2]);
+        e.repeat = d.repeat ? 1u : 0u;
+        dist_table.push_back(e);
+    }
+    SPB_RCUDA(upload(d_->emission_dists, dist_table.data(), dist_table.size() * sizeof(Emission_dist_gpu)));
+    SPB_RCUDA(upload(d_->volume_lights, volume_lights.data(), volume_lights.size() * sizeof(Volume_light_gpu)));
     scene_ready_ = true;
     return SPB_OK;
 }
@@ -4151,6 +4584,8 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     sg.env           = d_->env;
     sg.e_table       = d_->e_table;
     sg.media         = d_->media;
+    sg.volume_lights  = d_->volume_lights;
+    sg.emission_dists = d_->emission_dists;
     sg.inst_trace     = d_->inst_trace;
     sg.inst_shade     = d_->inst_shade;
     sg.inst_materials = d_->inst_materials;

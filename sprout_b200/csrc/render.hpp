@@ -49,7 +49,8 @@ struct Texture_desc {
 
 // A prop: a mesh placed by a row-major object-to-world matrix (translation in the last row, as
 // su_entity_set_transformation takes it; points are row vectors times the matrix), the
-// rotation its normals turn by, its materials per slot, and whether it is a light.
+// rotation its normals turn by, its materials per slot, and whether it is a light.  A light
+// prop's emitting medium needs a material of its own (Material::volume_light names one light).
 struct Instance_desc {
     uint32_t              mesh      = 0;
     float                 trafo[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
@@ -57,6 +58,9 @@ struct Instance_desc {
     std::vector<uint32_t> materials;  // slot -> index into Scene_desc::materials
     uint32_t              fallback  = 0;  // material of slots beyond `materials`
     bool                  light     = false;
+    // The mesh is the built-in Cube, [-1, 1]^3 in object space: an emitting medium inside it is
+    // a light that next-event estimation samples (Cube::sample_volume).
+    bool                  cube      = false;
 };
 
 // The scene as the host engine collects it (prop_bvh_wrapper.cpp, prop.cpp: props placing

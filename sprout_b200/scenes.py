@@ -521,11 +521,15 @@ def _look_at(position, target=(0.0, 0.0, 0.0)):
 
 
 def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -3.2),
-           max_bounces: int = 32, min_bounces: int = 4, environment=(0.3, 0.35, 0.4), integrator=None):
+           max_bounces: int = 32, min_bounces: int = 4, environment=(0.3, 0.35, 0.4), integrator=None,
+           medium=None, medium_light: bool = False, medium_shape: int = SHAPE_CUBE):
     """A 2 m Cube (built-in, [-1, 1]^3) filled with a density grid (VOLUME_MEDIUM), lit by a
     Sphere light of radius 0.25 (radiance 60) and a uniform Infinite_sphere environment; a
     pinhole camera at `position` looking at the centre with a 40 degree field of view; PTMIS
-    with max depth 32.  integrator: further PTMIS keys (e.g. this renderer's "instancing")."""
+    with max depth 32.  integrator: further PTMIS keys (e.g. this renderer's "instancing").
+    medium: Volumetric keys replacing VOLUME_MEDIUM's (e.g. "emission"); density None for a
+    homogeneous medium; medium_light: the medium's prop is a light too (su_create_light);
+    medium_shape: the built-in shape holding the medium (a Sphere has radius 1)."""
     cam = su.su_create_camera_perspective(width, height, VOLUME_FOV)
     su.set_transformation(cam, _look_at(position))
     ptmis = {"min_bounces": min_bounces, "max_bounces": max_bounces}
@@ -533,16 +537,19 @@ def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -
     su.su_create_integrators(json.dumps({"surface": {"PTMIS": ptmis}}).encode())
     su.su_create_sampler(spp)
     su.su_create_defaults()
-    image = su.image(density)
-    medium = _material(su, "Volumetric", density={"id": int(image)}, **VOLUME_MEDIUM)
+    params = dict(VOLUME_MEDIUM)
+    params.update(medium or {})
+    if density is not None:
+        params["density"] = {"id": int(su.image(density))}
+    fill = _material(su, "Volumetric", **params)
     lamp = _material(su, "Light", emission=[60.0, 60.0, 60.0])
     sky = _material(su, "Light", emission=[float(x) for x in environment])
-    for shape, mat, trafo in ((SHAPE_CUBE, medium, np.eye(4, dtype=np.float32)),
+    for shape, mat, trafo in ((medium_shape, fill, np.eye(4, dtype=np.float32)),
                               (SHAPE_SPHERE, lamp, _trafo(0.25, np.eye(3), (1.8, 2.2, -1.6))),
                               (SHAPE_INFINITE_SPHERE, sky, np.eye(4, dtype=np.float32))):
         prop = su.prop(shape, [mat])
         su.set_transformation(prop, trafo)
-        if mat != medium:
+        if mat != fill or medium_light:
             su.su_create_light(prop)
     return cam
 

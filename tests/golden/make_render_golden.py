@@ -39,6 +39,15 @@ GRID_MEDIUM = {"color": [0.9, 0.6, 0.4], "attenuation_distance": 0.03, "anisotro
 EMISSIVE_MEDIUM = {"color": [0.8, 0.8, 0.8], "subsurface_color": [0.3, 0.3, 0.3], "attenuation_distance": 0.1,
                    "anisotropy": 0.3, "emission": [6.0, 3.0, 1.0]}
 
+# The volume workload's density grid emitting (a Grid_emission: emission per unit absorption,
+# the absorption scaling with density), grey absorption; and with colour-dependent absorption,
+# where the light's normalisation by the largest absorption coefficient matters.
+GLOW = {"emission": [3.0, 1.5, 0.6]}
+GLOW_COLOR = {"emission": [3.0, 1.5, 0.6], "attenuation_color": [0.6, 0.4, 0.25]}
+# A thin homogeneous emitting medium.
+HAZE = {"attenuation_color": [0.5, 0.5, 0.5], "subsurface_color": [0.7, 0.7, 0.7], "attenuation_distance": 1.0,
+        "anisotropy": 0.3, "emission": [2.0, 1.0, 0.5]}
+
 # name -> (width, height, spp, scenes.cornell keyword arguments, density grid or None)
 CASES = {
     "cornell64_sub3": (64, 64, 4096, {"sphere_subdivisions": 3}, None),
@@ -60,6 +69,20 @@ CASES = {
     # a 2 m Cube of 32^3 fBm density (mu_t 20 per metre at density 1, albedo 0.9, g 0.6) lit
     # by a Sphere light and the environment, max depth 32
     "volume64": (64, 64, 2048, {"scene": "volume"}, scenes.fbm_density(32)),
+    # the volume's grid emitting: seen by the camera only (the cube is not a light) ...
+    "volume64_glow": (64, 64, 2048, {"scene": "volume", "medium": GLOW}, scenes.fbm_density(32)),
+    # ... and as a light (Volume_image: next-event samples drawn from the emission distribution,
+    # MIS against absorption events), with grey and with coloured absorption
+    "volume64_glow_light": (64, 64, 2048, {"scene": "volume", "medium": GLOW, "medium_light": True},
+                            scenes.fbm_density(32)),
+    "volume64_glow_color_light": (64, 64, 2048, {"scene": "volume", "medium": GLOW_COLOR, "medium_light": True},
+                                  scenes.fbm_density(32)),
+    # a homogeneous emitting cube as a light (Volume: uniform points inside it)
+    "volume64_haze_light": (64, 64, 2048, {"scene": "volume", "medium": HAZE, "medium_light": True}, None),
+    # the emitting grid in a Sphere as a light: next-event estimation cannot sample its inside,
+    # so its emission counts on every segment
+    "volume64_glow_sphere_light": (64, 64, 2048, {"scene": "volume", "medium": GLOW, "medium_light": True,
+                                                  "medium_shape": scenes.SHAPE_SPHERE}, scenes.fbm_density(32)),
     # the guiding workload's room (plain MIS): lit only through a doorway by the environment
     "doorway96": (96, 54, 8192, {"scene": "doorway"}, None),
     # a take file (tests/golden/takes/room.take, written for these tests in the reference's take
@@ -84,7 +107,9 @@ PATH = HERE / "cornell_reference.npz"
 # leave the 2048-spp reference image with 4 % noise in single 8x8 blocks (its 1024- and
 # 2048-spp images differ by that much), 1.6 % in 16x16 blocks; the dense medium 1.7 % and
 # 0.6 %.
-BLOCK = {"wavefront96": 16, "volume64": 16, "doorway96": 16, "doorway320": 20}
+BLOCK = {"wavefront96": 16, "volume64": 16, "doorway96": 16, "doorway320": 20, "volume64_glow": 16,
+         "volume64_glow_light": 16, "volume64_glow_color_light": 16, "volume64_haze_light": 16,
+         "volume64_glow_sphere_light": 16}
 
 
 def build(su, w, h, spp, kwargs, density=None):

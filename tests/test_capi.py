@@ -68,7 +68,8 @@ def test_c_api_without_gpu_state():
 
 def test_density_images_and_grid_materials():
     """su_create_image ids count from 0; a Volumetric "density" must name a one-channel image;
-    "emission" is taken by homogeneous media and refused beside a density grid."""
+    "emission" is taken by homogeneous media and by density grids (Grid_emission); temperature
+    grids are refused."""
     import json
 
     import numpy as np
@@ -92,8 +93,9 @@ def test_density_images_and_grid_materials():
         assert volumetric(density={"id": 1}) == capi.SU_RESOURCE_NULL  # three channels
         assert volumetric(density={"id": 7}) == capi.SU_RESOURCE_NULL  # no such image
         assert volumetric(density={"file": "smoke.sub"}) == capi.SU_RESOURCE_NULL
-        assert volumetric(density={"id": 0}, emission=[1, 1, 1]) == capi.SU_RESOURCE_NULL
-        assert volumetric(emission=[1, 0.5, 0.2], attenuation_distance=0.2) == 2  # homogeneous
+        assert volumetric(density={"id": 0}, emission=[1, 1, 1]) == 2  # an emitting grid
+        assert volumetric(emission=[1, 0.5, 0.2], attenuation_distance=0.2) == 3  # homogeneous
+        assert volumetric(density={"id": 0}, temperature={"id": 0}) == capi.SU_RESOURCE_NULL
     finally:
         assert su.su_release() == 0
 
