@@ -23,6 +23,7 @@
 #include "json.hpp"
 #include "postprocess.hpp"
 #include "render.hpp"
+#include "spectral.cuh"
 
 namespace {
 
@@ -70,9 +71,10 @@ struct Material_maps {
 
 // Host-side part of a Volumetric material with a density grid (Grid, volumetric_grid.cpp).
 struct Grid_ref {
-    uint32_t image   = Null;   // density image id, Null for homogeneous media
-    bool     nearest = false;  // "sampler": {"filter": "Nearest"}
-    bool     repeat  = false;  // "sampler": {"address": "Repeat"}
+    uint32_t image       = Null;   // density image id, Null for homogeneous media
+    uint32_t temperature = Null;   // temperature image id of an emitting grid, or Null
+    bool     nearest     = false;  // "sampler": {"filter": "Nearest"}
+    bool     repeat      = false;  // "sampler": {"address": "Repeat"}
 };
 
 struct Entity {
@@ -477,15 +479,32 @@ int32_t compile_scene() {
                 continue;
             }
             spb::render::Grid_medium gm;
-            auto const gi = std::find(grid_images.begin(), grid_images.end(), gr.image);
-            gm.grid = uint32_t(gi - grid_images.begin());
-            if (gi == grid_images.end()) {
-                Image const&             img = engine->images[gr.image];
+            // index of an image's grid in the scene (each image uploaded once)
+            auto const grid_of = [&](uint32_t image) {
+                auto const gi = std::find(grid_images.begin(), grid_images.end(), image);
+                if (gi != grid_images.end()) {
+                    return uint32_t(gi - grid_images.begin());
+                }
+                Image const&              img = engine->images[image];
                 spb::render::Density_grid g;
                 std::copy(img.dims, img.dims + 3, g.dims);
                 g.density = img.pixels.data();
                 scene.grids.push_back(g);
-                grid_images.push_back(gr.image);
+                grid_images.push_back(image);
+                return uint32_t(grid_images.size() - 1);
+            };
+            gm.grid = grid_of(gr.image);
+            if (gr.temperature != Null) {
+                // Grid_emission::commit (volumetric_grid.cpp:140-160): the emission times the
+                // black-body colour at 16 temperatures from 2000 to 5000 K
+                gm.temperature = grid_of(gr.temperature) + 1;
+                for (int k = 0; k < 16; ++k) {
+                    double c[3];
+                    spb::spectral::blackbody(2000.0 + double(k) / 15.0 * 3000.0, c);
+                    gm.blackbody[3 * k]     = float(em.emission.x * c[0]);
+                    gm.blackbody[3 * k + 1] = float(em.emission.y * c[1]);
+                    gm.blackbody[3 * k + 2] = float(em.emission.z * c[2]);
+                }
             }
             gm.nearest = gr.nearest;
             gm.repeat  = gr.repeat;
@@ -1584,9 +1603,22 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
             }
             grid.image = image;
         }
-        if (desc.find("temperature")) {
-            log(SU_LOG_ERROR, "su_create_material: temperature grids are not supported");
-            return Null;
+        if (spb::json::Value const* temperature = desc.find("temperature")) {
+            // "temperature": a one-channel image of the density's dimensions, looked up through
+            // a black-body table scaled by the emission (Grid_emission, material_provider.cpp:823-830)
+            spb::json::Value const* id   = temperature->is_object() ? temperature->find("id") : nullptr;
+            spb::json::Value const* file = temperature->is_object() ? temperature->find("file") : nullptr;
+            uint32_t const image = id && id->is_number() ? uint32_t(id->number)
+                                   : (file && file->is_string() ? load_sub_image(resolve(file->string, ""))
+                                                                : Null);
+            if (grid.image == Null || image >= engine->images.size() || engine->images[image].channels != 1 ||
+                !std::equal(engine->images[image].dims, engine->images[image].dims + 3,
+                            engine->images[grid.image].dims)) {
+                log(SU_LOG_ERROR, "su_create_material: temperature must name a one-channel image of the "
+                                  "density's dimensions");
+                return Null;
+            }
+            grid.temperature = image;
         }
         // "emission" (material_provider.cpp:805-806): the emitted radiance per unit absorption
         // (Material::collision_coefficients_emission, material.cpp:87-89); with a density grid

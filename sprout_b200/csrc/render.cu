@@ -83,7 +83,23 @@ struct Medium_gpu {
     int           cx, cy, cz;  // majorant cells per axis
     uint32_t      flags;       // bit 0: Nearest filter; bit 1: Repeat address mode
     uint32_t      pad;
+    // An emitting grid's temperature (same dimensions as the density) and the emission at 16
+    // temperatures (Grid_emission's black-body table); null without a temperature grid.
+    float const*  temperature;
+    float4 const* blackbody;
 };
+
+// The emission of a temperature grid's material at temperature x: Grid_emission's table of
+// 16 samples over [0, 1.2] (volumetric_grid.cpp:140-160), x clamped to the range and
+// interpolated linearly (Interpolated_function_1D::operator(), interpolated_function_1d.inl:86-96).
+__host__ __device__ inline V3 blackbody_emission(float4 const* table, float x) {
+    float const    o = fminf(fmaxf(x, 0.f), 1.2f) * 12.5f;
+    uint32_t const i = min(uint32_t(o), 15u);
+    float const    t = o - float(i);
+    float4 const   a = table[i];
+    float4 const   b = table[min(i + 1u, 15u)];
+    return v3(a.x + t * (b.x - a.x), a.y + t * (b.y - a.y), a.z + t * (b.z - a.z));
+}
 
 // A material texture (Texture_desc): texels as float4 (unused components 0), x fastest.
 struct Texture_gpu {
@@ -1057,7 +1073,9 @@ __device__ bool sample_volume_light(Scene_gpu const& s, uint32_t index, V3 ps, V
             return false;
         }
         pdf = prob * vl.pdf_factor;
-        rad = (__ldg(s.media[vl.medium].density + voxel) * vl.a_norm) * lmat.emission;
+        Medium_gpu const& g = s.media[vl.medium];
+        V3 const e = g.temperature ? blackbody_emission(g.blackbody, __ldg(g.temperature + voxel)) : lmat.emission;
+        rad        = (__ldg(g.density + voxel) * vl.a_norm) * e;
     }
     V3 const    o    = v3(2.f * uvw.x - 1.f, 2.f * uvw.y - 1.f, 2.f * uvw.z - 1.f);
     V3 const    wp   = v3(vl.m0.x * o.x + vl.m0.y * o.y + vl.m0.z * o.z + vl.m0.w,
@@ -1270,9 +1288,10 @@ __device__ __forceinline__ bool nearest_after_bounce(uint32_t depth) {
     return depth >= 3;
 }
 
-// Density at texture-space point uvw: Linear_3D::sample_1 (texture_sampler.cpp:175-188,
-// map :256-283) or Nearest_3D (:124-172), the latter also where `nearest` overrides the filter.
-__device__ float sample_density(Medium_gpu const& g, V3 uvw, bool nearest = false) {
+// A value of the grid's voxels at texture-space point uvw: Linear_3D::sample_1
+// (texture_sampler.cpp:175-188, map :256-283) or Nearest_3D (:124-172), the latter also where
+// `nearest` overrides the filter.
+__device__ float sample_voxels(Medium_gpu const& g, float const* __restrict__ voxels, V3 uvw, bool nearest) {
     bool const  repeat = g.flags & 2u;
     float const u      = address(uvw.x, repeat);
     float const v      = address(uvw.y, repeat);
@@ -1281,7 +1300,7 @@ __device__ float sample_density(Medium_gpu const& g, V3 uvw, bool nearest = fals
         int const x = min(int(u * float(g.nx)), g.nx - 1);
         int const y = min(int(v * float(g.ny)), g.ny - 1);
         int const z = min(int(w * float(g.nz)), g.nz - 1);
-        return __ldg(g.density + (size_t(z) * g.ny + y) * g.nx + x);
+        return __ldg(voxels + (size_t(z) * g.ny + y) * g.nx + x);
     }
     float const fu = u * float(g.nx) - 0.5f;
     float const fv = v * float(g.ny) - 0.5f;
@@ -1305,17 +1324,21 @@ __device__ float sample_density(Medium_gpu const& g, V3 uvw, bool nearest = fals
     size_t const p01 = (size_t(z0) * g.ny + y1) * g.nx;
     size_t const p10 = (size_t(z1) * g.ny + y0) * g.nx;
     size_t const p11 = (size_t(z1) * g.ny + y1) * g.nx;
-    float const c0 = __ldg(g.density + p00 + x0);
-    float const c1 = __ldg(g.density + p00 + x1);
-    float const c2 = __ldg(g.density + p01 + x0);
-    float const c3 = __ldg(g.density + p01 + x1);
-    float const c4 = __ldg(g.density + p10 + x0);
-    float const c5 = __ldg(g.density + p10 + x1);
-    float const c6 = __ldg(g.density + p11 + x0);
-    float const c7 = __ldg(g.density + p11 + x1);
+    float const c0 = __ldg(voxels + p00 + x0);
+    float const c1 = __ldg(voxels + p00 + x1);
+    float const c2 = __ldg(voxels + p01 + x0);
+    float const c3 = __ldg(voxels + p01 + x1);
+    float const c4 = __ldg(voxels + p10 + x0);
+    float const c5 = __ldg(voxels + p10 + x1);
+    float const c6 = __ldg(voxels + p11 + x0);
+    float const c7 = __ldg(voxels + p11 + x1);
     float const b0 = (1.f - t) * ((1.f - s) * c0 + s * c1) + t * ((1.f - s) * c2 + s * c3);
     float const b1 = (1.f - t) * ((1.f - s) * c4 + s * c5) + t * ((1.f - s) * c6 + s * c7);
     return (1.f - r) * b0 + r * b1;
+}
+
+__device__ __forceinline__ float sample_density(Medium_gpu const& g, V3 uvw, bool nearest = false) {
+    return sample_voxels(g, g.density, uvw, nearest);
 }
 
 // A material texture at uv (Nearest_2D / Linear_2D, texture_sampler.cpp:14-121): uv scaled,
@@ -1555,7 +1578,10 @@ __device__ int track_grid_emissive(Medium_gpu const& g, shading::Material const&
             float const pn = mn * c;
             float const r1 = rng.uniform();
             if (r1 < pa) {
-                li    = lw * ((1.f / (mt * pa)) * ma3) * m.emission;
+                V3 const e = g.temperature ? blackbody_emission(g.blackbody,
+                                                                sample_voxels(g, g.temperature, o + t * d, nearest))
+                                           : m.emission;
+                li    = lw * ((1.f / (mt * pa)) * ma3) * e;
                 lw    = v3(0.f, 0.f, 0.f);
                 t_out = t;
                 event = 2;
@@ -3137,6 +3163,7 @@ struct Renderer::Device {
     Volume_light_gpu*    volume_lights  = nullptr;  // emitting media that are lights
     Emission_dist_gpu*   emission_dists = nullptr;
     std::vector<float*>  dist_data;  // per emission distribution: prob, cdf_z, cdf_y, cdf_x
+    float4*              blackbody      = nullptr;  // 16 per medium: emission by temperature
     // the light tree's nodes as uploaded, and the splitting threshold their split radii are for
     std::vector<float>   light_tree_nodes;
     float                split_radii_threshold = -1.f;
@@ -3303,8 +3330,9 @@ __global__ void k_majorant_cells(float const* __restrict__ density, int nx, int 
     cells[i] = make_float2(mn, mx);
 }
 
-// The emission distribution of a density grid whose voxels emit density x emission
-// (Grid_emission::prepare_sampling, volumetric_grid.cpp:182-318, built with
+// The emission distribution of a density grid whose voxels emit density x emission, or
+// density x the emission at the voxel's temperature (Grid_emission::prepare_sampling,
+// volumetric_grid.cpp:182-318, built with
 // SU_IBL_MIS_COMPENSATION): voxel weights max(luminance - 0.6 average luminance, 0) (ACEScg
 // luminance) normalised to probabilities, with the cumulative sums over slices, rows and voxels
 // the device draws from (Distribution_3D over Distribution_2D over Distribution_1D).
@@ -3316,7 +3344,8 @@ struct Emission_dist_host {
     double             total      = 0.0;              // sum of the weights (0: nothing to draw)
 };
 
-Emission_dist_host emission_distribution(Density_grid const& g, V3 emission) {
+Emission_dist_host emission_distribution(Density_grid const& g, V3 emission, float const* temperature,
+                                         float4 const* blackbody) {
     size_t const nx = g.dims[0], ny = g.dims[1], nz = g.dims[2], n = nx * ny * nz;
     auto const   lum = [](double r, double gg, double b) {
         return 0.2722287168 * r + 0.6740817658 * gg + 0.0536895174 * b;
@@ -3327,10 +3356,11 @@ Emission_dist_host emission_distribution(Density_grid const& g, V3 emission) {
     double              sum[3] = {0.0, 0.0, 0.0};
     for (size_t v = 0; v < n; ++v) {
         double const d = g.density[v];
-        sum[0] += d * emission.x;
-        sum[1] += d * emission.y;
-        sum[2] += d * emission.z;
-        w[v] = lum(d * emission.x, d * emission.y, d * emission.z);
+        V3 const     e = temperature ? blackbody_emission(blackbody, temperature[v]) : emission;
+        sum[0] += d * e.x;
+        sum[1] += d * e.y;
+        sum[2] += d * e.z;
+        w[v] = lum(d * e.x, d * e.y, d * e.z);
     }
     for (int k = 0; k < 3; ++k) {
         out.average[k] = sum[k] / double(n);
@@ -3396,6 +3426,7 @@ void Renderer::free_grids() {
     d_->dist_data.clear();
     free_ptr(d_->volume_lights);
     free_ptr(d_->emission_dists);
+    free_ptr(d_->blackbody);
 }
 
 Renderer::Renderer() : d_(new Device) {
@@ -3948,7 +3979,14 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
                 if (!(maj_a > 0.0)) {
                     continue;  // a medium that absorbs nothing emits nothing
                 }
-                Emission_dist_host d = emission_distribution(scene.grids[gm.grid], m.emission);
+                std::vector<float4> table(16);
+                for (int k = 0; k < 16; ++k) {
+                    table[k] = make_float4(gm.blackbody[3 * k], gm.blackbody[3 * k + 1], gm.blackbody[3 * k + 2], 0.f);
+                }
+                bool const         hot = gm.temperature != 0;
+                Emission_dist_host d   = emission_distribution(
+                    scene.grids[gm.grid], m.emission, hot ? scene.grids[gm.temperature - 1].density : nullptr,
+                    hot ? table.data() : nullptr);
                 if (!(d.total > 0.0)) {
                     continue;
                 }
@@ -4091,10 +4129,23 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
         SPB_RCUDA(upload(d_->grid_density.back(), g.density, n * sizeof(float)));
     }
     d_->grid_cells.assign(scene.media.size(), nullptr);
+    std::vector<float4> tables(16 * std::max<size_t>(scene.media.size(), 1));
+    for (size_t k = 0; k < scene.media.size(); ++k) {
+        for (int i = 0; i < 16; ++i) {
+            float const* b    = scene.media[k].blackbody + 3 * i;
+            tables[16 * k + i] = make_float4(b[0], b[1], b[2], 0.f);
+        }
+    }
+    SPB_RCUDA(upload(d_->blackbody, tables.data(), tables.size() * sizeof(float4)));
     for (size_t k = 0; k < scene.media.size(); ++k) {
         Grid_medium const& gm = scene.media[k];
-        if (gm.grid >= scene.grids.size()) {
+        if (gm.grid >= scene.grids.size() || gm.temperature > scene.grids.size()) {
             error_ = "medium refers to a missing density grid";
+            return SPB_ERROR_ARGUMENT;
+        }
+        if (gm.temperature != 0 &&
+            !std::equal(scene.grids[gm.grid].dims, scene.grids[gm.grid].dims + 3, scene.grids[gm.temperature - 1].dims)) {
+            error_ = "a temperature grid must have its density grid's dimensions";
             return SPB_ERROR_ARGUMENT;
         }
         Density_grid const& g = scene.grids[gm.grid];
@@ -4114,6 +4165,10 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
         mg.cy    = cells[1];
         mg.cz    = cells[2];
         mg.flags = (gm.nearest ? 1u : 0u) | (gm.repeat ? 2u : 0u);
+        if (gm.temperature != 0) {
+            mg.temperature = d_->grid_density[gm.temperature - 1];
+            mg.blackbody   = d_->blackbody + 16 * k;
+        }
         int const num_cells = cells[0] * cells[1] * cells[2];
         free_ptr(d_->grid_cells[k]);
         SPB_RCUDA(dev_malloc(&d_->grid_cells[k], size_t(num_cells) * sizeof(float2)));

@@ -23,6 +23,12 @@ struct Grid_medium {
     bool     nearest        = false;  // Nearest_3D filter instead of Linear_3D
     bool     repeat         = false;  // Address_mode_repeat instead of clamp
     float    world_to_uvw[12] = {};   // rows: uvw_k = dot(row_k.xyz, p) + row_k.w
+    // An emitting grid's temperature (Grid_emission::set_temperature_map): 1 + index into
+    // Scene_desc::grids of a grid of the density's dimensions, 0 for none; and the material's
+    // emission times the black-body colour at 2000 + 200 k kelvin for k = 0..15 (RGB triples),
+    // looked up by temperature over [0, 1.2] (volumetric_grid.cpp:140-160).
+    uint32_t temperature    = 0;
+    float    blackbody[48]  = {};
 };
 
 // A mesh in object space, shared by the instances that place it.

@@ -68,8 +68,8 @@ def test_c_api_without_gpu_state():
 
 def test_density_images_and_grid_materials():
     """su_create_image ids count from 0; a Volumetric "density" must name a one-channel image;
-    "emission" is taken by homogeneous media and by density grids (Grid_emission); temperature
-    grids are refused."""
+    "emission" is taken by homogeneous media and by density grids (Grid_emission), and a
+    "temperature" image of the density's dimensions beside a density grid."""
     import json
 
     import numpy as np
@@ -95,7 +95,11 @@ def test_density_images_and_grid_materials():
         assert volumetric(density={"file": "smoke.sub"}) == capi.SU_RESOURCE_NULL
         assert volumetric(density={"id": 0}, emission=[1, 1, 1]) == 2  # an emitting grid
         assert volumetric(emission=[1, 0.5, 0.2], attenuation_distance=0.2) == 3  # homogeneous
-        assert volumetric(density={"id": 0}, temperature={"id": 0}) == capi.SU_RESOURCE_NULL
+        assert volumetric(density={"id": 0}, temperature={"id": 0}, emission=[1, 1, 1]) == 4
+        other = np.ones((3, 3, 4), np.float32)
+        assert su.image(other) == 2
+        assert volumetric(density={"id": 0}, temperature={"id": 2}) == capi.SU_RESOURCE_NULL  # other size
+        assert volumetric(temperature={"id": 0}) == capi.SU_RESOURCE_NULL  # no density
     finally:
         assert su.su_release() == 0
 
