@@ -2965,9 +2965,61 @@ __device__ __forceinline__ void spec_splat(float4* film, uint32_t film_base, int
     }
 }
 
+// ---- phase guiding at medium vertices (spectral mode; no counterpart in the reference) ----
+// A grid of cells over the scene box, each with one vMF lobe of the directions radiance
+// arrives from at the medium vertices inside it.  A training pass records, per scattering
+// vertex, the radiance the path later receives through the direction it left by (divided by
+// the throughput up to that direction), and sums weight x direction and weight per cell; a fit
+// turns the sums into a lobe (mean direction; concentration from the mean resultant length,
+// Banerjee et al. 2005).  Guided passes draw the continuation from the lobe with probability
+// `fraction` and from the Henyey-Greenstein phase function otherwise (one-sample MIS: the
+// weight is phase / mixture pdf, and the mixture pdf weighs light hits and next-event
+// estimation), so the estimate stays unbiased whatever the lobes are.
+struct Phase_guide {
+    float4*       sums;    // per cell while training: (sum w d, sum w)
+    uint32_t*     counts;  // per cell while training: directions recorded
+    float4 const* lobes;   // per cell after the fit: (mean direction, kappa); kappa 0: no lobe
+    float4        lo;      // scene box origin
+    float4        scale;   // cells per world unit on each axis
+    int           n;       // cells per axis
+    float         fraction;
+};
+
+constexpr int   Phase_cells      = 32;   // per axis
+constexpr int   Phase_ring       = 3;    // vertices a training path credits
+constexpr int   Phase_min_count  = 16;   // directions a cell needs for a lobe
+constexpr float Phase_kappa_max  = 64.f;
+
+__device__ __forceinline__ uint32_t phase_cell(Phase_guide const& g, V3 p) {
+    int const x = min(max(int((p.x - g.lo.x) * g.scale.x), 0), g.n - 1);
+    int const y = min(max(int((p.y - g.lo.y) * g.scale.y), 0), g.n - 1);
+    int const z = min(max(int((p.z - g.lo.z) * g.scale.z), 0), g.n - 1);
+    return uint32_t((z * g.n + y) * g.n + x);
+}
+
+// One cell's lobe from its sums.
+__global__ void k_phase_fit(Phase_guide g, float4* lobes) {
+    uint32_t const c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= uint32_t(g.n * g.n * g.n)) {
+        return;
+    }
+    float4 const sm = g.sums[c];
+    float4       l  = make_float4(0.f, 0.f, 1.f, 0.f);
+    float const  m  = sqrtf(sm.x * sm.x + sm.y * sm.y + sm.z * sm.z);
+    if (g.counts[c] >= uint32_t(Phase_min_count) && sm.w > 0.f && m > 0.f) {
+        float const r = fminf(m / sm.w, 0.999f);
+        l = make_float4(sm.x / m, sm.y / m, sm.z / m, fminf(r * (3.f - r * r) / (1.f - r * r), Phase_kappa_max));
+    }
+    lobes[c] = l;
+}
+
+// Kinds of spectral launch: plain, training the phase guide, guided by it.
+constexpr int Spectral_plain = 0, Spectral_train = 1, Spectral_guided = 2;
+
+template <int Mode>
 __global__ void __launch_bounds__(Trace_block)
     k_spectral(Scene_gpu s, Launch const* __restrict__ launch, uint64_t total, unsigned long long* next, float4* film,
-               uint32_t* overflow, unsigned long long* counts) {
+               uint32_t* overflow, unsigned long long* counts, Phase_guide guide) {
     Wave const     wave   = launch->wave;
     uint32_t const pixels = launch->pixels;
     uint2          stack[gpu::Stack_size];
@@ -3007,6 +3059,40 @@ __global__ void __launch_bounds__(Trace_block)
         bool           camera  = true;  // no scattering vertex yet
         float          pdf_prev = 0.f;  // phase pdf of the last continuation
         V3             prev_p   = o;    // its vertex
+        // training: the last Phase_ring vertices (newest first), their cell, direction, inverse
+        // throughput and the radiance credited to them
+        uint32_t ring_cell[Phase_ring];
+        V3       ring_dir[Phase_ring];
+        float    ring_inv[Phase_ring];
+        float    ring_acc[Phase_ring];
+        for (int k = 0; k < Phase_ring; ++k) {
+            ring_cell[k] = 0xFFFFFFFFu;
+            ring_dir[k]  = v3(0.f, 0.f, 0.f);
+            ring_inv[k]  = 0.f;
+            ring_acc[k]  = 0.f;
+        }
+        auto const credit = [&](spec::V4 dl) {  // radiance the path received after the ring's vertices
+            if constexpr (Mode == Spectral_train) {
+                float const x = spec::average(dl);
+                for (int k = 0; k < Phase_ring; ++k) {
+                    ring_acc[k] += x * ring_inv[k];
+                }
+            }
+        };
+        auto const deposit = [&](int k) {
+            if constexpr (Mode == Spectral_train) {
+                if (ring_cell[k] != 0xFFFFFFFFu && ring_acc[k] > 0.f && isfinite(ring_acc[k])) {
+                    float* const sm = reinterpret_cast<float*>(guide.sums + ring_cell[k]);
+                    atomicAdd(sm + 0, ring_acc[k] * ring_dir[k].x);
+                    atomicAdd(sm + 1, ring_acc[k] * ring_dir[k].y);
+                    atomicAdd(sm + 2, ring_acc[k] * ring_dir[k].z);
+                    atomicAdd(sm + 3, ring_acc[k]);
+                }
+                if (ring_cell[k] != 0xFFFFFFFFu) {
+                    atomicAdd(guide.counts + ring_cell[k], 1u);
+                }
+            }
+        };
         for (int seg = 0; seg < 1024; ++seg) {
             ++segments;
             gpu::Ray_state r;
@@ -3037,7 +3123,9 @@ __global__ void __launch_bounds__(Trace_block)
                     break;
                 }
                 if (depth >= wave.min_bounces) {
-                    float const q = spec::maximum(T);
+                    // unbiased Russian roulette: a throughput above 1 (spectral MIS and guide
+                    // weights can reach it) always continues
+                    float const q = fminf(spec::maximum(T), 1.f);
                     if (rng.uniform() > q) {
                         break;
                     }
@@ -3047,6 +3135,17 @@ __global__ void __launch_bounds__(Trace_block)
                 float const             g   = shading::van_de_hulst_anisotropy(m.g, depth);
                 V3 const                pos = o + t_sc * d;
                 V3 const                wo  = -d;
+                // the cell's lobe and its share of the continuation (guided launches)
+                guide::Lobe lobe{v3(0.f, 0.f, 1.f), 0.f, 0.f};
+                if constexpr (Mode == Spectral_guided) {
+                    float4 const l = guide.lobes[phase_cell(guide, pos)];
+                    if (l.w > 0.f) {
+                        lobe = guide::Lobe{v3(l.x, l.y, l.z), l.w, guide.fraction};
+                    }
+                }
+                auto const mixture = [&](V3 wi, float f) {  // pdf of the continuation proposal
+                    return lobe.weight > 0.f ? (1.f - lobe.weight) * f + lobe.weight * guide::vmf_pdf(lobe, wi) : f;
+                };
                 float const             select = rng.uniform();
                 float const             r1     = rng.uniform();
                 float const             r2     = rng.uniform();
@@ -3054,21 +3153,55 @@ __global__ void __launch_bounds__(Trace_block)
                 if (select_lights(s, pos, v3(0.f, 0.f, 1.f), true, select, false, pick) == 1) {
                     Light_sample ls;
                     if (sample_light(s, pos, v3(0.f, 0.f, 1.f), true, pick[0], r1, r2, rng, ls)) {
-                        float const f = shading::phase_hg(shading::dot(wo, ls.dir), g);
-                        float const w = ls.pdf / (ls.pdf * ls.pdf + f * f);
+                        float const f  = shading::phase_hg(shading::dot(wo, ls.dir), g);
+                        float const pc = mixture(ls.dir, f);
+                        float const w  = ls.pdf / (ls.pdf * ls.pdf + pc * pc);
                         spec::V4    tr;
                         ++shadows;
                         if (spec_transmit(s, pos, ls.dir, ls.dist, medium, depth, lambdas, rng, stack, overflow, tr)) {
-                            L = spec::add(L, spec::mul(spec::scale(w * f, T), spec::mul(tr, spec_of(ls.radiance, lambdas))));
+                            spec::V4 const dl =
+                                spec::mul(spec::scale(w * f, T), spec::mul(tr, spec_of(ls.radiance, lambdas)));
+                            L = spec::add(L, dl);
+                            credit(dl);
                         }
                     }
                 }
-                float    pdf;
-                V3 const wi = shading::sample_hg(wo, g, rng.uniform(), rng.uniform(), pdf);
+                float       pdf;
+                bool const  from_lobe = lobe.weight > 0.f && rng.uniform() < lobe.weight;
+                float const x0        = rng.uniform();
+                float const x1        = rng.uniform();
+                V3          wi;
+                if (from_lobe) {
+                    wi = guide::vmf_sample(lobe, x0, x1);
+                    pdf = shading::phase_hg(shading::dot(wo, wi), g);
+                } else {
+                    wi = shading::sample_hg(wo, g, x0, x1, pdf);
+                }
+                float const pm = mixture(wi, pdf);  // pdf is the phase value here
+                if (!(pm > 0.f)) {
+                    break;
+                }
+                T = spec::scale(pdf / pm, T);
+                if constexpr (Mode == Spectral_train) {
+                    deposit(Phase_ring - 1);
+                    for (int k = Phase_ring - 1; k > 0; --k) {
+                        ring_cell[k] = ring_cell[k - 1];
+                        ring_dir[k]  = ring_dir[k - 1];
+                        ring_inv[k]  = ring_inv[k - 1];
+                        ring_acc[k]  = ring_acc[k - 1];
+                    }
+                    // the incident radiance along wi, importance-weighted by 1 / pdf of the phase
+                    // sample, so that the lobe follows the radiance rather than the phase function
+                    float const tavg = spec::average(T);
+                    ring_cell[0] = phase_cell(guide, pos);
+                    ring_dir[0]  = wi;
+                    ring_inv[0]  = tavg > 0.f && pdf > 0.f ? 1.f / (tavg * pdf) : 0.f;
+                    ring_acc[0]  = 0.f;
+                }
                 o        = pos;
                 d        = wi;
                 tmin     = 0.f;
-                pdf_prev = pdf;
+                pdf_prev = pm;
                 prev_p   = pos;
                 camera   = false;
                 ++depth;
@@ -3082,7 +3215,9 @@ __global__ void __launch_bounds__(Trace_block)
                     if (!camera) {
                         w = power_heuristic(pdf_prev, s.env.w * (1.f / (4.f * shading::Pi)));
                     }
-                    L = spec::add(L, spec::scale(w, spec::mul(T, spec_of(v3(s.env.x, s.env.y, s.env.z), lambdas))));
+                    spec::V4 const dl = spec::scale(w, spec::mul(T, spec_of(v3(s.env.x, s.env.y, s.env.z), lambdas)));
+                    L                 = spec::add(L, dl);
+                    credit(dl);
                 }
                 break;
             }
@@ -3103,7 +3238,9 @@ __global__ void __launch_bounds__(Trace_block)
                         float const pdf_l = pick * (t * t) / (fabsf(cos_o) * area);
                         w                 = power_heuristic(pdf_prev, pdf_l);
                     }
-                    L = spec::add(L, spec::scale(w, spec::mul(T, spec_of(mat.emission, lambdas))));
+                    spec::V4 const dl = spec::scale(w, spec::mul(T, spec_of(mat.emission, lambdas)));
+                    L                 = spec::add(L, dl);
+                    credit(dl);
                 }
                 break;
             }
@@ -3113,6 +3250,9 @@ __global__ void __launch_bounds__(Trace_block)
             tmin   = offset_f(r.tbest);
         }
         spec_splat(film, launch->film_offsets[view], int(cam.w), int(cam.h), px, py, u, v, spec_readout(L, lambdas));
+        for (int k = 0; k < Phase_ring; ++k) {
+            deposit(k);
+        }
     }
     atomicAdd(counts, segments);
     atomicAdd(counts + 1, shadows);
@@ -3164,6 +3304,9 @@ struct Renderer::Device {
     Emission_dist_gpu*   emission_dists = nullptr;
     std::vector<float*>  dist_data;  // per emission distribution: prob, cdf_z, cdf_y, cdf_x
     float4*              blackbody      = nullptr;  // 16 per medium: emission by temperature
+    float4*              phase_sums     = nullptr;  // spectral mode's phase guide (Phase_guide)
+    uint32_t*            phase_counts   = nullptr;
+    float4*              phase_lobes    = nullptr;
     // the light tree's nodes as uploaded, and the splitting threshold their split radii are for
     std::vector<float>   light_tree_nodes;
     float                split_radii_threshold = -1.f;
@@ -3534,6 +3677,9 @@ Renderer::~Renderer() {
     free_ptr(d_->out);
     free_ptr(d_->cams);
     free_ptr(d_->spectral_work);
+    free_ptr(d_->phase_sums);
+    free_ptr(d_->phase_counts);
+    free_ptr(d_->phase_lobes);
     free_ptr(d_->view_offsets);
     free_ptr(d_->film_offsets);
     if (d_->stream) {
@@ -4600,11 +4746,8 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         d_->split_radii_threshold = settings_.split_threshold;
     }
     if (settings_.spectral) {
-        // the persistent spectral kernel keeps its paths in registers: no wave buffers
-        if (settings_.guiding) {
-            error_ = "spectral rendering has no path guiding";
-            return SPB_ERROR_ARGUMENT;
-        }
+        // the persistent spectral kernel keeps its paths in registers: no wave buffers; its
+        // guiding is the phase guide at medium vertices
         if (!d_->spectral_scene || d_->instanced) {
             error_ = "spectral rendering takes scenes of participating media (not emissive), emitters and the "
                      "environment, in one tree";
@@ -4616,12 +4759,11 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
     } else if (int32_t const st = ensure_buffers(max_wave * pixels, picks_per_path)) {
         return st;
     }
-    if (settings_.guiding) {
+    if (settings_.guiding && !settings_.spectral) {
         if (int32_t const st = ensure_guide(max_wave * pixels)) {
             return st;
         }
     }
-
 
     Scene_gpu sg;
     sg.nodes         = d_->nodes;
@@ -4946,24 +5088,70 @@ int32_t Renderer::render_spectral(void const* scene, uint32_t first_sample, uint
         SPB_RCUDA(dev_malloc(&d_->launch_dev, sizeof(Launch)));
         SPB_RCUDA(cudaMallocHost(&d_->launch_host, sizeof(Launch)));
     }
-    Wave wave{first_sample, num_samples, settings_.seed, settings_.min_bounces, settings_.max_bounces};
+    // With guiding, the first guide_train_spp samples (at most half of the call's) train the
+    // phase guide, a fit turns its sums into lobes, and the rest are guided by them.
+    uint32_t const cells = uint32_t(Phase_cells) * Phase_cells * Phase_cells;
+    uint32_t const train = settings_.guiding ? std::min(std::max(settings_.guide_train_spp, 1u), num_samples / 2) : 0u;
+    Phase_guide    pg{};
+    if (train != 0) {
+        if (!d_->phase_sums) {
+            SPB_RCUDA(dev_malloc(&d_->phase_sums, cells * sizeof(float4)));
+            SPB_RCUDA(dev_malloc(&d_->phase_counts, cells * sizeof(uint32_t)));
+            SPB_RCUDA(dev_malloc(&d_->phase_lobes, cells * sizeof(float4)));
+        }
+        SPB_RCUDA(cudaMemsetAsync(d_->phase_sums, 0, cells * sizeof(float4), st));
+        SPB_RCUDA(cudaMemsetAsync(d_->phase_counts, 0, cells * sizeof(uint32_t), st));
+        pg.sums     = d_->phase_sums;
+        pg.counts   = d_->phase_counts;
+        pg.lobes    = d_->phase_lobes;
+        pg.lo       = d_->bounds_lo;
+        pg.scale    = make_float4(d_->bounds_inv.x * Phase_cells, d_->bounds_inv.y * Phase_cells,
+                                  d_->bounds_inv.z * Phase_cells, 0.f);
+        pg.n        = Phase_cells;
+        pg.fraction = settings_.guide_fraction;
+    }
+    SPB_RCUDA(cudaMemsetAsync(d_->spectral_work, 0, 4 * sizeof(unsigned long long), st));
+    SPB_RCUDA(cudaMemsetAsync(d_->counters, 0, Counter_words * sizeof(uint32_t), st));
     d_->launch_host->cams         = d_->cams;
     d_->launch_host->view_offsets = d_->view_offsets;
     d_->launch_host->film_offsets = d_->film_offsets;
     d_->launch_host->num_views    = d_->num_views;
     d_->launch_host->pixels       = d_->traced_pixels;
-    d_->launch_host->wave         = wave;
-    SPB_RCUDA(cudaMemcpyAsync(d_->launch_dev, d_->launch_host, sizeof(Launch), cudaMemcpyHostToDevice, st));
-    SPB_RCUDA(cudaMemsetAsync(d_->spectral_work, 0, 4 * sizeof(unsigned long long), st));
-    SPB_RCUDA(cudaMemsetAsync(d_->counters, 0, Counter_words * sizeof(uint32_t), st));
+    // One persistent launch over samples [first, first + count) of every pixel of every view.
+    auto const launch = [&](int mode, uint32_t first, uint32_t count) -> int32_t {
+        // the launch block's pinned copy is free once the previous launch's copy has run
+        SPB_RCUDA(cudaStreamSynchronize(st));
+        d_->launch_host->wave = Wave{first, count, settings_.seed, settings_.min_bounces, settings_.max_bounces};
+        SPB_RCUDA(cudaMemcpyAsync(d_->launch_dev, d_->launch_host, sizeof(Launch), cudaMemcpyHostToDevice, st));
+        SPB_RCUDA(cudaMemsetAsync(d_->spectral_work, 0, sizeof(unsigned long long), st));
+        uint64_t const n      = uint64_t(d_->traced_pixels) * count;
+        int            per_sm = 0;
+        auto const     kernel = mode == Spectral_train ? k_spectral<Spectral_train>
+                                : mode == Spectral_guided ? k_spectral<Spectral_guided>
+                                                          : k_spectral<Spectral_plain>;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, Trace_block, 0);
+        uint32_t const grid = uint32_t(std::max(1, per_sm)) * d_->sms;
+        kernel<<<grid, Trace_block, 0, st>>>(sg, d_->launch_dev, n, d_->spectral_work, d_->film,
+                                             d_->counters + Overflow_slot, d_->spectral_work + 2, pg);
+        SPB_RCUDA(cudaGetLastError());
+        return SPB_OK;
+    };
     uint64_t const total = uint64_t(d_->traced_pixels) * num_samples;
-    int            per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spectral, Trace_block, 0);
-    uint32_t const grid = uint32_t(std::max(1, per_sm)) * d_->sms;
     SPB_RCUDA(cudaEventRecord(d_->ev0, st));
-    k_spectral<<<grid, Trace_block, 0, st>>>(sg, d_->launch_dev, total, d_->spectral_work, d_->film,
-                                              d_->counters + Overflow_slot, d_->spectral_work + 2);
-    SPB_RCUDA(cudaGetLastError());
+    if (train == 0) {
+        if (int32_t const e = launch(Spectral_plain, first_sample, num_samples)) {
+            return e;
+        }
+    } else {
+        if (int32_t const e = launch(Spectral_train, first_sample, train)) {
+            return e;
+        }
+        k_phase_fit<<<(cells + 255) / 256, 256, 0, st>>>(pg, d_->phase_lobes);
+        SPB_RCUDA(cudaGetLastError());
+        if (int32_t const e = launch(Spectral_guided, first_sample + train, num_samples - train)) {
+            return e;
+        }
+    }
     SPB_RCUDA(cudaEventRecord(d_->ev1, st));
     unsigned long long counts[4];
     uint32_t           host_ctr[4];

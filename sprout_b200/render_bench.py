@@ -150,6 +150,53 @@ VOLUME_CONFIG = ("2 m cube of 256^3 fBm density (5 octaves, seed 4), mu_t 20 per
                  "RGB delta/ratio tracking (the reference's transport; no hero wavelengths)")
 
 
+def measure_phase_guiding(side=256, spp=128, ref_spp=8192, fractions=(0.5,)):
+    """The phase guide of the spectral mode on the volume workload's first view (side x side):
+    plain and guided renders of spp samples per pixel against a plain render of ref_spp, each
+    with its relMSE (mean over pixels and channels of (x - r)^2 / (r^2 + 1e-2)) and device
+    seconds; efficiency = (relMSE x seconds) of plain / that of guided (above 1: guiding pays).
+    fractions: the guide's shares of the continuation to try (PTMIS "guiding": {"fraction"})."""
+    lib = _lib.load()
+    stats = _lib.RenderStats()
+    density = scenes.fbm_density(256)
+    position, _ = scenes.volume_views()[0]
+    su = capi.SuLibrary()
+    assert su.su_init(False) == 0
+    out = {"workload": "volume, spectral mode, phase guiding",
+           "config": f"{VOLUME_CONFIG.split('; RGB')[0]}; hero-wavelength spectral mode; first view at "
+                     f"{side}x{side}, {spp} spp; reference {ref_spp} spp plain"}
+    try:
+        scenes.volume(su, side, side, spp, density, position=position)
+
+        def frame(n, guiding):
+            ptmis = {"min_bounces": 4, "max_bounces": 32, "spectral": True}
+            if guiding is not None:
+                ptmis["guiding"] = guiding
+            assert su.su_create_integrators(json.dumps({"surface": {"PTMIS": ptmis}}).encode()) == 0
+            assert su.su_create_sampler(n) == 0
+            assert su.su_render_frame(0) == 0, su.messages
+            assert su.su_postprocess() == 0
+            img = su.framebuffer(side, side)[0][:, :, :3].copy()
+            assert lib.spb_render_last_stats(ctypes.byref(stats)) == 0
+            return img, stats.device_seconds
+
+        ref, ref_s = frame(ref_spp, None)
+        frame(spp, None)  # warm-up
+        plain, plain_s = frame(spp, None)
+        e_plain = rel_mse(plain, ref)
+        out["plain"] = {"rel_mse": round(e_plain, 6), "device_seconds": round(plain_s, 4)}
+        out["reference_device_seconds"] = round(ref_s, 3)
+        for f in fractions:
+            img, sec = frame(spp, {"fraction": f})
+            e = rel_mse(img, ref)
+            out[f"guided_{f}"] = {"rel_mse": round(e, 6), "device_seconds": round(sec, 4),
+                                  "mean_ratio": [round(float(x), 4) for x in img.mean((0, 1)) / ref.mean((0, 1))],
+                                  "efficiency": round(e_plain * plain_s / (e * sec), 3)}
+    finally:
+        su.su_release()
+    return out
+
+
 def measure_volume(views=4, spp=128, cpu_reference=False, batch=True, spectral=True):
     """The heterogeneous-volume workload: the first `views` of scenes.volume_views() (seeded
     camera positions, image sides U[256, 1024]) of one scene, built and uploaded once; each

@@ -2,7 +2,8 @@
 which renders RGB): checked against its FP64 CPU restatement (oracle/spectral_oracle.c, an
 independent estimator of the same image: one wavelength per path, global-majorant tracking,
 its own light choice), against the RGB renderer on a grey scene (where the upsampling basis
-reads back exactly), and for the view batch (each view traces the paths it traces alone).
+reads back exactly), and for the view batch (each view traces the paths it traces alone); also
+with the phase guide at medium vertices.
 
 Statistical bounds: image means per channel within 1 %; 4x4-pixel block means within 5 %
 (the oracle's own noise at 16,384 samples per pixel is about 2 %); relMSE (mean over pixels and
@@ -61,6 +62,15 @@ def assert_close(img, ref):
 def test_spectral_mode_matches_its_oracle():
     """A chromatic density-grid medium, a coloured sphere light and a blue environment."""
     img, desc = render(16384)
+    ref = oracle.spectral_render(desc, 16384)
+    assert_close(img, ref)
+
+
+def test_phase_guided_spectral_mode_matches_its_oracle():
+    """The same scene with the phase guide (PTMIS "guiding" in spectral mode): the first 16 spp
+    train it, the rest draw continuations from its lobes or the phase function (one-sample MIS),
+    so the image still matches the oracle's."""
+    img, desc = render(16384, integrator={"guiding": True})
     ref = oracle.spectral_render(desc, 16384)
     assert_close(img, ref)
 
