@@ -305,8 +305,9 @@ def run_reference_arm(args, world, rank):
 def measure_render(args, with_cpu):
     """Plain MIS path tracing through the su_* C API: the Cornell scene (512x512, 64 spp, with
     time to relMSE 0.01), the many-instances, many-lights scene (1920x1080, 256 spp, depth 12;
-    one warm-up frame, one timed frame), the heterogeneous volume (64 views, 128 spp) and the
-    doorway interior's time to relMSE 0.01, plain MIS against learned guiding (1280x720)."""
+    one warm-up frame, one timed frame), the heterogeneous volume (64 views, 128 spp; and the
+    spectral mode's phase guiding against plain on its first view) and the doorway interior's
+    time to relMSE 0.01, plain MIS against learned guiding (1280x720)."""
     from sprout_b200 import render_bench
 
     out = {"cornell": render_bench.measure("cornell", spp=args.render_spp, frames=3, convergence=True,
@@ -316,6 +317,7 @@ def measure_render(args, with_cpu):
         out["wavefront_flat"] = render_bench.measure("wavefront_flat", frames=1)
     if not args.no_volume:
         out["volume"] = render_bench.measure_volume(views=64, spp=128, cpu_reference=with_cpu)
+        out["volume"]["phase_guiding"] = render_bench.measure_phase_guiding(fractions=(0.1, 0.25))
     if not args.no_guiding:
         out["guiding"] = render_bench.measure_guiding()
     return out
