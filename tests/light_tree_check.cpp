@@ -8,7 +8,9 @@
 //     (and variance + mean^2) and node light count their number;
 //   - a splitting walk returns at most Max_light_picks lights (max_split_picks);
 //   - a node's bounding sphere contains its lights' triangles and its cone contains their
-//     normals (cos spread -1 when a two-sided light is below).
+//     normals (cos spread -1 when a two-sided light is below);
+//   - an emitting medium's light (a box, Light_input::volume != 0) is stored as
+//     (centre, -volume) with cone spread -1, a triangle with its (non-negative) area.
 // Prints "ok <name> <nodes> <depth> <most picks>" per tree or the first violation, and exits
 // non-zero on failure.
 #include <cmath>
@@ -164,6 +166,12 @@ bool check(std::vector<Light_input> const& in, uint32_t num_triangles, char cons
         uint32_t const slot     = (material - 5u) / 2u;
         if (material != 2u * slot + 5u || slot >= num_triangles || t.order[slot] != o) {
             k.fail("order", uint32_t(o));
+            break;
+        }
+        Light_input const& li = in[k.by_tri[slot]];
+        float const        w  = t.tris[12 * o + 3];
+        if (li.volume != 0 ? (w != -float(li.volume) || t.cones[12 * o + 7] != -1.f) : !(w >= 0.f)) {
+            k.fail("volume or triangle entry", uint32_t(o));
         }
     }
     uint32_t const picks = spb::render::max_split_picks(t, 0);
@@ -198,8 +206,16 @@ std::vector<Light_input> emitters(int n, int kind, uint32_t seed) {
         if (kind == 1) {
             l.a[2] = l.b[2] = l.c[2] = 2.0;  // coplanar, identical normals
         }
+        if (kind == 4 && i % 5 == 2) {  // an emitting medium's box among the triangles
+            for (int k = 0; k < 3; ++k) {
+                l.a[k] = c[k] - 0.3;
+                l.b[k] = c[k] + 0.3;
+                l.c[k] = c[k];
+            }
+            l.volume = uint32_t(i / 5) + 1;
+        }
         l.power     = std::exp(4.0 * u(g));
-        l.two_sided = (i % 7) == 3;
+        l.two_sided = (i % 7) == 3 || l.volume != 0;
         l.slot      = uint32_t(3 * i + 1);
         l.material  = 2u * l.slot + 5u;
         v.push_back(l);
@@ -217,5 +233,6 @@ int main() {
     ok &= check(emitters(1000, 1, 4), 3 * 1000 + 2, "coplanar");
     ok &= check(emitters(999, 2, 5), 3 * 999 + 2, "clusters");
     ok &= check(emitters(300, 3, 6), 3 * 300 + 2, "points");
+    ok &= check(emitters(500, 4, 7), 3 * 500 + 2, "volumes");
     return ok ? 0 : 1;
 }

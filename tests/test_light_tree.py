@@ -18,4 +18,4 @@ def test_light_tree_invariants(tmp_path):
                     str(ROOT / "sprout_b200" / "csrc" / "light_tree.cpp"), "-o", str(exe)], check=True)
     res = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert res.returncode == 0, res.stdout + res.stderr
-    assert res.stdout.count("ok ") == 6, res.stdout
+    assert res.stdout.count("ok ") == 7, res.stdout
