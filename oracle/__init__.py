@@ -271,11 +271,13 @@ class ScriptRecorder:
 
     def image(self, pixels):
         """su_create_image of a float32 array (depth, height, width) or (height, width): one
-        channel.  Returns the image id the reference assigns (images are numbered from 0)."""
+        channel; (depth, height, width, channels): several.  Returns the image id the reference
+        assigns (images are numbered from 0)."""
         a = np.ascontiguousarray(pixels, np.float32)
-        d, h, w = (a.shape if a.ndim == 3 else (1,) + a.shape)
+        c = a.shape[3] if a.ndim == 4 else 1
+        d, h, w = (a.shape[:3] if a.ndim >= 3 else (1,) + a.shape)
         off = self._blob(a)
-        self.lines.append(f"image 2 1 {w} {h} {d} {off}")
+        self.lines.append(f"image 2 {c} {w} {h} {d} {off}")
         self.n["image"] += 1
         return self.n["image"] - 1
 

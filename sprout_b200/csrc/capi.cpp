@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <list>
 #include <map>
 #include <memory>
 #include <string>
@@ -350,7 +351,8 @@ int32_t compile_scene() {
     fallback.f0       = V3{0.03497f, 0.03497f, 0.03497f};
     uint32_t const fallback_id = uint32_t(scene.materials.size());
     scene.materials.push_back(fallback);
-    std::vector<uint32_t> grid_images;  // image id of each scene.grids entry
+    std::vector<uint64_t> grid_images;  // image id << 2 | channel of each scene.grids entry
+    std::list<std::vector<float>> grid_channels;  // one channel of a multi-channel image, until uploaded
     std::map<uint32_t, uint32_t> scene_mesh;  // engine shape id -> scene mesh index
 
     // Texture maps: each (image, use, sampler, scale) once, its texels decoded for the use.
@@ -479,25 +481,39 @@ int32_t compile_scene() {
                 continue;
             }
             spb::render::Grid_medium gm;
-            // index of an image's grid in the scene (each image uploaded once)
-            auto const grid_of = [&](uint32_t image) {
-                auto const gi = std::find(grid_images.begin(), grid_images.end(), image);
+            // index of the grid of an image's channel in the scene (each uploaded once; the
+            // channels of a two-channel image as separate grids)
+            auto const grid_of = [&](uint32_t image, uint32_t channel) {
+                uint64_t const key = (uint64_t(image) << 2) | channel;
+                auto const     gi  = std::find(grid_images.begin(), grid_images.end(), key);
                 if (gi != grid_images.end()) {
                     return uint32_t(gi - grid_images.begin());
                 }
                 Image const&              img = engine->images[image];
                 spb::render::Density_grid g;
                 std::copy(img.dims, img.dims + 3, g.dims);
-                g.density = img.pixels.data();
+                if (img.channels == 1) {
+                    g.density = img.pixels.data();
+                } else {
+                    size_t const n = size_t(img.dims[0]) * img.dims[1] * img.dims[2];
+                    grid_channels.emplace_back(n);
+                    for (size_t v = 0; v < n; ++v) {
+                        grid_channels.back()[v] = img.pixels[v * img.channels + channel];
+                    }
+                    g.density = grid_channels.back().data();
+                }
                 scene.grids.push_back(g);
-                grid_images.push_back(image);
+                grid_images.push_back(key);
                 return uint32_t(grid_images.size() - 1);
             };
-            gm.grid = grid_of(gr.image);
+            gm.grid = grid_of(gr.image, 0);
+            if (engine->images[gr.image].channels == 2) {
+                gm.emission_scale = grid_of(gr.image, 1) + 1;
+            }
             if (gr.temperature != Null) {
                 // Grid_emission::commit (volumetric_grid.cpp:140-160): the emission times the
                 // black-body colour at 16 temperatures from 2000 to 5000 K
-                gm.temperature = grid_of(gr.temperature) + 1;
+                gm.temperature = grid_of(gr.temperature, 0) + 1;
                 for (int k = 0; k < 16; ++k) {
                     double c[3];
                     spb::spectral::blackbody(2000.0 + double(k) / 15.0 * 3000.0, c);
@@ -1597,8 +1613,11 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
             uint32_t const image = id && id->is_number() ? uint32_t(id->number)
                                    : (file && file->is_string() ? load_sub_image(resolve(file->string, ""))
                                                                 : Null);
-            if (image >= engine->images.size() || engine->images[image].channels != 1) {
-                log(SU_LOG_ERROR, "su_create_material: density must name a one-channel image id");
+            // one channel, or two: density and emission scale (Grid_emission with a
+            // two-channel density, volumetric_grid.cpp:80-127)
+            if (image >= engine->images.size() || engine->images[image].channels > 2 ||
+                engine->images[image].dims[2] < 1) {
+                log(SU_LOG_ERROR, "su_create_material: density must name a one- or two-channel image id");
                 return Null;
             }
             grid.image = image;

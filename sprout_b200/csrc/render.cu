@@ -87,6 +87,8 @@ struct Medium_gpu {
     // temperatures (Grid_emission's black-body table); null without a temperature grid.
     float const*  temperature;
     float4 const* blackbody;
+    // A two-channel density's second channel, scaling the emission; null for one channel.
+    float const*  scale;
 };
 
 // The emission of a temperature grid's material at temperature x: Grid_emission's table of
@@ -1074,8 +1076,9 @@ __device__ bool sample_volume_light(Scene_gpu const& s, uint32_t index, V3 ps, V
         }
         pdf = prob * vl.pdf_factor;
         Medium_gpu const& g = s.media[vl.medium];
-        V3 const e = g.temperature ? blackbody_emission(g.blackbody, __ldg(g.temperature + voxel)) : lmat.emission;
-        rad        = (__ldg(g.density + voxel) * vl.a_norm) * e;
+        V3 const    e = g.temperature ? blackbody_emission(g.blackbody, __ldg(g.temperature + voxel)) : lmat.emission;
+        float const d = __ldg(g.density + voxel) * (g.scale ? __ldg(g.scale + voxel) : 1.f);
+        rad           = (d * vl.a_norm) * e;
     }
     V3 const    o    = v3(2.f * uvw.x - 1.f, 2.f * uvw.y - 1.f, 2.f * uvw.z - 1.f);
     V3 const    wp   = v3(vl.m0.x * o.x + vl.m0.y * o.y + vl.m0.z * o.z + vl.m0.w,
@@ -1578,9 +1581,11 @@ __device__ int track_grid_emissive(Medium_gpu const& g, shading::Material const&
             float const pn = mn * c;
             float const r1 = rng.uniform();
             if (r1 < pa) {
-                V3 const e = g.temperature ? blackbody_emission(g.blackbody,
-                                                                sample_voxels(g, g.temperature, o + t * d, nearest))
-                                           : m.emission;
+                V3 e = g.temperature ? blackbody_emission(g.blackbody, sample_voxels(g, g.temperature, o + t * d, nearest))
+                                     : m.emission;
+                if (g.scale) {
+                    e = sample_voxels(g, g.scale, o + t * d, nearest) * e;
+                }
                 li    = lw * ((1.f / (mt * pa)) * ma3) * e;
                 lw    = v3(0.f, 0.f, 0.f);
                 t_out = t;
@@ -3474,7 +3479,8 @@ __global__ void k_majorant_cells(float const* __restrict__ density, int nx, int 
 }
 
 // The emission distribution of a density grid whose voxels emit density x emission, or
-// density x the emission at the voxel's temperature (Grid_emission::prepare_sampling,
+// density x the emission at the voxel's temperature, times the second channel of a
+// two-channel density (Grid_emission::prepare_sampling,
 // volumetric_grid.cpp:182-318, built with
 // SU_IBL_MIS_COMPENSATION): voxel weights max(luminance - 0.6 average luminance, 0) (ACEScg
 // luminance) normalised to probabilities, with the cumulative sums over slices, rows and voxels
@@ -3488,7 +3494,7 @@ struct Emission_dist_host {
 };
 
 Emission_dist_host emission_distribution(Density_grid const& g, V3 emission, float const* temperature,
-                                         float4 const* blackbody) {
+                                         float4 const* blackbody, float const* scale) {
     size_t const nx = g.dims[0], ny = g.dims[1], nz = g.dims[2], n = nx * ny * nz;
     auto const   lum = [](double r, double gg, double b) {
         return 0.2722287168 * r + 0.6740817658 * gg + 0.0536895174 * b;
@@ -3498,7 +3504,7 @@ Emission_dist_host emission_distribution(Density_grid const& g, V3 emission, flo
     std::vector<double> w(n);
     double              sum[3] = {0.0, 0.0, 0.0};
     for (size_t v = 0; v < n; ++v) {
-        double const d = g.density[v];
+        double const d = double(g.density[v]) * (scale ? scale[v] : 1.f);
         V3 const     e = temperature ? blackbody_emission(blackbody, temperature[v]) : emission;
         sum[0] += d * e.x;
         sum[1] += d * e.y;
@@ -4132,7 +4138,8 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
                 bool const         hot = gm.temperature != 0;
                 Emission_dist_host d   = emission_distribution(
                     scene.grids[gm.grid], m.emission, hot ? scene.grids[gm.temperature - 1].density : nullptr,
-                    hot ? table.data() : nullptr);
+                    hot ? table.data() : nullptr,
+                    gm.emission_scale != 0 ? scene.grids[gm.emission_scale - 1].density : nullptr);
                 if (!(d.total > 0.0)) {
                     continue;
                 }
@@ -4285,8 +4292,14 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
     SPB_RCUDA(upload(d_->blackbody, tables.data(), tables.size() * sizeof(float4)));
     for (size_t k = 0; k < scene.media.size(); ++k) {
         Grid_medium const& gm = scene.media[k];
-        if (gm.grid >= scene.grids.size() || gm.temperature > scene.grids.size()) {
+        if (gm.grid >= scene.grids.size() || gm.temperature > scene.grids.size() ||
+            gm.emission_scale > scene.grids.size()) {
             error_ = "medium refers to a missing density grid";
+            return SPB_ERROR_ARGUMENT;
+        }
+        if (gm.emission_scale != 0 && !std::equal(scene.grids[gm.grid].dims, scene.grids[gm.grid].dims + 3,
+                                                  scene.grids[gm.emission_scale - 1].dims)) {
+            error_ = "an emission-scale grid must have its density grid's dimensions";
             return SPB_ERROR_ARGUMENT;
         }
         if (gm.temperature != 0 &&
@@ -4314,6 +4327,9 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
         if (gm.temperature != 0) {
             mg.temperature = d_->grid_density[gm.temperature - 1];
             mg.blackbody   = d_->blackbody + 16 * k;
+        }
+        if (gm.emission_scale != 0) {
+            mg.scale = d_->grid_density[gm.emission_scale - 1];
         }
         int const num_cells = cells[0] * cells[1] * cells[2];
         free_ptr(d_->grid_cells[k]);

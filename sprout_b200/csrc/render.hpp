@@ -29,6 +29,9 @@ struct Grid_medium {
     // looked up by temperature over [0, 1.2] (volumetric_grid.cpp:140-160).
     uint32_t temperature    = 0;
     float    blackbody[48]  = {};
+    // A two-channel density's second channel, which scales the emission (Grid_emission,
+    // volumetric_grid.cpp:80-127): 1 + index into Scene_desc::grids, 0 for none.
+    uint32_t emission_scale = 0;
 };
 
 // A mesh in object space, shared by the instances that place it.

@@ -522,7 +522,8 @@ def _look_at(position, target=(0.0, 0.0, 0.0)):
 
 def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -3.2),
            max_bounces: int = 32, min_bounces: int = 4, environment=(0.3, 0.35, 0.4), integrator=None,
-           medium=None, medium_light: bool = False, medium_shape: int = SHAPE_CUBE, temperature_seed=None):
+           medium=None, medium_light: bool = False, medium_shape: int = SHAPE_CUBE, temperature_seed=None,
+           emission_scale_seed=None):
     """A 2 m Cube (built-in, [-1, 1]^3) filled with a density grid (VOLUME_MEDIUM), lit by a
     Sphere light of radius 0.25 (radiance 60) and a uniform Infinite_sphere environment; a
     pinhole camera at `position` looking at the centre with a 40 degree field of view; PTMIS
@@ -531,7 +532,8 @@ def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -
     homogeneous medium; medium_light: the medium's prop is a light too (su_create_light);
     medium_shape: the built-in shape holding the medium (a Sphere has radius 1); temperature_seed:
     give the density grid a temperature grid of its size, 0.9 + 0.3 x fBm of that seed (about
-    4250-5000 K on the emission's black-body scale)."""
+    4250-5000 K on the emission's black-body scale); emission_scale_seed: make the density a
+    two-channel image whose second channel, 0.5 + fBm of that seed, scales the emission."""
     cam = su.su_create_camera_perspective(width, height, VOLUME_FOV)
     su.set_transformation(cam, _look_at(position))
     ptmis = {"min_bounces": min_bounces, "max_bounces": max_bounces}
@@ -542,6 +544,10 @@ def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -
     params = dict(VOLUME_MEDIUM)
     params.update(medium or {})
     if density is not None:
+        if emission_scale_seed is not None:
+            # a two-channel density: the grid, and 0.5 + fBm of that seed scaling the emission
+            scale = 0.5 + fbm_density(density.shape[0], seed=emission_scale_seed)
+            density = np.stack([density, scale.astype(np.float32)], axis=-1)
         params["density"] = {"id": int(su.image(density))}
         if temperature_seed is not None:
             heat = 0.9 + 0.3 * fbm_density(density.shape[0], seed=temperature_seed)

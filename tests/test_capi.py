@@ -68,8 +68,9 @@ def test_c_api_without_gpu_state():
 
 def test_density_images_and_grid_materials():
     """su_create_image ids count from 0; a Volumetric "density" must name a one-channel image;
-    "emission" is taken by homogeneous media and by density grids (Grid_emission), and a
-    "temperature" image of the density's dimensions beside a density grid."""
+    "emission" is taken by homogeneous media and by density grids (Grid_emission), a
+    "temperature" image of the density's dimensions beside a density grid, and a two-channel
+    density (density, emission scale)."""
     import json
 
     import numpy as np
@@ -100,6 +101,9 @@ def test_density_images_and_grid_materials():
         assert su.image(other) == 2
         assert volumetric(density={"id": 0}, temperature={"id": 2}) == capi.SU_RESOURCE_NULL  # other size
         assert volumetric(temperature={"id": 0}) == capi.SU_RESOURCE_NULL  # no density
+        two = np.ones((2, 3, 4, 2), np.float32)  # density and emission scale
+        assert su.image(two) == 3
+        assert volumetric(density={"id": 3}, emission=[1, 1, 1]) == 5
     finally:
         assert su.su_release() == 0
 
