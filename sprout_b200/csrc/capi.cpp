@@ -74,6 +74,8 @@ struct Material_maps {
 struct Grid_ref {
     uint32_t image       = Null;   // density image id, Null for homogeneous media
     uint32_t temperature = Null;   // temperature image id of an emitting grid, or Null
+    uint32_t color       = Null;   // RGBA image id of a colour grid (Grid_color), or Null
+    float    distance    = 1.f;    // attenuation distance (a colour grid's coefficients)
     bool     nearest     = false;  // "sampler": {"filter": "Nearest"}
     bool     repeat      = false;  // "sampler": {"address": "Repeat"}
 };
@@ -472,7 +474,7 @@ int32_t compile_scene() {
             Material const& em = engine->materials[mat];
             bool const emitting_light = e.light && em.type == spb::shading::Type_volume &&
                                         (em.emission.x > 0.f || em.emission.y > 0.f || em.emission.z > 0.f);
-            if (gr.image == Null) {
+            if (gr.image == Null && gr.color == Null) {
                 if (emitting_light) {
                     // the light of an emitting medium is named by its material: one per prop
                     inst.materials[k] = uint32_t(scene.materials.size());
@@ -506,9 +508,18 @@ int32_t compile_scene() {
                 grid_images.push_back(key);
                 return uint32_t(grid_images.size() - 1);
             };
-            gm.grid = grid_of(gr.image, 0);
-            if (engine->images[gr.image].channels == 2) {
-                gm.emission_scale = grid_of(gr.image, 1) + 1;
+            if (gr.image != Null) {
+                gm.grid = grid_of(gr.image, 0);
+                if (engine->images[gr.image].channels == 2) {
+                    gm.emission_scale = grid_of(gr.image, 1) + 1;
+                }
+            } else {
+                // a colour grid: alpha is the density, rgb the colour its coefficients follow
+                gm.grid = grid_of(gr.color, 3);
+                for (uint32_t c = 0; c < 3; ++c) {
+                    gm.color[c] = grid_of(gr.color, c) + 1;
+                }
+                gm.color_distance = gr.distance;
             }
             if (gr.temperature != Null) {
                 // Grid_emission::commit (volumetric_grid.cpp:140-160): the emission times the
@@ -1639,6 +1650,21 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
             }
             grid.temperature = image;
         }
+        if (spb::json::Value const* color = desc.find("color"); color && color->is_object() && grid.image == Null) {
+            // "color": {"id": image} or {"file": ...} without a density: an RGBA grid whose colour
+            // sets the coefficients and whose alpha scales them (Grid_color,
+            // material_provider.cpp:834-840, volumetric_grid.cpp:336-395)
+            spb::json::Value const* id   = color->find("id");
+            spb::json::Value const* file = color->find("file");
+            uint32_t const image = id && id->is_number() ? uint32_t(id->number)
+                                   : (file && file->is_string() ? load_sub_image(resolve(file->string, ""))
+                                                                : Null);
+            if (image >= engine->images.size() || engine->images[image].channels != 4) {
+                log(SU_LOG_ERROR, "su_create_material: a colour grid must name a four-channel image");
+                return Null;
+            }
+            grid.color = image;
+        }
         // "emission" (material_provider.cpp:805-806): the emitted radiance per unit absorption
         // (Material::collision_coefficients_emission, material.cpp:87-89); with a density grid
         // the material is a Grid_emission (material_provider.cpp:823-830), whose absorption
@@ -1670,25 +1696,10 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
         float const distance = float(spb::json::number_or(desc.find("attenuation_distance"), 1.0));
         float const g = std::clamp(float(spb::json::number_or(desc.find("anisotropy"), 0.0)), -0.999f,
                                    0.999f);
-        float const acs[3]  = {ac.x, ac.y, ac.z};
-        float const sscs[3] = {ssc.x, ssc.y, ssc.z};
-        float       mu_a[3];
-        float       mu_s[3];
-        for (int k = 0; k < 3; ++k) {
-            float const ca     = std::clamp(acs[k], 0.01f, 0.991102f);
-            float const mu_t   = -std::log(ca) / distance;
-            float const x      = sscs[k];
-            float const root   = std::sqrt(9.59217f + 41.6808f * x + 17.7126f * x * x);
-            float const factor = std::clamp(4.097125f + 4.20863f * x - root, 0.f, 1.f);
-            float const fsq    = factor * factor;
-            float const pss    = (1.f - fsq) / (1.f - g * fsq);
-            mu_a[k]            = mu_t * (1.f - pss);
-            mu_s[k]            = mu_t - mu_a[k];
-        }
         m.type = spb::shading::Type_volume;
         m.g    = g;
-        m.mu_a = V3{mu_a[0], mu_a[1], mu_a[2]};
-        m.mu_s = V3{mu_s[0], mu_s[1], mu_s[2]};
+        spb::shading::attenuation(ac, ssc, distance, g, m.mu_a, m.mu_s);
+        grid.distance = distance;
     } else {
         log(SU_LOG_ERROR, "su_create_material: unsupported material type " + type);
         return Null;

@@ -155,6 +155,29 @@ constexpr uint32_t Type_light      = 1;
 constexpr uint32_t Type_volume     = 2;  // participating medium inside a closed mesh
 constexpr uint32_t Volume_light_unsampled = 0xFFFFFFFFu;
 
+// Absorption and scattering coefficients of a medium from its attenuation colour, subsurface
+// colour (the multiple-scattering albedo), attenuation distance and anisotropy
+// (attenuation_coefficient and scattering, collision_coefficients.inl:50-71): mu_t from the
+// colour a ray keeps after the distance, split by the single-scattering albedo that gives ssc.
+SPB_HD void attenuation(V3 ac, V3 ssc, float distance, float g, V3& mu_a, V3& mu_s) {
+    float const acs[3] = {ac.x, ac.y, ac.z};
+    float const xs[3]  = {ssc.x, ssc.y, ssc.z};
+    float       a[3], s[3];
+    for (int k = 0; k < 3; ++k) {
+        float const ca     = fminf(fmaxf(acs[k], 0.01f), 0.991102f);
+        float const mu_t   = -logf(ca) / distance;
+        float const x      = xs[k];
+        float const root   = sqrtf(9.59217f + 41.6808f * x + 17.7126f * x * x);
+        float const factor = fminf(fmaxf(4.097125f + 4.20863f * x - root, 0.f), 1.f);
+        float const fsq    = factor * factor;
+        float const pss    = (1.f - fsq) / (1.f - g * fsq);
+        a[k]               = mu_t * (1.f - pss);
+        s[k]               = mu_t - a[k];
+    }
+    mu_a = v3(a[0], a[1], a[2]);
+    mu_s = v3(s[0], s[1], s[2]);
+}
+
 // Henyey-Greenstein phase function of c = dot(wo, wi) (material.inl:15-19).
 SPB_HD float phase_hg(float c, float g) {
     float const gg    = g * g;

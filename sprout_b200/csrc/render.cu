@@ -89,6 +89,11 @@ struct Medium_gpu {
     float4 const* blackbody;
     // A two-channel density's second channel, scaling the emission; null for one channel.
     float const*  scale;
+    // A colour grid (Grid_color): density is its alpha, rgb its colour; null for a density grid.
+    // color_maj: the largest total coefficient any colour gives (-ln 0.01 / distance).
+    float const*  rgb[3];
+    float         color_distance;
+    float         color_maj;
 };
 
 // The emission of a temperature grid's material at temperature x: Grid_emission's table of
@@ -124,6 +129,7 @@ struct Volume_light_gpu {
     uint32_t medium;      // the density-grid medium (index into media) when dist != 0
     float    pdf_factor;  // voxels / largest absorption coefficient (Grid_emission::pdf_factor_)
     V3       a_norm;      // largest absorption coefficient / absorption coefficient (a_norm_)
+    uint32_t color;       // 1: a colour grid (medium), whose absorption at the point sets the radiance
 };
 
 // The 3-D distribution of a density grid's emitted luminance (Grid_emission::prepare_sampling
@@ -1061,6 +1067,9 @@ __device__ __forceinline__ float emission_prob(Emission_dist_gpu const& e, V3 uv
 // grid's factor); its radiance is the medium's absorption times emission
 // (Homogeneous::evaluate_radiance), or for a grid the nearest density times a_norm times the
 // emission (Grid_emission::evaluate_radiance with Filter::Nearest, Pathtracer_MIS::evaluate_light).
+__device__ void color_coefficients(Medium_gpu const& g, V3 uvw, bool nearest, float anisotropy, V3& mu_a,
+                                   V3& mu_s);
+
 __device__ bool sample_volume_light(Scene_gpu const& s, uint32_t index, V3 ps, V3 n, bool total_sphere,
                                     float pick_pdf, float r1, float r2, float r3, Light_sample& ls) {
     Volume_light_gpu const  vl   = s.volume_lights[index];
@@ -1079,6 +1088,12 @@ __device__ bool sample_volume_light(Scene_gpu const& s, uint32_t index, V3 ps, V
         V3 const    e = g.temperature ? blackbody_emission(g.blackbody, __ldg(g.temperature + voxel)) : lmat.emission;
         float const d = __ldg(g.density + voxel) * (g.scale ? __ldg(g.scale + voxel) : 1.f);
         rad           = (d * vl.a_norm) * e;
+    } else if (vl.color != 0) {
+        // a colour grid's Volume light: its absorption at the point, nearest voxel
+        // (Grid_color::evaluate_radiance with Filter::Nearest, volumetric_grid.cpp:336-343)
+        V3 ma, ms;
+        color_coefficients(s.media[vl.medium], uvw, true, lmat.g, ma, ms);
+        rad = ma * lmat.emission;
     }
     V3 const    o    = v3(2.f * uvw.x - 1.f, 2.f * uvw.y - 1.f, 2.f * uvw.z - 1.f);
     V3 const    wp   = v3(vl.m0.x * o.x + vl.m0.y * o.y + vl.m0.z * o.z + vl.m0.w,
@@ -1344,6 +1359,38 @@ __device__ __forceinline__ float sample_density(Medium_gpu const& g, V3 uvw, boo
     return sample_voxels(g, g.density, uvw, nearest);
 }
 
+// A colour grid's coefficients at uvw (Grid_color::collision_coefficients,
+// volumetric_grid.cpp:345-352): alpha x attenuation(rgb, rgb, distance, anisotropy).
+__device__ void color_coefficients(Medium_gpu const& g, V3 uvw, bool nearest, float anisotropy, V3& mu_a,
+                                   V3& mu_s) {
+    float const alpha = sample_voxels(g, g.density, uvw, nearest);
+    V3 const    c     = v3(sample_voxels(g, g.rgb[0], uvw, nearest), sample_voxels(g, g.rgb[1], uvw, nearest),
+                           sample_voxels(g, g.rgb[2], uvw, nearest));
+    shading::attenuation(c, c, g.color_distance, anisotropy, mu_a, mu_s);
+    mu_a = alpha * mu_a;
+    mu_s = alpha * mu_s;
+}
+
+// Coefficients of a grid medium at uvw: density x the material's (mu_s already scaled by the
+// similarity relation), or a colour grid's with its scattering scaled by srs.
+__device__ __forceinline__ void grid_coefficients(Medium_gpu const& g, shading::Material const& m, V3 mu_s,
+                                                  float srs, V3 uvw, bool nearest, V3& ma, V3& ms) {
+    if (g.rgb[0]) {
+        color_coefficients(g, uvw, nearest, m.g, ma, ms);
+        ms = srs * ms;
+    } else {
+        float const den = sample_density(g, uvw, nearest);
+        ma              = den * m.mu_a;
+        ms              = den * mu_s;
+    }
+}
+
+// Majorant of the total coefficient per unit density (the majorant cells hold the density's
+// maximum): the material's, or a colour grid's bound over every colour.
+__device__ __forceinline__ float grid_majorant(Medium_gpu const& g, shading::Material const& m, V3 mu_s, float srs) {
+    return g.rgb[0] ? g.color_maj * fmaxf(srs, 1.f) : shading::max_component(m.mu_a) + shading::max_component(mu_s);
+}
+
 // A material texture at uv (Nearest_2D / Linear_2D, texture_sampler.cpp:14-121): uv scaled,
 // wrapped or clamped, then the texel it falls in, or the bilinear blend of the four texels
 // around it (texel centres at half-integer positions); nearest overrides the filter.
@@ -1491,7 +1538,7 @@ __device__ bool track_grid(Medium_gpu const& g, shading::Material const& m, floa
     V3 const    o     = to_texture(g, ro);
     V3 const    d     = to_texture_dir(g, rd);
     V3 const    mu_s  = srs * m.mu_s;
-    float const maj_t = shading::max_component(m.mu_a) + shading::max_component(mu_s);
+    float const maj_t = grid_majorant(g, m, mu_s, srs);
     lw                = v3(1.f, 1.f, 1.f);
     int  steps        = 0;
     bool scattered    = false;
@@ -1506,9 +1553,8 @@ __device__ bool track_grid(Medium_gpu const& g, shading::Material const& m, floa
             if (t > tb) {
                 return false;
             }
-            float const den  = sample_density(g, o + t * d, nearest);
-            V3 const    ma   = den * m.mu_a;
-            V3 const    ms3  = den * mu_s;
+            V3 ma, ms3;
+            grid_coefficients(g, m, mu_s, srs, o + t * d, nearest, ma, ms3);
             V3 const    mu_n = v3(mt - (ma.x + ms3.x), mt - (ma.y + ms3.y), mt - (ma.z + ms3.z));
             float const ms   = ((ms3.x * lw.x) + (ms3.y * lw.y) + (ms3.z * lw.z)) * (1.f / 3.f);
             float const mn   = ((mu_n.x * lw.x) + (mu_n.y * lw.y) + (mu_n.z * lw.z)) * (1.f / 3.f);
@@ -1547,7 +1593,7 @@ __device__ int track_grid_emissive(Medium_gpu const& g, shading::Material const&
     V3 const    o     = to_texture(g, ro);
     V3 const    d     = to_texture_dir(g, rd);
     V3 const    mu_s  = srs * m.mu_s;
-    float const maj_t = shading::max_component(m.mu_a) + shading::max_component(mu_s);
+    float const maj_t = grid_majorant(g, m, mu_s, srs);
     lw                = v3(1.f, 1.f, 1.f);
     li                = v3(0.f, 0.f, 0.f);
     int steps         = 0;
@@ -1563,9 +1609,8 @@ __device__ int track_grid_emissive(Medium_gpu const& g, shading::Material const&
             if (t > tb) {
                 return false;
             }
-            float const den  = sample_density(g, o + t * d, nearest);
-            V3 const    ma3  = den * m.mu_a;
-            V3 const    ms3  = den * mu_s;
+            V3 ma3, ms3;
+            grid_coefficients(g, m, mu_s, srs, o + t * d, nearest, ma3, ms3);
             V3 const    mu_n = v3(mt - (ma3.x + ms3.x), mt - (ma3.y + ms3.y), mt - (ma3.z + ms3.z));
             float const ma   = ((ma3.x * lw.x) + (ma3.y * lw.y) + (ma3.z * lw.z)) * (1.f / 3.f);
             float const ms   = ((ms3.x * lw.x) + (ms3.y * lw.y) + (ms3.z * lw.z)) * (1.f / 3.f);
@@ -1623,8 +1668,9 @@ __device__ bool transmit_grid(Medium_gpu const& g, shading::Material const& m, f
     V3 const    o     = to_texture(g, ro);
     V3 const    d     = to_texture_dir(g, rd);
     V3 const    mu_s  = srs * m.mu_s;
-    float const maj_t = shading::max_component(m.mu_a) + shading::max_component(mu_s);
-    float const min_t = shading::min_component(m.mu_a) + shading::min_component(mu_s);
+    float const maj_t = grid_majorant(g, m, mu_s, srs);
+    // a colour grid has no minorant here: plain ratio tracking
+    float const min_t = g.rgb[0] ? 0.f : shading::min_component(m.mu_a) + shading::min_component(mu_s);
     int  steps        = 0;
     bool blocked      = false;
     walk_cells(g, o, d, t0, t1, [&](float2 cell, float ta, float tb) {
@@ -1652,8 +1698,14 @@ __device__ bool transmit_grid(Medium_gpu const& g, shading::Material const& m, f
             if (t > tb) {
                 return false;
             }
-            float const den = sample_density(g, o + t * d, nearest);
-            V3 const    mt3 = den * (m.mu_a + mu_s);
+            V3 mt3;
+            if (g.rgb[0]) {
+                V3 ma, ms;
+                color_coefficients(g, o + t * d, nearest, m.g, ma, ms);
+                mt3 = ma + srs * ms;
+            } else {
+                mt3 = sample_density(g, o + t * d, nearest) * (m.mu_a + mu_s);
+            }
             w = v3(w.x * ((mr - (mt3.x - cm)) * imr), w.y * ((mr - (mt3.y - cm)) * imr),
                    w.z * ((mr - (mt3.z - cm)) * imr));
             if (all_below_abort(w)) {
@@ -3854,7 +3906,8 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
                 bool const volume = sm.type == shading::Type_volume;
                 d_->has_media |= volume;
                 d_->spectral_scene &= sm.type == shading::Type_light ||
-                                      (volume && !(sm.emission.x > 0.f || sm.emission.y > 0.f || sm.emission.z > 0.f));
+                                      (volume && !(sm.emission.x > 0.f || sm.emission.y > 0.f || sm.emission.z > 0.f) &&
+                                       !(sm.medium != 0 && scene.media[sm.medium - 1].color[0] != 0));
                 tri_class.push_back(volume ? Class_boundary : Class_surface);
                 if (in.light && sm.type == shading::Type_light) {
                     double a[3], b[3], c[3];
@@ -4125,7 +4178,16 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
             // volumetric_material.cpp:40-44, or the grid's mean of density x emission)
             double average[3] = {double(m.mu_a.x) * m.emission.x, double(m.mu_a.y) * m.emission.y,
                                  double(m.mu_a.z) * m.emission.z};
-            if (m.medium != 0) {
+            if (m.medium != 0 && scene.media[m.medium - 1].color[0] != 0) {
+                // a colour grid: uniform points (a Volume light, not an image), its power from
+                // the material's default coefficients of 0.5 (Grid_color's cc_,
+                // volumetric_grid.cpp:320-324, through Material::prepare_sampling)
+                vl.medium = m.medium - 1;
+                vl.color  = 1;
+                for (int k = 0; k < 3; ++k) {
+                    average[k] = 0.5 * double((&m.emission.x)[k]);
+                }
+            } else if (m.medium != 0) {
                 Grid_medium const& gm = scene.media[m.medium - 1];
                 double const       maj_a = std::max({double(m.mu_a.x), double(m.mu_a.y), double(m.mu_a.z)});
                 if (!(maj_a > 0.0)) {
@@ -4330,6 +4392,19 @@ int32_t Renderer::set_scene(Scene_desc const& scene, uint32_t num_threads) {
         }
         if (gm.emission_scale != 0) {
             mg.scale = d_->grid_density[gm.emission_scale - 1];
+        }
+        if (gm.color[0] != 0) {
+            for (int c = 0; c < 3; ++c) {
+                if (gm.color[c] == 0 || gm.color[c] > scene.grids.size() ||
+                    !std::equal(scene.grids[gm.grid].dims, scene.grids[gm.grid].dims + 3,
+                                scene.grids[gm.color[c] - 1].dims)) {
+                    error_ = "a colour grid's channels must share its dimensions";
+                    return SPB_ERROR_ARGUMENT;
+                }
+                mg.rgb[c] = d_->grid_density[gm.color[c] - 1];
+            }
+            mg.color_distance = gm.color_distance;
+            mg.color_maj      = -std::log(0.01f) / gm.color_distance;
         }
         int const num_cells = cells[0] * cells[1] * cells[2];
         free_ptr(d_->grid_cells[k]);
@@ -4765,8 +4840,8 @@ int32_t Renderer::render(uint32_t first_sample, uint32_t num_samples) {
         // the persistent spectral kernel keeps its paths in registers: no wave buffers; its
         // guiding is the phase guide at medium vertices
         if (!d_->spectral_scene || d_->instanced) {
-            error_ = "spectral rendering takes scenes of participating media (not emissive), emitters and the "
-                     "environment, in one tree";
+            error_ = "spectral rendering takes scenes of homogeneous or density-grid media (not emitting), "
+                     "emitters and the environment, in one tree";
             return SPB_ERROR_ARGUMENT;
         }
         if (!d_->counters) {

@@ -32,6 +32,11 @@ struct Grid_medium {
     // A two-channel density's second channel, which scales the emission (Grid_emission,
     // volumetric_grid.cpp:80-127): 1 + index into Scene_desc::grids, 0 for none.
     uint32_t emission_scale = 0;
+    // A colour grid (Grid_color, volumetric_grid.cpp:336-395): `grid` is its alpha, these its
+    // red, green and blue (1 + index into Scene_desc::grids each, 0 for a density grid); the
+    // coefficients are alpha x attenuation(rgb, rgb, color_distance, anisotropy).
+    uint32_t color[3]       = {0, 0, 0};
+    float    color_distance = 1.f;
 };
 
 // A mesh in object space, shared by the instances that place it.

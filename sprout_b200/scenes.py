@@ -523,7 +523,7 @@ def _look_at(position, target=(0.0, 0.0, 0.0)):
 def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -3.2),
            max_bounces: int = 32, min_bounces: int = 4, environment=(0.3, 0.35, 0.4), integrator=None,
            medium=None, medium_light: bool = False, medium_shape: int = SHAPE_CUBE, temperature_seed=None,
-           emission_scale_seed=None):
+           emission_scale_seed=None, color_grid_seed=None):
     """A 2 m Cube (built-in, [-1, 1]^3) filled with a density grid (VOLUME_MEDIUM), lit by a
     Sphere light of radius 0.25 (radiance 60) and a uniform Infinite_sphere environment; a
     pinhole camera at `position` looking at the centre with a 40 degree field of view; PTMIS
@@ -533,7 +533,9 @@ def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -
     medium_shape: the built-in shape holding the medium (a Sphere has radius 1); temperature_seed:
     give the density grid a temperature grid of its size, 0.9 + 0.3 x fBm of that seed (about
     4250-5000 K on the emission's black-body scale); emission_scale_seed: make the density a
-    two-channel image whose second channel, 0.5 + fBm of that seed, scales the emission."""
+    two-channel image whose second channel, 0.5 + fBm of that seed, scales the emission;
+    color_grid_seed: a colour grid instead (RGBA, Grid_color): the density as alpha, each colour
+    channel 0.35 + 0.6 x fBm of seeds from that one."""
     cam = su.su_create_camera_perspective(width, height, VOLUME_FOV)
     su.set_transformation(cam, _look_at(position))
     ptmis = {"min_bounces": min_bounces, "max_bounces": max_bounces}
@@ -543,7 +545,11 @@ def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -
     su.su_create_defaults()
     params = dict(VOLUME_MEDIUM)
     params.update(medium or {})
-    if density is not None:
+    if density is not None and color_grid_seed is not None:
+        n = density.shape[0]
+        rgb = [0.35 + 0.6 * fbm_density(n, seed=color_grid_seed + k) for k in range(3)]
+        params["color"] = {"id": int(su.image(np.stack(rgb + [density], axis=-1).astype(np.float32)))}
+    elif density is not None:
         if emission_scale_seed is not None:
             # a two-channel density: the grid, and 0.5 + fBm of that seed scaling the emission
             scale = 0.5 + fbm_density(density.shape[0], seed=emission_scale_seed)

@@ -87,6 +87,11 @@ CASES = {
     # a two-channel density: the second channel scales the emission (camera and light)
     "volume64_glow2_light": (64, 64, 2048, {"scene": "volume", "medium": GLOW, "medium_light": True,
                                             "emission_scale_seed": 11}, scenes.fbm_density(32)),
+    # a colour grid (Grid_color): RGBA voxels, the coefficients from the colour times alpha
+    "volume64_color": (64, 64, 2048, {"scene": "volume", "color_grid_seed": 21}, scenes.fbm_density(32)),
+    # ... emitting, as a light (a Volume light: uniform points, the absorption at the point)
+    "volume64_color_glow_light": (64, 64, 2048, {"scene": "volume", "color_grid_seed": 21, "medium": GLOW,
+                                                 "medium_light": True}, scenes.fbm_density(32)),
     # the emitting grid in a Sphere as a light: next-event estimation cannot sample its inside,
     # so its emission counts on every segment
     "volume64_glow_sphere_light": (64, 64, 2048, {"scene": "volume", "medium": GLOW, "medium_light": True,
@@ -117,7 +122,8 @@ PATH = HERE / "cornell_reference.npz"
 # 0.6 %.
 BLOCK = {"wavefront96": 16, "volume64": 16, "doorway96": 16, "doorway320": 20, "volume64_glow": 16,
          "volume64_glow_light": 16, "volume64_glow_color_light": 16, "volume64_haze_light": 16,
-         "volume64_glow_sphere_light": 16, "volume64_fire_light": 16, "volume64_glow2_light": 16}
+         "volume64_glow_sphere_light": 16, "volume64_fire_light": 16, "volume64_glow2_light": 16,
+         "volume64_color": 16, "volume64_color_glow_light": 16}
 
 
 def build(su, w, h, spp, kwargs, density=None):

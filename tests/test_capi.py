@@ -69,8 +69,9 @@ def test_c_api_without_gpu_state():
 def test_density_images_and_grid_materials():
     """su_create_image ids count from 0; a Volumetric "density" must name a one-channel image;
     "emission" is taken by homogeneous media and by density grids (Grid_emission), a
-    "temperature" image of the density's dimensions beside a density grid, and a two-channel
-    density (density, emission scale)."""
+    "temperature" image of the density's dimensions beside a density grid, a two-channel
+    density (density, emission scale), and a four-channel "color" image without a density (a
+    colour grid)."""
     import json
 
     import numpy as np
@@ -104,6 +105,11 @@ def test_density_images_and_grid_materials():
         two = np.ones((2, 3, 4, 2), np.float32)  # density and emission scale
         assert su.image(two) == 3
         assert volumetric(density={"id": 3}, emission=[1, 1, 1]) == 5
+        rgba = np.full((2, 3, 4, 4), 0.5, np.float32)  # a colour grid (Grid_color)
+        assert su.image(rgba) == 4
+        assert volumetric(color={"id": 4}, attenuation_distance=0.1) == 6
+        assert volumetric(color={"id": 3}) == capi.SU_RESOURCE_NULL  # two channels
+        assert volumetric(color={"id": 4}, density={"id": 0}) == 7  # the density wins, as in the reference
     finally:
         assert su.su_release() == 0
 

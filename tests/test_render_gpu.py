@@ -83,7 +83,8 @@ CASES = ["cornell64_sub3", "cornell128_sub6", "cornell64_medium", "cornell64_emi
          "cornell64_lights", "wavefront96", "builtins96", "builtins96_backdrop", "volume64",
          "doorway96", "take_room96", "cornell512", "doorway320", "textured96",
          "volume64_glow", "volume64_glow_light", "volume64_glow_color_light", "volume64_haze_light",
-         "volume64_glow_sphere_light", "volume64_fire_light", "volume64_glow2_light"]
+         "volume64_glow_sphere_light", "volume64_fire_light", "volume64_glow2_light", "volume64_color",
+         "volume64_color_glow_light"]
 
 
 @pytest.mark.parametrize("name", CASES)
