@@ -270,14 +270,16 @@ class ScriptRecorder:
         return 1000 + self.n["material"] - 1
 
     def image(self, pixels):
-        """su_create_image of a float32 array (depth, height, width) or (height, width): one
-        channel; (depth, height, width, channels): several.  Returns the image id the reference
-        assigns (images are numbered from 0)."""
-        a = np.ascontiguousarray(pixels, np.float32)
+        """su_create_image of an array (depth, height, width) or (height, width): one channel;
+        (depth, height, width, channels): several; uint8 as Byte, anything else as Float.
+        Returns the image id the reference assigns (images are numbered from 0)."""
+        a = np.ascontiguousarray(pixels)
+        kind = 0 if a.dtype == np.uint8 else 2
+        a = a if a.dtype == np.uint8 else a.astype(np.float32)
         c = a.shape[3] if a.ndim == 4 else 1
         d, h, w = (a.shape[:3] if a.ndim >= 3 else (1,) + a.shape)
         off = self._blob(a)
-        self.lines.append(f"image 2 {c} {w} {h} {d} {off}")
+        self.lines.append(f"image {kind} {c} {w} {h} {d} {off}")
         self.n["image"] += 1
         return self.n["image"] - 1
 

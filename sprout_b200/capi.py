@@ -95,12 +95,15 @@ class SuLibrary:
             idx.ctypes.data, 0 if prt is None else prt.shape[0], None if prt is None else prt.ctypes.data)
 
     def image(self, pixels):
-        """su_create_image of float pixels: (depth, height, width) or (height, width) for one
-        channel, (depth, height, width, channels) for several."""
-        a = np.ascontiguousarray(pixels, np.float32)
+        """su_create_image of pixels (depth, height, width) or (height, width) for one channel,
+        (depth, height, width, channels) for several: uint8 as Byte, anything else as Float."""
+        a = np.ascontiguousarray(pixels)
+        kind, size = (0, 1) if a.dtype == np.uint8 else (2, 4)
+        a = a if a.dtype == np.uint8 else a.astype(np.float32)
+        self._keep.append(a)
         c = a.shape[3] if a.ndim == 4 else 1
         d, h, w = a.shape[:3] if a.ndim >= 3 else (1,) + a.shape
-        return self.lib.su_create_image(2, c, w, h, d, 0, 4 * c, a.ctypes.data)
+        return self.lib.su_create_image(kind, c, w, h, d, 0, size * c, a.ctypes.data)
 
     def image2d(self, pixels):
         """su_create_image of a 2-D image (height, width, channels): uint8 pixels as Byte (sRGB

@@ -485,8 +485,10 @@ int32_t compile_scene() {
             spb::render::Grid_medium gm;
             // index of the grid of an image's channel in the scene (each uploaded once; the
             // channels of a two-channel image as separate grids)
+            // (channels 4 to 6: a byte colour image's red, green and blue decoded from sRGB to
+            // linear ACEScg, as the reference's Byte4_sRGB texture reads them)
             auto const grid_of = [&](uint32_t image, uint32_t channel) {
-                uint64_t const key = (uint64_t(image) << 2) | channel;
+                uint64_t const key = (uint64_t(image) << 3) | channel;
                 auto const     gi  = std::find(grid_images.begin(), grid_images.end(), key);
                 if (gi != grid_images.end()) {
                     return uint32_t(gi - grid_images.begin());
@@ -500,7 +502,17 @@ int32_t compile_scene() {
                     size_t const n = size_t(img.dims[0]) * img.dims[1] * img.dims[2];
                     grid_channels.emplace_back(n);
                     for (size_t v = 0; v < n; ++v) {
-                        grid_channels.back()[v] = img.pixels[v * img.channels + channel];
+                        if (channel < 4) {
+                            grid_channels.back()[v] = img.pixels[v * img.channels + channel];
+                            continue;
+                        }
+                        float rgb[3];
+                        for (int k = 0; k < 3; ++k) {
+                            float const e = img.pixels[v * img.channels + k];
+                            rgb[k] = e <= 0.04045f ? e / 12.92f : std::pow((e + 0.055f) / 1.055f, 2.4f);
+                        }
+                        V3 const ap1 = srgb_to_ap1(V3{rgb[0], rgb[1], rgb[2]});
+                        grid_channels.back()[v] = channel == 4 ? ap1.x : (channel == 5 ? ap1.y : ap1.z);
                     }
                     g.density = grid_channels.back().data();
                 }
@@ -517,7 +529,7 @@ int32_t compile_scene() {
                 // a colour grid: alpha is the density, rgb the colour its coefficients follow
                 gm.grid = grid_of(gr.color, 3);
                 for (uint32_t c = 0; c < 3; ++c) {
-                    gm.color[c] = grid_of(gr.color, c) + 1;
+                    gm.color[c] = grid_of(gr.color, 4 + c) + 1;
                 }
                 gm.color_distance = gr.distance;
             }
@@ -1663,7 +1675,15 @@ SU_LIBRARY_API uint32_t su_create_material(char const* string) {
                 log(SU_LOG_ERROR, "su_create_material: a colour grid must name a four-channel image");
                 return Null;
             }
-            grid.color = image;
+            if (engine->images[image].encoded_bytes) {
+                grid.color = image;
+            } else {
+                // the reference reads 3-D colour only from four-channel byte images (sRGB and
+                // alpha, Texture::at_4, texture.cpp:320-338); any other image is not a texture
+                // there (texture_provider.cpp:17-116), and the material is homogeneous
+                log(SU_LOG_WARNING, "su_create_material: a colour grid takes a four-channel byte image; "
+                                    "rendering the homogeneous medium, as the reference does");
+            }
         }
         // "emission" (material_provider.cpp:805-806): the emitted radiance per unit absorption
         // (Material::collision_coefficients_emission, material.cpp:87-89); with a density grid

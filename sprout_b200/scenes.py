@@ -534,8 +534,9 @@ def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -
     give the density grid a temperature grid of its size, 0.9 + 0.3 x fBm of that seed (about
     4250-5000 K on the emission's black-body scale); emission_scale_seed: make the density a
     two-channel image whose second channel, 0.5 + fBm of that seed, scales the emission;
-    color_grid_seed: a colour grid instead (RGBA, Grid_color): the density as alpha, each colour
-    channel 0.35 + 0.6 x fBm of seeds from that one."""
+    color_grid_seed: a colour grid instead (Grid_color, from a four-channel byte image as the
+    reference takes it: sRGB colour and alpha): the density as alpha, each colour channel
+    0.35 + 0.6 x fBm of seeds from that one."""
     cam = su.su_create_camera_perspective(width, height, VOLUME_FOV)
     su.set_transformation(cam, _look_at(position))
     ptmis = {"min_bounces": min_bounces, "max_bounces": max_bounces}
@@ -548,7 +549,8 @@ def volume(su, width: int, height: int, spp: int, density, position=(3.0, 2.0, -
     if density is not None and color_grid_seed is not None:
         n = density.shape[0]
         rgb = [0.35 + 0.6 * fbm_density(n, seed=color_grid_seed + k) for k in range(3)]
-        params["color"] = {"id": int(su.image(np.stack(rgb + [density], axis=-1).astype(np.float32)))}
+        rgba = np.rint(255.0 * np.clip(np.stack(rgb + [density], axis=-1), 0.0, 1.0)).astype(np.uint8)
+        params["color"] = {"id": int(su.image(rgba))}
     elif density is not None:
         if emission_scale_seed is not None:
             # a two-channel density: the grid, and 0.5 + fBm of that seed scaling the emission

@@ -70,8 +70,8 @@ def test_density_images_and_grid_materials():
     """su_create_image ids count from 0; a Volumetric "density" must name a one-channel image;
     "emission" is taken by homogeneous media and by density grids (Grid_emission), a
     "temperature" image of the density's dimensions beside a density grid, a two-channel
-    density (density, emission scale), and a four-channel "color" image without a density (a
-    colour grid)."""
+    density (density, emission scale), and a four-channel byte "color" image without a density
+    (a colour grid; a float one leaves the medium homogeneous, as in the reference)."""
     import json
 
     import numpy as np
@@ -105,11 +105,14 @@ def test_density_images_and_grid_materials():
         two = np.ones((2, 3, 4, 2), np.float32)  # density and emission scale
         assert su.image(two) == 3
         assert volumetric(density={"id": 3}, emission=[1, 1, 1]) == 5
-        rgba = np.full((2, 3, 4, 4), 0.5, np.float32)  # a colour grid (Grid_color)
+        rgba = np.full((2, 3, 4, 4), 128, np.uint8)  # a colour grid (Grid_color): sRGB bytes and alpha
         assert su.image(rgba) == 4
         assert volumetric(color={"id": 4}, attenuation_distance=0.1) == 6
         assert volumetric(color={"id": 3}) == capi.SU_RESOURCE_NULL  # two channels
         assert volumetric(color={"id": 4}, density={"id": 0}) == 7  # the density wins, as in the reference
+        floats = np.full((2, 3, 4, 4), 0.5, np.float32)  # not a colour texture in the reference
+        assert su.image(floats) == 5
+        assert volumetric(color={"id": 5}) == 8  # homogeneous, with a warning
     finally:
         assert su.su_release() == 0
 
