@@ -197,7 +197,7 @@ def measure_phase_guiding(side=256, spp=128, ref_spp=8192, fractions=(0.5,)):
     return out
 
 
-def measure_volume(views=4, spp=128, cpu_reference=False, batch=True, spectral=True):
+def measure_volume(views=4, spp=128, cpu_reference=False, batch=True, spectral=True, density_side=256):
     """The heterogeneous-volume workload: the first `views` of scenes.volume_views() (seeded
     camera positions, image sides U[256, 1024]) of one scene, built and uploaded once; each
     view moves the camera and sets its resolution, then renders one frame.  Samples/s over the
@@ -206,10 +206,11 @@ def measure_volume(views=4, spp=128, cpu_reference=False, batch=True, spectral=T
     views are also rendered together in one spb_render_views call (after one untimed call),
     timed on the device and end to end (the call, with every view's image copied to the host).
     With spectral, the same batch once more in the hero-wavelength spectral mode (4 wavelengths
-    per path in [380, 720] nm; every view and sample in one persistent launch)."""
+    per path in [380, 720] nm; every view and sample in one persistent launch).  density_side:
+    the density grid's side (256 for the workload; smaller for profiling runs)."""
     lib = _lib.load()
     stats = _lib.RenderStats()
-    density = scenes.fbm_density(256)
+    density = scenes.fbm_density(density_side)
     chosen = scenes.volume_views()[:views]
     samples, seconds, rays, wall = 0, 0.0, 0, 0.0
     su = capi.SuLibrary()
@@ -260,7 +261,8 @@ def measure_volume(views=4, spp=128, cpu_reference=False, batch=True, spectral=T
                                     f"all {views} views and samples in one persistent launch"}
     finally:
         su.su_release()
-    out = {"workload": "volume", "config": f"{VOLUME_CONFIG}, {views} of 64 views (sides "
+    grid = "" if density_side == 256 else f" [density grid {density_side}^3 instead of 256^3]"
+    out = {"workload": "volume", "config": f"{VOLUME_CONFIG}{grid}, {views} of 64 views (sides "
                                            f"{[v[1] for v in chosen]}), {spp} spp",
            "msamples_s": round(samples / seconds / 1e6, 3), "mrays_s": round(rays / seconds / 1e6, 3),
            "device_seconds": round(seconds, 3),
@@ -460,6 +462,7 @@ def main():
                    help="doorway: one frame of the guiding workload (plain MIS, or --guided)")
     p.add_argument("--guided", action="store_true", help="doorway: learned path guiding")
     p.add_argument("--views", type=int, default=4, help="volume workload: number of views")
+    p.add_argument("--density", type=int, default=256, help="volume workload: the density grid's side")
     p.add_argument("--width", type=int)
     p.add_argument("--height", type=int)
     p.add_argument("--spp", type=int)
@@ -468,7 +471,7 @@ def main():
     p.add_argument("--cpu-reference", action="store_true")
     a = p.parse_args()
     if a.scene == "volume":
-        print(json.dumps(measure_volume(a.views, a.spp or 128, a.cpu_reference)))
+        print(json.dumps(measure_volume(a.views, a.spp or 128, a.cpu_reference, density_side=a.density)))
     elif a.scene == "guiding":
         print(json.dumps(measure_guiding(a.width or 1280, a.height or 720)))
     elif a.scene == "doorway":
